@@ -1,0 +1,360 @@
+"""Benchmark of the implicit soft-body step (PhysiK's World::Step on the GPU).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload block128|beam64|cube8|beam32] [--precision mixed|fp32|fp64]
+
+One JSON line on rank 0.  A "step" is one PHYSIK_Step (one implicit-Euler substep:
+per-tet corotated FEM, assembly of M + dt^2 K and its rhs, block-Jacobi PCG,
+integration) of the whole body.
+
+* value   -- steps/s with the state resident on the GPU, K steps timed with CUDA
+             events on the world's stream (max over ranks).
+* e2e     -- the same steps through the C ABI with host buffers: every step uploads
+             positions and velocities from pinned host memory (PHYSIK_B200_SetNodeStates),
+             steps, and reads them back (PHYSIK_B200_GetNodeStates); wall clock.
+* roofline-- the cooperative PCG kernel: algorithmic bytes per launch
+             (iterations x (40U + 4(n+1) + 24n + 132n) in FP32 storage,
+              iterations x (76U + 4(n+1) + 48n + 264n) in FP64) over its mean device time.
+* cpu_baseline -- the reference compiled from its own sources (oracle/_ref, FP32,
+             one thread: the reference is single-threaded), bounded sample of the same
+             workload.
+
+--impl reference times that reference CPU path alone on the same workload and prints
+the same line with "impl": "reference".  Multi-GPU (torchrun): a single body does not
+shard, so each rank runs an independent replica ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "implicit steps/s & PCG SpMV HBM GB/s, mixed vs FP64 GPU at ≤1e-5 rel err"
+
+WORKLOADS = {
+    "block128": (4, "block128x64x64: 545,025 vertices, 3,145,728 Kuhn tets, bottom pinned, E=5e5 nu=0.4, "
+                    "dt=1/60, CG tol 1e-6 / 100 iterations"),
+    "beam64": (2, "beam64x16x16: 18,785 vertices, 98,304 Kuhn tets, x=0 pinned, E=1e6 nu=0.45, dt=1/120, "
+                  "CG tol 1e-6 / 100 iterations"),
+    "cube8": (1, "cube8: 729 vertices, 3,072 Kuhn tets, jitter 0.1h, x=0 pinned, E=1e5 nu=0.3, dt=1/60"),
+    "beam32": (5, "beam32x8x8: 2,673 vertices, 12,288 Kuhn tets, per-element E, x=0 pinned, dt=1/60"),
+}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_iteration():
+    """DRAM bytes per PCG iteration from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "pcg_dram_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self, under_load_only=True):
+        if self.proc is None or self.file is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[4:]))
+                except ValueError:
+                    continue
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = np.array([r[0] for r in rows])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for n, v in zip(names, r[3][1:]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(r[1] for r in rows)),
+                "power_w_max": float(max(r[2] for r in rows)), "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def pcg_bytes_per_iteration(n, nnz, precision):
+    if precision == "fp64":
+        return 76 * nnz + 4 * (n + 1) + 48 * n + 264 * n
+    return 40 * nnz + 4 * (n + 1) + 24 * n + 132 * n
+
+
+def cpu_reference_sample(scene, budget_s=45.0, max_steps=None):
+    """Time the reference (FP32 build of its own sources) on the same workload.
+    One untimed step (it builds the component pattern), then timed steps until the
+    budget is spent (at least one)."""
+    from oracle import pyoracle as po
+
+    if not po.reference_available("f32"):
+        return None
+    t0 = time.perf_counter()
+    ref = po.Reference(scene, "f32")
+    setup = time.perf_counter() - t0
+    ref.step()
+    times = []
+    while True:
+        t = time.perf_counter()
+        if ref.step() != 0:
+            raise RuntimeError("reference step failed")
+        times.append(time.perf_counter() - t)
+        if sum(times) >= budget_s or (max_steps and len(times) >= max_steps):
+            break
+    stats = ref.cg_stats()
+    return dict(steps=len(times), seconds=float(sum(times)), steps_per_s=len(times) / sum(times),
+                setup_s=setup, cg_iterations=stats["iterations"])
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def dist_setup(gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return rank, world, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, value, local):
+    if pg is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_ours(args, scene, rank, world, local, pg):
+    import torch
+
+    from physik_b200 import _lib
+    from physik_b200.world import SimWorld
+
+    torch.cuda.set_device(local)
+    w = SimWorld(scene, precision=args.precision, device=local)
+    n_nodes = w.node_count
+    w.step()  # builds and uploads the scene
+    w.synchronize()
+    rs, col, _, _ = w.pattern()
+    n, nnz = len(rs) - 1, len(col)
+    stream = torch.cuda.ExternalStream(w.stream(), device=f"cuda:{local}")
+
+    for _ in range(args.warmup):
+        w.step()
+    w.synchronize()
+
+    # --- device-resident timed region -------------------------------------
+    w.enable_timing(True)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(pg)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            w.step()
+        stop.record(stream)
+        stop.synchronize()
+        torch.cuda.synchronize()
+    barrier(pg)
+    elapsed_ms = max_over_ranks(pg, start.elapsed_time(stop), local)
+    tm = w.timings()
+    stats = w.cg_stats()
+    clock = clocks.summary()
+
+    # --- end to end through the C ABI with pinned host buffers ------------
+    hx = torch.empty((n_nodes, 3), dtype=torch.float32, pin_memory=True).numpy()
+    hv = torch.empty((n_nodes, 3), dtype=torch.float32, pin_memory=True).numpy()
+    x0, v0 = w.state()
+    hx[:] = x0
+    hv[:] = v0
+    X = _lib.PX
+    ptr = lambda a: a.ctypes.data_as(__import__("ctypes").c_void_p)  # noqa: E731
+    for _ in range(max(1, args.warmup)):
+        X.PHYSIK_B200_SetNodeStates(w.h, ptr(hx), ptr(hv), n_nodes)
+        w.step()
+        X.PHYSIK_B200_GetNodeStates(w.h, ptr(hx), ptr(hv), n_nodes)
+    barrier(pg)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        X.PHYSIK_B200_SetNodeStates(w.h, ptr(hx), ptr(hv), n_nodes)
+        w.step()
+        X.PHYSIK_B200_GetNodeStates(w.h, ptr(hx), ptr(hv), n_nodes)
+    e2e_s = time.perf_counter() - t0
+    barrier(pg)
+    e2e_s = max_over_ranks(pg, e2e_s, local)
+    if not np.all(np.isfinite(hx)):
+        raise RuntimeError("non-finite state after the e2e steps")
+
+    steps_total = args.steps * world
+    value = steps_total / (elapsed_ms / 1e3)
+    iters = stats["iterations"]
+    bpi = pcg_bytes_per_iteration(n, nnz, args.precision)
+    solve_ms = tm["solve_ms"] / max(1, tm["steps"])
+    achieved = (bpi * iters) / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else None
+    peak, peak_kind = measured_peaks()
+    traffic = None
+    tpi = traffic_per_iteration()
+    if tpi and tpi.get("workload") == args.workload and tpi.get("precision") == args.precision:
+        traffic = float(tpi["dram_bytes_per_iteration"]) * iters
+    return dict(
+        value=value, ms_per_step=elapsed_ms / args.steps, e2e_s=e2e_s, n=n, nnz=nnz, nodes=n_nodes, iters=iters,
+        converged=stats["converged"], flags=stats["flags"], assemble_ms=tm["assemble_ms"] / max(1, tm["steps"]),
+        solve_ms=solve_ms, launches=tm["launches"], achieved=achieved, peak=peak, peak_kind=peak_kind,
+        traffic=traffic, clocks=clock, bytes_per_iteration=bpi, h2d=2 * 12 * n_nodes, d2h=2 * 12 * n_nodes)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=list(WORKLOADS), default="block128")
+    ap.add_argument("--precision", choices=["mixed", "fp32", "fp64"], default="mixed")
+    ap.add_argument("--cpu-budget", type=float, default=45.0, help="seconds of reference CPU time to sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    from physik_b200 import meshes
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    cfg, desc = WORKLOADS[args.workload]
+    scene = meshes.CONFIGS[cfg]()
+    base_config = {"workload": desc, "precision": args.precision, "gpus": world,
+                   "parallelism": "single GPU" if world == 1 else f"{world} independent replicas (a body does not shard)",
+                   "l2": "working set larger than the 126 MB L2 for block128; no flush"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        s = cpu_reference_sample(scene, budget_s=args.cpu_budget * 2)
+        if s is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing"}))
+            return
+        sample = (f"{s['steps']} timed PHYSIK_Step of {args.workload} after 1 untimed step, FP32 reference "
+                  f"compiled from its sources, 1 thread ({cpu_model()})")
+        line = {"impl": "reference", "metric": METRIC, "value": s["steps_per_s"], "unit": "steps/s",
+                "n_gpus": 0, "steps": s["steps"], "warmup": 1, "ms_per_step": 1e3 / s["steps_per_s"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": dict(base_config, precision="fp32 (reference)"),
+                "cpu_baseline": {"value": s["steps_per_s"], "unit": "steps/s", "cores": 1, "kind": "reference",
+                                 "sample": sample},
+                "e2e": {"value": s["steps_per_s"], "unit": "steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    r = run_ours(args, scene, rank, world, local, pg)
+    if rank != 0:
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    cpu = None
+    if not args.no_cpu_baseline:
+        s = cpu_reference_sample(scene, budget_s=args.cpu_budget, max_steps=None)
+        if s is not None:
+            cpu = {"value": s["steps_per_s"], "unit": "steps/s", "cores": 1, "kind": "reference",
+                   "sample": (f"{s['steps']} timed PHYSIK_Step of {args.workload} ({s['seconds']:.1f} s) after 1 "
+                              f"untimed step, FP32 reference compiled from its sources, 1 thread ({cpu_model()})")}
+    roof = None
+    if r["achieved"] is not None:
+        roof = {"bound": "hbm", "achieved": r["achieved"], "peak": r["peak"], "unit": "GB/s",
+                "frac": r["achieved"] / r["peak"], "traffic": r["traffic"],
+                "kernel": "pcg_kernel (cooperative PCG: fused symmetric BSR SpMV + block-Jacobi + dots + integrate)",
+                "peak_source": f"{r['peak_kind']} hbm_gbs (MEASURED_PEAKS.json)",
+                "bytes_per_iteration": r["bytes_per_iteration"], "iterations_per_launch": r["iters"]}
+    line = {
+        "metric": METRIC, "value": r["value"], "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if args.precision != "fp64" else "f64", "data": "synthetic",
+        "config": dict(base_config, dynamic_rows=r["n"], upper_blocks=r["nnz"], cg_iterations=r["iters"],
+                       converged=r["converged"], assemble_ms=r["assemble_ms"], pcg_ms=r["solve_ms"]),
+        "roofline": roof, "cpu_baseline": cpu,
+        "e2e": {"value": args.steps * world / r["e2e_s"], "unit": "steps/s", "h2d_bytes_per_step": r["h2d"],
+                "d2h_bytes_per_step": r["d2h"]},
+        "gpu_launches": r["launches"], "clocks": r["clocks"],
+    }
+    print(json.dumps(line))
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

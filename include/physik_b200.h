@@ -1,0 +1,189 @@
+/*
+ * physik_b200.h -- the drop-in C ABI of PhysiK's soft-body step, backed by sm_100a
+ * kernels.  The PHYSIK_* functions below keep the names, argument types and error
+ * behaviour of the reference's Unity-facing API (include/PhysiK/API/PhysiKAPI.h) for
+ * the implicit soft-body path, so a P/Invoke or ctypes binding written against the
+ * reference binds unchanged.  Each declaration cites the reference function it
+ * replaces (file:line in mauriciomedg/PhysiK).
+ *
+ * Error conventions kept from the reference: a NULL world is a silent no-op, getters
+ * return 0 / -1 / an invalid handle, out-pointers are written only when non-NULL.
+ * One deliberate difference: the reference lets World::ValidateNodeMasses throw
+ * std::runtime_error through PHYSIK_Step (src/Core/World/World.cpp:576-578); here the
+ * C ABI catches every exception at the boundary, leaves the state unchanged and
+ * records the message for PHYSIK_B200_GetLastError.
+ *
+ * PHYSIK_B200_* functions are extensions with no counterpart in the reference.
+ */
+#ifndef PHYSIK_B200_H
+#define PHYSIK_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define PHYSIK_B200_API __attribute__((visibility("default")))
+#else
+#define PHYSIK_B200_API
+#endif
+
+typedef void* PhysikWorldHandle;            /* PhysiK::WorldHandle (include/PhysiK/API/Handles.h:7) */
+typedef void* PhysikGeneratedTetMeshHandle; /* PhysiK::GeneratedTetMeshHandle (Handles.h:8) */
+
+/* PhysiK::ComponentHandle (Handles.h:10-19): index 0xFFFFFFFF or generation 0 is invalid. */
+typedef struct PhysikComponentHandle {
+    uint32_t index;
+    uint32_t generation;
+} PhysikComponentHandle;
+
+/* PhysikMaterialDesc (include/PhysiK/API/PhysiKAPI.h:16-22) */
+typedef struct PhysikMaterialDesc {
+    float density;
+    float youngModulus;
+    float poissonRatio;
+    float damping;
+} PhysikMaterialDesc;
+
+/* PhysiK::Vec3 (include/PhysiK/Math/Vec3.h:7-12): three packed floats. */
+typedef struct PhysikVec3 {
+    float x, y, z;
+} PhysikVec3;
+
+/* ---- world ------------------------------------------------------------ */
+/* PHYSIK_CreateWorld / PHYSIK_DestroyWorld   PhysiKAPI.h:57-58, PhysiKAPI.cpp:312-320 */
+PHYSIK_B200_API PhysikWorldHandle PHYSIK_CreateWorld(void);
+PHYSIK_B200_API void PHYSIK_DestroyWorld(PhysikWorldHandle world);
+/* PHYSIK_Step   PhysiKAPI.h:60, PhysiKAPI.cpp:322-328 -> World::Step (World.cpp:32-73) */
+PHYSIK_B200_API void PHYSIK_Step(PhysikWorldHandle world, float dt);
+/* PHYSIK_SetSubstepCount   PhysiKAPI.h:61, World.cpp:157-160 (count clamped to >= 1) */
+PHYSIK_B200_API void PHYSIK_SetSubstepCount(PhysikWorldHandle world, int substepCount);
+/* PHYSIK_SetSolverMode   PhysiKAPI.h:62, PhysiKAPI.cpp:338-345 (1 = implicit Euler, else explicit) */
+PHYSIK_B200_API void PHYSIK_SetSolverMode(PhysikWorldHandle world, int mode);
+/* CG settings   PhysiKAPI.h:63-72, World.cpp:177-205 (tolerance clamped to [1e-8, 0.1],
+ * non-finite ignored; iterations clamped to [1, 1024]) */
+PHYSIK_B200_API void PHYSIK_SetConjugateGradientTolerance(PhysikWorldHandle world, float tolerance);
+PHYSIK_B200_API float PHYSIK_GetConjugateGradientTolerance(PhysikWorldHandle world);
+PHYSIK_B200_API void PHYSIK_SetConjugateGradientMaxIterations(PhysikWorldHandle world, int maxIterations);
+PHYSIK_B200_API int PHYSIK_GetConjugateGradientMaxIterations(PhysikWorldHandle world);
+/* Last-solve diagnostics   PhysiKAPI.h:73-78, World.cpp:208-221 */
+PHYSIK_B200_API int PHYSIK_GetLastConjugateGradientIterations(PhysikWorldHandle world);
+PHYSIK_B200_API float PHYSIK_GetLastConjugateGradientResidualNorm(PhysikWorldHandle world);
+PHYSIK_B200_API int PHYSIK_DidLastConjugateGradientSolveConverge(PhysikWorldHandle world);
+/* PHYSIK_SetGravity   PhysiKAPI.h:79-83 (default gravity is zero) */
+PHYSIK_B200_API void PHYSIK_SetGravity(PhysikWorldHandle world, float x, float y, float z);
+/* PHYSIK_AddNode   PhysiKAPI.h:84-88, World.cpp:75-83 */
+PHYSIK_B200_API int PHYSIK_AddNode(PhysikWorldHandle world, float x, float y, float z);
+/* PHYSIK_SetNodeFixed / PHYSIK_IsNodeFixed   PhysiKAPI.h:90-97, World.cpp:403-423 (fixing zeroes the velocity) */
+PHYSIK_B200_API void PHYSIK_SetNodeFixed(PhysikWorldHandle world, int nodeIndex, int fixed);
+PHYSIK_B200_API int PHYSIK_IsNodeFixed(PhysikWorldHandle world, int nodeIndex);
+
+/* ---- generated meshes ------------------------------------------------- */
+/* PHYSIK_GenerateTetMesh   PhysiKAPI.h:99-103 -> TetMeshGenerator::Generate (TetMeshGenerator.cpp:153-282) */
+PHYSIK_B200_API PhysikGeneratedTetMeshHandle PHYSIK_GenerateTetMesh(const PhysikVec3* positions, int nodeCount,
+                                                                     const int* tetLocalNodeIndices, int tetCount);
+/* PhysiKAPI.h:105-130 */
+PHYSIK_B200_API int PHYSIK_IsGeneratedTetMeshHandleValid(PhysikGeneratedTetMeshHandle mesh);
+PHYSIK_B200_API void PHYSIK_DestroyGeneratedTetMesh(PhysikGeneratedTetMeshHandle mesh);
+PHYSIK_B200_API int PHYSIK_GetGeneratedTetMeshVertexCount(PhysikGeneratedTetMeshHandle mesh);
+PHYSIK_B200_API int PHYSIK_GetGeneratedTetMeshTetCount(PhysikGeneratedTetMeshHandle mesh);
+PHYSIK_B200_API int PHYSIK_GetGeneratedTetMeshTetIndexCount(PhysikGeneratedTetMeshHandle mesh);
+PHYSIK_B200_API int PHYSIK_GetGeneratedTetMeshVertex(PhysikGeneratedTetMeshHandle mesh, int vertexIndex, float* outX,
+                                                     float* outY, float* outZ);
+PHYSIK_B200_API int PHYSIK_GetGeneratedTetMeshTetNodeIndex(PhysikGeneratedTetMeshHandle mesh, int tetIndexArrayIndex,
+                                                           int* outNodeIndex);
+
+/* ---- components ------------------------------------------------------- */
+/* PHYSIK_CreateTetMeshComponent   PhysiKAPI.h:132-134, PhysiKAPI.cpp:599-616 */
+PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateTetMeshComponent(PhysikWorldHandle world,
+                                                                     PhysikGeneratedTetMeshHandle mesh);
+/* PHYSIK_CreateTetMeshPhysicsComponent   PhysiKAPI.h:136-139, PhysiKAPI.cpp:618-640 */
+PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateTetMeshPhysicsComponent(PhysikWorldHandle world,
+                                                                            PhysikGeneratedTetMeshHandle mesh,
+                                                                            const PhysikMaterialDesc* material);
+/* PhysiKAPI.h:141-157 */
+PHYSIK_B200_API int PHYSIK_GetTetMeshGlobalNodeBeginIndex(PhysikWorldHandle world, PhysikComponentHandle tetMesh);
+PHYSIK_B200_API int PHYSIK_GetTetMeshGlobalNodeCount(PhysikWorldHandle world, PhysikComponentHandle tetMesh);
+PHYSIK_B200_API int PHYSIK_GetTetMeshGlobalNodeIndex(PhysikWorldHandle world, PhysikComponentHandle tetMesh,
+                                                     int localNodeIndex);
+PHYSIK_B200_API void PHYSIK_SetTetMeshMaterial(PhysikWorldHandle world, PhysikComponentHandle component,
+                                               const PhysikMaterialDesc* material);
+/* PhysiKAPI.h:300-334 */
+PHYSIK_B200_API void PHYSIK_DestroyComponent(PhysikWorldHandle world, PhysikComponentHandle component);
+PHYSIK_B200_API int PHYSIK_IsComponentHandleValid(PhysikWorldHandle world, PhysikComponentHandle component);
+PHYSIK_B200_API int PHYSIK_GetTetMeshTetCount(PhysikWorldHandle world, PhysikComponentHandle component);
+PHYSIK_B200_API int PHYSIK_GetTetMeshNodeCount(PhysikWorldHandle world, PhysikComponentHandle component);
+PHYSIK_B200_API int PHYSIK_IsTetActive(PhysikWorldHandle world, PhysikComponentHandle component, int tetIndex);
+/* PHYSIK_SetTetActive   PhysiKAPI.h:321-325, PhysiKAPI.cpp:1324-1346 (node activity reconciled) */
+PHYSIK_B200_API void PHYSIK_SetTetActive(PhysikWorldHandle world, PhysikComponentHandle component, int tetIndex,
+                                         int active);
+PHYSIK_B200_API void PHYSIK_DeactivateTet(PhysikWorldHandle world, PhysikComponentHandle component, int tetIndex);
+PHYSIK_B200_API int PHYSIK_GetActiveTetCount(PhysikWorldHandle world, PhysikComponentHandle component);
+
+/* ---- node state ------------------------------------------------------- */
+/* PhysiKAPI.h:371-397, PhysiKAPI.cpp:1477-1558 (SetNodePosition zeroes the velocity) */
+PHYSIK_B200_API void PHYSIK_GetNodePosition(PhysikWorldHandle world, int nodeIndex, float* outX, float* outY,
+                                            float* outZ);
+PHYSIK_B200_API void PHYSIK_GetNodeVelocity(PhysikWorldHandle world, int nodeIndex, float* outX, float* outY,
+                                            float* outZ);
+PHYSIK_B200_API void PHYSIK_SetNodePosition(PhysikWorldHandle world, int nodeIndex, float x, float y, float z);
+PHYSIK_B200_API void PHYSIK_SetNodeVelocity(PhysikWorldHandle world, int nodeIndex, float x, float y, float z);
+
+/* ---- extensions (no counterpart in the reference) --------------------- */
+#define PHYSIK_B200_PRECISION_FP32 0  /* the reference's scalar type: float storage and dot products */
+#define PHYSIK_B200_PRECISION_MIXED 1 /* float storage, double CG scalars, double polar for near-inverted tets */
+#define PHYSIK_B200_PRECISION_FP64 2  /* double everywhere */
+PHYSIK_B200_API void PHYSIK_B200_SetPrecision(PhysikWorldHandle world, int precision);
+PHYSIK_B200_API int PHYSIK_B200_GetPrecision(PhysikWorldHandle world);
+PHYSIK_B200_API void PHYSIK_B200_SetDevice(PhysikWorldHandle world, int device);
+PHYSIK_B200_API int PHYSIK_B200_GetNodeCount(PhysikWorldHandle world);
+/* Bulk state, 3 values per node in world order; returns nodes copied or -1. */
+PHYSIK_B200_API int PHYSIK_B200_GetNodeStates(PhysikWorldHandle world, float* positions, float* velocities, int count);
+PHYSIK_B200_API int PHYSIK_B200_SetNodeStates(PhysikWorldHandle world, const float* positions, const float* velocities,
+                                              int count);
+PHYSIK_B200_API int PHYSIK_B200_GetNodeStatesF64(PhysikWorldHandle world, double* positions, double* velocities,
+                                                 int count);
+PHYSIK_B200_API int PHYSIK_B200_SetNodeStatesF64(PhysikWorldHandle world, const double* positions,
+                                                 const double* velocities, int count);
+/* Per-element Young's modulus (the reference's C++ route: Tet::youngModulus + RebuildTetFemCache). */
+PHYSIK_B200_API int PHYSIK_B200_SetTetMeshYoungModulus(PhysikWorldHandle world, PhysikComponentHandle component,
+                                                       const float* youngModulus, int tetCount);
+/* FemModel selector: 0 linear, 1 corotated (default), 2 NeoHookean (not implemented, as in the reference). */
+PHYSIK_B200_API int PHYSIK_B200_SetTetMeshFemModel(PhysikWorldHandle world, PhysikComponentHandle component, int model);
+/* Flags of the last device substep (PK_FLAG_* of include/pkcuda.h). */
+PHYSIK_B200_API unsigned PHYSIK_B200_GetLastStepFlags(PhysikWorldHandle world);
+/* Message of the last failure caught at this boundary ("" if none). */
+PHYSIK_B200_API const char* PHYSIK_B200_GetLastError(void);
+/* Builds the solver scene (lumped masses, dynamic-node mapping, canonical upper BSR
+ * pattern) without stepping; uploads it to the GPU when `upload` is non-zero (with
+ * upload = 0 no CUDA call is made).  Returns the dynamic row count or -1. */
+PHYSIK_B200_API int PHYSIK_B200_PrepareScene(PhysikWorldHandle world, int upload);
+/* The solver pattern (canonical upper BSR over dynamic rows) and node mapping of the
+ * last prepared scene (SolverData's matrix pattern, SolverData.cpp:389-401). */
+PHYSIK_B200_API int PHYSIK_B200_GetSolverSizes(PhysikWorldHandle world, int* dynamicRows, int* blocks);
+PHYSIK_B200_API int PHYSIK_B200_GetSolverPattern(PhysikWorldHandle world, int* rowStart, int* colIndex,
+                                                 int* nodeToDynamic);
+/* Assembled lumped masses per world node (SolverData::AssembleMasses). */
+PHYSIK_B200_API int PHYSIK_B200_GetSolverMasses(PhysikWorldHandle world, double* masses);
+/* The last substep's assembled system: values 9*blocks (column-major), rhs 3*rows,
+ * block-Jacobi inverse 9*rows, delta-v 3*rows. */
+PHYSIK_B200_API int PHYSIK_B200_GetSolverSystem(PhysikWorldHandle world, double* values, double* rhs, double* minv,
+                                                double* deltaVelocity);
+/* Device timing of the step phases (see pk_system_timings). */
+PHYSIK_B200_API int PHYSIK_B200_EnableTiming(PhysikWorldHandle world, int on);
+PHYSIK_B200_API int PHYSIK_B200_GetTimings(PhysikWorldHandle world, double* assembleMs, double* solveMs, int* steps,
+                                           long long* kernelLaunches);
+PHYSIK_B200_API int PHYSIK_B200_SetPcgGrid(PhysikWorldHandle world, int grid);
+/* The CUDA stream (cudaStream_t) the world's device work runs on, or NULL before the
+ * first upload; lets a caller record its own events around steps. */
+PHYSIK_B200_API void* PHYSIK_B200_GetStream(PhysikWorldHandle world);
+/* Waits for the device work queued by the world. */
+PHYSIK_B200_API int PHYSIK_B200_Synchronize(PhysikWorldHandle world);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PHYSIK_B200_H */

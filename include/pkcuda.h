@@ -1,0 +1,167 @@
+/*
+ * pkcuda.h -- the thin C ABI over the sm_100a kernels of PhysiK's implicit
+ * soft-body step.  Plain pointers and sizes, an int status on every call, one CUDA
+ * stream per system.  The C++ host layer (World, TetMeshPhysicsComponent,
+ * SolverData, SparseBlockMatrix, SolvePreconditionedConjugateGradient) calls these;
+ * tests call them directly for kernel-level parity.
+ *
+ * Reference interfaces each entry point replaces (paths inside mauriciomedg/PhysiK):
+ *   pk_system_step        one implicit substep: FEMModel::ComputeCorotationalElasticForces
+ *                         (src/Core/Physics/FEM/FEMModel.cpp:635-679) + TetMeshPhysicsComponent::
+ *                         UpdateSystem (src/Components/TetMeshPhysicsComponent.cpp:293-354) +
+ *                         SolverData::PrecomputeImplicitSolve / SolveImplicitLinearSystem
+ *                         (src/Core/Solvers/SolverData.cpp:126-212) + World::IntegrateImplicitEuler
+ *                         (src/Core/World/World.cpp:644-695); explicit mode replaces
+ *                         World::IntegrateExplicitEuler (World.cpp:697-725)
+ *   pk_bsr_multiply       SparseBlockMatrix::Multiply (src/Math/SparseBlockMatrix.cpp:209-268)
+ *   pk_pcg                SolvePreconditionedConjugateGradient
+ *                         (src/Core/Solvers/Linear/ConjugateGradientSolver.cpp:114-241,
+ *                          include/PhysiK/Core/Solvers/Linear/ConjugateGradientSolver.h:26-35)
+ *   pk_system_get_state_* / set_state_*   World::GetNodePosition / GetNodeVelocity and the
+ *                         PHYSIK_Get/SetNodePosition/Velocity accessors (src/API/PhysiKAPI.cpp:1477-1558),
+ *                         in bulk
+ *
+ * Threading: calls on one pk_system must be serialised by the caller (as the
+ * reference's World is single-threaded).  Steps are asynchronous on the system's
+ * stream; pk_system_stats and the get_* calls wait for it.
+ */
+#ifndef PKCUDA_H
+#define PKCUDA_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define PKCUDA_API __attribute__((visibility("default")))
+#else
+#define PKCUDA_API
+#endif
+
+/* Precision of a system: storage / accumulation. */
+#define PK_PREC_FP32 0  /* float storage, float dot products (the reference's scalar type) */
+#define PK_PREC_MIXED 1 /* float storage, double CG scalars and updates, double polar for near-inverted tets */
+#define PK_PREC_FP64 2  /* double everywhere */
+
+/* Return codes. */
+#define PK_OK 0
+#define PK_ERR_NO_DEVICE (-1)   /* no usable CUDA device */
+#define PK_ERR_CUDA (-2)        /* a CUDA call failed: pk_last_error() */
+#define PK_ERR_ARG (-3)         /* invalid argument */
+#define PK_ERR_STATE (-4)       /* call out of order (e.g. a step before the topology) */
+#define PK_ERR_UNSUPPORTED (-5) /* a size the kernels were not built for */
+#define PK_ERR_TIMEOUT (-6)     /* a grid barrier gave up waiting; the step was not applied */
+
+/* Step flags, reported in pk_step_stats.flags. */
+#define PK_FLAG_PRECOMPUTE_FAILED 0x1u /* non-finite velocity / stiffness block / rhs: no solve (SolverData.cpp:353-373) */
+#define PK_FLAG_SINGULAR_DIAG 0x2u     /* a diagonal block with |det| <= 1e-8 or non-finite (SolverData.cpp:284-303) */
+#define PK_FLAG_INVALID_RHS 0x4u       /* non-finite rhs or invalid settings: solution cleared (ConjugateGradientSolver.cpp:137-149) */
+#define PK_FLAG_BREAKDOWN 0x8u         /* d.q <= 0 or a non-finite CG scalar: iteration stopped early */
+#define PK_FLAG_NONFINITE_DV 0x10u     /* delta-v not finite: solve reported failure (SolverData.cpp:203-209) */
+#define PK_FLAG_INTEGRATE_ABORT 0x20u  /* integration would produce non-finite state: not applied (World.cpp:667-677) */
+#define PK_FLAG_POLAR_IDENTITY 0x40u   /* some polar decomposition fell back to the identity */
+#define PK_FLAG_POLAR_FP64 0x80u       /* some near-inverted tet used the double-precision polar (mixed mode) */
+#define PK_FLAG_BARRIER_TIMEOUT 0x100u /* a grid barrier timed out */
+#define PK_FLAG_ROW_TOO_LONG 0x200u    /* internal: a row exceeded the row kernel's slot count */
+#define PK_FLAG_SOLVED 0x1000u         /* SolveImplicitLinearSystem would return true */
+#define PK_FLAG_INTEGRATED 0x2000u     /* positions and velocities were advanced */
+#define PK_FLAG_CONVERGED 0x4000u      /* CG met its relative tolerance */
+
+typedef struct pk_step_params {
+    double dt;               /* substep size (World::Step divides the frame by the substep count) */
+    double gravity[3];
+    int max_iterations;      /* ConjugateGradientSettings::maxIterations */
+    double tolerance;        /* ConjugateGradientSettings::tolerance (relative, preconditioned) */
+    int use_jacobi;          /* ConjugateGradientSettings::useJacobiPreconditioner */
+    int linear;              /* 1: FemModel::Linear (R = I), 0: FemModel::Corotational */
+    int explicit_mode;       /* 1: SolverMode::Explicit, 0: SolverMode::ImplicitEuler */
+    int integrate;           /* 0: assemble and solve only (delta-v stays on the device) */
+} pk_step_params;
+
+typedef struct pk_step_stats {
+    int iterations;          /* ConjugateGradientResult::iterations */
+    int converged;           /* ConjugateGradientResult::converged */
+    double residual_norm;    /* ConjugateGradientResult::residualNorm = ||r||_2 */
+    unsigned flags;          /* PK_FLAG_* */
+    int polar_fp64_count;
+    int polar_identity_count;
+} pk_step_stats;
+
+typedef struct pk_cg_result {
+    int iterations;
+    int converged;
+    double residual_norm;
+    int have_solution;       /* 0 when the reference would have cleared the solution vector */
+} pk_cg_result;
+
+typedef struct pk_system pk_system;
+
+PKCUDA_API const char* pk_last_error(void);
+PKCUDA_API int pk_device_count(void);
+
+PKCUDA_API int pk_system_create(int device, int precision, pk_system** out);
+PKCUDA_API int pk_system_destroy(pk_system* sys);
+PKCUDA_API void* pk_system_stream(pk_system* sys);
+
+/* Nodes in world order: node_to_dyn[i] is node i's dynamic row or -1; mass[i] the
+ * assembled lumped mass (SolverData::AssembleMasses order).  Resets state to zero. */
+PKCUDA_API int pk_system_set_nodes(pk_system* sys, int node_count, const int* node_to_dyn, const double* mass);
+/* Either pointer may be NULL.  3*node_count values each. */
+PKCUDA_API int pk_system_set_state_f32(pk_system* sys, const float* x, const float* v);
+PKCUDA_API int pk_system_set_state_f64(pk_system* sys, const double* x, const double* v);
+PKCUDA_API int pk_system_get_state_f32(pk_system* sys, float* x, float* v);
+PKCUDA_API int pk_system_get_state_f64(pk_system* sys, double* x, double* v);
+
+/* Tets with world node ids and rest data already computed in the system precision
+ * (FEMModel::InitializeTetRestData, BuildElasticityMatrix's lambda and mu).
+ * enabled[t]: bit 0 = tet active, rest volume > 0 and its body simulated; bit 1 = linear FEM
+ * (FemModel::Linear, R = I) instead of corotated. */
+PKCUDA_API int pk_system_set_tets(pk_system* sys, int tet_count, const int* tet_nodes, const unsigned char* enabled,
+                                  const double* dm_inv, const double* volume, const double* lambda, const double* mu,
+                                  const double* damping);
+
+/* Dynamic rows: the canonical upper BSR of SolverData (row_start[dyn+1], col_index[nnz]),
+ * the row -> world node map, and per row the incidence list of its node's tets
+ * (entries t*4 + corner, ascending t). */
+PKCUDA_API int pk_system_set_pattern(pk_system* sys, int dyn_count, const int* dyn_to_node, const int* row_start,
+                                     const int* col_index, const int* inc_start, const int* inc_list);
+
+/* One substep, asynchronous on the system stream. */
+PKCUDA_API int pk_system_step(pk_system* sys, const pk_step_params* params);
+/* Waits for the last step and reports its statistics. */
+PKCUDA_API int pk_system_stats(pk_system* sys, pk_step_stats* out);
+
+/* The last assembled system (waits).  values: 9*nnz column-major; rhs, dv: 3*dyn;
+ * minv: 9*dyn.  Any pointer may be NULL. */
+PKCUDA_API int pk_system_get_system_f64(pk_system* sys, double* values, double* rhs, double* minv, double* dv);
+/* Overwrites the matrix, rhs and inverse preconditioner (same layout) and runs only the
+ * solve of pk_system_step (no assembly); used to drive the PCG on an exact system. */
+PKCUDA_API int pk_system_solve_given_f64(pk_system* sys, const double* values, const double* rhs,
+                                         const double* minv, const pk_step_params* params);
+
+/* Device-event timing of the step's phases on the system stream. */
+PKCUDA_API int pk_system_enable_timing(pk_system* sys, int on);
+/* Accumulated since enable: assembly (tet + row kernels) and solve (PCG kernel) times in ms,
+ * the number of timed steps, and the kernels launched. */
+PKCUDA_API int pk_system_timings(pk_system* sys, double* assemble_ms, double* solve_ms, int* steps,
+                                 long long* kernel_launches);
+/* Grid size of the cooperative PCG launch (0 = automatic).  Returns the grid used next. */
+PKCUDA_API int pk_system_set_pcg_grid(pk_system* sys, int grid);
+
+/* Standalone kernels on host arrays (values column-major, 9 per block). */
+PKCUDA_API int pk_bsr_multiply(int device, int precision, int n, const int* row_start, const int* col_index,
+                               const double* values, const double* x, double* y);
+PKCUDA_API int pk_pcg(int device, int precision, int n, const int* row_start, const int* col_index,
+                      const double* values, const double* b, const double* minv, int minv_count, int max_iterations,
+                      double tolerance, double* x, pk_cg_result* out);
+
+/* Builds the transposed index of an upper BSR: for row r the blocks (c, r), c < r.
+ * lt_start[n+1]; lt_row / lt_block sized nnz - n.  Host-only, no device needed. */
+PKCUDA_API int pk_bsr_transpose_index(int n, const int* row_start, const int* col_index, int* lt_start, int* lt_row,
+                                      int* lt_block);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PKCUDA_H */

@@ -93,8 +93,13 @@ def scene_arrays(scene):
 class Oracle:
     """The C restatement.  precision 'f32' reproduces the FP32 reference; 'f64' is the FP64 oracle."""
 
-    def __init__(self, scene, precision: str = "f64", linear: bool = False, use_jacobi: bool = True):
+    def __init__(self, scene, precision: str = "f64", linear: bool = False, use_jacobi: bool = True,
+                 float_inputs: bool = False):
+        """float_inputs: round dt, gravity, material and tolerance to float32 first -- the
+        values a caller of the float C ABI (PHYSIK_Step(float dt), PhysikMaterialDesc)
+        actually passes -- so an FP64 device run can be checked against identical inputs."""
         self.precision = precision
+        self.float_inputs = float_inputs
         self.dtype = np.float32 if precision == "f32" else np.float64
         self.lib = C.CDLL(oracle_library_path(precision))
         pre = f"pko_{precision}_"
@@ -105,6 +110,9 @@ class Oracle:
             self._f(n).restype = None
         self._f("step").restype = _i
         a = scene_arrays(scene)
+        if float_inputs:
+            for key in ("density", "young", "poisson", "damping"):
+                a[key] = a[key].astype(np.float32).astype(np.float64)
         self.arrays = a
         dt_ = self.dtype
         self.node_count = a["rest"].shape[0]
@@ -116,9 +124,10 @@ class Oracle:
         self.h = self._f("create")(
             _i(self.node_count), _ptr(k[0]), _i(self.tet_count), _ptr(k[1]), _i(len(scene.bodies)), _ptr(k[2]),
             _ptr(k[3]), _ptr(k[4]), _ptr(k[5]), _ptr(k[6]), _ptr(k[7]))
-        g = np.array(scene.gravity, dt_)
+        g = np.array(scene.gravity, np.float32 if float_inputs else np.float64).astype(dt_)
+        tol = float(np.float32(scene.tolerance)) if float_inputs else scene.tolerance
         self._f("set_settings")(_p(self.h), _ptr(g), _i(scene.max_iterations),
-                                (C.c_float if precision == "f32" else C.c_double)(scene.tolerance),
+                                (C.c_float if precision == "f32" else C.c_double)(tol),
                                 _i(1 if use_jacobi else 0), _i(1 if linear else 0))
         self._fixed = a["fixed"].copy()
         self._active = np.ones(self.node_count, np.uint8)
@@ -126,7 +135,7 @@ class Oracle:
         self.x = a["x"].astype(dt_)
         self.v = a["v"].astype(dt_)
         self.v[self._fixed.astype(bool)] = 0.0
-        self.dt = scene.dt
+        self.dt = float(np.float32(scene.dt)) if float_inputs else scene.dt
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -154,6 +163,8 @@ class Oracle:
 
     def step(self, dt: Optional[float] = None) -> int:
         dt = self.dt if dt is None else dt
+        if self.float_inputs:
+            dt = float(np.float32(dt))
         ctype = C.c_float if self.precision == "f32" else C.c_double
         self._f("step").argtypes = [_p, _p, _p, ctype]
         return self._f("step")(_p(self.h), _ptr(self.x), _ptr(self.v), ctype(dt))

@@ -1,0 +1,565 @@
+// The PHYSIK_* C ABI (include/physik_b200.h) over the host World.  Behaviour follows
+// the reference's src/API/PhysiKAPI.cpp for the soft-body path; every exception is
+// caught at this boundary and recorded for PHYSIK_B200_GetLastError.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <exception>
+#include <string>
+#include <unordered_set>
+#include <vector>
+
+#include "../../../include/physik_b200.h"
+#include "../../../include/pkcuda.h"
+#include "physik_core.h"
+
+using namespace PhysiK;
+
+namespace {
+
+thread_local std::string g_error;
+std::unordered_set<GeneratedTetMesh*> g_meshes;  // live generated meshes (PhysiKAPI.cpp:24)
+
+World* AsWorld(PhysikWorldHandle h) { return static_cast<World*>(h); }
+
+GeneratedTetMesh* AsMesh(PhysikGeneratedTetMeshHandle h)
+{
+    auto* m = static_cast<GeneratedTetMesh*>(h);
+    return (m && g_meshes.count(m)) ? m : nullptr;
+}
+
+ComponentHandle ToHandle(PhysikComponentHandle h) { return ComponentHandle{h.index, h.generation}; }
+PhysikComponentHandle FromHandle(ComponentHandle h) { return PhysikComponentHandle{h.index, h.generation}; }
+PhysikComponentHandle InvalidHandle() { return PhysikComponentHandle{0xFFFFFFFFu, 0u}; }
+
+TetMeshComponent* AsTetMesh(World* w, PhysikComponentHandle h)
+{
+    return w ? dynamic_cast<TetMeshComponent*>(w->GetComponent(ToHandle(h))) : nullptr;
+}
+TetMeshPhysicsComponent* AsTetMeshPhysics(World* w, PhysikComponentHandle h)
+{
+    return w ? dynamic_cast<TetMeshPhysicsComponent*>(w->GetComponent(ToHandle(h))) : nullptr;
+}
+
+bool ValidNode(const World& w, int i) { return i >= 0 && i < static_cast<int>(w.GetNodes().size()); }
+
+Material ToMaterial(const PhysikMaterialDesc& d)
+{
+    Material m;
+    m.density = d.density;
+    m.youngModulus = d.youngModulus;
+    m.poissonRatio = d.poissonRatio;
+    m.damping = d.damping;
+    return m;
+}
+
+// A node stays active while some active tet of an active tet mesh references it
+// (ReconcileTetNodeActiveStates, PhysiKAPI.cpp:159-229).
+void ReconcileNodes(World& w, const TetMeshComponent& mesh, int tetIndex)
+{
+    for (int corner = 0; corner < 4; ++corner) {
+        const int g = mesh.GetGlobalNodeIndex(mesh.GetTetNodeIndex(tetIndex, corner));
+        if (!ValidNode(w, g)) continue;
+        bool referenced = false;
+        for (const auto& c : w.GetComponents()) {
+            const auto* tm = dynamic_cast<const TetMeshComponent*>(c.get());
+            if (!tm || !tm->active) continue;
+            for (int t = 0; t < tm->GetTetCount() && !referenced; ++t) {
+                if (!tm->IsTetActive(t)) continue;
+                for (int k = 0; k < 4; ++k)
+                    if (tm->GetGlobalNodeIndex(tm->GetTetNodeIndex(t, k)) == g) referenced = true;
+            }
+            if (referenced) break;
+        }
+        w.SetNodeActive(g, referenced);
+    }
+}
+
+template <class F>
+auto Guard(F&& f, decltype(f()) fallback) -> decltype(f())
+{
+    try {
+        return f();
+    } catch (const std::exception& e) {
+        g_error = e.what();
+    } catch (...) {
+        g_error = "unknown error";
+    }
+    return fallback;
+}
+
+template <class F>
+void GuardVoid(F&& f)
+{
+    try {
+        f();
+    } catch (const std::exception& e) {
+        g_error = e.what();
+    } catch (...) {
+        g_error = "unknown error";
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+PHYSIK_B200_API PhysikWorldHandle PHYSIK_CreateWorld(void)
+{
+    return Guard([]() -> PhysikWorldHandle { return new World(); }, nullptr);
+}
+
+PHYSIK_B200_API void PHYSIK_DestroyWorld(PhysikWorldHandle world)
+{
+    GuardVoid([&] { delete AsWorld(world); });
+}
+
+PHYSIK_B200_API void PHYSIK_Step(PhysikWorldHandle world, float dt)
+{
+    if (World* w = AsWorld(world)) GuardVoid([&] { w->Step(dt); });
+}
+
+PHYSIK_B200_API void PHYSIK_SetSubstepCount(PhysikWorldHandle world, int substepCount)
+{
+    if (World* w = AsWorld(world)) w->SetSubstepCount(substepCount);
+}
+
+PHYSIK_B200_API void PHYSIK_SetSolverMode(PhysikWorldHandle world, int mode)
+{
+    if (World* w = AsWorld(world)) w->SetSolverMode(mode == 1 ? SolverMode::ImplicitEuler : SolverMode::Explicit);
+}
+
+PHYSIK_B200_API void PHYSIK_SetConjugateGradientTolerance(PhysikWorldHandle world, float tolerance)
+{
+    if (World* w = AsWorld(world)) w->SetConjugateGradientTolerance(tolerance);
+}
+
+PHYSIK_B200_API float PHYSIK_GetConjugateGradientTolerance(PhysikWorldHandle world)
+{
+    World* w = AsWorld(world);
+    return w ? w->GetConjugateGradientTolerance() : 0.0f;
+}
+
+PHYSIK_B200_API void PHYSIK_SetConjugateGradientMaxIterations(PhysikWorldHandle world, int maxIterations)
+{
+    if (World* w = AsWorld(world)) w->SetConjugateGradientMaxIterations(maxIterations);
+}
+
+PHYSIK_B200_API int PHYSIK_GetConjugateGradientMaxIterations(PhysikWorldHandle world)
+{
+    World* w = AsWorld(world);
+    return w ? w->GetConjugateGradientMaxIterations() : 0;
+}
+
+PHYSIK_B200_API int PHYSIK_GetLastConjugateGradientIterations(PhysikWorldHandle world)
+{
+    World* w = AsWorld(world);
+    return w ? Guard([&] { return w->GetLastConjugateGradientIterations(); }, 0) : 0;
+}
+
+PHYSIK_B200_API float PHYSIK_GetLastConjugateGradientResidualNorm(PhysikWorldHandle world)
+{
+    World* w = AsWorld(world);
+    return w ? Guard([&] { return w->GetLastConjugateGradientResidualNorm(); }, 0.0f) : 0.0f;
+}
+
+PHYSIK_B200_API int PHYSIK_DidLastConjugateGradientSolveConverge(PhysikWorldHandle world)
+{
+    World* w = AsWorld(world);
+    return w ? Guard([&] { return w->DidLastConjugateGradientSolveConverge() ? 1 : 0; }, 0) : 0;
+}
+
+PHYSIK_B200_API void PHYSIK_SetGravity(PhysikWorldHandle world, float x, float y, float z)
+{
+    if (World* w = AsWorld(world)) w->SetGravity(Vec3{x, y, z});
+}
+
+PHYSIK_B200_API int PHYSIK_AddNode(PhysikWorldHandle world, float x, float y, float z)
+{
+    World* w = AsWorld(world);
+    return w ? Guard([&] { return w->AddNode(Vec3{x, y, z}); }, -1) : -1;
+}
+
+PHYSIK_B200_API void PHYSIK_SetNodeFixed(PhysikWorldHandle world, int nodeIndex, int fixed)
+{
+    World* w = AsWorld(world);
+    if (w && ValidNode(*w, nodeIndex)) GuardVoid([&] { w->SetNodeFixed(nodeIndex, fixed != 0); });
+}
+
+PHYSIK_B200_API int PHYSIK_IsNodeFixed(PhysikWorldHandle world, int nodeIndex)
+{
+    World* w = AsWorld(world);
+    return (w && ValidNode(*w, nodeIndex) && w->IsNodeFixed(nodeIndex)) ? 1 : 0;
+}
+
+PHYSIK_B200_API PhysikGeneratedTetMeshHandle PHYSIK_GenerateTetMesh(const PhysikVec3* positions, int nodeCount,
+                                                                     const int* tetLocalNodeIndices, int tetCount)
+{
+    return Guard(
+        [&]() -> PhysikGeneratedTetMeshHandle {
+            auto* m = new GeneratedTetMesh(TetMeshGenerator::Generate(reinterpret_cast<const Vec3*>(positions),
+                                                                      nodeCount, tetLocalNodeIndices, tetCount));
+            g_meshes.insert(m);
+            return m;
+        },
+        nullptr);
+}
+
+PHYSIK_B200_API int PHYSIK_IsGeneratedTetMeshHandleValid(PhysikGeneratedTetMeshHandle mesh)
+{
+    return AsMesh(mesh) ? 1 : 0;
+}
+
+PHYSIK_B200_API void PHYSIK_DestroyGeneratedTetMesh(PhysikGeneratedTetMeshHandle mesh)
+{
+    GeneratedTetMesh* m = AsMesh(mesh);
+    if (!m) return;
+    g_meshes.erase(m);
+    delete m;
+}
+
+PHYSIK_B200_API int PHYSIK_GetGeneratedTetMeshVertexCount(PhysikGeneratedTetMeshHandle mesh)
+{
+    const GeneratedTetMesh* m = AsMesh(mesh);
+    return m ? static_cast<int>(m->positions.size()) : 0;
+}
+
+PHYSIK_B200_API int PHYSIK_GetGeneratedTetMeshTetCount(PhysikGeneratedTetMeshHandle mesh)
+{
+    const GeneratedTetMesh* m = AsMesh(mesh);
+    return m ? static_cast<int>(m->tetLocalNodeIndices.size() / 4u) : 0;
+}
+
+PHYSIK_B200_API int PHYSIK_GetGeneratedTetMeshTetIndexCount(PhysikGeneratedTetMeshHandle mesh)
+{
+    const GeneratedTetMesh* m = AsMesh(mesh);
+    return m ? static_cast<int>(m->tetLocalNodeIndices.size()) : 0;
+}
+
+PHYSIK_B200_API int PHYSIK_GetGeneratedTetMeshVertex(PhysikGeneratedTetMeshHandle mesh, int vertexIndex, float* outX,
+                                                     float* outY, float* outZ)
+{
+    const GeneratedTetMesh* m = AsMesh(mesh);
+    if (!m || !outX || !outY || !outZ || vertexIndex < 0 || vertexIndex >= static_cast<int>(m->positions.size()))
+        return 0;
+    const Vec3& p = m->positions[static_cast<std::size_t>(vertexIndex)];
+    *outX = p.x;
+    *outY = p.y;
+    *outZ = p.z;
+    return 1;
+}
+
+PHYSIK_B200_API int PHYSIK_GetGeneratedTetMeshTetNodeIndex(PhysikGeneratedTetMeshHandle mesh, int i, int* out)
+{
+    const GeneratedTetMesh* m = AsMesh(mesh);
+    if (!m || !out || i < 0 || i >= static_cast<int>(m->tetLocalNodeIndices.size())) return 0;
+    *out = m->tetLocalNodeIndices[static_cast<std::size_t>(i)];
+    return 1;
+}
+
+PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateTetMeshComponent(PhysikWorldHandle world,
+                                                                     PhysikGeneratedTetMeshHandle mesh)
+{
+    World* w = AsWorld(world);
+    const GeneratedTetMesh* m = AsMesh(mesh);
+    if (!w || !m || m->positions.empty() || m->tetLocalNodeIndices.empty()) return InvalidHandle();
+    return Guard(
+        [&] {
+            auto c = std::make_unique<TetMeshComponent>();
+            c->SetGeometry(*m);
+            return FromHandle(w->AddComponent(std::move(c)));
+        },
+        InvalidHandle());
+}
+
+PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateTetMeshPhysicsComponent(PhysikWorldHandle world,
+                                                                            PhysikGeneratedTetMeshHandle mesh,
+                                                                            const PhysikMaterialDesc* material)
+{
+    World* w = AsWorld(world);
+    const GeneratedTetMesh* m = AsMesh(mesh);
+    if (!w || !m || !material || m->positions.empty() || m->tetLocalNodeIndices.empty()) return InvalidHandle();
+    return Guard(
+        [&] {
+            auto c = TetMeshPhysicsComponent::CreateFromGeneratedTetMesh(*w, *m, ToMaterial(*material));
+            return FromHandle(w->AddComponent(std::move(c)));
+        },
+        InvalidHandle());
+}
+
+PHYSIK_B200_API int PHYSIK_GetTetMeshGlobalNodeBeginIndex(PhysikWorldHandle world, PhysikComponentHandle tetMesh)
+{
+    const TetMeshPhysicsComponent* c = AsTetMeshPhysics(AsWorld(world), tetMesh);
+    return c ? c->GetGlobalNodeBeginIndex() : -1;
+}
+
+PHYSIK_B200_API int PHYSIK_GetTetMeshGlobalNodeCount(PhysikWorldHandle world, PhysikComponentHandle tetMesh)
+{
+    const TetMeshPhysicsComponent* c = AsTetMeshPhysics(AsWorld(world), tetMesh);
+    return c ? c->GetGlobalNodeCount() : -1;
+}
+
+PHYSIK_B200_API int PHYSIK_GetTetMeshGlobalNodeIndex(PhysikWorldHandle world, PhysikComponentHandle tetMesh,
+                                                     int localNodeIndex)
+{
+    const TetMeshPhysicsComponent* c = AsTetMeshPhysics(AsWorld(world), tetMesh);
+    return c ? c->GetGlobalNodeIndex(localNodeIndex) : -1;
+}
+
+PHYSIK_B200_API void PHYSIK_SetTetMeshMaterial(PhysikWorldHandle world, PhysikComponentHandle component,
+                                               const PhysikMaterialDesc* material)
+{
+    TetMeshPhysicsComponent* c = AsTetMeshPhysics(AsWorld(world), component);
+    if (c && material) c->SetMaterial(ToMaterial(*material));
+}
+
+PHYSIK_B200_API void PHYSIK_DestroyComponent(PhysikWorldHandle world, PhysikComponentHandle component)
+{
+    if (World* w = AsWorld(world)) GuardVoid([&] { w->DestroyComponent(ToHandle(component)); });
+}
+
+PHYSIK_B200_API int PHYSIK_IsComponentHandleValid(PhysikWorldHandle world, PhysikComponentHandle component)
+{
+    World* w = AsWorld(world);
+    return (w && w->IsComponentHandleValid(ToHandle(component))) ? 1 : 0;
+}
+
+PHYSIK_B200_API int PHYSIK_GetTetMeshTetCount(PhysikWorldHandle world, PhysikComponentHandle component)
+{
+    const TetMeshComponent* c = AsTetMesh(AsWorld(world), component);
+    return c ? c->GetTetCount() : 0;
+}
+
+PHYSIK_B200_API int PHYSIK_GetTetMeshNodeCount(PhysikWorldHandle world, PhysikComponentHandle component)
+{
+    const TetMeshComponent* c = AsTetMesh(AsWorld(world), component);
+    return c ? c->GetNodeCount() : 0;
+}
+
+PHYSIK_B200_API int PHYSIK_IsTetActive(PhysikWorldHandle world, PhysikComponentHandle component, int tetIndex)
+{
+    const TetMeshComponent* c = AsTetMesh(AsWorld(world), component);
+    return (c && c->IsTetActive(tetIndex)) ? 1 : 0;
+}
+
+PHYSIK_B200_API void PHYSIK_SetTetActive(PhysikWorldHandle world, PhysikComponentHandle component, int tetIndex,
+                                         int active)
+{
+    World* w = AsWorld(world);
+    TetMeshComponent* c = AsTetMesh(w, component);
+    if (!c) return;
+    GuardVoid([&] {
+        if (c->SetTetActive(tetIndex, active != 0)) ReconcileNodes(*w, *c, tetIndex);
+    });
+}
+
+PHYSIK_B200_API void PHYSIK_DeactivateTet(PhysikWorldHandle world, PhysikComponentHandle component, int tetIndex)
+{
+    PHYSIK_SetTetActive(world, component, tetIndex, 0);
+}
+
+PHYSIK_B200_API int PHYSIK_GetActiveTetCount(PhysikWorldHandle world, PhysikComponentHandle component)
+{
+    const TetMeshComponent* c = AsTetMesh(AsWorld(world), component);
+    return c ? c->GetActiveTetCount() : 0;
+}
+
+PHYSIK_B200_API void PHYSIK_GetNodePosition(PhysikWorldHandle world, int nodeIndex, float* outX, float* outY,
+                                            float* outZ)
+{
+    World* w = AsWorld(world);
+    if (!w || !ValidNode(*w, nodeIndex)) return;
+    GuardVoid([&] {
+        const Vec3& p = w->GetNodePosition(nodeIndex);
+        if (outX) *outX = p.x;
+        if (outY) *outY = p.y;
+        if (outZ) *outZ = p.z;
+    });
+}
+
+PHYSIK_B200_API void PHYSIK_GetNodeVelocity(PhysikWorldHandle world, int nodeIndex, float* outX, float* outY,
+                                            float* outZ)
+{
+    World* w = AsWorld(world);
+    if (!w || !ValidNode(*w, nodeIndex)) return;
+    GuardVoid([&] {
+        const Vec3& v = w->GetNodeVelocity(nodeIndex);
+        if (outX) *outX = v.x;
+        if (outY) *outY = v.y;
+        if (outZ) *outZ = v.z;
+    });
+}
+
+PHYSIK_B200_API void PHYSIK_SetNodePosition(PhysikWorldHandle world, int nodeIndex, float x, float y, float z)
+{
+    World* w = AsWorld(world);
+    if (w && ValidNode(*w, nodeIndex)) GuardVoid([&] { w->SetNodePosition(nodeIndex, Vec3{x, y, z}); });
+}
+
+PHYSIK_B200_API void PHYSIK_SetNodeVelocity(PhysikWorldHandle world, int nodeIndex, float x, float y, float z)
+{
+    World* w = AsWorld(world);
+    if (w && ValidNode(*w, nodeIndex)) GuardVoid([&] { w->SetNodeVelocity(nodeIndex, Vec3{x, y, z}); });
+}
+
+// ---------------------------------------------------------------- extensions
+PHYSIK_B200_API void PHYSIK_B200_SetPrecision(PhysikWorldHandle world, int precision)
+{
+    World* w = AsWorld(world);
+    if (!w || precision < 0 || precision > 2) return;
+    GuardVoid([&] { w->SetPrecision(static_cast<Precision>(precision)); });
+}
+
+PHYSIK_B200_API int PHYSIK_B200_GetPrecision(PhysikWorldHandle world)
+{
+    World* w = AsWorld(world);
+    return w ? static_cast<int>(w->GetPrecision()) : -1;
+}
+
+PHYSIK_B200_API void PHYSIK_B200_SetDevice(PhysikWorldHandle world, int device)
+{
+    if (World* w = AsWorld(world)) GuardVoid([&] { w->SetDevice(device); });
+}
+
+PHYSIK_B200_API int PHYSIK_B200_GetNodeCount(PhysikWorldHandle world)
+{
+    World* w = AsWorld(world);
+    return w ? static_cast<int>(w->GetNodes().size()) : 0;
+}
+
+PHYSIK_B200_API int PHYSIK_B200_GetNodeStates(PhysikWorldHandle world, float* positions, float* velocities, int count)
+{
+    World* w = AsWorld(world);
+    if (!w || count != static_cast<int>(w->GetNodes().size())) return -1;
+    return Guard([&] { w->GetNodeStates(positions, velocities); return count; }, -1);
+}
+
+PHYSIK_B200_API int PHYSIK_B200_SetNodeStates(PhysikWorldHandle world, const float* positions, const float* velocities,
+                                              int count)
+{
+    World* w = AsWorld(world);
+    if (!w || count != static_cast<int>(w->GetNodes().size())) return -1;
+    return Guard([&] { w->SetNodeStates(positions, velocities); return count; }, -1);
+}
+
+PHYSIK_B200_API int PHYSIK_B200_GetNodeStatesF64(PhysikWorldHandle world, double* positions, double* velocities,
+                                                 int count)
+{
+    World* w = AsWorld(world);
+    if (!w || count != static_cast<int>(w->GetNodes().size())) return -1;
+    return Guard([&] { w->GetNodeStatesF64(positions, velocities); return count; }, -1);
+}
+
+PHYSIK_B200_API int PHYSIK_B200_SetNodeStatesF64(PhysikWorldHandle world, const double* positions,
+                                                 const double* velocities, int count)
+{
+    World* w = AsWorld(world);
+    if (!w || count != static_cast<int>(w->GetNodes().size())) return -1;
+    return Guard([&] { w->SetNodeStatesF64(positions, velocities); return count; }, -1);
+}
+
+PHYSIK_B200_API int PHYSIK_B200_SetTetMeshYoungModulus(PhysikWorldHandle world, PhysikComponentHandle component,
+                                                       const float* youngModulus, int tetCount)
+{
+    TetMeshPhysicsComponent* c = AsTetMeshPhysics(AsWorld(world), component);
+    if (!c || !youngModulus || tetCount != c->GetTetCount()) return 0;
+    for (int t = 0; t < tetCount; ++t) c->tets[static_cast<std::size_t>(t)].youngModulus = youngModulus[t];
+    c->RebuildTetFemCache();
+    return 1;
+}
+
+PHYSIK_B200_API int PHYSIK_B200_SetTetMeshFemModel(PhysikWorldHandle world, PhysikComponentHandle component, int model)
+{
+    TetMeshPhysicsComponent* c = AsTetMeshPhysics(AsWorld(world), component);
+    if (!c || model < 0 || model > 2) return 0;
+    c->SetFemModel(static_cast<FemModel>(model));
+    return 1;
+}
+
+PHYSIK_B200_API unsigned PHYSIK_B200_GetLastStepFlags(PhysikWorldHandle world)
+{
+    World* w = AsWorld(world);
+    return w ? Guard([&] { return w->GetLastStepFlags(); }, 0u) : 0u;
+}
+
+PHYSIK_B200_API const char* PHYSIK_B200_GetLastError(void) { return g_error.c_str(); }
+
+PHYSIK_B200_API int PHYSIK_B200_PrepareScene(PhysikWorldHandle world, int upload)
+{
+    World* w = AsWorld(world);
+    if (!w) return -1;
+    return Guard([&] { return w->PrepareScene(upload != 0); }, -1);
+}
+
+PHYSIK_B200_API int PHYSIK_B200_GetSolverSizes(PhysikWorldHandle world, int* dynamicRows, int* blocks)
+{
+    World* w = AsWorld(world);
+    if (!w || w->GetSceneDynamicCount() < 0) return -1;
+    if (dynamicRows) *dynamicRows = w->GetSceneDynamicCount();
+    if (blocks) *blocks = w->GetSceneBlockCount();
+    return 0;
+}
+
+PHYSIK_B200_API int PHYSIK_B200_GetSolverPattern(PhysikWorldHandle world, int* rowStart, int* colIndex,
+                                                 int* nodeToDynamic)
+{
+    World* w = AsWorld(world);
+    if (!w || w->GetSceneDynamicCount() < 0) return -1;
+    if (rowStart) std::copy(w->GetSceneRowStart()->begin(), w->GetSceneRowStart()->end(), rowStart);
+    if (colIndex) std::copy(w->GetSceneColIndex()->begin(), w->GetSceneColIndex()->end(), colIndex);
+    if (nodeToDynamic) std::copy(w->GetSceneNodeToDyn()->begin(), w->GetSceneNodeToDyn()->end(), nodeToDynamic);
+    return 0;
+}
+
+PHYSIK_B200_API int PHYSIK_B200_GetSolverMasses(PhysikWorldHandle world, double* masses)
+{
+    World* w = AsWorld(world);
+    if (!w || !w->GetSceneMass()) return -1;
+    if (masses) std::copy(w->GetSceneMass()->begin(), w->GetSceneMass()->end(), masses);
+    return 0;
+}
+
+PHYSIK_B200_API int PHYSIK_B200_GetSolverSystem(PhysikWorldHandle world, double* values, double* rhs, double* minv,
+                                                double* deltaVelocity)
+{
+    World* w = AsWorld(world);
+    if (!w || !w->GetDeviceSystem()) return -1;
+    return Guard([&] { return pk_system_get_system_f64(w->GetDeviceSystem(), values, rhs, minv, deltaVelocity); }, -1);
+}
+
+PHYSIK_B200_API int PHYSIK_B200_EnableTiming(PhysikWorldHandle world, int on)
+{
+    World* w = AsWorld(world);
+    if (!w || !w->GetDeviceSystem()) return -1;
+    return pk_system_enable_timing(w->GetDeviceSystem(), on);
+}
+
+PHYSIK_B200_API int PHYSIK_B200_GetTimings(PhysikWorldHandle world, double* assembleMs, double* solveMs, int* steps,
+                                           long long* kernelLaunches)
+{
+    World* w = AsWorld(world);
+    if (!w || !w->GetDeviceSystem()) return -1;
+    return pk_system_timings(w->GetDeviceSystem(), assembleMs, solveMs, steps, kernelLaunches);
+}
+
+PHYSIK_B200_API int PHYSIK_B200_SetPcgGrid(PhysikWorldHandle world, int grid)
+{
+    World* w = AsWorld(world);
+    if (!w || !w->GetDeviceSystem()) return -1;
+    return pk_system_set_pcg_grid(w->GetDeviceSystem(), grid);
+}
+
+PHYSIK_B200_API void* PHYSIK_B200_GetStream(PhysikWorldHandle world)
+{
+    World* w = AsWorld(world);
+    return (w && w->GetDeviceSystem()) ? pk_system_stream(w->GetDeviceSystem()) : nullptr;
+}
+
+PHYSIK_B200_API int PHYSIK_B200_Synchronize(PhysikWorldHandle world)
+{
+    World* w = AsWorld(world);
+    if (!w) return -1;
+    return Guard([&] { (void)w->GetLastStepFlags(); return 0; }, -1);
+}
+
+}  // extern "C"

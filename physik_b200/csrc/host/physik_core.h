@@ -1,0 +1,457 @@
+// physik_core.h -- the host-side mirror of PhysiK's soft-body path, backed by the
+// sm_100a kernels of libpkcuda.  Class and member names follow the reference's
+// component API so code written against it keeps compiling:
+//
+//   TetMeshGenerator        include/PhysiK/Geometry/TetMeshGenerator.h:7-46
+//   SparseBlockMatrix       include/PhysiK/Math/SparseBlockMatrix.h:14-42
+//   ConjugateGradient*      include/PhysiK/Core/Solvers/Linear/ConjugateGradientSolver.h:12-35
+//   LinearSolver            include/PhysiK/Core/Solvers/Linear/LinearSolver.h:13-55
+//   SolverData              include/PhysiK/Core/Solvers/SolverData.h:15-134
+//   Component / TetMesh*    include/PhysiK/Components/Component.h:13-44,
+//                           TetMeshComponent.h:11-42, TetMeshPhysicsComponent.h:13-85
+//   World                   include/PhysiK/Core/World/World.h:30-137
+//
+// What differs by design: node state lives on the GPU (the host copies are synced on
+// access), SolverData owns a device BSR, and World::Step launches one device substep
+// (tet kernel, row kernel, cooperative PCG + integration) per substep.
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <utility>
+#include <vector>
+
+#include "physik_math.h"
+
+struct pk_system;
+
+namespace PhysiK {
+
+// ------------------------------------------------------------------ handles / data
+struct ComponentHandle {
+    std::uint32_t index = 0xFFFFFFFFu;
+    std::uint32_t generation = 0u;
+    bool IsValid() const { return index != 0xFFFFFFFFu && generation != 0u; }
+};
+
+struct Node {
+    int stateIndex = -1;
+    bool active = true;
+    bool fixed = false;
+    bool hasRotation = false;
+};
+
+struct Material {
+    float density = 1.0f;
+    float youngModulus = 25.0f;
+    float poissonRatio = 0.3f;
+    float damping = 0.25f;
+};
+
+struct Tet {
+    int node0 = -1, node1 = -1, node2 = -1, node3 = -1;
+    bool active = true;
+    float restVolume = 0.0f;
+    Mat3 restDmInverse;
+    Vec3 restPositions[4];
+    Vec3 shapeFunctionGradients[4];
+    float youngModulus = 25.0f;
+    float poissonRatio = 0.3f;
+    float damping = 0.25f;
+};
+
+enum class FemModel : std::uint32_t { Linear = 0, Corotational = 1, NeoHookean = 2 };
+enum class SolverMode { Explicit, ImplicitEuler };
+enum class ComponentExecutionPriority : int {
+    ScriptComponent = 100,
+    CollisionSphereComponent = 200,
+    TetMeshComponent = 300,
+    TetMeshPhysicsComponent = 400,
+    TopologyMeshComponent = 500,
+    TetMeshMapperComponent = 600,
+    SurfaceExtractionComponent = 700,
+    SurfaceVisualComponent = 800,
+    VisualMeshComponent = 900,
+    Default = 1000
+};
+
+// Device precision of a World (extension: the reference is FP32 only).
+enum class Precision : int { FP32 = 0, Mixed = 1, FP64 = 2 };
+
+// ------------------------------------------------------------------ generator
+struct TetMeshBuildOptions {
+    bool weldCoincidentNodes = true;
+    float weldTolerance = 1.0e-5f;
+    bool removeDegenerateTets = true;
+};
+struct TetMeshTopologyDiagnostics {
+    int boundaryFaceCount = 0;
+    int internalFaceCount = 0;
+    int nonManifoldFaceCount = 0;
+};
+struct GeneratedTetMesh {
+    std::vector<Vec3> positions;
+    std::vector<int> tetLocalNodeIndices;
+    TetMeshTopologyDiagnostics topologyDiagnostics;
+    int rawNodeCount = 0;
+    int rawTetCount = 0;
+    int weldedNodeCount = 0;
+    int weldedAwayNodeCount = 0;
+    int removedDegenerateTetCount = 0;
+    float weldTolerance = 0.0f;
+};
+class TetMeshGenerator {
+public:
+    static GeneratedTetMesh Generate(const Vec3* positions, int nodeCount, const int* tetLocalNodeIndices, int tetCount,
+                                     const TetMeshBuildOptions& options = TetMeshBuildOptions{});
+};
+
+// ------------------------------------------------------------------ sparse matrix
+// Canonical upper BSR (row <= col), per-row sorted unique columns, column-major blocks.
+class SparseBlockMatrix {
+public:
+    int blockCount = 0;
+    std::vector<int> rowStart;
+    std::vector<int> colIndex;
+    std::vector<Mat3> values;
+
+    void Clear();
+    void ClearValues();
+    void BuildPattern(int newBlockCount, const std::vector<std::pair<int, int>>& blockCoordinates);
+    bool AddBlock(int rowBlock, int colBlock, const Mat3& block);
+    // y = A x on the GPU (symmetric product of the upper storage).
+    void Multiply(const std::vector<float>& input, std::vector<float>& output) const;
+    void Multiply(const std::vector<Vec3>& input, std::vector<Vec3>& output) const;
+    int FindBlockIndex(int rowBlock, int colBlock) const;
+
+private:
+    std::unordered_map<std::uint64_t, int> blockLookup;
+    static std::uint64_t MakeKey(int rowBlock, int colBlock);
+};
+
+// ------------------------------------------------------------------ solver
+struct ConjugateGradientSettings {
+    int maxIterations = 128;
+    float tolerance = 1.0e-4f;
+    bool useJacobiPreconditioner = true;
+};
+struct ConjugateGradientResult {
+    int iterations = 0;
+    float residualNorm = 0.0f;
+    bool converged = false;
+};
+// Block-Jacobi PCG on the GPU with the reference's argument checks and results.
+ConjugateGradientResult SolvePreconditionedConjugateGradient(std::vector<Vec3>& x, const SparseBlockMatrix& A,
+                                                             const std::vector<Vec3>& b, int maxIterations,
+                                                             float tolerance, const std::vector<Mat3>& MInv,
+                                                             std::vector<Vec3>& r, std::vector<Vec3>& d,
+                                                             std::vector<Vec3>& qOrS);
+
+struct LinearSolveSettings {
+    int maxIterations = 128;
+    float tolerance = 1.0e-5f;
+    bool useJacobiPreconditioner = true;
+};
+struct LinearSolveResult {
+    int iterations = 0;
+    float residualNorm = 0.0f;
+    bool converged = false;
+};
+class LinearSolver {
+public:
+    virtual ~LinearSolver() = default;
+    virtual LinearSolveResult Solve(const SparseBlockMatrix& matrix, const std::vector<Vec3>& rhs,
+                                    std::vector<Vec3>& solution, const LinearSolveSettings& settings) = 0;
+};
+// The GPU solver behind the reference's CurrentLinearSolver seam.
+class CurrentLinearSolver final : public LinearSolver {
+public:
+    LinearSolveResult Solve(const SparseBlockMatrix& matrix, const std::vector<Vec3>& rhs, std::vector<Vec3>& solution,
+                            const LinearSolveSettings& settings) override;
+
+private:
+    std::vector<Mat3> inversePreconditioner;
+    std::vector<Vec3> residual, direction, temp;
+};
+LinearSolver& GetCurrentLinearSolver();
+
+// Index of the process-wide CUDA device used by the solver entry points (default 0).
+int GetSolverDevice();
+void SetSolverDevice(int device);
+
+class World;
+class TetMeshPhysicsComponent;
+
+// ------------------------------------------------------------------ SolverData
+class SolverData {
+public:
+    struct NodeForce {
+        int node = -1;
+        Vec3 force;
+    };
+    struct NodeMass {
+        int node = -1;
+        float mass = 0.0f;
+    };
+    struct StiffnessBlock {
+        int nodeA = -1;
+        int nodeB = -1;
+        Mat3 block;
+    };
+
+    void Clear();
+    void ClearTransientState();
+    void MarkImplicitPatternDirty() { implicitPatternDirty = true; }
+
+    void AddNodeForce(int node, const Vec3& force) { nodeForces.push_back(NodeForce{node, force}); }
+    void AddNodeMass(int node, float mass) { nodeMasses.push_back(NodeMass{node, mass}); }
+    void AddStiffnessBlock(int nodeA, int nodeB, const Mat3& block)
+    {
+        stiffnessBlocks.push_back(StiffnessBlock{nodeA, nodeB, block});
+    }
+    // Device path: a soft body whose per-tet forces and stiffness the GPU computes.
+    void AddFemBody(const TetMeshPhysicsComponent* body) { femBodies.push_back(body); }
+
+    const std::vector<NodeForce>& GetNodeForces() const { return nodeForces; }
+    const std::vector<NodeMass>& GetNodeMasses() const { return nodeMasses; }
+    const std::vector<StiffnessBlock>& GetStiffnessBlocks() const { return stiffnessBlocks; }
+    const std::vector<const TetMeshPhysicsComponent*>& GetFemBodies() const { return femBodies; }
+
+    void AssembleMasses(int nodeCount);
+    bool HasNodeMassContribution(int nodeIndex) const;
+    float GetAssembledMassForNode(int nodeIndex) const;
+
+    // Generic path (host-emitted forces, masses and blocks): builds SolverData's
+    // mapping and pattern, assembles A and b and solves on the GPU.
+    bool PrecomputeImplicitSolve(const std::vector<Node>& nodes, const std::vector<Vec3>& nodeVelocities, float dt);
+    bool SolveImplicitLinearSystem(const ConjugateGradientSettings& settings);
+    const LinearSolveResult& GetLastLinearSolveResult() const { return lastLinearSolveResult; }
+    int GetLastCgIterationCount() const { return lastLinearSolveResult.iterations; }
+    float GetLastCgResidualNorm() const { return lastLinearSolveResult.residualNorm; }
+
+    int GetDynamicBlockForNode(int nodeIndex) const;
+    int GetDynamicBlockCount() const { return dynamicBlockCount; }
+    const std::vector<Vec3>& GetDeltaVelocity() const { return deltaVelocity; }
+    const std::vector<float>& GetAssembledMasses() const { return assembledMasses; }
+    const std::vector<Vec3>& GetAssembledForces() const { return assembledForces; }
+    const SparseBlockMatrix& GetMatrix() const { return matrix; }
+    const std::vector<Vec3>& GetRhs() const { return rhs; }
+
+private:
+    friend class World;
+    bool BuildDynamicNodeMapping(const std::vector<Node>& nodes);
+
+    std::vector<NodeForce> nodeForces;
+    std::vector<NodeMass> nodeMasses;
+    std::vector<StiffnessBlock> stiffnessBlocks;
+    std::vector<const TetMeshPhysicsComponent*> femBodies;
+
+    std::vector<float> assembledMasses;
+    std::vector<Vec3> assembledForces;
+    std::vector<int> nodeToDynamicBlock;
+    int dynamicBlockCount = 0;
+    std::vector<Vec3> rhs;
+    SparseBlockMatrix matrix;
+    std::vector<Vec3> deltaVelocity;
+    LinearSolveResult lastLinearSolveResult;
+    bool implicitPatternDirty = true;
+    bool precomputeOk = false;
+    float precomputeDt = 0.0f;
+};
+
+// ------------------------------------------------------------------ components
+enum class PhysicsEventType { TetMeshTopologyChanged };
+
+class Component {
+public:
+    bool active = true;
+    virtual ComponentExecutionPriority GetExecutionPriority() const { return ComponentExecutionPriority::Default; }
+    virtual void PreUpdate(World&, float) {}
+    virtual void UpdateSystem(World&, SolverData&, float) {}
+    virtual void PostUpdate(World&, float) {}
+    virtual ~Component() = default;
+};
+
+class TetMeshComponent : public Component {
+public:
+    std::vector<Vec3> restNodePositions;
+    std::vector<Vec3> nodePositions;
+    std::vector<Tet> tets;
+    bool topologyDirty = false;
+
+    ComponentExecutionPriority GetExecutionPriority() const override
+    {
+        return ComponentExecutionPriority::TetMeshComponent;
+    }
+    void SetGeometry(const GeneratedTetMesh& generatedMesh);
+    int GetNodeCount() const { return static_cast<int>(restNodePositions.size()); }
+    int GetTetCount() const { return static_cast<int>(tets.size()); }
+    int GetTetNodeIndex(int tetIndex, int cornerIndex) const;
+    const Vec3& GetLocalRestPosition(int localNodeIndex) const;
+    const Vec3& GetLocalCurrentPosition(int localNodeIndex) const;
+    virtual int GetGlobalNodeIndex(int localNodeIndex) const;
+    virtual void SetLocalCurrentPosition(int localNodeIndex, const Vec3& position);
+    bool IsTetActive(int tetIndex) const;
+    virtual bool SetTetActive(int tetIndex, bool active);
+    virtual bool DeactivateTet(int tetIndex) { return SetTetActive(tetIndex, false); }
+    int GetActiveTetCount() const;
+    void PostUpdate(World& world, float dt) override;
+};
+
+struct TetMeshPhysicsComponentDesc {
+    Material material;
+    FemModel femModel = FemModel::Corotational;
+};
+
+class TetMeshPhysicsComponent : public TetMeshComponent {
+public:
+    static std::unique_ptr<TetMeshPhysicsComponent> CreateFromGeneratedTetMesh(World& world,
+                                                                               const GeneratedTetMesh& generatedMesh,
+                                                                               const Material& material);
+    static std::unique_ptr<TetMeshPhysicsComponent> CreateFromGeneratedTetMesh(
+        World& world, const GeneratedTetMesh& generatedMesh, const TetMeshPhysicsComponentDesc& desc);
+
+    ComponentExecutionPriority GetExecutionPriority() const override
+    {
+        return ComponentExecutionPriority::TetMeshPhysicsComponent;
+    }
+
+    int globalNodeBeginIndex = -1;
+    int globalNodeCount = 0;
+    std::vector<Vec3> nodeVelocities;
+    Material material;
+    FemModel selectedFemModel = FemModel::Corotational;
+    bool physicsEnabled = true;
+
+    void SetMaterial(const Material& value);
+    void SetFemModel(FemModel value) { selectedFemModel = value; ++version; }
+    FemModel GetFemModel() const { return selectedFemModel; }
+    void RebuildFemRestData();
+    // Per-element material edits (Tet::youngModulus etc.) take effect after this call.
+    void RebuildTetFemCache() { ++version; }
+    void SyncCurrentPositionsFromWorld(const World& world);
+
+    int GetGlobalNodeBeginIndex() const { return globalNodeBeginIndex; }
+    int GetGlobalNodeCount() const { return globalNodeCount; }
+    int GetGlobalNodeIndex(int localNodeIndex) const override;
+    bool SetTetActive(int tetIndex, bool active) override;
+
+    void UpdateSystem(World& world, SolverData& solverData, float dt) override;
+    void PostUpdate(World& world, float dt) override;
+
+    // Bumped whenever rest data, material or tet activity changes.
+    std::uint64_t version = 1;
+};
+
+// ------------------------------------------------------------------ world
+struct DeviceScene;
+
+class World {
+public:
+    World();
+    ~World();
+    World(const World&) = delete;
+    World& operator=(const World&) = delete;
+
+    void Step(float frameDt);
+
+    int AddNode(const Vec3& position);
+    ComponentHandle AddComponent(std::unique_ptr<Component> component);
+    Component* GetComponent(ComponentHandle handle);
+    const Component* GetComponent(ComponentHandle handle) const;
+    void DestroyComponent(ComponentHandle handle);
+    bool IsComponentHandleValid(ComponentHandle handle) const;
+
+    void SetSubstepCount(int count);
+    int GetSubstepCount() const { return substepCount; }
+    void SetSolverMode(SolverMode mode) { solverMode = mode; }
+    SolverMode GetSolverMode() const { return solverMode; }
+    void SetConjugateGradientTolerance(float tolerance);
+    float GetConjugateGradientTolerance() const { return conjugateGradientSettings.tolerance; }
+    void SetConjugateGradientMaxIterations(int maxIterations);
+    int GetConjugateGradientMaxIterations() const { return conjugateGradientSettings.maxIterations; }
+    int GetLastConjugateGradientIterations() const;
+    float GetLastConjugateGradientResidualNorm() const;
+    bool DidLastConjugateGradientSolveConverge() const;
+    void SetGravity(const Vec3& value) { gravity = value; }
+    const Vec3& GetGravity() const { return gravity; }
+
+    // Device precision (extension).  Changing it rebuilds the device scene.
+    void SetPrecision(Precision p);
+    Precision GetPrecision() const { return precision; }
+    void SetDevice(int device);
+
+    Node& GetNode(int index);
+    const Node& GetNode(int index) const;
+    const std::vector<Node>& GetNodes() const { return nodes; }
+    const Vec3& GetNodePosition(int nodeIndex) const;
+    const Vec3& GetNodeVelocity(int nodeIndex) const;
+    void SetNodePosition(int index, const Vec3& position);  // zeroes the velocity, as the reference does
+    void SetNodeVelocity(int index, const Vec3& velocity);
+    void SetNodeFixed(int nodeIndex, bool fixed);
+    bool IsNodeFixed(int nodeIndex) const;
+    void SetNodeActive(int nodeIndex, bool active);
+    const std::vector<std::unique_ptr<Component>>& GetComponents() const { return components; }
+
+    // Bulk state access (extension): 3 floats (or doubles) per node, world order.
+    void GetNodeStates(float* positions, float* velocities) const;
+    void SetNodeStates(const float* positions, const float* velocities);
+    void GetNodeStatesF64(double* positions, double* velocities) const;
+    void SetNodeStatesF64(const double* positions, const double* velocities);
+
+    // Device access for measurement and tests (extension).
+    pk_system* GetDeviceSystem();
+    // Builds the host side of the device scene (and uploads it when `upload`): runs the
+    // components' UpdateSystem pass, then mass / mapping / pattern.  Returns dynamic rows.
+    int PrepareScene(bool upload);
+    int GetSceneDynamicCount() const;
+    int GetSceneBlockCount() const;
+    const std::vector<int>* GetSceneRowStart() const;
+    const std::vector<int>* GetSceneColIndex() const;
+    const std::vector<int>* GetSceneNodeToDyn() const;
+    const std::vector<double>* GetSceneMass() const;
+    unsigned GetLastStepFlags() const;
+    void MarkTopologyDirty() { ++topologyVersion; }
+    std::uint64_t GetTopologyVersion() const { return topologyVersion; }
+
+private:
+    friend class TetMeshPhysicsComponent;
+    void EnsureHostState() const;
+    void SyncStats() const;
+    void PreUpdateComponents(float dt);
+    void PostUpdateComponents(float dt);
+    void RunSubstep(float dt);
+    void CollectContributions(float dt);
+    void EnsureScene(bool upload);
+
+    std::vector<Node> nodes;
+    mutable std::vector<Vec3> positions;
+    mutable std::vector<Vec3> velocities;
+    mutable bool hostStale = false;   // device holds newer state than the host copies
+    bool deviceStale = true;          // host copies hold newer state than the device
+
+    std::vector<std::unique_ptr<Component>> components;
+    std::vector<std::uint32_t> componentGenerations;
+    std::vector<std::uint32_t> freeComponentSlots;
+    std::multimap<int, Component*> orderedComponents;
+
+    int substepCount = 1;
+    SolverMode solverMode = SolverMode::Explicit;
+    ConjugateGradientSettings conjugateGradientSettings;
+    Vec3 gravity{};
+    Precision precision = Precision::FP32;
+    int device = 0;
+    std::uint64_t topologyVersion = 1;
+
+    SolverData solverData;
+    std::unique_ptr<DeviceScene> scene;
+    mutable ConjugateGradientResult lastConjugateGradientResult;
+    mutable unsigned lastFlags = 0;
+    mutable bool statsPending = false;
+};
+
+}  // namespace PhysiK

@@ -1,0 +1,868 @@
+// World, the tet-mesh components and SolverData, with the device scene behind them.
+//
+// Stepping follows World::Step (src/Core/World/World.cpp:32-73): pre-update, then per
+// substep the components' UpdateSystem in execution-priority order, then the solve and
+// integration, then post-update.  TetMeshPhysicsComponent::UpdateSystem registers its
+// body with SolverData; the World then runs the whole substep on the GPU through one
+// pk_system (tet kernel, row kernel, cooperative PCG with fused integration).
+//
+// The device scene (rest data, lumped masses, dynamic-node mapping, canonical upper
+// BSR pattern, per-row tet incidence lists) is built on the host when the topology
+// changes, with the reference's rules:
+//   rest data       FEMModel::InitializeTetRestData (FEMModel.cpp:504-548)
+//   lambda, mu      FEMModel BuildElasticityMatrix (FEMModel.cpp:174-200)
+//   lumped mass     FEMModel::ComputeLumpedMass + ApplyMassContribution
+//                   (FEMModel.cpp:681-713, TetMeshPhysicsComponent.cpp:127-152)
+//   mass check      World::ValidateNodeMasses (World.cpp:560-580) -- throws
+//   dynamic rows    SolverData::BuildDynamicNodeMapping (SolverData.cpp:239-258)
+//   pattern         diagonal of every dynamic row plus every tet-edge block between two
+//                   dynamic nodes, from all tets of each simulated body, active or not
+//                   (TetMeshPhysicsComponent.cpp:36-60, 221-232, 341-353;
+//                    SolverData.cpp:321-405; SparseBlockMatrix.cpp:83-129)
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../../include/pkcuda.h"
+#include "physik_core.h"
+
+namespace PhysiK {
+
+namespace {
+
+constexpr float kMinConjugateGradientTolerance = 1.0e-8f;
+constexpr float kMaxConjugateGradientTolerance = 1.0e-1f;
+constexpr int kMinConjugateGradientMaxIterations = 1;
+constexpr int kMaxConjugateGradientMaxIterations = 1024;
+
+const Vec3 kZero{};
+
+void Check(int rc, const char* what)
+{
+    if (rc != PK_OK) throw std::runtime_error(std::string(what) + ": " + pk_last_error());
+}
+
+// Rest data of one tet in precision T (FEMModel.cpp:504-548).
+template <class T>
+struct RestData {
+    T volume = T(0);
+    detail::M<T> dm_inv{};
+};
+
+template <class T>
+RestData<T> ComputeRest(const Vec3& p0, const Vec3& p1, const Vec3& p2, const Vec3& p3)
+{
+    using V = detail::V<T>;
+    auto cv = [](const Vec3& p) { return V{T(p.x), T(p.y), T(p.z)}; };
+    const V r0 = cv(p0), r1 = cv(p1), r2 = cv(p2), r3 = cv(p3);
+    const detail::M<T> dm{{detail::sub(r1, r0), detail::sub(r2, r0), detail::sub(r3, r0)}};
+    const T det = detail::det(dm);
+    RestData<T> out;
+    const T vol = std::abs(det) / T(6);
+    if (vol <= T(1.0e-8)) {
+        out.volume = T(0);
+        out.dm_inv = detail::M<T>{{V{0, 0, 0}, V{0, 0, 0}, V{0, 0, 0}}};
+        return out;
+    }
+    out.volume = vol;
+    out.dm_inv = detail::inverse(dm);
+    return out;
+}
+
+// lambda and mu of BuildElasticityMatrix in precision T (zero when E <= 0).
+template <class T>
+void LameParameters(float young, float poisson, T& lambda, T& mu)
+{
+    const T e = std::max(T(0), T(young));
+    lambda = T(0);
+    mu = T(0);
+    if (e <= T(0)) return;
+    const T nu = std::max(T(-0.99), std::min(T(0.49), T(poisson)));
+    lambda = e * nu / ((T(1) + nu) * (T(1) - T(2) * nu));
+    mu = e / (T(2) * (T(1) + nu));
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ TetMeshComponent
+void TetMeshComponent::SetGeometry(const GeneratedTetMesh& mesh)
+{
+    restNodePositions = mesh.positions;
+    nodePositions = restNodePositions;
+    tets.clear();
+    const int count = static_cast<int>(mesh.tetLocalNodeIndices.size() / 4u);
+    const int nodeCount = static_cast<int>(restNodePositions.size());
+    tets.reserve(static_cast<std::size_t>(std::max(0, count)));
+    for (int t = 0; t < count; ++t) {
+        const int* n = &mesh.tetLocalNodeIndices[static_cast<std::size_t>(4 * t)];
+        bool ok = true;
+        for (int k = 0; k < 4; ++k) ok = ok && n[k] >= 0 && n[k] < nodeCount;
+        if (!ok) continue;
+        Tet tet;
+        tet.node0 = n[0];
+        tet.node1 = n[1];
+        tet.node2 = n[2];
+        tet.node3 = n[3];
+        tets.push_back(tet);
+    }
+}
+
+int TetMeshComponent::GetTetNodeIndex(int tetIndex, int corner) const
+{
+    if (tetIndex < 0 || tetIndex >= static_cast<int>(tets.size())) return -1;
+    const Tet& t = tets[static_cast<std::size_t>(tetIndex)];
+    switch (corner) {
+    case 0: return t.node0;
+    case 1: return t.node1;
+    case 2: return t.node2;
+    case 3: return t.node3;
+    default: return -1;
+    }
+}
+
+const Vec3& TetMeshComponent::GetLocalRestPosition(int i) const
+{
+    if (i < 0 || i >= static_cast<int>(restNodePositions.size())) return kZero;
+    return restNodePositions[static_cast<std::size_t>(i)];
+}
+
+const Vec3& TetMeshComponent::GetLocalCurrentPosition(int i) const
+{
+    if (i < 0 || i >= static_cast<int>(nodePositions.size())) return kZero;
+    return nodePositions[static_cast<std::size_t>(i)];
+}
+
+int TetMeshComponent::GetGlobalNodeIndex(int) const { return -1; }
+
+void TetMeshComponent::SetLocalCurrentPosition(int i, const Vec3& p)
+{
+    if (i < 0 || i >= static_cast<int>(nodePositions.size())) return;
+    nodePositions[static_cast<std::size_t>(i)] = p;
+}
+
+bool TetMeshComponent::IsTetActive(int tetIndex) const
+{
+    if (tetIndex < 0 || tetIndex >= static_cast<int>(tets.size())) return false;
+    return tets[static_cast<std::size_t>(tetIndex)].active;
+}
+
+bool TetMeshComponent::SetTetActive(int tetIndex, bool activeValue)
+{
+    if (tetIndex < 0 || tetIndex >= static_cast<int>(tets.size())) return false;
+    Tet& t = tets[static_cast<std::size_t>(tetIndex)];
+    if (t.active == activeValue) return false;
+    t.active = activeValue;
+    topologyDirty = true;
+    return true;
+}
+
+int TetMeshComponent::GetActiveTetCount() const
+{
+    int c = 0;
+    for (const Tet& t : tets) c += t.active ? 1 : 0;
+    return c;
+}
+
+void TetMeshComponent::PostUpdate(World&, float) { topologyDirty = false; }
+
+// ------------------------------------------------------------------ TetMeshPhysicsComponent
+std::unique_ptr<TetMeshPhysicsComponent> TetMeshPhysicsComponent::CreateFromGeneratedTetMesh(
+    World& world, const GeneratedTetMesh& mesh, const Material& material)
+{
+    TetMeshPhysicsComponentDesc desc;
+    desc.material = material;
+    return CreateFromGeneratedTetMesh(world, mesh, desc);
+}
+
+std::unique_ptr<TetMeshPhysicsComponent> TetMeshPhysicsComponent::CreateFromGeneratedTetMesh(
+    World& world, const GeneratedTetMesh& mesh, const TetMeshPhysicsComponentDesc& desc)
+{
+    auto c = std::make_unique<TetMeshPhysicsComponent>();
+    c->material = desc.material;
+    c->selectedFemModel = desc.femModel;
+    c->SetGeometry(mesh);
+    c->globalNodeBeginIndex = static_cast<int>(world.GetNodes().size());
+    c->globalNodeCount = static_cast<int>(c->restNodePositions.size());
+    for (const Vec3& p : c->restNodePositions) world.AddNode(p);
+    c->RebuildFemRestData();
+    return c;
+}
+
+void TetMeshPhysicsComponent::SetMaterial(const Material& value)
+{
+    material = value;
+    for (Tet& t : tets) {
+        t.youngModulus = value.youngModulus;
+        t.poissonRatio = value.poissonRatio;
+        t.damping = value.damping;
+    }
+    ++version;
+}
+
+void TetMeshPhysicsComponent::RebuildFemRestData()
+{
+    for (Tet& t : tets) {
+        t.youngModulus = material.youngModulus;
+        t.poissonRatio = material.poissonRatio;
+        t.damping = material.damping;
+        const int n[4] = {t.node0, t.node1, t.node2, t.node3};
+        for (int k = 0; k < 4; ++k) t.restPositions[k] = restNodePositions[static_cast<std::size_t>(n[k])];
+        const RestData<float> rd = ComputeRest<float>(t.restPositions[0], t.restPositions[1], t.restPositions[2],
+                                                      t.restPositions[3]);
+        t.restVolume = rd.volume;
+        if (rd.volume <= 0.0f) {
+            t.restDmInverse = Mat3::Zero();
+            for (Vec3& g : t.shapeFunctionGradients) g = Vec3{};
+            continue;
+        }
+        const auto& m = rd.dm_inv;
+        t.restDmInverse = Mat3::FromColumns(Vec3{m.c[0].x, m.c[0].y, m.c[0].z}, Vec3{m.c[1].x, m.c[1].y, m.c[1].z},
+                                            Vec3{m.c[2].x, m.c[2].y, m.c[2].z});
+        t.shapeFunctionGradients[1] = Vec3{m.c[0].x, m.c[1].x, m.c[2].x};
+        t.shapeFunctionGradients[2] = Vec3{m.c[0].y, m.c[1].y, m.c[2].y};
+        t.shapeFunctionGradients[3] = Vec3{m.c[0].z, m.c[1].z, m.c[2].z};
+        t.shapeFunctionGradients[0] =
+            -(t.shapeFunctionGradients[1] + t.shapeFunctionGradients[2] + t.shapeFunctionGradients[3]);
+    }
+    ++version;
+}
+
+void TetMeshPhysicsComponent::SyncCurrentPositionsFromWorld(const World& world)
+{
+    nodePositions.resize(static_cast<std::size_t>(globalNodeCount));
+    nodeVelocities.resize(static_cast<std::size_t>(globalNodeCount));
+    for (int i = 0; i < globalNodeCount; ++i) {
+        const int g = GetGlobalNodeIndex(i);
+        if (g < 0 || g >= static_cast<int>(world.GetNodes().size())) continue;
+        nodePositions[static_cast<std::size_t>(i)] = world.GetNodePosition(g);
+        nodeVelocities[static_cast<std::size_t>(i)] = world.GetNodeVelocity(g);
+    }
+}
+
+int TetMeshPhysicsComponent::GetGlobalNodeIndex(int local) const
+{
+    if (globalNodeBeginIndex < 0 || local < 0 || local >= globalNodeCount) return -1;
+    return globalNodeBeginIndex + local;
+}
+
+bool TetMeshPhysicsComponent::SetTetActive(int tetIndex, bool activeValue)
+{
+    const bool changed = TetMeshComponent::SetTetActive(tetIndex, activeValue);
+    if (changed) ++version;
+    return changed;
+}
+
+// The device computes this body's forces and stiffness; the host only registers it.
+// The component-local position copies are refreshed on demand (SyncCurrentPositionsFromWorld)
+// rather than every substep, so a step never waits for a device-to-host copy.
+void TetMeshPhysicsComponent::UpdateSystem(World&, SolverData& solverData, float)
+{
+    if (!physicsEnabled) return;
+    solverData.AddFemBody(this);
+}
+
+void TetMeshPhysicsComponent::PostUpdate(World& world, float dt) { TetMeshComponent::PostUpdate(world, dt); }
+
+// ------------------------------------------------------------------ SolverData
+void SolverData::Clear()
+{
+    ClearTransientState();
+    matrix.Clear();
+    implicitPatternDirty = true;
+}
+
+void SolverData::ClearTransientState()
+{
+    nodeForces.clear();
+    nodeMasses.clear();
+    stiffnessBlocks.clear();
+    femBodies.clear();
+    assembledMasses.clear();
+    assembledForces.clear();
+    nodeToDynamicBlock.clear();
+    dynamicBlockCount = 0;
+    rhs.clear();
+    deltaVelocity.clear();
+    lastLinearSolveResult = LinearSolveResult{};
+    precomputeOk = false;
+}
+
+void SolverData::AssembleMasses(int nodeCount)
+{
+    assembledMasses.assign(static_cast<std::size_t>(std::max(0, nodeCount)), 0.0f);
+    for (const NodeMass& m : nodeMasses) {
+        if (m.node < 0 || m.node >= nodeCount || !std::isfinite(m.mass) || m.mass <= 0.0f) continue;
+        assembledMasses[static_cast<std::size_t>(m.node)] += m.mass;
+    }
+}
+
+bool SolverData::HasNodeMassContribution(int nodeIndex) const
+{
+    for (const NodeMass& m : nodeMasses)
+        if (m.node == nodeIndex) return true;
+    return false;
+}
+
+float SolverData::GetAssembledMassForNode(int nodeIndex) const
+{
+    if (nodeIndex < 0 || nodeIndex >= static_cast<int>(assembledMasses.size())) return 0.0f;
+    return assembledMasses[static_cast<std::size_t>(nodeIndex)];
+}
+
+int SolverData::GetDynamicBlockForNode(int nodeIndex) const
+{
+    if (nodeIndex < 0 || nodeIndex >= static_cast<int>(nodeToDynamicBlock.size())) return -1;
+    return nodeToDynamicBlock[static_cast<std::size_t>(nodeIndex)];
+}
+
+bool SolverData::BuildDynamicNodeMapping(const std::vector<Node>& nodes)
+{
+    nodeToDynamicBlock.assign(nodes.size(), -1);
+    dynamicBlockCount = 0;
+    for (std::size_t i = 0; i < nodes.size(); ++i) {
+        const float m = assembledMasses[i];
+        if (nodes[i].active && !nodes[i].fixed && std::isfinite(m) && m > 0.0f)
+            nodeToDynamicBlock[i] = dynamicBlockCount++;
+    }
+    return dynamicBlockCount > 0;
+}
+
+// ------------------------------------------------------------------ device scene
+// Host-built topology of the simulated bodies plus the device system it is uploaded to.
+struct DeviceScene {
+    pk_system* sys = nullptr;
+    Precision precision = Precision::FP32;
+    int device = 0;
+    std::uint64_t worldVersion = 0;
+    std::vector<std::pair<const TetMeshPhysicsComponent*, std::uint64_t>> bodies;
+    bool built = false;
+    bool uploaded = false;
+    int nodeCount = 0;
+    int dynCount = 0;
+    int tetCount = 0;
+    std::vector<int> nodeToDyn, dynToNode, rowStart, colIndex, tetNodes, incStart, incList;
+    std::vector<unsigned char> enabled;
+    std::vector<double> mass, dmInv, volume, lam, mu, damp;
+
+    ~DeviceScene()
+    {
+        if (sys) pk_system_destroy(sys);
+    }
+    bool Matches(const World& w, const std::vector<const TetMeshPhysicsComponent*>& fem) const
+    {
+        if (!built || worldVersion != w.GetTopologyVersion() || precision != w.GetPrecision()) return false;
+        if (fem.size() != bodies.size()) return false;
+        for (std::size_t i = 0; i < fem.size(); ++i)
+            if (fem[i] != bodies[i].first || fem[i]->version != bodies[i].second) return false;
+        return true;
+    }
+};
+
+namespace {
+
+template <class T>
+void BuildHostScene(DeviceScene& sc, const World& w, const std::vector<const TetMeshPhysicsComponent*>& fem)
+{
+    const std::vector<Node>& nodes = w.GetNodes();
+    const int nn = static_cast<int>(nodes.size());
+    sc.tetNodes.clear();
+    sc.enabled.clear();
+    sc.dmInv.clear();
+    sc.volume.clear();
+    sc.lam.clear();
+    sc.mu.clear();
+    sc.damp.clear();
+    std::vector<T> massT(static_cast<std::size_t>(nn), T(0));
+    for (const TetMeshPhysicsComponent* body : fem) {
+        const int base = body->GetGlobalNodeBeginIndex();
+        const T density = std::max(T(0), T(body->material.density));
+        const bool femImplemented = body->GetFemModel() != FemModel::NeoHookean;
+        const unsigned char linearBit = body->GetFemModel() == FemModel::Linear ? 2 : 0;
+        for (const Tet& t : body->tets) {
+            const int n[4] = {t.node0 + base, t.node1 + base, t.node2 + base, t.node3 + base};
+            const RestData<T> rd = ComputeRest<T>(body->restNodePositions[t.node0], body->restNodePositions[t.node1],
+                                                  body->restNodePositions[t.node2], body->restNodePositions[t.node3]);
+            for (int k = 0; k < 4; ++k) sc.tetNodes.push_back(n[k]);
+            sc.enabled.push_back(static_cast<unsigned char>(
+                (t.active && rd.volume > T(0) && femImplemented ? 1 : 0) | linearBit));
+            for (int c = 0; c < 3; ++c) {
+                sc.dmInv.push_back(static_cast<double>(rd.dm_inv.c[c].x));
+                sc.dmInv.push_back(static_cast<double>(rd.dm_inv.c[c].y));
+                sc.dmInv.push_back(static_cast<double>(rd.dm_inv.c[c].z));
+            }
+            sc.volume.push_back(static_cast<double>(rd.volume));
+            T l, m;
+            LameParameters<T>(t.youngModulus, t.poissonRatio, l, m);
+            sc.lam.push_back(static_cast<double>(l));
+            sc.mu.push_back(static_cast<double>(m));
+            sc.damp.push_back(static_cast<double>(T(t.damping)));
+            // Lumped mass rho V / 4 to the non-fixed nodes of active tets, in tet order.
+            if (std::isfinite(static_cast<double>(density)) && t.active && std::isfinite(static_cast<double>(rd.volume)) &&
+                rd.volume > T(0)) {
+                const T nodal = density * rd.volume * T(0.25);
+                if (std::isfinite(static_cast<double>(nodal)) && nodal > T(0))
+                    for (int k = 0; k < 4; ++k)
+                        if (!nodes[static_cast<std::size_t>(n[k])].fixed) massT[static_cast<std::size_t>(n[k])] += nodal;
+            }
+        }
+    }
+    // World::ValidateNodeMasses
+    for (int i = 0; i < nn; ++i) {
+        const Node& nd = nodes[static_cast<std::size_t>(i)];
+        if (!nd.active || nd.fixed) continue;
+        const T m = massT[static_cast<std::size_t>(i)];
+        if (std::isfinite(static_cast<double>(m)) && m > T(0)) continue;
+        throw std::runtime_error("Non-fixed node has no physical mass contribution. nodeIndex=" + std::to_string(i));
+    }
+    // Dynamic rows.
+    sc.nodeToDyn.assign(static_cast<std::size_t>(nn), -1);
+    sc.dynToNode.clear();
+    for (int i = 0; i < nn; ++i) {
+        const Node& nd = nodes[static_cast<std::size_t>(i)];
+        const T m = massT[static_cast<std::size_t>(i)];
+        if (nd.active && !nd.fixed && std::isfinite(static_cast<double>(m)) && m > T(0)) {
+            sc.nodeToDyn[static_cast<std::size_t>(i)] = static_cast<int>(sc.dynToNode.size());
+            sc.dynToNode.push_back(i);
+        }
+    }
+    const int dyn = static_cast<int>(sc.dynToNode.size());
+    const int tetCount = static_cast<int>(sc.enabled.size());
+    // Per-row incidence lists (ascending tet id) and the canonical upper pattern.
+    sc.incStart.assign(static_cast<std::size_t>(dyn) + 1, 0);
+    for (int t = 0; t < tetCount; ++t)
+        for (int k = 0; k < 4; ++k) {
+            const int r = sc.nodeToDyn[static_cast<std::size_t>(sc.tetNodes[4 * t + k])];
+            if (r >= 0) sc.incStart[static_cast<std::size_t>(r) + 1]++;
+        }
+    for (int r = 0; r < dyn; ++r) sc.incStart[r + 1] += sc.incStart[r];
+    sc.incList.assign(static_cast<std::size_t>(sc.incStart[dyn]), 0);
+    {
+        std::vector<int> fill(sc.incStart.begin(), sc.incStart.end() - 1);
+        for (int t = 0; t < tetCount; ++t)
+            for (int k = 0; k < 4; ++k) {
+                const int r = sc.nodeToDyn[static_cast<std::size_t>(sc.tetNodes[4 * t + k])];
+                if (r >= 0) sc.incList[static_cast<std::size_t>(fill[r]++)] = t * 4 + k;
+            }
+    }
+    sc.rowStart.assign(static_cast<std::size_t>(dyn) + 1, 0);
+    sc.colIndex.clear();
+    std::vector<int> cols;
+    for (int r = 0; r < dyn; ++r) {
+        cols.clear();
+        cols.push_back(r);
+        for (int i = sc.incStart[r]; i < sc.incStart[r + 1]; ++i) {
+            const int t = sc.incList[static_cast<std::size_t>(i)] >> 2;
+            for (int k = 0; k < 4; ++k) {
+                const int c = sc.nodeToDyn[static_cast<std::size_t>(sc.tetNodes[4 * t + k])];
+                if (c >= r) cols.push_back(c);
+            }
+        }
+        std::sort(cols.begin(), cols.end());
+        cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+        sc.colIndex.insert(sc.colIndex.end(), cols.begin(), cols.end());
+        sc.rowStart[static_cast<std::size_t>(r) + 1] = static_cast<int>(sc.colIndex.size());
+    }
+    sc.mass.assign(massT.begin(), massT.end());
+    sc.nodeCount = nn;
+    sc.dynCount = dyn;
+    sc.tetCount = tetCount;
+}
+
+void UploadScene(DeviceScene& sc, const std::vector<Vec3>& positions, const std::vector<Vec3>& velocities)
+{
+    const int nn = sc.nodeCount;
+    Check(pk_system_set_nodes(sc.sys, nn, sc.nodeToDyn.data(), sc.mass.data()), "set_nodes");
+    std::vector<float> x(3 * static_cast<std::size_t>(nn)), v(3 * static_cast<std::size_t>(nn));
+    for (int i = 0; i < nn; ++i) {
+        x[3 * i] = positions[i].x; x[3 * i + 1] = positions[i].y; x[3 * i + 2] = positions[i].z;
+        v[3 * i] = velocities[i].x; v[3 * i + 1] = velocities[i].y; v[3 * i + 2] = velocities[i].z;
+    }
+    Check(pk_system_set_state_f32(sc.sys, x.data(), v.data()), "set_state");
+    Check(pk_system_set_tets(sc.sys, sc.tetCount, sc.tetNodes.data(), sc.enabled.data(), sc.dmInv.data(),
+                             sc.volume.data(), sc.lam.data(), sc.mu.data(), sc.damp.data()),
+          "set_tets");
+    Check(pk_system_set_pattern(sc.sys, sc.dynCount, sc.dynToNode.data(), sc.rowStart.data(), sc.colIndex.data(),
+                                sc.incStart.data(), sc.incList.data()),
+          "set_pattern");
+    sc.uploaded = true;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ World
+World::World() = default;
+World::~World() = default;
+
+void World::SetSubstepCount(int count) { substepCount = std::max(1, count); }
+
+void World::SetConjugateGradientTolerance(float tolerance)
+{
+    if (!std::isfinite(tolerance)) return;
+    conjugateGradientSettings.tolerance =
+        std::clamp(tolerance, kMinConjugateGradientTolerance, kMaxConjugateGradientTolerance);
+}
+
+void World::SetConjugateGradientMaxIterations(int maxIterations)
+{
+    conjugateGradientSettings.maxIterations =
+        std::clamp(maxIterations, kMinConjugateGradientMaxIterations, kMaxConjugateGradientMaxIterations);
+}
+
+void World::SetPrecision(Precision p)
+{
+    if (p == precision) return;
+    EnsureHostState();
+    precision = p;
+    scene.reset();
+    deviceStale = true;
+    ++topologyVersion;
+}
+
+void World::SetDevice(int dev)
+{
+    if (dev == device) return;
+    EnsureHostState();
+    device = dev;
+    scene.reset();
+    deviceStale = true;
+    ++topologyVersion;
+}
+
+int World::AddNode(const Vec3& position)
+{
+    EnsureHostState();
+    Node n;
+    n.stateIndex = static_cast<int>(positions.size());
+    nodes.push_back(n);
+    positions.push_back(position);
+    velocities.push_back(Vec3{});
+    deviceStale = true;
+    ++topologyVersion;
+    return static_cast<int>(nodes.size()) - 1;
+}
+
+ComponentHandle World::AddComponent(std::unique_ptr<Component> component)
+{
+    if (!component) return ComponentHandle{};
+    Component* raw = component.get();
+    std::uint32_t slot;
+    if (!freeComponentSlots.empty()) {
+        slot = freeComponentSlots.back();
+        freeComponentSlots.pop_back();
+        components[slot] = std::move(component);
+    } else {
+        components.push_back(std::move(component));
+        componentGenerations.push_back(1u);
+        slot = static_cast<std::uint32_t>(components.size() - 1);
+    }
+    orderedComponents.emplace(static_cast<int>(raw->GetExecutionPriority()), raw);
+    ++topologyVersion;
+    return ComponentHandle{slot, componentGenerations[slot]};
+}
+
+bool World::IsComponentHandleValid(ComponentHandle h) const
+{
+    if (!h.IsValid() || h.index >= components.size()) return false;
+    return componentGenerations[h.index] == h.generation && components[h.index] != nullptr;
+}
+
+Component* World::GetComponent(ComponentHandle h) { return IsComponentHandleValid(h) ? components[h.index].get() : nullptr; }
+const Component* World::GetComponent(ComponentHandle h) const
+{
+    return IsComponentHandleValid(h) ? components[h.index].get() : nullptr;
+}
+
+void World::DestroyComponent(ComponentHandle h)
+{
+    if (!IsComponentHandleValid(h)) return;
+    Component* c = components[h.index].get();
+    for (auto it = orderedComponents.begin(); it != orderedComponents.end();)
+        it = it->second == c ? orderedComponents.erase(it) : std::next(it);
+    components[h.index].reset();
+    if (++componentGenerations[h.index] == 0u) componentGenerations[h.index] = 1u;
+    freeComponentSlots.push_back(h.index);
+    ++topologyVersion;
+}
+
+Node& World::GetNode(int index) { return nodes.at(static_cast<std::size_t>(index)); }
+const Node& World::GetNode(int index) const { return nodes.at(static_cast<std::size_t>(index)); }
+
+void World::EnsureHostState() const
+{
+    if (!hostStale || !scene || !scene->uploaded) return;
+    const std::size_t n = positions.size();
+    std::vector<float> x(3 * n), v(3 * n);
+    Check(pk_system_get_state_f32(scene->sys, x.data(), v.data()), "get_state");
+    for (std::size_t i = 0; i < n; ++i) {
+        positions[i] = Vec3{x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+        velocities[i] = Vec3{v[3 * i], v[3 * i + 1], v[3 * i + 2]};
+    }
+    hostStale = false;
+}
+
+const Vec3& World::GetNodePosition(int i) const
+{
+    EnsureHostState();
+    return positions.at(static_cast<std::size_t>(i));
+}
+
+const Vec3& World::GetNodeVelocity(int i) const
+{
+    EnsureHostState();
+    return velocities.at(static_cast<std::size_t>(i));
+}
+
+void World::SetNodePosition(int i, const Vec3& p)
+{
+    EnsureHostState();
+    positions.at(static_cast<std::size_t>(i)) = p;
+    velocities.at(static_cast<std::size_t>(i)) = Vec3{};
+    deviceStale = true;
+}
+
+void World::SetNodeVelocity(int i, const Vec3& v)
+{
+    EnsureHostState();
+    velocities.at(static_cast<std::size_t>(i)) = v;
+    deviceStale = true;
+}
+
+void World::SetNodeFixed(int i, bool fixed)
+{
+    EnsureHostState();
+    Node& n = nodes.at(static_cast<std::size_t>(i));
+    if (fixed) velocities[static_cast<std::size_t>(i)] = Vec3{};
+    if (n.fixed != fixed) ++topologyVersion;
+    n.fixed = fixed;
+    deviceStale = true;
+}
+
+bool World::IsNodeFixed(int i) const { return nodes.at(static_cast<std::size_t>(i)).fixed; }
+
+void World::SetNodeActive(int i, bool activeValue)
+{
+    EnsureHostState();
+    Node& n = nodes.at(static_cast<std::size_t>(i));
+    if (n.active != activeValue) ++topologyVersion;
+    n.active = activeValue;
+    if (!activeValue) velocities[static_cast<std::size_t>(i)] = Vec3{};
+    deviceStale = true;
+}
+
+void World::GetNodeStates(float* x, float* v) const
+{
+    if (hostStale && scene && scene->uploaded) {
+        Check(pk_system_get_state_f32(scene->sys, x, v), "get_state");
+        return;
+    }
+    for (std::size_t i = 0; i < positions.size(); ++i) {
+        if (x) { x[3 * i] = positions[i].x; x[3 * i + 1] = positions[i].y; x[3 * i + 2] = positions[i].z; }
+        if (v) { v[3 * i] = velocities[i].x; v[3 * i + 1] = velocities[i].y; v[3 * i + 2] = velocities[i].z; }
+    }
+}
+
+void World::SetNodeStates(const float* x, const float* v)
+{
+    const bool live = scene && scene->uploaded && !deviceStale && scene->worldVersion == topologyVersion;
+    if (live && x && v) {
+        Check(pk_system_set_state_f32(scene->sys, x, v), "set_state");
+        hostStale = true;
+        return;
+    }
+    EnsureHostState();
+    for (std::size_t i = 0; i < positions.size(); ++i) {
+        if (x) positions[i] = Vec3{x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+        if (v) velocities[i] = Vec3{v[3 * i], v[3 * i + 1], v[3 * i + 2]};
+    }
+    deviceStale = true;
+}
+
+void World::GetNodeStatesF64(double* x, double* v) const
+{
+    if (hostStale && scene && scene->uploaded) {
+        Check(pk_system_get_state_f64(scene->sys, x, v), "get_state");
+        return;
+    }
+    for (std::size_t i = 0; i < positions.size(); ++i) {
+        if (x) { x[3 * i] = positions[i].x; x[3 * i + 1] = positions[i].y; x[3 * i + 2] = positions[i].z; }
+        if (v) { v[3 * i] = velocities[i].x; v[3 * i + 1] = velocities[i].y; v[3 * i + 2] = velocities[i].z; }
+    }
+}
+
+void World::SetNodeStatesF64(const double* x, const double* v)
+{
+    const bool live = scene && scene->uploaded && !deviceStale && scene->worldVersion == topologyVersion;
+    if (live && x && v) {
+        Check(pk_system_set_state_f64(scene->sys, x, v), "set_state");
+        hostStale = true;
+        return;
+    }
+    EnsureHostState();
+    for (std::size_t i = 0; i < positions.size(); ++i) {
+        if (x) positions[i] = Vec3{static_cast<float>(x[3 * i]), static_cast<float>(x[3 * i + 1]),
+                                   static_cast<float>(x[3 * i + 2])};
+        if (v) velocities[i] = Vec3{static_cast<float>(v[3 * i]), static_cast<float>(v[3 * i + 1]),
+                                    static_cast<float>(v[3 * i + 2])};
+    }
+    deviceStale = true;
+}
+
+void World::SyncStats() const
+{
+    if (!statsPending || !scene || !scene->uploaded) return;
+    pk_step_stats st{};
+    const int rc = pk_system_stats(scene->sys, &st);
+    statsPending = false;
+    lastFlags = st.flags;
+    if (rc == PK_ERR_TIMEOUT) throw std::runtime_error("device step timed out in a grid barrier");
+    Check(rc, "stats");
+    lastConjugateGradientResult.iterations = st.iterations;
+    lastConjugateGradientResult.residualNorm = static_cast<float>(st.residual_norm);
+    lastConjugateGradientResult.converged = st.converged != 0;
+}
+
+int World::GetLastConjugateGradientIterations() const
+{
+    SyncStats();
+    return lastConjugateGradientResult.iterations;
+}
+float World::GetLastConjugateGradientResidualNorm() const
+{
+    SyncStats();
+    return lastConjugateGradientResult.residualNorm;
+}
+bool World::DidLastConjugateGradientSolveConverge() const
+{
+    SyncStats();
+    return lastConjugateGradientResult.converged;
+}
+unsigned World::GetLastStepFlags() const
+{
+    SyncStats();
+    return lastFlags;
+}
+
+pk_system* World::GetDeviceSystem() { return scene && scene->uploaded ? scene->sys : nullptr; }
+
+void World::PreUpdateComponents(float dt)
+{
+    for (auto& e : orderedComponents)
+        if (e.second && e.second->active) e.second->PreUpdate(*this, dt);
+}
+
+void World::PostUpdateComponents(float dt)
+{
+    for (auto& e : orderedComponents)
+        if (e.second && e.second->active) e.second->PostUpdate(*this, dt);
+}
+
+void World::CollectContributions(float dt)
+{
+    solverData.ClearTransientState();
+    for (auto& e : orderedComponents)
+        if (e.second && e.second->active) e.second->UpdateSystem(*this, solverData, dt);
+    if (!solverData.GetNodeForces().empty() || !solverData.GetNodeMasses().empty() ||
+        !solverData.GetStiffnessBlocks().empty())
+        throw std::runtime_error("host-emitted SolverData contributions are not supported by the device step");
+}
+
+void World::EnsureScene(bool upload)
+{
+    const std::vector<const TetMeshPhysicsComponent*>& fem = solverData.GetFemBodies();
+    if (!scene || scene->precision != precision || scene->device != device) {
+        EnsureHostState();
+        scene = std::make_unique<DeviceScene>();
+        scene->precision = precision;
+        scene->device = device;
+    }
+    if (!scene->Matches(*this, fem)) {
+        EnsureHostState();
+        scene->built = false;
+        scene->uploaded = false;
+        scene->bodies.clear();
+        for (const TetMeshPhysicsComponent* b : fem) scene->bodies.emplace_back(b, b->version);
+        if (precision == Precision::FP64)
+            BuildHostScene<double>(*scene, *this, fem);
+        else
+            BuildHostScene<float>(*scene, *this, fem);
+        scene->worldVersion = topologyVersion;
+        scene->built = true;
+    }
+    if (upload && !scene->uploaded) {
+        EnsureHostState();
+        if (!scene->sys) Check(pk_system_create(device, static_cast<int>(precision), &scene->sys), "pk_system_create");
+        UploadScene(*scene, positions, velocities);
+        deviceStale = false;
+        hostStale = false;
+    }
+}
+
+int World::PrepareScene(bool upload)
+{
+    CollectContributions(0.0f);
+    EnsureScene(upload);
+    return scene->dynCount;
+}
+
+int World::GetSceneDynamicCount() const { return scene && scene->built ? scene->dynCount : -1; }
+int World::GetSceneBlockCount() const
+{
+    return scene && scene->built ? static_cast<int>(scene->colIndex.size()) : -1;
+}
+const std::vector<int>* World::GetSceneRowStart() const { return scene && scene->built ? &scene->rowStart : nullptr; }
+const std::vector<int>* World::GetSceneColIndex() const { return scene && scene->built ? &scene->colIndex : nullptr; }
+const std::vector<int>* World::GetSceneNodeToDyn() const { return scene && scene->built ? &scene->nodeToDyn : nullptr; }
+const std::vector<double>* World::GetSceneMass() const { return scene && scene->built ? &scene->mass : nullptr; }
+
+void World::RunSubstep(float dt)
+{
+    CollectContributions(dt);
+    EnsureScene(true);
+    if (deviceStale) {
+        std::vector<float> x(3 * positions.size()), v(3 * positions.size());
+        for (std::size_t i = 0; i < positions.size(); ++i) {
+            x[3 * i] = positions[i].x; x[3 * i + 1] = positions[i].y; x[3 * i + 2] = positions[i].z;
+            v[3 * i] = velocities[i].x; v[3 * i + 1] = velocities[i].y; v[3 * i + 2] = velocities[i].z;
+        }
+        Check(pk_system_set_state_f32(scene->sys, x.data(), v.data()), "set_state");
+        deviceStale = false;
+    }
+    if (scene->dynCount == 0) {
+        // No dynamic node: PrecomputeImplicitSolve fails and nothing moves.
+        if (solverMode == SolverMode::ImplicitEuler) lastConjugateGradientResult = ConjugateGradientResult{};
+        return;
+    }
+    pk_step_params p{};
+    p.dt = dt;
+    p.gravity[0] = gravity.x;
+    p.gravity[1] = gravity.y;
+    p.gravity[2] = gravity.z;
+    p.max_iterations = conjugateGradientSettings.maxIterations;
+    p.tolerance = conjugateGradientSettings.tolerance;
+    p.use_jacobi = conjugateGradientSettings.useJacobiPreconditioner ? 1 : 0;
+    p.linear = 0;
+    p.explicit_mode = solverMode == SolverMode::Explicit ? 1 : 0;
+    p.integrate = 1;
+    Check(pk_system_step(scene->sys, &p), "pk_system_step");
+    hostStale = true;
+    if (solverMode == SolverMode::ImplicitEuler) statsPending = true;
+}
+
+void World::Step(float frameDt)
+{
+    if (frameDt < 0.0f) return;
+    PreUpdateComponents(frameDt);
+    if (frameDt == 0.0f) {
+        PostUpdateComponents(frameDt);
+        return;
+    }
+    const int steps = std::max(1, substepCount);
+    const float dt = frameDt / static_cast<float>(steps);
+    for (int i = 0; i < steps; ++i) RunSubstep(dt);
+    PostUpdateComponents(frameDt);
+}
+
+}  // namespace PhysiK

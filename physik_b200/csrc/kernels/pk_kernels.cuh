@@ -1,0 +1,136 @@
+// pk_kernels.cuh -- device-side views and launchers shared by the kernel and ABI
+// translation units.  Everything here is internal to libpkcuda.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pk_math.cuh"
+
+namespace pk {
+
+// Step flags (mirrored in include/pkcuda.h as PK_FLAG_*).
+enum : unsigned {
+    kFlagPrecomputeFailed = 0x1u,
+    kFlagSingularDiag = 0x2u,
+    kFlagInvalidRhs = 0x4u,
+    kFlagBreakdown = 0x8u,
+    kFlagNonFiniteDv = 0x10u,
+    kFlagIntegrateAbort = 0x20u,
+    kFlagPolarIdentity = 0x40u,
+    kFlagPolarFp64 = 0x80u,
+    kFlagBarrierTimeout = 0x100u,
+    kFlagRowTooLong = 0x200u,
+    kFlagSolved = 0x1000u,
+    kFlagIntegrated = 0x2000u,
+    kFlagConverged = 0x4000u,
+};
+
+struct GridSync {
+    unsigned arrive;
+    unsigned gen;
+    int err;
+    int pad;
+};
+
+struct DevStats {
+    int iterations;
+    int converged;
+    double residual_norm;
+    unsigned flags;
+    int polar_fp64_count;
+    int polar_identity_count;
+    int pad;
+};
+
+// Upper-stored symmetric BSR plus its transpose index: for row r, the blocks (c, r)
+// with c < r are lt_block[lt_start[r] .. lt_start[r+1]) and c = lt_row[...].
+template <class Real>
+struct BsrView {
+    int n;
+    const int* row_start;
+    const int* col;
+    const Real* values;  // 9 per block, column-major
+    const int* lt_start;
+    const int* lt_row;
+    const int* lt_block;
+};
+
+template <class Real>
+struct TetView {
+    int tet_count;
+    const int4* nodes;               // world node ids
+    const unsigned char* enabled;    // bit 0: active, rest volume > 0, body simulated; bit 1: linear FEM
+    const Real* dm_inv;              // 9 per tet, column-major
+    const Real* params;              // 4 per tet: rest volume, lambda, mu, damping
+    Real* rot;                       // 9 per tet (R), rot[9t] = NaN when the tet is skipped this step
+    Real* stress;                    // 9 per tet (S = R * V * sigma)
+};
+
+template <class Real>
+struct AssemblyArgs {
+    TetView<Real> tets;
+    BsrView<Real> a;
+    int node_count;
+    const int* dyn_to_node;
+    const int* node_to_dyn;
+    const Real* mass;                // per world node
+    const Real* x;                   // 3 per world node
+    Real* v;                         // 3 per world node (written only in explicit mode)
+    Real* x_out;                     // explicit mode position update target
+    const int* inc_start;            // per dyn row
+    const int* inc_list;             // t*4 + a
+    Real* values;                    // out: A blocks
+    Real* rhs;                       // out: b
+    Real* minv;                      // out: block-Jacobi inverse
+    Real dt;
+    Real gravity[3];
+    int use_jacobi;
+    int linear;
+    int explicit_mode;
+    unsigned* flags;
+    DevStats* stats;
+};
+
+template <class Real, class Acc>
+struct PcgArgs {
+    BsrView<Real> a;
+    const Real* b;
+    const Real* minv;
+    Real* x;
+    Real* r;
+    Real* s;
+    Real* d0;
+    Real* d1;
+    Real* q;
+    Acc* part_a;      // [grid]
+    Acc* part_b;      // [grid * 2]
+    int* part_bad;    // [grid * 4]: phase A, init/phase B, final check
+    GridSync* sync;
+    int max_iterations;
+    Acc tolerance;
+    int skip_on_flags;     // skip the solve when assembly flagged failure
+    int integrate;
+    Real dt;
+    const int* dyn_to_node;
+    Real* node_x;
+    Real* node_v;
+    unsigned* flags;
+    DevStats* stats;
+};
+
+// Launchers (pk_kernels.cu).  All asynchronous on `stream`.
+template <class Real>
+cudaError_t launch_tet_kernel(const AssemblyArgs<Real>& args, bool fp64_polar_fallback, cudaStream_t stream);
+template <class Real>
+cudaError_t launch_row_kernel(const AssemblyArgs<Real>& args, int max_row_blocks, cudaStream_t stream);
+template <class Real, class Acc>
+cudaError_t launch_pcg_kernel(const PcgArgs<Real, Acc>& args, int grid, int threads, cudaStream_t stream);
+template <class Real, class Acc>
+int pcg_max_grid(int threads);
+template <class Real>
+cudaError_t launch_spmv_kernel(const BsrView<Real>& a, const Real* x, Real* y, cudaStream_t stream);
+
+constexpr int kPcgThreads = 512;
+
+}  // namespace pk

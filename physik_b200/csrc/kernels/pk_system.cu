@@ -1,0 +1,790 @@
+// pk_system.cu -- implementation of the C ABI in include/pkcuda.h: device buffers of
+// one soft-body system, uploads of the host-built topology, and the launch sequence
+// of one implicit substep (tet kernel, row kernel, cooperative PCG kernel).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../../../include/pkcuda.h"
+#include "pk_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what)
+{
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return PK_ERR_CUDA;
+}
+
+#define PK_CHECK(...)                                              \
+    do {                                                           \
+        cudaError_t e_ = (__VA_ARGS__);                            \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #__VA_ARGS__); \
+    } while (0)
+
+// Owned device allocation; freed on reset / destruction.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void reset()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t ensure(size_t want)
+    {
+        if (want <= bytes && p) return cudaSuccess;
+        reset();
+        if (want == 0) want = 16;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) bytes = want;
+        return e;
+    }
+    template <class T>
+    T* as() const
+    {
+        return static_cast<T*>(p);
+    }
+    ~DevBuf() { reset(); }
+};
+
+template <class Real>
+std::vector<Real> narrow(const double* src, size_t n)
+{
+    std::vector<Real> out(n);
+    for (size_t i = 0; i < n; ++i) out[i] = static_cast<Real>(src[i]);
+    return out;
+}
+
+int device_count_safe()
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+// Builds the transpose index of an upper BSR (for row r: blocks (c, r) with c < r).
+void build_transpose(int n, const int* row_start, const int* col, std::vector<int>& lt_start, std::vector<int>& lt_row,
+                     std::vector<int>& lt_block)
+{
+    lt_start.assign(static_cast<size_t>(n) + 1, 0);
+    for (int r = 0; r < n; ++r)
+        for (int k = row_start[r]; k < row_start[r + 1]; ++k)
+            if (col[k] != r) lt_start[col[k] + 1]++;
+    for (int r = 0; r < n; ++r) lt_start[r + 1] += lt_start[r];
+    lt_row.assign(static_cast<size_t>(lt_start[n]), 0);
+    lt_block.assign(static_cast<size_t>(lt_start[n]), 0);
+    std::vector<int> fill(lt_start.begin(), lt_start.end() - 1);
+    for (int r = 0; r < n; ++r)
+        for (int k = row_start[r]; k < row_start[r + 1]; ++k) {
+            const int c = col[k];
+            if (c == r) continue;
+            const int at = fill[c]++;
+            lt_row[at] = r;
+            lt_block[at] = k;
+        }
+}
+
+}  // namespace
+
+struct pk_system {
+    int device = 0;
+    int precision = PK_PREC_MIXED;
+    cudaStream_t stream = nullptr;
+    int node_count = 0, tet_count = 0, dyn_count = 0, nnz = 0, lt_count = 0, inc_count = 0, max_row = 0;
+    bool have_nodes = false, have_tets = false, have_pattern = false;
+    bool diag_first = false;  // every row starts with its diagonal block (needed by the row kernel)
+    int pcg_grid_override = 0;
+    int pcg_max_grid = 0;
+    // nodes
+    DevBuf x, v, mass, node_to_dyn;
+    // tets
+    DevBuf tet_nodes, tet_enabled, dm_inv, tet_params, rot, stress;
+    // rows
+    DevBuf dyn_to_node, row_start, col, lt_start, lt_row, lt_block, inc_start, inc_list, values, rhs, minv;
+    // solver
+    DevBuf px, pr, ps, pd0, pd1, pq, part_a, part_b, part_bad, sync, stats;
+    pk::DevStats* host_stats = nullptr;  // pinned
+    bool stats_pending = false;
+    // timing
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::array<int, 3>> ev_pending;  // indices into ev_pool
+    double t_assemble = 0, t_solve = 0;
+    int timed_steps = 0;
+    long long launches = 0;
+
+    size_t rsize() const { return precision == PK_PREC_FP64 ? sizeof(double) : sizeof(float); }
+};
+
+namespace {
+
+template <class Real>
+pk::AssemblyArgs<Real> assembly_args(pk_system* s, const pk_step_params& p)
+{
+    pk::AssemblyArgs<Real> a{};
+    a.tets.tet_count = s->tet_count;
+    a.tets.nodes = s->tet_nodes.as<int4>();
+    a.tets.enabled = s->tet_enabled.as<unsigned char>();
+    a.tets.dm_inv = s->dm_inv.as<Real>();
+    a.tets.params = s->tet_params.as<Real>();
+    a.tets.rot = s->rot.as<Real>();
+    a.tets.stress = s->stress.as<Real>();
+    a.a.n = s->dyn_count;
+    a.a.row_start = s->row_start.as<int>();
+    a.a.col = s->col.as<int>();
+    a.a.values = s->values.as<Real>();
+    a.a.lt_start = s->lt_start.as<int>();
+    a.a.lt_row = s->lt_row.as<int>();
+    a.a.lt_block = s->lt_block.as<int>();
+    a.node_count = s->node_count;
+    a.dyn_to_node = s->dyn_to_node.as<int>();
+    a.node_to_dyn = s->node_to_dyn.as<int>();
+    a.mass = s->mass.as<Real>();
+    a.x = s->x.as<Real>();
+    a.v = s->v.as<Real>();
+    a.x_out = s->x.as<Real>();
+    a.inc_start = s->inc_start.as<int>();
+    a.inc_list = s->inc_list.as<int>();
+    a.values = s->values.as<Real>();
+    a.rhs = s->rhs.as<Real>();
+    a.minv = s->minv.as<Real>();
+    a.dt = static_cast<Real>(p.dt);
+    for (int i = 0; i < 3; ++i) a.gravity[i] = static_cast<Real>(p.gravity[i]);
+    a.use_jacobi = p.use_jacobi;
+    a.linear = p.linear;
+    a.explicit_mode = p.explicit_mode;
+    pk::DevStats* st = s->stats.as<pk::DevStats>();
+    a.flags = &st->flags;
+    a.stats = st;
+    return a;
+}
+
+template <class Real, class Acc>
+pk::PcgArgs<Real, Acc> pcg_args(pk_system* s, const pk_step_params& p, int skip_on_flags)
+{
+    pk::PcgArgs<Real, Acc> a{};
+    a.a.n = s->dyn_count;
+    a.a.row_start = s->row_start.as<int>();
+    a.a.col = s->col.as<int>();
+    a.a.values = s->values.as<Real>();
+    a.a.lt_start = s->lt_start.as<int>();
+    a.a.lt_row = s->lt_row.as<int>();
+    a.a.lt_block = s->lt_block.as<int>();
+    a.b = s->rhs.as<Real>();
+    a.minv = s->minv.as<Real>();
+    a.x = s->px.as<Real>();
+    a.r = s->pr.as<Real>();
+    a.s = s->ps.as<Real>();
+    a.d0 = s->pd0.as<Real>();
+    a.d1 = s->pd1.as<Real>();
+    a.q = s->pq.as<Real>();
+    a.part_a = s->part_a.as<Acc>();
+    a.part_b = s->part_b.as<Acc>();
+    a.part_bad = s->part_bad.as<int>();
+    a.sync = s->sync.as<pk::GridSync>();
+    a.max_iterations = p.max_iterations;
+    a.tolerance = static_cast<Acc>(static_cast<Real>(p.tolerance));
+    a.skip_on_flags = skip_on_flags;
+    a.integrate = p.integrate;
+    a.dt = static_cast<Real>(p.dt);
+    a.dyn_to_node = s->dyn_to_node.as<int>();
+    a.node_x = s->x.as<Real>();
+    a.node_v = s->v.as<Real>();
+    pk::DevStats* st = s->stats.as<pk::DevStats>();
+    a.flags = &st->flags;
+    a.stats = st;
+    return a;
+}
+
+template <class Real, class Acc>
+int max_grid_for(pk_system* s)
+{
+    if (!s->pcg_max_grid) s->pcg_max_grid = pk::pcg_max_grid<Real, Acc>(pk::kPcgThreads);
+    return s->pcg_max_grid;
+}
+
+constexpr int kRowsPerBlockTarget = 32;
+
+template <class Real, class Acc>
+int pcg_grid_for(pk_system* s)
+{
+    const int mx = max_grid_for<Real, Acc>(s);
+    if (mx <= 0) return 0;
+    if (s->pcg_grid_override > 0) return std::min(mx, s->pcg_grid_override);
+    // Enough blocks that each phase is one pass over its rows (16 lanes per row in the
+    // SpMV), capped at one cooperative wave.
+    const int want = (s->dyn_count + kRowsPerBlockTarget - 1) / kRowsPerBlockTarget;
+    return std::max(1, std::min(mx, want));
+}
+
+int ensure_solver_buffers(pk_system* s, int grid_cap)
+{
+    const size_t rs = s->rsize();
+    const size_t v3 = 3 * rs * static_cast<size_t>(std::max(1, s->dyn_count));
+    PK_CHECK(s->px.ensure(v3));
+    PK_CHECK(s->pr.ensure(v3));
+    PK_CHECK(s->ps.ensure(v3));
+    PK_CHECK(s->pd0.ensure(v3));
+    PK_CHECK(s->pd1.ensure(v3));
+    PK_CHECK(s->pq.ensure(v3));
+    const size_t g = static_cast<size_t>(std::max(1, grid_cap));
+    PK_CHECK(s->part_a.ensure(g * sizeof(double)));
+    PK_CHECK(s->part_b.ensure(2 * g * sizeof(double)));
+    PK_CHECK(s->part_bad.ensure(4 * g * sizeof(int)));
+    PK_CHECK(s->sync.ensure(sizeof(pk::GridSync)));
+    return PK_OK;
+}
+
+template <class Real, class Acc>
+int run_pcg(pk_system* s, const pk_step_params& p, int skip_on_flags)
+{
+    const int grid = pcg_grid_for<Real, Acc>(s);
+    if (grid <= 0) return fail(PK_ERR_CUDA, "cooperative PCG kernel cannot be resident");
+    int rc = ensure_solver_buffers(s, max_grid_for<Real, Acc>(s));
+    if (rc) return rc;
+    PK_CHECK(cudaMemsetAsync(s->sync.p, 0, sizeof(pk::GridSync), s->stream));
+    pk::PcgArgs<Real, Acc> a = pcg_args<Real, Acc>(s, p, skip_on_flags);
+    PK_CHECK(pk::launch_pcg_kernel<Real, Acc>(a, grid, pk::kPcgThreads, s->stream));
+    s->launches += 1;
+    return PK_OK;
+}
+
+template <class Real>
+int run_step(pk_system* s, const pk_step_params& p)
+{
+    PK_CHECK(cudaMemsetAsync(s->stats.p, 0, sizeof(pk::DevStats), s->stream));
+    int evi[3] = {-1, -1, -1};
+    if (s->timing) {
+        for (int i = 0; i < 3; ++i) {
+            cudaEvent_t e;
+            PK_CHECK(cudaEventCreate(&e));
+            s->ev_pool.push_back(e);
+            evi[i] = static_cast<int>(s->ev_pool.size()) - 1;
+        }
+        PK_CHECK(cudaEventRecord(s->ev_pool[evi[0]], s->stream));
+    }
+    pk::AssemblyArgs<Real> a = assembly_args<Real>(s, p);
+    const bool fp64_polar = s->precision == PK_PREC_MIXED;
+    if (s->tet_count > 0) {
+        PK_CHECK(pk::launch_tet_kernel<Real>(a, fp64_polar, s->stream));
+        s->launches += 1;
+    }
+    if (s->dyn_count > 0) {
+        PK_CHECK(pk::launch_row_kernel<Real>(a, s->max_row, s->stream));
+        s->launches += 1;
+    }
+    if (s->timing) PK_CHECK(cudaEventRecord(s->ev_pool[evi[1]], s->stream));
+    if (!p.explicit_mode && s->dyn_count > 0) {
+        int rc;
+        if constexpr (std::is_same<Real, double>::value)
+            rc = run_pcg<double, double>(s, p, 1);
+        else if (s->precision == PK_PREC_FP32)
+            rc = run_pcg<float, float>(s, p, 1);
+        else
+            rc = run_pcg<float, double>(s, p, 1);
+        if (rc) return rc;
+    }
+    if (s->timing) {
+        PK_CHECK(cudaEventRecord(s->ev_pool[evi[2]], s->stream));
+        s->ev_pending.push_back({evi[0], evi[1], evi[2]});
+    }
+    PK_CHECK(cudaMemcpyAsync(s->host_stats, s->stats.p, sizeof(pk::DevStats), cudaMemcpyDeviceToHost, s->stream));
+    s->stats_pending = true;
+    return PK_OK;
+}
+
+int use_device(int device)
+{
+    if (device_count_safe() <= 0) return fail(PK_ERR_NO_DEVICE, "no CUDA device");
+    PK_CHECK(cudaSetDevice(device));
+    return PK_OK;
+}
+
+template <class Real>
+int upload_real(DevBuf& buf, const double* src, size_t n, cudaStream_t stream)
+{
+    PK_CHECK(buf.ensure(std::max<size_t>(n, 1) * sizeof(Real)));
+    if (n == 0 || !src) return PK_OK;
+    std::vector<Real> tmp = narrow<Real>(src, n);
+    PK_CHECK(cudaMemcpyAsync(buf.p, tmp.data(), n * sizeof(Real), cudaMemcpyHostToDevice, stream));
+    PK_CHECK(cudaStreamSynchronize(stream));
+    return PK_OK;
+}
+
+template <class T>
+int upload_raw(DevBuf& buf, const T* src, size_t n, cudaStream_t stream)
+{
+    PK_CHECK(buf.ensure(std::max<size_t>(n, 1) * sizeof(T)));
+    if (n == 0 || !src) return PK_OK;
+    PK_CHECK(cudaMemcpyAsync(buf.p, src, n * sizeof(T), cudaMemcpyHostToDevice, stream));
+    PK_CHECK(cudaStreamSynchronize(stream));
+    return PK_OK;
+}
+
+template <class Real>
+int download_real(const DevBuf& buf, double* dst, size_t n, cudaStream_t stream)
+{
+    if (!dst || n == 0) return PK_OK;
+    std::vector<Real> tmp(n);
+    PK_CHECK(cudaMemcpyAsync(tmp.data(), buf.p, n * sizeof(Real), cudaMemcpyDeviceToHost, stream));
+    PK_CHECK(cudaStreamSynchronize(stream));
+    for (size_t i = 0; i < n; ++i) dst[i] = static_cast<double>(tmp[i]);
+    return PK_OK;
+}
+
+int upload_real_any(pk_system* s, DevBuf& buf, const double* src, size_t n)
+{
+    return s->precision == PK_PREC_FP64 ? upload_real<double>(buf, src, n, s->stream)
+                                        : upload_real<float>(buf, src, n, s->stream);
+}
+int download_real_any(pk_system* s, const DevBuf& buf, double* dst, size_t n)
+{
+    return s->precision == PK_PREC_FP64 ? download_real<double>(buf, dst, n, s->stream)
+                                        : download_real<float>(buf, dst, n, s->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+PKCUDA_API const char* pk_last_error(void) { return g_last_error.c_str(); }
+
+PKCUDA_API int pk_device_count(void) { return device_count_safe(); }
+
+PKCUDA_API int pk_system_create(int device, int precision, pk_system** out)
+{
+    if (!out) return fail(PK_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (precision < PK_PREC_FP32 || precision > PK_PREC_FP64) return fail(PK_ERR_ARG, "bad precision");
+    int rc = use_device(device);
+    if (rc) return rc;
+    pk_system* s = new pk_system();
+    s->device = device;
+    s->precision = precision;
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete s;
+        return cuda_fail(e, "cudaStreamCreate");
+    }
+    e = cudaMallocHost(&s->host_stats, sizeof(pk::DevStats));
+    if (e == cudaSuccess) e = s->stats.ensure(sizeof(pk::DevStats));
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(s->stream);
+        delete s;
+        return cuda_fail(e, "stats allocation");
+    }
+    std::memset(s->host_stats, 0, sizeof(pk::DevStats));
+    *out = s;
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_destroy(pk_system* s)
+{
+    if (!s) return PK_OK;
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+    if (s->host_stats) cudaFreeHost(s->host_stats);
+    cudaStreamDestroy(s->stream);
+    delete s;
+    return PK_OK;
+}
+
+PKCUDA_API void* pk_system_stream(pk_system* s) { return s ? static_cast<void*>(s->stream) : nullptr; }
+
+PKCUDA_API int pk_system_set_nodes(pk_system* s, int node_count, const int* node_to_dyn, const double* mass)
+{
+    if (!s || node_count < 0 || (node_count > 0 && (!node_to_dyn || !mass))) return fail(PK_ERR_ARG, "set_nodes");
+    PK_CHECK(cudaSetDevice(s->device));
+    s->node_count = node_count;
+    int rc = upload_raw<int>(s->node_to_dyn, node_to_dyn, node_count, s->stream);
+    if (!rc) rc = upload_real_any(s, s->mass, mass, node_count);
+    if (rc) return rc;
+    const size_t bytes = 3 * s->rsize() * static_cast<size_t>(std::max(1, node_count));
+    PK_CHECK(s->x.ensure(bytes));
+    PK_CHECK(s->v.ensure(bytes));
+    PK_CHECK(cudaMemsetAsync(s->x.p, 0, bytes, s->stream));
+    PK_CHECK(cudaMemsetAsync(s->v.p, 0, bytes, s->stream));
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    s->have_nodes = true;
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_set_state_f64(pk_system* s, const double* x, const double* v)
+{
+    if (!s || !s->have_nodes) return fail(PK_ERR_STATE, "set_state before set_nodes");
+    PK_CHECK(cudaSetDevice(s->device));
+    const size_t n = 3 * static_cast<size_t>(s->node_count);
+    int rc = PK_OK;
+    if (x) rc = upload_real_any(s, s->x, x, n);
+    if (!rc && v) rc = upload_real_any(s, s->v, v, n);
+    return rc;
+}
+
+PKCUDA_API int pk_system_set_state_f32(pk_system* s, const float* x, const float* v)
+{
+    if (!s || !s->have_nodes) return fail(PK_ERR_STATE, "set_state before set_nodes");
+    PK_CHECK(cudaSetDevice(s->device));
+    const size_t n = 3 * static_cast<size_t>(s->node_count);
+    if (s->precision == PK_PREC_FP64) {
+        std::vector<double> tx, tv;
+        if (x) tx.assign(x, x + n);
+        if (v) tv.assign(v, v + n);
+        return pk_system_set_state_f64(s, x ? tx.data() : nullptr, v ? tv.data() : nullptr);
+    }
+    // float storage: copy straight from the caller's buffer (pinned buffers stay asynchronous)
+    if (x) PK_CHECK(cudaMemcpyAsync(s->x.p, x, n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+    if (v) PK_CHECK(cudaMemcpyAsync(s->v.p, v, n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_get_state_f64(pk_system* s, double* x, double* v)
+{
+    if (!s || !s->have_nodes) return fail(PK_ERR_STATE, "get_state before set_nodes");
+    PK_CHECK(cudaSetDevice(s->device));
+    const size_t n = 3 * static_cast<size_t>(s->node_count);
+    int rc = download_real_any(s, s->x, x, n);
+    if (!rc) rc = download_real_any(s, s->v, v, n);
+    return rc;
+}
+
+PKCUDA_API int pk_system_get_state_f32(pk_system* s, float* x, float* v)
+{
+    if (!s || !s->have_nodes) return fail(PK_ERR_STATE, "get_state before set_nodes");
+    PK_CHECK(cudaSetDevice(s->device));
+    const size_t n = 3 * static_cast<size_t>(s->node_count);
+    if (s->precision == PK_PREC_FP64) {
+        std::vector<double> tx(x ? n : 0), tv(v ? n : 0);
+        int rc = pk_system_get_state_f64(s, x ? tx.data() : nullptr, v ? tv.data() : nullptr);
+        if (rc) return rc;
+        for (size_t i = 0; x && i < n; ++i) x[i] = static_cast<float>(tx[i]);
+        for (size_t i = 0; v && i < n; ++i) v[i] = static_cast<float>(tv[i]);
+        return PK_OK;
+    }
+    if (x) PK_CHECK(cudaMemcpyAsync(x, s->x.p, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    if (v) PK_CHECK(cudaMemcpyAsync(v, s->v.p, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_set_tets(pk_system* s, int tet_count, const int* tet_nodes, const unsigned char* enabled,
+                                  const double* dm_inv, const double* volume, const double* lambda, const double* mu,
+                                  const double* damping)
+{
+    if (!s || tet_count < 0) return fail(PK_ERR_ARG, "set_tets");
+    if (tet_count > 0 && (!tet_nodes || !enabled || !dm_inv || !volume || !lambda || !mu || !damping))
+        return fail(PK_ERR_ARG, "set_tets: NULL array");
+    PK_CHECK(cudaSetDevice(s->device));
+    for (long long i = 0; i < 4ll * tet_count; ++i)
+        if (tet_nodes[i] < 0 || tet_nodes[i] >= s->node_count) return fail(PK_ERR_ARG, "tet node out of range");
+    s->tet_count = tet_count;
+    std::vector<double> params(4 * static_cast<size_t>(tet_count));
+    for (int t = 0; t < tet_count; ++t) {
+        params[4 * t + 0] = volume[t];
+        params[4 * t + 1] = lambda[t];
+        params[4 * t + 2] = mu[t];
+        params[4 * t + 3] = damping[t];
+    }
+    int rc = upload_raw<int>(s->tet_nodes, tet_nodes, 4 * static_cast<size_t>(tet_count), s->stream);
+    if (!rc) rc = upload_raw<unsigned char>(s->tet_enabled, enabled, tet_count, s->stream);
+    if (!rc) rc = upload_real_any(s, s->dm_inv, dm_inv, 9 * static_cast<size_t>(tet_count));
+    if (!rc) rc = upload_real_any(s, s->tet_params, params.data(), params.size());
+    if (rc) return rc;
+    PK_CHECK(s->rot.ensure(9 * s->rsize() * std::max<size_t>(1, tet_count)));
+    PK_CHECK(s->stress.ensure(9 * s->rsize() * std::max<size_t>(1, tet_count)));
+    s->have_tets = true;
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_set_pattern(pk_system* s, int dyn_count, const int* dyn_to_node, const int* row_start,
+                                     const int* col_index, const int* inc_start, const int* inc_list)
+{
+    if (!s || dyn_count < 0) return fail(PK_ERR_ARG, "set_pattern");
+    if (dyn_count > 0 && (!dyn_to_node || !row_start || !col_index || !inc_start)) return fail(PK_ERR_ARG, "NULL");
+    PK_CHECK(cudaSetDevice(s->device));
+    // Validate the pattern: monotone rows, sorted unique columns in [row, n).
+    const int nnz = dyn_count > 0 ? row_start[dyn_count] : 0;
+    if (dyn_count > 0 && row_start[0] != 0) return fail(PK_ERR_ARG, "row_start[0] != 0");
+    int max_row = 0;
+    bool diag_first = true;
+    for (int r = 0; r < dyn_count; ++r) {
+        const int a = row_start[r], b = row_start[r + 1];
+        if (b < a) return fail(PK_ERR_ARG, "row_start not monotone");
+        if (b == a || col_index[a] != r) diag_first = false;
+        for (int k = a; k < b; ++k) {
+            if (col_index[k] < r || col_index[k] >= dyn_count) return fail(PK_ERR_ARG, "column outside [row, n)");
+            if (k > a && col_index[k] <= col_index[k - 1]) return fail(PK_ERR_ARG, "columns not sorted and unique");
+        }
+        max_row = std::max(max_row, b - a);
+        if (dyn_to_node[r] < 0 || dyn_to_node[r] >= s->node_count) return fail(PK_ERR_ARG, "bad dyn_to_node");
+    }
+    const int inc = dyn_count > 0 ? inc_start[dyn_count] : 0;
+    for (int i = 0; i < inc; ++i)
+        if (inc_list[i] < 0 || (inc_list[i] >> 2) >= s->tet_count) return fail(PK_ERR_ARG, "bad incidence");
+    std::vector<int> lts, ltr, ltb;
+    build_transpose(dyn_count, row_start, col_index, lts, ltr, ltb);
+    s->dyn_count = dyn_count;
+    s->nnz = nnz;
+    s->lt_count = static_cast<int>(ltr.size());
+    s->inc_count = inc;
+    s->max_row = max_row;
+    s->diag_first = diag_first;
+    int rc = upload_raw<int>(s->dyn_to_node, dyn_to_node, dyn_count, s->stream);
+    if (!rc) rc = upload_raw<int>(s->row_start, row_start, dyn_count + 1, s->stream);
+    if (!rc) rc = upload_raw<int>(s->col, col_index, nnz, s->stream);
+    if (!rc) rc = upload_raw<int>(s->lt_start, lts.data(), lts.size(), s->stream);
+    if (!rc) rc = upload_raw<int>(s->lt_row, ltr.data(), ltr.size(), s->stream);
+    if (!rc) rc = upload_raw<int>(s->lt_block, ltb.data(), ltb.size(), s->stream);
+    if (!rc) rc = upload_raw<int>(s->inc_start, inc_start, dyn_count + 1, s->stream);
+    if (!rc) rc = upload_raw<int>(s->inc_list, inc_list, inc, s->stream);
+    if (rc) return rc;
+    const size_t rs = s->rsize();
+    PK_CHECK(s->values.ensure(9 * rs * std::max<size_t>(1, nnz)));
+    PK_CHECK(s->rhs.ensure(3 * rs * std::max<size_t>(1, dyn_count)));
+    PK_CHECK(s->minv.ensure(9 * rs * std::max<size_t>(1, dyn_count)));
+    rc = s->precision == PK_PREC_FP32 ? ensure_solver_buffers(s, max_grid_for<float, float>(s))
+         : s->precision == PK_PREC_MIXED ? ensure_solver_buffers(s, max_grid_for<float, double>(s))
+                                         : ensure_solver_buffers(s, max_grid_for<double, double>(s));
+    if (rc) return rc;
+    s->have_pattern = true;
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_step(pk_system* s, const pk_step_params* p)
+{
+    if (!s || !p) return fail(PK_ERR_ARG, "step");
+    if (!s->have_nodes || !s->have_tets || !s->have_pattern) return fail(PK_ERR_STATE, "step before topology");
+    if (!(p->dt > 0.0)) return fail(PK_ERR_ARG, "dt must be > 0");
+    if (s->dyn_count > 0 && !s->diag_first) return fail(PK_ERR_ARG, "every dynamic row needs its diagonal block first");
+    PK_CHECK(cudaSetDevice(s->device));
+    return s->precision == PK_PREC_FP64 ? run_step<double>(s, *p) : run_step<float>(s, *p);
+}
+
+PKCUDA_API int pk_system_stats(pk_system* s, pk_step_stats* out)
+{
+    if (!s || !out) return fail(PK_ERR_ARG, "stats");
+    PK_CHECK(cudaSetDevice(s->device));
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    std::memset(out, 0, sizeof(*out));
+    const pk::DevStats& d = *s->host_stats;
+    out->iterations = d.iterations;
+    out->converged = d.converged;
+    out->residual_norm = d.residual_norm;
+    out->flags = d.flags;
+    out->polar_fp64_count = d.polar_fp64_count;
+    out->polar_identity_count = d.polar_identity_count;
+    if (d.flags & PK_FLAG_BARRIER_TIMEOUT) return fail(PK_ERR_TIMEOUT, "grid barrier timed out");
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_get_system_f64(pk_system* s, double* values, double* rhs, double* minv, double* dv)
+{
+    if (!s || !s->have_pattern) return fail(PK_ERR_STATE, "get_system before set_pattern");
+    PK_CHECK(cudaSetDevice(s->device));
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    int rc = download_real_any(s, s->values, values, 9 * static_cast<size_t>(s->nnz));
+    if (!rc) rc = download_real_any(s, s->rhs, rhs, 3 * static_cast<size_t>(s->dyn_count));
+    if (!rc) rc = download_real_any(s, s->minv, minv, 9 * static_cast<size_t>(s->dyn_count));
+    if (!rc) rc = download_real_any(s, s->px, dv, 3 * static_cast<size_t>(s->dyn_count));
+    return rc;
+}
+
+PKCUDA_API int pk_system_solve_given_f64(pk_system* s, const double* values, const double* rhs, const double* minv,
+                                         const pk_step_params* p)
+{
+    if (!s || !p || !s->have_pattern) return fail(PK_ERR_STATE, "solve_given before set_pattern");
+    PK_CHECK(cudaSetDevice(s->device));
+    int rc = PK_OK;
+    if (values) rc = upload_real_any(s, s->values, values, 9 * static_cast<size_t>(s->nnz));
+    if (!rc && rhs) rc = upload_real_any(s, s->rhs, rhs, 3 * static_cast<size_t>(s->dyn_count));
+    if (!rc && minv) rc = upload_real_any(s, s->minv, minv, 9 * static_cast<size_t>(s->dyn_count));
+    if (rc) return rc;
+    PK_CHECK(cudaMemsetAsync(s->stats.p, 0, sizeof(pk::DevStats), s->stream));
+    if (s->dyn_count > 0) {
+        if (s->precision == PK_PREC_FP32) rc = run_pcg<float, float>(s, *p, 0);
+        else if (s->precision == PK_PREC_MIXED) rc = run_pcg<float, double>(s, *p, 0);
+        else rc = run_pcg<double, double>(s, *p, 0);
+        if (rc) return rc;
+    }
+    PK_CHECK(cudaMemcpyAsync(s->host_stats, s->stats.p, sizeof(pk::DevStats), cudaMemcpyDeviceToHost, s->stream));
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_enable_timing(pk_system* s, int on)
+{
+    if (!s) return fail(PK_ERR_ARG, "timing");
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+    s->ev_pool.clear();
+    s->ev_pending.clear();
+    s->t_assemble = s->t_solve = 0;
+    s->timed_steps = 0;
+    s->launches = 0;
+    s->timing = on != 0;
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_timings(pk_system* s, double* assemble_ms, double* solve_ms, int* steps,
+                                 long long* kernel_launches)
+{
+    if (!s) return fail(PK_ERR_ARG, "timings");
+    PK_CHECK(cudaSetDevice(s->device));
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    for (const auto& tr : s->ev_pending) {
+        float a = 0, b = 0;
+        PK_CHECK(cudaEventElapsedTime(&a, s->ev_pool[tr[0]], s->ev_pool[tr[1]]));
+        PK_CHECK(cudaEventElapsedTime(&b, s->ev_pool[tr[1]], s->ev_pool[tr[2]]));
+        s->t_assemble += a;
+        s->t_solve += b;
+        s->timed_steps += 1;
+    }
+    for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+    s->ev_pool.clear();
+    s->ev_pending.clear();
+    if (assemble_ms) *assemble_ms = s->t_assemble;
+    if (solve_ms) *solve_ms = s->t_solve;
+    if (steps) *steps = s->timed_steps;
+    if (kernel_launches) *kernel_launches = s->launches;
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_set_pcg_grid(pk_system* s, int grid)
+{
+    if (!s) return fail(PK_ERR_ARG, "pcg grid");
+    PK_CHECK(cudaSetDevice(s->device));
+    s->pcg_grid_override = std::max(0, grid);
+    if (s->precision == PK_PREC_FP32) return pcg_grid_for<float, float>(s);
+    if (s->precision == PK_PREC_MIXED) return pcg_grid_for<float, double>(s);
+    return pcg_grid_for<double, double>(s);
+}
+
+PKCUDA_API int pk_bsr_transpose_index(int n, const int* row_start, const int* col_index, int* lt_start, int* lt_row,
+                                      int* lt_block)
+{
+    if (n < 0 || (n > 0 && (!row_start || !col_index))) return fail(PK_ERR_ARG, "transpose index");
+    std::vector<int> a, b, c;
+    build_transpose(n, row_start, col_index, a, b, c);
+    if (lt_start) std::copy(a.begin(), a.end(), lt_start);
+    if (lt_row) std::copy(b.begin(), b.end(), lt_row);
+    if (lt_block) std::copy(c.begin(), c.end(), lt_block);
+    return static_cast<int>(b.size());
+}
+
+// Standalone SpMV on host arrays: y = A x with A stored upper-only.
+PKCUDA_API int pk_bsr_multiply(int device, int precision, int n, const int* row_start, const int* col_index,
+                               const double* values, const double* x, double* y)
+{
+    if (n < 0 || (n > 0 && (!row_start || !col_index || !values || !x || !y))) return fail(PK_ERR_ARG, "multiply");
+    if (n == 0) return PK_OK;
+    int rc = use_device(device);
+    if (rc) return rc;
+    pk_system* s = nullptr;
+    rc = pk_system_create(device, precision, &s);
+    if (rc) return rc;
+    struct Guard {
+        pk_system* s;
+        ~Guard() { pk_system_destroy(s); }
+    } guard{s};
+    const int nnz = row_start[n];
+    std::vector<int> lts, ltr, ltb;
+    build_transpose(n, row_start, col_index, lts, ltr, ltb);
+    DevBuf drs, dcol, dlts, dltr, dltb, dval, dx, dy;
+    rc = upload_raw<int>(drs, row_start, n + 1, s->stream);
+    if (!rc) rc = upload_raw<int>(dcol, col_index, nnz, s->stream);
+    if (!rc) rc = upload_raw<int>(dlts, lts.data(), lts.size(), s->stream);
+    if (!rc) rc = upload_raw<int>(dltr, ltr.data(), ltr.size(), s->stream);
+    if (!rc) rc = upload_raw<int>(dltb, ltb.data(), ltb.size(), s->stream);
+    if (!rc) rc = upload_real_any(s, dval, values, 9 * static_cast<size_t>(nnz));
+    if (!rc) rc = upload_real_any(s, dx, x, 3 * static_cast<size_t>(n));
+    if (rc) return rc;
+    PK_CHECK(dy.ensure(3 * s->rsize() * static_cast<size_t>(n)));
+    if (precision == PK_PREC_FP64) {
+        pk::BsrView<double> a{n, drs.as<int>(), dcol.as<int>(), dval.as<double>(), dlts.as<int>(), dltr.as<int>(),
+                              dltb.as<int>()};
+        PK_CHECK(pk::launch_spmv_kernel<double>(a, dx.as<double>(), dy.as<double>(), s->stream));
+    } else {
+        pk::BsrView<float> a{n, drs.as<int>(), dcol.as<int>(), dval.as<float>(), dlts.as<int>(), dltr.as<int>(),
+                             dltb.as<int>()};
+        PK_CHECK(pk::launch_spmv_kernel<float>(a, dx.as<float>(), dy.as<float>(), s->stream));
+    }
+    return download_real_any(s, dy, y, 3 * static_cast<size_t>(n));
+}
+
+// Standalone PCG on host arrays, with the reference's argument checks.
+PKCUDA_API int pk_pcg(int device, int precision, int n, const int* row_start, const int* col_index,
+                      const double* values, const double* b, const double* minv, int minv_count, int max_iterations,
+                      double tolerance, double* x, pk_cg_result* out)
+{
+    if (!out || n < 0) return fail(PK_ERR_ARG, "pcg");
+    std::memset(out, 0, sizeof(*out));
+    if (n == 0) {
+        out->converged = 1;  // empty rhs: cleared output, converged (ConjugateGradientSolver.cpp:124-131)
+        return PK_OK;
+    }
+    if (!row_start || !col_index || !values || !b || !x) return fail(PK_ERR_ARG, "pcg: NULL array");
+    if (minv_count != n || !minv) {
+        // ApplyPreconditioner fails on a size mismatch: x = 0, result cleared (:150-153).
+        bool bad = max_iterations <= 0 || !std::isfinite(tolerance) || tolerance <= 0.0;
+        for (int i = 0; i < 3 * n && !bad; ++i) bad = !std::isfinite(b[i]);
+        if (!bad) {
+            for (int i = 0; i < 3 * n; ++i) x[i] = 0.0;
+            out->have_solution = 1;
+        }
+        return PK_OK;
+    }
+    pk_system* s = nullptr;
+    int rc = pk_system_create(device, precision, &s);
+    if (rc) return rc;
+    struct Guard {
+        pk_system* s;
+        ~Guard() { pk_system_destroy(s); }
+    } guard{s};
+    std::vector<int> n2d(static_cast<size_t>(n));
+    std::vector<double> mass(static_cast<size_t>(n), 1.0);
+    std::vector<int> inc(static_cast<size_t>(n) + 1, 0);
+    for (int i = 0; i < n; ++i) n2d[i] = i;
+    rc = pk_system_set_nodes(s, n, n2d.data(), mass.data());
+    if (!rc) rc = pk_system_set_tets(s, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+    if (!rc) rc = pk_system_set_pattern(s, n, n2d.data(), row_start, col_index, inc.data(), nullptr);
+    if (rc) return rc;
+    pk_step_params p{};
+    p.dt = 1.0;
+    p.max_iterations = max_iterations;
+    p.tolerance = tolerance;
+    p.use_jacobi = 1;
+    p.integrate = 0;
+    rc = pk_system_solve_given_f64(s, values, b, minv, &p);
+    if (rc) return rc;
+    pk_step_stats st{};
+    rc = pk_system_stats(s, &st);
+    if (rc) return rc;
+    out->iterations = st.iterations;
+    out->converged = st.converged;
+    out->residual_norm = st.residual_norm;
+    out->have_solution = (st.flags & PK_FLAG_INVALID_RHS) ? 0 : 1;
+    if (out->have_solution) return download_real_any(s, s->px, x, 3 * static_cast<size_t>(n));
+    return PK_OK;
+}
+
+}  // extern "C"
