@@ -1,0 +1,271 @@
+// pk_device.cuh -- device helpers shared by the kernel translation units: vector
+// loads/stores, block and grid reductions in a fixed order, the bounded grid barrier of
+// the cooperative PCG launch, and the mbarrier / TMA bulk-copy primitives.
+// Everything here has internal linkage (one copy per translation unit).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "pk_kernels.cuh"
+
+namespace pk {
+namespace {
+
+constexpr unsigned long long kBarrierSpinLimit = 1ull << 24;  // ~seconds with back-off
+
+template <class Real>
+__device__ __forceinline__ Real qnan();
+template <>
+__device__ __forceinline__ float qnan<float>() { return __int_as_float(0x7fc00000); }
+template <>
+__device__ __forceinline__ double qnan<double>() { return __longlong_as_double(0x7ff8000000000000ll); }
+
+template <class Real>
+__device__ __forceinline__ V3<Real> ld3(const Real* p, int i)
+{
+    const Real* q = p + 3 * (size_t)i;
+    return V3<Real>{__ldg(q), __ldg(q + 1), __ldg(q + 2)};
+}
+// Loads of data written earlier in the same launch by another block: bypass L1.
+template <class Real>
+__device__ __forceinline__ V3<Real> ldcg3(const Real* p, int i)
+{
+    const Real* q = p + 3 * (size_t)i;
+    return V3<Real>{__ldcg(q), __ldcg(q + 1), __ldcg(q + 2)};
+}
+template <class Real>
+__device__ __forceinline__ V3<Real> ldplain3(const Real* p, int i)
+{
+    const Real* q = p + 3 * (size_t)i;
+    return V3<Real>{q[0], q[1], q[2]};
+}
+template <class Real>
+__device__ __forceinline__ void st3(Real* p, int i, V3<Real> v)
+{
+    Real* q = p + 3 * (size_t)i;
+    q[0] = v.x;
+    q[1] = v.y;
+    q[2] = v.z;
+}
+template <class Real>
+__device__ __forceinline__ M3<Real> ld9(const Real* p, size_t i)
+{
+    const Real* q = p + 9 * i;
+    M3<Real> m;
+    m.c[0] = V3<Real>{__ldg(q + 0), __ldg(q + 1), __ldg(q + 2)};
+    m.c[1] = V3<Real>{__ldg(q + 3), __ldg(q + 4), __ldg(q + 5)};
+    m.c[2] = V3<Real>{__ldg(q + 6), __ldg(q + 7), __ldg(q + 8)};
+    return m;
+}
+template <class Real>
+__device__ __forceinline__ void st9(Real* p, size_t i, const M3<Real>& m)
+{
+    Real* q = p + 9 * i;
+    q[0] = m.c[0].x; q[1] = m.c[0].y; q[2] = m.c[0].z;
+    q[3] = m.c[1].x; q[4] = m.c[1].y; q[5] = m.c[1].z;
+    q[6] = m.c[2].x; q[7] = m.c[2].y; q[8] = m.c[2].z;
+}
+template <class Acc, class Real>
+__device__ __forceinline__ Acc dot_acc(V3<Real> a, V3<Real> b)
+{
+    return Acc(a.x) * Acc(b.x) + Acc(a.y) * Acc(b.y) + Acc(a.z) * Acc(b.z);
+}
+// a + s*b evaluated in the accumulation type, rounded once to the storage type.
+template <class Real, class Acc>
+__device__ __forceinline__ V3<Real> axpy(V3<Real> a, Acc s, V3<Real> b)
+{
+    return V3<Real>{Real(Acc(a.x) + s * Acc(b.x)), Real(Acc(a.y) + s * Acc(b.y)), Real(Acc(a.z) + s * Acc(b.z))};
+}
+__device__ __forceinline__ bool acc_finite(float v) { return isfinite(v); }
+__device__ __forceinline__ bool acc_finite(double v) { return isfinite(v); }
+
+// ------------------------------------------------------------------ barrier
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v)
+{
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+// ------------------------------------------------------------------ TMA bulk copies
+// One-dimensional bulk copies global -> shared (cp.async.bulk, no multicast) completing
+// on an mbarrier with a transaction count.  Addresses and sizes are 16-byte multiples.
+constexpr unsigned kMbarSpinLimit = 1u << 22;
+
+__device__ __forceinline__ unsigned smem_addr(const void* p)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for the phase with the given parity; false after kMbarSpinLimit polls.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity)
+{
+    for (unsigned i = 0; i < kMbarSpinLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+// Sense-counting grid barrier for a cooperative launch.  Every wait is bounded: after
+// kBarrierSpinLimit polls it records the timeout in sync->err and returns false, and
+// every block also gives up as soon as it sees another block's timeout.
+__device__ bool grid_barrier(GridSync* sync, int* s_flag)
+{
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned nblocks = gridDim.x;
+        if (nblocks > 1) {
+            const unsigned gen = ld_acquire(&sync->gen);
+            const unsigned old = atom_add_acq_rel(&sync->arrive, 1u);
+            if (old == nblocks - 1) {
+                atomicExch(&sync->arrive, 0u);
+                st_release(&sync->gen, gen + 1u);
+            } else {
+                unsigned long long spins = 0;
+                while (ld_acquire(&sync->gen) == gen) {
+                    if (++spins > kBarrierSpinLimit) {
+                        atomicExch(&sync->err, 1);
+                        ok = 0;
+                        break;
+                    }
+                    if (spins > 32) __nanosleep(100);
+                    if (*(volatile int*)&sync->err) {
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
+        }
+        if (*(volatile int*)&sync->err) ok = 0;
+        *s_flag = ok;
+    }
+    __syncthreads();
+    return *s_flag != 0;
+}
+
+// Block-wide sum of N values (fixed shuffle tree, then warp 0 in order): identical
+// results on every run.  `sh` holds N*32 values.  Result valid in all threads.
+template <class Acc, int N>
+__device__ __forceinline__ void block_sum(Acc (&v)[N], Acc* sh)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], off);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < N; ++k) sh[k * 32 + warp] = v[k];
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            Acc t = lane < nw ? sh[k * 32 + lane] : Acc(0);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+            if (lane == 0) sh[k * 32] = t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = sh[k * 32];
+    __syncthreads();
+}
+
+__device__ __forceinline__ int block_or(int v, int* sh)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v = __reduce_or_sync(0xffffffffu, (unsigned)v);
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    int t = 0;
+    for (int w = 0; w < nw; ++w) t |= sh[w];
+    __syncthreads();
+    return t;
+}
+
+// Sum of the per-block partials part[i*stride + k] over all blocks, in a fixed order,
+// evaluated identically by every block.
+template <class Acc, int N>
+__device__ __forceinline__ void grid_sum(const Acc* part, int stride, Acc (&out)[N], Acc* sh)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            Acc t = Acc(0);
+            for (int i = lane; i < (int)gridDim.x; i += 32) t += __ldcg(part + (size_t)i * stride + k);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+            if (lane == 0) sh[k * 32] = t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < N; ++k) out[k] = sh[k * 32];
+    __syncthreads();
+}
+
+__device__ __forceinline__ int grid_or(const int* part, int stride, int* sh)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp == 0) {
+        int t = 0;
+        for (int i = lane; i < (int)gridDim.x; i += 32) t |= __ldcg(part + (size_t)i * stride);
+        t = (int)__reduce_or_sync(0xffffffffu, (unsigned)t);
+        if (lane == 0) sh[0] = t;
+    }
+    __syncthreads();
+    const int r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+}  // namespace
+}  // namespace pk

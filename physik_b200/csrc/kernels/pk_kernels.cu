@@ -12,228 +12,18 @@
 //                (TetMeshPhysicsComponent::UpdateSystem, TetMeshPhysicsComponent.cpp:293-354;
 //                 SolverData::AssembleImplicitMatrixAndRhs, SolverData.cpp:308-465;
 //                 SolverData::BuildInversePreconditioner, SolverData.cpp:260-306)
-//   pcg_kernel   one cooperative launch per solve: block-Jacobi PCG with the symmetric
-//                upper-BSR SpMV fused with d = s + beta d and the d.q partial sums, the
-//                x/r/s update fused with r.s, grid-wide reductions in fixed order (the
-//                result does not depend on timing), bounded grid barriers, and the
-//                all-or-nothing implicit Euler update fused at the end.
-//                (SolvePreconditionedConjugateGradient, ConjugateGradientSolver.cpp:114-241;
-//                 SparseBlockMatrix::Multiply, SparseBlockMatrix.cpp:209-268;
-//                 World::IntegrateImplicitEuler, World.cpp:644-695)
+//   spmv_kernel  y = A x for the upper-stored symmetric BSR (SparseBlockMatrix::Multiply,
+//                SparseBlockMatrix.cpp:209-268).
+// The PCG kernel lives in pk_pcg.cu.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
 
-#include "pk_kernels.cuh"
+#include "pk_device.cuh"
 
 namespace pk {
 
 namespace {
-
-constexpr unsigned long long kBarrierSpinLimit = 1ull << 24;  // ~seconds with back-off
-
-template <class Real>
-__device__ __forceinline__ Real qnan();
-template <>
-__device__ __forceinline__ float qnan<float>() { return __int_as_float(0x7fc00000); }
-template <>
-__device__ __forceinline__ double qnan<double>() { return __longlong_as_double(0x7ff8000000000000ll); }
-
-template <class Real>
-__device__ __forceinline__ V3<Real> ld3(const Real* p, int i)
-{
-    const Real* q = p + 3 * (size_t)i;
-    return V3<Real>{__ldg(q), __ldg(q + 1), __ldg(q + 2)};
-}
-// Loads of data written earlier in the same launch by another block: bypass L1.
-template <class Real>
-__device__ __forceinline__ V3<Real> ldcg3(const Real* p, int i)
-{
-    const Real* q = p + 3 * (size_t)i;
-    return V3<Real>{__ldcg(q), __ldcg(q + 1), __ldcg(q + 2)};
-}
-template <class Real>
-__device__ __forceinline__ V3<Real> ldplain3(const Real* p, int i)
-{
-    const Real* q = p + 3 * (size_t)i;
-    return V3<Real>{q[0], q[1], q[2]};
-}
-template <class Real>
-__device__ __forceinline__ void st3(Real* p, int i, V3<Real> v)
-{
-    Real* q = p + 3 * (size_t)i;
-    q[0] = v.x;
-    q[1] = v.y;
-    q[2] = v.z;
-}
-template <class Real>
-__device__ __forceinline__ M3<Real> ld9(const Real* p, size_t i)
-{
-    const Real* q = p + 9 * i;
-    M3<Real> m;
-    m.c[0] = V3<Real>{__ldg(q + 0), __ldg(q + 1), __ldg(q + 2)};
-    m.c[1] = V3<Real>{__ldg(q + 3), __ldg(q + 4), __ldg(q + 5)};
-    m.c[2] = V3<Real>{__ldg(q + 6), __ldg(q + 7), __ldg(q + 8)};
-    return m;
-}
-template <class Real>
-__device__ __forceinline__ void st9(Real* p, size_t i, const M3<Real>& m)
-{
-    Real* q = p + 9 * i;
-    q[0] = m.c[0].x; q[1] = m.c[0].y; q[2] = m.c[0].z;
-    q[3] = m.c[1].x; q[4] = m.c[1].y; q[5] = m.c[1].z;
-    q[6] = m.c[2].x; q[7] = m.c[2].y; q[8] = m.c[2].z;
-}
-template <class Acc, class Real>
-__device__ __forceinline__ Acc dot_acc(V3<Real> a, V3<Real> b)
-{
-    return Acc(a.x) * Acc(b.x) + Acc(a.y) * Acc(b.y) + Acc(a.z) * Acc(b.z);
-}
-// a + s*b evaluated in the accumulation type, rounded once to the storage type.
-template <class Real, class Acc>
-__device__ __forceinline__ V3<Real> axpy(V3<Real> a, Acc s, V3<Real> b)
-{
-    return V3<Real>{Real(Acc(a.x) + s * Acc(b.x)), Real(Acc(a.y) + s * Acc(b.y)), Real(Acc(a.z) + s * Acc(b.z))};
-}
-__device__ __forceinline__ bool acc_finite(float v) { return isfinite(v); }
-__device__ __forceinline__ bool acc_finite(double v) { return isfinite(v); }
-
-// ------------------------------------------------------------------ barrier
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
-{
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release(unsigned* p, unsigned v)
-{
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v)
-{
-    unsigned old;
-    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-    return old;
-}
-
-// Sense-counting grid barrier for a cooperative launch.  Every wait is bounded: after
-// kBarrierSpinLimit polls it records the timeout in sync->err and returns false, and
-// every block also gives up as soon as it sees another block's timeout.
-__device__ bool grid_barrier(GridSync* sync, int* s_flag)
-{
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        const unsigned nblocks = gridDim.x;
-        if (nblocks > 1) {
-            const unsigned gen = ld_acquire(&sync->gen);
-            const unsigned old = atom_add_acq_rel(&sync->arrive, 1u);
-            if (old == nblocks - 1) {
-                atomicExch(&sync->arrive, 0u);
-                st_release(&sync->gen, gen + 1u);
-            } else {
-                unsigned long long spins = 0;
-                while (ld_acquire(&sync->gen) == gen) {
-                    if (++spins > kBarrierSpinLimit) {
-                        atomicExch(&sync->err, 1);
-                        ok = 0;
-                        break;
-                    }
-                    if (spins > 32) __nanosleep(100);
-                    if (*(volatile int*)&sync->err) {
-                        ok = 0;
-                        break;
-                    }
-                }
-            }
-        }
-        if (*(volatile int*)&sync->err) ok = 0;
-        *s_flag = ok;
-    }
-    __syncthreads();
-    return *s_flag != 0;
-}
-
-// Block-wide sum of N values (fixed shuffle tree, then warp 0 in order): identical
-// results on every run.  `sh` holds N*32 values.  Result valid in all threads.
-template <class Acc, int N>
-__device__ __forceinline__ void block_sum(Acc (&v)[N], Acc* sh)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-    for (int k = 0; k < N; ++k)
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], off);
-    __syncthreads();
-    if (lane == 0)
-#pragma unroll
-        for (int k = 0; k < N; ++k) sh[k * 32 + warp] = v[k];
-    __syncthreads();
-    if (warp == 0) {
-#pragma unroll
-        for (int k = 0; k < N; ++k) {
-            Acc t = lane < nw ? sh[k * 32 + lane] : Acc(0);
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
-            if (lane == 0) sh[k * 32] = t;
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < N; ++k) v[k] = sh[k * 32];
-    __syncthreads();
-}
-
-__device__ __forceinline__ int block_or(int v, int* sh)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    v = __reduce_or_sync(0xffffffffu, (unsigned)v);
-    __syncthreads();
-    if (lane == 0) sh[warp] = v;
-    __syncthreads();
-    int t = 0;
-    for (int w = 0; w < nw; ++w) t |= sh[w];
-    __syncthreads();
-    return t;
-}
-
-// Sum of the per-block partials part[i*stride + k] over all blocks, in a fixed order,
-// evaluated identically by every block.
-template <class Acc, int N>
-__device__ __forceinline__ void grid_sum(const Acc* part, int stride, Acc (&out)[N], Acc* sh)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (warp == 0) {
-#pragma unroll
-        for (int k = 0; k < N; ++k) {
-            Acc t = Acc(0);
-            for (int i = lane; i < (int)gridDim.x; i += 32) t += __ldcg(part + (size_t)i * stride + k);
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
-            if (lane == 0) sh[k * 32] = t;
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < N; ++k) out[k] = sh[k * 32];
-    __syncthreads();
-}
-
-__device__ __forceinline__ int grid_or(const int* part, int stride, int* sh)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (warp == 0) {
-        int t = 0;
-        for (int i = lane; i < (int)gridDim.x; i += 32) t |= __ldcg(part + (size_t)i * stride);
-        t = (int)__reduce_or_sync(0xffffffffu, (unsigned)t);
-        if (lane == 0) sh[0] = t;
-    }
-    __syncthreads();
-    const int r = sh[0];
-    __syncthreads();
-    return r;
-}
 
 // ------------------------------------------------------------------ SpMV row
 // q_r = sum over the row's upper blocks B x_c plus its transposed lower blocks B^T x_c,
@@ -476,233 +266,6 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
     st9(A.minv, (size_t)r, mi);
 }
 
-// ------------------------------------------------------------------ PCG kernel
-template <class Real, class Acc>
-__global__ void __launch_bounds__(kPcgThreads, 2) pcg_kernel(PcgArgs<Real, Acc> P)
-{
-    __shared__ Acc sh_acc[3 * 32];
-    __shared__ int sh_int[32];
-    __shared__ int s_flag;
-    const int tid = threadIdx.x, T = blockDim.x, blk = blockIdx.x, G = gridDim.x;
-    const int n = P.a.n;
-    const int per = (n + G - 1) / G;
-    const int r0 = min(n, blk * per), r1 = min(n, r0 + per);
-    const int lane = tid & 31, warp = tid >> 5, nwarps = T >> 5;
-    const int half = lane >> 4, hl = lane & 15;
-
-    unsigned fl = 0;
-    int iterations = 0;
-    bool converged = false;
-    Acc residual = Acc(0);
-    bool have_x = true;
-    bool timed_out = false;
-
-    const unsigned in_flags = *(volatile unsigned*)P.flags;
-    if (P.skip_on_flags && (in_flags & (kFlagPrecomputeFailed | kFlagSingularDiag))) {
-        if (blk == 0 && tid == 0) {
-            P.stats->iterations = 0;
-            P.stats->converged = 0;
-            P.stats->residual_norm = 0.0;
-        }
-        return;
-    }
-
-    // x = 0, r = b, s = M^-1 r, d_prev = 0; delta = r.s; also |r|^2 and finiteness.
-    {
-        Acc loc[2] = {Acc(0), Acc(0)};
-        int bad = 0;
-        for (int r = r0 + tid; r < r1; r += T) {
-            const V3<Real> br = ld3(P.b, r);
-            if (!finite3(br)) bad |= 1;
-            const V3<Real> z{Real(0), Real(0), Real(0)};
-            st3(P.x, r, z);
-            st3(P.r, r, br);
-            st3(P.d0, r, z);
-            const M3<Real> mi = ld9(P.minv, (size_t)r);
-            const V3<Real> s = mul(mi, br);
-            if (!finite9(mi) || !finite3(s)) bad |= 2;
-            st3(P.s, r, s);
-            loc[0] += dot_acc<Acc>(br, s);
-            loc[1] += dot_acc<Acc>(br, br);
-        }
-        block_sum<Acc, 2>(loc, sh_acc);
-        bad = block_or(bad, sh_int);
-        if (tid == 0) {
-            P.part_b[2 * blk + 0] = loc[0];
-            P.part_b[2 * blk + 1] = loc[1];
-            P.part_bad[4 * blk + 1] = bad;
-        }
-    }
-    if (!grid_barrier(P.sync, &s_flag)) { timed_out = true; goto finish; }
-
-    {
-        Acc g[2];
-        grid_sum<Acc, 2>(P.part_b, 2, g, sh_acc);
-        const int bad = grid_or(P.part_bad + 1, 4, sh_int);
-        Acc delta = g[0];
-        Acc rr = g[1];
-        if (bad & 1) {  // non-finite rhs: the reference clears x (solve fails)
-            have_x = false;
-            fl |= kFlagInvalidRhs;
-            goto final_check;
-        }
-        if (P.max_iterations <= 0 || !acc_finite(P.tolerance) || P.tolerance <= Acc(0)) {
-            have_x = false;
-            fl |= kFlagInvalidRhs;
-            goto final_check;
-        }
-        if (bad & 2) goto final_check;  // preconditioner output not finite: x stays 0
-        if (!acc_finite(delta) || delta < Acc(0)) goto final_check;
-        const Acc target = P.tolerance * P.tolerance * delta;
-        if (!acc_finite(target)) goto final_check;
-        if (delta <= target) {
-            converged = true;
-            residual = (acc_finite(rr) && rr >= Acc(0)) ? sqrt(rr) : Acc(INFINITY);
-            goto final_check;
-        }
-        Acc beta = Acc(0);
-        Real* dcur = P.d0;
-        Real* dnext = P.d1;
-        for (int it = 0; it < P.max_iterations; ++it) {
-            if (delta <= target) {
-                converged = true;
-                break;
-            }
-            // Phase A: d_next = s + beta d_cur; q = A d_next; partial d_next . q
-            {
-                Acc loc[1] = {Acc(0)};
-                int qbad = 0;
-                for (int base = r0 + 2 * warp; base < r1; base += 2 * nwarps) {
-                    const int r = base + half;
-                    const bool valid = r < r1;
-                    const V3<Real> q = row_spmv<Real, 16>(P.a, valid ? r : -1, hl, P.s, dcur, Real(beta), true);
-                    if (valid && hl == 0) {
-                        const V3<Real> dn = ldcg3(P.s, r) + ldcg3(dcur, r) * Real(beta);
-                        st3(dnext, r, dn);
-                        st3(P.q, r, q);
-                        loc[0] += dot_acc<Acc>(dn, q);
-                        if (!finite3(q)) qbad = 1;
-                    }
-                }
-                block_sum<Acc, 1>(loc, sh_acc);
-                qbad = block_or(qbad, sh_int);
-                if (tid == 0) {
-                    P.part_a[blk] = loc[0];
-                    P.part_bad[4 * blk + 0] = qbad;
-                }
-            }
-            if (!grid_barrier(P.sync, &s_flag)) { timed_out = true; goto finish; }
-            Acc dq;
-            {
-                Acc g1[1];
-                grid_sum<Acc, 1>(P.part_a, 1, g1, sh_acc);
-                dq = g1[0];
-                if (grid_or(P.part_bad, 4, sh_int)) { fl |= kFlagBreakdown; break; }
-            }
-            if (!acc_finite(dq) || dq <= Acc(0)) { fl |= kFlagBreakdown; break; }
-            const Acc alpha = delta / dq;
-            if (!acc_finite(alpha)) { fl |= kFlagBreakdown; break; }
-            // Phase B: x += alpha d; r -= alpha q; s = M^-1 r; partial r.s and r.r
-            {
-                Acc loc[2] = {Acc(0), Acc(0)};
-                int sbad = 0;
-                for (int r = r0 + tid; r < r1; r += T) {
-                    const V3<Real> dn = ldcg3(dnext, r);
-                    const V3<Real> q = ldcg3(P.q, r);
-                    const V3<Real> xv = axpy<Real, Acc>(ldplain3(P.x, r), alpha, dn);
-                    const V3<Real> rv = axpy<Real, Acc>(ldplain3(P.r, r), -alpha, q);
-                    st3(P.x, r, xv);
-                    st3(P.r, r, rv);
-                    const V3<Real> s = mul(ld9(P.minv, (size_t)r), rv);
-                    if (!finite3(s)) sbad = 1;
-                    st3(P.s, r, s);
-                    loc[0] += dot_acc<Acc>(rv, s);
-                    loc[1] += dot_acc<Acc>(rv, rv);
-                }
-                block_sum<Acc, 2>(loc, sh_acc);
-                sbad = block_or(sbad, sh_int);
-                if (tid == 0) {
-                    P.part_b[2 * blk + 0] = loc[0];
-                    P.part_b[2 * blk + 1] = loc[1];
-                    P.part_bad[4 * blk + 1] = sbad;
-                }
-            }
-            if (!grid_barrier(P.sync, &s_flag)) { timed_out = true; goto finish; }
-            {
-                Acc g2[2];
-                grid_sum<Acc, 2>(P.part_b, 2, g2, sh_acc);
-                rr = g2[1];
-                if (grid_or(P.part_bad + 1, 4, sh_int)) { fl |= kFlagBreakdown; break; }
-                const Acc old = delta;
-                delta = g2[0];
-                if (!acc_finite(delta) || !acc_finite(old) || old <= Acc(0)) { fl |= kFlagBreakdown; break; }
-                beta = delta / old;
-                if (!acc_finite(beta)) { fl |= kFlagBreakdown; break; }
-            }
-            Real* t = dcur;
-            dcur = dnext;
-            dnext = t;
-            iterations = it + 1;
-        }
-        if (delta <= target) converged = true;
-        residual = (acc_finite(rr) && rr >= Acc(0)) ? sqrt(rr) : Acc(INFINITY);
-    }
-
-final_check:
-    // The solve succeeds when x is present and finite; integration is all-or-nothing.
-    {
-        int bad = 0;
-        for (int r = r0 + tid; r < r1; r += T) {
-            const V3<Real> dv = have_x ? ldplain3(P.x, r) : V3<Real>{Real(0), Real(0), Real(0)};
-            if (!finite3(dv)) bad |= 1;
-            if (P.integrate) {
-                const int node = __ldg(P.dyn_to_node + r);
-                const V3<Real> xo = ldplain3(P.node_x, node), vo = ldplain3(P.node_v, node);
-                const V3<Real> nv = vo + dv;
-                const V3<Real> nx = xo + nv * P.dt;
-                if (!finite3(xo) || !finite3(vo) || !finite3(nv) || !finite3(nx)) bad |= 2;
-            }
-        }
-        bad = block_or(bad, sh_int);
-        if (tid == 0) P.part_bad[4 * blk + 2] = bad;
-    }
-    if (!grid_barrier(P.sync, &s_flag)) { timed_out = true; goto finish; }
-    {
-        const int bad = grid_or(P.part_bad + 2, 4, sh_int);
-        const bool solved = have_x && !(bad & 1);
-        if (!have_x) fl |= kFlagInvalidRhs;
-        if (have_x && (bad & 1)) fl |= kFlagNonFiniteDv;
-        if (solved) fl |= kFlagSolved;
-        if (solved && P.integrate) {
-            if (bad & 2) {
-                fl |= kFlagIntegrateAbort;
-            } else {
-                for (int r = r0 + tid; r < r1; r += T) {
-                    const int node = __ldg(P.dyn_to_node + r);
-                    const V3<Real> dv = ldplain3(P.x, r);
-                    const V3<Real> nv = ldplain3(P.node_v, node) + dv;
-                    const V3<Real> nx = ldplain3(P.node_x, node) + nv * P.dt;
-                    st3(P.node_v, node, nv);
-                    st3(P.node_x, node, nx);
-                }
-                fl |= kFlagIntegrated;
-            }
-        }
-        if (converged) fl |= kFlagConverged;
-    }
-
-finish:
-    if (timed_out) fl |= kFlagBarrierTimeout;
-    if (blk == 0 && tid == 0) {
-        P.stats->iterations = iterations;
-        P.stats->converged = converged ? 1 : 0;
-        P.stats->residual_norm = (double)residual;
-        atomicOr(P.flags, fl);
-    } else if (timed_out && tid == 0) {
-        atomicOr(P.flags, kFlagBarrierTimeout);
-    }
-}
-
 // ------------------------------------------------------------------ SpMV kernel
 template <class Real>
 __global__ void __launch_bounds__(256) spmv_kernel(BsrView<Real> A, const Real* x, Real* y)
@@ -755,26 +318,6 @@ cudaError_t launch_row_kernel(const AssemblyArgs<Real>& args, int max_row_blocks
     return launch_rows<Real, 0>(args, stream);
 }
 
-template <class Real, class Acc>
-int pcg_max_grid(int threads)
-{
-    int dev = 0, sms = 0, per_sm = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<Real, Acc>, threads, 0) != cudaSuccess)
-        return 0;
-    return sms * per_sm;
-}
-
-template <class Real, class Acc>
-cudaError_t launch_pcg_kernel(const PcgArgs<Real, Acc>& args, int grid, int threads, cudaStream_t stream)
-{
-    PcgArgs<Real, Acc> a = args;
-    void* kargs[] = {&a};
-    return cudaLaunchCooperativeKernel((const void*)pcg_kernel<Real, Acc>, dim3(grid), dim3(threads), kargs, 0,
-                                       stream);
-}
-
 template <class Real>
 cudaError_t launch_spmv_kernel(const BsrView<Real>& a, const Real* x, Real* y, cudaStream_t stream)
 {
@@ -790,12 +333,6 @@ template cudaError_t launch_tet_kernel<float>(const AssemblyArgs<float>&, bool, 
 template cudaError_t launch_tet_kernel<double>(const AssemblyArgs<double>&, bool, cudaStream_t);
 template cudaError_t launch_row_kernel<float>(const AssemblyArgs<float>&, int, cudaStream_t);
 template cudaError_t launch_row_kernel<double>(const AssemblyArgs<double>&, int, cudaStream_t);
-template cudaError_t launch_pcg_kernel<float, float>(const PcgArgs<float, float>&, int, int, cudaStream_t);
-template cudaError_t launch_pcg_kernel<float, double>(const PcgArgs<float, double>&, int, int, cudaStream_t);
-template cudaError_t launch_pcg_kernel<double, double>(const PcgArgs<double, double>&, int, int, cudaStream_t);
-template int pcg_max_grid<float, float>(int);
-template int pcg_max_grid<float, double>(int);
-template int pcg_max_grid<double, double>(int);
 template cudaError_t launch_spmv_kernel<float>(const BsrView<float>&, const float*, float*, cudaStream_t);
 template cudaError_t launch_spmv_kernel<double>(const BsrView<double>&, const double*, double*, cudaStream_t);
 

@@ -99,9 +99,11 @@ struct PcgArgs {
     const Real* minv;
     Real* x;
     Real* r;
-    Real* s;
-    Real* d0;
-    Real* d1;
+    // Search-direction records, 8 values per row {s.x, s.y, s.z, 0, d.x, d.y, d.z, 0}
+    // (32-byte aligned for float), ping-ponged between iterations so a neighbour's
+    // s + beta*d is one 256-bit load.
+    Real* sd0;
+    Real* sd1;
     Real* q;
     Acc* part_a;      // [grid]
     Acc* part_b;      // [grid * 2]
@@ -117,7 +119,26 @@ struct PcgArgs {
     Real* node_v;
     unsigned* flags;
     DevStats* stats;
+    // SpMV tiles staged into shared memory by TMA bulk copies, 8 ints per tile:
+    // {first row, end row, rs0, row words, k0, blocks, e0, transpose entries}, each range
+    // widened to 16-byte boundaries; ntiles == 0 selects the unstaged SpMV.
+    int ntiles;
+    const int* tile_desc;
 };
+
+// Shared-memory tile of the staged SpMV: at most kTileRowCap row_start / lt_start
+// entries, kTileCapU upper blocks (values + columns) and kTileCapL transpose entries,
+// each range widened to 16-byte boundaries for the bulk copies.
+constexpr int kTileRowsMax = 64;
+constexpr int kTileRowCap = kTileRowsMax + 8;
+constexpr int kTileCapU = 576;
+constexpr int kTileCapL = 512;
+template <class Real>
+constexpr size_t tile_buffer_bytes()
+{
+    return size_t(2 * kTileRowCap) * 4 + size_t(kTileCapU) * 9 * sizeof(Real) + size_t(kTileCapU) * 4 +
+           size_t(2 * kTileCapL) * 4;
+}
 
 // Launchers (pk_kernels.cu).  All asynchronous on `stream`.
 template <class Real>
@@ -126,8 +147,9 @@ template <class Real>
 cudaError_t launch_row_kernel(const AssemblyArgs<Real>& args, int max_row_blocks, cudaStream_t stream);
 template <class Real, class Acc>
 cudaError_t launch_pcg_kernel(const PcgArgs<Real, Acc>& args, int grid, int threads, cudaStream_t stream);
+// Largest cooperative grid (one wave) for the staged (args.ntiles > 0) or unstaged kernel.
 template <class Real, class Acc>
-int pcg_max_grid(int threads);
+int pcg_max_grid(int threads, bool staged);
 template <class Real>
 cudaError_t launch_spmv_kernel(const BsrView<Real>& a, const Real* x, Real* y, cudaStream_t stream);
 

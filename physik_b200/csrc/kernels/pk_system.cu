@@ -7,6 +7,7 @@
 #include <array>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <type_traits>
@@ -47,12 +48,15 @@ struct DevBuf {
         p = nullptr;
         bytes = 0;
     }
+    // Every allocation carries kSlack extra bytes so bulk copies widened to 16-byte
+    // boundaries (at most 4 elements past an array's end) stay inside it.
+    static constexpr size_t kSlack = 1024;
     cudaError_t ensure(size_t want)
     {
         if (want <= bytes && p) return cudaSuccess;
         reset();
         if (want == 0) want = 16;
-        cudaError_t e = cudaMalloc(&p, want);
+        cudaError_t e = cudaMalloc(&p, want + kSlack);
         if (e == cudaSuccess) bytes = want;
         return e;
     }
@@ -104,6 +108,43 @@ void build_transpose(int n, const int* row_start, const int* col, std::vector<in
         }
 }
 
+// Greedy SpMV tiles for the staged PCG: consecutive rows, at most `rows` per tile, with
+// the 16-byte-widened row / upper-block / transpose spans inside the shared-memory caps.
+// Each tile becomes 8 ints {ra, rb, rs0, row words, k0, blocks, e0, transpose entries}.
+// Returns false when a single row does not fit (the unstaged kernel is used then).
+bool build_tiles(int n, const int* row_start, const std::vector<int>& lt_start, int rows, std::vector<int>& desc)
+{
+    desc.clear();
+    auto span = [&](int a, int b, int* out) {
+        const int rs0 = a & ~3, rs1 = (b + 1 + 3) & ~3;
+        const int k0 = row_start[a] & ~3, k1 = (row_start[b] + 3) & ~3;
+        const int e0 = lt_start[a] & ~3, e1 = (lt_start[b] + 3) & ~3;
+        if (out) {
+            out[0] = a; out[1] = b; out[2] = rs0; out[3] = rs1 - rs0;
+            out[4] = k0; out[5] = k1 - k0; out[6] = e0; out[7] = e1 - e0;
+        }
+        return rs1 - rs0 <= pk::kTileRowCap && k1 - k0 <= pk::kTileCapU && e1 - e0 <= pk::kTileCapL &&
+               k1 > k0;
+    };
+    int a = 0;
+    while (a < n) {
+        int b = a;
+        while (b < n && b - a < rows && span(a, b + 1, nullptr)) ++b;
+        if (b == a) return false;
+        int d[8];
+        span(a, b, d);
+        desc.insert(desc.end(), d, d + 8);
+        a = b;
+    }
+    return true;
+}
+
+bool staging_enabled()
+{
+    const char* e = std::getenv("PK_PCG_STAGED");
+    return !(e && e[0] == '0');
+}
+
 }  // namespace
 
 struct pk_system {
@@ -114,7 +155,10 @@ struct pk_system {
     bool have_nodes = false, have_tets = false, have_pattern = false;
     bool diag_first = false;  // every row starts with its diagonal block (needed by the row kernel)
     int pcg_grid_override = 0;
-    int pcg_max_grid = 0;
+    int pcg_max_grid = 0;         // cooperative wave of the unstaged PCG kernel
+    int pcg_max_grid_staged = 0;  // cooperative wave of the staged PCG kernel
+    int ntiles = 0;               // staged SpMV tiles (0: unstaged kernel)
+    DevBuf tiles;
     // nodes
     DevBuf x, v, mass, node_to_dyn;
     // tets
@@ -122,7 +166,7 @@ struct pk_system {
     // rows
     DevBuf dyn_to_node, row_start, col, lt_start, lt_row, lt_block, inc_start, inc_list, values, rhs, minv;
     // solver
-    DevBuf px, pr, ps, pd0, pd1, pq, part_a, part_b, part_bad, sync, stats;
+    DevBuf px, pr, psd0, psd1, pq, part_a, part_b, part_bad, sync, stats;
     pk::DevStats* host_stats = nullptr;  // pinned
     bool stats_pending = false;
     // timing
@@ -194,9 +238,8 @@ pk::PcgArgs<Real, Acc> pcg_args(pk_system* s, const pk_step_params& p, int skip_
     a.minv = s->minv.as<Real>();
     a.x = s->px.as<Real>();
     a.r = s->pr.as<Real>();
-    a.s = s->ps.as<Real>();
-    a.d0 = s->pd0.as<Real>();
-    a.d1 = s->pd1.as<Real>();
+    a.sd0 = s->psd0.as<Real>();
+    a.sd1 = s->psd1.as<Real>();
     a.q = s->pq.as<Real>();
     a.part_a = s->part_a.as<Acc>();
     a.part_b = s->part_b.as<Acc>();
@@ -213,14 +256,17 @@ pk::PcgArgs<Real, Acc> pcg_args(pk_system* s, const pk_step_params& p, int skip_
     pk::DevStats* st = s->stats.as<pk::DevStats>();
     a.flags = &st->flags;
     a.stats = st;
+    a.ntiles = s->ntiles;
+    a.tile_desc = s->tiles.as<int>();
     return a;
 }
 
 template <class Real, class Acc>
 int max_grid_for(pk_system* s)
 {
-    if (!s->pcg_max_grid) s->pcg_max_grid = pk::pcg_max_grid<Real, Acc>(pk::kPcgThreads);
-    return s->pcg_max_grid;
+    if (!s->pcg_max_grid) s->pcg_max_grid = pk::pcg_max_grid<Real, Acc>(pk::kPcgThreads, false);
+    if (!s->pcg_max_grid_staged) s->pcg_max_grid_staged = pk::pcg_max_grid<Real, Acc>(pk::kPcgThreads, true);
+    return std::max(s->pcg_max_grid, s->pcg_max_grid_staged);
 }
 
 constexpr int kRowsPerBlockTarget = 32;
@@ -228,7 +274,15 @@ constexpr int kRowsPerBlockTarget = 32;
 template <class Real, class Acc>
 int pcg_grid_for(pk_system* s)
 {
-    const int mx = max_grid_for<Real, Acc>(s);
+    max_grid_for<Real, Acc>(s);
+    if (s->ntiles > 0) {
+        // Staged kernel: whole tiles per block, one cooperative wave.
+        const int mxs = s->pcg_max_grid_staged;
+        if (mxs <= 0) return 0;
+        const int g = s->pcg_grid_override > 0 ? s->pcg_grid_override : mxs;
+        return std::max(1, std::min(std::min(mxs, g), s->ntiles));  // tiles are dealt round-robin
+    }
+    const int mx = s->pcg_max_grid;
     if (mx <= 0) return 0;
     if (s->pcg_grid_override > 0) return std::min(mx, s->pcg_grid_override);
     // Enough blocks that each phase is one pass over its rows (16 lanes per row in the
@@ -241,11 +295,11 @@ int ensure_solver_buffers(pk_system* s, int grid_cap)
 {
     const size_t rs = s->rsize();
     const size_t v3 = 3 * rs * static_cast<size_t>(std::max(1, s->dyn_count));
+    const size_t rec = 8 * rs * static_cast<size_t>(std::max(1, s->dyn_count));  // {s, 0, d, 0} records
     PK_CHECK(s->px.ensure(v3));
     PK_CHECK(s->pr.ensure(v3));
-    PK_CHECK(s->ps.ensure(v3));
-    PK_CHECK(s->pd0.ensure(v3));
-    PK_CHECK(s->pd1.ensure(v3));
+    PK_CHECK(s->psd0.ensure(rec));
+    PK_CHECK(s->psd1.ensure(rec));
     PK_CHECK(s->pq.ensure(v3));
     const size_t g = static_cast<size_t>(std::max(1, grid_cap));
     PK_CHECK(s->part_a.ensure(g * sizeof(double)));
@@ -566,6 +620,18 @@ PKCUDA_API int pk_system_set_pattern(pk_system* s, int dyn_count, const int* dyn
          : s->precision == PK_PREC_MIXED ? ensure_solver_buffers(s, max_grid_for<float, double>(s))
                                          : ensure_solver_buffers(s, max_grid_for<double, double>(s));
     if (rc) return rc;
+    // Staged SpMV tiles: as many rows per tile as fill one cooperative wave (16..64).
+    s->ntiles = 0;
+    if (staging_enabled() && dyn_count > 0 && s->pcg_max_grid_staged > 0) {
+        const int per_block = (dyn_count + s->pcg_max_grid_staged - 1) / s->pcg_max_grid_staged;
+        const int rows = per_block <= 16 ? 16 : (per_block <= 32 ? 32 : pk::kTileRowsMax);
+        std::vector<int> desc;
+        if (build_tiles(dyn_count, row_start, lts, rows, desc)) {
+            rc = upload_raw<int>(s->tiles, desc.data(), desc.size(), s->stream);
+            if (rc) return rc;
+            s->ntiles = static_cast<int>(desc.size() / 8);
+        }
+    }
     s->have_pattern = true;
     return PK_OK;
 }

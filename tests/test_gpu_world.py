@@ -179,3 +179,31 @@ def test_explicit_mode_matches_reference():
     xr, vr = ref.state()
     assert rel(x, xr) < 1e-6
     assert rel(v, vr) < 1e-4
+
+
+def test_unstaged_spmv_fallback_matches_oracle(monkeypatch):
+    """The PCG kernel without shared-memory tiles (used when a row does not fit a
+    tile) gives the same step as the staged one."""
+    monkeypatch.setenv("PK_PCG_STAGED", "0")
+    ex, ev, di = teacher_forced(two_bodies(), "fp64", 2)
+    assert ex <= 1e-12 and ev <= 1e-8 and di <= 1, (ex, ev, di)
+
+
+def test_staged_and_unstaged_agree_on_beam():
+    """Staged and unstaged SpMV on the 64x16x16 beam: same iterations, same state to rounding."""
+    import os
+    scene = meshes.config2()
+    out = []
+    for flag in ("1", "0"):
+        os.environ["PK_PCG_STAGED"] = flag
+        try:
+            w = SimWorld(scene, precision="fp64")
+            for _ in range(2):
+                w.step()
+            out.append((w.state(f64=True), w.cg_stats()["iterations"]))
+        finally:
+            os.environ.pop("PK_PCG_STAGED", None)
+    (xa, va), ia = out[0]
+    (xb, vb), ib = out[1]
+    assert ia == ib
+    assert rel(xa, xb) < 1e-13 and rel(va, vb) < 1e-9
