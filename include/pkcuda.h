@@ -155,6 +155,26 @@ PKCUDA_API int pk_pcg(int device, int precision, int n, const int* row_start, co
                       const double* values, const double* b, const double* minv, int minv_count, int max_iterations,
                       double tolerance, double* x, pk_cg_result* out);
 
+/* The block-Jacobi PCG solve of pk_pcg on caller-owned DEVICE buffers, allocating nothing.
+ * No counterpart in the reference: it serves callers that may not allocate device memory
+ * while they solve (a game-engine plugin solving inside its frame loop under a fixed
+ * memory budget, or a host that routes all device memory through its own pool).
+ * Inputs: the upper BSR (row_start[n+1], col_index, values: 9 per block in the precision's
+ * scalar type) with its transposed index from pk_bsr_transpose_index (lt_start[n+1],
+ * lt_row, lt_block), the rhs b (3n), the block-Jacobi inverse minv (9n); output x (3n).
+ * The CG working vectors live in one fixed 8 MiB array per GPU, held by every GPU that
+ * loads the library until exit: at most 32,768 rows (PK_ERR_UNSUPPORTED above that).
+ * All calls on a device share that array and it keeps the last call's contents (the call
+ * clears what must start at zero); calls whose GPU work overlaps race on it.  The first
+ * call on a device looks up the array's address, with that device current; make it
+ * before any stream capture begins.  Runs on `stream` of the current device and waits
+ * for it to return the statistics. */
+PKCUDA_API int pk_pcg_noalloc(int precision, int n, const int* row_start, const int* col_index, const void* values,
+                              const int* lt_start, const int* lt_row, const int* lt_block, const void* b,
+                              const void* minv, int max_iterations, double tolerance, void* x, pk_cg_result* out,
+                              void* stream);
+PKCUDA_API const char* pk_pcg_noalloc_last_error(void);
+
 /* Builds the transposed index of an upper BSR: for row r the blocks (c, r), c < r.
  * lt_start[n+1]; lt_row / lt_block sized nnz - n.  Host-only, no device needed. */
 PKCUDA_API int pk_bsr_transpose_index(int n, const int* row_start, const int* col_index, int* lt_start, int* lt_row,

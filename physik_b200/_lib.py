@@ -85,6 +85,8 @@ _SIGS = {
     "pk_bsr_multiply": (_i, [_i, _i, _i, _p, _p, _p, _p, _p]),
     "pk_pcg": (_i, [_i, _i, _i, _p, _p, _p, _p, _p, _i, _i, _d, _p, C.POINTER(PkCgResult)]),
     "pk_bsr_transpose_index": (_i, [_i, _p, _p, _p, _p, _p]),
+    "pk_pcg_noalloc": (_i, [_i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _i, _d, _p, C.POINTER(PkCgResult), _p]),
+    "pk_pcg_noalloc_last_error": (C.c_char_p, []),
     # physik_b200.h
     "PHYSIK_CreateWorld": (_p, []),
     "PHYSIK_DestroyWorld": (_v, [_p]),
