@@ -175,6 +175,16 @@ PKCUDA_API int pk_pcg_noalloc(int precision, int n, const int* row_start, const 
                               void* stream);
 PKCUDA_API const char* pk_pcg_noalloc_last_error(void);
 
+/* Host-only consistency check of the ring-staged PCG kernel's tiling (no device needed):
+ * builds its tiles for the upper BSR (values 9 per block, x 3 per row), replays the
+ * kernel's shared-memory staging byte for byte and evaluates y = A x through the staged
+ * data as the kernel's lanes index it.  Returns the number of index / span violations
+ * (0 = consistent), or a negative PK_ERR_* code; tiles and max_span (may be NULL)
+ * receive the tile count and the largest staged block span.  No counterpart in the
+ * reference (it checks this library's own layout). */
+PKCUDA_API int pk_ring_tiling_selfcheck(int precision, int n, const int* row_start, const int* col_index,
+                                        const double* values, const double* x, double* y, int* tiles, int* max_span);
+
 /* Builds the transposed index of an upper BSR: for row r the blocks (c, r), c < r.
  * lt_start[n+1]; lt_row / lt_block sized nnz - n.  Host-only, no device needed. */
 PKCUDA_API int pk_bsr_transpose_index(int n, const int* row_start, const int* col_index, int* lt_start, int* lt_row,

@@ -140,6 +140,90 @@ constexpr size_t tile_buffer_bytes()
            size_t(2 * kTileCapL) * 4;
 }
 
+// ------------------------------------------------------------------ ring-staged PCG
+// The ring-staged PCG kernel (pk_pcg_ring.cu) cuts the rows into tiles of at most kRows
+// consecutive rows and streams each tile's part of the matrix -- row extents, upper
+// blocks with their columns, and the transposed index (rows and block numbers of the
+// lower entries) -- into shared memory with TMA bulk copies, through a ring of kStages
+// buffers filled by one producer warp.  Consumer warps, in kRingGroups groups that take
+// every kRingGroups-th ring position, compute the tile's rows of q = A (s + beta d)
+// from the staged data plus gathers of the neighbours' {s, d} records and of the
+// transposed lower blocks (both L2 hits, as the grid sweeps one wavefront through the
+// matrix).  kStages is a multiple of kRingGroups, so a stage is always reused by the
+// group that used it last and its mbarrier parity cannot be mistaken.
+// Caps are in entries; every span is widened to 16-byte boundaries (row words to 4,
+// blocks and lower entries to 4).
+template <class Real>
+struct RingTile;
+template <>
+struct RingTile<float> {
+    static constexpr int kRows = 32, kRsCap = 40, kCapU = 320, kCapL = 288;
+    static constexpr int kStages = 12, kLanesPerRow = 4;  // 32 rows per consumer group of 4 warps (4 stages each)
+};
+template <>
+struct RingTile<double> {
+    static constexpr int kRows = 16, kRsCap = 24, kCapU = 160, kCapL = 144;
+    static constexpr int kStages = 12, kLanesPerRow = 8;  // 16 rows per consumer group of 4 warps
+};
+constexpr int kRingGroups = 3;  // 13 warps: at most 4 per SM sub-partition, so 128 registers
+constexpr int kRingGroupWarps = 4;
+constexpr int kRingConsumerWarps = kRingGroups * kRingGroupWarps;
+constexpr int kRingThreads = 32 * (kRingConsumerWarps + 1);  // + one producer warp
+constexpr int kRingDescInts = 8;  // per tile: ra, rb, rs0, nrs, k0, nk, e0, ne
+constexpr int kRingMaxTilesPerBlock = 512;
+
+constexpr size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Byte offsets of one ring stage, then of the block's descriptor table after the ring.
+template <class Real>
+struct RingLayout {
+    using T = RingTile<Real>;
+    static constexpr size_t kRs = 0;
+    static constexpr size_t kLts = kRs + 4 * T::kRsCap;
+    static constexpr size_t kVals = align_up(kLts + 4 * T::kRsCap, 16);
+    static constexpr size_t kCol = align_up(kVals + sizeof(Real) * 9 * T::kCapU, 16);
+    static constexpr size_t kLtr = align_up(kCol + 4 * T::kCapU, 16);
+    static constexpr size_t kLtb = align_up(kLtr + 4 * T::kCapL, 16);
+    static constexpr size_t kBytes = align_up(kLtb + 4 * T::kCapL, 128);
+    static constexpr size_t kTable = kBytes * T::kStages;
+    static constexpr size_t kTotal = kTable + 4 * kRingDescInts * size_t(kRingMaxTilesPerBlock);
+};
+
+// One block's published partials for a grid exchange (double buffered by generation).
+struct __align__(32) ExSlot {
+    double v0, v1;
+    int bad;
+    unsigned gen;
+    int pad0, pad1;
+};
+
+template <class Real, class Acc>
+struct RingPcgArgs {
+    BsrView<Real> a;
+    int nnz;                     // stored upper blocks
+    int ntiles;
+    const int* desc;             // kRingDescInts per tile
+    const Real* b;
+    const Real* minv;
+    Real* x;
+    Real* r;
+    Real* sd0;                   // {s.xyz, 0, d.xyz, 0} per row, ping-ponged
+    Real* sd1;
+    Real* q4;                    // {q.xyz, 0} per row
+    ExSlot* slots;               // [2][grid]
+    GridSync* sync;              // err flag
+    int max_iterations;
+    Acc tolerance;
+    int skip_on_flags;
+    int integrate;
+    Real dt;
+    const int* dyn_to_node;
+    Real* node_x;
+    Real* node_v;
+    unsigned* flags;
+    DevStats* stats;
+};
+
 // Launchers (pk_kernels.cu).  All asynchronous on `stream`.
 template <class Real>
 cudaError_t launch_tet_kernel(const AssemblyArgs<Real>& args, bool fp64_polar_fallback, cudaStream_t stream);
@@ -152,6 +236,11 @@ template <class Real, class Acc>
 int pcg_max_grid(int threads, bool staged);
 template <class Real>
 cudaError_t launch_spmv_kernel(const BsrView<Real>& a, const Real* x, Real* y, cudaStream_t stream);
+// Ring-staged PCG (pk_pcg_ring.cu): one block of kRingThreads per SM.
+template <class Real, class Acc>
+cudaError_t launch_pcg_ring_kernel(const RingPcgArgs<Real, Acc>& args, int grid, cudaStream_t stream);
+template <class Real, class Acc>
+int pcg_ring_max_grid();
 
 constexpr int kPcgThreads = 512;
 

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <iterator>
 #include <array>
 #include <cmath>
 #include <cstdio>
@@ -145,6 +146,49 @@ bool staging_enabled()
     return !(e && e[0] == '0');
 }
 
+// Which PCG kernel a system uses: the ring-staged kernel when its tiling fits, else the
+// TMA-staged or the unstaged one.  PK_PCG_KERNEL=staged / plain forces the older kernels.
+int requested_kernel()
+{
+    const char* e = std::getenv("PK_PCG_KERNEL");
+    if (e && std::strcmp(e, "staged") == 0) return 1;
+    if (e && std::strcmp(e, "plain") == 0) return 2;
+    return 0;
+}
+
+// Tiles of the ring-staged PCG kernel (pk::RingTile caps): consecutive rows, at most
+// kRows per tile, grown while the row words (widened to 4) and the upper-block and
+// transposed-entry spans (widened to multiples of 4) fit a ring stage.  Each tile is
+// kRingDescInts ints {ra, rb, rs0, row words, k0, blocks, e0, transposed entries}.
+// Returns false when a single row does not fit (an older kernel is used then).
+template <class Real>
+bool build_ring_tiles(int n, const int* row_start, const std::vector<int>& lts, std::vector<int>& desc)
+{
+    using T = pk::RingTile<Real>;
+    desc.clear();
+    auto span = [&](int a, int b, int* out) {
+        const int rs0 = a & ~3, rs1 = (b + 1 + 3) & ~3;
+        const int k0 = row_start[a] & ~3, k1 = (row_start[b] + 3) & ~3;
+        const int e0 = lts[a] & ~3, e1 = (lts[b] + 3) & ~3;
+        if (out) {
+            const int d[pk::kRingDescInts] = {a, b, rs0, rs1 - rs0, k0, k1 - k0, e0, e1 - e0};
+            std::copy(d, d + pk::kRingDescInts, out);
+        }
+        return rs1 - rs0 <= T::kRsCap && k1 - k0 <= T::kCapU && e1 - e0 <= T::kCapL && k1 > k0;
+    };
+    int a = 0;
+    while (a < n) {
+        int b = a;
+        while (b < n && b - a < T::kRows && span(a, b + 1, nullptr)) ++b;
+        if (b == a) return false;
+        int d[pk::kRingDescInts];
+        span(a, b, d);
+        desc.insert(desc.end(), d, d + pk::kRingDescInts);
+        a = b;
+    }
+    return true;
+}
+
 }  // namespace
 
 struct pk_system {
@@ -159,6 +203,9 @@ struct pk_system {
     int pcg_max_grid_staged = 0;  // cooperative wave of the staged PCG kernel
     int ntiles = 0;               // staged SpMV tiles (0: unstaged kernel)
     DevBuf tiles;
+    int ring_tiles = 0;           // ring-staged PCG tiles (0: not used)
+    int ring_max_grid = 0;
+    DevBuf ring_desc, q4, slots;
     // nodes
     DevBuf x, v, mass, node_to_dyn;
     // tets
@@ -310,8 +357,78 @@ int ensure_solver_buffers(pk_system* s, int grid_cap)
 }
 
 template <class Real, class Acc>
+int ring_max_grid(pk_system* s)
+{
+    if (!s->ring_max_grid) s->ring_max_grid = pk::pcg_ring_max_grid<Real, Acc>();
+    return s->ring_max_grid;
+}
+
+template <class Real, class Acc>
+int ring_grid_for(pk_system* s)
+{
+    const int mx = ring_max_grid<Real, Acc>(s);
+    if (mx <= 0) return 0;
+    const int g = s->pcg_grid_override > 0 ? std::min(s->pcg_grid_override, mx) : mx;
+    return std::max(1, std::min(g, s->ring_tiles));
+}
+
+template <class Real, class Acc>
+int run_pcg_ring(pk_system* s, const pk_step_params& p, int skip_on_flags)
+{
+    const int grid = ring_grid_for<Real, Acc>(s);
+    if (grid <= 0) return fail(PK_ERR_CUDA, "ring PCG kernel cannot be resident");
+    if ((s->ring_tiles + grid - 1) / grid > pk::kRingMaxTilesPerBlock)
+        return fail(PK_ERR_UNSUPPORTED, "ring PCG: too many tiles per block for this grid");
+    const size_t rs = s->rsize();
+    const size_t n = static_cast<size_t>(std::max(1, s->dyn_count));
+    PK_CHECK(s->q4.ensure(4 * rs * n));
+    PK_CHECK(s->slots.ensure(2 * sizeof(pk::ExSlot) * static_cast<size_t>(grid)));
+    PK_CHECK(cudaMemsetAsync(s->slots.p, 0, 2 * sizeof(pk::ExSlot) * static_cast<size_t>(grid), s->stream));
+    PK_CHECK(cudaMemsetAsync(s->sync.p, 0, sizeof(pk::GridSync), s->stream));
+    pk::RingPcgArgs<Real, Acc> a{};
+    a.a.n = s->dyn_count;
+    a.a.row_start = s->row_start.as<int>();
+    a.a.col = s->col.as<int>();
+    a.a.values = s->values.as<Real>();
+    a.a.lt_start = s->lt_start.as<int>();
+    a.a.lt_row = s->lt_row.as<int>();
+    a.a.lt_block = s->lt_block.as<int>();
+    a.nnz = s->nnz;
+    a.ntiles = s->ring_tiles;
+    a.desc = s->ring_desc.as<int>();
+    a.b = s->rhs.as<Real>();
+    a.minv = s->minv.as<Real>();
+    a.x = s->px.as<Real>();
+    a.r = s->pr.as<Real>();
+    a.sd0 = s->psd0.as<Real>();
+    a.sd1 = s->psd1.as<Real>();
+    a.q4 = s->q4.as<Real>();
+    a.slots = s->slots.as<pk::ExSlot>();
+    a.sync = s->sync.as<pk::GridSync>();
+    a.max_iterations = p.max_iterations;
+    a.tolerance = static_cast<Acc>(static_cast<Real>(p.tolerance));
+    a.skip_on_flags = skip_on_flags;
+    a.integrate = p.integrate;
+    a.dt = static_cast<Real>(p.dt);
+    a.dyn_to_node = s->dyn_to_node.as<int>();
+    a.node_x = s->x.as<Real>();
+    a.node_v = s->v.as<Real>();
+    pk::DevStats* st = s->stats.as<pk::DevStats>();
+    a.flags = &st->flags;
+    a.stats = st;
+    PK_CHECK(pk::launch_pcg_ring_kernel<Real, Acc>(a, grid, s->stream));
+    s->launches += 1;
+    return PK_OK;
+}
+
+template <class Real, class Acc>
 int run_pcg(pk_system* s, const pk_step_params& p, int skip_on_flags)
 {
+    if (s->ring_tiles > 0) {
+        int rc = ensure_solver_buffers(s, 1);
+        if (rc) return rc;
+        return run_pcg_ring<Real, Acc>(s, p, skip_on_flags);
+    }
     const int grid = pcg_grid_for<Real, Acc>(s);
     if (grid <= 0) return fail(PK_ERR_CUDA, "cooperative PCG kernel cannot be resident");
     int rc = ensure_solver_buffers(s, max_grid_for<Real, Acc>(s));
@@ -620,9 +737,25 @@ PKCUDA_API int pk_system_set_pattern(pk_system* s, int dyn_count, const int* dyn
          : s->precision == PK_PREC_MIXED ? ensure_solver_buffers(s, max_grid_for<float, double>(s))
                                          : ensure_solver_buffers(s, max_grid_for<double, double>(s));
     if (rc) return rc;
+    // Ring-staged PCG tiles (the default kernel).
+    s->ring_tiles = 0;
+    if (requested_kernel() == 0 && dyn_count > 0 && diag_first) {
+        std::vector<int> desc;
+        const bool ok = s->precision == PK_PREC_FP64 ? build_ring_tiles<double>(dyn_count, row_start, lts, desc)
+                                                     : build_ring_tiles<float>(dyn_count, row_start, lts, desc);
+        const int mx = s->precision == PK_PREC_FP32    ? ring_max_grid<float, float>(s)
+                       : s->precision == PK_PREC_MIXED ? ring_max_grid<float, double>(s)
+                                                       : ring_max_grid<double, double>(s);
+        const int ntiles = static_cast<int>(desc.size()) / pk::kRingDescInts;
+        if (ok && mx > 0 && (ntiles + mx - 1) / mx <= pk::kRingMaxTilesPerBlock) {
+            rc = upload_raw<int>(s->ring_desc, desc.data(), desc.size(), s->stream);
+            if (rc) return rc;
+            s->ring_tiles = ntiles;
+        }
+    }
     // Staged SpMV tiles: as many rows per tile as fill one cooperative wave (16..64).
     s->ntiles = 0;
-    if (staging_enabled() && dyn_count > 0 && s->pcg_max_grid_staged > 0) {
+    if (requested_kernel() != 2 && staging_enabled() && dyn_count > 0 && s->pcg_max_grid_staged > 0) {
         const int per_block = (dyn_count + s->pcg_max_grid_staged - 1) / s->pcg_max_grid_staged;
         const int rows = per_block <= 16 ? 16 : (per_block <= 32 ? 32 : pk::kTileRowsMax);
         std::vector<int> desc;
@@ -740,6 +873,11 @@ PKCUDA_API int pk_system_set_pcg_grid(pk_system* s, int grid)
     if (!s) return fail(PK_ERR_ARG, "pcg grid");
     PK_CHECK(cudaSetDevice(s->device));
     s->pcg_grid_override = std::max(0, grid);
+    if (s->ring_tiles > 0) {
+        if (s->precision == PK_PREC_FP32) return ring_grid_for<float, float>(s);
+        if (s->precision == PK_PREC_MIXED) return ring_grid_for<float, double>(s);
+        return ring_grid_for<double, double>(s);
+    }
     if (s->precision == PK_PREC_FP32) return pcg_grid_for<float, float>(s);
     if (s->precision == PK_PREC_MIXED) return pcg_grid_for<float, double>(s);
     return pcg_grid_for<double, double>(s);
@@ -755,6 +893,132 @@ PKCUDA_API int pk_bsr_transpose_index(int n, const int* row_start, const int* co
     if (lt_row) std::copy(b.begin(), b.end(), lt_row);
     if (lt_block) std::copy(c.begin(), c.end(), lt_block);
     return static_cast<int>(b.size());
+}
+
+}  // extern "C"
+
+namespace {
+
+// Host replay of the ring-staged kernel's phase A addressing (see pk_pcg_ring.cu): builds
+// the tiling, fills one stage buffer per tile byte for byte as the producer's bulk copies
+// do (same widened spans, same offsets, from arrays with the device allocations' slack),
+// then evaluates every row as the consumer lanes do: upper blocks and columns from the
+// stage, transposed lower blocks and neighbour values from the full arrays through the
+// staged transposed index.  Every index is checked against its capacity and span; the
+// number of violations is returned (0 = consistent).
+template <class Real>
+int ring_selfcheck(int n, const int* row_start, const int* col, const double* values_d, const double* x_d,
+                   double* y, int* out_tiles, int* out_max_span)
+{
+    using T = pk::RingTile<Real>;
+    using LY = pk::RingLayout<Real>;
+    std::vector<int> lts, ltr, ltb, desc;
+    build_transpose(n, row_start, col, lts, ltr, ltb);
+    if (!build_ring_tiles<Real>(n, row_start, lts, desc)) return -1;
+    const int nnz = n > 0 ? row_start[n] : 0;
+    const int ntiles = static_cast<int>(desc.size()) / pk::kRingDescInts;
+    // "Device" arrays with the same 1 KB slack as DevBuf.
+    auto padded = [](const void* src, size_t bytes) {
+        std::vector<unsigned char> v(bytes + DevBuf::kSlack, 0);
+        if (bytes) std::memcpy(v.data(), src, bytes);
+        return v;
+    };
+    std::vector<Real> vr(9 * static_cast<size_t>(nnz));
+    for (size_t i = 0; i < vr.size(); ++i) vr[i] = static_cast<Real>(values_d[i]);
+    const auto dvals = padded(vr.data(), sizeof(Real) * vr.size());
+    const auto drs = padded(row_start, 4 * size_t(n + 1));
+    const auto dlts = padded(lts.data(), 4 * lts.size());
+    const auto dcol = padded(col, 4 * size_t(nnz));
+    const auto dltr = padded(ltr.data(), 4 * ltr.size());
+    const auto dltb = padded(ltb.data(), 4 * ltb.size());
+    std::vector<unsigned char> stage(LY::kBytes);
+    int bad = 0, max_span = 0;
+    for (int t = 0; t < ntiles; ++t) {
+        const int* d = desc.data() + pk::kRingDescInts * t;
+        const int ra = d[0], rb = d[1], rs0 = d[2], nrs = d[3], k0 = d[4], nk = d[5], e0 = d[6], ne = d[7];
+        // The kernel's descriptor check.
+        const bool ok = rb > ra && rb - ra <= T::kRows && ra >= rs0 && nrs > 0 && nrs <= T::kRsCap &&
+                        rb + 1 <= rs0 + nrs && nk > 0 && nk <= T::kCapU && ne >= 0 && ne <= T::kCapL &&
+                        ((rs0 | nrs | k0 | nk | e0 | ne) & 3) == 0;
+        if (!ok) {
+            ++bad;
+            continue;
+        }
+        max_span = std::max(max_span, nk);
+        // Bulk copies: inside the source arrays plus slack, inside their stage regions.
+        bad += (4 * size_t(rs0 + nrs) > drs.size()) + (4 * size_t(rs0 + nrs) > dlts.size()) +
+               (sizeof(Real) * 9 * size_t(k0 + nk) > dvals.size()) + (4 * size_t(k0 + nk) > dcol.size()) +
+               (4 * size_t(e0 + ne) > dltr.size()) + (4 * size_t(e0 + ne) > dltb.size());
+        bad += (LY::kRs + 4 * size_t(nrs) > LY::kLts) + (LY::kLts + 4 * size_t(nrs) > LY::kVals) +
+               (LY::kVals + sizeof(Real) * 9 * size_t(nk) > LY::kCol) + (LY::kCol + 4 * size_t(nk) > LY::kLtr) +
+               (LY::kLtr + 4 * size_t(ne) > LY::kLtb) + (LY::kLtb + 4 * size_t(ne) > LY::kBytes);
+        if (bad) continue;
+        unsigned char* st = stage.data();
+        std::fill(stage.begin(), stage.end(), 0xFF);
+        std::memcpy(st + LY::kRs, drs.data() + 4 * size_t(rs0), 4 * nrs);
+        std::memcpy(st + LY::kLts, dlts.data() + 4 * size_t(rs0), 4 * nrs);
+        std::memcpy(st + LY::kVals, dvals.data() + sizeof(Real) * 9 * size_t(k0), sizeof(Real) * 9 * nk);
+        std::memcpy(st + LY::kCol, dcol.data() + 4 * size_t(k0), 4 * nk);
+        if (ne > 0) {
+            std::memcpy(st + LY::kLtr, dltr.data() + 4 * size_t(e0), 4 * ne);
+            std::memcpy(st + LY::kLtb, dltb.data() + 4 * size_t(e0), 4 * ne);
+        }
+        const int* srs = reinterpret_cast<const int*>(st + LY::kRs);
+        const int* slts = reinterpret_cast<const int*>(st + LY::kLts);
+        const Real* svals = reinterpret_cast<const Real*>(st + LY::kVals);
+        const int* scol = reinterpret_cast<const int*>(st + LY::kCol);
+        const int* sltr = reinterpret_cast<const int*>(st + LY::kLtr);
+        const int* sltb = reinterpret_cast<const int*>(st + LY::kLtb);
+        for (int lr = 0; lr < rb - ra; ++lr) {
+            const int r = ra + lr, o = r - rs0;
+            const int ks = srs[o], nu = srs[o + 1] - ks, ls = slts[o], tot = nu + (slts[o + 1] - ls);
+            bad += !(ks == row_start[r] && nu == row_start[r + 1] - row_start[r] && ls == lts[r]);
+            double acc[3] = {0, 0, 0};
+            for (int j = 0; j < tot; ++j) {
+                const bool lower = j >= nu;
+                int c, k;
+                const Real* B;
+                if (!lower) {
+                    const int kk = ks + j - k0;
+                    if (!(kk >= 0 && kk < nk && kk < T::kCapU)) { ++bad; continue; }
+                    c = scol[kk];
+                    B = svals + 9 * kk;
+                } else {
+                    const int ee = ls + (j - nu) - e0;
+                    if (!(ee >= 0 && ee < ne && ee < T::kCapL)) { ++bad; continue; }
+                    c = sltr[ee];
+                    k = sltb[ee];
+                    if (!(k >= 0 && k < nnz)) { ++bad; continue; }
+                    B = vr.data() + 9 * size_t(k);
+                }
+                if (!(c >= 0 && c < n)) { ++bad; continue; }
+                const double xc[3] = {double(Real(x_d[3 * c])), double(Real(x_d[3 * c + 1])),
+                                      double(Real(x_d[3 * c + 2]))};
+                for (int i = 0; i < 3; ++i)
+                    for (int m = 0; m < 3; ++m)
+                        acc[i] += lower ? double(B[3 * i + m]) * xc[m] : double(B[3 * m + i]) * xc[m];
+            }
+            for (int i = 0; i < 3; ++i) y[3 * r + i] = acc[i];
+        }
+    }
+    if (out_tiles) *out_tiles = ntiles;
+    if (out_max_span) *out_max_span = max_span;
+    return bad;
+}
+
+}  // namespace
+
+extern "C" {
+
+PKCUDA_API int pk_ring_tiling_selfcheck(int precision, int n, const int* row_start, const int* col_index,
+                                        const double* values, const double* x, double* y, int* tiles, int* max_span)
+{
+    if (n <= 0 || !row_start || !col_index || !values || !x || !y) return fail(PK_ERR_ARG, "selfcheck");
+    const int rc = precision == PK_PREC_FP64
+                       ? ring_selfcheck<double>(n, row_start, col_index, values, x, y, tiles, max_span)
+                       : ring_selfcheck<float>(n, row_start, col_index, values, x, y, tiles, max_span);
+    if (rc < 0) return fail(PK_ERR_UNSUPPORTED, "a row does not fit a ring stage");
+    return rc;
 }
 
 // Standalone SpMV on host arrays: y = A x with A stored upper-only.
