@@ -176,6 +176,16 @@ PHYSIK_B200_API int PHYSIK_B200_EnableTiming(PhysikWorldHandle world, int on);
 PHYSIK_B200_API int PHYSIK_B200_GetTimings(PhysikWorldHandle world, double* assembleMs, double* solveMs, int* steps,
                                            long long* kernelLaunches);
 PHYSIK_B200_API int PHYSIK_B200_SetPcgGrid(PhysikWorldHandle world, int grid);
+/* Batched solve: one PCG per tet-mesh physics component (own scalars, stopping test,
+ * iteration count and all-or-nothing integration, as a world holding only that body),
+ * all bodies in one launch, instead of the reference's single coupled PCG over the whole
+ * world.  The world's CG getters then report the largest iteration count, the largest
+ * residual and "converged" only if every body converged. */
+PHYSIK_B200_API void PHYSIK_B200_SetBatchedSolve(PhysikWorldHandle world, int on);
+/* One body's statistics of the last batched step; 0 on success, -1 if unavailable. */
+PHYSIK_B200_API int PHYSIK_B200_GetBodyConjugateGradientStats(PhysikWorldHandle world, PhysikComponentHandle body,
+                                                              int* iterations, int* converged, float* residualNorm,
+                                                              unsigned* flags);
 /* The CUDA stream (cudaStream_t) the world's device work runs on, or NULL before the
  * first upload; lets a caller record its own events around steps. */
 PHYSIK_B200_API void* PHYSIK_B200_GetStream(PhysikWorldHandle world);

@@ -126,6 +126,20 @@ PKCUDA_API int pk_system_set_tets(pk_system* sys, int tet_count, const int* tet_
 PKCUDA_API int pk_system_set_pattern(pk_system* sys, int dyn_count, const int* dyn_to_node, const int* row_start,
                                      const int* col_index, const int* inc_start, const int* inc_list);
 
+/* Batched per-body solve (no counterpart in the reference, whose World solves all of its
+ * bodies as one coupled system): the dynamic rows split into independent segments
+ * (bodies) [segment_row_start[b], segment_row_start[b+1]), covering all rows, with no
+ * block coupling two segments.  With batching on, pk_system_step runs one PCG per
+ * segment -- own scalars, stopping test, iteration count and all-or-nothing integration,
+ * as a reference World holding only that body -- all in one launch.  Step statistics then
+ * report the largest iteration count, the largest residual, and success flags that hold
+ * for every body.  Call set_segments after set_pattern (set_pattern clears them). */
+PKCUDA_API int pk_system_set_segments(pk_system* sys, int segment_count, const int* segment_row_start);
+PKCUDA_API int pk_system_set_batched(pk_system* sys, int on);
+/* Per-segment statistics of the last batched step (waits); any pointer may be NULL. */
+PKCUDA_API int pk_system_segment_stats(pk_system* sys, int segment_count, int* iterations, int* converged,
+                                       double* residual_norm, unsigned* flags);
+
 /* One substep, asynchronous on the system stream. */
 PKCUDA_API int pk_system_step(pk_system* sys, const pk_step_params* params);
 /* Waits for the last step and reports its statistics. */

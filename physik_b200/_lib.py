@@ -87,6 +87,10 @@ _SIGS = {
     "pk_bsr_transpose_index": (_i, [_i, _p, _p, _p, _p, _p]),
     "pk_pcg_noalloc": (_i, [_i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _i, _d, _p, C.POINTER(PkCgResult), _p]),
     "pk_pcg_noalloc_last_error": (C.c_char_p, []),
+    "pk_system_set_segments": (_i, [_p, _i, _p]),
+    "pk_system_set_batched": (_i, [_p, _i]),
+    "pk_system_segment_stats": (_i, [_p, _i, _p, _p, _p, _p]),
+    "pk_ring_tiling_selfcheck": (_i, [_i, _i, _p, _p, _p, _p, _p, _p, _p]),
     # physik_b200.h
     "PHYSIK_CreateWorld": (_p, []),
     "PHYSIK_DestroyWorld": (_v, [_p]),
@@ -150,6 +154,8 @@ _SIGS = {
     "PHYSIK_B200_EnableTiming": (_i, [_p, _i]),
     "PHYSIK_B200_GetTimings": (_i, [_p, _p, _p, _p, _p]),
     "PHYSIK_B200_SetPcgGrid": (_i, [_p, _i]),
+    "PHYSIK_B200_SetBatchedSolve": (_v, [_p, _i]),
+    "PHYSIK_B200_GetBodyConjugateGradientStats": (_i, [_p, _H, _p, _p, _p, _p]),
     "PHYSIK_B200_GetStream": (_p, [_p]),
     "PHYSIK_B200_Synchronize": (_i, [_p]),
 }

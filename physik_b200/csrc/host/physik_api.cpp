@@ -542,6 +542,35 @@ PHYSIK_B200_API int PHYSIK_B200_GetTimings(PhysikWorldHandle world, double* asse
     return pk_system_timings(w->GetDeviceSystem(), assembleMs, solveMs, steps, kernelLaunches);
 }
 
+PHYSIK_B200_API void PHYSIK_B200_SetBatchedSolve(PhysikWorldHandle world, int on)
+{
+    World* w = AsWorld(world);
+    if (w) w->SetBatchedSolve(on != 0);
+}
+
+PHYSIK_B200_API int PHYSIK_B200_GetBodyConjugateGradientStats(PhysikWorldHandle world, PhysikComponentHandle body,
+                                                              int* iterations, int* converged, float* residualNorm,
+                                                              unsigned* flags)
+{
+    World* w = AsWorld(world);
+    if (!w) return -1;
+    return Guard(
+        [&] {
+            Component* c = w->GetComponent(ToHandle(body));
+            int it = 0;
+            bool conv = false;
+            float res = 0.0f;
+            unsigned fl = 0;
+            if (!c || !w->GetBodyConjugateGradientStats(c, it, conv, res, fl)) return -1;
+            if (iterations) *iterations = it;
+            if (converged) *converged = conv ? 1 : 0;
+            if (residualNorm) *residualNorm = res;
+            if (flags) *flags = fl;
+            return 0;
+        },
+        -1);
+}
+
 PHYSIK_B200_API int PHYSIK_B200_SetPcgGrid(PhysikWorldHandle world, int grid)
 {
     World* w = AsWorld(world);

@@ -380,6 +380,15 @@ public:
     void SetGravity(const Vec3& value) { gravity = value; }
     const Vec3& GetGravity() const { return gravity; }
 
+    // Batched solve (extension): one PCG per TetMeshPhysicsComponent -- own scalars,
+    // stopping test, iteration count and all-or-nothing integration, as a World holding
+    // only that body -- instead of the reference's single coupled PCG over all bodies.
+    void SetBatchedSolve(bool on);
+    bool GetBatchedSolve() const { return batchedSolve; }
+    // Last step's solve statistics of one body in batched mode; false if unavailable.
+    bool GetBodyConjugateGradientStats(const Component* body, int& iterations, bool& converged, float& residualNorm,
+                                       unsigned& flags) const;
+
     // Device precision (extension).  Changing it rebuilds the device scene.
     void SetPrecision(Precision p);
     Precision GetPrecision() const { return precision; }
@@ -445,6 +454,7 @@ private:
     Vec3 gravity{};
     Precision precision = Precision::FP32;
     int device = 0;
+    bool batchedSolve = false;
     std::uint64_t topologyVersion = 1;
 
     SolverData solverData;

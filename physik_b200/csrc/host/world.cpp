@@ -344,6 +344,12 @@ struct DeviceScene {
     int dynCount = 0;
     int tetCount = 0;
     std::vector<int> nodeToDyn, dynToNode, rowStart, colIndex, tetNodes, incStart, incList;
+    // Batched solve: the bodies' dynamic row ranges in row order (segStart), each body's
+    // segment, and whether every dynamic row belongs to one body (else no batching).
+    std::vector<int> segStart;
+    std::vector<std::pair<const Component*, int>> bodySegment;
+    bool segmentsCover = false;
+    bool batchedOnDevice = false;
     std::vector<unsigned char> enabled;
     std::vector<double> mass, dmInv, volume, lam, mu, damp;
 
@@ -465,6 +471,43 @@ void BuildHostScene(DeviceScene& sc, const World& w, const std::vector<const Tet
         sc.colIndex.insert(sc.colIndex.end(), cols.begin(), cols.end());
         sc.rowStart[static_cast<std::size_t>(r) + 1] = static_cast<int>(sc.colIndex.size());
     }
+    // Body segments: each body's nodes are one contiguous world range, so its dynamic rows
+    // are one contiguous row range; bodies taken in node order.
+    {
+        std::vector<std::pair<int, const TetMeshPhysicsComponent*>> byBase;
+        for (const TetMeshPhysicsComponent* body : fem) byBase.emplace_back(body->GetGlobalNodeBeginIndex(), body);
+        std::sort(byBase.begin(), byBase.end(),
+                  [](const auto& a, const auto& b) { return a.first < b.first; });
+        sc.segStart.assign(1, 0);
+        sc.bodySegment.clear();
+        int covered = 0;
+        bool ok = true;
+        for (const auto& e : byBase) {
+            const int b0 = e.first, b1 = b0 + e.second->GetGlobalNodeCount();
+            int first = -1, last = -1;
+            for (int i = b0; i < b1 && i < nn; ++i) {
+                const int r = sc.nodeToDyn[static_cast<std::size_t>(i)];
+                if (r < 0) continue;
+                if (first < 0) first = r;
+                last = r;
+            }
+            if (first < 0) {  // no dynamic row: an empty segment
+                sc.bodySegment.emplace_back(e.second, static_cast<int>(sc.segStart.size()) - 1);
+                sc.segStart.push_back(covered);
+                continue;
+            }
+            if (first != covered || last - first + 1 != [&] {
+                    int c = 0;
+                    for (int i = b0; i < b1 && i < nn; ++i) c += sc.nodeToDyn[static_cast<std::size_t>(i)] >= 0;
+                    return c;
+                }())
+                ok = false;
+            sc.bodySegment.emplace_back(e.second, static_cast<int>(sc.segStart.size()) - 1);
+            covered = last + 1;
+            sc.segStart.push_back(covered);
+        }
+        sc.segmentsCover = ok && covered == dyn && !byBase.empty();
+    }
     sc.mass.assign(massT.begin(), massT.end());
     sc.nodeCount = nn;
     sc.dynCount = dyn;
@@ -487,6 +530,7 @@ void UploadScene(DeviceScene& sc, const std::vector<Vec3>& positions, const std:
     Check(pk_system_set_pattern(sc.sys, sc.dynCount, sc.dynToNode.data(), sc.rowStart.data(), sc.colIndex.data(),
                                 sc.incStart.data(), sc.incList.data()),
           "set_pattern");
+    sc.batchedOnDevice = false;
     sc.uploaded = true;
 }
 
@@ -800,6 +844,30 @@ void World::EnsureScene(bool upload)
     }
 }
 
+void World::SetBatchedSolve(bool on) { batchedSolve = on; }
+
+bool World::GetBodyConjugateGradientStats(const Component* body, int& iterations, bool& converged,
+                                          float& residualNorm, unsigned& flags) const
+{
+    SyncStats();
+    if (!scene || !scene->uploaded || !scene->batchedOnDevice) return false;
+    const int nseg = static_cast<int>(scene->segStart.size()) - 1;
+    for (const auto& e : scene->bodySegment) {
+        if (e.first != body) continue;
+        std::vector<int> it(static_cast<std::size_t>(nseg)), conv(static_cast<std::size_t>(nseg));
+        std::vector<double> res(static_cast<std::size_t>(nseg));
+        std::vector<unsigned> fl(static_cast<std::size_t>(nseg));
+        Check(pk_system_segment_stats(scene->sys, nseg, it.data(), conv.data(), res.data(), fl.data()),
+              "segment_stats");
+        iterations = it[static_cast<std::size_t>(e.second)];
+        converged = conv[static_cast<std::size_t>(e.second)] != 0;
+        residualNorm = static_cast<float>(res[static_cast<std::size_t>(e.second)]);
+        flags = fl[static_cast<std::size_t>(e.second)];
+        return true;
+    }
+    return false;
+}
+
 int World::PrepareScene(bool upload)
 {
     CollectContributions(0.0f);
@@ -846,6 +914,15 @@ void World::RunSubstep(float dt)
     p.linear = 0;
     p.explicit_mode = solverMode == SolverMode::Explicit ? 1 : 0;
     p.integrate = 1;
+    const bool batch = batchedSolve && scene->segmentsCover && scene->segStart.size() > 2;
+    if (batch != scene->batchedOnDevice) {
+        if (batch)
+            Check(pk_system_set_segments(scene->sys, static_cast<int>(scene->segStart.size()) - 1,
+                                         scene->segStart.data()),
+                  "set_segments");
+        Check(pk_system_set_batched(scene->sys, batch ? 1 : 0), "set_batched");
+        scene->batchedOnDevice = batch;
+    }
     Check(pk_system_step(scene->sys, &p), "pk_system_step");
     hostStale = true;
     if (solverMode == SolverMode::ImplicitEuler) statsPending = true;

@@ -267,5 +267,108 @@ __device__ __forceinline__ int grid_or(const int* part, int stride, int* sh)
     return r;
 }
 
+// ------------------------------------------------------------------ block reduction
+// Sum of N values and OR of one int over the block, in a fixed tree; valid in every
+// thread.  `sh` holds (N+1)*32 values of Acc, `shi` 32 ints.
+template <class Acc, int N>
+__device__ __forceinline__ void block_sum_or(Acc (&v)[N], int& bad, Acc* sh, int* shi)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], off);
+    bad = (int)__reduce_or_sync(0xffffffffu, (unsigned)bad);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) sh[k * 32 + warp] = v[k];
+        shi[warp] = bad;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            Acc t = lane < nw ? sh[k * 32 + lane] : Acc(0);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+            v[k] = t;
+        }
+        int b = lane < nw ? shi[lane] : 0;
+        b = (int)__reduce_or_sync(0xffffffffu, (unsigned)b);
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < N; ++k) sh[N * 32 + k] = v[k];
+            shi[0] = b;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = sh[N * 32 + k];
+    bad = shi[0];
+    __syncthreads();
+}
+
+// Group exchange among the `members` blocks whose slots are slots[0 .. members) of each of
+// the two generation buffers (buffer b at slots + b * stride): publishes this block's
+// (number `me`) sums of v (N <= 2) and OR of bad, waits for every member's slot of
+// generation `gen`, and returns the group-wide sums / OR, reduced in one fixed tree so
+// every member gets identical values.  False when a wait gave up or a block reported a
+// failure.  A group of one block is a block reduction.
+template <class Acc, int N>
+__device__ bool group_exchange(ExSlot* slots, int stride, int members, int me, GridSync* sync, unsigned gen,
+                               Acc (&v)[N], int& bad, Acc* sh, int* shi)
+{
+    static_assert(N >= 1 && N <= 2, "two partials per slot");
+    block_sum_or<Acc, N>(v, bad, sh, shi);
+    if (members <= 1) return !*(volatile int*)&sync->err;
+    const int G = members, tid = threadIdx.x;
+    ExSlot* buf = slots + (gen & 1u) * (unsigned)stride;
+    if (tid == 0) {
+        ExSlot* my = buf + me;
+        my->v0 = double(v[0]);
+        my->v1 = N > 1 ? double(v[N - 1]) : 0.0;
+        my->bad = bad;
+        __threadfence();
+        st_release(&my->gen, gen);
+    }
+    Acc pv[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) pv[k] = Acc(0);
+    int pb = 0, fail = 0;
+    for (int i = tid; i < G; i += blockDim.x) {
+        const ExSlot* sl = buf + i;
+        unsigned long long spins = 0;
+        while (ld_acquire(&sl->gen) != gen) {
+            if (++spins > kBarrierSpinLimit) {
+                atomicExch(&sync->err, 1);
+                fail = 1;
+                break;
+            }
+            if ((spins & 1023u) == 0 && *(volatile int*)&sync->err) {
+                fail = 1;
+                break;
+            }
+        }
+        if (fail) break;
+        pv[0] += Acc(__ldcg(&sl->v0));
+        if (N > 1) pv[N - 1] += Acc(__ldcg(&sl->v1));
+        pb |= __ldcg(&sl->bad);
+    }
+    pb |= fail << 30;
+    block_sum_or<Acc, N>(pv, pb, sh, shi);
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = pv[k];
+    bad = pb & ~(1 << 30);
+    return !(pb & (1 << 30)) && !*(volatile int*)&sync->err;
+}
+
+// The whole grid as one group (slots: two buffers of gridDim.x).
+template <class Acc, int N>
+__device__ __forceinline__ bool grid_exchange(ExSlot* slots, GridSync* sync, unsigned gen, Acc (&v)[N], int& bad,
+                                              Acc* sh, int* shi)
+{
+    return group_exchange<Acc, N>(slots, (int)gridDim.x, (int)gridDim.x, (int)blockIdx.x, sync, gen, v, bad, sh, shi);
+}
+
 }  // namespace
 }  // namespace pk

@@ -40,7 +40,7 @@ struct DevStats {
     unsigned flags;
     int polar_fp64_count;
     int polar_identity_count;
-    int pad;
+    unsigned batch_missing;  // batched solve: success flags some body lacks
 };
 
 // Upper-stored symmetric BSR plus its transpose index: for row r, the blocks (c, r)
@@ -224,6 +224,47 @@ struct RingPcgArgs {
     DevStats* stats;
 };
 
+// ------------------------------------------------------------------ batched PCG
+// Batched per-body solve (pk_pcg_batch.cu).  parts: 8 ints per block {body, first row,
+// end row, index in the body's group, first block of the group, group size, 0, 0}.
+constexpr int kBatchThreads = 256;
+
+struct BatchBodyStats {
+    int iterations;
+    int converged;
+    double residual_norm;
+    unsigned flags;
+    int pad;
+};
+
+template <class Real, class Acc>
+struct BatchPcgArgs {
+    BsrView<Real> a;
+    int nnz;
+    const int* parts;
+    const Real* b;
+    const Real* minv;
+    Real* x;
+    Real* r;
+    Real* sd0;
+    Real* sd1;
+    Real* q4;
+    ExSlot* slots;   // [2][grid]
+    GridSync* sync;  // err flag
+    int max_iterations;
+    Acc tolerance;
+    int skip_on_flags;
+    int integrate;
+    Real dt;
+    const int* dyn_to_node;
+    Real* node_x;
+    Real* node_v;
+    unsigned* flags;
+    unsigned* missing;
+    DevStats* stats;
+    BatchBodyStats* body_stats;
+};
+
 // Launchers (pk_kernels.cu).  All asynchronous on `stream`.
 template <class Real>
 cudaError_t launch_tet_kernel(const AssemblyArgs<Real>& args, bool fp64_polar_fallback, cudaStream_t stream);
@@ -236,6 +277,11 @@ template <class Real, class Acc>
 int pcg_max_grid(int threads, bool staged);
 template <class Real>
 cudaError_t launch_spmv_kernel(const BsrView<Real>& a, const Real* x, Real* y, cudaStream_t stream);
+// Batched per-body PCG (pk_pcg_batch.cu): cooperative, one block per body part.
+template <class Real, class Acc>
+cudaError_t launch_pcg_batch_kernel(const BatchPcgArgs<Real, Acc>& args, int grid, cudaStream_t stream);
+template <class Real, class Acc>
+int pcg_batch_max_grid();
 // Ring-staged PCG (pk_pcg_ring.cu): one block of kRingThreads per SM.
 template <class Real, class Acc>
 cudaError_t launch_pcg_ring_kernel(const RingPcgArgs<Real, Acc>& args, int grid, cudaStream_t stream);

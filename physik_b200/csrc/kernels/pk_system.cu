@@ -206,6 +206,12 @@ struct pk_system {
     int ring_tiles = 0;           // ring-staged PCG tiles (0: not used)
     int ring_max_grid = 0;
     DevBuf ring_desc, q4, slots;
+    // batched per-body solve
+    bool batched = false;
+    std::vector<int> seg_start;   // body row ranges: [seg_start[b], seg_start[b+1])
+    int batch_parts = 0;
+    int batch_max_grid = 0;
+    DevBuf batch_parts_buf, body_stats;
     // nodes
     DevBuf x, v, mass, node_to_dyn;
     // tets
@@ -421,9 +427,106 @@ int run_pcg_ring(pk_system* s, const pk_step_params& p, int skip_on_flags)
     return PK_OK;
 }
 
+template <class T>
+int upload_raw(DevBuf& buf, const T* src, size_t n, cudaStream_t stream);
+
+// Cuts every body (segment) into parts of about equal row count, one block each, so that
+// all parts fit one cooperative wave.  parts: 8 ints per block (see pk::BatchPcgArgs).
+int build_batch_parts(const std::vector<int>& seg, int capacity, std::vector<int>& parts)
+{
+    parts.clear();
+    const int nseg = static_cast<int>(seg.size()) - 1;
+    if (nseg <= 0 || capacity <= 0) return 0;
+    const long long total = seg[nseg] - seg[0];
+    long long rows_per_part = std::max<long long>(64, (total + capacity - 1) / capacity);
+    auto count = [&](long long R) {
+        long long c = 0;
+        for (int b = 0; b < nseg; ++b) {
+            const long long rows = seg[b + 1] - seg[b];
+            if (rows > 0) c += (rows + R - 1) / R;
+        }
+        return c;
+    };
+    while (count(rows_per_part) > capacity) rows_per_part += std::max<long long>(1, rows_per_part / 8);
+    for (int b = 0; b < nseg; ++b) {
+        const int rows = seg[b + 1] - seg[b];
+        if (rows <= 0) continue;
+        const int np = static_cast<int>((rows + rows_per_part - 1) / rows_per_part);
+        const int g0 = static_cast<int>(parts.size() / 8);
+        for (int i = 0; i < np; ++i) {
+            const int a = seg[b] + static_cast<int>(static_cast<long long>(rows) * i / np);
+            const int e = seg[b] + static_cast<int>(static_cast<long long>(rows) * (i + 1) / np);
+            parts.insert(parts.end(), {b, a, e, i, g0, np, 0, 0});
+        }
+    }
+    return static_cast<int>(parts.size() / 8);
+}
+
+template <class Real, class Acc>
+int run_pcg_batch(pk_system* s, const pk_step_params& p, int skip_on_flags)
+{
+    if (!s->batch_max_grid) s->batch_max_grid = pk::pcg_batch_max_grid<Real, Acc>();
+    if (s->batch_parts <= 0) {
+        std::vector<int> parts;
+        const int np = build_batch_parts(s->seg_start, s->batch_max_grid, parts);
+        if (np <= 0) return fail(PK_ERR_CUDA, "batched PCG: no resident blocks");
+        int rc = upload_raw<int>(s->batch_parts_buf, parts.data(), parts.size(), s->stream);
+        if (rc) return rc;
+        s->batch_parts = np;
+    }
+    const int grid = s->batch_parts;
+    const int nseg = static_cast<int>(s->seg_start.size()) - 1;
+    int rc = ensure_solver_buffers(s, 1);
+    if (rc) return rc;
+    const size_t rs = s->rsize();
+    PK_CHECK(s->q4.ensure(4 * rs * static_cast<size_t>(std::max(1, s->dyn_count))));
+    PK_CHECK(s->slots.ensure(2 * sizeof(pk::ExSlot) * static_cast<size_t>(grid)));
+    PK_CHECK(s->body_stats.ensure(sizeof(pk::BatchBodyStats) * static_cast<size_t>(std::max(1, nseg))));
+    PK_CHECK(cudaMemsetAsync(s->slots.p, 0, 2 * sizeof(pk::ExSlot) * static_cast<size_t>(grid), s->stream));
+    PK_CHECK(cudaMemsetAsync(s->body_stats.p, 0, sizeof(pk::BatchBodyStats) * static_cast<size_t>(std::max(1, nseg)),
+                             s->stream));
+    PK_CHECK(cudaMemsetAsync(s->sync.p, 0, sizeof(pk::GridSync), s->stream));
+    pk::BatchPcgArgs<Real, Acc> a{};
+    a.a.n = s->dyn_count;
+    a.a.row_start = s->row_start.as<int>();
+    a.a.col = s->col.as<int>();
+    a.a.values = s->values.as<Real>();
+    a.a.lt_start = s->lt_start.as<int>();
+    a.a.lt_row = s->lt_row.as<int>();
+    a.a.lt_block = s->lt_block.as<int>();
+    a.nnz = s->nnz;
+    a.parts = s->batch_parts_buf.as<int>();
+    a.b = s->rhs.as<Real>();
+    a.minv = s->minv.as<Real>();
+    a.x = s->px.as<Real>();
+    a.r = s->pr.as<Real>();
+    a.sd0 = s->psd0.as<Real>();
+    a.sd1 = s->psd1.as<Real>();
+    a.q4 = s->q4.as<Real>();
+    a.slots = s->slots.as<pk::ExSlot>();
+    a.sync = s->sync.as<pk::GridSync>();
+    a.max_iterations = p.max_iterations;
+    a.tolerance = static_cast<Acc>(static_cast<Real>(p.tolerance));
+    a.skip_on_flags = skip_on_flags;
+    a.integrate = p.integrate;
+    a.dt = static_cast<Real>(p.dt);
+    a.dyn_to_node = s->dyn_to_node.as<int>();
+    a.node_x = s->x.as<Real>();
+    a.node_v = s->v.as<Real>();
+    pk::DevStats* st = s->stats.as<pk::DevStats>();
+    a.flags = &st->flags;
+    a.missing = &st->batch_missing;
+    a.stats = st;
+    a.body_stats = s->body_stats.as<pk::BatchBodyStats>();
+    PK_CHECK(pk::launch_pcg_batch_kernel<Real, Acc>(a, grid, s->stream));
+    s->launches += 1;
+    return PK_OK;
+}
+
 template <class Real, class Acc>
 int run_pcg(pk_system* s, const pk_step_params& p, int skip_on_flags)
 {
+    if (s->batched && s->seg_start.size() >= 2) return run_pcg_batch<Real, Acc>(s, p, skip_on_flags);
     if (s->ring_tiles > 0) {
         int rc = ensure_solver_buffers(s, 1);
         if (rc) return rc;
@@ -737,6 +840,8 @@ PKCUDA_API int pk_system_set_pattern(pk_system* s, int dyn_count, const int* dyn
          : s->precision == PK_PREC_MIXED ? ensure_solver_buffers(s, max_grid_for<float, double>(s))
                                          : ensure_solver_buffers(s, max_grid_for<double, double>(s));
     if (rc) return rc;
+    s->seg_start.clear();
+    s->batch_parts = 0;
     // Ring-staged PCG tiles (the default kernel).
     s->ring_tiles = 0;
     if (requested_kernel() == 0 && dyn_count > 0 && diag_first) {
@@ -792,6 +897,12 @@ PKCUDA_API int pk_system_stats(pk_system* s, pk_step_stats* out)
     out->flags = d.flags;
     out->polar_fp64_count = d.polar_fp64_count;
     out->polar_identity_count = d.polar_identity_count;
+    if (s->batched && s->seg_start.size() >= 2 && !(d.flags & (PK_FLAG_PRECOMPUTE_FAILED | PK_FLAG_SINGULAR_DIAG))) {
+        // Success flags hold only when every body has them.
+        const unsigned success = PK_FLAG_SOLVED | PK_FLAG_INTEGRATED | PK_FLAG_CONVERGED;
+        out->flags = (d.flags & ~success) | (success & ~d.batch_missing);
+        out->converged = (d.batch_missing & PK_FLAG_CONVERGED) ? 0 : 1;
+    }
     if (d.flags & PK_FLAG_BARRIER_TIMEOUT) return fail(PK_ERR_TIMEOUT, "grid barrier timed out");
     return PK_OK;
 }
@@ -881,6 +992,60 @@ PKCUDA_API int pk_system_set_pcg_grid(pk_system* s, int grid)
     if (s->precision == PK_PREC_FP32) return pcg_grid_for<float, float>(s);
     if (s->precision == PK_PREC_MIXED) return pcg_grid_for<float, double>(s);
     return pcg_grid_for<double, double>(s);
+}
+
+PKCUDA_API int pk_system_set_segments(pk_system* s, int segment_count, const int* segment_row_start)
+{
+    if (!s || segment_count < 0 || (segment_count > 0 && !segment_row_start)) return fail(PK_ERR_ARG, "segments");
+    if (!s->have_pattern) return fail(PK_ERR_STATE, "set_segments before set_pattern");
+    if (segment_count > 0) {
+        if (segment_row_start[0] != 0 || segment_row_start[segment_count] != s->dyn_count)
+            return fail(PK_ERR_ARG, "segments must cover the dynamic rows");
+        for (int b = 0; b < segment_count; ++b)
+            if (segment_row_start[b + 1] < segment_row_start[b]) return fail(PK_ERR_ARG, "segments not monotone");
+        // A body's rows must not reference another body's rows (independent systems).
+        std::vector<int> seg_of(static_cast<size_t>(s->dyn_count));
+        for (int b = 0; b < segment_count; ++b)
+            for (int r = segment_row_start[b]; r < segment_row_start[b + 1]; ++r) seg_of[r] = b;
+        std::vector<int> rs(static_cast<size_t>(s->dyn_count) + 1), col(static_cast<size_t>(s->nnz));
+        PK_CHECK(cudaSetDevice(s->device));
+        PK_CHECK(cudaMemcpy(rs.data(), s->row_start.p, rs.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        PK_CHECK(cudaMemcpy(col.data(), s->col.p, col.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        for (int r = 0; r < s->dyn_count; ++r)
+            for (int k = rs[r]; k < rs[r + 1]; ++k)
+                if (seg_of[col[k]] != seg_of[r]) return fail(PK_ERR_ARG, "a block couples two segments");
+    }
+    s->seg_start.assign(segment_row_start, segment_row_start + (segment_count > 0 ? segment_count + 1 : 0));
+    s->batch_parts = 0;
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_set_batched(pk_system* s, int on)
+{
+    if (!s) return fail(PK_ERR_ARG, "batched");
+    s->batched = on != 0;
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_segment_stats(pk_system* s, int segment_count, int* iterations, int* converged,
+                                       double* residual_norm, unsigned* flags)
+{
+    if (!s || segment_count < 0) return fail(PK_ERR_ARG, "segment_stats");
+    const int nseg = static_cast<int>(s->seg_start.size()) - 1;
+    if (!s->batched || nseg <= 0) return fail(PK_ERR_STATE, "no batched solve");
+    if (segment_count != nseg) return fail(PK_ERR_ARG, "segment count mismatch");
+    PK_CHECK(cudaSetDevice(s->device));
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    std::vector<pk::BatchBodyStats> bs(static_cast<size_t>(nseg));
+    if (s->body_stats.p)
+        PK_CHECK(cudaMemcpy(bs.data(), s->body_stats.p, bs.size() * sizeof(pk::BatchBodyStats), cudaMemcpyDeviceToHost));
+    for (int b = 0; b < nseg; ++b) {
+        if (iterations) iterations[b] = bs[b].iterations;
+        if (converged) converged[b] = bs[b].converged;
+        if (residual_norm) residual_norm[b] = bs[b].residual_norm;
+        if (flags) flags[b] = bs[b].flags;
+    }
+    return PK_OK;
 }
 
 PKCUDA_API int pk_bsr_transpose_index(int n, const int* row_start, const int* col_index, int* lt_start, int* lt_row,

@@ -95,6 +95,16 @@ class SimWorld:
         if fn(self.h, _ptr(x), _ptr(v), self.node_count) < 0:
             raise PhysikError("SetNodeStates failed: " + self.error())
 
+    def set_batched(self, on: bool = True):
+        self.X.PHYSIK_B200_SetBatchedSolve(self.h, 1 if on else 0)
+
+    def body_stats(self, i: int):
+        it, conv, res, fl = C.c_int(), C.c_int(), C.c_float(), C.c_uint()
+        if self.X.PHYSIK_B200_GetBodyConjugateGradientStats(self.h, self.components[i], C.byref(it), C.byref(conv),
+                                                           C.byref(res), C.byref(fl)) != 0:
+            raise PhysikError("no batched statistics: " + self.error())
+        return dict(iterations=it.value, converged=conv.value, residual=res.value, flags=fl.value)
+
     def cg_stats(self):
         X, h = self.X, self.h
         return dict(iterations=X.PHYSIK_GetLastConjugateGradientIterations(h),

@@ -59,8 +59,6 @@ def _check(rs, col, precision, seed=0):
     return tiles.value, max_span.value
 
 
-L.PK.pk_ring_tiling_selfcheck.restype = C.c_int
-L.PK.pk_ring_tiling_selfcheck.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 5 + [C.c_void_p, C.c_void_p]
 
 
 @pytest.mark.parametrize("precision", [L.PK_PREC_MIXED, L.PK_PREC_FP64])
