@@ -176,6 +176,13 @@ PHYSIK_B200_API int PHYSIK_B200_EnableTiming(PhysikWorldHandle world, int on);
 PHYSIK_B200_API int PHYSIK_B200_GetTimings(PhysikWorldHandle world, double* assembleMs, double* solveMs, int* steps,
                                            long long* kernelLaunches);
 PHYSIK_B200_API int PHYSIK_B200_SetPcgGrid(PhysikWorldHandle world, int grid);
+/* Captures the device step in a CUDA graph and replays it (see pk_system_set_graph). */
+PHYSIK_B200_API void PHYSIK_B200_SetGraphCapture(PhysikWorldHandle world, int on);
+/* Picks the fastest PCG kernel and tile (or, batched, part) size for the world's scene by
+ * timing `repeats` solves of the last assembled system; call after a step.  Returns the
+ * chosen candidate (see pk_system_autotune) or -1; bestSolveMs (may be NULL) receives its
+ * mean solve time. */
+PHYSIK_B200_API int PHYSIK_B200_Autotune(PhysikWorldHandle world, int repeats, double* bestSolveMs);
 /* Batched solve: one PCG per tet-mesh physics component (own scalars, stopping test,
  * iteration count and all-or-nothing integration, as a world holding only that body),
  * all bodies in one launch, instead of the reference's single coupled PCG over the whole

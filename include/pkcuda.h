@@ -162,6 +162,19 @@ PKCUDA_API int pk_system_timings(pk_system* sys, double* assemble_ms, double* so
 /* Grid size of the cooperative PCG launch (0 = automatic).  Returns the grid used next. */
 PKCUDA_API int pk_system_set_pcg_grid(pk_system* sys, int grid);
 
+/* Captures each step into a CUDA graph (relaxed capture mode) and replays it: the first
+ * step after enabling runs normally (allocations, uploads), the next one with the same
+ * parameters is captured, later ones launch the graph.  Any topology, segment, grid or
+ * parameter change drops the graph.  With timing on, a graph step counts as solve time. */
+PKCUDA_API int pk_system_set_graph(pk_system* sys, int on);
+/* Autotuner: times `repeats` solves (without integration) of the last assembled system
+ * for each candidate and keeps the fastest -- unbatched: the ring-staged kernel, the
+ * TMA-staged kernel with 16 / 32 / 64-row tiles, the unstaged kernel; batched: the
+ * smallest part (32 .. 1024 rows) a body is cut into.  Needs one step first.  Reports the
+ * candidate index and its mean solve time.  Candidates differ only in summation order. */
+PKCUDA_API int pk_system_autotune(pk_system* sys, const pk_step_params* params, int repeats, int* chosen,
+                                  double* best_ms);
+
 /* Standalone kernels on host arrays (values column-major, 9 per block). */
 PKCUDA_API int pk_bsr_multiply(int device, int precision, int n, const int* row_start, const int* col_index,
                                const double* values, const double* x, double* y);

@@ -571,6 +571,19 @@ PHYSIK_B200_API int PHYSIK_B200_GetBodyConjugateGradientStats(PhysikWorldHandle 
         -1);
 }
 
+PHYSIK_B200_API void PHYSIK_B200_SetGraphCapture(PhysikWorldHandle world, int on)
+{
+    World* w = AsWorld(world);
+    if (w) w->SetGraphCapture(on != 0);
+}
+
+PHYSIK_B200_API int PHYSIK_B200_Autotune(PhysikWorldHandle world, int repeats, double* bestSolveMs)
+{
+    World* w = AsWorld(world);
+    if (!w) return -1;
+    return Guard([&] { return w->Autotune(repeats, bestSolveMs); }, -1);
+}
+
 PHYSIK_B200_API int PHYSIK_B200_SetPcgGrid(PhysikWorldHandle world, int grid)
 {
     World* w = AsWorld(world);

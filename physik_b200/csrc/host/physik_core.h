@@ -389,6 +389,13 @@ public:
     bool GetBodyConjugateGradientStats(const Component* body, int& iterations, bool& converged, float& residualNorm,
                                        unsigned& flags) const;
 
+    // CUDA-graph capture of the device step (extension).
+    void SetGraphCapture(bool on) { graphCapture = on; }
+    // Autotuner (extension): picks the fastest PCG kernel / tile or part size for the
+    // current scene by timing `repeats` solves of the last assembled system (call after a
+    // step).  Returns the chosen candidate index (see pk_system_autotune) or -1.
+    int Autotune(int repeats, double* bestMs);
+
     // Device precision (extension).  Changing it rebuilds the device scene.
     void SetPrecision(Precision p);
     Precision GetPrecision() const { return precision; }
@@ -455,6 +462,8 @@ private:
     Precision precision = Precision::FP32;
     int device = 0;
     bool batchedSolve = false;
+    bool graphCapture = false;
+    float lastSubstepDt = 0.0f;
     std::uint64_t topologyVersion = 1;
 
     SolverData solverData;

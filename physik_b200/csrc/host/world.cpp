@@ -350,6 +350,7 @@ struct DeviceScene {
     std::vector<std::pair<const Component*, int>> bodySegment;
     bool segmentsCover = false;
     bool batchedOnDevice = false;
+    bool graphOnDevice = false;
     std::vector<unsigned char> enabled;
     std::vector<double> mass, dmInv, volume, lam, mu, damp;
 
@@ -531,6 +532,7 @@ void UploadScene(DeviceScene& sc, const std::vector<Vec3>& positions, const std:
                                 sc.incStart.data(), sc.incList.data()),
           "set_pattern");
     sc.batchedOnDevice = false;
+    sc.graphOnDevice = false;
     sc.uploaded = true;
 }
 
@@ -846,6 +848,26 @@ void World::EnsureScene(bool upload)
 
 void World::SetBatchedSolve(bool on) { batchedSolve = on; }
 
+int World::Autotune(int repeats, double* bestMs)
+{
+    SyncStats();
+    if (!scene || !scene->uploaded || solverMode != SolverMode::ImplicitEuler || scene->dynCount == 0) return -1;
+    pk_step_params p{};
+    p.dt = lastSubstepDt > 0.0f ? lastSubstepDt : 1.0f / 60.0f;
+    p.gravity[0] = gravity.x;
+    p.gravity[1] = gravity.y;
+    p.gravity[2] = gravity.z;
+    p.max_iterations = conjugateGradientSettings.maxIterations;
+    p.tolerance = conjugateGradientSettings.tolerance;
+    p.use_jacobi = conjugateGradientSettings.useJacobiPreconditioner ? 1 : 0;
+    p.integrate = 0;
+    int chosen = -1;
+    double ms = 0.0;
+    Check(pk_system_autotune(scene->sys, &p, repeats, &chosen, &ms), "autotune");
+    if (bestMs) *bestMs = ms;
+    return chosen;
+}
+
 bool World::GetBodyConjugateGradientStats(const Component* body, int& iterations, bool& converged,
                                           float& residualNorm, unsigned& flags) const
 {
@@ -923,6 +945,11 @@ void World::RunSubstep(float dt)
         Check(pk_system_set_batched(scene->sys, batch ? 1 : 0), "set_batched");
         scene->batchedOnDevice = batch;
     }
+    if (graphCapture != scene->graphOnDevice) {
+        Check(pk_system_set_graph(scene->sys, graphCapture ? 1 : 0), "set_graph");
+        scene->graphOnDevice = graphCapture;
+    }
+    lastSubstepDt = dt;
     Check(pk_system_step(scene->sys, &p), "pk_system_step");
     hostStale = true;
     if (solverMode == SolverMode::ImplicitEuler) statsPending = true;

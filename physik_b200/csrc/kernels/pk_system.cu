@@ -211,7 +211,18 @@ struct pk_system {
     std::vector<int> seg_start;   // body row ranges: [seg_start[b], seg_start[b+1])
     int batch_parts = 0;
     int batch_max_grid = 0;
+    int batch_min_rows = 64;      // smallest part a body is cut into (autotuned)
     DevBuf batch_parts_buf, body_stats;
+    // kernel selection: -1 automatic (ring, else staged, else plain), 0 ring, 1 staged, 2 plain
+    int kernel_choice = -1;
+    int staged_rows = 0;          // rows per staged tile (0: chosen from the grid)
+    std::vector<int> h_row_start, h_lts;  // host copies for re-tiling
+    bool assembled = false;       // a step has assembled the system at least once
+    // CUDA graph of one step
+    bool use_graph = false;
+    cudaGraphExec_t graph_exec = nullptr;
+    pk_step_params graph_params{};
+    int graph_kernels = 0;
     // nodes
     DevBuf x, v, mass, node_to_dyn;
     // tets
@@ -432,13 +443,13 @@ int upload_raw(DevBuf& buf, const T* src, size_t n, cudaStream_t stream);
 
 // Cuts every body (segment) into parts of about equal row count, one block each, so that
 // all parts fit one cooperative wave.  parts: 8 ints per block (see pk::BatchPcgArgs).
-int build_batch_parts(const std::vector<int>& seg, int capacity, std::vector<int>& parts)
+int build_batch_parts(const std::vector<int>& seg, int capacity, int min_rows, std::vector<int>& parts)
 {
     parts.clear();
     const int nseg = static_cast<int>(seg.size()) - 1;
     if (nseg <= 0 || capacity <= 0) return 0;
     const long long total = seg[nseg] - seg[0];
-    long long rows_per_part = std::max<long long>(64, (total + capacity - 1) / capacity);
+    long long rows_per_part = std::max<long long>(std::max(1, min_rows), (total + capacity - 1) / capacity);
     auto count = [&](long long R) {
         long long c = 0;
         for (int b = 0; b < nseg; ++b) {
@@ -468,7 +479,7 @@ int run_pcg_batch(pk_system* s, const pk_step_params& p, int skip_on_flags)
     if (!s->batch_max_grid) s->batch_max_grid = pk::pcg_batch_max_grid<Real, Acc>();
     if (s->batch_parts <= 0) {
         std::vector<int> parts;
-        const int np = build_batch_parts(s->seg_start, s->batch_max_grid, parts);
+        const int np = build_batch_parts(s->seg_start, s->batch_max_grid, s->batch_min_rows, parts);
         if (np <= 0) return fail(PK_ERR_CUDA, "batched PCG: no resident blocks");
         int rc = upload_raw<int>(s->batch_parts_buf, parts.data(), parts.size(), s->stream);
         if (rc) return rc;
@@ -527,17 +538,23 @@ template <class Real, class Acc>
 int run_pcg(pk_system* s, const pk_step_params& p, int skip_on_flags)
 {
     if (s->batched && s->seg_start.size() >= 2) return run_pcg_batch<Real, Acc>(s, p, skip_on_flags);
-    if (s->ring_tiles > 0) {
+    const int kernel = s->kernel_choice >= 0 ? s->kernel_choice : (s->ring_tiles > 0 ? 0 : (s->ntiles > 0 ? 1 : 2));
+    if (kernel == 0 && s->ring_tiles > 0) {
         int rc = ensure_solver_buffers(s, 1);
         if (rc) return rc;
         return run_pcg_ring<Real, Acc>(s, p, skip_on_flags);
     }
+    // Staged (TMA tiles) or plain (unstaged) kernel.
+    const int saved_tiles = s->ntiles;
+    if (kernel == 2) s->ntiles = 0;
     const int grid = pcg_grid_for<Real, Acc>(s);
+    s->ntiles = saved_tiles;
     if (grid <= 0) return fail(PK_ERR_CUDA, "cooperative PCG kernel cannot be resident");
     int rc = ensure_solver_buffers(s, max_grid_for<Real, Acc>(s));
     if (rc) return rc;
     PK_CHECK(cudaMemsetAsync(s->sync.p, 0, sizeof(pk::GridSync), s->stream));
     pk::PcgArgs<Real, Acc> a = pcg_args<Real, Acc>(s, p, skip_on_flags);
+    if (kernel == 2) a.ntiles = 0;
     PK_CHECK(pk::launch_pcg_kernel<Real, Acc>(a, grid, pk::kPcgThreads, s->stream));
     s->launches += 1;
     return PK_OK;
@@ -583,6 +600,71 @@ int run_step(pk_system* s, const pk_step_params& p)
         s->ev_pending.push_back({evi[0], evi[1], evi[2]});
     }
     PK_CHECK(cudaMemcpyAsync(s->host_stats, s->stats.p, sizeof(pk::DevStats), cudaMemcpyDeviceToHost, s->stream));
+    s->stats_pending = true;
+    if (!p.explicit_mode) s->assembled = true;
+    return PK_OK;
+}
+
+void drop_graph(pk_system* s)
+{
+    if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+    s->graph_exec = nullptr;
+}
+
+bool same_params(const pk_step_params& a, const pk_step_params& b)
+{
+    return a.dt == b.dt && a.gravity[0] == b.gravity[0] && a.gravity[1] == b.gravity[1] &&
+           a.gravity[2] == b.gravity[2] && a.max_iterations == b.max_iterations && a.tolerance == b.tolerance &&
+           a.use_jacobi == b.use_jacobi && a.linear == b.linear && a.explicit_mode == b.explicit_mode &&
+           a.integrate == b.integrate;
+}
+
+// One step as a CUDA graph: captured (relaxed mode) on the first step with these
+// parameters after a plain step has made every allocation and upload, replayed after.
+template <class Real>
+int run_step_graph(pk_system* s, const pk_step_params& p)
+{
+    if (!s->graph_exec || !same_params(p, s->graph_params)) {
+        drop_graph(s);
+        const bool timing = s->timing;
+        const long long launches = s->launches;
+        s->timing = false;
+        PK_CHECK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeRelaxed));
+        const int rc = run_step<Real>(s, p);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(s->stream, &graph);
+        s->timing = timing;
+        s->graph_kernels = static_cast<int>(s->launches - launches);
+        s->launches = launches;
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (ec != cudaSuccess) return cuda_fail(ec, "cudaStreamEndCapture");
+        const cudaError_t ei = cudaGraphInstantiate(&s->graph_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ei != cudaSuccess) {
+            s->graph_exec = nullptr;
+            return cuda_fail(ei, "cudaGraphInstantiate");
+        }
+        s->graph_params = p;
+    }
+    int evi[2] = {-1, -1};
+    if (s->timing) {
+        for (int i = 0; i < 2; ++i) {
+            cudaEvent_t e;
+            PK_CHECK(cudaEventCreate(&e));
+            s->ev_pool.push_back(e);
+            evi[i] = static_cast<int>(s->ev_pool.size()) - 1;
+        }
+        PK_CHECK(cudaEventRecord(s->ev_pool[evi[0]], s->stream));
+    }
+    PK_CHECK(cudaGraphLaunch(s->graph_exec, s->stream));
+    if (s->timing) {
+        PK_CHECK(cudaEventRecord(s->ev_pool[evi[1]], s->stream));
+        s->ev_pending.push_back({evi[0], evi[0], evi[1]});  // the whole step counts as solve time
+    }
+    s->launches += s->graph_kernels;
     s->stats_pending = true;
     return PK_OK;
 }
@@ -677,6 +759,7 @@ PKCUDA_API int pk_system_destroy(pk_system* s)
     if (!s) return PK_OK;
     cudaSetDevice(s->device);
     cudaStreamSynchronize(s->stream);
+    drop_graph(s);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
     if (s->host_stats) cudaFreeHost(s->host_stats);
     cudaStreamDestroy(s->stream);
@@ -688,6 +771,7 @@ PKCUDA_API void* pk_system_stream(pk_system* s) { return s ? static_cast<void*>(
 
 PKCUDA_API int pk_system_set_nodes(pk_system* s, int node_count, const int* node_to_dyn, const double* mass)
 {
+    if (s) drop_graph(s);
     if (!s || node_count < 0 || (node_count > 0 && (!node_to_dyn || !mass))) return fail(PK_ERR_ARG, "set_nodes");
     PK_CHECK(cudaSetDevice(s->device));
     s->node_count = node_count;
@@ -765,6 +849,7 @@ PKCUDA_API int pk_system_set_tets(pk_system* s, int tet_count, const int* tet_no
                                   const double* dm_inv, const double* volume, const double* lambda, const double* mu,
                                   const double* damping)
 {
+    if (s) drop_graph(s);
     if (!s || tet_count < 0) return fail(PK_ERR_ARG, "set_tets");
     if (tet_count > 0 && (!tet_nodes || !enabled || !dm_inv || !volume || !lambda || !mu || !damping))
         return fail(PK_ERR_ARG, "set_tets: NULL array");
@@ -842,6 +927,10 @@ PKCUDA_API int pk_system_set_pattern(pk_system* s, int dyn_count, const int* dyn
     if (rc) return rc;
     s->seg_start.clear();
     s->batch_parts = 0;
+    s->assembled = false;
+    drop_graph(s);
+    s->h_row_start.assign(row_start, row_start + dyn_count + 1);
+    s->h_lts = lts;
     // Ring-staged PCG tiles (the default kernel).
     s->ring_tiles = 0;
     if (requested_kernel() == 0 && dyn_count > 0 && diag_first) {
@@ -862,7 +951,8 @@ PKCUDA_API int pk_system_set_pattern(pk_system* s, int dyn_count, const int* dyn
     s->ntiles = 0;
     if (requested_kernel() != 2 && staging_enabled() && dyn_count > 0 && s->pcg_max_grid_staged > 0) {
         const int per_block = (dyn_count + s->pcg_max_grid_staged - 1) / s->pcg_max_grid_staged;
-        const int rows = per_block <= 16 ? 16 : (per_block <= 32 ? 32 : pk::kTileRowsMax);
+        const int rows = s->staged_rows > 0 ? s->staged_rows
+                                            : (per_block <= 16 ? 16 : (per_block <= 32 ? 32 : pk::kTileRowsMax));
         std::vector<int> desc;
         if (build_tiles(dyn_count, row_start, lts, rows, desc)) {
             rc = upload_raw<int>(s->tiles, desc.data(), desc.size(), s->stream);
@@ -881,6 +971,8 @@ PKCUDA_API int pk_system_step(pk_system* s, const pk_step_params* p)
     if (!(p->dt > 0.0)) return fail(PK_ERR_ARG, "dt must be > 0");
     if (s->dyn_count > 0 && !s->diag_first) return fail(PK_ERR_ARG, "every dynamic row needs its diagonal block first");
     PK_CHECK(cudaSetDevice(s->device));
+    if (s->use_graph && s->assembled)
+        return s->precision == PK_PREC_FP64 ? run_step_graph<double>(s, *p) : run_step_graph<float>(s, *p);
     return s->precision == PK_PREC_FP64 ? run_step<double>(s, *p) : run_step<float>(s, *p);
 }
 
@@ -983,6 +1075,7 @@ PKCUDA_API int pk_system_set_pcg_grid(pk_system* s, int grid)
 {
     if (!s) return fail(PK_ERR_ARG, "pcg grid");
     PK_CHECK(cudaSetDevice(s->device));
+    drop_graph(s);
     s->pcg_grid_override = std::max(0, grid);
     if (s->ring_tiles > 0) {
         if (s->precision == PK_PREC_FP32) return ring_grid_for<float, float>(s);
@@ -1017,12 +1110,14 @@ PKCUDA_API int pk_system_set_segments(pk_system* s, int segment_count, const int
     }
     s->seg_start.assign(segment_row_start, segment_row_start + (segment_count > 0 ? segment_count + 1 : 0));
     s->batch_parts = 0;
+    drop_graph(s);
     return PK_OK;
 }
 
 PKCUDA_API int pk_system_set_batched(pk_system* s, int on)
 {
     if (!s) return fail(PK_ERR_ARG, "batched");
+    if (s->batched != (on != 0)) drop_graph(s);
     s->batched = on != 0;
     return PK_OK;
 }
@@ -1045,6 +1140,115 @@ PKCUDA_API int pk_system_segment_stats(pk_system* s, int segment_count, int* ite
         if (residual_norm) residual_norm[b] = bs[b].residual_norm;
         if (flags) flags[b] = bs[b].flags;
     }
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_set_graph(pk_system* s, int on)
+{
+    if (!s) return fail(PK_ERR_ARG, "graph");
+    PK_CHECK(cudaSetDevice(s->device));
+    if (!on) {
+        cudaStreamSynchronize(s->stream);
+        drop_graph(s);
+    }
+    s->use_graph = on != 0;
+    return PK_OK;
+}
+
+namespace {
+
+// Times `repeats` solves (no integration) of the assembled system with the current
+// kernel settings; mean milliseconds, or a negative PK_ERR_* code.
+double time_solves(pk_system* s, const pk_step_params& p, int repeats)
+{
+    pk_step_params q = p;
+    q.integrate = 0;
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return PK_ERR_CUDA;
+    int rc = PK_OK;
+    auto solve = [&] {
+        if (s->precision == PK_PREC_FP32) return run_pcg<float, float>(s, q, 0);
+        if (s->precision == PK_PREC_MIXED) return run_pcg<float, double>(s, q, 0);
+        return run_pcg<double, double>(s, q, 0);
+    };
+    rc = solve();  // warm-up (also builds batch parts)
+    if (!rc && cudaEventRecord(e0, s->stream) != cudaSuccess) rc = PK_ERR_CUDA;
+    for (int i = 0; i < repeats && !rc; ++i) rc = solve();
+    float ms = 0.0f;
+    if (!rc && (cudaEventRecord(e1, s->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+        rc = PK_ERR_CUDA;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc ? double(rc) : double(ms) / std::max(1, repeats);
+}
+
+}  // namespace
+
+PKCUDA_API int pk_system_autotune(pk_system* s, const pk_step_params* p, int repeats, int* chosen, double* best_ms)
+{
+    if (!s || !p) return fail(PK_ERR_ARG, "autotune");
+    if (!s->have_pattern || !s->assembled || s->dyn_count <= 0)
+        return fail(PK_ERR_STATE, "autotune needs an assembled system (step once first)");
+    PK_CHECK(cudaSetDevice(s->device));
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    drop_graph(s);
+    repeats = std::max(1, repeats);
+    int best = -1;
+    double best_t = 1e300;
+    if (s->batched && s->seg_start.size() >= 2) {
+        // Candidates: the smallest part a body is cut into.
+        const int cand[] = {32, 64, 128, 256, 512, 1024};
+        int i = 0;
+        for (int rows : cand) {
+            s->batch_min_rows = rows;
+            s->batch_parts = 0;
+            const double t = time_solves(s, *p, repeats);
+            if (t < 0) return static_cast<int>(t);
+            if (t < best_t) best_t = t, best = i;
+            ++i;
+        }
+        s->batch_min_rows = cand[best];
+        s->batch_parts = 0;
+    } else {
+        // Candidates: ring kernel; staged kernel with 16 / 32 / 64-row tiles; plain kernel.
+        struct Cand {
+            int kernel, rows;
+        };
+        const Cand cand[] = {{0, 0}, {1, 16}, {1, 32}, {1, pk::kTileRowsMax}, {2, 0}};
+        auto retile = [&](int rows) -> int {
+            std::vector<int> desc;
+            s->ntiles = 0;
+            if (!build_tiles(s->dyn_count, s->h_row_start.data(), s->h_lts, rows, desc)) return PK_OK;
+            int rc = upload_raw<int>(s->tiles, desc.data(), desc.size(), s->stream);
+            if (rc) return rc;
+            s->ntiles = static_cast<int>(desc.size() / 8);
+            return PK_OK;
+        };
+        int i = 0;
+        for (const Cand& c : cand) {
+            if (c.kernel == 0 && s->ring_tiles <= 0) { ++i; continue; }
+            if (c.kernel == 1) {
+                int rc = retile(c.rows);
+                if (rc) return rc;
+                if (s->ntiles <= 0) { ++i; continue; }
+            }
+            s->kernel_choice = c.kernel;
+            const double t = time_solves(s, *p, repeats);
+            if (t < 0) return static_cast<int>(t);
+            if (t < best_t) best_t = t, best = i;
+            ++i;
+        }
+        if (best < 0) return fail(PK_ERR_UNSUPPORTED, "no PCG kernel candidate");
+        s->kernel_choice = cand[best].kernel;
+        s->staged_rows = cand[best].rows;
+        if (cand[best].kernel == 1) {
+            int rc = retile(cand[best].rows);
+            if (rc) return rc;
+        }
+    }
+    if (chosen) *chosen = best;
+    if (best_ms) *best_ms = best_t;
     return PK_OK;
 }
 

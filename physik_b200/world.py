@@ -98,6 +98,16 @@ class SimWorld:
     def set_batched(self, on: bool = True):
         self.X.PHYSIK_B200_SetBatchedSolve(self.h, 1 if on else 0)
 
+    def set_graph(self, on: bool = True):
+        self.X.PHYSIK_B200_SetGraphCapture(self.h, 1 if on else 0)
+
+    def autotune(self, repeats: int = 3):
+        ms = C.c_double()
+        chosen = self.X.PHYSIK_B200_Autotune(self.h, repeats, C.byref(ms))
+        if chosen < 0:
+            raise PhysikError("autotune failed: " + self.error())
+        return chosen, ms.value
+
     def body_stats(self, i: int):
         it, conv, res, fl = C.c_int(), C.c_int(), C.c_float(), C.c_uint()
         if self.X.PHYSIK_B200_GetBodyConjugateGradientStats(self.h, self.components[i], C.byref(it), C.byref(conv),
