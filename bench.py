@@ -1,27 +1,35 @@
 """Benchmark of the implicit soft-body step (PhysiK's World::Step on the GPU).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload block128|beam64|cube8|beam32] [--precision mixed|fp32|fp64]
+                    [--workload block128|beam64|cube8|beam32|batched256] [--precision mixed|fp32|fp64]
 
 One JSON line on rank 0.  A "step" is one PHYSIK_Step (one implicit-Euler substep:
 per-tet corotated FEM, assembly of M + dt^2 K and its rhs, block-Jacobi PCG,
-integration) of the whole body.
+integration) of the whole workload.  The PCG kernel (and its tile or part size) is the
+one the library's autotuner picks for the scene after the first step.
 
 * value   -- steps/s with the state resident on the GPU, K steps timed with CUDA
              events on the world's stream (max over ranks).
 * e2e     -- the same steps through the C ABI with host buffers: every step uploads
              positions and velocities from pinned host memory (PHYSIK_B200_SetNodeStates),
              steps, and reads them back (PHYSIK_B200_GetNodeStates); wall clock.
-* roofline-- the cooperative PCG kernel: algorithmic bytes per launch
-             (iterations x (40U + 4(n+1) + 24n + 132n) in FP32 storage,
-              iterations x (76U + 4(n+1) + 48n + 264n) in FP64) over its mean device time.
+* roofline-- the PCG kernel: algorithmic bytes per solve (CG iterations x
+             (40U + 4(n+1) + 24n + 132n) in FP32 storage, (76U + 4(n+1) + 48n + 264n) in
+             FP64; per body for the batched solve) over its mean device time.
+* config.fp64_gpu -- the plain FP64 GPU step (one coupled PCG, FP64 everywhere) on the
+             same workload, and the mixed step's relative position error against it
+             from one shared state.
 * cpu_baseline -- the reference compiled from its own sources (oracle/_ref, FP32,
              one thread: the reference is single-threaded), bounded sample of the same
-             workload.
+             workload (for the batched workload: a sample of bodies, each in its own
+             reference World, scaled to the batch).
+
+batched256 runs one PCG per body in one launch, replayed as a CUDA graph.
 
 --impl reference times that reference CPU path alone on the same workload and prints
 the same line with "impl": "reference".  Multi-GPU (torchrun): a single body does not
-shard, so each rank runs an independent replica ("scaling": "weak").
+shard, so each rank runs an independent replica ("scaling": "weak"); the batched bodies
+are independent, so rank r steps bodies r, r + N, ... ("scaling": "strong", no collective).
 """
 from __future__ import annotations
 
@@ -47,6 +55,9 @@ WORKLOADS = {
                   "CG tol 1e-6 / 100 iterations"),
     "cube8": (1, "cube8: 729 vertices, 3,072 Kuhn tets, jitter 0.1h, x=0 pinned, E=1e5 nu=0.3, dt=1/60"),
     "beam32": (5, "beam32x8x8: 2,673 vertices, 12,288 Kuhn tets, per-element E, x=0 pinned, dt=1/60"),
+    "batched256": (3, "batched256: 256 independent Kuhn boxes, cells per axis U{4..24} (seed 1), E log-uniform "
+                      "[1e4,1e6], nu U[0.25,0.45], random rotation and rigid velocity N(0,0.5^2), x=0 face pinned, "
+                      "dt=1/60, CG tol 1e-6 / 100 iterations, one PCG per body"),
 }
 
 
@@ -200,6 +211,35 @@ def max_over_ranks(pg, value, local):
     return float(t.item())
 
 
+def batched_bytes(rs, col, n2d, scene, body_iters, precision):
+    """Algorithmic PCG bytes of one batched solve: per body, its iterations times the
+    per-iteration bytes of its own diagonal block of the matrix."""
+    total, base, row0 = 0, 0, 0
+    for b, body in enumerate(scene.bodies):
+        nodes = body.positions.shape[0]
+        dyn = n2d[base:base + nodes]
+        rows = int(np.count_nonzero(dyn >= 0))
+        if rows:
+            nnz = int(rs[row0 + rows] - rs[row0])
+            total += body_iters[b] * pcg_bytes_per_iteration(rows, nnz, precision)
+        base += nodes
+        row0 += rows
+    return total
+
+
+def time_steps(w, stream, steps):
+    import torch
+
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(steps):
+        w.step()
+    stop.record(stream)
+    stop.synchronize()
+    return start.elapsed_time(stop)
+
+
 def run_ours(args, scene, rank, world, local, pg):
     import torch
 
@@ -207,11 +247,15 @@ def run_ours(args, scene, rank, world, local, pg):
     from physik_b200.world import SimWorld
 
     torch.cuda.set_device(local)
+    batched = args.workload == "batched256"
     w = SimWorld(scene, precision=args.precision, device=local)
     n_nodes = w.node_count
+    w.set_batched(batched)
     w.step()  # builds and uploads the scene
     w.synchronize()
-    rs, col, _, _ = w.pattern()
+    tuned = w.autotune(3)  # picks the PCG kernel / tile or part size for this scene
+    w.set_graph(batched)   # the batched step (many small bodies) is replayed as one CUDA graph
+    rs, col, n2d, _ = w.pattern()
     n, nnz = len(rs) - 1, len(col)
     stream = torch.cuda.ExternalStream(w.stream(), device=f"cuda:{local}")
 
@@ -221,21 +265,37 @@ def run_ours(args, scene, rank, world, local, pg):
 
     # --- device-resident timed region -------------------------------------
     w.enable_timing(True)
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(pg)
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
-        start.record(stream)
-        for _ in range(args.steps):
-            w.step()
-        stop.record(stream)
-        stop.synchronize()
+        elapsed_ms = time_steps(w, stream, args.steps)
         torch.cuda.synchronize()
     barrier(pg)
-    elapsed_ms = max_over_ranks(pg, start.elapsed_time(stop), local)
+    elapsed_ms = max_over_ranks(pg, elapsed_ms, local)
     tm = w.timings()
     stats = w.cg_stats()
     clock = clocks.summary()
+    if not (stats["flags"] & _lib.FLAG_INTEGRATED) or tm["steps"] != args.steps:
+        raise RuntimeError(f"timed steps did not all run: flags {stats['flags']:#x}, {tm['steps']} timed steps, "
+                           f"last error: {w.error()}")
+
+    # PCG kernel time for the roofline: graph steps time as a whole, so a few extra steps
+    # run with plain launches to split assembly and solve.
+    if batched:
+        w.set_graph(False)
+        w.enable_timing(True)
+        w.step()
+        w.step()
+        w.synchronize()
+        tm_split = w.timings()
+        w.set_graph(True)
+        body_iters = [w.body_stats(i)["iterations"] for i in range(len(scene.bodies))]
+        bytes_per_solve = batched_bytes(rs, col, n2d, scene, body_iters, args.precision)
+    else:
+        tm_split = tm
+        bytes_per_solve = pcg_bytes_per_iteration(n, nnz, args.precision) * stats["iterations"]
+    solve_ms = tm_split["solve_ms"] / max(1, tm_split["steps"])
+    assemble_ms = tm_split["assemble_ms"] / max(1, tm_split["steps"])
 
     # --- end to end through the C ABI with pinned host buffers ------------
     hx = torch.empty((n_nodes, 3), dtype=torch.float32, pin_memory=True).numpy()
@@ -261,22 +321,75 @@ def run_ours(args, scene, rank, world, local, pg):
     if not np.all(np.isfinite(hx)):
         raise RuntimeError("non-finite state after the e2e steps")
 
-    steps_total = args.steps * world
+    # --- the plain FP64 GPU step on the same workload (one coupled solve), and the
+    # mixed step's position error against it from one shared state ---------------
+    fp64 = None
+    if world == 1 and args.precision != "fp64" and not args.no_fp64:
+        ref = SimWorld(scene, precision="fp64", device=local)
+        ref.step()
+        ref.synchronize()
+        ref_stream = torch.cuda.ExternalStream(ref.stream(), device=f"cuda:{local}")
+        for _ in range(2):
+            ref.step()
+        k = max(2, min(args.steps, 10))
+        ref_ms = time_steps(ref, ref_stream, k)
+        xs, vs = w.state(f64=True)
+        ref.set_state(xs, vs, f64=True)
+        w.set_state(xs, vs, f64=True)
+        ref.step()
+        w.step()
+        xr, _ = ref.state(f64=True)
+        xm, _ = w.state(f64=True)
+        err = float(np.linalg.norm(xm - xr) / np.linalg.norm(xr))
+        fp64 = {"steps_per_s": k / (ref_ms / 1e3), "ms_per_step": ref_ms / k, "steps": k,
+                "solve": "one coupled PCG over all bodies, FP64 storage and arithmetic",
+                "mixed_position_rel_err_vs_fp64_one_step": err}
+        del ref
+
+    steps_total = args.steps * world if not batched else args.steps
     value = steps_total / (elapsed_ms / 1e3)
-    iters = stats["iterations"]
-    bpi = pcg_bytes_per_iteration(n, nnz, args.precision)
-    solve_ms = tm["solve_ms"] / max(1, tm["steps"])
-    achieved = (bpi * iters) / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else None
+    achieved = bytes_per_solve / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else None
     peak, peak_kind = measured_peaks()
     traffic = None
     tpi = traffic_per_iteration()
-    if tpi and tpi.get("workload") == args.workload and tpi.get("precision") == args.precision:
-        traffic = float(tpi["dram_bytes_per_iteration"]) * iters
+    if tpi and tpi.get("workload") == args.workload and tpi.get("precision") == args.precision and not batched:
+        traffic = float(tpi["dram_bytes_per_iteration"]) * stats["iterations"]
     return dict(
-        value=value, ms_per_step=elapsed_ms / args.steps, e2e_s=e2e_s, n=n, nnz=nnz, nodes=n_nodes, iters=iters,
-        converged=stats["converged"], flags=stats["flags"], assemble_ms=tm["assemble_ms"] / max(1, tm["steps"]),
+        value=value, ms_per_step=elapsed_ms / args.steps, e2e_s=e2e_s, n=n, nnz=nnz, nodes=n_nodes,
+        iters=stats["iterations"], converged=stats["converged"], flags=stats["flags"], assemble_ms=assemble_ms,
         solve_ms=solve_ms, launches=tm["launches"], achieved=achieved, peak=peak, peak_kind=peak_kind,
-        traffic=traffic, clocks=clock, bytes_per_iteration=bpi, h2d=2 * 12 * n_nodes, d2h=2 * 12 * n_nodes)
+        traffic=traffic, clocks=clock, bytes_per_solve=bytes_per_solve, h2d=2 * 12 * n_nodes, d2h=2 * 12 * n_nodes,
+        tuned=tuned, fp64=fp64, batched=batched)
+
+
+def reference_sample(args, scene):
+    """The reference on the host cores.  One body: its PHYSIK_Step, one thread (the
+    reference is single-threaded).  Batched bodies: each body stepped in a reference World
+    of its own (what the batched solve computes per body), a sample of bodies timed and
+    scaled to the whole batch."""
+    if args.workload != "batched256":
+        s = cpu_reference_sample(scene, budget_s=args.cpu_budget)
+        if s is None:
+            return None
+        s["sample"] = (f"{s['steps']} timed PHYSIK_Step of {args.workload} ({s['seconds']:.1f} s) after 1 untimed "
+                       f"step, FP32 reference compiled from its sources, 1 thread ({cpu_model()})")
+        return s
+    from physik_b200 import meshes
+
+    sample = list(range(0, len(scene.bodies), 16))  # 16 of the 256 bodies, every 16th
+    total, steps = 0.0, 0
+    for i in sample:
+        sub = meshes.Scene(f"body{i}", [scene.bodies[i]], dt=scene.dt, steps=scene.steps)
+        s = cpu_reference_sample(sub, budget_s=args.cpu_budget / len(sample), max_steps=3)
+        if s is None:
+            return None
+        total += s["seconds"] / s["steps"]
+        steps = s["steps"]
+    per_batch_step = total * len(scene.bodies) / len(sample)
+    return {"steps_per_s": 1.0 / per_batch_step, "steps": steps, "seconds": total,
+            "sample": (f"{len(sample)} of {len(scene.bodies)} bodies (every 16th), each in its own reference World, "
+                       f"{steps} timed PHYSIK_Step each after 1 untimed step, scaled to the whole batch; FP32 "
+                       f"reference compiled from its sources, 1 thread ({cpu_model()})")}
 
 
 def main():
@@ -289,6 +402,7 @@ def main():
     ap.add_argument("--precision", choices=["mixed", "fp32", "fp64"], default="mixed")
     ap.add_argument("--cpu-budget", type=float, default=45.0, help="seconds of reference CPU time to sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GPU comparison")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -297,25 +411,30 @@ def main():
     rank, world, local, pg = dist_setup(args.gpus)
     cfg, desc = WORKLOADS[args.workload]
     scene = meshes.CONFIGS[cfg]()
-    base_config = {"workload": desc, "precision": args.precision, "gpus": world,
-                   "parallelism": "single GPU" if world == 1 else f"{world} independent replicas (a body does not shard)",
-                   "l2": "working set larger than the 126 MB L2 for block128; no flush"}
+    batched = args.workload == "batched256"
+    if batched and world > 1:
+        # Bodies are independent: rank r steps bodies r, r + N, ... (no collective).
+        scene = meshes.Scene(scene.name, scene.bodies[rank::world], dt=scene.dt, steps=scene.steps)
+    if batched:
+        parallelism = "single GPU" if world == 1 else f"{world} GPUs, bodies sharded by rank, no collective"
+    else:
+        parallelism = "single GPU" if world == 1 else f"{world} independent replicas (a body does not shard)"
+    base_config = {"workload": desc, "precision": args.precision, "gpus": world, "parallelism": parallelism,
+                   "l2": "working set larger than the 126 MB L2; no flush between steps"}
 
     if args.impl == "reference":
         if rank != 0:
             return
-        s = cpu_reference_sample(scene, budget_s=args.cpu_budget * 2)
+        s = reference_sample(args, scene)
         if s is None:
             print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing"}))
             return
-        sample = (f"{s['steps']} timed PHYSIK_Step of {args.workload} after 1 untimed step, FP32 reference "
-                  f"compiled from its sources, 1 thread ({cpu_model()})")
         line = {"impl": "reference", "metric": METRIC, "value": s["steps_per_s"], "unit": "steps/s",
                 "n_gpus": 0, "steps": s["steps"], "warmup": 1, "ms_per_step": 1e3 / s["steps_per_s"],
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic", "config": dict(base_config, precision="fp32 (reference)"),
+                "higher_is_better": True, "scaling": "strong" if batched else "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic", "config": dict(base_config, precision="fp32 (reference)"),
                 "cpu_baseline": {"value": s["steps_per_s"], "unit": "steps/s", "cores": 1, "kind": "reference",
-                                 "sample": sample},
+                                 "sample": s["sample"]},
                 "e2e": {"value": s["steps_per_s"], "unit": "steps/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -328,27 +447,36 @@ def main():
         return
     cpu = None
     if not args.no_cpu_baseline:
-        s = cpu_reference_sample(scene, budget_s=args.cpu_budget, max_steps=None)
+        s = reference_sample(args, scene)
         if s is not None:
             cpu = {"value": s["steps_per_s"], "unit": "steps/s", "cores": 1, "kind": "reference",
-                   "sample": (f"{s['steps']} timed PHYSIK_Step of {args.workload} ({s['seconds']:.1f} s) after 1 "
-                              f"untimed step, FP32 reference compiled from its sources, 1 thread ({cpu_model()})")}
+                   "sample": s["sample"]}
     roof = None
     if r["achieved"] is not None:
+        kernel = ("pcg_batch_kernel (cooperative per-body PCG: symmetric BSR SpMV + block-Jacobi + dots + integrate)"
+                  if r["batched"] else
+                  "PCG kernel chosen by the autotuner (cooperative: fused symmetric BSR SpMV + block-Jacobi + dots"
+                  " + integrate)")
         roof = {"bound": "hbm", "achieved": r["achieved"], "peak": r["peak"], "unit": "GB/s",
-                "frac": r["achieved"] / r["peak"], "traffic": r["traffic"],
-                "kernel": "pcg_kernel (cooperative PCG: fused symmetric BSR SpMV + block-Jacobi + dots + integrate)",
+                "frac": r["achieved"] / r["peak"], "traffic": r["traffic"], "kernel": kernel,
                 "peak_source": f"{r['peak_kind']} hbm_gbs (MEASURED_PEAKS.json)",
-                "bytes_per_iteration": r["bytes_per_iteration"], "iterations_per_launch": r["iters"]}
+                "algorithmic_bytes_per_solve": r["bytes_per_solve"],
+                "bytes_formula": "per CG iteration 40U + 4(n+1) + 24n + 132n (FP32 storage), "
+                                 "76U + 4(n+1) + 48n + 264n (FP64)"}
+    cfg_out = dict(base_config, dynamic_rows=r["n"], upper_blocks=r["nnz"], cg_iterations=r["iters"],
+                   converged=r["converged"], assemble_ms=r["assemble_ms"], pcg_ms=r["solve_ms"],
+                   autotuned_candidate=r["tuned"][0], batched_per_body_solve=r["batched"],
+                   cuda_graph=r["batched"])
+    if r["fp64"] is not None:
+        cfg_out["fp64_gpu"] = r["fp64"]
     line = {
         "metric": METRIC, "value": r["value"], "unit": "steps/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+        "scaling": "strong" if r["batched"] else "weak",
         "vs_baseline": None, "dtype": "f32" if args.precision != "fp64" else "f64", "data": "synthetic",
-        "config": dict(base_config, dynamic_rows=r["n"], upper_blocks=r["nnz"], cg_iterations=r["iters"],
-                       converged=r["converged"], assemble_ms=r["assemble_ms"], pcg_ms=r["solve_ms"]),
-        "roofline": roof, "cpu_baseline": cpu,
-        "e2e": {"value": args.steps * world / r["e2e_s"], "unit": "steps/s", "h2d_bytes_per_step": r["h2d"],
-                "d2h_bytes_per_step": r["d2h"]},
+        "config": cfg_out, "roofline": roof, "cpu_baseline": cpu,
+        "e2e": {"value": (args.steps * (1 if r["batched"] else world)) / r["e2e_s"], "unit": "steps/s",
+                "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
         "gpu_launches": r["launches"], "clocks": r["clocks"],
     }
     print(json.dumps(line))

@@ -168,16 +168,24 @@ __global__ void __launch_bounds__(kBatchThreads, 2) pcg_batch_kernel(BatchPcgArg
             Acc dq[1] = {Acc(0)};
             int qbad = 0;
             const Real rb = Real(beta);
+            // The next pass's row extents are loaded while this pass's entries are in flight.
+            auto extents = [&](int row, int4& e) {
+                e = make_int4(0, 0, 0, 0);
+                if (row < r1) {
+                    e.x = __ldg(P.a.row_start + row);
+                    e.y = __ldg(P.a.row_start + row + 1);
+                    e.z = __ldg(P.a.lt_start + row);
+                    e.w = __ldg(P.a.lt_start + row + 1);
+                }
+            };
+            int4 ext_next;
+            extents(r0 + tid / LPR, ext_next);
             for (int base = r0; base < r1; base += kRowsPerPass) {
                 const int r = base + tid / LPR;
                 const bool valid = r < r1;
-                int ks = 0, nu = 0, ls = 0, tot = 0;
-                if (valid) {
-                    ks = __ldg(P.a.row_start + r);
-                    nu = __ldg(P.a.row_start + r + 1) - ks;
-                    ls = __ldg(P.a.lt_start + r);
-                    tot = nu + (__ldg(P.a.lt_start + r + 1) - ls);
-                }
+                const int4 ext = ext_next;
+                extents(r + kRowsPerPass, ext_next);
+                const int ks = ext.x, nu = ext.y - ext.x, ls = ext.z, tot = nu + (ext.w - ext.z);
                 V3<Real> acc{Real(0), Real(0), Real(0)};
                 for (int j0 = sub; j0 < tot; j0 += NE * LPR) {
                     int c[NE], kb[NE];

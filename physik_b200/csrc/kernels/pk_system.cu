@@ -473,8 +473,10 @@ int build_batch_parts(const std::vector<int>& seg, int capacity, int min_rows, s
     return static_cast<int>(parts.size() / 8);
 }
 
+// Builds and uploads the batched solve's part table if it is missing (synchronous: never
+// called while a stream capture is open).
 template <class Real, class Acc>
-int run_pcg_batch(pk_system* s, const pk_step_params& p, int skip_on_flags)
+int ensure_batch_parts(pk_system* s)
 {
     if (!s->batch_max_grid) s->batch_max_grid = pk::pcg_batch_max_grid<Real, Acc>();
     if (s->batch_parts <= 0) {
@@ -485,6 +487,22 @@ int run_pcg_batch(pk_system* s, const pk_step_params& p, int skip_on_flags)
         if (rc) return rc;
         s->batch_parts = np;
     }
+    return PK_OK;
+}
+
+int ensure_batch_parts_any(pk_system* s)
+{
+    if (!s->batched || s->seg_start.size() < 2) return PK_OK;
+    if (s->precision == PK_PREC_FP32) return ensure_batch_parts<float, float>(s);
+    if (s->precision == PK_PREC_MIXED) return ensure_batch_parts<float, double>(s);
+    return ensure_batch_parts<double, double>(s);
+}
+
+template <class Real, class Acc>
+int run_pcg_batch(pk_system* s, const pk_step_params& p, int skip_on_flags)
+{
+    int rc0 = ensure_batch_parts<Real, Acc>(s);
+    if (rc0) return rc0;
     const int grid = s->batch_parts;
     const int nseg = static_cast<int>(s->seg_start.size()) - 1;
     int rc = ensure_solver_buffers(s, 1);
@@ -626,6 +644,9 @@ int run_step_graph(pk_system* s, const pk_step_params& p)
 {
     if (!s->graph_exec || !same_params(p, s->graph_params)) {
         drop_graph(s);
+        // Everything built lazily (allocations, uploads) must exist before the capture.
+        int prc = ensure_batch_parts_any(s);
+        if (prc) return prc;
         const bool timing = s->timing;
         const long long launches = s->launches;
         s->timing = false;
@@ -1210,6 +1231,8 @@ PKCUDA_API int pk_system_autotune(pk_system* s, const pk_step_params* p, int rep
         }
         s->batch_min_rows = cand[best];
         s->batch_parts = 0;
+        int rc = ensure_batch_parts_any(s);
+        if (rc) return rc;
     } else {
         // Candidates: ring kernel; staged kernel with 16 / 32 / 64-row tiles; plain kernel.
         struct Cand {

@@ -99,3 +99,23 @@ def test_autotuned_batched_matches_untuned():
     xt, vt = tuned.state(f64=True)
     xp, vp = plain.state(f64=True)
     assert rel(xt, xp) <= 1e-12 and rel(vt, vp) <= 1e-8
+
+
+def test_graph_after_autotune_batched_matches_plain():
+    """The autotuner rebuilds the batched part table; the next graph capture must see it."""
+    scene = scene_two_bodies()
+    tuned = SimWorld(scene, precision="fp64")
+    plain = SimWorld(scene, precision="fp64")
+    for w in (tuned, plain):
+        w.set_batched(True)
+        w.step()
+    tuned.autotune(2)
+    tuned.set_graph(True)
+    for _ in range(4):
+        tuned.step()
+        plain.step()
+    st = tuned.cg_stats()
+    assert st["flags"] & L.FLAG_INTEGRATED, (hex(st["flags"]), tuned.error())
+    xt, _ = tuned.state(f64=True)
+    xp, _ = plain.state(f64=True)
+    assert rel(xt, xp) <= 1e-12
