@@ -176,6 +176,17 @@ PHYSIK_B200_API int PHYSIK_B200_EnableTiming(PhysikWorldHandle world, int on);
 PHYSIK_B200_API int PHYSIK_B200_GetTimings(PhysikWorldHandle world, double* assembleMs, double* solveMs, int* steps,
                                            long long* kernelLaunches);
 PHYSIK_B200_API int PHYSIK_B200_SetPcgGrid(PhysikWorldHandle world, int grid);
+/* Adjoint of one implicit substep of size dt (no counterpart in the reference): with the
+ * world at the state the substep starts from and the loss sensitivities to the state
+ * after it (3 doubles per node each, world order), writes the sensitivities to the current
+ * state and adds each tet's sensitivity to its log Young's modulus to youngLogBar (may be
+ * NULL; tets of the tet-mesh physics components in creation order, see
+ * PHYSIK_B200_GetTetCount).  The state is left unchanged.  0 on success, -1 on failure. */
+PHYSIK_B200_API int PHYSIK_B200_AdjointStep(PhysikWorldHandle world, float dt, const double* positionsBarNext,
+                                            const double* velocitiesBarNext, double* positionsBar,
+                                            double* velocitiesBar, double* youngLogBar);
+/* Tets of the world's tet-mesh physics components (the adjoint's tet order), or -1. */
+PHYSIK_B200_API int PHYSIK_B200_GetTetCount(PhysikWorldHandle world);
 /* Captures the device step in a CUDA graph and replays it (see pk_system_set_graph). */
 PHYSIK_B200_API void PHYSIK_B200_SetGraphCapture(PhysikWorldHandle world, int on);
 /* Picks the fastest PCG kernel and tile (or, batched, part) size for the world's scene by

@@ -162,6 +162,18 @@ PKCUDA_API int pk_system_timings(pk_system* sys, double* assemble_ms, double* so
 /* Grid size of the cooperative PCG launch (0 = automatic).  Returns the grid used next. */
 PKCUDA_API int pk_system_set_pcg_grid(pk_system* sys, int grid);
 
+/* Backward (adjoint) step of pk_system_step -- no counterpart in the reference.  With the
+ * system at the state (x, v) a forward step starts from, and the loss sensitivities to
+ * the state after that step (xbar_next, vbar_next: 3*node_count each, world order), it
+ * writes the sensitivities to (x, v) (xbar, vbar) and ADDS each tet's sensitivity to its
+ * log Young's modulus to theta_bar[tet] (may be NULL).  It re-runs the step's assembly and
+ * solve (no integration, state unchanged), solves the adjoint system A w = g with the same
+ * PCG (A is symmetric; the solve is treated as exact), and evaluates the element terms on
+ * the GPU (pk_adjoint.cu).  The velocity sensitivity of fixed nodes is passed through
+ * unchanged.  A batched system is differentiated as one coupled solve. */
+PKCUDA_API int pk_system_adjoint_step(pk_system* sys, const pk_step_params* params, const double* xbar_next,
+                                      const double* vbar_next, double* xbar, double* vbar, double* theta_bar);
+
 /* Captures each step into a CUDA graph (relaxed capture mode) and replays it: the first
  * step after enabling runs normally (allocations, uploads), the next one with the same
  * parameters is captured, later ones launch the graph.  Any topology, segment, grid or

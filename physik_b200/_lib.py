@@ -92,6 +92,7 @@ _SIGS = {
     "pk_system_segment_stats": (_i, [_p, _i, _p, _p, _p, _p]),
     "pk_ring_tiling_selfcheck": (_i, [_i, _i, _p, _p, _p, _p, _p, _p, _p]),
     "pk_system_set_graph": (_i, [_p, _i]),
+    "pk_system_adjoint_step": (_i, [_p, C.POINTER(PkStepParams), _p, _p, _p, _p, _p]),
     "pk_system_autotune": (_i, [_p, C.POINTER(PkStepParams), _i, _p, _p]),
     # physik_b200.h
     "PHYSIK_CreateWorld": (_p, []),
@@ -158,6 +159,8 @@ _SIGS = {
     "PHYSIK_B200_SetPcgGrid": (_i, [_p, _i]),
     "PHYSIK_B200_SetBatchedSolve": (_v, [_p, _i]),
     "PHYSIK_B200_SetGraphCapture": (_v, [_p, _i]),
+    "PHYSIK_B200_AdjointStep": (_i, [_p, _f, _p, _p, _p, _p, _p]),
+    "PHYSIK_B200_GetTetCount": (_i, [_p]),
     "PHYSIK_B200_Autotune": (_i, [_p, _i, _p]),
     "PHYSIK_B200_GetBodyConjugateGradientStats": (_i, [_p, _H, _p, _p, _p, _p]),
     "PHYSIK_B200_GetStream": (_p, [_p]),

@@ -571,6 +571,27 @@ PHYSIK_B200_API int PHYSIK_B200_GetBodyConjugateGradientStats(PhysikWorldHandle 
         -1);
 }
 
+PHYSIK_B200_API int PHYSIK_B200_AdjointStep(PhysikWorldHandle world, float dt, const double* positionsBarNext,
+                                            const double* velocitiesBarNext, double* positionsBar,
+                                            double* velocitiesBar, double* youngLogBar)
+{
+    World* w = AsWorld(world);
+    if (!w || !positionsBarNext || !velocitiesBarNext || !positionsBar || !velocitiesBar) return -1;
+    return Guard(
+        [&] {
+            w->AdjointStep(dt, positionsBarNext, velocitiesBarNext, positionsBar, velocitiesBar, youngLogBar);
+            return 0;
+        },
+        -1);
+}
+
+PHYSIK_B200_API int PHYSIK_B200_GetTetCount(PhysikWorldHandle world)
+{
+    World* w = AsWorld(world);
+    if (!w) return -1;
+    return Guard([&] { return w->PrepareScene(false) >= 0 ? w->GetSceneTetCount() : -1; }, -1);
+}
+
 PHYSIK_B200_API void PHYSIK_B200_SetGraphCapture(PhysikWorldHandle world, int on)
 {
     World* w = AsWorld(world);

@@ -389,6 +389,15 @@ public:
     bool GetBodyConjugateGradientStats(const Component* body, int& iterations, bool& converged, float& residualNorm,
                                        unsigned& flags) const;
 
+    // Adjoint of one implicit substep (extension, no counterpart in the reference): with
+    // the world at the state a substep of size dt starts from and the loss sensitivities
+    // to the state after it (3 doubles per node each), writes the sensitivities to the
+    // current state and adds each tet's log-Young's-modulus sensitivity to thetaBar
+    // (tets of the tet-mesh physics components in creation order).  See
+    // pk_system_adjoint_step.
+    void AdjointStep(float dt, const double* xbarNext, const double* vbarNext, double* xbar, double* vbar,
+                     double* thetaBar);
+
     // CUDA-graph capture of the device step (extension).
     void SetGraphCapture(bool on) { graphCapture = on; }
     // Autotuner (extension): picks the fastest PCG kernel / tile or part size for the
@@ -426,6 +435,7 @@ public:
     int PrepareScene(bool upload);
     int GetSceneDynamicCount() const;
     int GetSceneBlockCount() const;
+    int GetSceneTetCount() const;
     const std::vector<int>* GetSceneRowStart() const;
     const std::vector<int>* GetSceneColIndex() const;
     const std::vector<int>* GetSceneNodeToDyn() const;

@@ -848,6 +848,35 @@ void World::EnsureScene(bool upload)
 
 void World::SetBatchedSolve(bool on) { batchedSolve = on; }
 
+void World::AdjointStep(float dt, const double* xbarNext, const double* vbarNext, double* xbar, double* vbar,
+                        double* thetaBar)
+{
+    if (solverMode != SolverMode::ImplicitEuler) throw std::runtime_error("the adjoint step needs the implicit solver");
+    if (!(dt > 0.0f)) throw std::runtime_error("dt must be > 0");
+    CollectContributions(dt);
+    EnsureScene(true);
+    if (deviceStale) {
+        std::vector<float> x(3 * positions.size()), v(3 * positions.size());
+        for (std::size_t i = 0; i < positions.size(); ++i) {
+            x[3 * i] = positions[i].x; x[3 * i + 1] = positions[i].y; x[3 * i + 2] = positions[i].z;
+            v[3 * i] = velocities[i].x; v[3 * i + 1] = velocities[i].y; v[3 * i + 2] = velocities[i].z;
+        }
+        Check(pk_system_set_state_f32(scene->sys, x.data(), v.data()), "set_state");
+        deviceStale = false;
+    }
+    pk_step_params p{};
+    p.dt = dt;
+    p.gravity[0] = gravity.x;
+    p.gravity[1] = gravity.y;
+    p.gravity[2] = gravity.z;
+    p.max_iterations = conjugateGradientSettings.maxIterations;
+    p.tolerance = conjugateGradientSettings.tolerance;
+    p.use_jacobi = conjugateGradientSettings.useJacobiPreconditioner ? 1 : 0;
+    p.integrate = 0;
+    Check(pk_system_adjoint_step(scene->sys, &p, xbarNext, vbarNext, xbar, vbar, thetaBar), "adjoint_step");
+    statsPending = false;
+}
+
 int World::Autotune(int repeats, double* bestMs)
 {
     SyncStats();
@@ -902,6 +931,7 @@ int World::GetSceneBlockCount() const
 {
     return scene && scene->built ? static_cast<int>(scene->colIndex.size()) : -1;
 }
+int World::GetSceneTetCount() const { return scene && scene->built ? scene->tetCount : -1; }
 const std::vector<int>* World::GetSceneRowStart() const { return scene && scene->built ? &scene->rowStart : nullptr; }
 const std::vector<int>* World::GetSceneColIndex() const { return scene && scene->built ? &scene->colIndex : nullptr; }
 const std::vector<int>* World::GetSceneNodeToDyn() const { return scene && scene->built ? &scene->nodeToDyn : nullptr; }

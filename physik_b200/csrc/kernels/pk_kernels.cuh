@@ -265,6 +265,29 @@ struct BatchPcgArgs {
     BatchBodyStats* body_stats;
 };
 
+// ------------------------------------------------------------------ adjoint step
+// Backward element kernel (pk_adjoint.cu): per tet, the sensitivities of
+// J = dt w.f(x) - dt^2 w.K(x) z to the tet's node positions (12 doubles) and to its
+// log Young's modulus.
+template <class Real>
+struct AdjointArgs {
+    int tet_count;
+    const int4* nodes;
+    const unsigned char* enabled;
+    const Real* dm_inv;
+    const Real* params;      // V, lambda, mu, damping
+    const Real* x;           // per world node
+    const Real* v;
+    const int* node_to_dyn;
+    const double* w;         // adjoint solution, per dynamic row
+    const double* du;        // the step's delta-v, per dynamic row
+    double dt;
+    int linear;
+    unsigned* flags;
+    double* tet_grad;        // out: 12 per tet
+    double* tet_theta;       // out: 1 per tet
+};
+
 // Launchers (pk_kernels.cu).  All asynchronous on `stream`.
 template <class Real>
 cudaError_t launch_tet_kernel(const AssemblyArgs<Real>& args, bool fp64_polar_fallback, cudaStream_t stream);
@@ -277,6 +300,8 @@ template <class Real, class Acc>
 int pcg_max_grid(int threads, bool staged);
 template <class Real>
 cudaError_t launch_spmv_kernel(const BsrView<Real>& a, const Real* x, Real* y, cudaStream_t stream);
+template <class Real>
+cudaError_t launch_adjoint_tet_kernel(const AdjointArgs<Real>& args, cudaStream_t stream);
 // Batched per-body PCG (pk_pcg_batch.cu): cooperative, one block per body part.
 template <class Real, class Acc>
 cudaError_t launch_pcg_batch_kernel(const BatchPcgArgs<Real, Acc>& args, int grid, cudaStream_t stream);

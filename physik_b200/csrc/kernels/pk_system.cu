@@ -217,6 +217,11 @@ struct pk_system {
     int kernel_choice = -1;
     int staged_rows = 0;          // rows per staged tile (0: chosen from the grid)
     std::vector<int> h_row_start, h_lts;  // host copies for re-tiling
+    // host copies for the adjoint step's assembly of node sensitivities
+    std::vector<int> h_node_to_dyn, h_dyn_to_node, h_tet_nodes;
+    std::vector<unsigned char> h_enabled;
+    std::vector<double> h_mass, h_damping;
+    DevBuf adj_w, adj_du, adj_grad, adj_theta;
     bool assembled = false;       // a step has assembled the system at least once
     // CUDA graph of one step
     bool use_graph = false;
@@ -796,6 +801,8 @@ PKCUDA_API int pk_system_set_nodes(pk_system* s, int node_count, const int* node
     if (!s || node_count < 0 || (node_count > 0 && (!node_to_dyn || !mass))) return fail(PK_ERR_ARG, "set_nodes");
     PK_CHECK(cudaSetDevice(s->device));
     s->node_count = node_count;
+    s->h_node_to_dyn.assign(node_to_dyn, node_to_dyn + node_count);
+    s->h_mass.assign(mass, mass + node_count);
     int rc = upload_raw<int>(s->node_to_dyn, node_to_dyn, node_count, s->stream);
     if (!rc) rc = upload_real_any(s, s->mass, mass, node_count);
     if (rc) return rc;
@@ -878,6 +885,9 @@ PKCUDA_API int pk_system_set_tets(pk_system* s, int tet_count, const int* tet_no
     for (long long i = 0; i < 4ll * tet_count; ++i)
         if (tet_nodes[i] < 0 || tet_nodes[i] >= s->node_count) return fail(PK_ERR_ARG, "tet node out of range");
     s->tet_count = tet_count;
+    s->h_tet_nodes.assign(tet_nodes, tet_nodes + 4 * static_cast<size_t>(tet_count));
+    s->h_enabled.assign(enabled, enabled + tet_count);
+    s->h_damping.assign(damping, damping + tet_count);
     std::vector<double> params(4 * static_cast<size_t>(tet_count));
     for (int t = 0; t < tet_count; ++t) {
         params[4 * t + 0] = volume[t];
@@ -951,6 +961,7 @@ PKCUDA_API int pk_system_set_pattern(pk_system* s, int dyn_count, const int* dyn
     s->assembled = false;
     drop_graph(s);
     s->h_row_start.assign(row_start, row_start + dyn_count + 1);
+    s->h_dyn_to_node.assign(dyn_to_node, dyn_to_node + dyn_count);
     s->h_lts = lts;
     // Ring-staged PCG tiles (the default kernel).
     s->ring_tiles = 0;
@@ -1273,6 +1284,145 @@ PKCUDA_API int pk_system_autotune(pk_system* s, const pk_step_params* p, int rep
     if (chosen) *chosen = best;
     if (best_ms) *best_ms = best_t;
     return PK_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+template <class Real>
+int adjoint_step(pk_system* s, const pk_step_params& p, const double* xbar_next, const double* vbar_next, double* xbar,
+                 double* vbar, double* theta_bar)
+{
+    const int n = s->dyn_count, nn = s->node_count, T = s->tet_count;
+    // 1. The forward step at the current state, without integration: A, b, delta-v.
+    pk_step_params q = p;
+    q.integrate = 0;
+    q.explicit_mode = 0;
+    int rc = run_step<Real>(s, q);
+    if (rc) return rc;
+    pk_step_stats st{};
+    rc = pk_system_stats(s, &st);
+    if (rc) return rc;
+    if (!(st.flags & PK_FLAG_SOLVED)) return fail(PK_ERR_STATE, "adjoint: the forward solve failed");
+    std::vector<double> du(3 * static_cast<size_t>(n)), g(3 * static_cast<size_t>(n));
+    rc = download_real<Real>(s->px, du.data(), du.size(), s->stream);
+    if (rc) return rc;
+    // 2. Adjoint right-hand side: adjoint of v' plus dt times the adjoint of x' (dynamic rows).
+    for (int r = 0; r < n; ++r) {
+        const int node = s->h_dyn_to_node[r];
+        for (int c = 0; c < 3; ++c) g[3 * r + c] = vbar_next[3 * node + c] + p.dt * xbar_next[3 * node + c];
+    }
+    rc = upload_real<Real>(s->rhs, g.data(), g.size(), s->stream);
+    if (rc) return rc;
+    // 3. A w = g with the same PCG (A symmetric).
+    if (s->precision == PK_PREC_FP32) rc = run_pcg<float, float>(s, q, 0);
+    else if (s->precision == PK_PREC_MIXED) rc = run_pcg<float, double>(s, q, 0);
+    else rc = run_pcg<double, double>(s, q, 0);
+    if (rc) return rc;
+    PK_CHECK(cudaMemcpyAsync(s->host_stats, s->stats.p, sizeof(pk::DevStats), cudaMemcpyDeviceToHost, s->stream));
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    if (!(s->host_stats->flags & PK_FLAG_SOLVED)) return fail(PK_ERR_STATE, "adjoint: the adjoint solve failed");
+    std::vector<double> w(3 * static_cast<size_t>(n)), aw(3 * static_cast<size_t>(n));
+    rc = download_real<Real>(s->px, w.data(), w.size(), s->stream);
+    if (rc) return rc;
+    // A w (for the velocity sensitivity dt^2 K w = A w - M w)
+    pk::BsrView<Real> view{};
+    view.n = n;
+    view.row_start = s->row_start.as<int>();
+    view.col = s->col.as<int>();
+    view.values = s->values.as<Real>();
+    view.lt_start = s->lt_start.as<int>();
+    view.lt_row = s->lt_row.as<int>();
+    view.lt_block = s->lt_block.as<int>();
+    PK_CHECK(pk::launch_spmv_kernel<Real>(view, s->px.as<Real>(), s->pq.as<Real>(), s->stream));
+    rc = download_real<Real>(s->pq, aw.data(), aw.size(), s->stream);
+    if (rc) return rc;
+    // 4. Element sensitivities.
+    PK_CHECK(s->adj_w.ensure(sizeof(double) * w.size()));
+    PK_CHECK(s->adj_du.ensure(sizeof(double) * du.size()));
+    PK_CHECK(s->adj_grad.ensure(sizeof(double) * 12 * static_cast<size_t>(std::max(1, T))));
+    PK_CHECK(s->adj_theta.ensure(sizeof(double) * static_cast<size_t>(std::max(1, T))));
+    PK_CHECK(cudaMemcpyAsync(s->adj_w.p, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, s->stream));
+    PK_CHECK(cudaMemcpyAsync(s->adj_du.p, du.data(), sizeof(double) * du.size(), cudaMemcpyHostToDevice, s->stream));
+    pk::AdjointArgs<Real> a{};
+    a.tet_count = T;
+    a.nodes = s->tet_nodes.as<int4>();
+    a.enabled = s->tet_enabled.as<unsigned char>();
+    a.dm_inv = s->dm_inv.as<Real>();
+    a.params = s->tet_params.as<Real>();
+    a.x = s->x.as<Real>();
+    a.v = s->v.as<Real>();
+    a.node_to_dyn = s->node_to_dyn.as<int>();
+    a.w = s->adj_w.as<double>();
+    a.du = s->adj_du.as<double>();
+    a.dt = static_cast<double>(static_cast<Real>(p.dt));
+    a.linear = p.linear;
+    a.flags = &s->stats.as<pk::DevStats>()->flags;
+    a.tet_grad = s->adj_grad.as<double>();
+    a.tet_theta = s->adj_theta.as<double>();
+    PK_CHECK(pk::launch_adjoint_tet_kernel<Real>(a, s->stream));
+    std::vector<double> grad(12 * static_cast<size_t>(T)), th(static_cast<size_t>(T));
+    if (T > 0) {
+        PK_CHECK(cudaMemcpyAsync(grad.data(), s->adj_grad.p, sizeof(double) * grad.size(), cudaMemcpyDeviceToHost,
+                                 s->stream));
+        PK_CHECK(cudaMemcpyAsync(th.data(), s->adj_theta.p, sizeof(double) * th.size(), cudaMemcpyDeviceToHost,
+                                 s->stream));
+    }
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    // 5. Node sensitivities before the step.  Positions: x' = x + dt v' carries the
+    // adjoint of x' back unchanged, plus dJ/dx on dynamic nodes (fixed nodes never move).
+    // Velocities: v' = v + du carries g back on dynamic rows, plus d(w.b)/dv = -dt^2 K w
+    // - dt c w with dt^2 K w = A w - m w (c: the damping of the node's active tets);
+    // fixed nodes keep their adjoint (their velocity only enters through b's coupling
+    // blocks, which the dynamic-row matrix does not hold: not propagated).
+    std::copy(xbar_next, xbar_next + 3 * static_cast<size_t>(nn), xbar);
+    std::copy(vbar_next, vbar_next + 3 * static_cast<size_t>(nn), vbar);
+    std::vector<double> csum(static_cast<size_t>(nn), 0.0);
+    for (int t = 0; t < T; ++t) {
+        if (!(s->h_enabled[t] & 1u)) continue;
+        for (int k = 0; k < 4; ++k) {
+            const int node = s->h_tet_nodes[4 * static_cast<size_t>(t) + k];
+            csum[node] += s->h_damping[t];
+            if (s->h_node_to_dyn[node] < 0) continue;
+            for (int c = 0; c < 3; ++c) xbar[3 * node + c] += grad[12 * static_cast<size_t>(t) + 3 * k + c];
+        }
+        if (theta_bar) theta_bar[t] += th[t];
+    }
+    for (int r = 0; r < n; ++r) {
+        const int node = s->h_dyn_to_node[r];
+        const double m = s->h_mass[node];
+        for (int c = 0; c < 3; ++c)
+            vbar[3 * node + c] = g[3 * r + c] - aw[3 * r + c] + m * w[3 * r + c] - p.dt * csum[node] * w[3 * r + c];
+    }
+    return PK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+PKCUDA_API int pk_system_adjoint_step(pk_system* s, const pk_step_params* p, const double* xbar_next,
+                                      const double* vbar_next, double* xbar, double* vbar, double* theta_bar)
+{
+    if (!s || !p || !xbar_next || !vbar_next || !xbar || !vbar) return fail(PK_ERR_ARG, "adjoint_step");
+    if (!s->have_nodes || !s->have_tets || !s->have_pattern) return fail(PK_ERR_STATE, "adjoint before topology");
+    if (!(p->dt > 0.0)) return fail(PK_ERR_ARG, "dt must be > 0");
+    if (s->dyn_count > 0 && !s->diag_first) return fail(PK_ERR_ARG, "every dynamic row needs its diagonal block first");
+    PK_CHECK(cudaSetDevice(s->device));
+    drop_graph(s);
+    if (s->dyn_count == 0) {
+        std::copy(xbar_next, xbar_next + 3 * static_cast<size_t>(s->node_count), xbar);
+        std::copy(vbar_next, vbar_next + 3 * static_cast<size_t>(s->node_count), vbar);
+        return PK_OK;
+    }
+    const bool batched = s->batched;
+    s->batched = false;  // one coupled solve: the adjoint of the world's step
+    const int rc = s->precision == PK_PREC_FP64
+                       ? adjoint_step<double>(s, *p, xbar_next, vbar_next, xbar, vbar, theta_bar)
+                       : adjoint_step<float>(s, *p, xbar_next, vbar_next, xbar, vbar, theta_bar);
+    s->batched = batched;
+    return rc;
 }
 
 PKCUDA_API int pk_bsr_transpose_index(int n, const int* row_start, const int* col_index, int* lt_start, int* lt_row,

@@ -98,6 +98,26 @@ class SimWorld:
     def set_batched(self, on: bool = True):
         self.X.PHYSIK_B200_SetBatchedSolve(self.h, 1 if on else 0)
 
+    def tet_count(self) -> int:
+        return int(self.X.PHYSIK_B200_GetTetCount(self.h))
+
+    def set_tet_young(self, body: int, young):
+        ty = np.ascontiguousarray(young, np.float32)
+        if not self.X.PHYSIK_B200_SetTetMeshYoungModulus(self.h, self.components[body], _ptr(ty), ty.shape[0]):
+            raise PhysikError("per-tet Young's modulus rejected: " + self.error())
+
+    def adjoint_step(self, xbar_next, vbar_next, theta_bar, dt: Optional[float] = None):
+        """Sensitivities to the current state, given those to the state after one step;
+        adds the log-Young's-modulus sensitivities to theta_bar (float64, one per tet)."""
+        xbar_next = np.ascontiguousarray(xbar_next, np.float64)
+        vbar_next = np.ascontiguousarray(vbar_next, np.float64)
+        xbar = np.zeros_like(xbar_next)
+        vbar = np.zeros_like(vbar_next)
+        if self.X.PHYSIK_B200_AdjointStep(self.h, self.dt if dt is None else dt, _ptr(xbar_next), _ptr(vbar_next),
+                                          _ptr(xbar), _ptr(vbar), _ptr(theta_bar)) != 0:
+            raise PhysikError("adjoint step failed: " + self.error())
+        return xbar, vbar
+
     def set_graph(self, on: bool = True):
         self.X.PHYSIK_B200_SetGraphCapture(self.h, 1 if on else 0)
 
