@@ -202,13 +202,25 @@ def barrier(pg):
 
 
 def max_over_ranks(pg, value, local):
+    """The largest value over the ranks (a CUDA tensor with NCCL, a host tensor with gloo)."""
     if pg is None:
         return value
     import torch
 
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    device = f"cuda:{local}" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def shard_scene(scene, rank, world):
+    """Independent bodies split over ranks: rank r keeps bodies r, r + world, ..."""
+    from physik_b200 import meshes
+
+    if world <= 1:
+        return scene
+    return meshes.Scene(scene.name, scene.bodies[rank::world], dt=scene.dt, steps=scene.steps,
+                        gravity=scene.gravity, tolerance=scene.tolerance, max_iterations=scene.max_iterations)
 
 
 def batched_bytes(rs, col, n2d, scene, body_iters, precision):
@@ -414,7 +426,7 @@ def main():
     batched = args.workload == "batched256"
     if batched and world > 1:
         # Bodies are independent: rank r steps bodies r, r + N, ... (no collective).
-        scene = meshes.Scene(scene.name, scene.bodies[rank::world], dt=scene.dt, steps=scene.steps)
+        scene = shard_scene(scene, rank, world)
     if batched:
         parallelism = "single GPU" if world == 1 else f"{world} GPUs, bodies sharded by rank, no collective"
     else:
