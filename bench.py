@@ -70,6 +70,17 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+KERNEL_NAMES = {
+    "slab": "pcg_slab_kernel (cooperative, one block per part: search directions resident in shared memory, "
+            "full symmetric rows streamed by TMA, block-Jacobi, dots, integrate)",
+    "ring": "pcg_ring_kernel (cooperative: TMA-staged upper BSR rows, L2 gathers of lower blocks and records, "
+            "block-Jacobi, dots, integrate)",
+    "staged": "pcg_kernel (cooperative, TMA-staged tiles)",
+    "plain": "pcg_kernel (cooperative, unstaged)",
+    "batched": "pcg_batch_kernel (cooperative per-body PCG: symmetric BSR SpMV + block-Jacobi + dots + integrate)",
+}
+
+
 def traffic_per_iteration():
     """DRAM bytes per PCG iteration from the committed ncu summary, if present."""
     path = os.path.join(ROOT, "profiles", "pcg_dram_traffic.json")
@@ -274,6 +285,7 @@ def run_ours(args, scene, rank, world, local, pg):
     for _ in range(args.warmup):
         w.step()
     w.synchronize()
+    pcg_kernel, pcg_blocks = w.pcg_kernel()
 
     # --- device-resident timed region -------------------------------------
     w.enable_timing(True)
@@ -364,14 +376,15 @@ def run_ours(args, scene, rank, world, local, pg):
     peak, peak_kind = measured_peaks()
     traffic = None
     tpi = traffic_per_iteration()
-    if tpi and tpi.get("workload") == args.workload and tpi.get("precision") == args.precision and not batched:
+    if (tpi and tpi.get("workload") == args.workload and tpi.get("precision") == args.precision
+            and tpi.get("kernel") == pcg_kernel and not batched):
         traffic = float(tpi["dram_bytes_per_iteration"]) * stats["iterations"]
     return dict(
         value=value, ms_per_step=elapsed_ms / args.steps, e2e_s=e2e_s, n=n, nnz=nnz, nodes=n_nodes,
         iters=stats["iterations"], converged=stats["converged"], flags=stats["flags"], assemble_ms=assemble_ms,
         solve_ms=solve_ms, launches=tm["launches"], achieved=achieved, peak=peak, peak_kind=peak_kind,
         traffic=traffic, clocks=clock, bytes_per_solve=bytes_per_solve, h2d=2 * 12 * n_nodes, d2h=2 * 12 * n_nodes,
-        tuned=tuned, fp64=fp64, batched=batched)
+        tuned=tuned, fp64=fp64, batched=batched, pcg_kernel=pcg_kernel, pcg_blocks=pcg_blocks)
 
 
 def reference_sample(args, scene):
@@ -465,10 +478,7 @@ def main():
                    "sample": s["sample"]}
     roof = None
     if r["achieved"] is not None:
-        kernel = ("pcg_batch_kernel (cooperative per-body PCG: symmetric BSR SpMV + block-Jacobi + dots + integrate)"
-                  if r["batched"] else
-                  "PCG kernel chosen by the autotuner (cooperative: fused symmetric BSR SpMV + block-Jacobi + dots"
-                  " + integrate)")
+        kernel = KERNEL_NAMES.get(r["pcg_kernel"], r["pcg_kernel"]) + f", {r['pcg_blocks']} blocks"
         roof = {"bound": "hbm", "achieved": r["achieved"], "peak": r["peak"], "unit": "GB/s",
                 "frac": r["achieved"] / r["peak"], "traffic": r["traffic"], "kernel": kernel,
                 "peak_source": f"{r['peak_kind']} hbm_gbs (MEASURED_PEAKS.json)",
@@ -477,7 +487,8 @@ def main():
                                  "76U + 4(n+1) + 48n + 264n (FP64)"}
     cfg_out = dict(base_config, dynamic_rows=r["n"], upper_blocks=r["nnz"], cg_iterations=r["iters"],
                    converged=r["converged"], assemble_ms=r["assemble_ms"], pcg_ms=r["solve_ms"],
-                   autotuned_candidate=r["tuned"][0], batched_per_body_solve=r["batched"],
+                   autotuned_candidate=r["tuned"][0], pcg_kernel=r["pcg_kernel"], pcg_blocks=r["pcg_blocks"],
+                   batched_per_body_solve=r["batched"],
                    cuda_graph=r["batched"])
     if r["fp64"] is not None:
         cfg_out["fp64_gpu"] = r["fp64"]

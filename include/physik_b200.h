@@ -194,6 +194,10 @@ PHYSIK_B200_API void PHYSIK_B200_SetGraphCapture(PhysikWorldHandle world, int on
  * chosen candidate (see pk_system_autotune) or -1; bestSolveMs (may be NULL) receives its
  * mean solve time. */
 PHYSIK_B200_API int PHYSIK_B200_Autotune(PhysikWorldHandle world, int repeats, double* bestSolveMs);
+/* The PCG kernel of the last step's solve (see pk_system_pcg_kernel: 0 ring-staged, 1
+ * TMA-staged, 2 unstaged, 3 part-resident, 4 batched) or -1; blocks (may be NULL)
+ * receives the blocks it ran on. */
+PHYSIK_B200_API int PHYSIK_B200_GetPcgKernel(PhysikWorldHandle world, int* blocks);
 /* Batched solve: one PCG per tet-mesh physics component (own scalars, stopping test,
  * iteration count and all-or-nothing integration, as a world holding only that body),
  * all bodies in one launch, instead of the reference's single coupled PCG over the whole

@@ -174,14 +174,19 @@ PKCUDA_API int pk_system_set_pcg_grid(pk_system* sys, int grid);
 PKCUDA_API int pk_system_adjoint_step(pk_system* sys, const pk_step_params* params, const double* xbar_next,
                                       const double* vbar_next, double* xbar, double* vbar, double* theta_bar);
 
+/* The PCG kernel of the last solve: 0 ring-staged, 1 TMA-staged, 2 unstaged, 3
+ * part-resident, 4 batched per-body; -1 before the first solve (or a negative PK_ERR_*).
+ * blocks (may be NULL) receives the blocks it ran on. */
+PKCUDA_API int pk_system_pcg_kernel(pk_system* sys, int* blocks);
 /* Captures each step into a CUDA graph (relaxed capture mode) and replays it: the first
  * step after enabling runs normally (allocations, uploads), the next one with the same
  * parameters is captured, later ones launch the graph.  Any topology, segment, grid or
  * parameter change drops the graph.  With timing on, a graph step counts as solve time. */
 PKCUDA_API int pk_system_set_graph(pk_system* sys, int on);
 /* Autotuner: times `repeats` solves (without integration) of the last assembled system
- * for each candidate and keeps the fastest -- unbatched: the ring-staged kernel, the
- * TMA-staged kernel with 16 / 32 / 64-row tiles, the unstaged kernel; batched: the
+ * for each candidate and keeps the fastest -- unbatched: the ring-staged kernel (0), the
+ * TMA-staged kernel with 16 / 32 / 64-row tiles (1-3), the unstaged kernel (4), the
+ * part-resident kernel (5, FP32 storage, where its layout applies); batched: the
  * smallest part (32 .. 1024 rows) a body is cut into.  Needs one step first.  Reports the
  * candidate index and its mean solve time.  Candidates differ only in summation order. */
 PKCUDA_API int pk_system_autotune(pk_system* sys, const pk_step_params* params, int repeats, int* chosen,
@@ -223,6 +228,16 @@ PKCUDA_API const char* pk_pcg_noalloc_last_error(void);
  * reference (it checks this library's own layout). */
 PKCUDA_API int pk_ring_tiling_selfcheck(int precision, int n, const int* row_start, const int* col_index,
                                         const double* values, const double* x, double* y, int* tiles, int* max_span);
+
+/* CPU self-check of the part-resident PCG kernel's layout: builds it for the upper BSR
+ * (parts parts, cut by coords -- 3 doubles per row -- or, when coords is NULL, as
+ * contiguous row ranges), fills the block stream as the device fill does (float
+ * storage) and evaluates y = A x by decoding the tiles exactly as the kernel's lanes read
+ * them.  info (may be NULL) receives {parts, largest window, most tiles in a part, stream
+ * KiB}.  PK_ERR_UNSUPPORTED when the layout does not apply (a window or a row too large).
+ * No counterpart in the reference (it checks this library's own layout). */
+PKCUDA_API int pk_slab_plan_selfcheck(int n, const int* row_start, const int* col_index, const double* values,
+                                      const double* x, const double* coords, int parts, double* y, int* info);
 
 /* Builds the transposed index of an upper BSR: for row r the blocks (c, r), c < r.
  * lt_start[n+1]; lt_row / lt_block sized nnz - n.  Host-only, no device needed. */

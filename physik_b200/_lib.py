@@ -91,9 +91,11 @@ _SIGS = {
     "pk_system_set_batched": (_i, [_p, _i]),
     "pk_system_segment_stats": (_i, [_p, _i, _p, _p, _p, _p]),
     "pk_ring_tiling_selfcheck": (_i, [_i, _i, _p, _p, _p, _p, _p, _p, _p]),
+    "pk_slab_plan_selfcheck": (_i, [_i, _p, _p, _p, _p, _p, _i, _p, _p]),
     "pk_system_set_graph": (_i, [_p, _i]),
     "pk_system_adjoint_step": (_i, [_p, C.POINTER(PkStepParams), _p, _p, _p, _p, _p]),
     "pk_system_autotune": (_i, [_p, C.POINTER(PkStepParams), _i, _p, _p]),
+    "pk_system_pcg_kernel": (_i, [_p, _p]),
     # physik_b200.h
     "PHYSIK_CreateWorld": (_p, []),
     "PHYSIK_DestroyWorld": (_v, [_p]),
@@ -162,6 +164,7 @@ _SIGS = {
     "PHYSIK_B200_AdjointStep": (_i, [_p, _f, _p, _p, _p, _p, _p]),
     "PHYSIK_B200_GetTetCount": (_i, [_p]),
     "PHYSIK_B200_Autotune": (_i, [_p, _i, _p]),
+    "PHYSIK_B200_GetPcgKernel": (_i, [_p, _p]),
     "PHYSIK_B200_GetBodyConjugateGradientStats": (_i, [_p, _H, _p, _p, _p, _p]),
     "PHYSIK_B200_GetStream": (_p, [_p]),
     "PHYSIK_B200_Synchronize": (_i, [_p]),
@@ -178,6 +181,7 @@ PX = physik
 
 # include/pkcuda.h constants
 PK_PREC_FP32, PK_PREC_MIXED, PK_PREC_FP64 = 0, 1, 2
+PK_ERR_UNSUPPORTED = -5
 FLAG_PRECOMPUTE_FAILED = 0x1
 FLAG_SINGULAR_DIAG = 0x2
 FLAG_INVALID_RHS = 0x4

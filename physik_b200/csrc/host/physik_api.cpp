@@ -605,6 +605,13 @@ PHYSIK_B200_API int PHYSIK_B200_Autotune(PhysikWorldHandle world, int repeats, d
     return Guard([&] { return w->Autotune(repeats, bestSolveMs); }, -1);
 }
 
+PHYSIK_B200_API int PHYSIK_B200_GetPcgKernel(PhysikWorldHandle world, int* blocks)
+{
+    World* w = AsWorld(world);
+    if (!w) return -1;
+    return Guard([&] { return w->GetPcgKernel(blocks); }, -1);
+}
+
 PHYSIK_B200_API int PHYSIK_B200_SetPcgGrid(PhysikWorldHandle world, int grid)
 {
     World* w = AsWorld(world);

@@ -404,6 +404,8 @@ public:
     // current scene by timing `repeats` solves of the last assembled system (call after a
     // step).  Returns the chosen candidate index (see pk_system_autotune) or -1.
     int Autotune(int repeats, double* bestMs);
+    // PCG kernel of the last solve (see pk_system_pcg_kernel) and its block count.
+    int GetPcgKernel(int* blocks) const;
 
     // Device precision (extension).  Changing it rebuilds the device scene.
     void SetPrecision(Precision p);

@@ -877,6 +877,13 @@ void World::AdjointStep(float dt, const double* xbarNext, const double* vbarNext
     statsPending = false;
 }
 
+int World::GetPcgKernel(int* blocks) const
+{
+    if (blocks) *blocks = 0;
+    if (!scene || !scene->sys) return -1;
+    return pk_system_pcg_kernel(scene->sys, blocks);
+}
+
 int World::Autotune(int repeats, double* bestMs)
 {
     SyncStats();

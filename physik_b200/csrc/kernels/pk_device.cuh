@@ -362,6 +362,84 @@ __device__ bool group_exchange(ExSlot* slots, int stride, int members, int me, G
     return !(pb & (1 << 30)) && !*(volatile int*)&sync->err;
 }
 
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v)
+{
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid exchange through one arrival counter (sync->arrive, zero at launch; exchanges
+// numbered gen = 1, 2, ...): each block stores its partials in its slot of the buffer of
+// the generation's parity and adds one to the counter with release semantics; warp 0 of
+// every block waits (bounded) until the counter reaches gen * gridDim.x, then reads all
+// slots -- lane i the slots i, i + 32, ... in order -- and reduces them in a fixed shuffle
+// tree, so every block gets identical sums.  One poller warp per block on one address,
+// instead of one poller per slot.  The parity buffers keep a block that runs ahead from
+// overwriting a slot that another block has not read yet: to publish generation g + 2 it
+// must have seen every block publish g + 1, which each does only after reading g.
+template <class Acc, int N>
+__device__ bool count_exchange(ExSlot* slots, GridSync* sync, unsigned gen, Acc (&v)[N], int& bad, Acc* sh, int* shi)
+{
+    static_assert(N >= 1 && N <= 2, "two partials per slot");
+    block_sum_or<Acc, N>(v, bad, sh, shi);
+    const int G = gridDim.x, tid = threadIdx.x, lane = tid & 31;
+    if (G <= 1) return !*(volatile int*)&sync->err;
+    ExSlot* buf = slots + (gen & 1u) * (unsigned)G;
+    if (tid < 32) {
+        if (tid == 0) {
+            ExSlot* my = buf + blockIdx.x;
+            my->v0 = double(v[0]);
+            my->v1 = N > 1 ? double(v[N - 1]) : 0.0;
+            my->bad = bad;
+            __threadfence();
+            red_release_add(&sync->arrive, 1u);
+        }
+        const unsigned target = gen * (unsigned)G;
+        int fail = 0;
+        unsigned long long spins = 0;
+        while ((int)(ld_acquire(&sync->arrive) - target) < 0) {
+            if (++spins > kBarrierSpinLimit) {
+                atomicExch(&sync->err, 1);
+                fail = 1;
+                break;
+            }
+            if ((spins & 1023u) == 0 && *(volatile int*)&sync->err) {
+                fail = 1;
+                break;
+            }
+        }
+        fail = __any_sync(0xffffffffu, fail) ? 1 : 0;
+        Acc pv[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) pv[k] = Acc(0);
+        int pb = 0;
+        if (!fail) {
+            for (int i = lane; i < G; i += 32) {
+                pv[0] += Acc(__ldcg(&buf[i].v0));
+                if (N > 1) pv[N - 1] += Acc(__ldcg(&buf[i].v1));
+                pb |= __ldcg(&buf[i].bad);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) pv[k] += __shfl_xor_sync(0xffffffffu, pv[k], off);
+        pb = (int)__reduce_or_sync(0xffffffffu, (unsigned)pb);
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < N; ++k) sh[N * 32 + k] = pv[k];
+            shi[0] = pb;
+            shi[1] = fail;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = sh[N * 32 + k];
+    bad = shi[0];
+    const int failed = shi[1];
+    __syncthreads();
+    return !failed && !*(volatile int*)&sync->err;
+}
+
 // The whole grid as one group (slots: two buffers of gridDim.x).
 template <class Acc, int N>
 __device__ __forceinline__ bool grid_exchange(ExSlot* slots, GridSync* sync, unsigned gen, Acc (&v)[N], int& bad,

@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include "pk_math.cuh"
+#include "pk_slab_plan.h"
 
 namespace pk {
 
@@ -265,6 +266,56 @@ struct BatchPcgArgs {
     BatchBodyStats* body_stats;
 };
 
+// ------------------------------------------------------------------ part-resident PCG
+// The part-resident ("slab") PCG kernel (pk_pcg_slab.cu; layout in pk_slab_plan.h): one
+// block per part, FP32 storage.  Shared memory: the window's search directions
+// (kSlabWinCap x 3 floats), the ring of kSlabStages tile stages, the part's tile table.
+constexpr int kSlabGroups = 3;
+constexpr int kSlabGroupWarps = 4;
+constexpr int kSlabConsumerWarps = kSlabGroups * kSlabGroupWarps;
+constexpr int kSlabThreads = 32 * (kSlabConsumerWarps + 1);  // + one producer warp
+constexpr size_t kSlabWinBytes = 12 * size_t(kSlabWinCap);
+constexpr size_t kSlabRingOffset = kSlabWinBytes;
+constexpr size_t kSlabTableOffset = kSlabRingOffset + size_t(kSlabStages) * kSlabStageBytes;
+constexpr size_t kSlabSmemBytes = kSlabTableOffset + 16 * size_t(kSlabMaxTiles);
+static_assert(kSlabStages % kSlabGroups == 0, "a stage must always return to the same consumer group");
+static_assert(kSlabWinBytes % 128 == 0 && kSlabStageBytes % 128 == 0, "stages must stay 128-byte aligned");
+static_assert(kSlabSmemBytes + 2048 <= 232448, "dynamic + static shared memory must fit one block per SM");
+static_assert(kSlabRows * kSlabLanesPerRow == 32 * kSlabGroupWarps, "one tile row per lane group");
+
+template <class Acc>
+struct SlabPcgArgs {
+    int n;                       // dynamic rows
+    const int* part_info;        // kSlabPartInts per block
+    const int4* tile_desc;       // per tile: stream offset / 16, bytes, first local row, rows
+    int tile_count;
+    int halo_count;
+    const unsigned char* stream;
+    unsigned long long stream_bytes;
+    const int* halo_src;         // slab index of each halo row
+    const int* perm;             // slab index -> dynamic row
+    const float* b;              // per dynamic row
+    const float* minv;
+    float* x;                    // per dynamic row: delta-v out
+    float* xs;                   // 4 per slab row
+    float* rs;
+    float* qs;
+    float* ss;
+    float* minvs;                // 12 per slab row (three padded columns)
+    ExSlot* slots;               // [2][grid]
+    GridSync* sync;
+    int max_iterations;
+    Acc tolerance;
+    int skip_on_flags;
+    int integrate;
+    float dt;
+    const int* dyn_to_node;
+    float* node_x;
+    float* node_v;
+    unsigned* flags;
+    DevStats* stats;
+};
+
 // ------------------------------------------------------------------ adjoint step
 // Backward element kernel (pk_adjoint.cu): per tet, the sensitivities of
 // J = dt w.f(x) - dt^2 w.K(x) z to the tet's node positions (12 doubles) and to its
@@ -312,6 +363,15 @@ template <class Real, class Acc>
 cudaError_t launch_pcg_ring_kernel(const RingPcgArgs<Real, Acc>& args, int grid, cudaStream_t stream);
 template <class Real, class Acc>
 int pcg_ring_max_grid();
+
+// Part-resident PCG (pk_pcg_slab.cu): cooperative, one block of kSlabThreads per part.
+template <class Acc>
+cudaError_t launch_pcg_slab_kernel(const SlabPcgArgs<Acc>& args, int grid, cudaStream_t stream);
+template <class Acc>
+int pcg_slab_max_grid();
+// Writes the assembled upper blocks and their transposes into the slab stream.
+cudaError_t launch_slab_fill_kernel(const float* values, int nnz, const unsigned* pos_u, const unsigned* pos_l,
+                                    float* stream, unsigned long long stream_floats, cudaStream_t stream_);
 
 constexpr int kPcgThreads = 512;
 

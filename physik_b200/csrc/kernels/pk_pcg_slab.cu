@@ -1,0 +1,622 @@
+// pk_pcg_slab.cu -- the part-resident cooperative block-Jacobi PCG kernel.
+//
+// The same solve as the other PCG kernels (SolvePreconditionedConjugateGradient,
+// src/Core/Solvers/Linear/ConjugateGradientSolver.cpp:114-241, with the SpMV of
+// SparseBlockMatrix::Multiply, src/Math/SparseBlockMatrix.cpp:209-268, and
+// World::IntegrateImplicitEuler, src/Core/World/World.cpp:644-695, fused at the end), for
+// FP32 storage, laid out so that HBM only streams the matrix:
+//
+// * One block per part (pk_slab_plan.h).  The search directions d of the part's window
+//   (its rows, then its halo) stay in shared memory for the whole solve.  At the start of
+//   an iteration every block rebuilds its window as d = s + beta d from the s values the
+//   rows' owners published (s of the halo rows comes from the neighbouring parts), so
+//   the SpMV reads d only from shared memory.
+// * The part's rows are streamed as tiles of full symmetric rows (upper blocks and the
+//   transposes of the lower ones, 16-bit window columns) by one producer warp, one TMA
+//   bulk copy per tile into a ring of stages, with an L2 evict-first policy so the
+//   streamed matrix does not push the CG vectors out of L2.  The producer runs ahead
+//   into the next iteration's first tiles while the block exchanges and updates.
+// * Three consumer groups of four warps take every third ring position; four lanes per
+//   row, up to four blocks per lane in flight.  Per row the products are summed lane by lane and then in a fixed shuffle tree,
+//   the partial dot products of every phase in a fixed block tree, and the grid
+//   exchange reduces the blocks' partials in one fixed tree that every block evaluates
+//   identically: all blocks take the same decisions and a run repeats bit for bit.
+//
+// Vectors x, r, q, s are kept per slab row (float4) and M^-1 as three padded columns, so
+// the per-row phases read them coalesced.  Every wait is bounded; a wait that gives up
+// sets the error flag and the kernel leaves through its normal exit, after waiting
+// (bounded) for its own bulk copies still in flight.  No TMA multicast is used.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "pk_device.cuh"
+
+namespace pk {
+namespace {
+
+__device__ __forceinline__ void mbar_arrive_slab(unsigned long long* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ unsigned long long l2_evict_first_policy()
+{
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+// Bulk copy global -> shared with an L2 cache-policy hint (no multicast).
+__device__ __forceinline__ void bulk_g2s_hint(void* dst, const void* src, unsigned bytes, unsigned long long* bar,
+                                              unsigned long long pol)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::
+            "r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(pol)
+        : "memory");
+}
+
+__device__ __forceinline__ V3<float> ldv4(const float* p)
+{
+    const float4 a = __ldcg(reinterpret_cast<const float4*>(p));
+    return V3<float>{a.x, a.y, a.z};
+}
+__device__ __forceinline__ void stv4(float* p, V3<float> v)
+{
+    __stcg(reinterpret_cast<float4*>(p), make_float4(v.x, v.y, v.z, 0.f));
+}
+// M^-1 of a slab row: three padded columns.
+__device__ __forceinline__ M3<float> ldm12(const float* p)
+{
+    const float4 a = __ldcg(reinterpret_cast<const float4*>(p));
+    const float4 b = __ldcg(reinterpret_cast<const float4*>(p) + 1);
+    const float4 c = __ldcg(reinterpret_cast<const float4*>(p) + 2);
+    M3<float> m;
+    m.c[0] = V3<float>{a.x, a.y, a.z};
+    m.c[1] = V3<float>{b.x, b.y, b.z};
+    m.c[2] = V3<float>{c.x, c.y, c.z};
+    return m;
+}
+__device__ __forceinline__ void stm12(float* p, const M3<float>& m)
+{
+    __stcg(reinterpret_cast<float4*>(p), make_float4(m.c[0].x, m.c[0].y, m.c[0].z, 0.f));
+    __stcg(reinterpret_cast<float4*>(p) + 1, make_float4(m.c[1].x, m.c[1].y, m.c[1].z, 0.f));
+    __stcg(reinterpret_cast<float4*>(p) + 2, make_float4(m.c[2].x, m.c[2].y, m.c[2].z, 0.f));
+}
+
+template <class Acc>
+__global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<Acc> P)
+{
+    constexpr int S = kSlabStages;
+    constexpr int LPR = kSlabLanesPerRow;
+    extern __shared__ __align__(128) unsigned char dyn[];
+    __shared__ __align__(8) unsigned long long full_bar[S];
+    __shared__ __align__(8) unsigned long long empty_bar[S];
+    __shared__ Acc sh_acc[3 * 32];
+    __shared__ int sh_int[32];
+    __shared__ int s_fail;
+    __shared__ int s_bad;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, blk = blockIdx.x;
+    const bool producer = warp == kSlabConsumerWarps;
+    const bool consumer = warp < kSlabConsumerWarps;
+    const int group = warp / kSlabGroupWarps;
+    const int slot_row = ((warp % kSlabGroupWarps) * 32 + lane) / LPR;  // tile row of this lane
+    const int sub = lane % LPR;
+    float* win = reinterpret_cast<float*>(dyn);  // 3 floats per window row
+    unsigned char* ring_base = dyn + kSlabRingOffset;
+    int4* table = reinterpret_cast<int4*>(dyn + kSlabTableOffset);
+
+    // The part: rows [row0, row0 + m) of the slab order, halo rows halo_src[halo0 ..
+    // halo0 + h), tiles [tile0, tile0 + ntiles).  A part that does not fit the block's
+    // tables (the host never builds one) is emptied and reports a breakdown.
+    int row0, m, halo0, h, tile0, ntiles;
+    {
+        const int4 a = __ldg(reinterpret_cast<const int4*>(P.part_info) + 2 * blk);
+        const int4 b = __ldg(reinterpret_cast<const int4*>(P.part_info) + 2 * blk + 1);
+        row0 = a.x;
+        m = a.y;
+        halo0 = a.z;
+        h = a.w;
+        tile0 = b.x;
+        ntiles = b.y;
+    }
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], kSlabGroupWarps);
+        }
+        mbar_fence_init();
+        s_fail = 0;
+        s_bad = 0;
+    }
+    __syncthreads();
+    if (m < 0 || h < 0 || m + h > kSlabWinCap || row0 < 0 || row0 + m > P.n || ntiles < 0 ||
+        ntiles > kSlabMaxTiles || halo0 < 0 || halo0 + h > P.halo_count || tile0 < 0 ||
+        tile0 + ntiles > P.tile_count) {
+        m = h = ntiles = 0;
+        row0 = 0;
+        if (tid == 0) s_bad = 1;
+    }
+    const int wn = m + h;
+    // Tile descriptors, checked once: a bad one (never built by the host) becomes an empty
+    // tile and reports a breakdown.
+    for (int i = tid; i < ntiles; i += blockDim.x) {
+        int4 d = __ldg(P.tile_desc + tile0 + i);
+        const int ne = (d.y - kSlabHeaderBytes) / kSlabEntryBytes;
+        const bool ok = d.x >= 0 && d.y >= kSlabHeaderBytes && d.y <= kSlabStageBytes && (d.y & 15) == 0 &&
+                        d.y == kSlabHeaderBytes + kSlabEntryBytes * ne && ne <= kSlabCapE && d.w >= 1 &&
+                        d.w <= kSlabRows && d.z >= 0 && d.z + d.w <= m &&
+                        16ull * (unsigned long long)d.x + (unsigned long long)d.y <= P.stream_bytes;
+        if (!ok) {
+            d = make_int4(0, 0, 0, 0);
+            s_bad = 1;
+        }
+        table[i] = d;
+    }
+    __syncthreads();
+
+    const unsigned in_flags = *(volatile unsigned*)P.flags;
+    if (P.skip_on_flags && (in_flags & (kFlagPrecomputeFailed | kFlagSingularDiag))) {
+        if (blk == 0 && tid == 0) {
+            P.stats->iterations = 0;
+            P.stats->converged = 0;
+            P.stats->residual_norm = 0.0;
+        }
+        return;
+    }
+
+    const unsigned long long pol = l2_evict_first_policy();
+    unsigned ring = 0;    // ring positions consumed so far (ntiles per iteration)
+    unsigned issued = 0;  // ring positions issued by the producer (producer lane 0 only)
+    unsigned xgen = 0;
+
+    // Phase A: q = A d for the part's rows (d from the window), partial d.q.
+    auto phase_a = [&](Acc& dq, int& qbad) {
+        if (ntiles == 0) return;
+        if (producer) {
+            if (lane == 0) {
+                // This iteration's tiles, then the next iteration's first ones.
+                const unsigned end = ring + (unsigned)ntiles + (unsigned)min(S, ntiles);
+                for (; issued < end; ++issued) {
+                    const unsigned p = issued;
+                    const int s = (int)(p % S);
+                    const unsigned u = p / S;
+                    if (u > 0 && !mbar_wait(&empty_bar[s], (u - 1) & 1u)) {
+                        s_fail = 1;
+                        break;
+                    }
+                    const int4 d = table[p % (unsigned)ntiles];
+                    mbar_arrive_expect_tx(&full_bar[s], (unsigned)d.y);
+                    if (d.y > 0)
+                        bulk_g2s_hint(ring_base + (size_t)s * kSlabStageBytes, P.stream + 16 * (size_t)d.x,
+                                      (unsigned)d.y, &full_bar[s], pol);
+                }
+            }
+            __syncwarp();
+        } else if (consumer) {
+            const float* wv = win;
+            const int wmax = max(wn - 1, 0);
+            const unsigned first = ring + (unsigned)((group - (int)(ring % kSlabGroups) + kSlabGroups) % kSlabGroups);
+            for (unsigned p = first; p < ring + (unsigned)ntiles; p += kSlabGroups) {
+                const int s = (int)(p % S);
+                const unsigned u = p / S;
+                if (!mbar_wait(&full_bar[s], u & 1u)) {
+                    s_fail = 1;
+                    break;
+                }
+                const int4 d = table[p - ring];
+                const unsigned char* st = ring_base + (size_t)s * kSlabStageBytes;
+                const int ne = d.y > 0 ? (d.y - kSlabHeaderBytes) / kSlabEntryBytes : 0;
+                const unsigned short* roff = reinterpret_cast<const unsigned short*>(st);
+                const float* vals = reinterpret_cast<const float*>(st + kSlabHeaderBytes);
+                const unsigned short* lcol = reinterpret_cast<const unsigned short*>(st + kSlabHeaderBytes + 36 * ne);
+                const bool valid = slot_row < d.w;
+                int e0 = 0, e1 = 0;
+                if (valid) {
+                    e0 = min((int)roff[slot_row], ne);
+                    e1 = min((int)roff[slot_row + 1], ne);
+                }
+                V3<float> acc{0.f, 0.f, 0.f};
+                // kEntries independent entries per lane per pass, every load issued before
+                // the products; a dead slot re-reads the pass's first entry and adds nothing.
+                constexpr int kEntries = 4;
+                for (int j0 = e0 + sub; j0 < e1; j0 += kEntries * LPR) {
+                    int jj[kEntries];
+                    bool live[kEntries];
+#pragma unroll
+                    for (int q = 0; q < kEntries; ++q) {
+                        jj[q] = j0 + q * LPR;
+                        live[q] = jj[q] < e1;
+                        if (!live[q]) jj[q] = j0;
+                    }
+                    float xv[kEntries][3], bv[kEntries][9];
+#pragma unroll
+                    for (int q = 0; q < kEntries; ++q) {
+                        const int c = 3 * min((int)lcol[jj[q]], wmax);
+                        xv[q][0] = wv[c];
+                        xv[q][1] = wv[c + 1];
+                        xv[q][2] = wv[c + 2];
+#pragma unroll
+                        for (int e = 0; e < 9; ++e) bv[q][e] = vals[9 * jj[q] + e];
+                    }
+#pragma unroll
+                    for (int q = 0; q < kEntries; ++q) {
+                        // Column-major block: element (i, c) is v[3c + i].
+                        const float* v = bv[q];
+                        if (live[q]) {
+                            acc.x += v[0] * xv[q][0] + v[3] * xv[q][1] + v[6] * xv[q][2];
+                            acc.y += v[1] * xv[q][0] + v[4] * xv[q][1] + v[7] * xv[q][2];
+                            acc.z += v[2] * xv[q][0] + v[5] * xv[q][1] + v[8] * xv[q][2];
+                        }
+                    }
+                }
+#pragma unroll
+                for (int off = LPR / 2; off > 0; off >>= 1) {
+                    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+                    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
+                    acc.z += __shfl_xor_sync(0xffffffffu, acc.z, off);
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive_slab(&empty_bar[s]);  // this warp is done with the stage
+                if (valid && sub == 0) {
+                    const int li = d.z + slot_row;
+                    stv4(P.qs + 4 * (size_t)(row0 + li), acc);
+                    dq += dot_acc<Acc>(V3<float>{wv[3 * li], wv[3 * li + 1], wv[3 * li + 2]}, acc);
+                    if (!finite3(acc)) qbad = 1;
+                }
+            }
+        }
+        ring += (unsigned)ntiles;
+    };
+
+    unsigned fl = 0;
+    int iterations = 0;
+    bool converged = false;
+    Acc residual = Acc(0);
+    bool have_x = true;
+    bool timed_out = false;
+    Acc delta = Acc(0), rr = Acc(0), target = Acc(0);
+    {
+        // x = 0, r = b, s = M^-1 r (slab order), d = 0 in the window; r.s, |r|^2, finiteness.
+        Acc v[2] = {Acc(0), Acc(0)};
+        int bad = s_bad ? 4 : 0;
+        for (int i = tid; i < m; i += blockDim.x) {
+            const int g = row0 + i;
+            int c = __ldg(P.perm + g);
+            if ((unsigned)c >= (unsigned)P.n) {
+                c = 0;
+                bad |= 4;
+            }
+            const V3<float> br = ld3(P.b, c);
+            if (!finite3(br)) bad |= 1;
+            const M3<float> mi = ld9(P.minv, (size_t)c);
+            const V3<float> sv = mul(mi, br);
+            if (!finite9(mi) || !finite3(sv)) bad |= 2;
+            stv4(P.xs + 4 * (size_t)g, V3<float>{0.f, 0.f, 0.f});
+            stv4(P.rs + 4 * (size_t)g, br);
+            stv4(P.ss + 4 * (size_t)g, sv);
+            stm12(P.minvs + 12 * (size_t)g, mi);
+            v[0] += dot_acc<Acc>(br, sv);
+            v[1] += dot_acc<Acc>(br, br);
+        }
+        for (int w = tid; w < 3 * wn; w += blockDim.x) win[w] = 0.f;
+        if (!count_exchange<Acc, 2>(P.slots, P.sync, ++xgen, v, bad, sh_acc, sh_int)) {
+            timed_out = true;
+            goto finish;
+        }
+        delta = v[0];
+        rr = v[1];
+        if (bad & 4) {  // a malformed layout: report, do not solve
+            have_x = false;
+            fl |= kFlagBreakdown;
+            goto final_check;
+        }
+        if (bad & 1) {  // non-finite rhs: the reference clears x (the solve fails)
+            have_x = false;
+            fl |= kFlagInvalidRhs;
+            goto final_check;
+        }
+        if (P.max_iterations <= 0 || !acc_finite(P.tolerance) || P.tolerance <= Acc(0)) {
+            have_x = false;
+            fl |= kFlagInvalidRhs;
+            goto final_check;
+        }
+        if (bad & 2) goto final_check;  // preconditioner output not finite: x stays 0
+        if (!acc_finite(delta) || delta < Acc(0)) goto final_check;
+        target = P.tolerance * P.tolerance * delta;
+        if (!acc_finite(target)) goto final_check;
+    }
+    if (delta <= target) {
+        converged = true;
+        residual = (acc_finite(rr) && rr >= Acc(0)) ? sqrt(rr) : Acc(INFINITY);
+        goto final_check;
+    }
+    {
+        Acc beta = Acc(0);
+        for (int it = 0; it < P.max_iterations; ++it) {
+            if (delta <= target) {
+                converged = true;
+                break;
+            }
+            // Window: d = s + beta d, s from the rows' owners.
+            {
+                // kWinBatch entries per thread per pass: their halo indices, then their s
+                // values are all in flight before any is used.
+                constexpr int kWinBatch = 8;
+                const float bt = float(beta);
+                const int step = (int)blockDim.x;
+                int wbad = 0;
+                for (int w0 = tid; w0 < wn; w0 += kWinBatch * step) {
+                    int g[kWinBatch];
+#pragma unroll
+                    for (int k = 0; k < kWinBatch; ++k) {
+                        const int w = w0 + k * step;
+                        int gi = 0;
+                        if (w < wn) gi = w < m ? row0 + w : __ldg(P.halo_src + halo0 + (w - m));
+                        if ((unsigned)gi >= (unsigned)P.n) {
+                            gi = 0;
+                            wbad = 1;
+                        }
+                        g[k] = gi;
+                    }
+                    float4 sv[kWinBatch];
+#pragma unroll
+                    for (int k = 0; k < kWinBatch; ++k) sv[k] = __ldcg(reinterpret_cast<const float4*>(P.ss) + g[k]);
+#pragma unroll
+                    for (int k = 0; k < kWinBatch; ++k) {
+                        const int w = w0 + k * step;
+                        if (w < wn) {
+                            float* d = win + 3 * w;
+                            d[0] = sv[k].x + d[0] * bt;
+                            d[1] = sv[k].y + d[1] * bt;
+                            d[2] = sv[k].z + d[2] * bt;
+                        }
+                    }
+                }
+                if (wbad) s_bad = 1;
+            }
+            __syncthreads();
+            Acc dq[1] = {Acc(0)};
+            int qbad = 0;
+            phase_a(dq[0], qbad);
+            if (s_bad) qbad = 1;
+            if (s_fail) {
+                qbad = 1;
+                atomicExch(&P.sync->err, 1);
+            }
+            if (!count_exchange<Acc, 1>(P.slots, P.sync, ++xgen, dq, qbad, sh_acc, sh_int)) {
+                timed_out = true;
+                goto finish;
+            }
+            if (qbad) {
+                fl |= kFlagBreakdown;
+                break;
+            }
+            if (!acc_finite(dq[0]) || dq[0] <= Acc(0)) {
+                fl |= kFlagBreakdown;
+                break;
+            }
+            const Acc alpha = delta / dq[0];
+            if (!acc_finite(alpha)) {
+                fl |= kFlagBreakdown;
+                break;
+            }
+            // Phase B: x += alpha d; r -= alpha q; s = M^-1 r; partials r.s and r.r.
+            // kRowBatch rows per thread per pass, all their loads issued before any store.
+            Acc v[2] = {Acc(0), Acc(0)};
+            int sbad = 0;
+            {
+                constexpr int kRowBatch = 2;
+                const int step = (int)blockDim.x;
+                for (int i0 = tid; i0 < m; i0 += kRowBatch * step) {
+                    int li[kRowBatch];
+                    bool ok[kRowBatch];
+#pragma unroll
+                    for (int k = 0; k < kRowBatch; ++k) {
+                        const int i = i0 + k * step;
+                        ok[k] = i < m;
+                        li[k] = ok[k] ? i : i0;
+                    }
+                    V3<float> dn[kRowBatch], q[kRowBatch], xo[kRowBatch], ro[kRowBatch];
+                    M3<float> mi[kRowBatch];
+#pragma unroll
+                    for (int k = 0; k < kRowBatch; ++k) {
+                        const size_t g = (size_t)(row0 + li[k]);
+                        const float* d = win + 3 * li[k];
+                        dn[k] = V3<float>{d[0], d[1], d[2]};
+                        q[k] = ldv4(P.qs + 4 * g);
+                        xo[k] = ldv4(P.xs + 4 * g);
+                        ro[k] = ldv4(P.rs + 4 * g);
+                        mi[k] = ldm12(P.minvs + 12 * g);
+                    }
+#pragma unroll
+                    for (int k = 0; k < kRowBatch; ++k) {
+                        if (!ok[k]) continue;
+                        const size_t g = (size_t)(row0 + li[k]);
+                        const V3<float> xv = axpy<float, Acc>(xo[k], alpha, dn[k]);
+                        const V3<float> rv = axpy<float, Acc>(ro[k], -alpha, q[k]);
+                        stv4(P.xs + 4 * g, xv);
+                        stv4(P.rs + 4 * g, rv);
+                        const V3<float> sv = mul(mi[k], rv);
+                        if (!finite3(sv)) sbad = 1;
+                        stv4(P.ss + 4 * g, sv);
+                        v[0] += dot_acc<Acc>(rv, sv);
+                        v[1] += dot_acc<Acc>(rv, rv);
+                    }
+                }
+            }
+            if (!count_exchange<Acc, 2>(P.slots, P.sync, ++xgen, v, sbad, sh_acc, sh_int)) {
+                timed_out = true;
+                goto finish;
+            }
+            rr = v[1];
+            if (sbad) {
+                fl |= kFlagBreakdown;
+                break;
+            }
+            const Acc old = delta;
+            delta = v[0];
+            if (!acc_finite(delta) || !acc_finite(old) || old <= Acc(0)) {
+                fl |= kFlagBreakdown;
+                break;
+            }
+            beta = delta / old;
+            if (!acc_finite(beta)) {
+                fl |= kFlagBreakdown;
+                break;
+            }
+            iterations = it + 1;
+        }
+        if (delta <= target) converged = true;
+        residual = (acc_finite(rr) && rr >= Acc(0)) ? sqrt(rr) : Acc(INFINITY);
+    }
+
+final_check:
+    // delta-v back in dynamic-row order; the solve succeeds when it is present and
+    // finite; integration is all-or-nothing.
+    {
+        int bad = 0;
+        Acc none[1] = {Acc(0)};
+        for (int i = tid; i < m; i += blockDim.x) {
+            const int g = row0 + i;
+            const int c = __ldg(P.perm + g);
+            if ((unsigned)c >= (unsigned)P.n) {
+                bad |= 1;
+                continue;
+            }
+            const V3<float> dv = have_x ? ldv4(P.xs + 4 * (size_t)g) : V3<float>{0.f, 0.f, 0.f};
+            st3(P.x, c, dv);
+            if (!finite3(dv)) bad |= 1;
+            if (P.integrate) {
+                const int node = __ldg(P.dyn_to_node + c);
+                const V3<float> xo = ldplain3(P.node_x, node), vo = ldplain3(P.node_v, node);
+                const V3<float> nv = vo + dv;
+                const V3<float> nx = xo + nv * P.dt;
+                if (!finite3(xo) || !finite3(vo) || !finite3(nv) || !finite3(nx)) bad |= 2;
+            }
+        }
+        if (!count_exchange<Acc, 1>(P.slots, P.sync, ++xgen, none, bad, sh_acc, sh_int)) {
+            timed_out = true;
+            goto finish;
+        }
+        const bool solved = have_x && !(bad & 1);
+        if (!have_x && !(fl & kFlagBreakdown)) fl |= kFlagInvalidRhs;
+        if (have_x && (bad & 1)) fl |= kFlagNonFiniteDv;
+        if (solved) fl |= kFlagSolved;
+        if (solved && P.integrate) {
+            if (bad & 2) {
+                fl |= kFlagIntegrateAbort;
+            } else {
+                for (int i = tid; i < m; i += blockDim.x) {
+                    const int g = row0 + i;
+                    const int c = __ldg(P.perm + g);
+                    const int node = __ldg(P.dyn_to_node + c);
+                    const V3<float> dv = ldv4(P.xs + 4 * (size_t)g);
+                    const V3<float> nv = ldplain3(P.node_v, node) + dv;
+                    const V3<float> nx = ldplain3(P.node_x, node) + nv * P.dt;
+                    st3(P.node_v, node, nv);
+                    st3(P.node_x, node, nx);
+                }
+                fl |= kFlagIntegrated;
+            }
+        }
+        if (converged) fl |= kFlagConverged;
+    }
+
+finish:
+    if (timed_out) fl |= kFlagBarrierTimeout;
+    // Bulk copies issued ahead (the next iteration's first tiles) or cut short by a
+    // timeout must land before the block exits: wait for the last S positions issued.
+    if (producer && lane == 0) {
+        for (unsigned k = 0; k < (unsigned)S && k < issued; ++k) {
+            const unsigned p = issued - 1 - k;
+            (void)mbar_wait(&full_bar[p % S], (p / S) & 1u);
+        }
+    }
+    if (blk == 0 && tid == 0) {
+        P.stats->iterations = iterations;
+        P.stats->converged = converged ? 1 : 0;
+        P.stats->residual_norm = (double)residual;
+        atomicOr(P.flags, fl);
+    } else if (timed_out && tid == 0) {
+        atomicOr(P.flags, kFlagBarrierTimeout);
+    }
+}
+
+// One thread per canonical upper block: its copy and its transpose into the stream.
+__global__ void slab_fill_kernel(const float* __restrict__ values, int nnz, const unsigned* __restrict__ pos_u,
+                                 const unsigned* __restrict__ pos_l, float* __restrict__ out,
+                                 unsigned long long out_floats)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nnz) return;
+    float v[9];
+    const float* src = values + 9 * (size_t)k;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) v[e] = __ldg(src + e);
+    const unsigned pu = __ldg(pos_u + k), pl = __ldg(pos_l + k);
+    if (pu != kSlabNoPos && (unsigned long long)pu + 9 <= out_floats) {
+        float* d = out + pu;
+#pragma unroll
+        for (int e = 0; e < 9; ++e) d[e] = v[e];
+    }
+    if (pl != kSlabNoPos && (unsigned long long)pl + 9 <= out_floats) {
+        float* d = out + pl;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) d[3 * c + i] = v[3 * i + c];
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ launchers
+template <class Acc>
+static cudaError_t slab_prepare()
+{
+    return cudaFuncSetAttribute(pcg_slab_kernel<Acc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(kSlabSmemBytes));
+}
+
+template <class Acc>
+int pcg_slab_max_grid()
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if (slab_prepare<Acc>() != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_slab_kernel<Acc>, kSlabThreads, kSlabSmemBytes) !=
+        cudaSuccess)
+        return 0;
+    return sms * per_sm;
+}
+
+template <class Acc>
+cudaError_t launch_pcg_slab_kernel(const SlabPcgArgs<Acc>& args, int grid, cudaStream_t stream)
+{
+    SlabPcgArgs<Acc> a = args;
+    void* kargs[] = {&a};
+    cudaError_t e = slab_prepare<Acc>();
+    if (e != cudaSuccess) return e;
+    return cudaLaunchCooperativeKernel((const void*)pcg_slab_kernel<Acc>, dim3(grid), dim3(kSlabThreads), kargs,
+                                       kSlabSmemBytes, stream);
+}
+
+cudaError_t launch_slab_fill_kernel(const float* values, int nnz, const unsigned* pos_u, const unsigned* pos_l,
+                                    float* out, unsigned long long out_floats, cudaStream_t stream)
+{
+    if (nnz <= 0) return cudaSuccess;
+    const int threads = 256;
+    slab_fill_kernel<<<(nnz + threads - 1) / threads, threads, 0, stream>>>(values, nnz, pos_u, pos_l, out,
+                                                                             out_floats);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_pcg_slab_kernel<float>(const SlabPcgArgs<float>&, int, cudaStream_t);
+template cudaError_t launch_pcg_slab_kernel<double>(const SlabPcgArgs<double>&, int, cudaStream_t);
+template int pcg_slab_max_grid<float>();
+template int pcg_slab_max_grid<double>();
+
+}  // namespace pk

@@ -1,0 +1,266 @@
+// pk_slab_plan.cpp -- builds the part-resident PCG kernel's layout (see pk_slab_plan.h).
+#include "pk_slab_plan.h"
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <numeric>
+
+namespace pk {
+namespace {
+
+// Recursive coordinate bisection of ids[lo, hi) into `nparts` parts numbered from part0:
+// split across the widest axis of the bounding box at the weighted position that gives
+// the two halves weight in proportion to their part counts.  Ties break by row id, so
+// the result depends only on the inputs.
+void rcb(std::vector<int>& ids, size_t lo, size_t hi, int part0, int nparts, const double* xyz,
+         const std::vector<double>& w, std::vector<int>& part_of)
+{
+    if (nparts <= 1 || hi - lo <= 1) {
+        for (size_t i = lo; i < hi; ++i) part_of[ids[i]] = part0;
+        return;
+    }
+    double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+    for (size_t i = lo; i < hi; ++i)
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = std::min(mn[a], xyz[3 * (size_t)ids[i] + a]);
+            mx[a] = std::max(mx[a], xyz[3 * (size_t)ids[i] + a]);
+        }
+    int ax = 0;
+    for (int a = 1; a < 3; ++a)
+        if (mx[a] - mn[a] > mx[ax] - mn[ax]) ax = a;
+    std::sort(ids.begin() + lo, ids.begin() + hi, [&](int a, int b) {
+        const double ca = xyz[3 * (size_t)a + ax], cb = xyz[3 * (size_t)b + ax];
+        return ca < cb || (ca == cb && a < b);
+    });
+    const int left = nparts / 2;
+    double total = 0.0;
+    for (size_t i = lo; i < hi; ++i) total += w[ids[i]];
+    const double target = total * left / nparts;
+    size_t cut = lo;
+    double acc = 0.0;
+    while (cut < hi && acc + 0.5 * w[ids[cut]] < target) acc += w[ids[cut++]];
+    // keep at least one row per part on each side when possible
+    const size_t rows = hi - lo;
+    if (rows >= (size_t)nparts) {
+        cut = std::max(cut, lo + (size_t)left);
+        cut = std::min(cut, hi - (size_t)(nparts - left));
+    }
+    rcb(ids, lo, cut, part0, left, xyz, w, part_of);
+    rcb(ids, cut, hi, part0 + left, nparts - left, xyz, w, part_of);
+}
+
+inline void put_u16(std::vector<unsigned char>& s, size_t off, unsigned v)
+{
+    const uint16_t x = static_cast<uint16_t>(v);
+    std::memcpy(s.data() + off, &x, 2);
+}
+inline unsigned get_u16(const std::vector<unsigned char>& s, size_t off)
+{
+    uint16_t x;
+    std::memcpy(&x, s.data() + off, 2);
+    return x;
+}
+
+}  // namespace
+
+std::string build_slab_plan(int n, const int* row_start, const int* col, const int* lt_start, const int* lt_row,
+                            const int* lt_block, const double* coords, int parts, SlabPlan& out)
+{
+    out = SlabPlan{};
+    if (n <= 0 || parts <= 0) return "empty system";
+    parts = std::min(parts, n);
+    const int nnz = row_start[n];
+    std::vector<int> len(n);
+    for (int r = 0; r < n; ++r) len[r] = (row_start[r + 1] - row_start[r]) + (lt_start[r + 1] - lt_start[r]);
+    for (int r = 0; r < n; ++r)
+        if (len[r] > kSlabCapE) return "a row has more blocks than a tile holds";
+
+    // 1. parts
+    std::vector<int> part_of(n, 0);
+    std::vector<double> w(n);
+    for (int r = 0; r < n; ++r) w[r] = len[r] + 4.0;  // streamed blocks + per-row vector work
+    if (coords) {
+        std::vector<int> ids(n);
+        std::iota(ids.begin(), ids.end(), 0);
+        rcb(ids, 0, (size_t)n, 0, parts, coords, w, part_of);
+    } else {
+        const double total = std::accumulate(w.begin(), w.end(), 0.0);
+        double acc = 0.0;
+        for (int r = 0; r < n; ++r) {
+            part_of[r] = std::min(parts - 1, static_cast<int>(acc * parts / total));
+            acc += w[r];
+        }
+    }
+    // 2. slab order: parts in order, rows ascending inside a part
+    std::vector<int> count(parts + 1, 0);
+    for (int r = 0; r < n; ++r) ++count[part_of[r] + 1];
+    for (int p = 0; p < parts; ++p) count[p + 1] += count[p];
+    for (int p = 0; p < parts; ++p)
+        if (count[p + 1] == count[p]) return "a part has no rows";
+    out.perm.assign(n, 0);
+    std::vector<int> inv(n);
+    {
+        std::vector<int> fill(count.begin(), count.end() - 1);
+        for (int r = 0; r < n; ++r) {
+            const int g = fill[part_of[r]]++;
+            out.perm[g] = r;
+            inv[r] = g;
+        }
+    }
+    out.n = n;
+    out.parts = parts;
+    out.part_info.assign((size_t)kSlabPartInts * parts, 0);
+    out.pos_u.assign(nnz, kSlabNoPos);
+    out.pos_l.assign(nnz, kSlabNoPos);
+
+    // 3. per part: halo, window indices, tiles, stream
+    std::vector<int> win_of(n, -1);  // window index of a row inside the current part
+    struct Entry {
+        int win;     // window index of the column
+        int block;   // canonical upper block
+        bool lower;  // transpose of that block
+    };
+    std::vector<Entry> row_entries;
+    size_t stream_bytes = 0;
+    for (int p = 0; p < parts; ++p) {
+        const int g0 = count[p], g1 = count[p + 1], m = g1 - g0;
+        for (int g = g0; g < g1; ++g) win_of[out.perm[g]] = g - g0;
+        // halo rows, ascending slab index
+        std::vector<int> halo;
+        for (int g = g0; g < g1; ++g) {
+            const int r = out.perm[g];
+            for (int k = row_start[r]; k < row_start[r + 1]; ++k)
+                if (part_of[col[k]] != p) halo.push_back(inv[col[k]]);
+            for (int e = lt_start[r]; e < lt_start[r + 1]; ++e)
+                if (part_of[lt_row[e]] != p) halo.push_back(inv[lt_row[e]]);
+        }
+        std::sort(halo.begin(), halo.end());
+        halo.erase(std::unique(halo.begin(), halo.end()), halo.end());
+        const int h = static_cast<int>(halo.size());
+        if (m + h > kSlabWinCap) {
+            for (int g = g0; g < g1; ++g) win_of[out.perm[g]] = -1;
+            return "a part's window exceeds shared memory";
+        }
+        for (int i = 0; i < h; ++i) win_of[out.perm[halo[i]]] = m + i;
+        const int halo0 = static_cast<int>(out.halo_src.size());
+        out.halo_src.insert(out.halo_src.end(), halo.begin(), halo.end());
+
+        // tiles of consecutive owned rows
+        const int tile0 = static_cast<int>(out.tile_desc.size() / 4);
+        int a = 0;
+        while (a < m) {
+            int b = a, entries = 0;
+            while (b < m && b - a < kSlabRows) {
+                const int e = entries + len[out.perm[g0 + b]];
+                if (((e + 7) & ~7) > kSlabCapE) break;
+                entries = e;
+                ++b;
+            }
+            if (b == a) return "a row has more blocks than a tile holds";
+            const int ne = (entries + 7) & ~7;
+            const size_t bytes = (size_t)kSlabHeaderBytes + (size_t)kSlabEntryBytes * ne;
+            const size_t off = stream_bytes;
+            stream_bytes += bytes;  // bytes is a multiple of 16 (ne is a multiple of 8)
+            out.stream.resize(stream_bytes, 0);
+            const size_t vals_off = off + kSlabHeaderBytes;
+            const size_t col_off = vals_off + 36 * (size_t)ne;
+            int j = 0;
+            for (int i = a; i < b; ++i) {
+                const int r = out.perm[g0 + i];
+                put_u16(out.stream, off + 2 * (size_t)(i - a), (unsigned)j);
+                row_entries.clear();
+                for (int k = row_start[r]; k < row_start[r + 1]; ++k) row_entries.push_back({win_of[col[k]], k, false});
+                for (int e = lt_start[r]; e < lt_start[r + 1]; ++e)
+                    row_entries.push_back({win_of[lt_row[e]], lt_block[e], true});
+                std::sort(row_entries.begin(), row_entries.end(),
+                          [](const Entry& x, const Entry& y) { return x.win < y.win; });
+                for (const Entry& en : row_entries) {
+                    const unsigned fpos = static_cast<unsigned>((vals_off + 36 * (size_t)j) / 4);
+                    (en.lower ? out.pos_l : out.pos_u)[en.block] = fpos;
+                    put_u16(out.stream, col_off + 2 * (size_t)j, (unsigned)en.win);
+                    ++j;
+                }
+            }
+            put_u16(out.stream, off + 2 * (size_t)(b - a), (unsigned)j);
+            if (off / 16 > 0x7fffffffULL || stream_bytes / 4 >= 0xffffffffULL) return "stream too large";
+            out.tile_desc.insert(out.tile_desc.end(), {static_cast<int>(off / 16), static_cast<int>(bytes), a, b - a});
+            a = b;
+        }
+        const int ntiles = static_cast<int>(out.tile_desc.size() / 4) - tile0;
+        if (ntiles > kSlabMaxTiles) return "a part has more tiles than the table holds";
+        int* pi = out.part_info.data() + (size_t)kSlabPartInts * p;
+        pi[0] = g0;
+        pi[1] = m;
+        pi[2] = halo0;
+        pi[3] = h;
+        pi[4] = tile0;
+        pi[5] = ntiles;
+        out.max_window = std::max(out.max_window, m + h);
+        out.max_tiles = std::max(out.max_tiles, ntiles);
+        out.max_rows = std::max(out.max_rows, m);
+        for (int g = g0; g < g1; ++g) win_of[out.perm[g]] = -1;
+        for (int i = 0; i < h; ++i) win_of[out.perm[halo[i]]] = -1;
+    }
+    // Every block has its copy; every off-diagonal block also its transpose.
+    for (int k = 0; k < nnz; ++k)
+        if (out.pos_u[k] == kSlabNoPos) return "internal: block without a position";
+    for (int r = 0; r < n; ++r)
+        for (int k = row_start[r]; k < row_start[r + 1]; ++k)
+            if ((col[k] != r) != (out.pos_l[k] != kSlabNoPos)) return "internal: transposed copy mismatch";
+    return "";
+}
+
+void slab_spmv_host(const SlabPlan& plan, int nnz, const double* values, const double* x, double* y)
+{
+    // Fill, as the fill kernel does (float storage).
+    std::vector<unsigned char> s = plan.stream;
+    const size_t sfloats = s.size() / 4;
+    auto put = [&](unsigned fpos, int e, double v) {
+        const float f = static_cast<float>(v);
+        std::memcpy(s.data() + 4 * ((size_t)fpos + e), &f, 4);
+    };
+    for (int k = 0; k < nnz; ++k) {
+        const double* b = values + 9 * (size_t)k;
+        if (plan.pos_u[k] != kSlabNoPos && plan.pos_u[k] + 9 <= sfloats)
+            for (int e = 0; e < 9; ++e) put(plan.pos_u[k], e, b[e]);
+        if (plan.pos_l[k] != kSlabNoPos && plan.pos_l[k] + 9 <= sfloats)
+            for (int i = 0; i < 3; ++i)
+                for (int m = 0; m < 3; ++m) put(plan.pos_l[k], 3 * m + i, b[3 * i + m]);
+    }
+    // Decode tile by tile with the kernel's clamps.
+    for (int p = 0; p < plan.parts; ++p) {
+        const int* pi = plan.part_info.data() + (size_t)kSlabPartInts * p;
+        const int g0 = pi[0], m = pi[1], halo0 = pi[2], h = pi[3], tile0 = pi[4], ntiles = pi[5];
+        const int wn = m + h;
+        std::vector<double> win(3 * (size_t)wn);
+        for (int w = 0; w < wn; ++w) {
+            const int g = w < m ? g0 + w : plan.halo_src[halo0 + w - m];
+            const int r = plan.perm[g];
+            for (int a = 0; a < 3; ++a) win[3 * (size_t)w + a] = static_cast<double>(static_cast<float>(x[3 * (size_t)r + a]));
+        }
+        for (int t = 0; t < ntiles; ++t) {
+            const int* d = plan.tile_desc.data() + 4 * (size_t)(tile0 + t);
+            const size_t off = 16 * (size_t)d[0];
+            const int bytes = d[1];
+            const int ne = bytes >= kSlabHeaderBytes ? (bytes - kSlabHeaderBytes) / kSlabEntryBytes : 0;
+            const size_t vals_off = off + kSlabHeaderBytes, col_off = vals_off + 36 * (size_t)ne;
+            for (int i = 0; i < d[3]; ++i) {
+                const int e0 = std::min<int>(get_u16(s, off + 2 * (size_t)i), ne);
+                const int e1 = std::min<int>(get_u16(s, off + 2 * (size_t)(i + 1)), ne);
+                double acc[3] = {0, 0, 0};
+                for (int j = e0; j < e1; ++j) {
+                    const int c = std::min<int>(get_u16(s, col_off + 2 * (size_t)j), wn - 1);
+                    float v[9];
+                    std::memcpy(v, s.data() + vals_off + 36 * (size_t)j, 36);
+                    for (int a = 0; a < 3; ++a)
+                        for (int mm = 0; mm < 3; ++mm) acc[a] += double(v[3 * mm + a]) * win[3 * (size_t)c + mm];
+                }
+                const int r = plan.perm[g0 + d[2] + i];
+                for (int a = 0; a < 3; ++a) y[3 * (size_t)r + a] = acc[a];
+            }
+        }
+    }
+}
+
+}  // namespace pk

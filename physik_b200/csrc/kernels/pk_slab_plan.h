@@ -1,0 +1,74 @@
+// pk_slab_plan.h -- host-side layout of the part-resident ("slab") PCG kernel.
+//
+// The rows of the solve are split into parts, one per block of the cooperative launch
+// (one block per SM), by recursive coordinate bisection of the rows' node positions.  A
+// part owns a set of rows (consecutive in "slab order": parts in order, each part's rows
+// in ascending dynamic-row order); its window is its own rows followed by its halo (the
+// rows of other parts its rows couple to).  The search direction of the whole window
+// lives in shared memory for the whole solve, so the SpMV gathers only from shared memory.
+//
+// The matrix is stored once more, per part, as a stream of tiles of at most kSlabRows
+// consecutive owned rows.  A row holds every block of its full symmetric row -- the
+// stored upper blocks (r, c) and the transposes of the lower ones (c, r) -- so no block is
+// fetched by another row.  A tile is one contiguous run of bytes that one TMA bulk copy
+// moves into a ring stage:
+//     [kSlabHeaderBytes: u16 row offsets, rows + 1 used]
+//     [entries x 9 floats: the blocks, column-major]
+//     [entries x u16: window index of each block's column]
+// with the entry count padded to a multiple of 8 so both arrays start on 16-byte
+// boundaries.  pos_u / pos_l give, for each canonical upper block k, the float offsets of
+// its copy and of its transpose in the stream; a fill kernel writes them after assembly.
+//
+// Plain C++ (no CUDA), shared by the runtime and its CPU self-check.
+#pragma once
+
+#include <cstddef>
+#include <string>
+#include <vector>
+
+namespace pk {
+
+// Tiles are large (about 19 KB for rows of 15 blocks): on B200 a bulk copy's throughput
+// per SM grows with its size (measured: ~3.1 TB/s over all SMs with 9 KB copies, ~5.3
+// TB/s with 16 KB, ~5.8 TB/s with 32 KB), not with the number of copies in flight.
+constexpr int kSlabRows = 32;          // rows per tile
+constexpr int kSlabLanesPerRow = 4;    // consumer lanes per row (32 rows per 128-thread group)
+constexpr int kSlabHeaderBytes = 80;   // u16 row offsets of a tile (rows + 1 used)
+constexpr int kSlabEntryBytes = 38;    // 9 floats + u16 column
+constexpr int kSlabCapE = 512;         // entries per tile
+constexpr int kSlabStageBytes = 19584; // >= kSlabHeaderBytes + kSlabCapE * kSlabEntryBytes, 128-byte multiple
+constexpr int kSlabStages = 6;         // multiple of the consumer groups
+constexpr int kSlabWinCap = 6144;      // window rows (owned + halo) per part
+constexpr int kSlabMaxTiles = 128;     // tiles per part
+constexpr int kSlabPartInts = 8;       // per part: row0, rows, halo0, halo rows, tile0, tiles, 0, 0
+constexpr unsigned kSlabNoPos = 0xffffffffu;
+
+static_assert(kSlabHeaderBytes + kSlabCapE * kSlabEntryBytes <= kSlabStageBytes, "stage too small");
+static_assert(kSlabCapE % 8 == 0, "entry cap must keep 16-byte alignment");
+static_assert(kSlabHeaderBytes % 16 == 0, "blocks must start on a 16-byte boundary");
+static_assert(2 * (kSlabRows + 1) <= kSlabHeaderBytes, "header too small");
+
+struct SlabPlan {
+    int n = 0;
+    int parts = 0;
+    std::vector<int> perm;       // slab index -> dynamic row
+    std::vector<int> part_info;  // kSlabPartInts per part
+    std::vector<int> halo_src;   // slab index of every halo row, part by part
+    std::vector<int> tile_desc;  // 4 per tile: stream offset / 16, bytes, first local row, rows
+    std::vector<unsigned char> stream;  // headers and columns filled, blocks zero
+    std::vector<unsigned> pos_u, pos_l; // per canonical upper block: float offsets (kSlabNoPos: none)
+    int max_window = 0, max_tiles = 0, max_rows = 0;
+};
+
+// Builds the layout for `parts` parts of the upper-stored pattern (row_start, col) with
+// its transpose index (lt_start, lt_row, lt_block).  coords: 3 doubles per row (NULL:
+// contiguous parts of the dynamic-row order).  Returns "" on success, otherwise why the
+// layout does not apply (a window or a row too large); `out` is then unusable.
+std::string build_slab_plan(int n, const int* row_start, const int* col, const int* lt_start, const int* lt_row,
+                            const int* lt_block, const double* coords, int parts, SlabPlan& out);
+
+// y = A x through the plan exactly as the kernel reads it (fill, then tile decoding with
+// the kernel's clamps), in double: the CPU self-check of a plan.
+void slab_spmv_host(const SlabPlan& plan, int nnz, const double* values, const double* x, double* y);
+
+}  // namespace pk

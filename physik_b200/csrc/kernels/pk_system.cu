@@ -146,14 +146,18 @@ bool staging_enabled()
     return !(e && e[0] == '0');
 }
 
-// Which PCG kernel a system uses: the ring-staged kernel when its tiling fits, else the
-// TMA-staged or the unstaged one.  PK_PCG_KERNEL=staged / plain forces the older kernels.
+// Which PCG kernel a system uses: the part-resident kernel when its layout applies (FP32
+// storage, windows that fit shared memory), else the ring-staged kernel when its tiling
+// fits, else the TMA-staged or the unstaged one.  PK_PCG_KERNEL=slab / ring / staged /
+// plain asks for one (-1: automatic, 0 ring, 1 staged, 2 plain, 3 slab).
 int requested_kernel()
 {
     const char* e = std::getenv("PK_PCG_KERNEL");
+    if (e && std::strcmp(e, "ring") == 0) return 0;
     if (e && std::strcmp(e, "staged") == 0) return 1;
     if (e && std::strcmp(e, "plain") == 0) return 2;
-    return 0;
+    if (e && std::strcmp(e, "slab") == 0) return 3;
+    return -1;
 }
 
 // Tiles of the ring-staged PCG kernel (pk::RingTile caps): consecutive rows, at most
@@ -213,8 +217,21 @@ struct pk_system {
     int batch_max_grid = 0;
     int batch_min_rows = 64;      // smallest part a body is cut into (autotuned)
     DevBuf batch_parts_buf, body_stats;
-    // kernel selection: -1 automatic (ring, else staged, else plain), 0 ring, 1 staged, 2 plain
+    // part-resident PCG (FP32 storage): layout built lazily at the first solve
+    bool slab_tried = false;
+    bool slab_filled = false;     // the block stream holds the current values
+    int slab_parts = 0;           // blocks of the slab kernel (0: layout not available)
+    int slab_tile_count = 0, slab_halo_count = 0;
+    int slab_max_grid = 0;
+    std::string slab_reason;      // why the layout does not apply
+    unsigned long long slab_stream_bytes = 0;
+    DevBuf slab_part_info, slab_tiles, slab_stream, slab_halo, slab_perm, slab_pos_u, slab_pos_l;
+    DevBuf slab_xs, slab_rs, slab_qs, slab_ss, slab_minvs;
+    // kernel selection: -1 automatic (slab, else ring, else staged, else plain), 0 ring,
+    // 1 staged, 2 plain, 3 slab
     int kernel_choice = -1;
+    int last_kernel = -1;         // kernel of the last solve (4: batched), blocks it ran on
+    int last_blocks = 0;
     int staged_rows = 0;          // rows per staged tile (0: chosen from the grid)
     std::vector<int> h_row_start, h_lts;  // host copies for re-tiling
     // host copies for the adjoint step's assembly of node sensitivities
@@ -440,11 +457,167 @@ int run_pcg_ring(pk_system* s, const pk_step_params& p, int skip_on_flags)
     a.stats = st;
     PK_CHECK(pk::launch_pcg_ring_kernel<Real, Acc>(a, grid, s->stream));
     s->launches += 1;
+    s->last_blocks = grid;
     return PK_OK;
 }
 
 template <class T>
 int upload_raw(DevBuf& buf, const T* src, size_t n, cudaStream_t stream);
+template <class Real>
+int download_real(const DevBuf& buf, double* dst, size_t n, cudaStream_t stream);
+
+void reset_slab(pk_system* s)
+{
+    s->slab_tried = false;
+    s->slab_filled = false;
+    s->slab_parts = 0;
+    s->slab_reason.clear();
+}
+
+// Copies the assembled upper blocks (and their transposes) into the slab stream.
+int slab_fill(pk_system* s)
+{
+    PK_CHECK(pk::launch_slab_fill_kernel(s->values.as<float>(), s->nnz, s->slab_pos_u.as<unsigned>(),
+                                         s->slab_pos_l.as<unsigned>(), s->slab_stream.as<float>(),
+                                         s->slab_stream_bytes / 4, s->stream));
+    s->launches += 1;
+    s->slab_filled = true;
+    return PK_OK;
+}
+
+bool slab_allowed(const pk_system* s)
+{
+    const int rk = requested_kernel();
+    return s->precision != PK_PREC_FP64 && (rk == -1 || rk == 3) && s->dyn_count > 0 && s->have_pattern;
+}
+
+// Builds and uploads the part-resident kernel's layout if it has not been tried yet for
+// this pattern and grid (synchronous: never called while a stream capture is open).
+// Parts are cut by the rows' node positions at this moment.  Not applicable (too large
+// a window, too long a row) leaves slab_parts at 0 and the reason in slab_reason.
+template <class Acc>
+int ensure_slab(pk_system* s)
+{
+    if (s->slab_tried || !slab_allowed(s)) return PK_OK;
+    s->slab_tried = true;
+    s->slab_parts = 0;
+    if (!s->slab_max_grid) s->slab_max_grid = pk::pcg_slab_max_grid<Acc>();
+    int grid = s->slab_max_grid;
+    if (s->pcg_grid_override > 0) grid = std::min(grid, s->pcg_grid_override);
+    grid = std::min(grid, std::max(1, s->dyn_count / 64));
+    if (grid <= 0) {
+        s->slab_reason = "kernel cannot be resident";
+        return PK_OK;
+    }
+    const int n = s->dyn_count;
+    // node positions -> per-row coordinates
+    std::vector<double> nodes(3 * static_cast<size_t>(std::max(1, s->node_count)), 0.0);
+    if (s->node_count > 0) {
+        int rc = download_real<float>(s->x, nodes.data(), 3 * static_cast<size_t>(s->node_count), s->stream);
+        if (rc) return rc;
+    }
+    std::vector<double> coords(3 * static_cast<size_t>(n));
+    for (int r = 0; r < n; ++r)
+        for (int a = 0; a < 3; ++a) coords[3 * (size_t)r + a] = nodes[3 * (size_t)s->h_dyn_to_node[r] + a];
+    std::vector<int> col(static_cast<size_t>(s->nnz)), ltr(static_cast<size_t>(s->lt_count)),
+        ltb(static_cast<size_t>(s->lt_count));
+    PK_CHECK(cudaMemcpy(col.data(), s->col.p, col.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    if (s->lt_count > 0) {
+        PK_CHECK(cudaMemcpy(ltr.data(), s->lt_row.p, ltr.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        PK_CHECK(cudaMemcpy(ltb.data(), s->lt_block.p, ltb.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    }
+    pk::SlabPlan plan;
+    const std::string why = pk::build_slab_plan(n, s->h_row_start.data(), col.data(), s->h_lts.data(), ltr.data(),
+                                                ltb.data(), coords.data(), grid, plan);
+    if (!why.empty()) {
+        s->slab_reason = why;
+        return PK_OK;
+    }
+    int rc = upload_raw<int>(s->slab_part_info, plan.part_info.data(), plan.part_info.size(), s->stream);
+    if (!rc) rc = upload_raw<int>(s->slab_tiles, plan.tile_desc.data(), plan.tile_desc.size(), s->stream);
+    if (!rc) rc = upload_raw<unsigned char>(s->slab_stream, plan.stream.data(), plan.stream.size(), s->stream);
+    if (!rc && !plan.halo_src.empty())
+        rc = upload_raw<int>(s->slab_halo, plan.halo_src.data(), plan.halo_src.size(), s->stream);
+    if (!rc) rc = upload_raw<int>(s->slab_perm, plan.perm.data(), plan.perm.size(), s->stream);
+    if (!rc) rc = upload_raw<unsigned>(s->slab_pos_u, plan.pos_u.data(), plan.pos_u.size(), s->stream);
+    if (!rc) rc = upload_raw<unsigned>(s->slab_pos_l, plan.pos_l.data(), plan.pos_l.size(), s->stream);
+    if (rc) return rc;
+    const size_t rows = static_cast<size_t>(n);
+    PK_CHECK(s->slab_xs.ensure(16 * rows));
+    PK_CHECK(s->slab_rs.ensure(16 * rows));
+    PK_CHECK(s->slab_qs.ensure(16 * rows));
+    PK_CHECK(s->slab_ss.ensure(16 * rows));
+    PK_CHECK(s->slab_minvs.ensure(48 * rows));
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    s->slab_stream_bytes = plan.stream.size();
+    s->slab_tile_count = static_cast<int>(plan.tile_desc.size() / 4);
+    s->slab_halo_count = static_cast<int>(plan.halo_src.size());
+    s->slab_parts = plan.parts;
+    return PK_OK;
+}
+
+int ensure_slab_any(pk_system* s)
+{
+    if (s->precision == PK_PREC_FP32) return ensure_slab<float>(s);
+    if (s->precision == PK_PREC_MIXED) return ensure_slab<double>(s);
+    return PK_OK;
+}
+
+template <class Real, class Acc>
+int run_pcg_slab(pk_system* s, const pk_step_params& p, int skip_on_flags)
+{
+    if constexpr (!std::is_same<Real, float>::value) {
+        return fail(PK_ERR_UNSUPPORTED, "part-resident PCG: FP32 storage only");
+    } else {
+        const int grid = s->slab_parts;
+        if (grid <= 0) return fail(PK_ERR_UNSUPPORTED, "part-resident PCG layout not available");
+        int rc = ensure_solver_buffers(s, 1);
+        if (rc) return rc;
+        PK_CHECK(s->slots.ensure(2 * sizeof(pk::ExSlot) * static_cast<size_t>(grid)));
+        PK_CHECK(cudaMemsetAsync(s->slots.p, 0, 2 * sizeof(pk::ExSlot) * static_cast<size_t>(grid), s->stream));
+        PK_CHECK(cudaMemsetAsync(s->sync.p, 0, sizeof(pk::GridSync), s->stream));
+        if (!s->slab_filled) {
+            rc = slab_fill(s);
+            if (rc) return rc;
+        }
+        pk::SlabPcgArgs<Acc> a{};
+        a.n = s->dyn_count;
+        a.part_info = s->slab_part_info.as<int>();
+        a.tile_desc = s->slab_tiles.as<int4>();
+        a.tile_count = s->slab_tile_count;
+        a.halo_count = s->slab_halo_count;
+        a.stream = s->slab_stream.as<unsigned char>();
+        a.stream_bytes = s->slab_stream_bytes;
+        a.halo_src = s->slab_halo.as<int>();
+        a.perm = s->slab_perm.as<int>();
+        a.b = s->rhs.as<float>();
+        a.minv = s->minv.as<float>();
+        a.x = s->px.as<float>();
+        a.xs = s->slab_xs.as<float>();
+        a.rs = s->slab_rs.as<float>();
+        a.qs = s->slab_qs.as<float>();
+        a.ss = s->slab_ss.as<float>();
+        a.minvs = s->slab_minvs.as<float>();
+        a.slots = s->slots.as<pk::ExSlot>();
+        a.sync = s->sync.as<pk::GridSync>();
+        a.max_iterations = p.max_iterations;
+        a.tolerance = static_cast<Acc>(static_cast<float>(p.tolerance));
+        a.skip_on_flags = skip_on_flags;
+        a.integrate = p.integrate;
+        a.dt = static_cast<float>(p.dt);
+        a.dyn_to_node = s->dyn_to_node.as<int>();
+        a.node_x = s->x.as<float>();
+        a.node_v = s->v.as<float>();
+        pk::DevStats* st = s->stats.as<pk::DevStats>();
+        a.flags = &st->flags;
+        a.stats = st;
+        PK_CHECK(pk::launch_pcg_slab_kernel<Acc>(a, grid, s->stream));
+        s->launches += 1;
+        s->last_kernel = 3;
+        s->last_blocks = grid;
+        return PK_OK;
+    }
+}
 
 // Cuts every body (segment) into parts of about equal row count, one block each, so that
 // all parts fit one cooperative wave.  parts: 8 ints per block (see pk::BatchPcgArgs).
@@ -554,14 +727,32 @@ int run_pcg_batch(pk_system* s, const pk_step_params& p, int skip_on_flags)
     a.body_stats = s->body_stats.as<pk::BatchBodyStats>();
     PK_CHECK(pk::launch_pcg_batch_kernel<Real, Acc>(a, grid, s->stream));
     s->launches += 1;
+    s->last_blocks = grid;
     return PK_OK;
+}
+
+// The PCG kernel the next unbatched solve uses (0 ring, 1 staged, 2 plain, 3 slab).
+int solve_kernel(const pk_system* s)
+{
+    if (s->kernel_choice == 3 && s->slab_parts <= 0) return s->ring_tiles > 0 ? 0 : (s->ntiles > 0 ? 1 : 2);
+    if (s->kernel_choice >= 0) return s->kernel_choice;
+    return s->slab_parts > 0 ? 3 : (s->ring_tiles > 0 ? 0 : (s->ntiles > 0 ? 1 : 2));
 }
 
 template <class Real, class Acc>
 int run_pcg(pk_system* s, const pk_step_params& p, int skip_on_flags)
 {
-    if (s->batched && s->seg_start.size() >= 2) return run_pcg_batch<Real, Acc>(s, p, skip_on_flags);
-    const int kernel = s->kernel_choice >= 0 ? s->kernel_choice : (s->ring_tiles > 0 ? 0 : (s->ntiles > 0 ? 1 : 2));
+    if (s->batched && s->seg_start.size() >= 2) {
+        s->last_kernel = 4;
+        return run_pcg_batch<Real, Acc>(s, p, skip_on_flags);
+    }
+    if constexpr (std::is_same<Real, float>::value) {
+        int rc = ensure_slab<Acc>(s);
+        if (rc) return rc;
+    }
+    const int kernel = solve_kernel(s);
+    s->last_kernel = kernel;
+    if (kernel == 3) return run_pcg_slab<Real, Acc>(s, p, skip_on_flags);
     if (kernel == 0 && s->ring_tiles > 0) {
         int rc = ensure_solver_buffers(s, 1);
         if (rc) return rc;
@@ -580,6 +771,8 @@ int run_pcg(pk_system* s, const pk_step_params& p, int skip_on_flags)
     if (kernel == 2) a.ntiles = 0;
     PK_CHECK(pk::launch_pcg_kernel<Real, Acc>(a, grid, pk::kPcgThreads, s->stream));
     s->launches += 1;
+    s->last_kernel = a.ntiles > 0 ? 1 : 2;
+    s->last_blocks = grid;
     return PK_OK;
 }
 
@@ -606,6 +799,19 @@ int run_step(pk_system* s, const pk_step_params& p)
     if (s->dyn_count > 0) {
         PK_CHECK(pk::launch_row_kernel<Real>(a, s->max_row, s->stream));
         s->launches += 1;
+        s->slab_filled = false;
+        // The part-resident kernel reads the blocks from its own stream: fill it here so
+        // the solve time below is the PCG kernel's alone.
+        if constexpr (std::is_same<Real, float>::value) {
+            if (!p.explicit_mode && !(s->batched && s->seg_start.size() >= 2)) {
+                int rc = s->precision == PK_PREC_MIXED ? ensure_slab<double>(s) : ensure_slab<float>(s);
+                if (rc) return rc;
+                if (solve_kernel(s) == 3) {
+                    rc = slab_fill(s);
+                    if (rc) return rc;
+                }
+            }
+        }
     }
     if (s->timing) PK_CHECK(cudaEventRecord(s->ev_pool[evi[1]], s->stream));
     if (!p.explicit_mode && s->dyn_count > 0) {
@@ -651,6 +857,7 @@ int run_step_graph(pk_system* s, const pk_step_params& p)
         drop_graph(s);
         // Everything built lazily (allocations, uploads) must exist before the capture.
         int prc = ensure_batch_parts_any(s);
+        if (!prc) prc = ensure_slab_any(s);
         if (prc) return prc;
         const bool timing = s->timing;
         const long long launches = s->launches;
@@ -963,9 +1170,11 @@ PKCUDA_API int pk_system_set_pattern(pk_system* s, int dyn_count, const int* dyn
     s->h_row_start.assign(row_start, row_start + dyn_count + 1);
     s->h_dyn_to_node.assign(dyn_to_node, dyn_to_node + dyn_count);
     s->h_lts = lts;
-    // Ring-staged PCG tiles (the default kernel).
+    reset_slab(s);
+    // Ring-staged PCG tiles (the kernel used where the part-resident one does not apply).
     s->ring_tiles = 0;
-    if (requested_kernel() == 0 && dyn_count > 0 && diag_first) {
+    const int rk = requested_kernel();
+    if ((rk == -1 || rk == 0 || rk == 3) && dyn_count > 0 && diag_first) {
         std::vector<int> desc;
         const bool ok = s->precision == PK_PREC_FP64 ? build_ring_tiles<double>(dyn_count, row_start, lts, desc)
                                                      : build_ring_tiles<float>(dyn_count, row_start, lts, desc);
@@ -1050,6 +1259,7 @@ PKCUDA_API int pk_system_solve_given_f64(pk_system* s, const double* values, con
     PK_CHECK(cudaSetDevice(s->device));
     int rc = PK_OK;
     if (values) rc = upload_real_any(s, s->values, values, 9 * static_cast<size_t>(s->nnz));
+    if (values) s->slab_filled = false;
     if (!rc && rhs) rc = upload_real_any(s, s->rhs, rhs, 3 * static_cast<size_t>(s->dyn_count));
     if (!rc && minv) rc = upload_real_any(s, s->minv, minv, 9 * static_cast<size_t>(s->dyn_count));
     if (rc) return rc;
@@ -1109,6 +1319,7 @@ PKCUDA_API int pk_system_set_pcg_grid(pk_system* s, int grid)
     PK_CHECK(cudaSetDevice(s->device));
     drop_graph(s);
     s->pcg_grid_override = std::max(0, grid);
+    reset_slab(s);
     if (s->ring_tiles > 0) {
         if (s->precision == PK_PREC_FP32) return ring_grid_for<float, float>(s);
         if (s->precision == PK_PREC_MIXED) return ring_grid_for<float, double>(s);
@@ -1173,6 +1384,13 @@ PKCUDA_API int pk_system_segment_stats(pk_system* s, int segment_count, int* ite
         if (flags) flags[b] = bs[b].flags;
     }
     return PK_OK;
+}
+
+PKCUDA_API int pk_system_pcg_kernel(pk_system* s, int* blocks)
+{
+    if (!s) return fail(PK_ERR_ARG, "pcg_kernel");
+    if (blocks) *blocks = s->last_blocks;
+    return s->last_kernel;
 }
 
 PKCUDA_API int pk_system_set_graph(pk_system* s, int on)
@@ -1245,11 +1463,14 @@ PKCUDA_API int pk_system_autotune(pk_system* s, const pk_step_params* p, int rep
         int rc = ensure_batch_parts_any(s);
         if (rc) return rc;
     } else {
-        // Candidates: ring kernel; staged kernel with 16 / 32 / 64-row tiles; plain kernel.
+        // Candidates: ring kernel; staged kernel with 16 / 32 / 64-row tiles; plain kernel;
+        // part-resident kernel.
         struct Cand {
             int kernel, rows;
         };
-        const Cand cand[] = {{0, 0}, {1, 16}, {1, 32}, {1, pk::kTileRowsMax}, {2, 0}};
+        const Cand cand[] = {{0, 0}, {1, 16}, {1, 32}, {1, pk::kTileRowsMax}, {2, 0}, {3, 0}};
+        int rc0 = ensure_slab_any(s);
+        if (rc0) return rc0;
         auto retile = [&](int rows) -> int {
             std::vector<int> desc;
             s->ntiles = 0;
@@ -1262,6 +1483,7 @@ PKCUDA_API int pk_system_autotune(pk_system* s, const pk_step_params* p, int rep
         int i = 0;
         for (const Cand& c : cand) {
             if (c.kernel == 0 && s->ring_tiles <= 0) { ++i; continue; }
+            if (c.kernel == 3 && s->slab_parts <= 0) { ++i; continue; }
             if (c.kernel == 1) {
                 int rc = retile(c.rows);
                 if (rc) return rc;
@@ -1316,6 +1538,7 @@ int adjoint_step(pk_system* s, const pk_step_params& p, const double* xbar_next,
     rc = upload_real<Real>(s->rhs, g.data(), g.size(), s->stream);
     if (rc) return rc;
     // 3. A w = g with the same PCG (A symmetric).
+    PK_CHECK(cudaMemsetAsync(s->stats.p, 0, sizeof(pk::DevStats), s->stream));
     if (s->precision == PK_PREC_FP32) rc = run_pcg<float, float>(s, q, 0);
     else if (s->precision == PK_PREC_MIXED) rc = run_pcg<float, double>(s, q, 0);
     else rc = run_pcg<double, double>(s, q, 0);
@@ -1551,6 +1774,35 @@ int ring_selfcheck(int n, const int* row_start, const int* col, const double* va
 }  // namespace
 
 extern "C" {
+
+PKCUDA_API int pk_slab_plan_selfcheck(int n, const int* row_start, const int* col_index, const double* values,
+                                      const double* x, const double* coords, int parts, double* y, int* info)
+{
+    if (n <= 0 || parts <= 0 || !row_start || !col_index || !values || !x || !y)
+        return fail(PK_ERR_ARG, "slab selfcheck");
+    if (row_start[0] != 0) return fail(PK_ERR_ARG, "row_start[0] != 0");
+    for (int r = 0; r < n; ++r) {
+        if (row_start[r + 1] < row_start[r]) return fail(PK_ERR_ARG, "row_start not monotone");
+        for (int k = row_start[r]; k < row_start[r + 1]; ++k) {
+            if (col_index[k] < r || col_index[k] >= n) return fail(PK_ERR_ARG, "column outside [row, n)");
+            if (k > row_start[r] && col_index[k] <= col_index[k - 1]) return fail(PK_ERR_ARG, "columns not sorted");
+        }
+    }
+    std::vector<int> lts, ltr, ltb;
+    build_transpose(n, row_start, col_index, lts, ltr, ltb);
+    pk::SlabPlan plan;
+    const std::string why =
+        pk::build_slab_plan(n, row_start, col_index, lts.data(), ltr.data(), ltb.data(), coords, parts, plan);
+    if (!why.empty()) return fail(PK_ERR_UNSUPPORTED, "slab layout: " + why);
+    pk::slab_spmv_host(plan, row_start[n], values, x, y);
+    if (info) {
+        info[0] = plan.parts;
+        info[1] = plan.max_window;
+        info[2] = plan.max_tiles;
+        info[3] = static_cast<int>(plan.stream.size() / 1024);
+    }
+    return PK_OK;
+}
 
 PKCUDA_API int pk_ring_tiling_selfcheck(int precision, int n, const int* row_start, const int* col_index,
                                         const double* values, const double* x, double* y, int* tiles, int* max_span)

@@ -128,6 +128,14 @@ class SimWorld:
             raise PhysikError("autotune failed: " + self.error())
         return chosen, ms.value
 
+    PCG_KERNELS = {0: "ring", 1: "staged", 2: "plain", 3: "slab", 4: "batched"}
+
+    def pcg_kernel(self):
+        """(name, blocks) of the PCG kernel the last step's solve ran on."""
+        blocks = C.c_int()
+        k = self.X.PHYSIK_B200_GetPcgKernel(self.h, C.byref(blocks))
+        return self.PCG_KERNELS.get(k, "none"), blocks.value
+
     def body_stats(self, i: int):
         it, conv, res, fl = C.c_int(), C.c_int(), C.c_float(), C.c_uint()
         if self.X.PHYSIK_B200_GetBodyConjugateGradientStats(self.h, self.components[i], C.byref(it), C.byref(conv),

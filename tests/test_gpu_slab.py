@@ -1,0 +1,126 @@
+"""The part-resident ("slab") PCG kernel on the GPU, against the oracle and the other kernels.
+
+The kernel keeps each part's search directions in shared memory and streams full
+symmetric rows; it runs wherever the storage is FP32 (FP32 and mixed precision) and the
+parts' windows fit.  Checked here:
+
+* it is the kernel the automatic choice picks for FP32-storage worlds, with one block per
+  part, and not for FP64;
+* one mixed-precision step equals the FP64 oracle's step (the reference's CPU solve in
+  double, teacher-forced from the same state) within the mixed-precision bar (positions
+  1e-5 relative), on a box cut into a few parts, on the 64x16x16 beam cut into one part
+  per SM (halos on every side), and on a two-body world;
+* FP32 steps follow the FP32 reference restatement within FP32 rounding;
+* it agrees with the ring-staged kernel on the same step (both FP32 storage; they differ
+  only in the order of sums);
+* the solve is deterministic: two worlds stepped alike are bit-identical, and a graph
+  replay equals plain launches.
+"""
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+from physik_b200 import meshes
+
+pytestmark = pytest.mark.gpu
+
+L = pytest.importorskip("physik_b200._lib")
+from physik_b200.world import SimWorld  # noqa: E402
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def two_bodies():
+    s = meshes.small_box(9, 6, 5)
+    s.bodies += meshes.small_box(7, 8, 4, young=5e4, seed=11).bodies
+    s.bodies[1].initial_velocities = np.tile(np.array([0.3, -0.2, 0.1], np.float32),
+                                             (s.bodies[1].positions.shape[0], 1))
+    return s
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp32"])
+def test_slab_is_the_default_for_fp32_storage(precision):
+    w = SimWorld(meshes.config1(), precision=precision)
+    w.step()
+    name, blocks = w.pcg_kernel()
+    assert name == "slab" and blocks >= 1, (name, blocks, w.error())
+    assert w.cg_stats()["flags"] & L.FLAG_INTEGRATED
+    w64 = SimWorld(meshes.config1(), precision="fp64")
+    w64.step()
+    assert w64.pcg_kernel()[0] == "ring"
+
+
+@pytest.mark.parametrize("make", [meshes.config1, meshes.config2, two_bodies], ids=["cube8", "beam64", "two_bodies"])
+def test_slab_mixed_matches_fp64_oracle(make):
+    scene = make()
+    gpu = SimWorld(scene, precision="mixed")
+    ora = po.Oracle(scene, "f64", float_inputs=True)
+    for _ in range(2):
+        gpu.set_state(ora.x, ora.v, f64=True)
+        gpu.step()
+        ora.step()
+        assert gpu.pcg_kernel()[0] == "slab"
+        x, v = gpu.state(f64=True)
+        st = gpu.cg_stats()
+        assert st["flags"] & L.FLAG_INTEGRATED, hex(st["flags"])
+        assert rel(x, ora.x) <= 1e-5
+        assert rel(v, ora.v) <= 2e-3
+        assert abs(st["iterations"] - ora.last_stats()["iterations"]) <= 3
+
+
+def test_slab_beam64_uses_one_block_per_part():
+    w = SimWorld(meshes.config2(), precision="mixed")
+    w.step()
+    name, blocks = w.pcg_kernel()
+    assert name == "slab" and blocks > 64, (name, blocks)
+
+
+def test_slab_fp32_follows_fp32_reference():
+    scene = meshes.config1()
+    gpu = SimWorld(scene, precision="fp32")
+    ora = po.Oracle(scene, "f32")
+    for _ in range(3):
+        gpu.set_state(ora.x, ora.v, f64=True)
+        gpu.step()
+        ora.step()
+        x, v = gpu.state(f64=True)
+        assert gpu.pcg_kernel()[0] == "slab"
+        assert rel(x, ora.x) <= 1e-6
+        assert rel(v, ora.v) <= 2e-3
+        assert abs(gpu.cg_stats()["iterations"] - ora.last_stats()["iterations"]) <= 3
+
+
+def test_slab_agrees_with_ring_kernel(monkeypatch):
+    scene = meshes.config2()
+    slab = SimWorld(scene, precision="mixed")
+    slab.step()
+    assert slab.pcg_kernel()[0] == "slab"
+    monkeypatch.setenv("PK_PCG_KERNEL", "ring")
+    ring = SimWorld(scene, precision="mixed")
+    ring.step()
+    assert ring.pcg_kernel()[0] == "ring"
+    xs, vs = slab.state(f64=True)
+    xr, vr = ring.state(f64=True)
+    assert rel(xs, xr) <= 1e-6
+    assert rel(vs, vr) <= 1e-3
+    assert abs(slab.cg_stats()["iterations"] - ring.cg_stats()["iterations"]) <= 2
+
+
+def test_slab_is_deterministic_and_graph_replay_is_bit_identical():
+    scene = two_bodies()
+    a = SimWorld(scene, precision="mixed")
+    b = SimWorld(scene, precision="mixed")
+    g = SimWorld(scene, precision="mixed")
+    g.set_graph(True)
+    for _ in range(5):
+        a.step()
+        b.step()
+        g.step()
+    xa, va = a.state(f64=True)
+    for w in (b, g):
+        x, v = w.state(f64=True)
+        np.testing.assert_array_equal(x, xa)
+        np.testing.assert_array_equal(v, va)
+    assert g.pcg_kernel()[0] == "slab"

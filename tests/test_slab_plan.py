@@ -1,0 +1,113 @@
+"""Layout of the part-resident PCG kernel, checked on the CPU (no GPU needed).
+
+``pk_slab_plan_selfcheck`` cuts the rows into parts by their node positions, builds each
+part's window (its rows, then the halo rows of other parts it couples to) and its stream
+of tiles of full symmetric rows with 16-bit window columns, fills the stream from the
+upper blocks as the device fill does (each block and the transpose of each off-diagonal
+one), and evaluates y = A x by decoding the tiles exactly as the kernel's lanes read
+them.  The product must equal the symmetric upper-BSR product
+(SparseBlockMatrix::Multiply, src/Math/SparseBlockMatrix.cpp:209-268) computed with
+numpy, for patterns built by the drop-in host layer: structured boxes, the 128x64x64
+block cut into 148 parts (the B200's SM count), a randomly numbered body, several
+bodies, and parts cut without positions.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from physik_b200 import _lib as L
+from physik_b200 import meshes
+from physik_b200.world import SimWorld
+
+from tests.test_ring_tiling import sym_upper_spmv
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _pattern_and_coords(scene):
+    w = SimWorld(scene)
+    w.prepare(upload=False)
+    rs, col, n2d, _ = w.pattern()
+    pos = np.concatenate([(b.initial_positions if b.initial_positions is not None else b.positions)
+                          for b in scene.bodies]).astype(np.float64)
+    n = len(rs) - 1
+    coords = np.zeros((n, 3))
+    dyn = n2d >= 0
+    coords[n2d[dyn]] = pos[dyn]
+    return rs.astype(np.int32), col.astype(np.int32), coords
+
+
+def _check(rs, col, coords, parts, seed=0):
+    n = len(rs) - 1
+    rng = np.random.default_rng(seed)
+    vals = rng.standard_normal(9 * len(col)).astype(np.float32).astype(np.float64)
+    x = rng.standard_normal((n, 3)).astype(np.float32).astype(np.float64)
+    y = np.full((n, 3), np.nan)
+    info = np.zeros(4, np.int32)
+    cp = _ptr(coords) if coords is not None else None
+    rc = L.PK.pk_slab_plan_selfcheck(n, _ptr(rs), _ptr(col), _ptr(vals), _ptr(x), cp, parts, _ptr(y), _ptr(info))
+    assert rc == 0, L.last_error()
+    ref = sym_upper_spmv(rs, col, vals, x)
+    np.testing.assert_allclose(y, ref, rtol=1e-12, atol=1e-10)
+    return info
+
+
+@pytest.mark.parametrize("parts", [1, 3, 16])
+def test_slab_plan_structured_boxes(parts):
+    for scene in (meshes.config1(), meshes.small_box(7, 3, 5), meshes.config5()):
+        rs, col, coords = _pattern_and_coords(scene)
+        info = _check(rs, col, coords, parts)
+        assert info[0] == min(parts, len(rs) - 1)
+        assert 0 < info[1] <= 6144
+
+
+def test_slab_plan_block128_at_148_parts_fits_shared_memory():
+    scene = meshes.config4()
+    rs, col, coords = _pattern_and_coords(scene)
+    info = _check(rs, col, coords, 148, seed=5)
+    n = len(rs) - 1
+    assert info[0] == 148
+    assert info[1] <= 6144  # window of every part inside the kernel's shared-memory window
+    assert info[2] <= 128
+    assert info[1] < 2 * (n // 148)  # coordinate cuts keep halos well below the part size
+
+
+def test_slab_plan_randomly_numbered_body():
+    scene = meshes.small_box(6, 5, 4)
+    body = scene.bodies[0]
+    rng = np.random.default_rng(3)
+    perm = rng.permutation(body.positions.shape[0])
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(perm.size)
+    body.positions = body.positions[perm]
+    body.tets = inv[body.tets].astype(np.int32)
+    body.pinned = body.pinned[perm]
+    rs, col, coords = _pattern_and_coords(scene)
+    _check(rs, col, coords, 5, seed=2)
+    _check(rs, col, None, 5, seed=2)  # contiguous parts of the scattered numbering
+
+
+def test_slab_plan_bodies_and_rows_without_positions():
+    scene = meshes.small_box(4, 3, 3)
+    scene.bodies.append(meshes.small_box(3, 5, 2, seed=9).bodies[0])
+    rs, col, coords = _pattern_and_coords(scene)
+    for parts in (1, 2, 7):
+        _check(rs, col, coords, parts, seed=4)
+        _check(rs, col, None, parts, seed=4)
+    # every row in one spot: the cuts fall back to row order and still cover every row
+    _check(rs, col, np.zeros_like(coords), 4, seed=6)
+
+
+def test_slab_plan_rejects_too_large_windows():
+    rs, col, coords = _pattern_and_coords(meshes.config2())
+    n = len(rs) - 1
+    vals = np.zeros(9 * len(col))
+    x = np.zeros((n, 3))
+    y = np.zeros((n, 3))
+    # one part: the whole 18k-row beam is one window, more than shared memory holds
+    rc = L.PK.pk_slab_plan_selfcheck(n, _ptr(rs), _ptr(col), _ptr(vals), _ptr(x), _ptr(coords), 1, _ptr(y), None)
+    assert rc == L.PK_ERR_UNSUPPORTED
+    assert "window" in L.last_error()
