@@ -376,23 +376,35 @@ __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v)
 // instead of one poller per slot.  The parity buffers keep a block that runs ahead from
 // overwriting a slot that another block has not read yet: to publish generation g + 2 it
 // must have seen every block publish g + 1, which each does only after reading g.
+//
+// Split in two halves so a block can issue independent loads while it waits:
+// count_publish reduces the block's partials (ending with a block barrier, so every
+// store of the block made before it is visible to the block) and publishes them;
+// count_finish waits and reduces.  count_exchange is both.
 template <class Acc, int N>
-__device__ bool count_exchange(ExSlot* slots, GridSync* sync, unsigned gen, Acc (&v)[N], int& bad, Acc* sh, int* shi)
+__device__ __forceinline__ void count_publish(ExSlot* slots, GridSync* sync, unsigned gen, Acc (&v)[N], int& bad,
+                                              Acc* sh, int* shi)
 {
     static_assert(N >= 1 && N <= 2, "two partials per slot");
     block_sum_or<Acc, N>(v, bad, sh, shi);
+    const int G = gridDim.x;
+    if (G > 1 && threadIdx.x == 0) {
+        ExSlot* my = slots + (gen & 1u) * (unsigned)G + blockIdx.x;
+        my->v0 = double(v[0]);
+        my->v1 = N > 1 ? double(v[N - 1]) : 0.0;
+        my->bad = bad;
+        __threadfence();
+        red_release_add(&sync->arrive, 1u);
+    }
+}
+
+template <class Acc, int N>
+__device__ bool count_finish(ExSlot* slots, GridSync* sync, unsigned gen, Acc (&v)[N], int& bad, Acc* sh, int* shi)
+{
     const int G = gridDim.x, tid = threadIdx.x, lane = tid & 31;
     if (G <= 1) return !*(volatile int*)&sync->err;
-    ExSlot* buf = slots + (gen & 1u) * (unsigned)G;
+    const ExSlot* buf = slots + (gen & 1u) * (unsigned)G;
     if (tid < 32) {
-        if (tid == 0) {
-            ExSlot* my = buf + blockIdx.x;
-            my->v0 = double(v[0]);
-            my->v1 = N > 1 ? double(v[N - 1]) : 0.0;
-            my->bad = bad;
-            __threadfence();
-            red_release_add(&sync->arrive, 1u);
-        }
         const unsigned target = gen * (unsigned)G;
         int fail = 0;
         unsigned long long spins = 0;
@@ -438,6 +450,14 @@ __device__ bool count_exchange(ExSlot* slots, GridSync* sync, unsigned gen, Acc 
     const int failed = shi[1];
     __syncthreads();
     return !failed && !*(volatile int*)&sync->err;
+}
+
+template <class Acc, int N>
+__device__ __forceinline__ bool count_exchange(ExSlot* slots, GridSync* sync, unsigned gen, Acc (&v)[N], int& bad,
+                                               Acc* sh, int* shi)
+{
+    count_publish<Acc, N>(slots, sync, gen, v, bad, sh, shi);
+    return count_finish<Acc, N>(slots, sync, gen, v, bad, sh, shi);
 }
 
 // The whole grid as one group (slots: two buffers of gridDim.x).

@@ -282,6 +282,8 @@ static_assert(kSlabStages % kSlabGroups == 0, "a stage must always return to the
 static_assert(kSlabWinBytes % 128 == 0 && kSlabStageBytes % 128 == 0, "stages must stay 128-byte aligned");
 static_assert(kSlabSmemBytes + 2048 <= 232448, "dynamic + static shared memory must fit one block per SM");
 static_assert(kSlabRows * kSlabLanesPerRow == 32 * kSlabGroupWarps, "one tile row per lane group");
+static_assert(kSlabRowThreads == 32 * kSlabConsumerWarps, "the consumer warps own the rows");
+static_assert(kSlabGroups * kSlabRowsPerThread * 16 <= 512, "row records must fit tensor memory");
 
 template <class Acc>
 struct SlabPcgArgs {
@@ -297,11 +299,8 @@ struct SlabPcgArgs {
     const float* b;              // per dynamic row
     const float* minv;
     float* x;                    // per dynamic row: delta-v out
-    float* xs;                   // 4 per slab row
-    float* rs;
-    float* qs;
-    float* ss;
-    float* minvs;                // 12 per slab row (three padded columns)
+    float* qs;                   // 4 per slab row: q of phase A
+    float* ss;                   // 4 per slab row: s published for the window passes
     ExSlot* slots;               // [2][grid]
     GridSync* sync;
     int max_iterations;

@@ -22,8 +22,11 @@
 //   exchange reduces the blocks' partials in one fixed tree that every block evaluates
 //   identically: all blocks take the same decisions and a run repeats bit for bit.
 //
-// Vectors x, r, q, s are kept per slab row (float4) and M^-1 as three padded columns, so
-// the per-row phases read them coalesced.  Every wait is bounded; a wait that gives up
+// Each row's x, r and M^-1 live in tensor memory (TMEM) for the whole solve: the twelve
+// consumer warps own rows t + 384k (t = their thread, k < 10), and warp w keeps row k at
+// TMEM lane 32 (w % 4) + lane, columns 160 (w / 4) + 16k .. + 15, read and written with
+// tcgen05.ld / tcgen05.st.  Only q (phase A -> phase B, other threads) and the published
+// s go through global memory.  Every wait is bounded; a wait that gives up
 // sets the error flag and the kernel leaves through its normal exit, after waiting
 // (bounded) for its own bulk copies still in flight.  No TMA multicast is used.
 #include <cuda_runtime.h>
@@ -65,23 +68,51 @@ __device__ __forceinline__ void stv4(float* p, V3<float> v)
 {
     __stcg(reinterpret_cast<float4*>(p), make_float4(v.x, v.y, v.z, 0.f));
 }
-// M^-1 of a slab row: three padded columns.
-__device__ __forceinline__ M3<float> ldm12(const float* p)
+// ------------------------------------------------------------------ tensor memory
+// One row record: 16 32-bit columns {x.xyz, r.xyz, M^-1 (9, column-major), unused}.  Each
+// load / store is warp-wide (.sync.aligned) and waits for its own completion.
+struct RowRec {
+    unsigned w[16];
+};
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, RowRec& r)
 {
-    const float4 a = __ldcg(reinterpret_cast<const float4*>(p));
-    const float4 b = __ldcg(reinterpret_cast<const float4*>(p) + 1);
-    const float4 c = __ldcg(reinterpret_cast<const float4*>(p) + 2);
-    M3<float> m;
-    m.c[0] = V3<float>{a.x, a.y, a.z};
-    m.c[1] = V3<float>{b.x, b.y, b.z};
-    m.c[2] = V3<float>{c.x, c.y, c.z};
-    return m;
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r.w[0]), "=r"(r.w[1]), "=r"(r.w[2]), "=r"(r.w[3]), "=r"(r.w[4]), "=r"(r.w[5]), "=r"(r.w[6]),
+          "=r"(r.w[7]), "=r"(r.w[8]), "=r"(r.w[9]), "=r"(r.w[10]), "=r"(r.w[11]), "=r"(r.w[12]), "=r"(r.w[13]),
+          "=r"(r.w[14]), "=r"(r.w[15])
+        : "r"(taddr)
+        : "memory");
 }
-__device__ __forceinline__ void stm12(float* p, const M3<float>& m)
+__device__ __forceinline__ void tmem_st16(unsigned taddr, const RowRec& r)
 {
-    __stcg(reinterpret_cast<float4*>(p), make_float4(m.c[0].x, m.c[0].y, m.c[0].z, 0.f));
-    __stcg(reinterpret_cast<float4*>(p) + 1, make_float4(m.c[1].x, m.c[1].y, m.c[1].z, 0.f));
-    __stcg(reinterpret_cast<float4*>(p) + 2, make_float4(m.c[2].x, m.c[2].y, m.c[2].z, 0.f));
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};\n\t"
+        "tcgen05.wait::st.sync.aligned;" ::"r"(taddr),
+        "r"(r.w[0]), "r"(r.w[1]), "r"(r.w[2]), "r"(r.w[3]), "r"(r.w[4]), "r"(r.w[5]), "r"(r.w[6]), "r"(r.w[7]),
+        "r"(r.w[8]), "r"(r.w[9]), "r"(r.w[10]), "r"(r.w[11]), "r"(r.w[12]), "r"(r.w[13]), "r"(r.w[14]), "r"(r.w[15])
+        : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ V3<float> rec3(const RowRec& r, int o)
+{
+    return V3<float>{__uint_as_float(r.w[o]), __uint_as_float(r.w[o + 1]), __uint_as_float(r.w[o + 2])};
+}
+__device__ __forceinline__ void put3(RowRec& r, int o, V3<float> v)
+{
+    r.w[o] = __float_as_uint(v.x);
+    r.w[o + 1] = __float_as_uint(v.y);
+    r.w[o + 2] = __float_as_uint(v.z);
+}
+__device__ __forceinline__ M3<float> rec_minv(const RowRec& r)
+{
+    M3<float> m;
+    m.c[0] = rec3(r, 6);
+    m.c[1] = rec3(r, 9);
+    m.c[2] = rec3(r, 12);
+    return m;
 }
 
 template <class Acc>
@@ -96,6 +127,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     __shared__ int sh_int[32];
     __shared__ int s_fail;
     __shared__ int s_bad;
+    __shared__ unsigned s_tmem;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, blk = blockIdx.x;
     const bool producer = warp == kSlabConsumerWarps;
@@ -131,7 +163,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
         s_bad = 0;
     }
     __syncthreads();
-    if (m < 0 || h < 0 || m + h > kSlabWinCap || row0 < 0 || row0 + m > P.n || ntiles < 0 ||
+    if (m < 0 || m > kSlabMaxRows || h < 0 || m + h > kSlabWinCap || row0 < 0 || row0 + m > P.n || ntiles < 0 ||
         ntiles > kSlabMaxTiles || halo0 < 0 || halo0 + h > P.halo_count || tile0 < 0 ||
         tile0 + ntiles > P.tile_count) {
         m = h = ntiles = 0;
@@ -166,6 +198,21 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
         return;
     }
 
+    // Tensor memory for the rows' x, r, M^-1 (all 512 columns: one block per SM).
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
+                     "r"(512u)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tmem_fence_before();
+    __syncthreads();
+    tmem_fence_after();
+    const bool row_owner = warp < kSlabConsumerWarps;  // the 384 threads of the per-row phases
+    const int rt = tid;                                 // rows rt + 384 k
+    const int krows = (m + kSlabRowThreads - 1) / kSlabRowThreads;
+    const unsigned tmem_row0 =
+        s_tmem + ((32u * (unsigned)(warp % 4)) << 16) + (unsigned)((warp / 4) * kSlabRowsPerThread * 16);
     const unsigned long long pol = l2_evict_first_policy();
     unsigned ring = 0;    // ring positions consumed so far (ntiles per iteration)
     unsigned issued = 0;  // ring positions issued by the producer (producer lane 0 only)
@@ -278,27 +325,37 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     bool timed_out = false;
     Acc delta = Acc(0), rr = Acc(0), target = Acc(0);
     {
-        // x = 0, r = b, s = M^-1 r (slab order), d = 0 in the window; r.s, |r|^2, finiteness.
+        // x = 0, r = b, M^-1 into tensor memory; s = M^-1 r published; d = 0 in the window;
+        // r.s, |r|^2, finiteness.
         Acc v[2] = {Acc(0), Acc(0)};
         int bad = s_bad ? 4 : 0;
-        for (int i = tid; i < m; i += blockDim.x) {
-            const int g = row0 + i;
-            int c = __ldg(P.perm + g);
-            if ((unsigned)c >= (unsigned)P.n) {
-                c = 0;
-                bad |= 4;
+        if (row_owner) {
+            for (int k = 0; k < krows; ++k) {
+                const int i = rt + kSlabRowThreads * k;
+                RowRec rec{};
+                if (i < m) {
+                    const int g = row0 + i;
+                    int c = __ldg(P.perm + g);
+                    if ((unsigned)c >= (unsigned)P.n) {
+                        c = 0;
+                        bad |= 4;
+                    }
+                    const V3<float> br = ld3(P.b, c);
+                    if (!finite3(br)) bad |= 1;
+                    const M3<float> mi = ld9(P.minv, (size_t)c);
+                    const V3<float> sv = mul(mi, br);
+                    if (!finite9(mi) || !finite3(sv)) bad |= 2;
+                    put3(rec, 0, V3<float>{0.f, 0.f, 0.f});
+                    put3(rec, 3, br);
+                    put3(rec, 6, mi.c[0]);
+                    put3(rec, 9, mi.c[1]);
+                    put3(rec, 12, mi.c[2]);
+                    stv4(P.ss + 4 * (size_t)g, sv);
+                    v[0] += dot_acc<Acc>(br, sv);
+                    v[1] += dot_acc<Acc>(br, br);
+                }
+                tmem_st16(tmem_row0 + 16u * (unsigned)k, rec);
             }
-            const V3<float> br = ld3(P.b, c);
-            if (!finite3(br)) bad |= 1;
-            const M3<float> mi = ld9(P.minv, (size_t)c);
-            const V3<float> sv = mul(mi, br);
-            if (!finite9(mi) || !finite3(sv)) bad |= 2;
-            stv4(P.xs + 4 * (size_t)g, V3<float>{0.f, 0.f, 0.f});
-            stv4(P.rs + 4 * (size_t)g, br);
-            stv4(P.ss + 4 * (size_t)g, sv);
-            stm12(P.minvs + 12 * (size_t)g, mi);
-            v[0] += dot_acc<Acc>(br, sv);
-            v[1] += dot_acc<Acc>(br, br);
         }
         for (int w = tid; w < 3 * wn; w += blockDim.x) win[w] = 0.f;
         if (!count_exchange<Acc, 2>(P.slots, P.sync, ++xgen, v, bad, sh_acc, sh_int)) {
@@ -385,7 +442,17 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                 qbad = 1;
                 atomicExch(&P.sync->err, 1);
             }
-            if (!count_exchange<Acc, 1>(P.slots, P.sync, ++xgen, dq, qbad, sh_acc, sh_int)) {
+            count_publish<Acc, 1>(P.slots, P.sync, ++xgen, dq, qbad, sh_acc, sh_int);
+            // Phase B's q (written by other threads in phase A, visible after the publish's
+            // block barrier) loads while the exchange completes.
+            V3<float> qv[kSlabRowsPerThread];
+#pragma unroll
+            for (int k = 0; k < kSlabRowsPerThread; ++k) {
+                const int i = rt + kSlabRowThreads * k;
+                qv[k] = (row_owner && k < krows && i < m) ? ldv4(P.qs + 4 * (size_t)(row0 + i))
+                                                          : V3<float>{0.f, 0.f, 0.f};
+            }
+            if (!count_finish<Acc, 1>(P.slots, P.sync, xgen, dq, qbad, sh_acc, sh_int)) {
                 timed_out = true;
                 goto finish;
             }
@@ -402,48 +469,30 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                 fl |= kFlagBreakdown;
                 break;
             }
-            // Phase B: x += alpha d; r -= alpha q; s = M^-1 r; partials r.s and r.r.
-            // kRowBatch rows per thread per pass, all their loads issued before any store.
+            // Phase B: x += alpha d; r -= alpha q; s = M^-1 r; partials r.s and r.r.  x, r,
+            // M^-1 from tensor memory; q was loaded while the exchange completed.
             Acc v[2] = {Acc(0), Acc(0)};
             int sbad = 0;
-            {
-                constexpr int kRowBatch = 2;
-                const int step = (int)blockDim.x;
-                for (int i0 = tid; i0 < m; i0 += kRowBatch * step) {
-                    int li[kRowBatch];
-                    bool ok[kRowBatch];
+            if (row_owner) {
 #pragma unroll
-                    for (int k = 0; k < kRowBatch; ++k) {
-                        const int i = i0 + k * step;
-                        ok[k] = i < m;
-                        li[k] = ok[k] ? i : i0;
-                    }
-                    V3<float> dn[kRowBatch], q[kRowBatch], xo[kRowBatch], ro[kRowBatch];
-                    M3<float> mi[kRowBatch];
-#pragma unroll
-                    for (int k = 0; k < kRowBatch; ++k) {
-                        const size_t g = (size_t)(row0 + li[k]);
-                        const float* d = win + 3 * li[k];
-                        dn[k] = V3<float>{d[0], d[1], d[2]};
-                        q[k] = ldv4(P.qs + 4 * g);
-                        xo[k] = ldv4(P.xs + 4 * g);
-                        ro[k] = ldv4(P.rs + 4 * g);
-                        mi[k] = ldm12(P.minvs + 12 * g);
-                    }
-#pragma unroll
-                    for (int k = 0; k < kRowBatch; ++k) {
-                        if (!ok[k]) continue;
-                        const size_t g = (size_t)(row0 + li[k]);
-                        const V3<float> xv = axpy<float, Acc>(xo[k], alpha, dn[k]);
-                        const V3<float> rv = axpy<float, Acc>(ro[k], -alpha, q[k]);
-                        stv4(P.xs + 4 * g, xv);
-                        stv4(P.rs + 4 * g, rv);
-                        const V3<float> sv = mul(mi[k], rv);
+                for (int k = 0; k < kSlabRowsPerThread; ++k) {
+                    if (k >= krows) break;
+                    const int i = rt + kSlabRowThreads * k;
+                    RowRec rec;
+                    tmem_ld16(tmem_row0 + 16u * (unsigned)k, rec);
+                    if (i < m) {
+                        const float* d = win + 3 * i;
+                        const V3<float> xv = axpy<float, Acc>(rec3(rec, 0), alpha, V3<float>{d[0], d[1], d[2]});
+                        const V3<float> rv = axpy<float, Acc>(rec3(rec, 3), -alpha, qv[k]);
+                        const V3<float> sv = mul(rec_minv(rec), rv);
                         if (!finite3(sv)) sbad = 1;
-                        stv4(P.ss + 4 * g, sv);
+                        stv4(P.ss + 4 * (size_t)(row0 + i), sv);
                         v[0] += dot_acc<Acc>(rv, sv);
                         v[1] += dot_acc<Acc>(rv, rv);
+                        put3(rec, 0, xv);
+                        put3(rec, 3, rv);
                     }
+                    tmem_st16(tmem_row0 + 16u * (unsigned)k, rec);
                 }
             }
             if (!count_exchange<Acc, 2>(P.slots, P.sync, ++xgen, v, sbad, sh_acc, sh_int)) {
@@ -478,22 +527,28 @@ final_check:
     {
         int bad = 0;
         Acc none[1] = {Acc(0)};
-        for (int i = tid; i < m; i += blockDim.x) {
-            const int g = row0 + i;
-            const int c = __ldg(P.perm + g);
-            if ((unsigned)c >= (unsigned)P.n) {
-                bad |= 1;
-                continue;
-            }
-            const V3<float> dv = have_x ? ldv4(P.xs + 4 * (size_t)g) : V3<float>{0.f, 0.f, 0.f};
-            st3(P.x, c, dv);
-            if (!finite3(dv)) bad |= 1;
-            if (P.integrate) {
-                const int node = __ldg(P.dyn_to_node + c);
-                const V3<float> xo = ldplain3(P.node_x, node), vo = ldplain3(P.node_v, node);
-                const V3<float> nv = vo + dv;
-                const V3<float> nx = xo + nv * P.dt;
-                if (!finite3(xo) || !finite3(vo) || !finite3(nv) || !finite3(nx)) bad |= 2;
+        if (row_owner) {
+            for (int k = 0; k < krows; ++k) {
+                const int i = rt + kSlabRowThreads * k;
+                RowRec rec;
+                tmem_ld16(tmem_row0 + 16u * (unsigned)k, rec);
+                if (i >= m) continue;
+                const int g = row0 + i;
+                const int c = __ldg(P.perm + g);
+                if ((unsigned)c >= (unsigned)P.n) {
+                    bad |= 1;
+                    continue;
+                }
+                const V3<float> dv = have_x ? rec3(rec, 0) : V3<float>{0.f, 0.f, 0.f};
+                st3(P.x, c, dv);
+                if (!finite3(dv)) bad |= 1;
+                if (P.integrate) {
+                    const int node = __ldg(P.dyn_to_node + c);
+                    const V3<float> xo = ldplain3(P.node_x, node), vo = ldplain3(P.node_v, node);
+                    const V3<float> nv = vo + dv;
+                    const V3<float> nx = xo + nv * P.dt;
+                    if (!finite3(xo) || !finite3(vo) || !finite3(nv) || !finite3(nx)) bad |= 2;
+                }
             }
         }
         if (!count_exchange<Acc, 1>(P.slots, P.sync, ++xgen, none, bad, sh_acc, sh_int)) {
@@ -508,11 +563,11 @@ final_check:
             if (bad & 2) {
                 fl |= kFlagIntegrateAbort;
             } else {
-                for (int i = tid; i < m; i += blockDim.x) {
+                for (int i = row_owner ? rt : m; i < m; i += kSlabRowThreads) {
                     const int g = row0 + i;
                     const int c = __ldg(P.perm + g);
                     const int node = __ldg(P.dyn_to_node + c);
-                    const V3<float> dv = ldv4(P.xs + 4 * (size_t)g);
+                    const V3<float> dv = ldplain3(P.x, c);  // written above by this thread
                     const V3<float> nv = ldplain3(P.node_v, node) + dv;
                     const V3<float> nx = ldplain3(P.node_x, node) + nv * P.dt;
                     st3(P.node_v, node, nv);
@@ -533,6 +588,13 @@ finish:
             const unsigned p = issued - 1 - k;
             (void)mbar_wait(&full_bar[p % S], (p / S) & 1u);
         }
+    }
+    // Release the tensor memory once every warp's accesses are done.
+    tmem_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tmem_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s_tmem), "r"(512u) : "memory");
     }
     if (blk == 0 && tid == 0) {
         P.stats->iterations = iterations;

@@ -125,6 +125,7 @@ std::string build_slab_plan(int n, const int* row_start, const int* col, const i
     size_t stream_bytes = 0;
     for (int p = 0; p < parts; ++p) {
         const int g0 = count[p], g1 = count[p + 1], m = g1 - g0;
+        if (m > kSlabMaxRows) return "a part has more rows than tensor memory holds";
         for (int g = g0; g < g1; ++g) win_of[out.perm[g]] = g - g0;
         // halo rows, ascending slab index
         std::vector<int> halo;

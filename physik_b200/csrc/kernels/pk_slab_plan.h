@@ -40,6 +40,9 @@ constexpr int kSlabStageBytes = 19584; // >= kSlabHeaderBytes + kSlabCapE * kSla
 constexpr int kSlabStages = 6;         // multiple of the consumer groups
 constexpr int kSlabWinCap = 6144;      // window rows (owned + halo) per part
 constexpr int kSlabMaxTiles = 128;     // tiles per part
+constexpr int kSlabRowThreads = 384;   // threads owning rows in the per-row phases
+constexpr int kSlabRowsPerThread = 10; // row records per thread in tensor memory
+constexpr int kSlabMaxRows = kSlabRowThreads * kSlabRowsPerThread;  // rows per part
 constexpr int kSlabPartInts = 8;       // per part: row0, rows, halo0, halo rows, tile0, tiles, 0, 0
 constexpr unsigned kSlabNoPos = 0xffffffffu;
 

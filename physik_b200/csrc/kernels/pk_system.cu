@@ -226,7 +226,7 @@ struct pk_system {
     std::string slab_reason;      // why the layout does not apply
     unsigned long long slab_stream_bytes = 0;
     DevBuf slab_part_info, slab_tiles, slab_stream, slab_halo, slab_perm, slab_pos_u, slab_pos_l;
-    DevBuf slab_xs, slab_rs, slab_qs, slab_ss, slab_minvs;
+    DevBuf slab_qs, slab_ss;
     // kernel selection: -1 automatic (slab, else ring, else staged, else plain), 0 ring,
     // 1 staged, 2 plain, 3 slab
     int kernel_choice = -1;
@@ -543,11 +543,8 @@ int ensure_slab(pk_system* s)
     if (!rc) rc = upload_raw<unsigned>(s->slab_pos_l, plan.pos_l.data(), plan.pos_l.size(), s->stream);
     if (rc) return rc;
     const size_t rows = static_cast<size_t>(n);
-    PK_CHECK(s->slab_xs.ensure(16 * rows));
-    PK_CHECK(s->slab_rs.ensure(16 * rows));
     PK_CHECK(s->slab_qs.ensure(16 * rows));
     PK_CHECK(s->slab_ss.ensure(16 * rows));
-    PK_CHECK(s->slab_minvs.ensure(48 * rows));
     PK_CHECK(cudaStreamSynchronize(s->stream));
     s->slab_stream_bytes = plan.stream.size();
     s->slab_tile_count = static_cast<int>(plan.tile_desc.size() / 4);
@@ -593,11 +590,8 @@ int run_pcg_slab(pk_system* s, const pk_step_params& p, int skip_on_flags)
         a.b = s->rhs.as<float>();
         a.minv = s->minv.as<float>();
         a.x = s->px.as<float>();
-        a.xs = s->slab_xs.as<float>();
-        a.rs = s->slab_rs.as<float>();
         a.qs = s->slab_qs.as<float>();
         a.ss = s->slab_ss.as<float>();
-        a.minvs = s->slab_minvs.as<float>();
         a.slots = s->slots.as<pk::ExSlot>();
         a.sync = s->sync.as<pk::GridSync>();
         a.max_iterations = p.max_iterations;

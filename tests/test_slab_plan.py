@@ -101,13 +101,29 @@ def test_slab_plan_bodies_and_rows_without_positions():
     _check(rs, col, np.zeros_like(coords), 4, seed=6)
 
 
-def test_slab_plan_rejects_too_large_windows():
-    rs, col, coords = _pattern_and_coords(meshes.config2())
+def _reject(rs, col, coords, parts):
     n = len(rs) - 1
     vals = np.zeros(9 * len(col))
     x = np.zeros((n, 3))
     y = np.zeros((n, 3))
-    # one part: the whole 18k-row beam is one window, more than shared memory holds
-    rc = L.PK.pk_slab_plan_selfcheck(n, _ptr(rs), _ptr(col), _ptr(vals), _ptr(x), _ptr(coords), 1, _ptr(y), None)
+    cp = _ptr(coords) if coords is not None else None
+    rc = L.PK.pk_slab_plan_selfcheck(n, _ptr(rs), _ptr(col), _ptr(vals), _ptr(x), cp, parts, _ptr(y), None)
     assert rc == L.PK_ERR_UNSUPPORTED
-    assert "window" in L.last_error()
+    return L.last_error()
+
+
+def test_slab_plan_rejects_parts_that_do_not_fit():
+    # one part for the whole 18k-row beam: more rows than tensor memory holds
+    rs, col, coords = _pattern_and_coords(meshes.config2())
+    assert "tensor memory" in _reject(rs, col, coords, 1)
+    # randomly numbered beam cut into contiguous id ranges: every part touches most rows
+    scene = meshes.config2()
+    body = scene.bodies[0]
+    perm = np.random.default_rng(5).permutation(body.positions.shape[0])
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(perm.size)
+    body.positions = body.positions[perm]
+    body.tets = inv[body.tets].astype(np.int32)
+    body.pinned = body.pinned[perm]
+    rs, col, _ = _pattern_and_coords(scene)
+    assert "window" in _reject(rs, col, None, 6)
