@@ -393,7 +393,9 @@ __device__ __forceinline__ void count_publish(ExSlot* slots, GridSync* sync, uns
         my->v0 = double(v[0]);
         my->v1 = N > 1 ? double(v[N - 1]) : 0.0;
         my->bad = bad;
-        __threadfence();
+        // Release fence (cumulative over the block's stores ordered before it by the block
+        // barrier), then the release increment.
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
         red_release_add(&sync->arrive, 1u);
     }
 }
