@@ -362,12 +362,14 @@ def run_ours(args, scene, rank, world, local, pg):
         w.set_state(xs, vs, f64=True)
         ref.step()
         w.step()
-        xr, _ = ref.state(f64=True)
-        xm, _ = w.state(f64=True)
+        xr, vr = ref.state(f64=True)
+        xm, vm = w.state(f64=True)
         err = float(np.linalg.norm(xm - xr) / np.linalg.norm(xr))
+        verr = float(np.linalg.norm(vm - vr) / max(np.linalg.norm(vr), 1e-300))
         fp64 = {"steps_per_s": k / (ref_ms / 1e3), "ms_per_step": ref_ms / k, "steps": k,
                 "solve": "one coupled PCG over all bodies, FP64 storage and arithmetic",
-                "mixed_position_rel_err_vs_fp64_one_step": err}
+                "mixed_position_rel_err_vs_fp64_one_step": err,
+                "mixed_velocity_rel_err_vs_fp64_one_step": verr}
         del ref
 
     steps_total = args.steps * world if not batched else args.steps

@@ -198,6 +198,11 @@ PHYSIK_B200_API int PHYSIK_B200_Autotune(PhysikWorldHandle world, int repeats, d
  * TMA-staged, 2 unstaged, 3 part-resident, 4 batched) or -1; blocks (may be NULL)
  * receives the blocks it ran on. */
 PHYSIK_B200_API int PHYSIK_B200_GetPcgKernel(PhysikWorldHandle world, int* blocks);
+/* FP64 outer true-residual refinement of the implicit solve for FP32 and mixed precision
+ * (no counterpart in the reference; see pk_system_set_refinement): up to `passes`
+ * correction solves (0..16, 0 = off, the default) within the step's iteration budget,
+ * until the true residual meets the CG's stopping target.  0 on success, -1 on error. */
+PHYSIK_B200_API int PHYSIK_B200_SetRefinement(PhysikWorldHandle world, int passes);
 /* Batched solve: one PCG per tet-mesh physics component (own scalars, stopping test,
  * iteration count and all-or-nothing integration, as a world holding only that body),
  * all bodies in one launch, instead of the reference's single coupled PCG over the whole

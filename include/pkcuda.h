@@ -174,6 +174,15 @@ PKCUDA_API int pk_system_set_pcg_grid(pk_system* sys, int grid);
 PKCUDA_API int pk_system_adjoint_step(pk_system* sys, const pk_step_params* params, const double* xbar_next,
                                       const double* vbar_next, double* xbar, double* vbar, double* theta_bar);
 
+/* FP64 outer true-residual refinement for FP32 storage (FP32 and mixed precision,
+ * unbatched; no counterpart in the reference): after the step's PCG, while the true
+ * residual b - A x computed with FP64 arithmetic over the assembled blocks misses the
+ * reference's stopping target r^T M^-1 r <= tol^2 b^T M^-1 b and iterations remain of the
+ * step's max_iterations, up to `passes` correction solves are run and added in FP64; the
+ * update then uses the FP64 delta-v.  The step's statistics become the total iterations
+ * and the true residual's convergence and norm.  0 (the default) turns it off.  Such
+ * steps synchronise with the host and are not graph-captured. */
+PKCUDA_API int pk_system_set_refinement(pk_system* sys, int passes);
 /* The PCG kernel of the last solve: 0 ring-staged, 1 TMA-staged, 2 unstaged, 3
  * part-resident, 4 batched per-body; -1 before the first solve (or a negative PK_ERR_*).
  * blocks (may be NULL) receives the blocks it ran on. */

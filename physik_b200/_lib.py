@@ -96,6 +96,7 @@ _SIGS = {
     "pk_system_adjoint_step": (_i, [_p, C.POINTER(PkStepParams), _p, _p, _p, _p, _p]),
     "pk_system_autotune": (_i, [_p, C.POINTER(PkStepParams), _i, _p, _p]),
     "pk_system_pcg_kernel": (_i, [_p, _p]),
+    "pk_system_set_refinement": (_i, [_p, _i]),
     # physik_b200.h
     "PHYSIK_CreateWorld": (_p, []),
     "PHYSIK_DestroyWorld": (_v, [_p]),
@@ -165,6 +166,7 @@ _SIGS = {
     "PHYSIK_B200_GetTetCount": (_i, [_p]),
     "PHYSIK_B200_Autotune": (_i, [_p, _i, _p]),
     "PHYSIK_B200_GetPcgKernel": (_i, [_p, _p]),
+    "PHYSIK_B200_SetRefinement": (_i, [_p, _i]),
     "PHYSIK_B200_GetBodyConjugateGradientStats": (_i, [_p, _H, _p, _p, _p, _p]),
     "PHYSIK_B200_GetStream": (_p, [_p]),
     "PHYSIK_B200_Synchronize": (_i, [_p]),

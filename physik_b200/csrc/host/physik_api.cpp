@@ -612,6 +612,14 @@ PHYSIK_B200_API int PHYSIK_B200_GetPcgKernel(PhysikWorldHandle world, int* block
     return Guard([&] { return w->GetPcgKernel(blocks); }, -1);
 }
 
+PHYSIK_B200_API int PHYSIK_B200_SetRefinement(PhysikWorldHandle world, int passes)
+{
+    World* w = AsWorld(world);
+    if (!w || passes < 0 || passes > 16) return -1;
+    w->SetRefinement(passes);
+    return 0;
+}
+
 PHYSIK_B200_API int PHYSIK_B200_SetPcgGrid(PhysikWorldHandle world, int grid)
 {
     World* w = AsWorld(world);

@@ -400,6 +400,10 @@ public:
 
     // CUDA-graph capture of the device step (extension).
     void SetGraphCapture(bool on) { graphCapture = on; }
+    // FP64 outer true-residual refinement passes for FP32 storage (extension; see
+    // pk_system_set_refinement).  0: off.
+    void SetRefinement(int passes) { refinePasses = passes < 0 ? 0 : passes; }
+    int GetRefinement() const { return refinePasses; }
     // Autotuner (extension): picks the fastest PCG kernel / tile or part size for the
     // current scene by timing `repeats` solves of the last assembled system (call after a
     // step).  Returns the chosen candidate index (see pk_system_autotune) or -1.
@@ -475,6 +479,7 @@ private:
     int device = 0;
     bool batchedSolve = false;
     bool graphCapture = false;
+    int refinePasses = 0;
     float lastSubstepDt = 0.0f;
     std::uint64_t topologyVersion = 1;
 

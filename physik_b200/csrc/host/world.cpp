@@ -351,6 +351,7 @@ struct DeviceScene {
     bool segmentsCover = false;
     bool batchedOnDevice = false;
     bool graphOnDevice = false;
+    int refineOnDevice = 0;
     std::vector<unsigned char> enabled;
     std::vector<double> mass, dmInv, volume, lam, mu, damp;
 
@@ -533,6 +534,7 @@ void UploadScene(DeviceScene& sc, const std::vector<Vec3>& positions, const std:
           "set_pattern");
     sc.batchedOnDevice = false;
     sc.graphOnDevice = false;
+    sc.refineOnDevice = 0;
     sc.uploaded = true;
 }
 
@@ -985,6 +987,10 @@ void World::RunSubstep(float dt)
     if (graphCapture != scene->graphOnDevice) {
         Check(pk_system_set_graph(scene->sys, graphCapture ? 1 : 0), "set_graph");
         scene->graphOnDevice = graphCapture;
+    }
+    if (refinePasses != scene->refineOnDevice) {
+        Check(pk_system_set_refinement(scene->sys, refinePasses), "set_refinement");
+        scene->refineOnDevice = refinePasses;
     }
     lastSubstepDt = dt;
     Check(pk_system_step(scene->sys, &p), "pk_system_step");

@@ -315,6 +315,39 @@ struct SlabPcgArgs {
     DevStats* stats;
 };
 
+// ------------------------------------------------------------------ FP64 refinement
+// Kernels of the outer true-residual refinement (pk_refine.cu).
+constexpr int kRefineThreads = 256;
+
+template <class Real>
+struct RefineArgs {
+    BsrView<Real> a;
+    const Real* b;           // assembled right-hand side (kept while corrections run)
+    const Real* minv;
+    const double* x64;       // FP64 solution so far (NULL: x = 0)
+    Real* rhs_out;           // residual rounded to Real: the next correction's rhs (may be NULL)
+    double* partials;        // 2 per block: r^T M^-1 r, r.r
+    int* bad;                // non-finite residual / update flags (cleared by the caller)
+    // update
+    Real* dx;                // delta-v in the storage type (written by the update)
+    int integrate;
+    Real dt;
+    const int* dyn_to_node;
+    Real* node_x;
+    Real* node_v;
+};
+
+template <class Real>
+int refine_residual_blocks(int n);
+template <class Real>
+cudaError_t launch_refine_residual(const RefineArgs<Real>& args, cudaStream_t stream);
+template <class Real>
+cudaError_t launch_refine_accumulate(double* x64, const Real* dx, int count, int first, cudaStream_t stream);
+// Check pass (delta-v rounded and written to args.dx, finiteness into *args.bad), then, if
+// args.integrate, the update of velocities and positions when nothing failed.
+template <class Real>
+cudaError_t launch_refine_update(const RefineArgs<Real>& args, cudaStream_t stream);
+
 // ------------------------------------------------------------------ adjoint step
 // Backward element kernel (pk_adjoint.cu): per tet, the sensitivities of
 // J = dt w.f(x) - dt^2 w.K(x) z to the tet's node positions (12 doubles) and to its

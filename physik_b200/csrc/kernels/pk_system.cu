@@ -227,6 +227,9 @@ struct pk_system {
     unsigned long long slab_stream_bytes = 0;
     DevBuf slab_part_info, slab_tiles, slab_stream, slab_halo, slab_perm, slab_pos_u, slab_pos_l;
     DevBuf slab_qs, slab_ss;
+    // FP64 outer true-residual refinement (FP32 storage, unbatched): passes, buffers
+    int refine_passes = 0;
+    DevBuf ref_x64, ref_rhs, ref_part, ref_bad;
     // kernel selection: -1 automatic (slab, else ring, else staged, else plain), 0 ring,
     // 1 staged, 2 plain, 3 slab
     int kernel_choice = -1;
@@ -770,6 +773,131 @@ int run_pcg(pk_system* s, const pk_step_params& p, int skip_on_flags)
     return PK_OK;
 }
 
+// The solve with the FP64 outer true-residual refinement (pk_refine.cu): the first solve
+// as usual but without integration; then, while the true residual r = b - A x (FP64 over
+// the stored blocks, x accumulated in FP64) misses the reference's target r^T M^-1 r <=
+// tol^2 b^T M^-1 b and iterations remain of the step's budget, a correction solve A e = r
+// to the matching relative tolerance, x += e.  Finally the all-or-nothing update from the
+// FP64 delta-v.  Statistics: total iterations, convergence and norm of the true residual.
+// Synchronous (the host reads each residual), so such steps are never graph-captured.
+template <class Real, class Acc>
+int run_pcg_refined(pk_system* s, const pk_step_params& p, int skip_on_flags)
+{
+    const int n = s->dyn_count;
+    const size_t n3 = 3 * static_cast<size_t>(n);
+    pk_step_params q = p;
+    q.integrate = 0;
+    int rc = run_pcg<Real, Acc>(s, q, skip_on_flags);
+    if (rc) return rc;
+    pk::DevStats st{};
+    PK_CHECK(cudaMemcpyAsync(&st, s->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s->stream));
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    if (!(st.flags & pk::kFlagSolved)) return PK_OK;  // nothing to refine or integrate
+    const int blocks = pk::refine_residual_blocks<Real>(n);
+    PK_CHECK(s->ref_x64.ensure(sizeof(double) * n3));
+    PK_CHECK(s->ref_rhs.ensure(sizeof(Real) * n3));
+    PK_CHECK(s->ref_part.ensure(2 * sizeof(double) * static_cast<size_t>(blocks)));
+    PK_CHECK(s->ref_bad.ensure(sizeof(int)));
+    PK_CHECK(cudaMemcpyAsync(s->ref_rhs.p, s->rhs.p, sizeof(Real) * n3, cudaMemcpyDeviceToDevice, s->stream));
+    PK_CHECK(pk::launch_refine_accumulate<Real>(s->ref_x64.as<double>(), s->px.as<Real>(), static_cast<int>(n3), 1,
+                                                s->stream));
+    pk::RefineArgs<Real> a{};
+    a.a.n = n;
+    a.a.row_start = s->row_start.as<int>();
+    a.a.col = s->col.as<int>();
+    a.a.values = s->values.as<Real>();
+    a.a.lt_start = s->lt_start.as<int>();
+    a.a.lt_row = s->lt_row.as<int>();
+    a.a.lt_block = s->lt_block.as<int>();
+    a.b = s->ref_rhs.as<Real>();
+    a.minv = s->minv.as<Real>();
+    a.partials = s->ref_part.as<double>();
+    a.bad = s->ref_bad.as<int>();
+    std::vector<double> part(2 * static_cast<size_t>(blocks));
+    // r = b - A x (x == NULL: r = b); returns false on a non-finite residual.
+    auto residual = [&](const double* x, Real* rhs_out, double& rho, double& rr) -> int {
+        a.x64 = x;
+        a.rhs_out = rhs_out;
+        PK_CHECK(cudaMemsetAsync(s->ref_bad.p, 0, sizeof(int), s->stream));
+        PK_CHECK(pk::launch_refine_residual<Real>(a, s->stream));
+        int bad = 0;
+        PK_CHECK(cudaMemcpyAsync(part.data(), s->ref_part.p, sizeof(double) * part.size(), cudaMemcpyDeviceToHost,
+                                 s->stream));
+        PK_CHECK(cudaMemcpyAsync(&bad, s->ref_bad.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+        PK_CHECK(cudaStreamSynchronize(s->stream));
+        rho = 0.0;
+        rr = 0.0;
+        for (int i = 0; i < blocks; ++i) {
+            rho += part[2 * static_cast<size_t>(i)];
+            rr += part[2 * static_cast<size_t>(i) + 1];
+        }
+        return bad || !std::isfinite(rho) || !std::isfinite(rr) ? 1 : 0;
+    };
+    double rho0 = 0.0, rr0 = 0.0, rho = 0.0, rr = 0.0;
+    residual(nullptr, nullptr, rho0, rr0);
+    const double tol = static_cast<double>(static_cast<Real>(p.tolerance));
+    const double target = tol * tol * rho0;
+    int total = st.iterations;
+    bool converged = false;
+    for (int pass = 0;; ++pass) {
+        if (residual(s->ref_x64.as<double>(), s->rhs.as<Real>(), rho, rr)) break;
+        if (rho <= target) {
+            converged = true;
+            break;
+        }
+        const int remaining = p.max_iterations - total;
+        if (remaining <= 0 || pass >= s->refine_passes || !(rho > 0.0)) break;
+        q.max_iterations = remaining;
+        q.tolerance = std::sqrt(target / rho);
+        PK_CHECK(cudaMemsetAsync(s->stats.p, 0, sizeof(pk::DevStats), s->stream));
+        rc = run_pcg<Real, Acc>(s, q, 0);
+        if (rc) break;
+        pk::DevStats cs{};
+        PK_CHECK(cudaMemcpyAsync(&cs, s->stats.p, sizeof(cs), cudaMemcpyDeviceToHost, s->stream));
+        PK_CHECK(cudaStreamSynchronize(s->stream));
+        total += cs.iterations;
+        if (!(cs.flags & pk::kFlagSolved)) break;  // a failed correction is discarded
+        PK_CHECK(pk::launch_refine_accumulate<Real>(s->ref_x64.as<double>(), s->px.as<Real>(), static_cast<int>(n3),
+                                                    0, s->stream));
+        if (total >= p.max_iterations || pass + 1 > s->refine_passes) {
+            residual(s->ref_x64.as<double>(), nullptr, rho, rr);
+            converged = rho <= target;
+            break;
+        }
+    }
+    PK_CHECK(cudaMemcpyAsync(s->rhs.p, s->ref_rhs.p, sizeof(Real) * n3, cudaMemcpyDeviceToDevice, s->stream));
+    if (rc) return rc;
+    // The update from the FP64 delta-v (all or nothing), delta-v kept in px.
+    a.x64 = s->ref_x64.as<double>();
+    a.dx = s->px.as<Real>();
+    a.integrate = p.integrate;
+    a.dt = static_cast<Real>(p.dt);
+    a.dyn_to_node = s->dyn_to_node.as<int>();
+    a.node_x = s->x.as<Real>();
+    a.node_v = s->v.as<Real>();
+    PK_CHECK(cudaMemsetAsync(s->ref_bad.p, 0, sizeof(int), s->stream));
+    PK_CHECK(pk::launch_refine_update<Real>(a, s->stream));
+    int bad = 0;
+    PK_CHECK(cudaMemcpyAsync(&bad, s->ref_bad.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    unsigned fl = st.flags & ~(pk::kFlagConverged | pk::kFlagIntegrated | pk::kFlagSolved);
+    if (bad & 1) {
+        fl |= pk::kFlagNonFiniteDv;
+    } else {
+        fl |= pk::kFlagSolved;
+        if (p.integrate) fl |= (bad & 2) ? pk::kFlagIntegrateAbort : pk::kFlagIntegrated;
+    }
+    if (converged) fl |= pk::kFlagConverged;
+    pk::DevStats out = st;
+    out.iterations = total;
+    out.converged = converged ? 1 : 0;
+    out.residual_norm = std::sqrt(std::max(rr, 0.0));
+    out.flags = fl;
+    PK_CHECK(cudaMemcpyAsync(s->stats.p, &out, sizeof(out), cudaMemcpyHostToDevice, s->stream));
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    return PK_OK;
+}
+
 template <class Real>
 int run_step(pk_system* s, const pk_step_params& p)
 {
@@ -810,12 +938,13 @@ int run_step(pk_system* s, const pk_step_params& p)
     if (s->timing) PK_CHECK(cudaEventRecord(s->ev_pool[evi[1]], s->stream));
     if (!p.explicit_mode && s->dyn_count > 0) {
         int rc;
+        const bool refine = s->refine_passes > 0 && !(s->batched && s->seg_start.size() >= 2);
         if constexpr (std::is_same<Real, double>::value)
             rc = run_pcg<double, double>(s, p, 1);
         else if (s->precision == PK_PREC_FP32)
-            rc = run_pcg<float, float>(s, p, 1);
+            rc = refine ? run_pcg_refined<float, float>(s, p, 1) : run_pcg<float, float>(s, p, 1);
         else
-            rc = run_pcg<float, double>(s, p, 1);
+            rc = refine ? run_pcg_refined<float, double>(s, p, 1) : run_pcg<float, double>(s, p, 1);
         if (rc) return rc;
     }
     if (s->timing) {
@@ -847,6 +976,11 @@ bool same_params(const pk_step_params& a, const pk_step_params& b)
 template <class Real>
 int run_step_graph(pk_system* s, const pk_step_params& p)
 {
+    // A refined step reads residuals on the host between its solves: not capturable.
+    if (s->refine_passes > 0 && s->precision != PK_PREC_FP64 && !p.explicit_mode) {
+        drop_graph(s);
+        return run_step<Real>(s, p);
+    }
     if (!s->graph_exec || !same_params(p, s->graph_params)) {
         drop_graph(s);
         // Everything built lazily (allocations, uploads) must exist before the capture.
@@ -1377,6 +1511,14 @@ PKCUDA_API int pk_system_segment_stats(pk_system* s, int segment_count, int* ite
         if (residual_norm) residual_norm[b] = bs[b].residual_norm;
         if (flags) flags[b] = bs[b].flags;
     }
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_set_refinement(pk_system* s, int passes)
+{
+    if (!s || passes < 0 || passes > 16) return fail(PK_ERR_ARG, "refinement passes must be 0..16");
+    if (s->refine_passes != passes) drop_graph(s);
+    s->refine_passes = passes;
     return PK_OK;
 }
 

@@ -128,6 +128,11 @@ class SimWorld:
             raise PhysikError("autotune failed: " + self.error())
         return chosen, ms.value
 
+    def set_refinement(self, passes: int):
+        """FP64 outer true-residual refinement passes (FP32 / mixed precision); 0: off."""
+        if self.X.PHYSIK_B200_SetRefinement(self.h, passes) != 0:
+            raise PhysikError("bad refinement pass count")
+
     PCG_KERNELS = {0: "ring", 1: "staged", 2: "plain", 3: "slab", 4: "batched"}
 
     def pcg_kernel(self):
