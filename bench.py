@@ -78,6 +78,8 @@ KERNEL_NAMES = {
     "staged": "pcg_kernel (cooperative, TMA-staged tiles)",
     "plain": "pcg_kernel (cooperative, unstaged)",
     "batched": "pcg_batch_kernel (cooperative per-body PCG: symmetric BSR SpMV + block-Jacobi + dots + integrate)",
+    "slab-batched": "pcg_slab_kernel with one group of parts per body (per-body CG scalars and exchanges; "
+                    "bodies packed into a few cooperative launches)",
 }
 
 

@@ -184,7 +184,8 @@ PKCUDA_API int pk_system_adjoint_step(pk_system* sys, const pk_step_params* para
  * steps synchronise with the host and are not graph-captured. */
 PKCUDA_API int pk_system_set_refinement(pk_system* sys, int passes);
 /* The PCG kernel of the last solve: 0 ring-staged, 1 TMA-staged, 2 unstaged, 3
- * part-resident, 4 batched per-body; -1 before the first solve (or a negative PK_ERR_*).
+ * part-resident, 4 per-body batch kernel, 5 part-resident with one group of parts per body
+ * (batched solve); -1 before the first solve (or a negative PK_ERR_*).
  * blocks (may be NULL) receives the blocks it ran on. */
 PKCUDA_API int pk_system_pcg_kernel(pk_system* sys, int* blocks);
 /* Captures each step into a CUDA graph (relaxed capture mode) and replays it: the first
@@ -195,8 +196,9 @@ PKCUDA_API int pk_system_set_graph(pk_system* sys, int on);
 /* Autotuner: times `repeats` solves (without integration) of the last assembled system
  * for each candidate and keeps the fastest -- unbatched: the ring-staged kernel (0), the
  * TMA-staged kernel with 16 / 32 / 64-row tiles (1-3), the unstaged kernel (4), the
- * part-resident kernel (5, FP32 storage, where its layout applies); batched: the
- * smallest part (32 .. 1024 rows) a body is cut into.  Needs one step first.  Reports the
+ * part-resident kernel (5, FP32 storage, where its layout applies); batched: the per-body
+ * batch kernel with the smallest part (32 .. 1024 rows) a body is cut into (0-5), the
+ * part-resident kernel with one group of parts per body (6, FP32 storage).  Needs one step first.  Reports the
  * candidate index and its mean solve time.  Candidates differ only in summation order. */
 PKCUDA_API int pk_system_autotune(pk_system* sys, const pk_step_params* params, int repeats, int* chosen,
                                   double* best_ms);
@@ -247,6 +249,15 @@ PKCUDA_API int pk_ring_tiling_selfcheck(int precision, int n, const int* row_sta
  * No counterpart in the reference (it checks this library's own layout). */
 PKCUDA_API int pk_slab_plan_selfcheck(int n, const int* row_start, const int* col_index, const double* values,
                                       const double* x, const double* coords, int parts, double* y, int* info);
+
+/* The same for the per-body (batched) layout: rows in segments (bodies), every body cut
+ * into parts that fit, bodies packed into launches of at most max_blocks parts; also
+ * checks that every part's group is its body's consecutive parts within one launch.
+ * info (may be NULL) receives {parts, largest window, most tiles in a part, stream KiB,
+ * launches}. */
+PKCUDA_API int pk_slab_plan_batched_selfcheck(int n, const int* row_start, const int* col_index, const double* values,
+                                              const double* x, const double* coords, const int* segment_row_start,
+                                              int segment_count, int max_blocks, double* y, int* info);
 
 /* Builds the transposed index of an upper BSR: for row r the blocks (c, r), c < r.
  * lt_start[n+1]; lt_row / lt_block sized nnz - n.  Host-only, no device needed. */

@@ -92,6 +92,7 @@ _SIGS = {
     "pk_system_segment_stats": (_i, [_p, _i, _p, _p, _p, _p]),
     "pk_ring_tiling_selfcheck": (_i, [_i, _i, _p, _p, _p, _p, _p, _p, _p]),
     "pk_slab_plan_selfcheck": (_i, [_i, _p, _p, _p, _p, _p, _i, _p, _p]),
+    "pk_slab_plan_batched_selfcheck": (_i, [_i, _p, _p, _p, _p, _p, _p, _i, _i, _p, _p]),
     "pk_system_set_graph": (_i, [_p, _i]),
     "pk_system_adjoint_step": (_i, [_p, C.POINTER(PkStepParams), _p, _p, _p, _p, _p]),
     "pk_system_autotune": (_i, [_p, C.POINTER(PkStepParams), _i, _p, _p]),

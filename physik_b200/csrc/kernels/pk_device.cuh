@@ -381,14 +381,18 @@ __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v)
 // count_publish reduces the block's partials (ending with a block barrier, so every
 // store of the block made before it is visible to the block) and publishes them;
 // count_finish waits and reduces.  count_exchange is both.
+//
+// A group is `size` consecutive blocks starting at block `first` that share one arrival
+// counter `counter` (zero at launch); the whole grid is the group (0, gridDim.x).  Slots
+// are indexed by block in both generation buffers of gridDim.x slots.
 template <class Acc, int N>
-__device__ __forceinline__ void count_publish(ExSlot* slots, GridSync* sync, unsigned gen, Acc (&v)[N], int& bad,
-                                              Acc* sh, int* shi)
+__device__ __forceinline__ void count_publish(ExSlot* slots, unsigned* counter, int size, unsigned gen, Acc (&v)[N],
+                                              int& bad, Acc* sh, int* shi)
 {
     static_assert(N >= 1 && N <= 2, "two partials per slot");
     block_sum_or<Acc, N>(v, bad, sh, shi);
     const int G = gridDim.x;
-    if (G > 1 && threadIdx.x == 0) {
+    if (size > 1 && threadIdx.x == 0) {
         ExSlot* my = slots + (gen & 1u) * (unsigned)G + blockIdx.x;
         my->v0 = double(v[0]);
         my->v1 = N > 1 ? double(v[N - 1]) : 0.0;
@@ -396,21 +400,22 @@ __device__ __forceinline__ void count_publish(ExSlot* slots, GridSync* sync, uns
         // Release fence (cumulative over the block's stores ordered before it by the block
         // barrier), then the release increment.
         asm volatile("fence.acq_rel.gpu;" ::: "memory");
-        red_release_add(&sync->arrive, 1u);
+        red_release_add(counter, 1u);
     }
 }
 
 template <class Acc, int N>
-__device__ bool count_finish(ExSlot* slots, GridSync* sync, unsigned gen, Acc (&v)[N], int& bad, Acc* sh, int* shi)
+__device__ bool count_finish(ExSlot* slots, unsigned* counter, int first, int size, GridSync* sync, unsigned gen,
+                             Acc (&v)[N], int& bad, Acc* sh, int* shi)
 {
     const int G = gridDim.x, tid = threadIdx.x, lane = tid & 31;
-    if (G <= 1) return !*(volatile int*)&sync->err;
-    const ExSlot* buf = slots + (gen & 1u) * (unsigned)G;
+    if (size <= 1) return !*(volatile int*)&sync->err;
+    const ExSlot* buf = slots + (gen & 1u) * (unsigned)G + first;
     if (tid < 32) {
-        const unsigned target = gen * (unsigned)G;
+        const unsigned target = gen * (unsigned)size;
         int fail = 0;
         unsigned long long spins = 0;
-        while ((int)(ld_acquire(&sync->arrive) - target) < 0) {
+        while ((int)(ld_acquire(counter) - target) < 0) {
             if (++spins > kBarrierSpinLimit) {
                 atomicExch(&sync->err, 1);
                 fail = 1;
@@ -427,7 +432,7 @@ __device__ bool count_finish(ExSlot* slots, GridSync* sync, unsigned gen, Acc (&
         for (int k = 0; k < N; ++k) pv[k] = Acc(0);
         int pb = 0;
         if (!fail) {
-            for (int i = lane; i < G; i += 32) {
+            for (int i = lane; i < size; i += 32) {
                 pv[0] += Acc(__ldcg(&buf[i].v0));
                 if (N > 1) pv[N - 1] += Acc(__ldcg(&buf[i].v1));
                 pb |= __ldcg(&buf[i].bad);
@@ -455,11 +460,11 @@ __device__ bool count_finish(ExSlot* slots, GridSync* sync, unsigned gen, Acc (&
 }
 
 template <class Acc, int N>
-__device__ __forceinline__ bool count_exchange(ExSlot* slots, GridSync* sync, unsigned gen, Acc (&v)[N], int& bad,
-                                               Acc* sh, int* shi)
+__device__ __forceinline__ bool count_exchange(ExSlot* slots, unsigned* counter, int first, int size, GridSync* sync,
+                                               unsigned gen, Acc (&v)[N], int& bad, Acc* sh, int* shi)
 {
-    count_publish<Acc, N>(slots, sync, gen, v, bad, sh, shi);
-    return count_finish<Acc, N>(slots, sync, gen, v, bad, sh, shi);
+    count_publish<Acc, N>(slots, counter, size, gen, v, bad, sh, shi);
+    return count_finish<Acc, N>(slots, counter, first, size, sync, gen, v, bad, sh, shi);
 }
 
 // The whole grid as one group (slots: two buffers of gridDim.x).

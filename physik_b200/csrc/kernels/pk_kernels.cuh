@@ -302,7 +302,8 @@ struct SlabPcgArgs {
     float* qs;                   // 4 per slab row: q of phase A
     float* ss;                   // 4 per slab row: s published for the window passes
     ExSlot* slots;               // [2][grid]
-    GridSync* sync;
+    unsigned* group_count;       // [grid]: arrival counter of the group starting at each block (zeroed)
+    GridSync* sync;              // err flag
     int max_iterations;
     Acc tolerance;
     int skip_on_flags;
@@ -313,6 +314,13 @@ struct SlabPcgArgs {
     float* node_v;
     unsigned* flags;
     DevStats* stats;
+    // Per-body solves (grouped): each block's body, the per-body statistics and the success
+    // flags some body lacks; 0 / NULL for the coupled solve (one group of all blocks).
+    int grouped;
+    const int* part_body;        // [grid]
+    int nbodies;
+    BatchBodyStats* body_stats;
+    unsigned* missing;
 };
 
 // ------------------------------------------------------------------ FP64 refinement

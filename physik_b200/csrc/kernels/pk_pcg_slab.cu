@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     // The part: rows [row0, row0 + m) of the slab order, halo rows halo_src[halo0 ..
     // halo0 + h), tiles [tile0, tile0 + ntiles).  A part that does not fit the block's
     // tables (the host never builds one) is emptied and reports a breakdown.
-    int row0, m, halo0, h, tile0, ntiles;
+    int row0, m, halo0, h, tile0, ntiles, gfirst, gsize;
     {
         const int4 a = __ldg(reinterpret_cast<const int4*>(P.part_info) + 2 * blk);
         const int4 b = __ldg(reinterpret_cast<const int4*>(P.part_info) + 2 * blk + 1);
@@ -152,6 +152,8 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
         h = a.w;
         tile0 = b.x;
         ntiles = b.y;
+        gfirst = b.z;  // this part's group: blocks [gfirst, gfirst + gsize) of the launch
+        gsize = b.w;
     }
     if (tid == 0) {
         for (int s = 0; s < S; ++s) {
@@ -163,6 +165,24 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
         s_bad = 0;
     }
     __syncthreads();
+    // A group must hold this block; the coupled solve is one group of the whole grid.
+    const bool group_ok = gfirst >= 0 && gsize >= 1 && gfirst + gsize <= (int)gridDim.x && blk >= gfirst &&
+                          blk < gfirst + gsize && (P.grouped || (gfirst == 0 && gsize == (int)gridDim.x));
+    int body = 0;
+    if (P.grouped) {
+        body = __ldg(P.part_body + blk);
+        if ((unsigned)body >= (unsigned)P.nbodies) body = -1;
+    }
+    if (!group_ok || body < 0) {
+        // Not a valid group (the host never builds one): the block works alone and fails.
+        gfirst = blk;
+        gsize = 1;
+        body = 0;
+        if (tid == 0) s_bad = 1;
+    }
+    unsigned* const gcount = P.group_count + gfirst;  // the group's arrival counter
+    BatchBodyStats* const bs = P.grouped ? P.body_stats + body : nullptr;
+    const bool leader = P.grouped ? blk == gfirst : blk == 0;
     if (m < 0 || m > kSlabMaxRows || h < 0 || m + h > kSlabWinCap || row0 < 0 || row0 + m > P.n || ntiles < 0 ||
         ntiles > kSlabMaxTiles || halo0 < 0 || halo0 + h > P.halo_count || tile0 < 0 ||
         tile0 + ntiles > P.tile_count) {
@@ -190,10 +210,17 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
 
     const unsigned in_flags = *(volatile unsigned*)P.flags;
     if (P.skip_on_flags && (in_flags & (kFlagPrecomputeFailed | kFlagSingularDiag))) {
-        if (blk == 0 && tid == 0) {
-            P.stats->iterations = 0;
-            P.stats->converged = 0;
-            P.stats->residual_norm = 0.0;
+        if (leader && tid == 0) {
+            if (P.grouped) {
+                bs->iterations = 0;
+                bs->converged = 0;
+                bs->residual_norm = 0.0;
+                bs->flags = 0;
+            } else {
+                P.stats->iterations = 0;
+                P.stats->converged = 0;
+                P.stats->residual_norm = 0.0;
+            }
         }
         return;
     }
@@ -358,7 +385,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
             }
         }
         for (int w = tid; w < 3 * wn; w += blockDim.x) win[w] = 0.f;
-        if (!count_exchange<Acc, 2>(P.slots, P.sync, ++xgen, v, bad, sh_acc, sh_int)) {
+        if (!count_exchange<Acc, 2>(P.slots, gcount, gfirst, gsize, P.sync, ++xgen, v, bad, sh_acc, sh_int)) {
             timed_out = true;
             goto finish;
         }
@@ -442,7 +469,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                 qbad = 1;
                 atomicExch(&P.sync->err, 1);
             }
-            count_publish<Acc, 1>(P.slots, P.sync, ++xgen, dq, qbad, sh_acc, sh_int);
+            count_publish<Acc, 1>(P.slots, gcount, gsize, ++xgen, dq, qbad, sh_acc, sh_int);
             // Phase B's q (written by other threads in phase A, visible after the publish's
             // block barrier) loads while the exchange completes.
             V3<float> qv[kSlabRowsPerThread];
@@ -452,7 +479,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                 qv[k] = (row_owner && k < krows && i < m) ? ldv4(P.qs + 4 * (size_t)(row0 + i))
                                                           : V3<float>{0.f, 0.f, 0.f};
             }
-            if (!count_finish<Acc, 1>(P.slots, P.sync, xgen, dq, qbad, sh_acc, sh_int)) {
+            if (!count_finish<Acc, 1>(P.slots, gcount, gfirst, gsize, P.sync, xgen, dq, qbad, sh_acc, sh_int)) {
                 timed_out = true;
                 goto finish;
             }
@@ -495,7 +522,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                     tmem_st16(tmem_row0 + 16u * (unsigned)k, rec);
                 }
             }
-            if (!count_exchange<Acc, 2>(P.slots, P.sync, ++xgen, v, sbad, sh_acc, sh_int)) {
+            if (!count_exchange<Acc, 2>(P.slots, gcount, gfirst, gsize, P.sync, ++xgen, v, sbad, sh_acc, sh_int)) {
                 timed_out = true;
                 goto finish;
             }
@@ -551,7 +578,7 @@ final_check:
                 }
             }
         }
-        if (!count_exchange<Acc, 1>(P.slots, P.sync, ++xgen, none, bad, sh_acc, sh_int)) {
+        if (!count_exchange<Acc, 1>(P.slots, gcount, gfirst, gsize, P.sync, ++xgen, none, bad, sh_acc, sh_int)) {
             timed_out = true;
             goto finish;
         }
@@ -596,7 +623,22 @@ finish:
         tmem_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s_tmem), "r"(512u) : "memory");
     }
-    if (blk == 0 && tid == 0) {
+    if (leader && tid == 0 && P.grouped) {
+        // Per body; world-wide: the largest iteration count and residual, the OR of the
+        // failure flags and the AND of the success flags (missing: what some body lacks).
+        bs->iterations = iterations;
+        bs->converged = converged ? 1 : 0;
+        bs->residual_norm = (double)residual;
+        bs->flags = fl;
+        atomicMax(&P.stats->iterations, iterations);
+        if (residual >= Acc(0))  // non-negative doubles order like their bit patterns
+            atomicMax(reinterpret_cast<unsigned long long*>(&P.stats->residual_norm),
+                      (unsigned long long)__double_as_longlong((double)residual));
+        atomicOr(P.flags, fl & ~(kFlagSolved | kFlagIntegrated | kFlagConverged));
+        if (!(fl & kFlagSolved)) atomicOr(P.missing, kFlagSolved);
+        if (!(fl & kFlagIntegrated)) atomicOr(P.missing, kFlagIntegrated);
+        if (!(fl & kFlagConverged)) atomicOr(P.missing, kFlagConverged);
+    } else if (leader && tid == 0) {
         P.stats->iterations = iterations;
         P.stats->converged = converged ? 1 : 0;
         P.stats->residual_norm = (double)residual;

@@ -64,34 +64,16 @@ inline unsigned get_u16(const std::vector<unsigned char>& s, size_t off)
 
 }  // namespace
 
-std::string build_slab_plan(int n, const int* row_start, const int* col, const int* lt_start, const int* lt_row,
-                            const int* lt_block, const double* coords, int parts, SlabPlan& out)
-{
-    out = SlabPlan{};
-    if (n <= 0 || parts <= 0) return "empty system";
-    parts = std::min(parts, n);
-    const int nnz = row_start[n];
-    std::vector<int> len(n);
-    for (int r = 0; r < n; ++r) len[r] = (row_start[r + 1] - row_start[r]) + (lt_start[r + 1] - lt_start[r]);
-    for (int r = 0; r < n; ++r)
-        if (len[r] > kSlabCapE) return "a row has more blocks than a tile holds";
+namespace {
 
-    // 1. parts
-    std::vector<int> part_of(n, 0);
-    std::vector<double> w(n);
-    for (int r = 0; r < n; ++r) w[r] = len[r] + 4.0;  // streamed blocks + per-row vector work
-    if (coords) {
-        std::vector<int> ids(n);
-        std::iota(ids.begin(), ids.end(), 0);
-        rcb(ids, 0, (size_t)n, 0, parts, coords, w, part_of);
-    } else {
-        const double total = std::accumulate(w.begin(), w.end(), 0.0);
-        double acc = 0.0;
-        for (int r = 0; r < n; ++r) {
-            part_of[r] = std::min(parts - 1, static_cast<int>(acc * parts / total));
-            acc += w[r];
-        }
-    }
+// The layout for a given assignment of rows to parts (part_of[r] in [0, parts), every part
+// non-empty): slab order, windows, halos, tiles, stream and block positions.  Group
+// fields of part_info are left for the caller.
+std::string build_layout(int n, const int* row_start, const int* col, const int* lt_start, const int* lt_row,
+                         const int* lt_block, const std::vector<int>& part_of, const std::vector<int>& len, int parts,
+                         SlabPlan& out)
+{
+    const int nnz = row_start[n];
     // 2. slab order: parts in order, rows ascending inside a part
     std::vector<int> count(parts + 1, 0);
     for (int r = 0; r < n; ++r) ++count[part_of[r] + 1];
@@ -209,6 +191,168 @@ std::string build_slab_plan(int n, const int* row_start, const int* col, const i
     for (int r = 0; r < n; ++r)
         for (int k = row_start[r]; k < row_start[r + 1]; ++k)
             if ((col[k] != r) != (out.pos_l[k] != kSlabNoPos)) return "internal: transposed copy mismatch";
+    return "";
+}
+
+}  // namespace
+
+std::string build_slab_plan(int n, const int* row_start, const int* col, const int* lt_start, const int* lt_row,
+                            const int* lt_block, const double* coords, int parts, SlabPlan& out)
+{
+    out = SlabPlan{};
+    if (n <= 0 || parts <= 0) return "empty system";
+    parts = std::min(parts, n);
+    std::vector<int> len(n);
+    for (int r = 0; r < n; ++r) len[r] = (row_start[r + 1] - row_start[r]) + (lt_start[r + 1] - lt_start[r]);
+    for (int r = 0; r < n; ++r)
+        if (len[r] > kSlabCapE) return "a row has more blocks than a tile holds";
+    std::vector<int> part_of(n, 0);
+    std::vector<double> w(n);
+    for (int r = 0; r < n; ++r) w[r] = len[r] + 4.0;  // streamed blocks + per-row vector work
+    if (coords) {
+        std::vector<int> ids(n);
+        std::iota(ids.begin(), ids.end(), 0);
+        rcb(ids, 0, (size_t)n, 0, parts, coords, w, part_of);
+    } else {
+        const double total = std::accumulate(w.begin(), w.end(), 0.0);
+        double acc = 0.0;
+        for (int r = 0; r < n; ++r) {
+            part_of[r] = std::min(parts - 1, static_cast<int>(acc * parts / total));
+            acc += w[r];
+        }
+    }
+    const std::string why = build_layout(n, row_start, col, lt_start, lt_row, lt_block, part_of, len, parts, out);
+    if (!why.empty()) return why;
+    for (int p = 0; p < parts; ++p) {
+        out.part_info[(size_t)kSlabPartInts * p + 6] = 0;
+        out.part_info[(size_t)kSlabPartInts * p + 7] = parts;
+    }
+    out.part_body.assign(parts, 0);
+    out.launch_start = {0, parts};
+    return "";
+}
+
+std::string build_slab_plan_batched(int n, const int* row_start, const int* col, const int* lt_start,
+                                    const int* lt_row, const int* lt_block, const double* coords, const int* seg,
+                                    int nseg, int max_blocks, SlabPlan& out)
+{
+    out = SlabPlan{};
+    if (n <= 0 || nseg <= 0 || max_blocks <= 0) return "empty system";
+    if (seg[0] != 0 || seg[nseg] != n) return "segments do not cover the rows";
+    std::vector<int> len(n);
+    for (int r = 0; r < n; ++r) len[r] = (row_start[r + 1] - row_start[r]) + (lt_start[r + 1] - lt_start[r]);
+    for (int r = 0; r < n; ++r)
+        if (len[r] > kSlabCapE) return "a row has more blocks than a tile holds";
+    std::vector<double> w(n);
+    for (int r = 0; r < n; ++r) w[r] = len[r] + 4.0;
+    // 1. every body into parts: the fewest whose rows and windows fit
+    std::vector<int> body_parts(nseg, 0);
+    std::vector<std::vector<int>> body_assign(nseg);  // part (0..k-1) of each of the body's rows
+    for (int b = 0; b < nseg; ++b) {
+        const int s0 = seg[b], rows = seg[b + 1] - seg[b];
+        if (rows <= 0) continue;
+        int k = (rows + kSlabMaxRows - 1) / kSlabMaxRows;
+        for (;; ++k) {
+            if (k > rows || k > max_blocks) return "a body does not fit one launch";
+            std::vector<int> a(rows, 0);
+            if (k > 1) {
+                if (coords) {
+                    std::vector<int> ids(rows);
+                    std::iota(ids.begin(), ids.end(), 0);
+                    std::vector<double> xyz(3 * (size_t)rows), wb(rows);
+                    for (int i = 0; i < rows; ++i) {
+                        for (int c = 0; c < 3; ++c) xyz[3 * (size_t)i + c] = coords[3 * (size_t)(s0 + i) + c];
+                        wb[i] = w[s0 + i];
+                    }
+                    rcb(ids, 0, (size_t)rows, 0, k, xyz.data(), wb, a);
+                } else {
+                    double total = 0.0, acc = 0.0;
+                    for (int i = 0; i < rows; ++i) total += w[s0 + i];
+                    for (int i = 0; i < rows; ++i) {
+                        a[i] = std::min(k - 1, static_cast<int>(acc * k / total));
+                        acc += w[s0 + i];
+                    }
+                }
+            }
+            // rows and windows of the k parts (rows of one body couple only within it)
+            std::vector<int> cnt(k, 0);
+            for (int i = 0; i < rows; ++i) ++cnt[a[i]];
+            bool ok = true;
+            for (int p = 0; p < k && ok; ++p) ok = cnt[p] > 0 && cnt[p] <= kSlabMaxRows;
+            if (ok) {
+                std::vector<std::vector<int>> halo(k);
+                for (int i = 0; i < rows; ++i) {
+                    const int r = s0 + i, p = a[i];
+                    for (int kk = row_start[r]; kk < row_start[r + 1]; ++kk) {
+                        const int c = col[kk];
+                        if (c < s0 || c >= seg[b + 1]) return "a block couples two bodies";
+                        if (a[c - s0] != p) halo[p].push_back(c);
+                    }
+                    for (int e = lt_start[r]; e < lt_start[r + 1]; ++e) {
+                        const int c = lt_row[e];
+                        if (c < s0 || c >= seg[b + 1]) return "a block couples two bodies";
+                        if (a[c - s0] != p) halo[p].push_back(c);
+                    }
+                }
+                for (int p = 0; p < k && ok; ++p) {
+                    std::sort(halo[p].begin(), halo[p].end());
+                    halo[p].erase(std::unique(halo[p].begin(), halo[p].end()), halo[p].end());
+                    ok = cnt[p] + static_cast<int>(halo[p].size()) <= kSlabWinCap;
+                }
+            }
+            if (ok) {
+                body_parts[b] = k;
+                body_assign[b] = std::move(a);
+                break;
+            }
+        }
+    }
+    // 2. bodies into launches, largest parts first (a launch lasts as long as its slowest
+    // part), at most max_blocks parts per launch, a body never split across launches
+    std::vector<int> order;
+    for (int b = 0; b < nseg; ++b)
+        if (body_parts[b] > 0) order.push_back(b);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const double rx = double(seg[x + 1] - seg[x]) / body_parts[x], ry = double(seg[y + 1] - seg[y]) / body_parts[y];
+        return rx > ry;
+    });
+    std::vector<int> launch_of(nseg, -1), launch_fill;
+    for (int b : order) {
+        int l = 0;
+        while (l < static_cast<int>(launch_fill.size()) && launch_fill[l] + body_parts[b] > max_blocks) ++l;
+        if (l == static_cast<int>(launch_fill.size())) launch_fill.push_back(0);
+        launch_of[b] = l;
+        launch_fill[l] += body_parts[b];
+    }
+    // 3. global part numbers: launch by launch, bodies in that launch in size order
+    std::vector<int> part_of(n, 0);
+    std::vector<int> part_body, group_first, group_size;
+    out.launch_start.assign(1, 0);
+    for (int l = 0; l < static_cast<int>(launch_fill.size()); ++l) {
+        int local = 0;
+        for (int b : order) {
+            if (launch_of[b] != l) continue;
+            const int first = static_cast<int>(part_body.size());
+            for (int i = 0; i < seg[b + 1] - seg[b]; ++i) part_of[seg[b] + i] = first + body_assign[b][i];
+            for (int p = 0; p < body_parts[b]; ++p) {
+                part_body.push_back(b);
+                group_first.push_back(local);
+                group_size.push_back(body_parts[b]);
+            }
+            local += body_parts[b];
+        }
+        out.launch_start.push_back(static_cast<int>(part_body.size()));
+    }
+    const int parts = static_cast<int>(part_body.size());
+    std::vector<int> launch_start = out.launch_start;
+    const std::string why = build_layout(n, row_start, col, lt_start, lt_row, lt_block, part_of, len, parts, out);
+    if (!why.empty()) return why;
+    for (int p = 0; p < parts; ++p) {
+        out.part_info[(size_t)kSlabPartInts * p + 6] = group_first[p];
+        out.part_info[(size_t)kSlabPartInts * p + 7] = group_size[p];
+    }
+    out.part_body = part_body;
+    out.launch_start = launch_start;
     return "";
 }
 

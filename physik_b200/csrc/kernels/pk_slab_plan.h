@@ -43,7 +43,10 @@ constexpr int kSlabMaxTiles = 128;     // tiles per part
 constexpr int kSlabRowThreads = 384;   // threads owning rows in the per-row phases
 constexpr int kSlabRowsPerThread = 10; // row records per thread in tensor memory
 constexpr int kSlabMaxRows = kSlabRowThreads * kSlabRowsPerThread;  // rows per part
-constexpr int kSlabPartInts = 8;       // per part: row0, rows, halo0, halo rows, tile0, tiles, 0, 0
+// Per part: row0, rows, halo0, halo rows, tile0, tiles, and for per-body solves the part's
+// group (its body's parts, consecutive blocks of one launch): first block (within the
+// launch) and size; a single group of all parts for the coupled solve.
+constexpr int kSlabPartInts = 8;
 constexpr unsigned kSlabNoPos = 0xffffffffu;
 
 static_assert(kSlabHeaderBytes + kSlabCapE * kSlabEntryBytes <= kSlabStageBytes, "stage too small");
@@ -60,6 +63,8 @@ struct SlabPlan {
     std::vector<int> tile_desc;  // 4 per tile: stream offset / 16, bytes, first local row, rows
     std::vector<unsigned char> stream;  // headers and columns filled, blocks zero
     std::vector<unsigned> pos_u, pos_l; // per canonical upper block: float offsets (kSlabNoPos: none)
+    std::vector<int> part_body;  // body (segment) of each part; 0 for the coupled solve
+    std::vector<int> launch_start;  // parts [launch_start[l], launch_start[l + 1]) form launch l
     int max_window = 0, max_tiles = 0, max_rows = 0;
 };
 
@@ -69,6 +74,15 @@ struct SlabPlan {
 // layout does not apply (a window or a row too large); `out` is then unusable.
 std::string build_slab_plan(int n, const int* row_start, const int* col, const int* lt_start, const int* lt_row,
                             const int* lt_block, const double* coords, int parts, SlabPlan& out);
+
+// The layout for per-body solves: the rows split into bodies (segments
+// [seg[b], seg[b + 1]), no block coupling two bodies), every body cut by coordinate
+// bisection (NULL coords: contiguous ranges) into as few parts as its rows and window
+// allow, and the bodies packed, largest parts first, into launches of at most
+// max_blocks parts.  Returns "" on success, otherwise why the layout does not apply.
+std::string build_slab_plan_batched(int n, const int* row_start, const int* col, const int* lt_start,
+                                    const int* lt_row, const int* lt_block, const double* coords, const int* seg,
+                                    int nseg, int max_blocks, SlabPlan& out);
 
 // y = A x through the plan exactly as the kernel reads it (fill, then tile decoding with
 // the kernel's clamps), in double: the CPU self-check of a plan.

@@ -222,6 +222,10 @@ struct pk_system {
     bool slab_filled = false;     // the block stream holds the current values
     int slab_parts = 0;           // blocks of the slab kernel (0: layout not available)
     int slab_tile_count = 0, slab_halo_count = 0;
+    bool slab_for_bodies = false;   // the layout is the per-body one (batched solve)
+    bool batch_slab = true;         // batched solve: part-resident kernel where it applies
+    std::vector<int> slab_launch;   // per-body layout: parts of each launch
+    DevBuf slab_part_body, slab_gcount;
     int slab_max_grid = 0;
     std::string slab_reason;      // why the layout does not apply
     unsigned long long slab_stream_bytes = 0;
@@ -494,6 +498,8 @@ bool slab_allowed(const pk_system* s)
     return s->precision != PK_PREC_FP64 && (rk == -1 || rk == 3) && s->dyn_count > 0 && s->have_pattern;
 }
 
+bool batched_solve(const pk_system* s) { return s->batched && s->seg_start.size() >= 2; }
+
 // Builds and uploads the part-resident kernel's layout if it has not been tried yet for
 // this pattern and grid (synchronous: never called while a stream capture is open).
 // Parts are cut by the rows' node positions at this moment.  Not applicable (too large
@@ -501,13 +507,16 @@ bool slab_allowed(const pk_system* s)
 template <class Acc>
 int ensure_slab(pk_system* s)
 {
+    const bool bodies = batched_solve(s);
+    if (s->slab_tried && s->slab_for_bodies != bodies) reset_slab(s);  // batched mode changed
     if (s->slab_tried || !slab_allowed(s)) return PK_OK;
     s->slab_tried = true;
+    s->slab_for_bodies = bodies;
     s->slab_parts = 0;
     if (!s->slab_max_grid) s->slab_max_grid = pk::pcg_slab_max_grid<Acc>();
     int grid = s->slab_max_grid;
     if (s->pcg_grid_override > 0) grid = std::min(grid, s->pcg_grid_override);
-    grid = std::min(grid, std::max(1, s->dyn_count / 64));
+    if (!bodies) grid = std::min(grid, std::max(1, s->dyn_count / 64));
     if (grid <= 0) {
         s->slab_reason = "kernel cannot be resident";
         return PK_OK;
@@ -530,8 +539,12 @@ int ensure_slab(pk_system* s)
         PK_CHECK(cudaMemcpy(ltb.data(), s->lt_block.p, ltb.size() * sizeof(int), cudaMemcpyDeviceToHost));
     }
     pk::SlabPlan plan;
-    const std::string why = pk::build_slab_plan(n, s->h_row_start.data(), col.data(), s->h_lts.data(), ltr.data(),
-                                                ltb.data(), coords.data(), grid, plan);
+    const std::string why =
+        bodies ? pk::build_slab_plan_batched(n, s->h_row_start.data(), col.data(), s->h_lts.data(), ltr.data(),
+                                             ltb.data(), coords.data(), s->seg_start.data(),
+                                             static_cast<int>(s->seg_start.size()) - 1, grid, plan)
+               : pk::build_slab_plan(n, s->h_row_start.data(), col.data(), s->h_lts.data(), ltr.data(), ltb.data(),
+                                     coords.data(), grid, plan);
     if (!why.empty()) {
         s->slab_reason = why;
         return PK_OK;
@@ -544,7 +557,15 @@ int ensure_slab(pk_system* s)
     if (!rc) rc = upload_raw<int>(s->slab_perm, plan.perm.data(), plan.perm.size(), s->stream);
     if (!rc) rc = upload_raw<unsigned>(s->slab_pos_u, plan.pos_u.data(), plan.pos_u.size(), s->stream);
     if (!rc) rc = upload_raw<unsigned>(s->slab_pos_l, plan.pos_l.data(), plan.pos_l.size(), s->stream);
+    if (!rc) rc = upload_raw<int>(s->slab_part_body, plan.part_body.data(), plan.part_body.size(), s->stream);
     if (rc) return rc;
+    int widest = 1;
+    for (size_t l = 0; l + 1 < plan.launch_start.size(); ++l)
+        widest = std::max(widest, plan.launch_start[l + 1] - plan.launch_start[l]);
+    PK_CHECK(s->slab_gcount.ensure(sizeof(unsigned) * static_cast<size_t>(widest)));
+    PK_CHECK(s->slots.ensure(2 * sizeof(pk::ExSlot) * static_cast<size_t>(widest)));
+    if (bodies) PK_CHECK(s->body_stats.ensure(sizeof(pk::BatchBodyStats) * s->seg_start.size()));
+    s->slab_launch = plan.launch_start;
     const size_t rows = static_cast<size_t>(n);
     PK_CHECK(s->slab_qs.ensure(16 * rows));
     PK_CHECK(s->slab_ss.ensure(16 * rows));
@@ -569,13 +590,15 @@ int run_pcg_slab(pk_system* s, const pk_step_params& p, int skip_on_flags)
     if constexpr (!std::is_same<Real, float>::value) {
         return fail(PK_ERR_UNSUPPORTED, "part-resident PCG: FP32 storage only");
     } else {
-        const int grid = s->slab_parts;
-        if (grid <= 0) return fail(PK_ERR_UNSUPPORTED, "part-resident PCG layout not available");
+        if (s->slab_parts <= 0 || s->slab_launch.size() < 2)
+            return fail(PK_ERR_UNSUPPORTED, "part-resident PCG layout not available");
+        const bool bodies = s->slab_for_bodies;
+        const int nseg = static_cast<int>(s->seg_start.size()) - 1;
         int rc = ensure_solver_buffers(s, 1);
         if (rc) return rc;
-        PK_CHECK(s->slots.ensure(2 * sizeof(pk::ExSlot) * static_cast<size_t>(grid)));
-        PK_CHECK(cudaMemsetAsync(s->slots.p, 0, 2 * sizeof(pk::ExSlot) * static_cast<size_t>(grid), s->stream));
-        PK_CHECK(cudaMemsetAsync(s->sync.p, 0, sizeof(pk::GridSync), s->stream));
+        if (bodies)
+            PK_CHECK(cudaMemsetAsync(s->body_stats.p, 0, sizeof(pk::BatchBodyStats) * static_cast<size_t>(nseg),
+                                     s->stream));
         if (!s->slab_filled) {
             rc = slab_fill(s);
             if (rc) return rc;
@@ -608,10 +631,25 @@ int run_pcg_slab(pk_system* s, const pk_step_params& p, int skip_on_flags)
         pk::DevStats* st = s->stats.as<pk::DevStats>();
         a.flags = &st->flags;
         a.stats = st;
-        PK_CHECK(pk::launch_pcg_slab_kernel<Acc>(a, grid, s->stream));
-        s->launches += 1;
-        s->last_kernel = 3;
-        s->last_blocks = grid;
+        a.group_count = s->slab_gcount.as<unsigned>();
+        a.grouped = bodies ? 1 : 0;
+        a.nbodies = bodies ? nseg : 1;
+        a.body_stats = bodies ? s->body_stats.as<pk::BatchBodyStats>() : nullptr;
+        a.missing = &st->batch_missing;
+        // One launch per group of parts (the coupled solve: one launch of all parts).
+        const int launches = static_cast<int>(s->slab_launch.size()) - 1;
+        for (int l = 0; l < launches; ++l) {
+            const int p0 = s->slab_launch[l], grid = s->slab_launch[l + 1] - p0;
+            PK_CHECK(cudaMemsetAsync(s->slots.p, 0, 2 * sizeof(pk::ExSlot) * static_cast<size_t>(grid), s->stream));
+            PK_CHECK(cudaMemsetAsync(s->slab_gcount.p, 0, sizeof(unsigned) * static_cast<size_t>(grid), s->stream));
+            PK_CHECK(cudaMemsetAsync(s->sync.p, 0, sizeof(pk::GridSync), s->stream));
+            a.part_info = s->slab_part_info.as<int>() + static_cast<size_t>(pk::kSlabPartInts) * p0;
+            a.part_body = s->slab_part_body.as<int>() + p0;
+            PK_CHECK(pk::launch_pcg_slab_kernel<Acc>(a, grid, s->stream));
+            s->launches += 1;
+        }
+        s->last_kernel = bodies ? 5 : 3;
+        s->last_blocks = s->slab_parts;
         return PK_OK;
     }
 }
@@ -739,7 +777,16 @@ int solve_kernel(const pk_system* s)
 template <class Real, class Acc>
 int run_pcg(pk_system* s, const pk_step_params& p, int skip_on_flags)
 {
-    if (s->batched && s->seg_start.size() >= 2) {
+    if (batched_solve(s)) {
+        // Per-body solves: the part-resident kernel with one group of parts per body where
+        // its layout applies, else the per-body batch kernel.
+        if constexpr (std::is_same<Real, float>::value) {
+            if (s->batch_slab) {
+                int rc = ensure_slab<Acc>(s);
+                if (rc) return rc;
+                if (s->slab_parts > 0 && s->slab_for_bodies) return run_pcg_slab<Real, Acc>(s, p, skip_on_flags);
+            }
+        }
         s->last_kernel = 4;
         return run_pcg_batch<Real, Acc>(s, p, skip_on_flags);
     }
@@ -925,10 +972,11 @@ int run_step(pk_system* s, const pk_step_params& p)
         // The part-resident kernel reads the blocks from its own stream: fill it here so
         // the solve time below is the PCG kernel's alone.
         if constexpr (std::is_same<Real, float>::value) {
-            if (!p.explicit_mode && !(s->batched && s->seg_start.size() >= 2)) {
+            if (!p.explicit_mode && (!batched_solve(s) || s->batch_slab)) {
                 int rc = s->precision == PK_PREC_MIXED ? ensure_slab<double>(s) : ensure_slab<float>(s);
                 if (rc) return rc;
-                if (solve_kernel(s) == 3) {
+                const bool uses = batched_solve(s) ? (s->slab_parts > 0 && s->slab_for_bodies) : solve_kernel(s) == 3;
+                if (uses) {
                     rc = slab_fill(s);
                     if (rc) return rc;
                 }
@@ -1481,6 +1529,7 @@ PKCUDA_API int pk_system_set_segments(pk_system* s, int segment_count, const int
     }
     s->seg_start.assign(segment_row_start, segment_row_start + (segment_count > 0 ? segment_count + 1 : 0));
     s->batch_parts = 0;
+    reset_slab(s);
     drop_graph(s);
     return PK_OK;
 }
@@ -1583,9 +1632,21 @@ PKCUDA_API int pk_system_autotune(pk_system* s, const pk_step_params* p, int rep
     int best = -1;
     double best_t = 1e300;
     if (s->batched && s->seg_start.size() >= 2) {
-        // Candidates: the smallest part a body is cut into.
+        // Candidates: the per-body batch kernel with the smallest part a body is cut into
+        // (0-5); the part-resident kernel with one group per body (6) where it applies.
         const int cand[] = {32, 64, 128, 256, 512, 1024};
         int i = 0;
+        double slab_t = -1.0;
+        if (s->precision != PK_PREC_FP64) {
+            s->batch_slab = true;
+            int rc = ensure_slab_any(s);
+            if (rc) return rc;
+            if (s->slab_parts > 0 && s->slab_for_bodies) {
+                slab_t = time_solves(s, *p, repeats);
+                if (slab_t < 0) return static_cast<int>(slab_t);
+            }
+        }
+        s->batch_slab = false;
         for (int rows : cand) {
             s->batch_min_rows = rows;
             s->batch_parts = 0;
@@ -1598,6 +1659,11 @@ PKCUDA_API int pk_system_autotune(pk_system* s, const pk_step_params* p, int rep
         s->batch_parts = 0;
         int rc = ensure_batch_parts_any(s);
         if (rc) return rc;
+        if (slab_t >= 0.0 && slab_t < best_t) {
+            best_t = slab_t;
+            best = 6;
+            s->batch_slab = true;
+        }
     } else {
         // Candidates: ring kernel; staged kernel with 16 / 32 / 64-row tiles; plain kernel;
         // part-resident kernel.
@@ -1910,6 +1976,51 @@ int ring_selfcheck(int n, const int* row_start, const int* col, const double* va
 }  // namespace
 
 extern "C" {
+
+PKCUDA_API int pk_slab_plan_batched_selfcheck(int n, const int* row_start, const int* col_index, const double* values,
+                                              const double* x, const double* coords, const int* segment_row_start,
+                                              int segment_count, int max_blocks, double* y, int* info)
+{
+    if (n <= 0 || segment_count <= 0 || max_blocks <= 0 || !row_start || !col_index || !values || !x || !y ||
+        !segment_row_start)
+        return fail(PK_ERR_ARG, "slab batched selfcheck");
+    for (int r = 0; r < n; ++r)
+        for (int k = row_start[r]; k < row_start[r + 1]; ++k)
+            if (col_index[k] < r || col_index[k] >= n) return fail(PK_ERR_ARG, "column outside [row, n)");
+    std::vector<int> lts, ltr, ltb;
+    build_transpose(n, row_start, col_index, lts, ltr, ltb);
+    pk::SlabPlan plan;
+    const std::string why = pk::build_slab_plan_batched(n, row_start, col_index, lts.data(), ltr.data(), ltb.data(),
+                                                        coords, segment_row_start, segment_count, max_blocks, plan);
+    if (!why.empty()) return fail(PK_ERR_UNSUPPORTED, "slab layout: " + why);
+    // Groups: consecutive parts of one body inside one launch, sizes matching.
+    const int launches = static_cast<int>(plan.launch_start.size()) - 1;
+    for (int l = 0; l < launches; ++l) {
+        const int p0 = plan.launch_start[l], p1 = plan.launch_start[l + 1];
+        if (p1 - p0 > max_blocks || p1 <= p0) return fail(PK_ERR_STATE, "slab layout: bad launch");
+        for (int p = p0; p < p1; ++p) {
+            const int* pi = plan.part_info.data() + static_cast<size_t>(pk::kSlabPartInts) * p;
+            const int first = pi[6], size = pi[7];
+            if (first < 0 || size < 1 || p0 + first + size > p1 || p - p0 < first || p - p0 >= first + size)
+                return fail(PK_ERR_STATE, "slab layout: bad group");
+            for (int q = p0 + first; q < p0 + first + size; ++q)
+                if (plan.part_body[q] != plan.part_body[p]) return fail(PK_ERR_STATE, "slab layout: mixed group");
+            const int b = plan.part_body[p];
+            const int r0 = plan.perm[pi[0]];
+            if (r0 < segment_row_start[b] || r0 >= segment_row_start[b + 1])
+                return fail(PK_ERR_STATE, "slab layout: part outside its body");
+        }
+    }
+    pk::slab_spmv_host(plan, row_start[n], values, x, y);
+    if (info) {
+        info[0] = plan.parts;
+        info[1] = plan.max_window;
+        info[2] = plan.max_tiles;
+        info[3] = static_cast<int>(plan.stream.size() / 1024);
+        info[4] = launches;
+    }
+    return PK_OK;
+}
 
 PKCUDA_API int pk_slab_plan_selfcheck(int n, const int* row_start, const int* col_index, const double* values,
                                       const double* x, const double* coords, int parts, double* y, int* info)

@@ -133,7 +133,7 @@ class SimWorld:
         if self.X.PHYSIK_B200_SetRefinement(self.h, passes) != 0:
             raise PhysikError("bad refinement pass count")
 
-    PCG_KERNELS = {0: "ring", 1: "staged", 2: "plain", 3: "slab", 4: "batched"}
+    PCG_KERNELS = {0: "ring", 1: "staged", 2: "plain", 3: "slab", 4: "batched", 5: "slab-batched"}
 
     def pcg_kernel(self):
         """(name, blocks) of the PCG kernel the last step's solve ran on."""

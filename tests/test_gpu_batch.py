@@ -5,7 +5,9 @@ stopping test.  The batched step must reproduce, for every body of a many-body w
 step of a one-body world: here against the FP64 oracle run on each body alone (fed the
 same float32 inputs the C ABI passes) and against the unbatched GPU path on each body
 alone.  Bodies differ in size (some are split over several blocks), stiffness, rotation
-and initial velocity, as in the batched uneven-bodies workload.  Tolerances as in the
+and initial velocity, as in the batched uneven-bodies workload.  With FP32 storage the
+batched solve runs on the part-resident kernel with one group of parts per body (checked
+also when the bodies need several launches); the per-body batch kernel serves FP64.  Tolerances as in the
 step parity tests: FP64 positions 1e-12 / velocities 1e-8, mixed positions 1e-5 against
 the FP64 oracle; CG iterations within one.
 """
@@ -135,3 +137,51 @@ def test_batched_toggle_back_to_coupled():
     xa, _ = a.state(f64=True)
     xb, _ = b.state(f64=True)
     assert rel(xa, xb) <= 1e-13
+
+
+@pytest.mark.parametrize("blocks", [0, 2])
+def test_batched_part_resident_kernel_matches_one_body_worlds(blocks):
+    """Mixed precision, batched: the part-resident kernel with a group of parts per body.
+    blocks = 2 caps a launch at two parts, so the five bodies take three launches."""
+    scene = uneven_bodies(count=5, seed=7)
+    gpu = SimWorld(scene, precision="mixed")
+    gpu.set_batched(True)
+    if blocks:
+        gpu.step()
+        gpu.set_pcg_grid(blocks)
+    oracles = [po.Oracle(one_body_scene(scene, i), "f64") for i in range(len(scene.bodies))]
+    sl = body_slices(scene)
+    for step in range(2):
+        gpu.set_state(np.concatenate([o.x for o in oracles]), np.concatenate([o.v for o in oracles]), f64=True)
+        gpu.step()
+        for o in oracles:
+            o.step()
+        assert gpu.pcg_kernel()[0] == "slab-batched", gpu.pcg_kernel()
+        x, v = gpu.state(f64=True)
+        for i, o in enumerate(oracles):
+            assert rel(x[sl[i]], o.x) <= 1e-5, (step, i, rel(x[sl[i]], o.x))
+            assert rel(v[sl[i]], o.v) <= 2e-3, (step, i, rel(v[sl[i]], o.v))
+            bs = gpu.body_stats(i)
+            assert bs["flags"] & L.FLAG_INTEGRATED, hex(bs["flags"])
+            assert abs(bs["iterations"] - o.last_stats()["iterations"]) <= 3, (bs, o.last_stats())
+        st = gpu.cg_stats()
+        assert st["iterations"] == max(gpu.body_stats(i)["iterations"] for i in range(len(oracles)))
+        assert st["flags"] & L.FLAG_INTEGRATED
+
+
+def test_batched_part_resident_agrees_with_batch_kernel(monkeypatch):
+    scene = uneven_bodies(count=4, seed=11)
+    slab = SimWorld(scene, precision="mixed")
+    slab.set_batched(True)
+    slab.step()
+    assert slab.pcg_kernel()[0] == "slab-batched"
+    monkeypatch.setenv("PK_PCG_KERNEL", "ring")  # no part-resident layout: the batch kernel
+    other = SimWorld(scene, precision="mixed")
+    other.set_batched(True)
+    other.step()
+    assert other.pcg_kernel()[0] == "batched"
+    xs, _ = slab.state(f64=True)
+    xo, _ = other.state(f64=True)
+    assert rel(xs, xo) <= 1e-6
+    for i in range(len(scene.bodies)):
+        assert abs(slab.body_stats(i)["iterations"] - other.body_stats(i)["iterations"]) <= 2

@@ -127,3 +127,53 @@ def test_slab_plan_rejects_parts_that_do_not_fit():
     body.pinned = body.pinned[perm]
     rs, col, _ = _pattern_and_coords(scene)
     assert "window" in _reject(rs, col, None, 6)
+
+
+def _segments(scene, n2d):
+    """Dynamic-row ranges of the bodies (rows are numbered body by body)."""
+    seg, base = [0], 0
+    for b in scene.bodies:
+        nodes = b.positions.shape[0]
+        seg.append(seg[-1] + int(np.count_nonzero(n2d[base:base + nodes] >= 0)))
+        base += nodes
+    return np.asarray(seg, np.int32)
+
+
+def _check_batched(scene, max_blocks, coords_on=True, seed=0):
+    w = SimWorld(scene)
+    w.prepare(upload=False)
+    rs, col, n2d, _ = w.pattern()
+    rs, col = rs.astype(np.int32), col.astype(np.int32)
+    n = len(rs) - 1
+    pos = np.concatenate([(b.initial_positions if b.initial_positions is not None else b.positions)
+                          for b in scene.bodies]).astype(np.float64)
+    coords = np.zeros((n, 3))
+    coords[n2d[n2d >= 0]] = pos[n2d >= 0]
+    seg = _segments(scene, n2d)
+    rng = np.random.default_rng(seed)
+    vals = rng.standard_normal(9 * len(col)).astype(np.float32).astype(np.float64)
+    x = rng.standard_normal((n, 3)).astype(np.float32).astype(np.float64)
+    y = np.full((n, 3), np.nan)
+    info = np.zeros(5, np.int32)
+    cp = _ptr(coords) if coords_on else None
+    rc = L.PK.pk_slab_plan_batched_selfcheck(n, _ptr(rs), _ptr(col), _ptr(vals), _ptr(x), cp, _ptr(seg),
+                                             len(seg) - 1, max_blocks, _ptr(y), _ptr(info))
+    assert rc == 0, L.last_error()
+    np.testing.assert_allclose(y, sym_upper_spmv(rs, col, vals, x), rtol=1e-12, atol=1e-10)
+    return info
+
+
+def test_batched_plan_small_worlds():
+    scene = meshes.small_box(4, 3, 3)
+    scene.bodies += meshes.small_box(3, 5, 2, seed=9).bodies + meshes.small_box(2, 2, 2, seed=5).bodies
+    for max_blocks, coords_on in ((1, True), (2, True), (148, True), (3, False)):
+        info = _check_batched(scene, max_blocks, coords_on)
+        assert info[0] == 3 and info[4] == -(-3 // max_blocks)  # one part per small body
+
+
+def test_batched_plan_256_uneven_bodies():
+    scene = meshes.config3()
+    info = _check_batched(scene, 148, seed=3)
+    parts, launches = int(info[0]), int(info[4])
+    assert parts >= 256 and launches == -(-parts // 148) or launches == -(-parts // 148) + 1
+    assert info[1] <= 6144 and info[2] <= 128
