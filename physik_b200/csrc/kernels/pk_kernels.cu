@@ -149,6 +149,10 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
         for (int j = 0; j < nu; ++j)
             for (int e = 0; e < 9; ++e) PK_ACC(j, e) = Real(0);
 
+    // The row's columns in registers (MAXU > 0): the slot search below compares registers.
+    int colr[MAXU > 0 ? MAXU : 1];
+#pragma unroll
+    for (int j = 0; j < (MAXU > 0 ? MAXU : 1); ++j) colr[j] = (MAXU > 0 && j < nu) ? __ldg(A.a.col + ks + j) : -1;
     const V3<Real> vr = ld3(A.v, node);
     V3<Real> fsum{Real(0), Real(0), Real(0)};
     V3<Real> kv{Real(0), Real(0), Real(0)};
@@ -167,9 +171,9 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
                 bad |= !finite3(vb[b]);
             }
         }
-        const Real* rp = A.tets.rot + 9 * (size_t)t;
-        if (isnan(__ldcg(rp))) continue;  // skipped tet: no force, no stiffness
+        // R is NaN-marked for a skipped tet (written by the tet kernel, an earlier launch).
         const M3<Real> R = ld9(A.tets.rot, (size_t)t);
+        if (isnan(R.c[0].x)) continue;  // skipped tet: no force, no stiffness
         const M3<Real> S = ld9(A.tets.stress, (size_t)t);
         const M3<Real> dmi = ld9(A.tets.dm_inv, (size_t)t);
         const Real* prm = A.tets.params + 4 * (size_t)t;
@@ -180,7 +184,10 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
         gr[2] = v3<Real>(dmi.c[0].y, dmi.c[1].y, dmi.c[2].y);
         gr[3] = v3<Real>(dmi.c[0].z, dmi.c[1].z, dmi.c[2].z);
         gr[0] = -((gr[1] + gr[2]) + gr[3]);
-        const V3<Real> ga = gr[a];
+        V3<Real> ga = gr[0];  // selects: a dynamic index would put gr in local memory
+#pragma unroll
+        for (int k = 1; k < 4; ++k)
+            if (a == k) ga = gr[k];
         // Force on node a from this tet: elastic -S g_a plus damping -c v_a.
         const V3<Real> fa = (-mul(S, ga)) + vr * (-damp);
         if (finite3(fa)) fsum = fsum + fa;
@@ -202,8 +209,15 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
             kv = kv + mul(K, vb[b]);
             const int c = __ldg(A.node_to_dyn + nb[b]);
             if (c >= r) {
-                int slot = 0;
-                while (slot < nu && __ldg(A.a.col + ks + slot) != c) ++slot;
+                int slot = nu;
+                if (MAXU > 0) {
+#pragma unroll
+                    for (int j = (MAXU > 0 ? MAXU : 1) - 1; j >= 0; --j)
+                        if (colr[j] == c) slot = j;
+                } else {
+                    slot = 0;
+                    while (slot < nu && __ldg(A.a.col + ks + slot) != c) ++slot;
+                }
                 if (slot < nu) {
                     PK_ACC(slot, 0) += K.c[0].x; PK_ACC(slot, 1) += K.c[0].y; PK_ACC(slot, 2) += K.c[0].z;
                     PK_ACC(slot, 3) += K.c[1].x; PK_ACC(slot, 4) += K.c[1].y; PK_ACC(slot, 5) += K.c[1].z;
