@@ -158,11 +158,25 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
     V3<Real> kv{Real(0), Real(0), Real(0)};
     bool bad = false;
     const int i0 = __ldg(A.inc_start + r), i1 = __ldg(A.inc_start + r + 1);
+    // The next incidence's code, tet nodes and their rows are loaded while this one is
+    // processed (the chain code -> nodes -> rows would otherwise start each iteration).
+    int code_n = 0;
+    int4 tn_n = make_int4(0, 0, 0, 0), dyn_n = make_int4(-1, -1, -1, -1);
+    auto fetch = [&](int i) {
+        code_n = __ldg(A.inc_list + i);
+        tn_n = __ldg(A.tets.nodes + (code_n >> 2));
+        if (!A.explicit_mode)
+            dyn_n = make_int4(__ldg(A.node_to_dyn + tn_n.x), __ldg(A.node_to_dyn + tn_n.y),
+                              __ldg(A.node_to_dyn + tn_n.z), __ldg(A.node_to_dyn + tn_n.w));
+    };
+    if (i0 < i1) fetch(i0);
     for (int i = i0; i < i1; ++i) {
-        const int code = __ldg(A.inc_list + i);
+        const int code = code_n;
         const int t = code >> 2, a = code & 3;
-        const int4 tn = __ldg(A.tets.nodes + t);
+        const int4 tn = tn_n;
         const int nb[4] = {tn.x, tn.y, tn.z, tn.w};
+        const int dyn[4] = {dyn_n.x, dyn_n.y, dyn_n.z, dyn_n.w};
+        if (i + 1 < i1) fetch(i + 1);
         V3<Real> vb[4];
         if (!A.explicit_mode) {
 #pragma unroll
@@ -207,7 +221,7 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
             K.c[2] = pa * (l * pb.z) + pb * (m * pa.z) + rrt.c[2] * md;
             bad |= !finite9(K);
             kv = kv + mul(K, vb[b]);
-            const int c = __ldg(A.node_to_dyn + nb[b]);
+            const int c = dyn[b];
             if (c >= r) {
                 int slot = nu;
                 if (MAXU > 0) {
