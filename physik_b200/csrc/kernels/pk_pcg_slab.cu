@@ -94,6 +94,15 @@ __device__ __forceinline__ void tmem_st16(unsigned taddr, const RowRec& r)
         "r"(r.w[8]), "r"(r.w[9]), "r"(r.w[10]), "r"(r.w[11]), "r"(r.w[12]), "r"(r.w[13]), "r"(r.w[14]), "r"(r.w[15])
         : "memory");
 }
+// x and r of a row record (its first 8 columns: x.xyz, r.xyz and two M^-1 words as they
+// were), without waiting: the caller waits once (tmem_wait_st) before the next reads.
+__device__ __forceinline__ void tmem_st8_nowait(unsigned taddr, const RowRec& r)
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(r.w[0]),
+                 "r"(r.w[1]), "r"(r.w[2]), "r"(r.w[3]), "r"(r.w[4]), "r"(r.w[5]), "r"(r.w[6]), "r"(r.w[7])
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ V3<float> rec3(const RowRec& r, int o)
@@ -501,6 +510,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
             Acc v[2] = {Acc(0), Acc(0)};
             int sbad = 0;
             if (row_owner) {
+                // Stores of x, r (8 columns) without waits: one wait after the loop.
 #pragma unroll
                 for (int k = 0; k < kSlabRowsPerThread; ++k) {
                     if (k >= krows) break;
@@ -519,8 +529,9 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                         put3(rec, 0, xv);
                         put3(rec, 3, rv);
                     }
-                    tmem_st16(tmem_row0 + 16u * (unsigned)k, rec);
+                    tmem_st8_nowait(tmem_row0 + 16u * (unsigned)k, rec);
                 }
+                tmem_wait_st();
             }
             if (!count_exchange<Acc, 2>(P.slots, gcount, gfirst, gsize, P.sync, ++xgen, v, sbad, sh_acc, sh_int)) {
                 timed_out = true;
