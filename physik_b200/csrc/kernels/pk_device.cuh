@@ -328,8 +328,7 @@ __device__ bool group_exchange(ExSlot* slots, int stride, int members, int me, G
         my->v0 = double(v[0]);
         my->v1 = N > 1 ? double(v[N - 1]) : 0.0;
         my->bad = bad;
-        __threadfence();
-        st_release(&my->gen, gen);
+        st_release(&my->gen, gen);  // cumulative: no separate fence
     }
     Acc pv[N];
 #pragma unroll
@@ -397,9 +396,8 @@ __device__ __forceinline__ void count_publish(ExSlot* slots, unsigned* counter, 
         my->v0 = double(v[0]);
         my->v1 = N > 1 ? double(v[N - 1]) : 0.0;
         my->bad = bad;
-        // Release fence (cumulative over the block's stores ordered before it by the block
-        // barrier), then the release increment.
-        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+        // The release increment: a release is cumulative, so it also orders the block's
+        // stores that the block barrier ordered before it (no separate fence).
         red_release_add(counter, 1u);
     }
 }
