@@ -409,9 +409,11 @@ template <class Acc>
 cudaError_t launch_pcg_slab_kernel(const SlabPcgArgs<Acc>& args, int grid, cudaStream_t stream);
 template <class Acc>
 int pcg_slab_max_grid();
-// Writes the assembled upper blocks and their transposes into the slab stream.
-cudaError_t launch_slab_fill_kernel(const float* values, int nnz, const unsigned* pos_u, const unsigned* pos_l,
-                                    float* stream, unsigned long long stream_floats, cudaStream_t stream_);
+// Writes the assembled upper blocks and their transposes into the slab stream, tile by
+// tile (tile_desc: 4 ints per tile; tile_entry0: ntiles + 1 offsets into fill_src).
+cudaError_t launch_slab_fill_kernel(const float* values, int nnz, const int* tile_desc, const int* tile_entry0,
+                                    int ntiles, const unsigned* fill_src, int nentries, float* stream,
+                                    unsigned long long stream_floats, cudaStream_t stream_);
 
 constexpr int kPcgThreads = 512;
 

@@ -659,29 +659,44 @@ finish:
     }
 }
 
-// One thread per canonical upper block: its copy and its transpose into the stream.
-__global__ void slab_fill_kernel(const float* __restrict__ values, int nnz, const unsigned* __restrict__ pos_u,
-                                 const unsigned* __restrict__ pos_l, float* __restrict__ out,
-                                 unsigned long long out_floats)
+// One block per tile: the tile's value area (9 floats per entry, a multiple of 4 floats
+// starting on a 16-byte boundary) written in stream order with 16-byte stores, each float
+// gathered from its upper block -- element j = 3 c + i of a transposed entry is element
+// 3 i + c of the block; padding entries are zero.  A tile that does not match its entry
+// list (the host never builds one) is left alone.
+constexpr int kSlabFillThreads = 128;
+__global__ void __launch_bounds__(kSlabFillThreads)
+    slab_fill_kernel(const float* __restrict__ values, int nnz, const int4* __restrict__ tile_desc,
+                     const int* __restrict__ tile_entry0, int ntiles, const unsigned* __restrict__ fill_src,
+                     int nentries, float* __restrict__ out, unsigned long long out_floats)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nnz) return;
-    float v[9];
-    const float* src = values + 9 * (size_t)k;
+    const int t = blockIdx.x;
+    if (t >= ntiles) return;
+    const int4 d = __ldg(tile_desc + t);
+    const int e0 = __ldg(tile_entry0 + t), e1 = __ldg(tile_entry0 + t + 1);
+    const int ne = e1 - e0;
+    const unsigned long long v0 = 4ull * (unsigned long long)d.x + kSlabHeaderBytes / 4;
+    if (e0 < 0 || ne < 0 || e1 > nentries || d.x < 0 || (ne & 7) != 0 || d.y != kSlabHeaderBytes + kSlabEntryBytes * ne ||
+        v0 + 9ull * (unsigned long long)ne > out_floats)
+        return;
+    float4* dst = reinterpret_cast<float4*>(out + v0);
+    const unsigned* src = fill_src + e0;
+    const int n4 = 9 * ne / 4;
+    for (int f4 = threadIdx.x; f4 < n4; f4 += kSlabFillThreads) {
+        float v[4];
 #pragma unroll
-    for (int e = 0; e < 9; ++e) v[e] = __ldg(src + e);
-    const unsigned pu = __ldg(pos_u + k), pl = __ldg(pos_l + k);
-    if (pu != kSlabNoPos && (unsigned long long)pu + 9 <= out_floats) {
-        float* d = out + pu;
-#pragma unroll
-        for (int e = 0; e < 9; ++e) d[e] = v[e];
-    }
-    if (pl != kSlabNoPos && (unsigned long long)pl + 9 <= out_floats) {
-        float* d = out + pl;
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) d[3 * c + i] = v[3 * i + c];
+        for (int q = 0; q < 4; ++q) {
+            const int f = 4 * f4 + q;
+            const int e = f / 9, j = f - 9 * e;
+            const unsigned s = __ldg(src + e);
+            v[q] = 0.f;
+            if (s != kSlabNoPos) {
+                const unsigned k = s & ~kSlabLowerBit;
+                const int jj = (s & kSlabLowerBit) ? 3 * (j % 3) + j / 3 : j;
+                if (k < (unsigned)nnz) v[q] = __ldg(values + 9 * (size_t)k + jj);
+            }
+        }
+        dst[f4] = make_float4(v[0], v[1], v[2], v[3]);
     }
 }
 
@@ -719,13 +734,14 @@ cudaError_t launch_pcg_slab_kernel(const SlabPcgArgs<Acc>& args, int grid, cudaS
                                        kSlabSmemBytes, stream);
 }
 
-cudaError_t launch_slab_fill_kernel(const float* values, int nnz, const unsigned* pos_u, const unsigned* pos_l,
-                                    float* out, unsigned long long out_floats, cudaStream_t stream)
+cudaError_t launch_slab_fill_kernel(const float* values, int nnz, const int* tile_desc, const int* tile_entry0,
+                                    int ntiles, const unsigned* fill_src, int nentries, float* out,
+                                    unsigned long long out_floats, cudaStream_t stream)
 {
-    if (nnz <= 0) return cudaSuccess;
-    const int threads = 256;
-    slab_fill_kernel<<<(nnz + threads - 1) / threads, threads, 0, stream>>>(values, nnz, pos_u, pos_l, out,
-                                                                             out_floats);
+    if (ntiles <= 0) return cudaSuccess;
+    slab_fill_kernel<<<ntiles, kSlabFillThreads, 0, stream>>>(values, nnz, reinterpret_cast<const int4*>(tile_desc),
+                                                               tile_entry0, ntiles, fill_src, nentries, out,
+                                                               out_floats);
     return cudaGetLastError();
 }
 

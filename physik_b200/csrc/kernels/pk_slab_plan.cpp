@@ -93,8 +93,9 @@ std::string build_layout(int n, const int* row_start, const int* col, const int*
     out.n = n;
     out.parts = parts;
     out.part_info.assign((size_t)kSlabPartInts * parts, 0);
-    out.pos_u.assign(nnz, kSlabNoPos);
-    out.pos_l.assign(nnz, kSlabNoPos);
+    out.fill_src.clear();
+    out.tile_entry0.clear();
+    std::vector<unsigned char> seen(nnz, 0);  // bit 0: copy placed, bit 1: transpose placed
 
     // 3. per part: halo, window indices, tiles, stream
     std::vector<int> win_of(n, -1);  // window index of a row inside the current part
@@ -159,12 +160,16 @@ std::string build_layout(int n, const int* row_start, const int* col, const int*
                 std::sort(row_entries.begin(), row_entries.end(),
                           [](const Entry& x, const Entry& y) { return x.win < y.win; });
                 for (const Entry& en : row_entries) {
-                    const unsigned fpos = static_cast<unsigned>((vals_off + 36 * (size_t)j) / 4);
-                    (en.lower ? out.pos_l : out.pos_u)[en.block] = fpos;
+                    const unsigned char bit = en.lower ? 2 : 1;
+                    if (seen[en.block] & bit) return "internal: a block placed twice";
+                    seen[en.block] |= bit;
+                    out.fill_src.push_back(static_cast<unsigned>(en.block) | (en.lower ? kSlabLowerBit : 0u));
                     put_u16(out.stream, col_off + 2 * (size_t)j, (unsigned)en.win);
                     ++j;
                 }
             }
+            for (int e = j; e < ne; ++e) out.fill_src.push_back(kSlabNoPos);
+            out.tile_entry0.push_back(static_cast<int>(out.fill_src.size()) - ne);
             put_u16(out.stream, off + 2 * (size_t)(b - a), (unsigned)j);
             if (off / 16 > 0x7fffffffULL || stream_bytes / 4 >= 0xffffffffULL) return "stream too large";
             out.tile_desc.insert(out.tile_desc.end(), {static_cast<int>(off / 16), static_cast<int>(bytes), a, b - a});
@@ -185,12 +190,14 @@ std::string build_layout(int n, const int* row_start, const int* col, const int*
         for (int g = g0; g < g1; ++g) win_of[out.perm[g]] = -1;
         for (int i = 0; i < h; ++i) win_of[out.perm[halo[i]]] = -1;
     }
+    out.tile_entry0.push_back(static_cast<int>(out.fill_src.size()));
+    if (out.fill_src.size() > 0x7fffffffu) return "stream too large";  // block ids stay below kSlabLowerBit (int)
     // Every block has its copy; every off-diagonal block also its transpose.
     for (int k = 0; k < nnz; ++k)
-        if (out.pos_u[k] == kSlabNoPos) return "internal: block without a position";
+        if (!(seen[k] & 1)) return "internal: block without a copy";
     for (int r = 0; r < n; ++r)
         for (int k = row_start[r]; k < row_start[r + 1]; ++k)
-            if ((col[k] != r) != (out.pos_l[k] != kSlabNoPos)) return "internal: transposed copy mismatch";
+            if ((col[k] != r) != ((seen[k] & 2) != 0)) return "internal: transposed copy mismatch";
     return "";
 }
 
@@ -399,17 +406,24 @@ void slab_spmv_host(const SlabPlan& plan, int nnz, const double* values, const d
     // Fill, as the fill kernel does (float storage).
     std::vector<unsigned char> s = plan.stream;
     const size_t sfloats = s.size() / 4;
-    auto put = [&](unsigned fpos, int e, double v) {
-        const float f = static_cast<float>(v);
-        std::memcpy(s.data() + 4 * ((size_t)fpos + e), &f, 4);
-    };
-    for (int k = 0; k < nnz; ++k) {
-        const double* b = values + 9 * (size_t)k;
-        if (plan.pos_u[k] != kSlabNoPos && plan.pos_u[k] + 9 <= sfloats)
-            for (int e = 0; e < 9; ++e) put(plan.pos_u[k], e, b[e]);
-        if (plan.pos_l[k] != kSlabNoPos && plan.pos_l[k] + 9 <= sfloats)
-            for (int i = 0; i < 3; ++i)
-                for (int m = 0; m < 3; ++m) put(plan.pos_l[k], 3 * m + i, b[3 * i + m]);
+    const size_t ntiles_all = plan.tile_desc.size() / 4;
+    for (size_t t = 0; t < ntiles_all; ++t) {
+        // The tile's value area, float by float in stream order; element j = 3 c + i of a
+        // transposed entry is element 3 i + c of its block.
+        const int e0 = plan.tile_entry0[t], ne = plan.tile_entry0[t + 1] - e0;
+        const size_t v0 = 4 * (size_t)plan.tile_desc[4 * t] + kSlabHeaderBytes / 4;
+        if (v0 + 9 * (size_t)ne > sfloats) continue;
+        for (int f = 0; f < 9 * ne; ++f) {
+            const int e = f / 9, j = f - 9 * e;
+            const unsigned src = plan.fill_src[(size_t)e0 + e];
+            float v = 0.f;
+            if (src != kSlabNoPos) {
+                const unsigned k = src & ~kSlabLowerBit;
+                const int jj = (src & kSlabLowerBit) ? 3 * (j % 3) + j / 3 : j;
+                if (k < (unsigned)nnz) v = static_cast<float>(values[9 * (size_t)k + jj]);
+            }
+            std::memcpy(s.data() + 4 * (v0 + f), &v, 4);
+        }
     }
     // Decode tile by tile with the kernel's clamps.
     for (int p = 0; p < plan.parts; ++p) {

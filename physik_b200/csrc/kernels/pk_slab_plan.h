@@ -16,8 +16,9 @@
 //     [entries x 9 floats: the blocks, column-major]
 //     [entries x u16: window index of each block's column]
 // with the entry count padded to a multiple of 8 so both arrays start on 16-byte
-// boundaries.  pos_u / pos_l give, for each canonical upper block k, the float offsets of
-// its copy and of its transpose in the stream; a fill kernel writes them after assembly.
+// boundaries.  fill_src names, for every entry of every tile in stream order, the
+// canonical upper block it copies (kSlabLowerBit: its transpose; kSlabNoPos: padding);
+// after assembly a fill kernel writes each tile's blocks in stream order from it.
 //
 // Plain C++ (no CUDA), shared by the runtime and its CPU self-check.
 #pragma once
@@ -47,7 +48,8 @@ constexpr int kSlabMaxRows = kSlabRowThreads * kSlabRowsPerThread;  // rows per 
 // group (its body's parts, consecutive blocks of one launch): first block (within the
 // launch) and size; a single group of all parts for the coupled solve.
 constexpr int kSlabPartInts = 8;
-constexpr unsigned kSlabNoPos = 0xffffffffu;
+constexpr unsigned kSlabNoPos = 0xffffffffu;   // a padding entry
+constexpr unsigned kSlabLowerBit = 0x80000000u; // the entry is the transpose of the block
 
 static_assert(kSlabHeaderBytes + kSlabCapE * kSlabEntryBytes <= kSlabStageBytes, "stage too small");
 static_assert(kSlabCapE % 8 == 0, "entry cap must keep 16-byte alignment");
@@ -62,7 +64,8 @@ struct SlabPlan {
     std::vector<int> halo_src;   // slab index of every halo row, part by part
     std::vector<int> tile_desc;  // 4 per tile: stream offset / 16, bytes, first local row, rows
     std::vector<unsigned char> stream;  // headers and columns filled, blocks zero
-    std::vector<unsigned> pos_u, pos_l; // per canonical upper block: float offsets (kSlabNoPos: none)
+    std::vector<unsigned> fill_src;  // per entry, tile by tile: upper block | kSlabLowerBit, or kSlabNoPos
+    std::vector<int> tile_entry0;    // per tile + 1: the tile's first fill_src index
     std::vector<int> part_body;  // body (segment) of each part; 0 for the coupled solve
     std::vector<int> launch_start;  // parts [launch_start[l], launch_start[l + 1]) form launch l
     int max_window = 0, max_tiles = 0, max_rows = 0;

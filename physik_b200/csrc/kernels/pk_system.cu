@@ -229,7 +229,8 @@ struct pk_system {
     int slab_max_grid = 0;
     std::string slab_reason;      // why the layout does not apply
     unsigned long long slab_stream_bytes = 0;
-    DevBuf slab_part_info, slab_tiles, slab_stream, slab_halo, slab_perm, slab_pos_u, slab_pos_l;
+    DevBuf slab_part_info, slab_tiles, slab_stream, slab_halo, slab_perm, slab_fill_src, slab_tile_e0;
+    int slab_fill_entries = 0;
     DevBuf slab_qs, slab_ss;
     // FP64 outer true-residual refinement (FP32 storage, unbatched): passes, buffers
     int refine_passes = 0;
@@ -484,9 +485,10 @@ void reset_slab(pk_system* s)
 // Copies the assembled upper blocks (and their transposes) into the slab stream.
 int slab_fill(pk_system* s)
 {
-    PK_CHECK(pk::launch_slab_fill_kernel(s->values.as<float>(), s->nnz, s->slab_pos_u.as<unsigned>(),
-                                         s->slab_pos_l.as<unsigned>(), s->slab_stream.as<float>(),
-                                         s->slab_stream_bytes / 4, s->stream));
+    PK_CHECK(pk::launch_slab_fill_kernel(s->values.as<float>(), s->nnz, s->slab_tiles.as<int>(),
+                                         s->slab_tile_e0.as<int>(), s->slab_tile_count,
+                                         s->slab_fill_src.as<unsigned>(), s->slab_fill_entries,
+                                         s->slab_stream.as<float>(), s->slab_stream_bytes / 4, s->stream));
     s->launches += 1;
     s->slab_filled = true;
     return PK_OK;
@@ -555,8 +557,8 @@ int ensure_slab(pk_system* s)
     if (!rc && !plan.halo_src.empty())
         rc = upload_raw<int>(s->slab_halo, plan.halo_src.data(), plan.halo_src.size(), s->stream);
     if (!rc) rc = upload_raw<int>(s->slab_perm, plan.perm.data(), plan.perm.size(), s->stream);
-    if (!rc) rc = upload_raw<unsigned>(s->slab_pos_u, plan.pos_u.data(), plan.pos_u.size(), s->stream);
-    if (!rc) rc = upload_raw<unsigned>(s->slab_pos_l, plan.pos_l.data(), plan.pos_l.size(), s->stream);
+    if (!rc) rc = upload_raw<unsigned>(s->slab_fill_src, plan.fill_src.data(), plan.fill_src.size(), s->stream);
+    if (!rc) rc = upload_raw<int>(s->slab_tile_e0, plan.tile_entry0.data(), plan.tile_entry0.size(), s->stream);
     if (!rc) rc = upload_raw<int>(s->slab_part_body, plan.part_body.data(), plan.part_body.size(), s->stream);
     if (rc) return rc;
     int widest = 1;
@@ -572,6 +574,7 @@ int ensure_slab(pk_system* s)
     PK_CHECK(cudaStreamSynchronize(s->stream));
     s->slab_stream_bytes = plan.stream.size();
     s->slab_tile_count = static_cast<int>(plan.tile_desc.size() / 4);
+    s->slab_fill_entries = static_cast<int>(plan.fill_src.size());
     s->slab_halo_count = static_cast<int>(plan.halo_src.size());
     s->slab_parts = plan.parts;
     return PK_OK;
