@@ -65,27 +65,71 @@ __device__ __forceinline__ V3<Real> row_spmv(const BsrView<Real>& A, int r, int 
     return acc;
 }
 
+// ------------------------------------------------------------------ tet records
+// A record of kTetRec values moved with 16-byte accesses (it starts on a 16-byte boundary).
+__device__ __forceinline__ void st_rec(float* p, const float (&w)[kTetRec])
+{
+#pragma unroll
+    for (int i = 0; i < kTetRec / 4; ++i)
+        reinterpret_cast<float4*>(p)[i] = make_float4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+}
+__device__ __forceinline__ void st_rec(double* p, const double (&w)[kTetRec])
+{
+#pragma unroll
+    for (int i = 0; i < kTetRec / 2; ++i) reinterpret_cast<double2*>(p)[i] = make_double2(w[2 * i], w[2 * i + 1]);
+}
+__device__ __forceinline__ void ld_rec(const float* p, float (&w)[kTetRec])
+{
+#pragma unroll
+    for (int i = 0; i < kTetRec / 4; ++i) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(p) + i);
+        w[4 * i] = v.x;
+        w[4 * i + 1] = v.y;
+        w[4 * i + 2] = v.z;
+        w[4 * i + 3] = v.w;
+    }
+}
+__device__ __forceinline__ void ld_rec(const double* p, double (&w)[kTetRec])
+{
+#pragma unroll
+    for (int i = 0; i < kTetRec / 2; ++i) {
+        const double2 v = __ldg(reinterpret_cast<const double2*>(p) + i);
+        w[2 * i] = v.x;
+        w[2 * i + 1] = v.y;
+    }
+}
+template <class Real>
+__device__ __forceinline__ M3<Real> rd9(const Real* q)
+{
+    M3<Real> m;
+    m.c[0] = V3<Real>{q[0], q[1], q[2]};
+    m.c[1] = V3<Real>{q[3], q[4], q[5]};
+    m.c[2] = V3<Real>{q[6], q[7], q[8]};
+    return m;
+}
+
 // ------------------------------------------------------------------ tet kernel
 template <class Real, bool kFp64Polar>
 __global__ void __launch_bounds__(256) tet_kernel(AssemblyArgs<Real> A)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= A.tets.tet_count) return;
-    Real* rot = A.tets.rot + 9 * (size_t)t;
+    Real* rec = A.tets.rec + kTetRec * (size_t)t;
     const Real* prm = A.tets.params + 4 * (size_t)t;
     const Real vol = __ldg(prm + 0);
     const unsigned char en = __ldg(A.tets.enabled + t);
     if (!(en & 1u) || !(vol > Real(0))) {
-        rot[0] = qnan<Real>();
+        rec[0] = qnan<Real>();
         return;
     }
     const bool linear = A.linear || (en & 2u);
     const int4 n = __ldg(A.tets.nodes + t);
     const V3<Real> x0 = ld3(A.x, n.x), x1 = ld3(A.x, n.y), x2 = ld3(A.x, n.z), x3 = ld3(A.x, n.w);
     const M3<Real> ds = mcols(x1 - x0, x2 - x0, x3 - x0);
-    const M3<Real> f = mul(ds, ld9(A.tets.dm_inv, (size_t)t));
+    const M3<Real> dmi = ld9(A.tets.dm_inv, (size_t)t);
+    const M3<Real> f = mul(ds, dmi);
     if (!finite9(f)) {
-        rot[0] = qnan<Real>();
+        rec[0] = qnan<Real>();
         return;
     }
     M3<Real> R = mident<Real>();
@@ -121,8 +165,16 @@ __global__ void __launch_bounds__(256) tet_kernel(AssemblyArgs<Real> A)
     const Real sxy = vol * two_mu * exy, syz = vol * two_mu * eyz, sxz = vol * two_mu * exz;
     const M3<Real> sig = mcols(v3<Real>(sxx, sxy, sxz), v3<Real>(sxy, syy, syz), v3<Real>(sxz, syz, szz));
     const M3<Real> S = linear ? sig : mul(R, sig);
-    st9(A.tets.rot, (size_t)t, R);
-    st9(A.tets.stress, (size_t)t, S);
+    Real w[kTetRec];
+    st9(w, 0, R);
+    st9(w + 9, 0, S);
+    st9(w + 18, 0, dmi);
+    w[27] = vol;
+    w[28] = lam;
+    w[29] = mu;
+    w[30] = __ldg(prm + 3);
+    w[31] = Real(0);
+    st_rec(rec, w);
 }
 
 // ------------------------------------------------------------------ row kernel
@@ -185,13 +237,15 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
                 bad |= !finite3(vb[b]);
             }
         }
-        // R is NaN-marked for a skipped tet (written by the tet kernel, an earlier launch).
-        const M3<Real> R = ld9(A.tets.rot, (size_t)t);
+        // The tet's record (the tet kernel's, an earlier launch); R is NaN-marked for a
+        // skipped tet.
+        Real w[kTetRec];
+        ld_rec(A.tets.rec + kTetRec * (size_t)t, w);
+        const M3<Real> R = rd9(w);
         if (isnan(R.c[0].x)) continue;  // skipped tet: no force, no stiffness
-        const M3<Real> S = ld9(A.tets.stress, (size_t)t);
-        const M3<Real> dmi = ld9(A.tets.dm_inv, (size_t)t);
-        const Real* prm = A.tets.params + 4 * (size_t)t;
-        const Real vol = __ldg(prm + 0), lam = __ldg(prm + 1), mu = __ldg(prm + 2), damp = __ldg(prm + 3);
+        const M3<Real> S = rd9(w + 9);
+        const M3<Real> dmi = rd9(w + 18);
+        const Real vol = w[27], lam = w[28], mu = w[29], damp = w[30];
         // Shape gradients: g1..g3 are the rows of DmInv, g0 = -(g1+g2+g3).
         V3<Real> gr[4];
         gr[1] = v3<Real>(dmi.c[0].x, dmi.c[1].x, dmi.c[2].x);

@@ -64,9 +64,12 @@ struct TetView {
     const unsigned char* enabled;    // bit 0: active, rest volume > 0, body simulated; bit 1: linear FEM
     const Real* dm_inv;              // 9 per tet, column-major
     const Real* params;              // 4 per tet: rest volume, lambda, mu, damping
-    Real* rot;                       // 9 per tet (R), rot[9t] = NaN when the tet is skipped this step
-    Real* stress;                    // 9 per tet (S = R * V * sigma)
+    // kTetRec per tet, written by the tet kernel each step for the row kernel (one aligned
+    // record per tet): R (9), S = R * V * sigma (9), DmInv (9), rest volume, lambda, mu,
+    // damping, unused; rec[kTetRec t] = NaN when the tet is skipped this step.
+    Real* rec;
 };
+constexpr int kTetRec = 32;
 
 template <class Real>
 struct AssemblyArgs {

@@ -256,7 +256,7 @@ struct pk_system {
     // nodes
     DevBuf x, v, mass, node_to_dyn;
     // tets
-    DevBuf tet_nodes, tet_enabled, dm_inv, tet_params, rot, stress;
+    DevBuf tet_nodes, tet_enabled, dm_inv, tet_params, tet_rec;
     // rows
     DevBuf dyn_to_node, row_start, col, lt_start, lt_row, lt_block, inc_start, inc_list, values, rhs, minv;
     // solver
@@ -285,8 +285,7 @@ pk::AssemblyArgs<Real> assembly_args(pk_system* s, const pk_step_params& p)
     a.tets.enabled = s->tet_enabled.as<unsigned char>();
     a.tets.dm_inv = s->dm_inv.as<Real>();
     a.tets.params = s->tet_params.as<Real>();
-    a.tets.rot = s->rot.as<Real>();
-    a.tets.stress = s->stress.as<Real>();
+    a.tets.rec = s->tet_rec.as<Real>();
     a.a.n = s->dyn_count;
     a.a.row_start = s->row_start.as<int>();
     a.a.col = s->col.as<int>();
@@ -1286,8 +1285,7 @@ PKCUDA_API int pk_system_set_tets(pk_system* s, int tet_count, const int* tet_no
     if (!rc) rc = upload_real_any(s, s->dm_inv, dm_inv, 9 * static_cast<size_t>(tet_count));
     if (!rc) rc = upload_real_any(s, s->tet_params, params.data(), params.size());
     if (rc) return rc;
-    PK_CHECK(s->rot.ensure(9 * s->rsize() * std::max<size_t>(1, tet_count)));
-    PK_CHECK(s->stress.ensure(9 * s->rsize() * std::max<size_t>(1, tet_count)));
+    PK_CHECK(s->tet_rec.ensure(pk::kTetRec * s->rsize() * std::max<size_t>(1, tet_count)));
     s->have_tets = true;
     return PK_OK;
 }
