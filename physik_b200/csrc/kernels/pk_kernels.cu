@@ -66,17 +66,19 @@ __device__ __forceinline__ V3<Real> row_spmv(const BsrView<Real>& A, int r, int 
 }
 
 // ------------------------------------------------------------------ tet records
-// A record of kTetRec values moved with 16-byte accesses (it starts on a 16-byte boundary).
-__device__ __forceinline__ void st_rec(float* p, const float (&w)[kTetRec])
+// A record of kTetRec values moved with 16-byte accesses (it starts on a 16-byte boundary);
+// the tet kernel stores its first 18 values (R, S) each step.
+__device__ __forceinline__ void st_rec_rs(float* p, const float (&w)[18])
 {
 #pragma unroll
-    for (int i = 0; i < kTetRec / 4; ++i)
+    for (int i = 0; i < 4; ++i)
         reinterpret_cast<float4*>(p)[i] = make_float4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+    reinterpret_cast<float2*>(p)[8] = make_float2(w[16], w[17]);
 }
-__device__ __forceinline__ void st_rec(double* p, const double (&w)[kTetRec])
+__device__ __forceinline__ void st_rec_rs(double* p, const double (&w)[18])
 {
 #pragma unroll
-    for (int i = 0; i < kTetRec / 2; ++i) reinterpret_cast<double2*>(p)[i] = make_double2(w[2 * i], w[2 * i + 1]);
+    for (int i = 0; i < 9; ++i) reinterpret_cast<double2*>(p)[i] = make_double2(w[2 * i], w[2 * i + 1]);
 }
 __device__ __forceinline__ void ld_rec(const float* p, float (&w)[kTetRec])
 {
@@ -98,6 +100,24 @@ __device__ __forceinline__ void ld_rec(const double* p, double (&w)[kTetRec])
         w[2 * i + 1] = v.y;
     }
 }
+__device__ __forceinline__ void ld_rec_static(const float* p, float (&w)[12])
+{
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        const float2 v = __ldg(reinterpret_cast<const float2*>(p + 18) + i);
+        w[2 * i] = v.x;
+        w[2 * i + 1] = v.y;
+    }
+}
+__device__ __forceinline__ void ld_rec_static(const double* p, double (&w)[12])
+{
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        const double2 v = __ldg(reinterpret_cast<const double2*>(p + 18) + i);
+        w[2 * i] = v.x;
+        w[2 * i + 1] = v.y;
+    }
+}
 template <class Real>
 __device__ __forceinline__ M3<Real> rd9(const Real* q)
 {
@@ -115,8 +135,11 @@ __global__ void __launch_bounds__(256) tet_kernel(AssemblyArgs<Real> A)
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= A.tets.tet_count) return;
     Real* rec = A.tets.rec + kTetRec * (size_t)t;
-    const Real* prm = A.tets.params + 4 * (size_t)t;
-    const Real vol = __ldg(prm + 0);
+    // The record's static part: DmInv (values 18..26), volume, lambda, mu (27..29), read
+    // with 8-byte loads (value 18 starts on an 8-byte boundary).
+    Real st[12];
+    ld_rec_static(rec, st);
+    const Real vol = st[9];
     const unsigned char en = __ldg(A.tets.enabled + t);
     if (!(en & 1u) || !(vol > Real(0))) {
         rec[0] = qnan<Real>();
@@ -126,7 +149,7 @@ __global__ void __launch_bounds__(256) tet_kernel(AssemblyArgs<Real> A)
     const int4 n = __ldg(A.tets.nodes + t);
     const V3<Real> x0 = ld3(A.x, n.x), x1 = ld3(A.x, n.y), x2 = ld3(A.x, n.z), x3 = ld3(A.x, n.w);
     const M3<Real> ds = mcols(x1 - x0, x2 - x0, x3 - x0);
-    const M3<Real> dmi = ld9(A.tets.dm_inv, (size_t)t);
+    const M3<Real> dmi = rd9(st);
     const M3<Real> f = mul(ds, dmi);
     if (!finite9(f)) {
         rec[0] = qnan<Real>();
@@ -156,7 +179,7 @@ __global__ void __launch_bounds__(256) tet_kernel(AssemblyArgs<Real> A)
     const Real exy = Real(0.5) * (g.c[1].x + g.c[0].y);
     const Real eyz = Real(0.5) * (g.c[2].y + g.c[1].z);
     const Real exz = Real(0.5) * (g.c[2].x + g.c[0].z);
-    const Real lam = __ldg(prm + 1), mu = __ldg(prm + 2);
+    const Real lam = st[10], mu = st[11];
     const Real tr = exx + eyy + ezz;
     const Real two_mu = Real(2) * mu;
     // V * sigma, sigma = lambda tr(eps) I + 2 mu eps  (engineering-shear D of BuildElasticityMatrix)
@@ -165,16 +188,22 @@ __global__ void __launch_bounds__(256) tet_kernel(AssemblyArgs<Real> A)
     const Real sxy = vol * two_mu * exy, syz = vol * two_mu * eyz, sxz = vol * two_mu * exz;
     const M3<Real> sig = mcols(v3<Real>(sxx, sxy, sxz), v3<Real>(sxy, syy, syz), v3<Real>(sxz, syz, szz));
     const M3<Real> S = linear ? sig : mul(R, sig);
-    Real w[kTetRec];
+    Real w[18];
     st9(w, 0, R);
     st9(w + 9, 0, S);
-    st9(w + 18, 0, dmi);
-    w[27] = vol;
-    w[28] = lam;
-    w[29] = mu;
-    w[30] = __ldg(prm + 3);
-    w[31] = Real(0);
-    st_rec(rec, w);
+    st_rec_rs(rec, w);
+}
+
+template <class Real>
+__global__ void tet_pack_kernel(const Real* __restrict__ dm_inv, const Real* __restrict__ params, Real* rec,
+                                int tet_count)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tet_count) return;
+    Real* q = rec + kTetRec * (size_t)t;
+    for (int e = 0; e < 9; ++e) q[18 + e] = dm_inv[9 * (size_t)t + e];
+    for (int e = 0; e < 4; ++e) q[27 + e] = params[4 * (size_t)t + e];
+    q[31] = Real(0);
 }
 
 // ------------------------------------------------------------------ row kernel
@@ -376,6 +405,14 @@ cudaError_t launch_tet_kernel(const AssemblyArgs<Real>& args, bool fp64_polar_fa
     return cudaGetLastError();
 }
 
+template <class Real>
+cudaError_t launch_tet_pack(const Real* dm_inv, const Real* params, Real* rec, int tet_count, cudaStream_t stream)
+{
+    if (tet_count <= 0) return cudaSuccess;
+    tet_pack_kernel<Real><<<(tet_count + 255) / 256, 256, 0, stream>>>(dm_inv, params, rec, tet_count);
+    return cudaGetLastError();
+}
+
 template <class Real, int MAXU>
 static cudaError_t launch_rows(const AssemblyArgs<Real>& args, cudaStream_t stream)
 {
@@ -413,6 +450,8 @@ cudaError_t launch_spmv_kernel(const BsrView<Real>& a, const Real* x, Real* y, c
 
 template cudaError_t launch_tet_kernel<float>(const AssemblyArgs<float>&, bool, cudaStream_t);
 template cudaError_t launch_tet_kernel<double>(const AssemblyArgs<double>&, bool, cudaStream_t);
+template cudaError_t launch_tet_pack<float>(const float*, const float*, float*, int, cudaStream_t);
+template cudaError_t launch_tet_pack<double>(const double*, const double*, double*, int, cudaStream_t);
 template cudaError_t launch_row_kernel<float>(const AssemblyArgs<float>&, int, cudaStream_t);
 template cudaError_t launch_row_kernel<double>(const AssemblyArgs<double>&, int, cudaStream_t);
 template cudaError_t launch_spmv_kernel<float>(const BsrView<float>&, const float*, float*, cudaStream_t);

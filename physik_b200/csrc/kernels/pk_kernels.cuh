@@ -64,9 +64,10 @@ struct TetView {
     const unsigned char* enabled;    // bit 0: active, rest volume > 0, body simulated; bit 1: linear FEM
     const Real* dm_inv;              // 9 per tet, column-major
     const Real* params;              // 4 per tet: rest volume, lambda, mu, damping
-    // kTetRec per tet, written by the tet kernel each step for the row kernel (one aligned
-    // record per tet): R (9), S = R * V * sigma (9), DmInv (9), rest volume, lambda, mu,
-    // damping, unused; rec[kTetRec t] = NaN when the tet is skipped this step.
+    // kTetRec per tet, read by the row kernel (one aligned record per tet): R (9) and
+    // S = R * V * sigma (9), written by the tet kernel each step (rec[kTetRec t] = NaN when
+    // the tet is skipped this step), then DmInv (9), rest volume, lambda, mu, damping and
+    // one unused value, written once when the tets are set (launch_tet_pack).
     Real* rec;
 };
 constexpr int kTetRec = 32;
@@ -385,6 +386,9 @@ struct AdjointArgs {
 // Launchers (pk_kernels.cu).  All asynchronous on `stream`.
 template <class Real>
 cudaError_t launch_tet_kernel(const AssemblyArgs<Real>& args, bool fp64_polar_fallback, cudaStream_t stream);
+// The static part of the tet records (DmInv and the material of every tet).
+template <class Real>
+cudaError_t launch_tet_pack(const Real* dm_inv, const Real* params, Real* rec, int tet_count, cudaStream_t stream);
 template <class Real>
 cudaError_t launch_row_kernel(const AssemblyArgs<Real>& args, int max_row_blocks, cudaStream_t stream);
 template <class Real, class Acc>

@@ -1286,6 +1286,12 @@ PKCUDA_API int pk_system_set_tets(pk_system* s, int tet_count, const int* tet_no
     if (!rc) rc = upload_real_any(s, s->tet_params, params.data(), params.size());
     if (rc) return rc;
     PK_CHECK(s->tet_rec.ensure(pk::kTetRec * s->rsize() * std::max<size_t>(1, tet_count)));
+    if (s->precision == PK_PREC_FP64)
+        PK_CHECK(pk::launch_tet_pack<double>(s->dm_inv.as<double>(), s->tet_params.as<double>(),
+                                             s->tet_rec.as<double>(), tet_count, s->stream));
+    else
+        PK_CHECK(pk::launch_tet_pack<float>(s->dm_inv.as<float>(), s->tet_params.as<float>(),
+                                            s->tet_rec.as<float>(), tet_count, s->stream));
     s->have_tets = true;
     return PK_OK;
 }
