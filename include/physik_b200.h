@@ -131,6 +131,18 @@ PHYSIK_B200_API void PHYSIK_GetNodeVelocity(PhysikWorldHandle world, int nodeInd
 PHYSIK_B200_API void PHYSIK_SetNodePosition(PhysikWorldHandle world, int nodeIndex, float x, float y, float z);
 PHYSIK_B200_API void PHYSIK_SetNodeVelocity(PhysikWorldHandle world, int nodeIndex, float x, float y, float z);
 
+/* ---- point connections ----------------------------------------------- */
+/* PHYSIK_GetPointConnectionCount / PHYSIK_AddPointConnection   PhysiKAPI.h:353-369,
+ * PhysiKAPI.cpp:1431-1475, World.cpp:126-131: a transient barycentric spring between the
+ * point sum_i w_i x(node_i) and a target, kept until the end of the next PHYSIK_Step
+ * (dropped at once unless its four nodes exist and are active); its forces and stiffness
+ * blocks (PointConnection.cpp:55-140) join the device system of that step. */
+PHYSIK_B200_API int PHYSIK_GetPointConnectionCount(PhysikWorldHandle world);
+PHYSIK_B200_API void PHYSIK_AddPointConnection(PhysikWorldHandle world, int node0, int node1, int node2, int node3,
+                                               float barycentricX, float barycentricY, float barycentricZ,
+                                               float barycentricW, float targetX, float targetY, float targetZ,
+                                               float stiffness, float damping);
+
 /* ---- extensions (no counterpart in the reference) --------------------- */
 #define PHYSIK_B200_PRECISION_FP32 0  /* the reference's scalar type: float storage and dot products */
 #define PHYSIK_B200_PRECISION_MIXED 1 /* float storage, double CG scalars, double polar for near-inverted tets */
@@ -139,7 +151,10 @@ PHYSIK_B200_API void PHYSIK_B200_SetPrecision(PhysikWorldHandle world, int preci
 PHYSIK_B200_API int PHYSIK_B200_GetPrecision(PhysikWorldHandle world);
 PHYSIK_B200_API void PHYSIK_B200_SetDevice(PhysikWorldHandle world, int device);
 PHYSIK_B200_API int PHYSIK_B200_GetNodeCount(PhysikWorldHandle world);
-/* Bulk state, 3 values per node in world order; returns nodes copied or -1. */
+/* Bulk state, 3 values per node in world order; returns nodes copied or -1.  The F64
+ * variants move FP64 values to and from the device system once it is uploaded (after the
+ * first step, or PHYSIK_B200_PrepareScene(world, 1)); before that the world keeps its state
+ * in float host copies. */
 PHYSIK_B200_API int PHYSIK_B200_GetNodeStates(PhysikWorldHandle world, float* positions, float* velocities, int count);
 PHYSIK_B200_API int PHYSIK_B200_SetNodeStates(PhysikWorldHandle world, const float* positions, const float* velocities,
                                               int count);

@@ -126,6 +126,20 @@ PKCUDA_API int pk_system_set_tets(pk_system* sys, int tet_count, const int* tet_
 PKCUDA_API int pk_system_set_pattern(pk_system* sys, int dyn_count, const int* dyn_to_node, const int* row_start,
                                      const int* col_index, const int* inc_start, const int* inc_list);
 
+/* Transient point connections for the next steps (PointConnection::UpdateSystem,
+ * src/Core/PhysicsConnections/PointConnection.cpp:55-140), evaluated on the device during
+ * assembly: nodes[4*count] world nodes; params[9*count] barycentric weights (4), target
+ * position (3), stiffness, damping; per dynamic row the list of entries connection*4 +
+ * corner whose corner node is that row and whose weight is non-zero, in connection order
+ * (inc_start[dyn+1], inc_list).  The pattern must already hold the blocks the connections
+ * couple (every pair of corners with non-zero weights whose rows are both dynamic), and
+ * the caller drops connections whose nodes are inactive or whose stiffness or damping is
+ * negative or not finite (World::HasValidNodeIndices and the checks of UpdateSystem).
+ * count 0 removes them; set_pattern removes them too.  With connections present the
+ * batched solve runs as one coupled solve and the adjoint step is refused. */
+PKCUDA_API int pk_system_set_connections(pk_system* sys, int count, const int* nodes, const double* params,
+                                         const int* inc_start, const int* inc_list);
+
 /* Batched per-body solve (no counterpart in the reference, whose World solves all of its
  * bodies as one coupled system): the dynamic rows split into independent segments
  * (bodies) [segment_row_start[b], segment_row_start[b+1]), covering all rows, with no

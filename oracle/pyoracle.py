@@ -287,6 +287,9 @@ class Reference:
         L.ref_dump_begin.restype = _i
         L.ref_dump_copy.argtypes = [_p] + [_p] * 9
         L.ref_dump_cg.argtypes = [_p, _p, _p, _p]
+        L.ref_add_point_connection.argtypes = [_p, _p, _p, _p, _d, _d]
+        L.ref_point_connection_count.argtypes = [_p]
+        L.ref_point_connection_count.restype = _i
         self.h = L.ref_world_create()
         self.precision = precision
         self.dt = scene.dt
@@ -318,6 +321,16 @@ class Reference:
     def set_tet_young(self, body, young):
         y = np.ascontiguousarray(young, np.float64)
         self.lib.ref_set_tet_young(self.h, body, _ptr(y))
+
+    def add_point_connection(self, nodes, weights, target, stiffness, damping=0.0):
+        """World::AddPointConnection (kept until the end of the next step)."""
+        n = np.ascontiguousarray(nodes, np.int32)
+        w = np.ascontiguousarray(weights, np.float64)
+        t = np.ascontiguousarray(target, np.float64)
+        self.lib.ref_add_point_connection(self.h, _ptr(n), _ptr(w), _ptr(t), float(stiffness), float(damping))
+
+    def point_connection_count(self) -> int:
+        return int(self.lib.ref_point_connection_count(self.h))
 
     def set_state(self, x, v):
         x = np.ascontiguousarray(x, np.float64)

@@ -28,6 +28,7 @@
 #define private public
 #define protected public
 #include "PhysiK/Components/TetMeshPhysicsComponent.h"
+#include "PhysiK/Core/PhysicsConnections/PointConnection.h"
 #include "PhysiK/Core/Solvers/SolverData.h"
 #include "PhysiK/Core/World/World.h"
 #include "PhysiK/Geometry/TetMeshGenerator.h"
@@ -145,6 +146,30 @@ __attribute__((visibility("default"))) void ref_get_state(void* h, double* x, do
         if (x) { x[3 * i] = p.x; x[3 * i + 1] = p.y; x[3 * i + 2] = p.z; }
         if (v) { v[3 * i] = q.x; v[3 * i + 1] = q.y; v[3 * i + 2] = q.z; }
     }
+}
+
+// World::AddPointConnection (kept until the end of the next World::Step).
+__attribute__((visibility("default"))) void ref_add_point_connection(void* h, const int* nodes4, const double* weights4,
+                                                                     const double* target3, double stiffness,
+                                                                     double damping)
+{
+    PointConnection c;
+    c.node0 = nodes4[0];
+    c.node1 = nodes4[1];
+    c.node2 = nodes4[2];
+    c.node3 = nodes4[3];
+    c.barycentric = Vec4{static_cast<Real>(weights4[0]), static_cast<Real>(weights4[1]),
+                         static_cast<Real>(weights4[2]), static_cast<Real>(weights4[3])};
+    c.targetPosition = Vec3{static_cast<Real>(target3[0]), static_cast<Real>(target3[1]),
+                            static_cast<Real>(target3[2])};
+    c.stiffness = static_cast<Real>(stiffness);
+    c.damping = static_cast<Real>(damping);
+    H(h)->world.AddPointConnection(c);
+}
+
+__attribute__((visibility("default"))) int ref_point_connection_count(void* h)
+{
+    return H(h)->world.GetTransientConnectionCount();
 }
 
 // World::Step.  Returns 0, or -1 if the reference threw (e.g. a massless dynamic node).

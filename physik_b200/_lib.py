@@ -98,6 +98,7 @@ _SIGS = {
     "pk_system_autotune": (_i, [_p, C.POINTER(PkStepParams), _i, _p, _p]),
     "pk_system_pcg_kernel": (_i, [_p, _p]),
     "pk_system_set_refinement": (_i, [_p, _i]),
+    "pk_system_set_connections": (_i, [_p, _i, _p, _p, _p, _p]),
     # physik_b200.h
     "PHYSIK_CreateWorld": (_p, []),
     "PHYSIK_DestroyWorld": (_v, [_p]),
@@ -141,6 +142,8 @@ _SIGS = {
     "PHYSIK_GetNodeVelocity": (_v, [_p, _i, _p, _p, _p]),
     "PHYSIK_SetNodePosition": (_v, [_p, _i, _f, _f, _f]),
     "PHYSIK_SetNodeVelocity": (_v, [_p, _i, _f, _f, _f]),
+    "PHYSIK_GetPointConnectionCount": (_i, [_p]),
+    "PHYSIK_AddPointConnection": (_v, [_p, _i, _i, _i, _i] + [_f] * 9),
     "PHYSIK_B200_SetPrecision": (_v, [_p, _i]),
     "PHYSIK_B200_GetPrecision": (_i, [_p]),
     "PHYSIK_B200_SetDevice": (_v, [_p, _i]),

@@ -402,6 +402,32 @@ PHYSIK_B200_API void PHYSIK_SetNodeVelocity(PhysikWorldHandle world, int nodeInd
     if (w && ValidNode(*w, nodeIndex)) GuardVoid([&] { w->SetNodeVelocity(nodeIndex, Vec3{x, y, z}); });
 }
 
+// ---------------------------------------------------------------- point connections
+PHYSIK_B200_API int PHYSIK_GetPointConnectionCount(PhysikWorldHandle world)
+{
+    World* w = AsWorld(world);
+    return w ? w->GetTransientConnectionCount() : 0;
+}
+
+PHYSIK_B200_API void PHYSIK_AddPointConnection(PhysikWorldHandle world, int node0, int node1, int node2, int node3,
+                                               float barycentricX, float barycentricY, float barycentricZ,
+                                               float barycentricW, float targetX, float targetY, float targetZ,
+                                               float stiffness, float damping)
+{
+    World* w = AsWorld(world);
+    if (!w) return;
+    PointConnection c;
+    c.node0 = node0;
+    c.node1 = node1;
+    c.node2 = node2;
+    c.node3 = node3;
+    c.barycentric = Vec4{barycentricX, barycentricY, barycentricZ, barycentricW};
+    c.targetPosition = Vec3{targetX, targetY, targetZ};
+    c.stiffness = stiffness;
+    c.damping = damping;
+    GuardVoid([&] { w->AddPointConnection(c); });
+}
+
 // ---------------------------------------------------------------- extensions
 PHYSIK_B200_API void PHYSIK_B200_SetPrecision(PhysikWorldHandle world, int precision)
 {
@@ -524,6 +550,7 @@ PHYSIK_B200_API int PHYSIK_B200_GetSolverSystem(PhysikWorldHandle world, double*
 {
     World* w = AsWorld(world);
     if (!w || !w->GetDeviceSystem()) return -1;
+    if (!w->SceneMatchesDevice()) return -1;  // the caller's arrays are sized by the host scene
     return Guard([&] { return pk_system_get_system_f64(w->GetDeviceSystem(), values, rhs, minv, deltaVelocity); }, -1);
 }
 

@@ -10,6 +10,7 @@
 //   Component / TetMesh*    include/PhysiK/Components/Component.h:13-44,
 //                           TetMeshComponent.h:11-42, TetMeshPhysicsComponent.h:13-85
 //   World                   include/PhysiK/Core/World/World.h:30-137
+//   PointConnection         include/PhysiK/Core/PhysicsConnections/PointConnection.h:12-26
 //
 // What differs by design: node state lives on the GPU (the host copies are synced on
 // access), SolverData owns a device BSR, and World::Step launches one device substep
@@ -350,6 +351,23 @@ public:
 // ------------------------------------------------------------------ world
 struct DeviceScene;
 
+// A transient barycentric spring (PointConnection.h:12-26): the point sum_i w_i x(node_i)
+// pulled towards targetPosition with `stiffness`, its velocity damped with `damping`.
+// World::AddPointConnection keeps it until the end of the frame's World::Step.  Its
+// contributions (PointConnection::UpdateSystem, PointConnection.cpp:55-140: the force
+// times each corner's weight, blocks stiffness * w_i * w_j * I between its corners) are
+// evaluated on the device during assembly.
+struct PointConnection {
+    int node0 = -1;
+    int node1 = -1;
+    int node2 = -1;
+    int node3 = -1;
+    Vec4 barycentric;
+    Vec3 targetPosition;
+    float stiffness = 0.0f;
+    float damping = 0.0f;
+};
+
 class World {
 public:
     World();
@@ -428,6 +446,13 @@ public:
     void SetNodeActive(int nodeIndex, bool active);
     const std::vector<std::unique_ptr<Component>>& GetComponents() const { return components; }
 
+    // Transient point connections (World.cpp:126-131, 727-759): added if its four nodes
+    // exist and are active; cleared when the next World::Step ends (those added during a
+    // substep, after that substep).
+    void AddPointConnection(const PointConnection& connection);
+    int GetTransientConnectionCount() const { return static_cast<int>(transientConnections.size()); }
+    bool HasValidNodeIndices(const PointConnection& connection) const;
+
     // Bulk state access (extension): 3 floats (or doubles) per node, world order.
     void GetNodeStates(float* positions, float* velocities) const;
     void SetNodeStates(const float* positions, const float* velocities);
@@ -436,6 +461,9 @@ public:
 
     // Device access for measurement and tests (extension).
     pk_system* GetDeviceSystem();
+    // Whether the device holds the pattern the host scene describes (a prepare after the
+    // end of a frame with point connections changes the host's before the next upload).
+    bool SceneMatchesDevice() const;
     // Builds the host side of the device scene (and uploads it when `upload`): runs the
     // components' UpdateSystem pass, then mass / mapping / pattern.  Returns dynamic rows.
     int PrepareScene(bool upload);
@@ -459,6 +487,10 @@ private:
     void RunSubstep(float dt);
     void CollectContributions(float dt);
     void EnsureScene(bool upload);
+    bool SyncConnections();
+    void MarkSubstepConnectionBegin() { firstSubstepConnectionIndex = transientConnections.size(); }
+    void ClearSubstepConnections();
+    void ClearFrameConnections();
 
     std::vector<Node> nodes;
     mutable std::vector<Vec3> positions;
@@ -482,6 +514,10 @@ private:
     int refinePasses = 0;
     float lastSubstepDt = 0.0f;
     std::uint64_t topologyVersion = 1;
+
+    std::vector<PointConnection> transientConnections;
+    std::size_t firstSubstepConnectionIndex = 0;
+    std::uint64_t connectionVersion = 1;  // bumped whenever transientConnections changes
 
     SolverData solverData;
     std::unique_ptr<DeviceScene> scene;

@@ -28,6 +28,14 @@ struct Vec3 {
 };
 
 constexpr Vec3 operator*(float s, const Vec3& v) { return v * s; }
+
+// include/PhysiK/Math/Vec4.h: four floats (barycentric weights of a point connection).
+struct Vec4 {
+    float x = 0.0f;
+    float y = 0.0f;
+    float z = 0.0f;
+    float w = 0.0f;
+};
 constexpr float Dot(const Vec3& a, const Vec3& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 constexpr Vec3 Cross(const Vec3& a, const Vec3& b)
 {

@@ -354,6 +354,16 @@ struct DeviceScene {
     int refineOnDevice = 0;
     std::vector<unsigned char> enabled;
     std::vector<double> mass, dmInv, volume, lam, mu, damp;
+    // The FEM bodies' pattern; rowStart / colIndex above are it joined with the blocks of
+    // the current point connections (connPairs, canonical row <= column).
+    std::vector<int> femRowStart, femColIndex;
+    std::vector<std::pair<int, int>> connPairs;
+    std::uint64_t connVersion = 0;  // World::connectionVersion the connection arrays are for
+    int connCount = 0;
+    std::vector<int> connNodes, connIncStart, connIncList;
+    std::vector<double> connParams;
+    bool connOnDevice = false;
+    int devDyn = -1, devNnz = -1;  // the pattern the device holds
 
     ~DeviceScene()
     {
@@ -514,6 +524,12 @@ void BuildHostScene(DeviceScene& sc, const World& w, const std::vector<const Tet
     sc.nodeCount = nn;
     sc.dynCount = dyn;
     sc.tetCount = tetCount;
+    sc.femRowStart = sc.rowStart;
+    sc.femColIndex = sc.colIndex;
+    sc.connPairs.clear();
+    sc.connVersion = 0;
+    sc.connCount = 0;
+    sc.connOnDevice = false;
 }
 
 void UploadScene(DeviceScene& sc, const std::vector<Vec3>& positions, const std::vector<Vec3>& velocities)
@@ -532,6 +548,8 @@ void UploadScene(DeviceScene& sc, const std::vector<Vec3>& positions, const std:
     Check(pk_system_set_pattern(sc.sys, sc.dynCount, sc.dynToNode.data(), sc.rowStart.data(), sc.colIndex.data(),
                                 sc.incStart.data(), sc.incList.data()),
           "set_pattern");
+    sc.devDyn = sc.dynCount;
+    sc.devNnz = static_cast<int>(sc.colIndex.size());
     sc.batchedOnDevice = false;
     sc.graphOnDevice = false;
     sc.refineOnDevice = 0;
@@ -795,6 +813,12 @@ unsigned World::GetLastStepFlags() const
 
 pk_system* World::GetDeviceSystem() { return scene && scene->uploaded ? scene->sys : nullptr; }
 
+bool World::SceneMatchesDevice() const
+{
+    return scene && scene->uploaded && scene->devDyn == scene->dynCount &&
+           scene->devNnz == static_cast<int>(scene->colIndex.size());
+}
+
 void World::PreUpdateComponents(float dt)
 {
     for (auto& e : orderedComponents)
@@ -839,13 +863,141 @@ void World::EnsureScene(bool upload)
         scene->worldVersion = topologyVersion;
         scene->built = true;
     }
+    const bool patternChanged = SyncConnections();
     if (upload && !scene->uploaded) {
         EnsureHostState();
         if (!scene->sys) Check(pk_system_create(device, static_cast<int>(precision), &scene->sys), "pk_system_create");
         UploadScene(*scene, positions, velocities);
+        scene->connOnDevice = false;
         deviceStale = false;
         hostStale = false;
+    } else if (upload && patternChanged) {
+        DeviceScene& sc = *scene;
+        Check(pk_system_set_pattern(sc.sys, sc.dynCount, sc.dynToNode.data(), sc.rowStart.data(), sc.colIndex.data(),
+                                    sc.incStart.data(), sc.incList.data()),
+              "set_pattern");
+        sc.devDyn = sc.dynCount;
+        sc.devNnz = static_cast<int>(sc.colIndex.size());
+        sc.batchedOnDevice = false;  // set_pattern drops the segments
+        sc.connOnDevice = false;
     }
+    if (upload && scene->uploaded && !scene->connOnDevice) {
+        DeviceScene& sc = *scene;
+        Check(pk_system_set_connections(sc.sys, sc.connCount, sc.connNodes.data(), sc.connParams.data(),
+                                        sc.connIncStart.data(), sc.connIncList.data()),
+              "set_connections");
+        sc.connOnDevice = true;
+    }
+}
+
+// The device arrays of the current point connections and the pattern they need:
+// PointConnection::UpdateSystem's checks that do not depend on the state (valid, active
+// nodes; finite, non-negative stiffness and damping) drop a connection; each kept one
+// lists its corners with a non-zero weight under their dynamic rows (connection order),
+// and with stiffness > 0 couples every pair of them (SolverData::AssembleImplicitMatrixAndRhs
+// gives both orientations one canonical block, SolverData.cpp:337-393).  Returns whether
+// the joined pattern changed.
+bool World::SyncConnections()
+{
+    DeviceScene& sc = *scene;
+    if (sc.connVersion == connectionVersion) return false;
+    sc.connVersion = connectionVersion;
+    sc.connNodes.clear();
+    sc.connParams.clear();
+    std::vector<std::pair<int, int>> pairs;
+    std::vector<std::pair<int, int>> inc;  // (row, connection * 4 + corner)
+    int count = 0;
+    for (const PointConnection& pc : transientConnections) {
+        if (!HasValidNodeIndices(pc) || !std::isfinite(pc.stiffness) || !std::isfinite(pc.damping) ||
+            pc.stiffness < 0.0f || pc.damping < 0.0f)
+            continue;
+        const int nd[4] = {pc.node0, pc.node1, pc.node2, pc.node3};
+        const float w[4] = {pc.barycentric.x, pc.barycentric.y, pc.barycentric.z, pc.barycentric.w};
+        for (int a = 0; a < 4; ++a) {
+            sc.connNodes.push_back(nd[a]);
+            sc.connParams.push_back(w[a]);
+        }
+        sc.connParams.push_back(pc.targetPosition.x);
+        sc.connParams.push_back(pc.targetPosition.y);
+        sc.connParams.push_back(pc.targetPosition.z);
+        sc.connParams.push_back(pc.stiffness);
+        sc.connParams.push_back(pc.damping);
+        for (int a = 0; a < 4; ++a) {
+            const int ra = sc.nodeToDyn[static_cast<std::size_t>(nd[a])];
+            if (w[a] == 0.0f || ra < 0) continue;
+            inc.emplace_back(ra, count * 4 + a);
+            if (!(pc.stiffness > 0.0f)) continue;
+            for (int b = 0; b < 4; ++b) {
+                const int rb = sc.nodeToDyn[static_cast<std::size_t>(nd[b])];
+                if (w[b] == 0.0f || rb < 0) continue;
+                pairs.emplace_back(std::min(ra, rb), std::max(ra, rb));
+            }
+        }
+        ++count;
+    }
+    sc.connCount = count;
+    const int dyn = sc.dynCount;
+    sc.connIncStart.assign(static_cast<std::size_t>(dyn) + 1, 0);
+    for (const auto& e : inc) sc.connIncStart[static_cast<std::size_t>(e.first) + 1]++;
+    for (int r = 0; r < dyn; ++r) sc.connIncStart[r + 1] += sc.connIncStart[r];
+    sc.connIncList.assign(inc.size(), 0);
+    {
+        std::vector<int> fill(sc.connIncStart.begin(), sc.connIncStart.end() - 1);
+        for (const auto& e : inc) sc.connIncList[static_cast<std::size_t>(fill[e.first]++)] = e.second;
+    }
+    sc.connOnDevice = false;
+    std::sort(pairs.begin(), pairs.end());
+    pairs.erase(std::unique(pairs.begin(), pairs.end()), pairs.end());
+    if (pairs == sc.connPairs) return false;
+    sc.connPairs = pairs;
+    sc.rowStart.assign(static_cast<std::size_t>(dyn) + 1, 0);
+    sc.colIndex.clear();
+    std::vector<int> cols;
+    std::size_t pi = 0;
+    for (int r = 0; r < dyn; ++r) {
+        cols.assign(sc.femColIndex.begin() + sc.femRowStart[r], sc.femColIndex.begin() + sc.femRowStart[r + 1]);
+        for (; pi < pairs.size() && pairs[pi].first == r; ++pi) cols.push_back(pairs[pi].second);
+        std::sort(cols.begin(), cols.end());
+        cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+        sc.colIndex.insert(sc.colIndex.end(), cols.begin(), cols.end());
+        sc.rowStart[static_cast<std::size_t>(r) + 1] = static_cast<int>(sc.colIndex.size());
+    }
+    return true;
+}
+
+void World::AddPointConnection(const PointConnection& connection)
+{
+    if (!HasValidNodeIndices(connection)) return;
+    transientConnections.push_back(connection);
+    ++connectionVersion;
+}
+
+bool World::HasValidNodeIndices(const PointConnection& c) const
+{
+    const int n = static_cast<int>(nodes.size());
+    const int nd[4] = {c.node0, c.node1, c.node2, c.node3};
+    for (int i : nd)
+        if (i < 0 || i >= n || !nodes[static_cast<std::size_t>(i)].active) return false;
+    return true;
+}
+
+void World::ClearSubstepConnections()
+{
+    if (firstSubstepConnectionIndex > transientConnections.size())
+        firstSubstepConnectionIndex = transientConnections.size();
+    if (transientConnections.size() != firstSubstepConnectionIndex) {
+        transientConnections.resize(firstSubstepConnectionIndex);
+        ++connectionVersion;
+    }
+}
+
+void World::ClearFrameConnections()
+{
+    if (!transientConnections.empty()) {
+        transientConnections.clear();
+        ++connectionVersion;
+    }
+    firstSubstepConnectionIndex = 0;
 }
 
 void World::SetBatchedSolve(bool on) { batchedSolve = on; }
@@ -854,6 +1006,7 @@ void World::AdjointStep(float dt, const double* xbarNext, const double* vbarNext
                         double* thetaBar)
 {
     if (solverMode != SolverMode::ImplicitEuler) throw std::runtime_error("the adjoint step needs the implicit solver");
+    if (!transientConnections.empty()) throw std::runtime_error("the adjoint step does not take point connections");
     if (!(dt > 0.0f)) throw std::runtime_error("dt must be > 0");
     CollectContributions(dt);
     EnsureScene(true);
@@ -975,7 +1128,8 @@ void World::RunSubstep(float dt)
     p.linear = 0;
     p.explicit_mode = solverMode == SolverMode::Explicit ? 1 : 0;
     p.integrate = 1;
-    const bool batch = batchedSolve && scene->segmentsCover && scene->segStart.size() > 2;
+    // Point connections may couple bodies: one coupled solve while any is present.
+    const bool batch = batchedSolve && scene->segmentsCover && scene->segStart.size() > 2 && scene->connCount == 0;
     if (batch != scene->batchedOnDevice) {
         if (batch)
             Check(pk_system_set_segments(scene->sys, static_cast<int>(scene->segStart.size()) - 1,
@@ -1002,14 +1156,20 @@ void World::Step(float frameDt)
 {
     if (frameDt < 0.0f) return;
     PreUpdateComponents(frameDt);
+    MarkSubstepConnectionBegin();
     if (frameDt == 0.0f) {
         PostUpdateComponents(frameDt);
+        ClearFrameConnections();
         return;
     }
     const int steps = std::max(1, substepCount);
     const float dt = frameDt / static_cast<float>(steps);
-    for (int i = 0; i < steps; ++i) RunSubstep(dt);
+    for (int i = 0; i < steps; ++i) {
+        RunSubstep(dt);
+        ClearSubstepConnections();
+    }
     PostUpdateComponents(frameDt);
+    ClearFrameConnections();
 }
 
 }  // namespace PhysiK

@@ -325,6 +325,62 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
             }
         }
     }
+    // Transient point connections with a corner at this row (PointConnection::UpdateSystem,
+    // PointConnection.cpp:55-140): the connection's force times this corner's weight, and
+    // for stiffness > 0 the blocks k w_a w_b I to every corner b with a non-zero weight --
+    // K v_b into the rhs for every b, and into the matrix where the column is a dynamic row
+    // c >= r (the reference emits both orientations and keeps the upper one).
+    if (A.conn_inc_start) {
+        const int j0 = __ldg(A.conn_inc_start + r), j1 = __ldg(A.conn_inc_start + r + 1);
+        for (int i = j0; i < j1; ++i) {
+            const int code = __ldg(A.conn_inc_list + i);
+            const int ci = code >> 2, a = code & 3;
+            if ((unsigned)ci >= (unsigned)A.conn_count) {
+                bad = true;
+                continue;
+            }
+            const Real* ev = A.conn_eval + 4 * (size_t)ci;
+            if (!(ev[3] != Real(0))) continue;  // point, velocity or target not finite: nothing
+            const int4 cn = __ldg(A.conn_nodes + ci);
+            const int nb[4] = {cn.x, cn.y, cn.z, cn.w};
+            const Real* q = A.conn_params + kConnParams * (size_t)ci;
+            const Real w[4] = {__ldg(q), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3)};
+            Real wa = w[0];
+#pragma unroll
+            for (int b = 1; b < 4; ++b)
+                if (a == b) wa = w[b];
+            fsum = fsum + V3<Real>{ev[0], ev[1], ev[2]} * wa;
+            const Real k = __ldg(q + 7);
+            if (A.explicit_mode || !(k > Real(0))) continue;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                if (w[b] == Real(0)) continue;
+                const Real kab = k * wa * w[b];
+                bad |= !isfinite(kab);
+                const V3<Real> vb = ld3(A.v, nb[b]);
+                kv = kv + vb * kab;
+                const int c = __ldg(A.node_to_dyn + nb[b]);
+                if (c >= r) {
+                    int slot = nu;
+                    if (MAXU > 0) {
+#pragma unroll
+                        for (int j = (MAXU > 0 ? MAXU : 1) - 1; j >= 0; --j)
+                            if (colr[j] == c) slot = j;
+                    } else {
+                        slot = 0;
+                        while (slot < nu && __ldg(A.a.col + ks + slot) != c) ++slot;
+                    }
+                    if (slot < nu) {
+                        PK_ACC(slot, 0) += kab;
+                        PK_ACC(slot, 4) += kab;
+                        PK_ACC(slot, 8) += kab;
+                    } else {
+                        bad = true;  // pattern does not hold the block: host/device mismatch
+                    }
+                }
+            }
+        }
+    }
     const Real m = __ldg(A.mass + node);
     const V3<Real> grav{A.gravity[0], A.gravity[1], A.gravity[2]};
     fsum = fsum + grav * m;
@@ -377,6 +433,42 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
     st9(A.minv, (size_t)r, mi);
 }
 
+// ------------------------------------------------------------------ point connections
+// One thread per connection (PointConnection::UpdateSystem, PointConnection.cpp:55-108):
+// the weighted point and velocity of its four nodes, left to right; if they and the
+// target are finite, the force k (target - point) - c velocity, else the connection
+// contributes nothing this step.  Evaluated before the row kernel, which in explicit mode
+// overwrites the nodes' state.
+template <class Real>
+__global__ void conn_kernel(AssemblyArgs<Real> A)
+{
+    const int ci = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ci >= A.conn_count) return;
+    const int4 cn = __ldg(A.conn_nodes + ci);
+    const int nb[4] = {cn.x, cn.y, cn.z, cn.w};
+    const Real* q = A.conn_params + kConnParams * (size_t)ci;
+    V3<Real> p = ld3(A.x, nb[0]) * __ldg(q);
+    V3<Real> u = ld3(A.v, nb[0]) * __ldg(q);
+#pragma unroll
+    for (int b = 1; b < 4; ++b) {
+        p = p + ld3(A.x, nb[b]) * __ldg(q + b);
+        u = u + ld3(A.v, nb[b]) * __ldg(q + b);
+    }
+    const V3<Real> target{__ldg(q + 4), __ldg(q + 5), __ldg(q + 6)};
+    Real* ev = A.conn_eval + 4 * (size_t)ci;
+    if (!finite3(p) || !finite3(u) || !finite3(target)) {
+        ev[0] = ev[1] = ev[2] = Real(0);
+        ev[3] = Real(0);
+        return;
+    }
+    const Real k = __ldg(q + 7), damp = __ldg(q + 8);
+    const V3<Real> f = (target - p) * k + u * (-damp);
+    ev[0] = f.x;
+    ev[1] = f.y;
+    ev[2] = f.z;
+    ev[3] = Real(1);
+}
+
 // ------------------------------------------------------------------ SpMV kernel
 template <class Real>
 __global__ void __launch_bounds__(256) spmv_kernel(BsrView<Real> A, const Real* x, Real* y)
@@ -410,6 +502,14 @@ cudaError_t launch_tet_pack(const Real* dm_inv, const Real* params, Real* rec, i
 {
     if (tet_count <= 0) return cudaSuccess;
     tet_pack_kernel<Real><<<(tet_count + 255) / 256, 256, 0, stream>>>(dm_inv, params, rec, tet_count);
+    return cudaGetLastError();
+}
+
+template <class Real>
+cudaError_t launch_conn_kernel(const AssemblyArgs<Real>& args, cudaStream_t stream)
+{
+    if (args.conn_count <= 0) return cudaSuccess;
+    conn_kernel<Real><<<(args.conn_count + 127) / 128, 128, 0, stream>>>(args);
     return cudaGetLastError();
 }
 
@@ -451,6 +551,8 @@ cudaError_t launch_spmv_kernel(const BsrView<Real>& a, const Real* x, Real* y, c
 template cudaError_t launch_tet_kernel<float>(const AssemblyArgs<float>&, bool, cudaStream_t);
 template cudaError_t launch_tet_kernel<double>(const AssemblyArgs<double>&, bool, cudaStream_t);
 template cudaError_t launch_tet_pack<float>(const float*, const float*, float*, int, cudaStream_t);
+template cudaError_t launch_conn_kernel<float>(const AssemblyArgs<float>&, cudaStream_t);
+template cudaError_t launch_conn_kernel<double>(const AssemblyArgs<double>&, cudaStream_t);
 template cudaError_t launch_tet_pack<double>(const double*, const double*, double*, int, cudaStream_t);
 template cudaError_t launch_row_kernel<float>(const AssemblyArgs<float>&, int, cudaStream_t);
 template cudaError_t launch_row_kernel<double>(const AssemblyArgs<double>&, int, cudaStream_t);

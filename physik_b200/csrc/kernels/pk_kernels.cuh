@@ -95,7 +95,16 @@ struct AssemblyArgs {
     int explicit_mode;
     unsigned* flags;
     DevStats* stats;
+    // Transient point connections (PointConnection::UpdateSystem); conn_inc_start is
+    // NULL when there are none.
+    int conn_count;
+    const int4* conn_nodes;          // 4 world nodes per connection
+    const Real* conn_params;         // kConnParams per connection: weights (4), target (3), stiffness, damping
+    Real* conn_eval;                 // 4 per connection: its force (3) and 1 when it applies this step, else 0
+    const int* conn_inc_start;       // per dyn row
+    const int* conn_inc_list;        // connection*4 + corner (corners with a non-zero weight)
 };
+constexpr int kConnParams = 9;
 
 template <class Real, class Acc>
 struct PcgArgs {
@@ -389,6 +398,10 @@ cudaError_t launch_tet_kernel(const AssemblyArgs<Real>& args, bool fp64_polar_fa
 // The static part of the tet records (DmInv and the material of every tet).
 template <class Real>
 cudaError_t launch_tet_pack(const Real* dm_inv, const Real* params, Real* rec, int tet_count, cudaStream_t stream);
+// Per point connection, before the row kernel: its weighted point and velocity, whether it
+// applies this step, and its force (args.conn_eval).
+template <class Real>
+cudaError_t launch_conn_kernel(const AssemblyArgs<Real>& args, cudaStream_t stream);
 template <class Real>
 cudaError_t launch_row_kernel(const AssemblyArgs<Real>& args, int max_row_blocks, cudaStream_t stream);
 template <class Real, class Acc>

@@ -210,6 +210,9 @@ struct pk_system {
     int ring_tiles = 0;           // ring-staged PCG tiles (0: not used)
     int ring_max_grid = 0;
     DevBuf ring_desc, q4, slots;
+    // transient point connections (cleared by set_pattern)
+    int conn_count = 0;
+    DevBuf conn_nodes, conn_params, conn_eval, conn_inc_start, conn_inc_list;
     // batched per-body solve
     bool batched = false;
     std::vector<int> seg_start;   // body row ranges: [seg_start[b], seg_start[b+1])
@@ -313,6 +316,14 @@ pk::AssemblyArgs<Real> assembly_args(pk_system* s, const pk_step_params& p)
     pk::DevStats* st = s->stats.as<pk::DevStats>();
     a.flags = &st->flags;
     a.stats = st;
+    if (s->conn_count > 0) {
+        a.conn_count = s->conn_count;
+        a.conn_nodes = s->conn_nodes.as<int4>();
+        a.conn_params = s->conn_params.as<Real>();
+        a.conn_eval = s->conn_eval.as<Real>();
+        a.conn_inc_start = s->conn_inc_start.as<int>();
+        a.conn_inc_list = s->conn_inc_list.as<int>();
+    }
     return a;
 }
 
@@ -499,7 +510,9 @@ bool slab_allowed(const pk_system* s)
     return s->precision != PK_PREC_FP64 && (rk == -1 || rk == 3) && s->dyn_count > 0 && s->have_pattern;
 }
 
-bool batched_solve(const pk_system* s) { return s->batched && s->seg_start.size() >= 2; }
+// Point connections may couple bodies: with any present the step solves one coupled
+// system, as the reference always does.
+bool batched_solve(const pk_system* s) { return s->batched && s->seg_start.size() >= 2 && s->conn_count == 0; }
 
 // Builds and uploads the part-resident kernel's layout if it has not been tried yet for
 // this pattern and grid (synchronous: never called while a stream capture is open).
@@ -968,6 +981,10 @@ int run_step(pk_system* s, const pk_step_params& p)
         s->launches += 1;
     }
     if (s->dyn_count > 0) {
+        if (s->conn_count > 0) {
+            PK_CHECK(pk::launch_conn_kernel<Real>(a, s->stream));
+            s->launches += 1;
+        }
         PK_CHECK(pk::launch_row_kernel<Real>(a, s->max_row, s->stream));
         s->launches += 1;
         s->slab_filled = false;
@@ -988,7 +1005,7 @@ int run_step(pk_system* s, const pk_step_params& p)
     if (s->timing) PK_CHECK(cudaEventRecord(s->ev_pool[evi[1]], s->stream));
     if (!p.explicit_mode && s->dyn_count > 0) {
         int rc;
-        const bool refine = s->refine_passes > 0 && !(s->batched && s->seg_start.size() >= 2);
+        const bool refine = s->refine_passes > 0 && !batched_solve(s);
         if constexpr (std::is_same<Real, double>::value)
             rc = run_pcg<double, double>(s, p, 1);
         else if (s->precision == PK_PREC_FP32)
@@ -1296,6 +1313,37 @@ PKCUDA_API int pk_system_set_tets(pk_system* s, int tet_count, const int* tet_no
     return PK_OK;
 }
 
+PKCUDA_API int pk_system_set_connections(pk_system* s, int count, const int* nodes, const double* params,
+                                         const int* inc_start, const int* inc_list)
+{
+    if (s) drop_graph(s);
+    if (!s || count < 0) return fail(PK_ERR_ARG, "set_connections");
+    if (count > 0 && !s->have_pattern) return fail(PK_ERR_STATE, "connections before the pattern");
+    if (count > 0 && (!nodes || !params || !inc_start || (!inc_list && inc_start[s->dyn_count] > 0)))
+        return fail(PK_ERR_ARG, "set_connections: NULL array");
+    if (count > (1 << 29)) return fail(PK_ERR_ARG, "too many connections");
+    PK_CHECK(cudaSetDevice(s->device));
+    s->conn_count = 0;
+    if (count == 0) return PK_OK;
+    for (long long i = 0; i < 4ll * count; ++i)
+        if (nodes[i] < 0 || nodes[i] >= s->node_count) return fail(PK_ERR_ARG, "connection node out of range");
+    const int n = s->dyn_count;
+    if (inc_start[0] != 0) return fail(PK_ERR_ARG, "conn inc_start[0] != 0");
+    for (int r = 0; r < n; ++r)
+        if (inc_start[r + 1] < inc_start[r]) return fail(PK_ERR_ARG, "conn inc_start not monotone");
+    const int total = inc_start[n];
+    for (int i = 0; i < total; ++i)
+        if (inc_list[i] < 0 || (inc_list[i] >> 2) >= count) return fail(PK_ERR_ARG, "bad connection incidence");
+    int rc = upload_raw<int>(s->conn_nodes, nodes, 4 * static_cast<size_t>(count), s->stream);
+    if (!rc) rc = upload_real_any(s, s->conn_params, params, pk::kConnParams * static_cast<size_t>(count));
+    if (!rc) rc = upload_raw<int>(s->conn_inc_start, inc_start, static_cast<size_t>(n) + 1, s->stream);
+    if (!rc && total > 0) rc = upload_raw<int>(s->conn_inc_list, inc_list, total, s->stream);
+    if (rc) return rc;
+    PK_CHECK(s->conn_eval.ensure(4 * s->rsize() * static_cast<size_t>(count)));
+    s->conn_count = count;
+    return PK_OK;
+}
+
 PKCUDA_API int pk_system_set_pattern(pk_system* s, int dyn_count, const int* dyn_to_node, const int* row_start,
                                      const int* col_index, const int* inc_start, const int* inc_list)
 {
@@ -1348,6 +1396,7 @@ PKCUDA_API int pk_system_set_pattern(pk_system* s, int dyn_count, const int* dyn
     if (rc) return rc;
     s->seg_start.clear();
     s->batch_parts = 0;
+    s->conn_count = 0;
     s->assembled = false;
     drop_graph(s);
     s->h_row_start.assign(row_start, row_start + dyn_count + 1);
@@ -1841,6 +1890,7 @@ PKCUDA_API int pk_system_adjoint_step(pk_system* s, const pk_step_params* p, con
     if (!s->have_nodes || !s->have_tets || !s->have_pattern) return fail(PK_ERR_STATE, "adjoint before topology");
     if (!(p->dt > 0.0)) return fail(PK_ERR_ARG, "dt must be > 0");
     if (s->dyn_count > 0 && !s->diag_first) return fail(PK_ERR_ARG, "every dynamic row needs its diagonal block first");
+    if (s->conn_count > 0) return fail(PK_ERR_STATE, "the adjoint step does not take point connections");
     PK_CHECK(cudaSetDevice(s->device));
     drop_graph(s);
     if (s->dyn_count == 0) {

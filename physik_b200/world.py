@@ -95,6 +95,17 @@ class SimWorld:
         if fn(self.h, _ptr(x), _ptr(v), self.node_count) < 0:
             raise PhysikError("SetNodeStates failed: " + self.error())
 
+    def add_point_connection(self, nodes, weights, target, stiffness: float, damping: float = 0.0):
+        """PHYSIK_AddPointConnection: a spring from sum_i weights[i] x(nodes[i]) to `target`,
+        kept until the end of the next step."""
+        n = [int(i) for i in nodes]
+        w = [float(x) for x in weights]
+        t = [float(x) for x in target]
+        self.X.PHYSIK_AddPointConnection(self.h, *n, *w, *t, float(stiffness), float(damping))
+
+    def point_connection_count(self) -> int:
+        return int(self.X.PHYSIK_GetPointConnectionCount(self.h))
+
     def set_batched(self, on: bool = True):
         self.X.PHYSIK_B200_SetBatchedSolve(self.h, 1 if on else 0)
 

@@ -163,3 +163,51 @@ def test_massless_dynamic_node_is_reported_not_thrown():
     X.PHYSIK_AddNode(w.h, 5.0, 5.0, 5.0)  # active, not fixed, no tet: no mass
     assert X.PHYSIK_B200_PrepareScene(w.h, 0) == -1
     assert "no physical mass" in w.error()
+
+
+def _connection_scene():
+    s = meshes.small_box(2, 2, 2)
+    s.bodies += meshes.small_box(3, 2, 2, young=5e4, seed=11).bodies
+    return s
+
+
+def _connections(scene):
+    """Point connections of the checks below: inside body 0, across the two bodies, one with
+    a pinned corner, one without stiffness (forces only), one with repeated nodes, and one
+    naming a node that does not exist (never added)."""
+    n0 = scene.bodies[0].positions.shape[0]
+    n1 = scene.bodies[1].positions.shape[0]
+    pinned0 = int(np.nonzero(scene.bodies[0].pinned)[0][0])
+    return [
+        ((1, 4, 6, 7), (0.25, 0.25, 0.25, 0.25), (0.05, 0.12, 0.3), 40.0, 0.5),
+        ((5, n0 + 7, 0, 0), (0.5, 0.5, 0.0, 0.0), (0.1, 0.1, 0.1), 80.0, 0.0),
+        ((pinned0, 8, 2, 3), (0.4, 0.3, 0.2, 0.1), (0.0, -0.1, 0.2), 25.0, 0.1),
+        ((n0 + 2, n0 + 3, n0 + 9, n0 + 10), (0.1, 0.2, 0.3, 0.4), (0.3, 0.0, 0.0), 0.0, 1.0),
+        ((n0 + 5, n0 + 5, n0 + 6, n0 + 6), (0.3, 0.2, 0.25, 0.25), (0.2, 0.2, 0.0), 15.0, 0.0),
+        ((0, 1, 2, n0 + n1 + 3), (0.25, 0.25, 0.25, 0.25), (0.0, 0.0, 0.0), 10.0, 0.0),
+    ]
+
+
+@needs_ref
+def test_point_connection_pattern_matches_reference():
+    """PHYSIK_AddPointConnection (PhysiKAPI.h:353-369): the connections' blocks join the
+    pattern as SolverData::AssembleImplicitMatrixAndRhs builds it (SolverData.cpp:308-393),
+    and only connections whose nodes exist are kept (World.cpp:126-131, 748-759)."""
+    scene = _connection_scene()
+    w = SimWorld(scene)
+    ref = po.Reference(scene, "f32")
+    for c in _connections(scene):
+        w.add_point_connection(*c)
+        ref.add_point_connection(*c)
+    assert w.point_connection_count() == ref.point_connection_count() == len(_connections(scene)) - 1
+    w.prepare(upload=False)
+    rs, col, n2d, mass = w.pattern()
+    s = ref.system()
+    np.testing.assert_array_equal(rs, s.row_start)
+    np.testing.assert_array_equal(col, s.col)
+    np.testing.assert_array_equal(n2d, s.node_to_dyn)
+    np.testing.assert_array_equal(mass, s.mass)
+    # The blocks across the two bodies are new.
+    plain = SimWorld(scene)
+    plain.prepare(upload=False)
+    assert len(col) > len(plain.pattern()[1])
