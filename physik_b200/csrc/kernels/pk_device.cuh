@@ -368,8 +368,10 @@ __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v)
 
 // Grid exchange through one arrival counter (sync->arrive, zero at launch; exchanges
 // numbered gen = 1, 2, ...): each block stores its partials in its slot of the buffer of
-// the generation's parity and adds one to the counter with release semantics; warp 0 of
-// every block waits (bounded) until the counter reaches gen * gridDim.x, then reads all
+// the generation's parity and adds one to the counter with release semantics; the last
+// warp of every block (in the part-resident kernel the producer warp, which has no row
+// loads of its own in flight while it waits: polling from a warp with outstanding loads
+// measured slower) waits (bounded) until the counter reaches gen * gridDim.x, then reads all
 // slots -- lane i the slots i, i + 32, ... in order -- and reduces them in a fixed shuffle
 // tree, so every block gets identical sums.  One poller warp per block on one address,
 // instead of one poller per slot.  The parity buffers keep a block that runs ahead from
@@ -409,7 +411,7 @@ __device__ bool count_finish(ExSlot* slots, unsigned* counter, int first, int si
     const int G = gridDim.x, tid = threadIdx.x, lane = tid & 31;
     if (size <= 1) return !*(volatile int*)&sync->err;
     const ExSlot* buf = slots + (gen & 1u) * (unsigned)G + first;
-    if (tid < 32) {
+    if ((tid >> 5) == (int)(blockDim.x >> 5) - 1) {
         const unsigned target = gen * (unsigned)size;
         int fail = 0;
         unsigned long long spins = 0;
