@@ -1316,32 +1316,44 @@ PKCUDA_API int pk_system_set_tets(pk_system* s, int tet_count, const int* tet_no
 PKCUDA_API int pk_system_set_connections(pk_system* s, int count, const int* nodes, const double* params,
                                          const int* inc_start, const int* inc_list)
 {
-    if (s) drop_graph(s);
     if (!s || count < 0) return fail(PK_ERR_ARG, "set_connections");
-    if (count > 0 && !s->have_pattern) return fail(PK_ERR_STATE, "connections before the pattern");
-    if (count > 0 && (!nodes || !params || !inc_start || (!inc_list && inc_start[s->dyn_count] > 0)))
-        return fail(PK_ERR_ARG, "set_connections: NULL array");
-    if (count > (1 << 29)) return fail(PK_ERR_ARG, "too many connections");
-    PK_CHECK(cudaSetDevice(s->device));
+    // A captured step reads the connection buffers in place: it stays valid when only
+    // their contents change (same count, no buffer moved), e.g. a drag's new target.
+    const int old_count = s->conn_count;
+    const void* old_bufs[5] = {s->conn_nodes.p, s->conn_params.p, s->conn_eval.p, s->conn_inc_start.p,
+                               s->conn_inc_list.p};
     s->conn_count = 0;
-    if (count == 0) return PK_OK;
-    for (long long i = 0; i < 4ll * count; ++i)
-        if (nodes[i] < 0 || nodes[i] >= s->node_count) return fail(PK_ERR_ARG, "connection node out of range");
-    const int n = s->dyn_count;
-    if (inc_start[0] != 0) return fail(PK_ERR_ARG, "conn inc_start[0] != 0");
-    for (int r = 0; r < n; ++r)
-        if (inc_start[r + 1] < inc_start[r]) return fail(PK_ERR_ARG, "conn inc_start not monotone");
-    const int total = inc_start[n];
-    for (int i = 0; i < total; ++i)
-        if (inc_list[i] < 0 || (inc_list[i] >> 2) >= count) return fail(PK_ERR_ARG, "bad connection incidence");
-    int rc = upload_raw<int>(s->conn_nodes, nodes, 4 * static_cast<size_t>(count), s->stream);
-    if (!rc) rc = upload_real_any(s, s->conn_params, params, pk::kConnParams * static_cast<size_t>(count));
-    if (!rc) rc = upload_raw<int>(s->conn_inc_start, inc_start, static_cast<size_t>(n) + 1, s->stream);
-    if (!rc && total > 0) rc = upload_raw<int>(s->conn_inc_list, inc_list, total, s->stream);
-    if (rc) return rc;
-    PK_CHECK(s->conn_eval.ensure(4 * s->rsize() * static_cast<size_t>(count)));
-    s->conn_count = count;
-    return PK_OK;
+    const int rc = [&]() -> int {
+        if (count == 0) return PK_OK;
+        if (!s->have_pattern) return fail(PK_ERR_STATE, "connections before the pattern");
+        if (!nodes || !params || !inc_start || (!inc_list && inc_start[s->dyn_count] > 0))
+            return fail(PK_ERR_ARG, "set_connections: NULL array");
+        if (count > (1 << 29)) return fail(PK_ERR_ARG, "too many connections");
+        PK_CHECK(cudaSetDevice(s->device));
+        for (long long i = 0; i < 4ll * count; ++i)
+            if (nodes[i] < 0 || nodes[i] >= s->node_count) return fail(PK_ERR_ARG, "connection node out of range");
+        const int n = s->dyn_count;
+        if (inc_start[0] != 0) return fail(PK_ERR_ARG, "conn inc_start[0] != 0");
+        for (int r = 0; r < n; ++r)
+            if (inc_start[r + 1] < inc_start[r]) return fail(PK_ERR_ARG, "conn inc_start not monotone");
+        const int total = inc_start[n];
+        for (int i = 0; i < total; ++i)
+            if (inc_list[i] < 0 || (inc_list[i] >> 2) >= count) return fail(PK_ERR_ARG, "bad connection incidence");
+        int r = upload_raw<int>(s->conn_nodes, nodes, 4 * static_cast<size_t>(count), s->stream);
+        if (!r) r = upload_real_any(s, s->conn_params, params, pk::kConnParams * static_cast<size_t>(count));
+        if (!r) r = upload_raw<int>(s->conn_inc_start, inc_start, static_cast<size_t>(n) + 1, s->stream);
+        if (!r && total > 0) r = upload_raw<int>(s->conn_inc_list, inc_list, total, s->stream);
+        if (r) return r;
+        PK_CHECK(s->conn_eval.ensure(4 * s->rsize() * static_cast<size_t>(count)));
+        s->conn_count = count;
+        return PK_OK;
+    }();
+    const void* new_bufs[5] = {s->conn_nodes.p, s->conn_params.p, s->conn_eval.p, s->conn_inc_start.p,
+                               s->conn_inc_list.p};
+    bool same = rc == PK_OK && s->conn_count == old_count;
+    for (int i = 0; i < 5 && same; ++i) same = old_bufs[i] == new_bufs[i];
+    if (!same) drop_graph(s);
+    return rc;
 }
 
 PKCUDA_API int pk_system_set_pattern(pk_system* s, int dyn_count, const int* dyn_to_node, const int* row_start,
