@@ -393,6 +393,17 @@ void BuildHostScene(DeviceScene& sc, const World& w, const std::vector<const Tet
     sc.lam.clear();
     sc.mu.clear();
     sc.damp.clear();
+    {
+        std::size_t tets = 0;
+        for (const TetMeshPhysicsComponent* body : fem) tets += body->tets.size();
+        sc.tetNodes.reserve(4 * tets);
+        sc.enabled.reserve(tets);
+        sc.dmInv.reserve(9 * tets);
+        sc.volume.reserve(tets);
+        sc.lam.reserve(tets);
+        sc.mu.reserve(tets);
+        sc.damp.reserve(tets);
+    }
     std::vector<T> massT(static_cast<std::size_t>(nn), T(0));
     for (const TetMeshPhysicsComponent* body : fem) {
         const int base = body->GetGlobalNodeBeginIndex();
@@ -467,19 +478,24 @@ void BuildHostScene(DeviceScene& sc, const World& w, const std::vector<const Tet
     }
     sc.rowStart.assign(static_cast<std::size_t>(dyn) + 1, 0);
     sc.colIndex.clear();
+    sc.colIndex.reserve(static_cast<std::size_t>(sc.incStart[dyn]) / 2 + static_cast<std::size_t>(dyn));
     std::vector<int> cols;
+    std::vector<int> seen(static_cast<std::size_t>(dyn), -1);  // the last row that listed the column
     for (int r = 0; r < dyn; ++r) {
         cols.clear();
         cols.push_back(r);
+        seen[static_cast<std::size_t>(r)] = r;
         for (int i = sc.incStart[r]; i < sc.incStart[r + 1]; ++i) {
             const int t = sc.incList[static_cast<std::size_t>(i)] >> 2;
             for (int k = 0; k < 4; ++k) {
                 const int c = sc.nodeToDyn[static_cast<std::size_t>(sc.tetNodes[4 * t + k])];
-                if (c >= r) cols.push_back(c);
+                if (c > r && seen[static_cast<std::size_t>(c)] != r) {
+                    seen[static_cast<std::size_t>(c)] = r;
+                    cols.push_back(c);
+                }
             }
         }
         std::sort(cols.begin(), cols.end());
-        cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
         sc.colIndex.insert(sc.colIndex.end(), cols.begin(), cols.end());
         sc.rowStart[static_cast<std::size_t>(r) + 1] = static_cast<int>(sc.colIndex.size());
     }
