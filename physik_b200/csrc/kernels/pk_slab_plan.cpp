@@ -2,19 +2,52 @@
 #include "pk_slab_plan.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <numeric>
+#include <thread>
 
 namespace pk {
 namespace {
+
+// Host threads for the layout build (at most 16; 1 when none can be started).
+int plan_threads()
+{
+    const unsigned hw = std::thread::hardware_concurrency();
+    return static_cast<int>(std::max(1u, std::min(16u, hw)));
+}
+
+// f(i, thread) for i in [0, count) on up to plan_threads() threads, items handed out in
+// order; each item must write only its own outputs, so the result does not depend on the
+// thread count.  Falls back to one thread if a thread cannot be started.
+template <class F>
+void parallel_items(int count, F&& f)
+{
+    const int nt = std::min(count, plan_threads());
+    if (nt <= 1) {
+        for (int i = 0; i < count; ++i) f(i, 0);
+        return;
+    }
+    std::atomic<int> next{0};
+    auto work = [&](int t) {
+        for (int i; (i = next.fetch_add(1)) < count;) f(i, t);
+    };
+    std::vector<std::thread> pool;
+    try {
+        for (int t = 1; t < nt; ++t) pool.emplace_back(work, t);
+    } catch (...) {
+    }
+    work(0);
+    for (std::thread& th : pool) th.join();
+}
 
 // Recursive coordinate bisection of ids[lo, hi) into `nparts` parts numbered from part0:
 // split across the widest axis of the bounding box at the weighted position that gives
 // the two halves weight in proportion to their part counts.  Ties break by row id, so
 // the result depends only on the inputs.
 void rcb(std::vector<int>& ids, size_t lo, size_t hi, int part0, int nparts, const double* xyz,
-         const std::vector<double>& w, std::vector<int>& part_of)
+         const std::vector<double>& w, std::vector<int>& part_of, int depth = 0)
 {
     if (nparts <= 1 || hi - lo <= 1) {
         for (size_t i = lo; i < hi; ++i) part_of[ids[i]] = part0;
@@ -46,8 +79,23 @@ void rcb(std::vector<int>& ids, size_t lo, size_t hi, int part0, int nparts, con
         cut = std::max(cut, lo + (size_t)left);
         cut = std::min(cut, hi - (size_t)(nparts - left));
     }
-    rcb(ids, lo, cut, part0, left, xyz, w, part_of);
-    rcb(ids, cut, hi, part0 + left, nparts - left, xyz, w, part_of);
+    // The two halves touch disjoint ids: the first levels of large cuts run them on two
+    // threads (same result).
+    if (depth < 4 && hi - lo >= 65536 && plan_threads() > 1) {
+        bool threaded = false;
+        std::thread first;
+        try {
+            first = std::thread([&] { rcb(ids, lo, cut, part0, left, xyz, w, part_of, depth + 1); });
+            threaded = true;
+        } catch (...) {
+        }
+        if (!threaded) rcb(ids, lo, cut, part0, left, xyz, w, part_of, depth + 1);
+        rcb(ids, cut, hi, part0 + left, nparts - left, xyz, w, part_of, depth + 1);
+        if (threaded) first.join();
+        return;
+    }
+    rcb(ids, lo, cut, part0, left, xyz, w, part_of, depth + 1);
+    rcb(ids, cut, hi, part0 + left, nparts - left, xyz, w, part_of, depth + 1);
 }
 
 inline void put_u16(std::vector<unsigned char>& s, size_t off, unsigned v)
@@ -67,14 +115,20 @@ inline unsigned get_u16(const std::vector<unsigned char>& s, size_t off)
 namespace {
 
 // The layout for a given assignment of rows to parts (part_of[r] in [0, parts), every part
-// non-empty): slab order, windows, halos, tiles, stream and block positions.  Group
-// fields of part_info are left for the caller.
+// non-empty): slab order, windows, halos, tiles, stream and the fill list.  Group fields
+// of part_info are left for the caller.
+//
+// Pass 1 (serial) cuts every part's rows into tiles from the rows' block counts alone,
+// which fixes every tile's place in the stream and in the fill list; pass 2 builds the
+// parts' halos, windows and tile contents in parallel, each part writing only its own
+// tiles; pass 3 joins the halos in part order and checks that every block was placed
+// once (and its transpose once, off the diagonal).
 std::string build_layout(int n, const int* row_start, const int* col, const int* lt_start, const int* lt_row,
                          const int* lt_block, const std::vector<int>& part_of, const std::vector<int>& len, int parts,
                          SlabPlan& out)
 {
     const int nnz = row_start[n];
-    // 2. slab order: parts in order, rows ascending inside a part
+    // slab order: parts in order, rows ascending inside a part
     std::vector<int> count(parts + 1, 0);
     for (int r = 0; r < n; ++r) ++count[part_of[r] + 1];
     for (int p = 0; p < parts; ++p) count[p + 1] += count[p];
@@ -95,23 +149,65 @@ std::string build_layout(int n, const int* row_start, const int* col, const int*
     out.part_info.assign((size_t)kSlabPartInts * parts, 0);
     out.fill_src.clear();
     out.tile_entry0.clear();
-    std::vector<unsigned char> seen(nnz, 0);  // bit 0: copy placed, bit 1: transpose placed
+    out.tile_desc.clear();
+    out.halo_src.clear();
 
-    // 3. per part: halo, window indices, tiles, stream
-    std::vector<int> win_of(n, -1);  // window index of a row inside the current part
+    // Pass 1: tiles of consecutive owned rows, at most kSlabRows rows and kSlabCapE
+    // entries (padded to a multiple of 8 so the arrays stay 16-byte aligned).
+    std::vector<int> part_tile0(parts + 1, 0);
+    size_t stream_bytes = 0, entries = 0;
+    for (int p = 0; p < parts; ++p) {
+        const int g0 = count[p], m = count[p + 1] - g0;
+        if (m > kSlabMaxRows) return "a part has more rows than tensor memory holds";
+        part_tile0[p] = static_cast<int>(out.tile_desc.size() / 4);
+        int a = 0;
+        while (a < m) {
+            int b = a, e = 0;
+            while (b < m && b - a < kSlabRows) {
+                const int e2 = e + len[out.perm[g0 + b]];
+                if (((e2 + 7) & ~7) > kSlabCapE) break;
+                e = e2;
+                ++b;
+            }
+            if (b == a) return "a row has more blocks than a tile holds";
+            const int ne = (e + 7) & ~7;
+            const size_t bytes = (size_t)kSlabHeaderBytes + (size_t)kSlabEntryBytes * ne;
+            if (stream_bytes / 16 > 0x7fffffffULL || (stream_bytes + bytes) / 4 >= 0xffffffffULL)
+                return "stream too large";
+            out.tile_desc.insert(out.tile_desc.end(),
+                                 {static_cast<int>(stream_bytes / 16), static_cast<int>(bytes), a, b - a});
+            out.tile_entry0.push_back(static_cast<int>(entries));
+            stream_bytes += bytes;  // bytes is a multiple of 16 (ne is a multiple of 8)
+            entries += ne;
+            if (entries > 0x7fffffffu) return "stream too large";
+            a = b;
+        }
+        if (static_cast<int>(out.tile_desc.size() / 4) - part_tile0[p] > kSlabMaxTiles)
+            return "a part has more tiles than the table holds";
+    }
+    part_tile0[parts] = static_cast<int>(out.tile_desc.size() / 4);
+    out.tile_entry0.push_back(static_cast<int>(entries));
+    out.stream.assign(stream_bytes, 0);
+    out.fill_src.assign(entries, kSlabNoPos);
+
+    // Pass 2: per part, its halo (rows of other parts its rows couple to, ascending slab
+    // index), window indices, and its tiles' row offsets, blocks (upper copies and lower
+    // transposes, by window index) and columns.
     struct Entry {
         int win;     // window index of the column
         int block;   // canonical upper block
         bool lower;  // transpose of that block
     };
-    std::vector<Entry> row_entries;
-    size_t stream_bytes = 0;
-    for (int p = 0; p < parts; ++p) {
+    const int nt = std::min(parts, plan_threads());
+    std::vector<std::vector<int>> win_of(nt);
+    std::vector<std::vector<int>> halos(parts);
+    std::vector<const char*> errors(parts, nullptr);
+    parallel_items(parts, [&](int p, int t) {
+        std::vector<int>& wo = win_of[t];
+        if (wo.empty()) wo.assign(n, -1);
         const int g0 = count[p], g1 = count[p + 1], m = g1 - g0;
-        if (m > kSlabMaxRows) return "a part has more rows than tensor memory holds";
-        for (int g = g0; g < g1; ++g) win_of[out.perm[g]] = g - g0;
-        // halo rows, ascending slab index
-        std::vector<int> halo;
+        for (int g = g0; g < g1; ++g) wo[out.perm[g]] = g - g0;
+        std::vector<int>& halo = halos[p];
         for (int g = g0; g < g1; ++g) {
             const int r = out.perm[g];
             for (int k = row_start[r]; k < row_start[r + 1]; ++k)
@@ -123,76 +219,67 @@ std::string build_layout(int n, const int* row_start, const int* col, const int*
         halo.erase(std::unique(halo.begin(), halo.end()), halo.end());
         const int h = static_cast<int>(halo.size());
         if (m + h > kSlabWinCap) {
-            for (int g = g0; g < g1; ++g) win_of[out.perm[g]] = -1;
-            return "a part's window exceeds shared memory";
+            errors[p] = "a part's window exceeds shared memory";
+            for (int g = g0; g < g1; ++g) wo[out.perm[g]] = -1;
+            return;
         }
-        for (int i = 0; i < h; ++i) win_of[out.perm[halo[i]]] = m + i;
-        const int halo0 = static_cast<int>(out.halo_src.size());
-        out.halo_src.insert(out.halo_src.end(), halo.begin(), halo.end());
-
-        // tiles of consecutive owned rows
-        const int tile0 = static_cast<int>(out.tile_desc.size() / 4);
-        int a = 0;
-        while (a < m) {
-            int b = a, entries = 0;
-            while (b < m && b - a < kSlabRows) {
-                const int e = entries + len[out.perm[g0 + b]];
-                if (((e + 7) & ~7) > kSlabCapE) break;
-                entries = e;
-                ++b;
-            }
-            if (b == a) return "a row has more blocks than a tile holds";
-            const int ne = (entries + 7) & ~7;
-            const size_t bytes = (size_t)kSlabHeaderBytes + (size_t)kSlabEntryBytes * ne;
-            const size_t off = stream_bytes;
-            stream_bytes += bytes;  // bytes is a multiple of 16 (ne is a multiple of 8)
-            out.stream.resize(stream_bytes, 0);
+        for (int i = 0; i < h; ++i) wo[out.perm[halo[i]]] = m + i;
+        std::vector<Entry> row_entries;
+        for (int ti = part_tile0[p]; ti < part_tile0[p + 1]; ++ti) {
+            const int* d = out.tile_desc.data() + 4 * (size_t)ti;
+            const size_t off = 16 * (size_t)d[0];
+            const int a = d[2], b = d[2] + d[3];
+            const int ne = out.tile_entry0[ti + 1] - out.tile_entry0[ti];
             const size_t vals_off = off + kSlabHeaderBytes;
             const size_t col_off = vals_off + 36 * (size_t)ne;
+            unsigned* src = out.fill_src.data() + out.tile_entry0[ti];
             int j = 0;
             for (int i = a; i < b; ++i) {
                 const int r = out.perm[g0 + i];
                 put_u16(out.stream, off + 2 * (size_t)(i - a), (unsigned)j);
                 row_entries.clear();
-                for (int k = row_start[r]; k < row_start[r + 1]; ++k) row_entries.push_back({win_of[col[k]], k, false});
+                for (int k = row_start[r]; k < row_start[r + 1]; ++k) row_entries.push_back({wo[col[k]], k, false});
                 for (int e = lt_start[r]; e < lt_start[r + 1]; ++e)
-                    row_entries.push_back({win_of[lt_row[e]], lt_block[e], true});
+                    row_entries.push_back({wo[lt_row[e]], lt_block[e], true});
                 std::sort(row_entries.begin(), row_entries.end(),
                           [](const Entry& x, const Entry& y) { return x.win < y.win; });
                 for (const Entry& en : row_entries) {
-                    const unsigned char bit = en.lower ? 2 : 1;
-                    if (seen[en.block] & bit) return "internal: a block placed twice";
-                    seen[en.block] |= bit;
-                    out.fill_src.push_back(static_cast<unsigned>(en.block) | (en.lower ? kSlabLowerBit : 0u));
+                    src[j] = static_cast<unsigned>(en.block) | (en.lower ? kSlabLowerBit : 0u);
                     put_u16(out.stream, col_off + 2 * (size_t)j, (unsigned)en.win);
                     ++j;
                 }
             }
-            for (int e = j; e < ne; ++e) out.fill_src.push_back(kSlabNoPos);
-            out.tile_entry0.push_back(static_cast<int>(out.fill_src.size()) - ne);
             put_u16(out.stream, off + 2 * (size_t)(b - a), (unsigned)j);
-            if (off / 16 > 0x7fffffffULL || stream_bytes / 4 >= 0xffffffffULL) return "stream too large";
-            out.tile_desc.insert(out.tile_desc.end(), {static_cast<int>(off / 16), static_cast<int>(bytes), a, b - a});
-            a = b;
         }
-        const int ntiles = static_cast<int>(out.tile_desc.size() / 4) - tile0;
-        if (ntiles > kSlabMaxTiles) return "a part has more tiles than the table holds";
+        for (int g = g0; g < g1; ++g) wo[out.perm[g]] = -1;
+        for (int i = 0; i < h; ++i) wo[out.perm[halo[i]]] = -1;
+    });
+    for (int p = 0; p < parts; ++p)
+        if (errors[p]) return errors[p];
+
+    // Pass 3: halos in part order, part descriptors, and every block placed once.
+    for (int p = 0; p < parts; ++p) {
+        const int g0 = count[p], m = count[p + 1] - g0, h = static_cast<int>(halos[p].size());
         int* pi = out.part_info.data() + (size_t)kSlabPartInts * p;
         pi[0] = g0;
         pi[1] = m;
-        pi[2] = halo0;
+        pi[2] = static_cast<int>(out.halo_src.size());
         pi[3] = h;
-        pi[4] = tile0;
-        pi[5] = ntiles;
+        pi[4] = part_tile0[p];
+        pi[5] = part_tile0[p + 1] - part_tile0[p];
+        out.halo_src.insert(out.halo_src.end(), halos[p].begin(), halos[p].end());
         out.max_window = std::max(out.max_window, m + h);
-        out.max_tiles = std::max(out.max_tiles, ntiles);
+        out.max_tiles = std::max(out.max_tiles, pi[5]);
         out.max_rows = std::max(out.max_rows, m);
-        for (int g = g0; g < g1; ++g) win_of[out.perm[g]] = -1;
-        for (int i = 0; i < h; ++i) win_of[out.perm[halo[i]]] = -1;
     }
-    out.tile_entry0.push_back(static_cast<int>(out.fill_src.size()));
-    if (out.fill_src.size() > 0x7fffffffu) return "stream too large";  // block ids stay below kSlabLowerBit (int)
-    // Every block has its copy; every off-diagonal block also its transpose.
+    std::vector<unsigned char> seen(nnz, 0);  // bit 0: copy placed, bit 1: transpose placed
+    for (const unsigned src : out.fill_src) {
+        if (src == kSlabNoPos) continue;
+        const unsigned k = src & ~kSlabLowerBit;
+        const unsigned char bit = (src & kSlabLowerBit) ? 2 : 1;
+        if (k >= (unsigned)nnz || (seen[k] & bit)) return "internal: a block placed twice";
+        seen[k] |= bit;
+    }
     for (int k = 0; k < nnz; ++k)
         if (!(seen[k] & 1)) return "internal: block without a copy";
     for (int r = 0; r < n; ++r)
