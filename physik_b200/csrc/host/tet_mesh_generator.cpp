@@ -4,7 +4,9 @@
 // drop tets with out-of-range, repeated or near-coplanar corners (6V)^2 <= 1e-24, and
 // count boundary / internal / non-manifold faces.  The node order it produces fixes the
 // world node order and therefore the BSR pattern, so it is reproduced exactly.
+#include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <unordered_map>
 #include <vector>
 
@@ -37,13 +39,6 @@ struct Face {
     int a, b, c;
     bool operator==(const Face& o) const { return a == o.a && b == o.b && c == o.c; }
 };
-struct FaceHash {
-    std::size_t operator()(const Face& f) const
-    {
-        return (static_cast<std::size_t>(f.a) * 1000003u) ^ (static_cast<std::size_t>(f.b) * 998244353u) ^
-               static_cast<std::size_t>(f.c);
-    }
-};
 Face SortedFace(int a, int b, int c)
 {
     if (b < a) std::swap(a, b);
@@ -67,7 +62,14 @@ GeneratedTetMesh TetMeshGenerator::Generate(const Vec3* positions, int nodeCount
     const float tol2 = tol * tol;
     const bool weld = options.weldCoincidentNodes && tol > 0.0f;
     std::vector<int> remap(static_cast<std::size_t>(nodeCount), -1);
-    std::unordered_map<Cell, std::vector<int>, CellHash> grid;
+    // Hash grid: per cell the first and last kept node, chained in insertion order
+    // through `next` (no allocation per cell).
+    std::unordered_map<Cell, std::pair<int, int>, CellHash> grid;
+    std::vector<int> next;
+    if (weld) {
+        grid.reserve(static_cast<std::size_t>(nodeCount));
+        next.reserve(static_cast<std::size_t>(nodeCount));
+    }
     out.positions.reserve(static_cast<std::size_t>(nodeCount));
     for (int i = 0; i < nodeCount; ++i) {
         const Vec3& p = positions[i];
@@ -79,7 +81,7 @@ GeneratedTetMesh TetMeshGenerator::Generate(const Vec3* positions, int nodeCount
                     for (int dx = -1; dx <= 1 && found < 0; ++dx) {
                         auto it = grid.find(Cell{c.x + dx, c.y + dy, c.z + dz});
                         if (it == grid.end()) continue;
-                        for (int cand : it->second)
+                        for (int cand = it->second.first; cand >= 0; cand = next[static_cast<std::size_t>(cand)])
                             if ((out.positions[static_cast<std::size_t>(cand)] - p).LengthSquared() <= tol2) {
                                 found = cand;
                                 break;
@@ -93,7 +95,14 @@ GeneratedTetMesh TetMeshGenerator::Generate(const Vec3* positions, int nodeCount
         const int id = static_cast<int>(out.positions.size());
         out.positions.push_back(p);
         remap[static_cast<std::size_t>(i)] = id;
-        if (weld) grid[CellOf(p, tol)].push_back(id);
+        if (weld) {
+            next.push_back(-1);
+            auto ins = grid.emplace(CellOf(p, tol), std::make_pair(id, id));
+            if (!ins.second) {
+                next[static_cast<std::size_t>(ins.first->second.second)] = id;
+                ins.first->second.second = id;
+            }
+        }
     }
     out.weldedNodeCount = static_cast<int>(out.positions.size());
     out.weldedAwayNodeCount = out.rawNodeCount - out.weldedNodeCount;
@@ -131,19 +140,48 @@ GeneratedTetMesh TetMeshGenerator::Generate(const Vec3* positions, int nodeCount
         }
     }
 
-    std::unordered_map<Face, int, FaceHash> faces;
+    // Faces by how many kept tets share them: every tet's four sorted faces, sorted, then
+    // counted run by run (the same counts as a map from face to tets).
     const int kept = static_cast<int>(out.tetLocalNodeIndices.size() / 4u);
+    std::vector<Face> faces;
+    faces.reserve(4 * static_cast<std::size_t>(kept));
     for (int t = 0; t < kept; ++t) {
         const int* n = &out.tetLocalNodeIndices[static_cast<std::size_t>(4 * t)];
-        ++faces[SortedFace(n[0], n[1], n[2])];
-        ++faces[SortedFace(n[0], n[3], n[1])];
-        ++faces[SortedFace(n[0], n[2], n[3])];
-        ++faces[SortedFace(n[1], n[3], n[2])];
+        faces.push_back(SortedFace(n[0], n[1], n[2]));
+        faces.push_back(SortedFace(n[0], n[3], n[1]));
+        faces.push_back(SortedFace(n[0], n[2], n[3]));
+        faces.push_back(SortedFace(n[1], n[3], n[2]));
     }
-    for (const auto& f : faces) {
-        if (f.second == 1) ++out.topologyDiagnostics.boundaryFaceCount;
-        else if (f.second == 2) ++out.topologyDiagnostics.internalFaceCount;
-        else if (f.second > 2) ++out.topologyDiagnostics.nonManifoldFaceCount;
+    const int nn = static_cast<int>(out.positions.size());
+    if (nn < (1 << 21)) {
+        // 21 bits per node index: one 64-bit key per face.
+        std::vector<std::uint64_t> keys(faces.size());
+        for (std::size_t i = 0; i < faces.size(); ++i)
+            keys[i] = (static_cast<std::uint64_t>(faces[i].a) << 42) | (static_cast<std::uint64_t>(faces[i].b) << 21) |
+                      static_cast<std::uint64_t>(faces[i].c);
+        std::sort(keys.begin(), keys.end());
+        for (std::size_t i = 0; i < keys.size();) {
+            std::size_t j = i + 1;
+            while (j < keys.size() && keys[j] == keys[i]) ++j;
+            const std::size_t k = j - i;
+            if (k == 1) ++out.topologyDiagnostics.boundaryFaceCount;
+            else if (k == 2) ++out.topologyDiagnostics.internalFaceCount;
+            else ++out.topologyDiagnostics.nonManifoldFaceCount;
+            i = j;
+        }
+    } else {
+        std::sort(faces.begin(), faces.end(), [](const Face& x, const Face& y) {
+            return x.a < y.a || (x.a == y.a && (x.b < y.b || (x.b == y.b && x.c < y.c)));
+        });
+        for (std::size_t i = 0; i < faces.size();) {
+            std::size_t j = i + 1;
+            while (j < faces.size() && faces[j] == faces[i]) ++j;
+            const std::size_t k = j - i;
+            if (k == 1) ++out.topologyDiagnostics.boundaryFaceCount;
+            else if (k == 2) ++out.topologyDiagnostics.internalFaceCount;
+            else ++out.topologyDiagnostics.nonManifoldFaceCount;
+            i = j;
+        }
     }
     return out;
 }
