@@ -202,7 +202,7 @@ std::string build_layout(int n, const int* row_start, const int* col, const int*
     std::vector<std::vector<int>> win_of(nt);
     std::vector<std::vector<int>> halos(parts);
     std::vector<const char*> errors(parts, nullptr);
-    parallel_items(parts, [&](int p, int t) {
+    auto build_part = [&](int p, int t) {
         std::vector<int>& wo = win_of[t];
         if (wo.empty()) wo.assign(n, -1);
         const int g0 = count[p], g1 = count[p + 1], m = g1 - g0;
@@ -253,6 +253,13 @@ std::string build_layout(int n, const int* row_start, const int* col, const int*
         }
         for (int g = g0; g < g1; ++g) wo[out.perm[g]] = -1;
         for (int i = 0; i < h; ++i) wo[out.perm[halo[i]]] = -1;
+    };
+    parallel_items(parts, [&](int p, int t) {
+        try {
+            build_part(p, t);
+        } catch (...) {  // nothing may leave a worker thread
+            errors[p] = "host memory exhausted while building the layout";
+        }
     });
     for (int p = 0; p < parts; ++p)
         if (errors[p]) return errors[p];
