@@ -908,11 +908,13 @@ void World::EnsureScene(bool upload)
 
 // The device arrays of the current point connections and the pattern they need:
 // PointConnection::UpdateSystem's checks that do not depend on the state (valid, active
-// nodes; finite, non-negative stiffness and damping) drop a connection; each kept one
-// lists its corners with a non-zero weight under their dynamic rows (connection order),
-// and with stiffness > 0 couples every pair of them (SolverData::AssembleImplicitMatrixAndRhs
-// gives both orientations one canonical block, SolverData.cpp:337-393).  Returns whether
-// the joined pattern changed.
+// nodes; finite, non-negative stiffness and damping; finite target) drop a connection;
+// each kept one lists its corners with a non-zero weight under their dynamic rows
+// (connection order), and with stiffness > 0 couples every pair of them
+// (SolverData::AssembleImplicitMatrixAndRhs gives both orientations one canonical block,
+// SolverData.cpp:337-393).  A kept connection whose point or velocity is not finite in a
+// step contributes nothing then (the device checks), its blocks staying in the pattern as
+// zeros.  Returns whether the joined pattern changed.
 bool World::SyncConnections()
 {
     DeviceScene& sc = *scene;
@@ -925,7 +927,8 @@ bool World::SyncConnections()
     int count = 0;
     for (const PointConnection& pc : transientConnections) {
         if (!HasValidNodeIndices(pc) || !std::isfinite(pc.stiffness) || !std::isfinite(pc.damping) ||
-            pc.stiffness < 0.0f || pc.damping < 0.0f)
+            pc.stiffness < 0.0f || pc.damping < 0.0f || !std::isfinite(pc.targetPosition.x) ||
+            !std::isfinite(pc.targetPosition.y) || !std::isfinite(pc.targetPosition.z))
             continue;
         const int nd[4] = {pc.node0, pc.node1, pc.node2, pc.node3};
         const float w[4] = {pc.barycentric.x, pc.barycentric.y, pc.barycentric.z, pc.barycentric.w};

@@ -173,8 +173,9 @@ def _connection_scene():
 
 def _connections(scene):
     """Point connections of the checks below: inside body 0, across the two bodies, one with
-    a pinned corner, one without stiffness (forces only), one with repeated nodes, and one
-    naming a node that does not exist (never added)."""
+    a pinned corner, one without stiffness (forces only), one with repeated nodes, one
+    naming a node that does not exist (never added), and one with a non-finite target (kept,
+    but it adds no block)."""
     n0 = scene.bodies[0].positions.shape[0]
     n1 = scene.bodies[1].positions.shape[0]
     pinned0 = int(np.nonzero(scene.bodies[0].pinned)[0][0])
@@ -185,6 +186,7 @@ def _connections(scene):
         ((n0 + 2, n0 + 3, n0 + 9, n0 + 10), (0.1, 0.2, 0.3, 0.4), (0.3, 0.0, 0.0), 0.0, 1.0),
         ((n0 + 5, n0 + 5, n0 + 6, n0 + 6), (0.3, 0.2, 0.25, 0.25), (0.2, 0.2, 0.0), 15.0, 0.0),
         ((0, 1, 2, n0 + n1 + 3), (0.25, 0.25, 0.25, 0.25), (0.0, 0.0, 0.0), 10.0, 0.0),
+        ((2, n0 + 11, 3, 4), (0.5, 0.5, 0.0, 0.0), (float("nan"), 0.0, 0.0), 30.0, 0.0),
     ]
 
 
