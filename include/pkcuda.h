@@ -106,6 +106,9 @@ PKCUDA_API void* pk_system_stream(pk_system* sys);
 /* Nodes in world order: node_to_dyn[i] is node i's dynamic row or -1; mass[i] the
  * assembled lumped mass (SolverData::AssembleMasses order).  Resets state to zero. */
 PKCUDA_API int pk_system_set_nodes(pk_system* sys, int node_count, const int* node_to_dyn, const double* mass);
+/* New lumped masses for the same nodes (after tets were deactivated or a material changed,
+ * with the dynamic-row map unchanged); the nodes' state is kept. */
+PKCUDA_API int pk_system_set_masses(pk_system* sys, const double* mass);
 /* Either pointer may be NULL.  3*node_count values each. */
 PKCUDA_API int pk_system_set_state_f32(pk_system* sys, const float* x, const float* v);
 PKCUDA_API int pk_system_set_state_f64(pk_system* sys, const double* x, const double* v);

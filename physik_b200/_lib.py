@@ -99,6 +99,7 @@ _SIGS = {
     "pk_system_pcg_kernel": (_i, [_p, _p]),
     "pk_system_set_refinement": (_i, [_p, _i]),
     "pk_system_set_connections": (_i, [_p, _i, _p, _p, _p, _p]),
+    "pk_system_set_masses": (_i, [_p, _p]),
     # physik_b200.h
     "PHYSIK_CreateWorld": (_p, []),
     "PHYSIK_DestroyWorld": (_v, [_p]),

@@ -726,6 +726,9 @@ bool World::IsNodeFixed(int i) const { return nodes.at(static_cast<std::size_t>(
 
 void World::SetNodeActive(int i, bool activeValue)
 {
+    // An active node that stays active changes nothing (the tet-deactivation reconcile
+    // asks this of every corner): leave the state where it is, on the device.
+    if (activeValue && nodes.at(static_cast<std::size_t>(i)).active) return;
     EnsureHostState();
     Node& n = nodes.at(static_cast<std::size_t>(i));
     if (n.active != activeValue) ++topologyVersion;
@@ -868,6 +871,20 @@ void World::EnsureScene(bool upload)
     }
     if (!scene->Matches(*this, fem)) {
         EnsureHostState();
+        // What the device holds: when a rebuild keeps the dynamic rows, the pattern, the
+        // incidences and the tets' nodes (tets deactivated while their nodes stay dynamic,
+        // a material change), only the masses and the tet data are uploaded again -- the
+        // device keeps its state, its PCG layouts and its segments.
+        const bool update = scene->uploaded && scene->connPairs.empty();
+        std::vector<int> oldN2D, oldRowStart, oldCol, oldIncStart, oldInc, oldTets;
+        if (update) {
+            oldN2D.swap(scene->nodeToDyn);
+            oldRowStart.swap(scene->femRowStart);
+            oldCol.swap(scene->femColIndex);
+            oldIncStart.swap(scene->incStart);
+            oldInc.swap(scene->incList);
+            oldTets.swap(scene->tetNodes);
+        }
         scene->built = false;
         scene->uploaded = false;
         scene->bodies.clear();
@@ -878,6 +895,15 @@ void World::EnsureScene(bool upload)
             BuildHostScene<float>(*scene, *this, fem);
         scene->worldVersion = topologyVersion;
         scene->built = true;
+        DeviceScene& sc = *scene;
+        if (update && oldN2D == sc.nodeToDyn && oldRowStart == sc.femRowStart && oldCol == sc.femColIndex &&
+            oldIncStart == sc.incStart && oldInc == sc.incList && oldTets == sc.tetNodes) {
+            Check(pk_system_set_masses(sc.sys, sc.mass.data()), "set_masses");
+            Check(pk_system_set_tets(sc.sys, sc.tetCount, sc.tetNodes.data(), sc.enabled.data(), sc.dmInv.data(),
+                                     sc.volume.data(), sc.lam.data(), sc.mu.data(), sc.damp.data()),
+                  "set_tets");
+            sc.uploaded = true;
+        }
     }
     const bool patternChanged = SyncConnections();
     if (upload && !scene->uploaded) {

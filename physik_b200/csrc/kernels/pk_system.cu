@@ -1275,6 +1275,16 @@ PKCUDA_API int pk_system_get_state_f32(pk_system* s, float* x, float* v)
     return PK_OK;
 }
 
+PKCUDA_API int pk_system_set_masses(pk_system* s, const double* mass)
+{
+    if (s) drop_graph(s);
+    if (!s || !mass) return fail(PK_ERR_ARG, "set_masses");
+    if (!s->have_nodes) return fail(PK_ERR_STATE, "masses before the nodes");
+    PK_CHECK(cudaSetDevice(s->device));
+    s->h_mass.assign(mass, mass + s->node_count);
+    return upload_real_any(s, s->mass, mass, s->node_count);
+}
+
 PKCUDA_API int pk_system_set_tets(pk_system* s, int tet_count, const int* tet_nodes, const unsigned char* enabled,
                                   const double* dm_inv, const double* volume, const double* lambda, const double* mu,
                                   const double* damping)

@@ -207,3 +207,30 @@ def test_staged_and_unstaged_agree_on_beam():
     (xb, vb), ib = out[1]
     assert ia == ib
     assert rel(xa, xb) < 1e-13 and rel(va, vb) < 1e-9
+
+
+def test_deactivation_between_steps_keeps_device_state():
+    """Tets deactivated between steps while their nodes stay in other tets: the pattern is
+    unchanged, so only masses and tet data go to the device again and its FP64 state carries
+    over exactly; the following free steps match the oracle with the same tets off."""
+    scene = meshes.small_box(3, 2, 2)
+    gpu = SimWorld(scene, precision="fp64")
+    ora = po.Oracle(scene, "f64", float_inputs=True)
+    for _ in range(2):
+        gpu.set_state(ora.x, ora.v, f64=True)
+        gpu.step()
+        ora.step()
+    off = [30, 40]
+    active = np.ones(scene.tet_count, np.uint8)
+    active[off] = 0
+    tets = scene.bodies[0].tets
+    assert len(np.unique(tets[active.astype(bool)])) == scene.vertex_count  # every node stays in a tet
+    for t in off:
+        L.PX.PHYSIK_SetTetActive(gpu.h, gpu.components[0], t, 0)
+    ora.set_tet_active(active)
+    for _ in range(2):
+        gpu.step()
+        ora.step()
+        x, v = gpu.state(f64=True)
+        assert rel(x, ora.x) < 1e-12, rel(x, ora.x)
+        assert rel(v, ora.v) < 1e-8, rel(v, ora.v)
