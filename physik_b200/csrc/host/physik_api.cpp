@@ -60,16 +60,17 @@ void ReconcileNodes(World& w, const TetMeshComponent& mesh, int tetIndex)
     for (int corner = 0; corner < 4; ++corner) {
         const int g = mesh.GetGlobalNodeIndex(mesh.GetTetNodeIndex(tetIndex, corner));
         if (!ValidNode(w, g)) continue;
+        // Any active tet of an active mesh with g as a corner (through each mesh's cached
+        // node-to-tet lists instead of a scan of every tet).
         bool referenced = false;
         for (const auto& c : w.GetComponents()) {
             const auto* tm = dynamic_cast<const TetMeshComponent*>(c.get());
             if (!tm || !tm->active) continue;
-            for (int t = 0; t < tm->GetTetCount() && !referenced; ++t) {
-                if (!tm->IsTetActive(t)) continue;
-                for (int k = 0; k < 4; ++k)
-                    if (tm->GetGlobalNodeIndex(tm->GetTetNodeIndex(t, k)) == g) referenced = true;
+            const int local = tm->GetLocalNodeIndexOf(g);
+            if (local >= 0 && tm->HasActiveTetAtLocalNode(local)) {
+                referenced = true;
+                break;
             }
-            if (referenced) break;
         }
         w.SetNodeActive(g, referenced);
     }

@@ -301,6 +301,17 @@ public:
     virtual bool DeactivateTet(int tetIndex) { return SetTetActive(tetIndex, false); }
     int GetActiveTetCount() const;
     void PostUpdate(World& world, float dt) override;
+    // The local index of world node `globalNodeIndex` in this mesh, or -1.
+    int GetLocalNodeIndexOf(int globalNodeIndex) const;
+    // Whether an active tet of this mesh has local node `localNodeIndex` as a corner (the
+    // node-to-tet lists are built on first use and dropped by SetGeometry or when `tets`
+    // is resized or moved).
+    bool HasActiveTetAtLocalNode(int localNodeIndex) const;
+
+private:
+    mutable std::vector<int> nodeTetStart, nodeTetList;
+    mutable std::size_t nodeTetCount = 0;
+    mutable const Tet* nodeTetData = nullptr;
 };
 
 struct TetMeshPhysicsComponentDesc {

@@ -90,6 +90,9 @@ void LameParameters(float young, float poisson, T& lambda, T& mu)
 // ------------------------------------------------------------------ TetMeshComponent
 void TetMeshComponent::SetGeometry(const GeneratedTetMesh& mesh)
 {
+    nodeTetStart.clear();
+    nodeTetList.clear();
+    nodeTetData = nullptr;
     restNodePositions = mesh.positions;
     nodePositions = restNodePositions;
     tets.clear();
@@ -141,6 +144,42 @@ void TetMeshComponent::SetLocalCurrentPosition(int i, const Vec3& p)
 {
     if (i < 0 || i >= static_cast<int>(nodePositions.size())) return;
     nodePositions[static_cast<std::size_t>(i)] = p;
+}
+
+int TetMeshComponent::GetLocalNodeIndexOf(int globalNodeIndex) const
+{
+    // GetGlobalNodeIndex is begin + local for the meshes that own world nodes, -1 otherwise.
+    const int n = GetNodeCount();
+    if (n <= 0) return -1;
+    const int begin = GetGlobalNodeIndex(0);
+    if (begin < 0) return -1;
+    const int local = globalNodeIndex - begin;
+    return (local >= 0 && local < n && GetGlobalNodeIndex(local) == globalNodeIndex) ? local : -1;
+}
+
+bool TetMeshComponent::HasActiveTetAtLocalNode(int localNodeIndex) const
+{
+    const int n = GetNodeCount();
+    if (localNodeIndex < 0 || localNodeIndex >= n) return false;
+    if (nodeTetData != tets.data() || nodeTetCount != tets.size() || nodeTetStart.size() != static_cast<std::size_t>(n) + 1) {
+        nodeTetStart.assign(static_cast<std::size_t>(n) + 1, 0);
+        for (const Tet& t : tets)
+            for (int k : {t.node0, t.node1, t.node2, t.node3})
+                if (k >= 0 && k < n) ++nodeTetStart[static_cast<std::size_t>(k) + 1];
+        for (int i = 0; i < n; ++i) nodeTetStart[i + 1] += nodeTetStart[i];
+        nodeTetList.assign(static_cast<std::size_t>(nodeTetStart[n]), 0);
+        std::vector<int> fill(nodeTetStart.begin(), nodeTetStart.end() - 1);
+        for (int ti = 0; ti < static_cast<int>(tets.size()); ++ti) {
+            const Tet& t = tets[static_cast<std::size_t>(ti)];
+            for (int k : {t.node0, t.node1, t.node2, t.node3})
+                if (k >= 0 && k < n) nodeTetList[static_cast<std::size_t>(fill[k]++)] = ti;
+        }
+        nodeTetData = tets.data();
+        nodeTetCount = tets.size();
+    }
+    for (int i = nodeTetStart[localNodeIndex]; i < nodeTetStart[localNodeIndex + 1]; ++i)
+        if (tets[static_cast<std::size_t>(nodeTetList[static_cast<std::size_t>(i)])].active) return true;
+    return false;
 }
 
 bool TetMeshComponent::IsTetActive(int tetIndex) const
