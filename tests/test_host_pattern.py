@@ -213,3 +213,21 @@ def test_point_connection_pattern_matches_reference():
     plain = SimWorld(scene)
     plain.prepare(upload=False)
     assert len(col) > len(plain.pattern()[1])
+
+
+def test_point_connection_needs_active_nodes():
+    """World::AddPointConnection keeps a connection only if its four nodes exist and are
+    active (World.cpp:126-131, 748-759): a node whose tets are all deactivated is inactive."""
+    scene = meshes.small_box(2, 2, 2)
+    w = SimWorld(scene)
+    tets = scene.bodies[0].tets
+    node = 0
+    around = np.nonzero((tets == node).any(axis=1))[0]
+    for t in around:
+        L.PX.PHYSIK_SetTetActive(w.h, w.components[0], int(t), 0)
+    w.add_point_connection((node, 1, 2, 3), (0.25, 0.25, 0.25, 0.25), (0.0, 0.0, 0.0), 10.0)
+    assert w.point_connection_count() == 0
+    other = int(tets[np.setdiff1d(np.arange(len(tets)), around)[0], 0])
+    w.add_point_connection((other, other, other, other), (1.0, 0.0, 0.0, 0.0), (0.0, 0.0, 0.0), 10.0)
+    w.add_point_connection((-1, 1, 2, 3), (0.25, 0.25, 0.25, 0.25), (0.0, 0.0, 0.0), 10.0)
+    assert w.point_connection_count() == 1
