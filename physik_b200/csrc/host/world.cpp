@@ -24,6 +24,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../../include/pkcuda.h"
@@ -39,6 +40,37 @@ constexpr int kMinConjugateGradientMaxIterations = 1;
 constexpr int kMaxConjugateGradientMaxIterations = 1024;
 
 const Vec3 kZero{};
+
+// f(lo, hi) over [0, count) in contiguous chunks on up to 16 host threads (one thread
+// for small counts or when no thread can be started); chunks write disjoint outputs.
+template <class F>
+void ParallelRanges(std::size_t count, F&& f)
+{
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const std::size_t nt = count < 65536 ? 1 : std::min<std::size_t>(hw, count / 16384);
+    if (nt <= 1) {
+        f(std::size_t(0), count);
+        return;
+    }
+    const std::size_t chunk = (count + nt - 1) / nt;
+    std::vector<std::thread> pool;
+    std::size_t started = 0;
+    try {
+        for (std::size_t t = 1; t < nt; ++t) {
+            const std::size_t lo = t * chunk, hi = std::min(count, lo + chunk);
+            if (lo >= hi) break;
+            pool.emplace_back([&f, lo, hi] { f(lo, hi); });
+            started = t;
+        }
+    } catch (...) {
+    }
+    f(std::size_t(0), std::min(count, chunk));
+    for (std::size_t t = started + 1; t < nt; ++t) {  // chunks whose thread could not start
+        const std::size_t lo = t * chunk, hi = std::min(count, lo + chunk);
+        if (lo < hi) f(lo, hi);
+    }
+    for (std::thread& th : pool) th.join();
+}
 
 void Check(int rc, const char* what)
 {
@@ -425,56 +457,63 @@ void BuildHostScene(DeviceScene& sc, const World& w, const std::vector<const Tet
 {
     const std::vector<Node>& nodes = w.GetNodes();
     const int nn = static_cast<int>(nodes.size());
-    sc.tetNodes.clear();
-    sc.enabled.clear();
-    sc.dmInv.clear();
-    sc.volume.clear();
-    sc.lam.clear();
-    sc.mu.clear();
-    sc.damp.clear();
-    {
-        std::size_t tets = 0;
-        for (const TetMeshPhysicsComponent* body : fem) tets += body->tets.size();
-        sc.tetNodes.reserve(4 * tets);
-        sc.enabled.reserve(tets);
-        sc.dmInv.reserve(9 * tets);
-        sc.volume.reserve(tets);
-        sc.lam.reserve(tets);
-        sc.mu.reserve(tets);
-        sc.damp.reserve(tets);
-    }
+    std::size_t total = 0;
+    for (const TetMeshPhysicsComponent* body : fem) total += body->tets.size();
+    sc.tetNodes.assign(4 * total, 0);
+    sc.enabled.assign(total, 0);
+    sc.dmInv.assign(9 * total, 0.0);
+    sc.volume.assign(total, 0.0);
+    sc.lam.assign(total, 0.0);
+    sc.mu.assign(total, 0.0);
+    sc.damp.assign(total, 0.0);
+    std::vector<T> nodal(total, T(0));  // each tet's lumped mass share (0: none)
     std::vector<T> massT(static_cast<std::size_t>(nn), T(0));
+    std::size_t first = 0;
     for (const TetMeshPhysicsComponent* body : fem) {
         const int base = body->GetGlobalNodeBeginIndex();
         const T density = std::max(T(0), T(body->material.density));
         const bool femImplemented = body->GetFemModel() != FemModel::NeoHookean;
         const unsigned char linearBit = body->GetFemModel() == FemModel::Linear ? 2 : 0;
-        for (const Tet& t : body->tets) {
-            const int n[4] = {t.node0 + base, t.node1 + base, t.node2 + base, t.node3 + base};
-            const RestData<T> rd = ComputeRest<T>(body->restNodePositions[t.node0], body->restNodePositions[t.node1],
-                                                  body->restNodePositions[t.node2], body->restNodePositions[t.node3]);
-            for (int k = 0; k < 4; ++k) sc.tetNodes.push_back(n[k]);
-            sc.enabled.push_back(static_cast<unsigned char>(
-                (t.active && rd.volume > T(0) && femImplemented ? 1 : 0) | linearBit));
-            for (int c = 0; c < 3; ++c) {
-                sc.dmInv.push_back(static_cast<double>(rd.dm_inv.c[c].x));
-                sc.dmInv.push_back(static_cast<double>(rd.dm_inv.c[c].y));
-                sc.dmInv.push_back(static_cast<double>(rd.dm_inv.c[c].z));
+        const std::vector<Tet>& tets = body->tets;
+        // Per tet, independent of the others (on host threads for large bodies).
+        ParallelRanges(tets.size(), [&](std::size_t lo, std::size_t hi) {
+            for (std::size_t i = lo; i < hi; ++i) {
+                const Tet& t = tets[i];
+                const std::size_t g = first + i;
+                const RestData<T> rd = ComputeRest<T>(body->restNodePositions[t.node0], body->restNodePositions[t.node1],
+                                                      body->restNodePositions[t.node2], body->restNodePositions[t.node3]);
+                sc.tetNodes[4 * g + 0] = t.node0 + base;
+                sc.tetNodes[4 * g + 1] = t.node1 + base;
+                sc.tetNodes[4 * g + 2] = t.node2 + base;
+                sc.tetNodes[4 * g + 3] = t.node3 + base;
+                sc.enabled[g] = static_cast<unsigned char>((t.active && rd.volume > T(0) && femImplemented ? 1 : 0) |
+                                                           linearBit);
+                for (int c = 0; c < 3; ++c) {
+                    sc.dmInv[9 * g + 3 * c + 0] = static_cast<double>(rd.dm_inv.c[c].x);
+                    sc.dmInv[9 * g + 3 * c + 1] = static_cast<double>(rd.dm_inv.c[c].y);
+                    sc.dmInv[9 * g + 3 * c + 2] = static_cast<double>(rd.dm_inv.c[c].z);
+                }
+                sc.volume[g] = static_cast<double>(rd.volume);
+                T l, m;
+                LameParameters<T>(t.youngModulus, t.poissonRatio, l, m);
+                sc.lam[g] = static_cast<double>(l);
+                sc.mu[g] = static_cast<double>(m);
+                sc.damp[g] = static_cast<double>(T(t.damping));
+                if (std::isfinite(static_cast<double>(density)) && t.active &&
+                    std::isfinite(static_cast<double>(rd.volume)) && rd.volume > T(0)) {
+                    const T share = density * rd.volume * T(0.25);
+                    if (std::isfinite(static_cast<double>(share)) && share > T(0)) nodal[g] = share;
+                }
             }
-            sc.volume.push_back(static_cast<double>(rd.volume));
-            T l, m;
-            LameParameters<T>(t.youngModulus, t.poissonRatio, l, m);
-            sc.lam.push_back(static_cast<double>(l));
-            sc.mu.push_back(static_cast<double>(m));
-            sc.damp.push_back(static_cast<double>(T(t.damping)));
-            // Lumped mass rho V / 4 to the non-fixed nodes of active tets, in tet order.
-            if (std::isfinite(static_cast<double>(density)) && t.active && std::isfinite(static_cast<double>(rd.volume)) &&
-                rd.volume > T(0)) {
-                const T nodal = density * rd.volume * T(0.25);
-                if (std::isfinite(static_cast<double>(nodal)) && nodal > T(0))
-                    for (int k = 0; k < 4; ++k)
-                        if (!nodes[static_cast<std::size_t>(n[k])].fixed) massT[static_cast<std::size_t>(n[k])] += nodal;
-            }
+        });
+        first += tets.size();
+    }
+    // Lumped mass rho V / 4 to the non-fixed nodes of active tets, summed in tet order.
+    for (std::size_t g = 0; g < total; ++g) {
+        if (!(nodal[g] > T(0))) continue;
+        for (int k = 0; k < 4; ++k) {
+            const int n = sc.tetNodes[4 * g + k];
+            if (!nodes[static_cast<std::size_t>(n)].fixed) massT[static_cast<std::size_t>(n)] += nodal[g];
         }
     }
     // World::ValidateNodeMasses
