@@ -66,6 +66,12 @@ GeneratedTetMesh TetMeshGenerator::Generate(const Vec3* positions, int nodeCount
     // through `next` (no allocation per cell).
     std::unordered_map<Cell, std::pair<int, int>, CellHash> grid;
     std::vector<int> next;
+    // A bit per hashed cell, set when a node is stored in the cell: a clear bit means the
+    // cell is empty, so most of the 27 neighbour probes skip the map.
+    constexpr std::size_t kOccBits = std::size_t(1) << 24;
+    std::vector<std::uint64_t> occ(weld ? kOccBits / 64 : 0, 0);
+    const CellHash hasher;
+    auto occ_bit = [&](const Cell& c) { return hasher(c) & (kOccBits - 1); };
     if (weld) {
         grid.reserve(static_cast<std::size_t>(nodeCount));
         next.reserve(static_cast<std::size_t>(nodeCount));
@@ -79,7 +85,10 @@ GeneratedTetMesh TetMeshGenerator::Generate(const Vec3* positions, int nodeCount
             for (int dz = -1; dz <= 1 && found < 0; ++dz)
                 for (int dy = -1; dy <= 1 && found < 0; ++dy)
                     for (int dx = -1; dx <= 1 && found < 0; ++dx) {
-                        auto it = grid.find(Cell{c.x + dx, c.y + dy, c.z + dz});
+                        const Cell nc{c.x + dx, c.y + dy, c.z + dz};
+                        const std::size_t bit = occ_bit(nc);
+                        if (!(occ[bit >> 6] >> (bit & 63) & 1u)) continue;
+                        auto it = grid.find(nc);
                         if (it == grid.end()) continue;
                         for (int cand = it->second.first; cand >= 0; cand = next[static_cast<std::size_t>(cand)])
                             if ((out.positions[static_cast<std::size_t>(cand)] - p).LengthSquared() <= tol2) {
@@ -97,7 +106,10 @@ GeneratedTetMesh TetMeshGenerator::Generate(const Vec3* positions, int nodeCount
         remap[static_cast<std::size_t>(i)] = id;
         if (weld) {
             next.push_back(-1);
-            auto ins = grid.emplace(CellOf(p, tol), std::make_pair(id, id));
+            const Cell pc = CellOf(p, tol);
+            const std::size_t bit = occ_bit(pc);
+            occ[bit >> 6] |= std::uint64_t(1) << (bit & 63);
+            auto ins = grid.emplace(pc, std::make_pair(id, id));
             if (!ins.second) {
                 next[static_cast<std::size_t>(ins.first->second.second)] = id;
                 ins.first->second.second = id;
