@@ -177,3 +177,26 @@ def test_batched_plan_256_uneven_bodies():
     parts, launches = int(info[0]), int(info[4])
     assert parts >= 256 and launches == -(-parts // 148) or launches == -(-parts // 148) + 1
     assert info[1] <= 6144 and info[2] <= 128
+
+
+def test_slab_plan_pattern_joined_with_point_connections():
+    """The pattern with point-connection blocks (two bodies joined, PHYSIK_AddPointConnection)
+    through the part-resident layout: the blocks coupling the bodies cross parts."""
+    scene = meshes.small_box(4, 3, 3)
+    scene.bodies.append(meshes.small_box(3, 5, 2, seed=9).bodies[0])
+    n0 = scene.bodies[0].positions.shape[0]
+    w = SimWorld(scene)
+    w.add_point_connection((5, n0 + 7, 9, n0 + 12), (0.25, 0.25, 0.25, 0.25), (0.1, 0.1, 0.1), 50.0)
+    w.add_point_connection((20, 21, n0 + 30, n0 + 31), (0.4, 0.1, 0.3, 0.2), (0.0, 0.2, 0.1), 10.0)
+    w.prepare(upload=False)
+    rs, col, n2d, _ = w.pattern()
+    rs, col = rs.astype(np.int32), col.astype(np.int32)
+    plain = SimWorld(scene)
+    plain.prepare(upload=False)
+    assert len(col) > len(plain.pattern()[1])
+    pos = np.concatenate([b.positions for b in scene.bodies]).astype(np.float64)
+    coords = np.zeros((len(rs) - 1, 3))
+    dyn = n2d >= 0
+    coords[n2d[dyn]] = pos[dyn]
+    for parts in (2, 5):
+        _check(rs, col, coords, parts, seed=7)
