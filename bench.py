@@ -2,6 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload block128|beam64|cube8|beam32|batched256] [--precision mixed|fp32|fp64]
+    python bench.py --workload block128 --profile-steps 3 [--against-fp64]   (profiling runs)
 
 One JSON line on rank 0.  A "step" is one PHYSIK_Step (one implicit-Euler substep:
 per-tet corotated FEM, assembly of M + dt^2 K and its rhs, block-Jacobi PCG,
@@ -93,26 +94,40 @@ def traffic_per_iteration():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """nvidia-smi clock / throttle sampling around the timed region.  The sampler starts
+    before the warm-up and waits until it is writing; mark() records the wall-clock window
+    of the timed region and summary() keeps only the samples taken inside it."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device):
+    def __init__(self, device, period_ms=20):
         self.device = device
+        self.period_ms = period_ms
         self.proc = None
         self.file = None
+        self.window = None
 
     def __enter__(self):
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "50"], stdout=self.file, stderr=subprocess.DEVNULL)
+                 "-lms", str(self.period_ms)], stdout=self.file, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return self
+        deadline = time.time() + 10.0  # wait until the sampler writes (its start-up takes a moment)
+        while time.time() < deadline and self.proc.poll() is None:
+            self.file.flush()
+            if os.path.getsize(self.file.name) > 0:
+                break
+            time.sleep(0.02)
         return self
+
+    def mark(self, t0, t1):
+        self.window = (t0, t1)
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -122,7 +137,18 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self, under_load_only=True):
+    @staticmethod
+    def _stamp(text):
+        import datetime
+
+        for fmt in ("%Y/%m/%d %H:%M:%S.%f", "%Y/%m/%d %H:%M:%S"):
+            try:
+                return datetime.datetime.strptime(text.strip(), fmt).timestamp()
+            except ValueError:
+                continue
+        return None
+
+    def summary(self):
         if self.proc is None or self.file is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
         self.file.flush()
@@ -130,24 +156,30 @@ class ClockSampler:
         with open(self.file.name) as f:
             for line in f:
                 parts = [p.strip() for p in line.split(",")]
-                if len(parts) < 9:
+                if len(parts) < 10:
                     continue
                 try:
-                    rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[4:]))
+                    rows.append((self._stamp(parts[0]), float(parts[2]), float(parts[3]), float(parts[4]), parts[5:]))
                 except ValueError:
                     continue
         os.unlink(self.file.name)
+        if self.window is not None:
+            t0, t1 = self.window
+            rows = [r for r in rows if r[0] is not None and t0 <= r[0] <= t1]
         if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = np.array([r[0] for r in rows])
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples in the timed region"],
+                    "period_ms": self.period_ms}
+        sm = np.array([r[1] for r in rows])
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
         for r in rows:
-            for n, v in zip(names, r[3][1:]):
+            for n, v in zip(names, r[4][1:]):
                 if v.lower().startswith("active"):
                     reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(r[1] for r in rows)),
-                "power_w_max": float(max(r[2] for r in rows)), "samples": len(rows), "reasons": sorted(reasons)}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(r[2] for r in rows)),
+                "power_w_max": float(max(r[3] for r in rows)), "samples": len(rows), "period_ms": self.period_ms,
+                "window_s": round(self.window[1] - self.window[0], 4) if self.window else None,
+                "reasons": sorted(reasons)}
 
 
 def pcg_bytes_per_iteration(n, nnz, precision):
@@ -284,18 +316,22 @@ def run_ours(args, scene, rank, world, local, pg):
     n, nnz = len(rs) - 1, len(col)
     stream = torch.cuda.ExternalStream(w.stream(), device=f"cuda:{local}")
 
-    for _ in range(args.warmup):
-        w.step()
-    w.synchronize()
-    pcg_kernel, pcg_blocks = w.pcg_kernel()
-
-    # --- device-resident timed region -------------------------------------
-    w.enable_timing(True)
-    barrier(pg)
-    torch.cuda.synchronize()
+    # The clock sampler starts before the warm-up (its start-up takes a moment) and keeps
+    # the samples of the timed region only.
     with ClockSampler(local) as clocks:
+        for _ in range(args.warmup):
+            w.step()
+        w.synchronize()
+        pcg_kernel, pcg_blocks = w.pcg_kernel()
+
+        # --- device-resident timed region ---------------------------------
+        w.enable_timing(True)
+        barrier(pg)
+        torch.cuda.synchronize()
+        t_begin = time.time()
         elapsed_ms = time_steps(w, stream, args.steps)
         torch.cuda.synchronize()
+        clocks.mark(t_begin, time.time())
     barrier(pg)
     elapsed_ms = max_over_ranks(pg, elapsed_ms, local)
     tm = w.timings()
@@ -358,7 +394,15 @@ def run_ours(args, scene, rank, world, local, pg):
         for _ in range(2):
             ref.step()
         k = max(2, min(args.steps, 10))
+        ref.enable_timing(True)
         ref_ms = time_steps(ref, ref_stream, k)
+        ref_tm = ref.timings()
+        ref_stats = ref.cg_stats()
+        ref_kernel, ref_blocks = ref.pcg_kernel()
+        ref_solve_ms = ref_tm["solve_ms"] / max(1, ref_tm["steps"])
+        ref_bytes = pcg_bytes_per_iteration(n, nnz, "fp64") * ref_stats["iterations"]
+        ref_achieved = ref_bytes / (ref_solve_ms / 1e3) / 1e9 if ref_solve_ms > 0 else None
+        peak64, _ = measured_peaks()
         xs, vs = w.state(f64=True)
         ref.set_state(xs, vs, f64=True)
         w.set_state(xs, vs, f64=True)
@@ -370,6 +414,12 @@ def run_ours(args, scene, rank, world, local, pg):
         verr = float(np.linalg.norm(vm - vr) / max(np.linalg.norm(vr), 1e-300))
         fp64 = {"steps_per_s": k / (ref_ms / 1e3), "ms_per_step": ref_ms / k, "steps": k,
                 "solve": "one coupled PCG over all bodies, FP64 storage and arithmetic",
+                "pcg_kernel": ref_kernel, "pcg_blocks": ref_blocks, "cg_iterations": ref_stats["iterations"],
+                "pcg_ms": ref_solve_ms, "assemble_ms": ref_tm["assemble_ms"] / max(1, ref_tm["steps"]),
+                "algorithmic_bytes_per_solve": ref_bytes,
+                "spmv_gbs": ref_achieved,
+                "frac": (ref_achieved / peak64) if ref_achieved else None,
+                "bytes_formula": "per CG iteration 76U + 4(n+1) + 48n + 264n (FP64 storage)",
                 "mixed_position_rel_err_vs_fp64_one_step": err,
                 "mixed_velocity_rel_err_vs_fp64_one_step": verr}
         del ref
@@ -421,6 +471,46 @@ def reference_sample(args, scene):
                        f"reference compiled from its sources, 1 thread ({cpu_model()})")}
 
 
+def profile_run(args, scene):
+    """A small, fixed launch sequence for profilers: build the world, step it
+    --profile-steps times (per step one tet, one row, one fill and one PCG launch), print
+    the PCG kernel, CG iterations and the step's device time split.  No autotuning, no
+    FP64 comparison, no CPU baseline.  With --against-fp64 every step of the world under
+    test instead starts from an FP64 world's state and its position / velocity
+    differences are printed."""
+    from physik_b200.world import SimWorld
+
+    w = SimWorld(scene, precision=args.precision)
+    w.set_batched(args.workload == "batched256")
+    if args.against_fp64:
+        ref = SimWorld(scene, precision="fp64")
+        for k in range(args.profile_steps):
+            x, v = ref.state(f64=True)
+            w.set_state(x, v, f64=True)
+            ref.step()
+            w.step()
+            xr, vr = ref.state(f64=True)
+            xw, vw = w.state(f64=True)
+            ex = np.linalg.norm(xw - xr) / max(np.linalg.norm(xr), 1e-300)
+            ev = np.linalg.norm(vw - vr) / max(np.linalg.norm(vr), 1e-300)
+            print(f"{args.workload} {args.precision} step {k + 1}: positions {ex:.2e}, velocities {ev:.2e} "
+                  f"(relative to FP64); CG iterations {w.cg_stats()['iterations']} "
+                  f"(FP64 {ref.cg_stats()['iterations']})")
+        return
+    w.step()  # builds and uploads the scene; timing starts with the next step
+    w.enable_timing(True)
+    for _ in range(max(0, args.profile_steps - 1)):
+        w.step()
+    w.synchronize()
+    st = w.cg_stats()
+    tm = w.timings()
+    kernel, blocks = w.pcg_kernel()
+    k = max(1, tm["steps"])
+    print(f"{args.workload} {args.precision}: {args.profile_steps} steps, PCG kernel {kernel} on {blocks} blocks, "
+          f"CG iterations {st['iterations']}, flags {st['flags']:#x}, assembly {tm['assemble_ms'] / k:.3f} ms, "
+          f"solve {tm['solve_ms'] / k:.3f} ms per step")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -432,13 +522,20 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=45.0, help="seconds of reference CPU time to sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GPU comparison")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="profiling mode: step the workload this many times, print what ran, no JSON line")
+    ap.add_argument("--against-fp64", action="store_true",
+                    help="with --profile-steps: per-step differences against an FP64 world")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
     from physik_b200 import meshes
 
-    rank, world, local, pg = dist_setup(args.gpus)
     cfg, desc = WORKLOADS[args.workload]
+    if args.profile_steps > 0:
+        profile_run(args, meshes.CONFIGS[cfg]())
+        return
+    rank, world, local, pg = dist_setup(args.gpus)
     scene = meshes.CONFIGS[cfg]()
     batched = args.workload == "batched256"
     if batched and world > 1:
@@ -482,9 +579,13 @@ def main():
                    "sample": s["sample"]}
     roof = None
     if r["achieved"] is not None:
+        traffic_src = ("profiles/pcg_dram_traffic.json: DRAM bytes per CG iteration of an ncu capture of this "
+                       "kernel on this workload, times this run's iterations" if r["traffic"] is not None else
+                       "no ncu capture of this kernel and workload committed")
         kernel = KERNEL_NAMES.get(r["pcg_kernel"], r["pcg_kernel"]) + f", {r['pcg_blocks']} blocks"
         roof = {"bound": "hbm", "achieved": r["achieved"], "peak": r["peak"], "unit": "GB/s",
-                "frac": r["achieved"] / r["peak"], "traffic": r["traffic"], "kernel": kernel,
+                "frac": r["achieved"] / r["peak"], "traffic": r["traffic"], "traffic_source": traffic_src,
+                "kernel": kernel,
                 "peak_source": f"{r['peak_kind']} hbm_gbs (MEASURED_PEAKS.json)",
                 "algorithmic_bytes_per_solve": r["bytes_per_solve"],
                 "bytes_formula": "per CG iteration 40U + 4(n+1) + 24n + 132n (FP32 storage), "

@@ -108,6 +108,16 @@ PHYSIK_B200_API int PHYSIK_GetTetMeshGlobalNodeBeginIndex(PhysikWorldHandle worl
 PHYSIK_B200_API int PHYSIK_GetTetMeshGlobalNodeCount(PhysikWorldHandle world, PhysikComponentHandle tetMesh);
 PHYSIK_B200_API int PHYSIK_GetTetMeshGlobalNodeIndex(PhysikWorldHandle world, PhysikComponentHandle tetMesh,
                                                      int localNodeIndex);
+/* PHYSIK_SetTetMeshLocalCurrentPosition / PHYSIK_GetTetMeshLocalCurrentPosition
+ * PhysiKAPI.h:236-251, PhysiKAPI.cpp:992-1053: a tet mesh's own copy of its node
+ * positions (TetMeshComponent::nodePositions).  A physics mesh's copy is the world's
+ * positions at the start of the last substep it took part in (creation positions before
+ * its first step); Set writes that copy only, not the world's node, and the next substep
+ * overwrites it.  Return 1, or 0 for an invalid world, mesh, index or NULL out-pointer. */
+PHYSIK_B200_API int PHYSIK_SetTetMeshLocalCurrentPosition(PhysikWorldHandle world, PhysikComponentHandle tetMesh,
+                                                          int localNodeIndex, float x, float y, float z);
+PHYSIK_B200_API int PHYSIK_GetTetMeshLocalCurrentPosition(PhysikWorldHandle world, PhysikComponentHandle tetMesh,
+                                                          int localNodeIndex, float* outX, float* outY, float* outZ);
 PHYSIK_B200_API void PHYSIK_SetTetMeshMaterial(PhysikWorldHandle world, PhysikComponentHandle component,
                                                const PhysikMaterialDesc* material);
 /* PhysiKAPI.h:300-334 */

@@ -114,6 +114,14 @@ PKCUDA_API int pk_system_set_state_f32(pk_system* sys, const float* x, const flo
 PKCUDA_API int pk_system_set_state_f64(pk_system* sys, const double* x, const double* v);
 PKCUDA_API int pk_system_get_state_f32(pk_system* sys, float* x, float* v);
 PKCUDA_API int pk_system_get_state_f64(pk_system* sys, double* x, double* v);
+/* Copies the node positions, on the device and in stream order, into a snapshot buffer
+ * (the host calls it at the start of every substep: TetMeshPhysicsComponent's
+ * SyncCurrentPositionsFromWorld, TetMeshPhysicsComponent.cpp:234-252, keeps the positions
+ * a component's GetLocalCurrentPosition returns, TetMeshComponent.cpp:113-122).
+ * pk_system_get_snapshot_f32 reads nodes [first_node, first_node + count) of the last
+ * snapshot (3 floats each) and waits for the stream. */
+PKCUDA_API int pk_system_snapshot_positions(pk_system* sys);
+PKCUDA_API int pk_system_get_snapshot_f32(pk_system* sys, int first_node, int count, float* x);
 
 /* Tets with world node ids and rest data already computed in the system precision
  * (FEMModel::InitializeTetRestData, BuildElasticityMatrix's lambda and mu).
@@ -233,7 +241,9 @@ PKCUDA_API int pk_pcg(int device, int precision, int n, const int* row_start, co
  * memory budget, or a host that routes all device memory through its own pool).
  * Inputs: the upper BSR (row_start[n+1], col_index, values: 9 per block in the precision's
  * scalar type) with its transposed index from pk_bsr_transpose_index (lt_start[n+1],
- * lt_row, lt_block), the rhs b (3n), the block-Jacobi inverse minv (9n); output x (3n).
+ * lt_row, lt_block; a matrix without off-diagonal blocks passes 1-element lt_row /
+ * lt_block buffers: every pointer must be non-NULL when n > 0), the rhs b (3n), the
+ * block-Jacobi inverse minv (9n); output x (3n).
  * The CG working vectors live in one fixed 8 MiB array per GPU, held by every GPU that
  * loads the library until exit: at most 32,768 rows (PK_ERR_UNSUPPORTED above that).
  * All calls on a device share that array and it keeps the last call's contents (the call
@@ -246,6 +256,15 @@ PKCUDA_API int pk_pcg_noalloc(int precision, int n, const int* row_start, const 
                               const void* minv, int max_iterations, double tolerance, void* x, pk_cg_result* out,
                               void* stream);
 PKCUDA_API const char* pk_pcg_noalloc_last_error(void);
+
+/* Device check of the bounded waits every PCG kernel's grid exchange makes: `blocks`
+ * (2..64) co-resident blocks exchange two partial sums as a group of blocks + missing
+ * members, each wait giving up after `limit` polls.  out (3 doubles per block) receives
+ * {1 if the block's exchange succeeded else 0, sum of 1..blocks, blocks}.  Returns PK_OK
+ * when every exchange completed; PK_ERR_TIMEOUT when a wait ran out (always, for
+ * missing > 0) -- the launch still ends normally and the context stays usable.  No
+ * counterpart in the reference (it checks this library's failure path). */
+PKCUDA_API int pk_exchange_wait_selftest(int device, int blocks, int missing, unsigned long long limit, double* out);
 
 /* Host-only consistency check of the ring-staged PCG kernel's tiling (no device needed):
  * builds its tiles for the upper BSR (values 9 per block, x 3 per row), replays the

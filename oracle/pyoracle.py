@@ -322,6 +322,22 @@ class Reference:
         y = np.ascontiguousarray(young, np.float64)
         self.lib.ref_set_tet_young(self.h, body, _ptr(y))
 
+    def set_fem_model(self, body, model):
+        """TetMeshPhysicsComponent::SetFemModel: 0 linear, 1 corotated, 2 NeoHookean."""
+        self.lib.ref_set_fem_model.argtypes = [_p, _i, _i]
+        self.lib.ref_set_fem_model(self.h, body, model)
+
+    def local_positions(self, body, count):
+        """TetMeshComponent::GetLocalCurrentPosition for every node of a body."""
+        out = np.zeros((count, 3))
+        self.lib.ref_get_local_positions.argtypes = [_p, _i, _p]
+        self.lib.ref_get_local_positions(self.h, body, _ptr(out))
+        return out
+
+    def set_local_position(self, body, node, p):
+        self.lib.ref_set_local_position.argtypes = [_p, _i, _i, _d, _d, _d]
+        self.lib.ref_set_local_position(self.h, body, node, *[float(c) for c in p])
+
     def add_point_connection(self, nodes, weights, target, stiffness, damping=0.0):
         """World::AddPointConnection (kept until the end of the next step)."""
         n = np.ascontiguousarray(nodes, np.int32)

@@ -100,6 +100,36 @@ __attribute__((visibility("default"))) int ref_body_tet_count(void* h, int body)
     return static_cast<int>(H(h)->bodies.at(static_cast<std::size_t>(body))->tets.size());
 }
 
+// TetMeshComponent::GetLocalCurrentPosition / SetLocalCurrentPosition of a body through the
+// reference's own C ABI (PHYSIK_GetTetMeshLocalCurrentPosition, PhysiKAPI.cpp:1021-1053, needs
+// the component handle, which this harness does not keep, so the component methods that
+// those functions call are used directly).  Positions cross as double.
+__attribute__((visibility("default"))) int ref_get_local_positions(void* h, int body, double* out)
+{
+    TetMeshPhysicsComponent* c = H(h)->bodies.at(static_cast<std::size_t>(body));
+    const int count = c->GetNodeCount();
+    for (int i = 0; i < count; ++i) {
+        const Vec3& p = c->GetLocalCurrentPosition(i);
+        out[3 * i] = p.x;
+        out[3 * i + 1] = p.y;
+        out[3 * i + 2] = p.z;
+    }
+    return count;
+}
+
+__attribute__((visibility("default"))) void ref_set_local_position(void* h, int body, int node, double x, double y,
+                                                                   double z)
+{
+    H(h)->bodies.at(static_cast<std::size_t>(body))
+        ->SetLocalCurrentPosition(node, Vec3{static_cast<Real>(x), static_cast<Real>(y), static_cast<Real>(z)});
+}
+
+// TetMeshPhysicsComponent::SetFemModel (FemModel: 0 linear, 1 corotated, 2 NeoHookean).
+__attribute__((visibility("default"))) void ref_set_fem_model(void* h, int body, int model)
+{
+    H(h)->bodies.at(static_cast<std::size_t>(body))->SetFemModel(static_cast<FemModel>(model));
+}
+
 // Per-element Young's modulus through the C++ route (Tet::youngModulus +
 // TetMeshPhysicsComponent::RebuildTetFemCache).
 __attribute__((visibility("default"))) void ref_set_tet_young(void* h, int body, const double* young)

@@ -117,6 +117,7 @@ _SIGS = {
     "PHYSIK_AddNode": (_i, [_p, _f, _f, _f]),
     "PHYSIK_SetNodeFixed": (_v, [_p, _i, _i]),
     "PHYSIK_IsNodeFixed": (_i, [_p, _i]),
+    "pk_exchange_wait_selftest": (_i, [_i, _i, _i, C.c_ulonglong, _p]),
     "PHYSIK_GenerateTetMesh": (_p, [_p, _i, _p, _i]),
     "PHYSIK_IsGeneratedTetMeshHandleValid": (_i, [_p]),
     "PHYSIK_DestroyGeneratedTetMesh": (_v, [_p]),
@@ -130,6 +131,8 @@ _SIGS = {
     "PHYSIK_GetTetMeshGlobalNodeBeginIndex": (_i, [_p, _H]),
     "PHYSIK_GetTetMeshGlobalNodeCount": (_i, [_p, _H]),
     "PHYSIK_GetTetMeshGlobalNodeIndex": (_i, [_p, _H, _i]),
+    "PHYSIK_SetTetMeshLocalCurrentPosition": (_i, [_p, _H, _i, _f, _f, _f]),
+    "PHYSIK_GetTetMeshLocalCurrentPosition": (_i, [_p, _H, _i, _p, _p, _p]),
     "PHYSIK_SetTetMeshMaterial": (_v, [_p, _H, C.POINTER(MaterialDesc)]),
     "PHYSIK_DestroyComponent": (_v, [_p, _H]),
     "PHYSIK_IsComponentHandleValid": (_i, [_p, _H]),

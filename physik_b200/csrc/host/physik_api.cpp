@@ -307,6 +307,40 @@ PHYSIK_B200_API int PHYSIK_GetTetMeshGlobalNodeIndex(PhysikWorldHandle world, Ph
     return c ? c->GetGlobalNodeIndex(localNodeIndex) : -1;
 }
 
+PHYSIK_B200_API int PHYSIK_SetTetMeshLocalCurrentPosition(PhysikWorldHandle world, PhysikComponentHandle tetMesh,
+                                                          int localNodeIndex, float x, float y, float z)
+{
+    World* w = AsWorld(world);
+    TetMeshComponent* c = AsTetMesh(w, tetMesh);
+    if (!c || localNodeIndex < 0 || localNodeIndex >= c->GetNodeCount()) return 0;
+    return Guard(
+        [&]() -> int {
+            if (auto* p = dynamic_cast<TetMeshPhysicsComponent*>(c)) w->RefreshLocalPositions(*p);
+            c->SetLocalCurrentPosition(localNodeIndex, Vec3{x, y, z});
+            return 1;
+        },
+        0);
+}
+
+PHYSIK_B200_API int PHYSIK_GetTetMeshLocalCurrentPosition(PhysikWorldHandle world, PhysikComponentHandle tetMesh,
+                                                          int localNodeIndex, float* outX, float* outY, float* outZ)
+{
+    World* w = AsWorld(world);
+    if (!w || !outX || !outY || !outZ) return 0;
+    TetMeshComponent* c = AsTetMesh(w, tetMesh);
+    if (!c || localNodeIndex < 0 || localNodeIndex >= c->GetNodeCount()) return 0;
+    return Guard(
+        [&]() -> int {
+            if (auto* p = dynamic_cast<TetMeshPhysicsComponent*>(c)) w->RefreshLocalPositions(*p);
+            const Vec3& v = c->GetLocalCurrentPosition(localNodeIndex);
+            *outX = v.x;
+            *outY = v.y;
+            *outZ = v.z;
+            return 1;
+        },
+        0);
+}
+
 PHYSIK_B200_API void PHYSIK_SetTetMeshMaterial(PhysikWorldHandle world, PhysikComponentHandle component,
                                                const PhysikMaterialDesc* material)
 {

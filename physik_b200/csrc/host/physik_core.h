@@ -357,6 +357,12 @@ public:
 
     // Bumped whenever rest data, material or tet activity changes.
     std::uint64_t version = 1;
+    // nodePositions is the world's positions at the start of the last substep in which
+    // this component was active (SyncCurrentPositionsFromWorld).  The device keeps that
+    // snapshot; the host copy is refreshed on access: snapshotWanted is the world's
+    // snapshot generation this component's copy should show, snapshotLoaded the one it
+    // holds.
+    std::uint64_t snapshotWanted = 0, snapshotLoaded = 0;
 };
 
 // ------------------------------------------------------------------ world
@@ -486,6 +492,9 @@ public:
     const std::vector<int>* GetSceneNodeToDyn() const;
     const std::vector<double>* GetSceneMass() const;
     unsigned GetLastStepFlags() const;
+    // Brings a component's nodePositions up to the snapshot of the last substep it took part
+    // in (TetMeshPhysicsComponent::SyncCurrentPositionsFromWorld, done lazily).
+    void RefreshLocalPositions(TetMeshPhysicsComponent& component) const;
     void MarkTopologyDirty() { ++topologyVersion; }
     std::uint64_t GetTopologyVersion() const { return topologyVersion; }
 
@@ -498,6 +507,7 @@ private:
     void RunSubstep(float dt);
     void CollectContributions(float dt);
     void EnsureScene(bool upload);
+    void FlushLocalPositionSnapshots();  // host copies of every stale component snapshot
     bool SyncConnections();
     void MarkSubstepConnectionBegin() { firstSubstepConnectionIndex = transientConnections.size(); }
     void ClearSubstepConnections();
@@ -535,6 +545,7 @@ private:
     mutable ConjugateGradientResult lastConjugateGradientResult;
     mutable unsigned lastFlags = 0;
     mutable bool statsPending = false;
+    std::uint64_t snapshotGeneration = 0;  // substeps whose start positions the device snapshot held
 };
 
 }  // namespace PhysiK

@@ -942,6 +942,7 @@ void World::EnsureScene(bool upload)
 {
     const std::vector<const TetMeshPhysicsComponent*>& fem = solverData.GetFemBodies();
     if (!scene || scene->precision != precision || scene->device != device) {
+        FlushLocalPositionSnapshots();
         EnsureHostState();
         scene = std::make_unique<DeviceScene>();
         scene->precision = precision;
@@ -985,6 +986,7 @@ void World::EnsureScene(bool upload)
     }
     const bool patternChanged = SyncConnections();
     if (upload && !scene->uploaded) {
+        FlushLocalPositionSnapshots();  // the upload drops the device snapshot
         EnsureHostState();
         if (!scene->sys) Check(pk_system_create(device, static_cast<int>(precision), &scene->sys), "pk_system_create");
         UploadScene(*scene, positions, velocities);
@@ -1204,6 +1206,30 @@ bool World::GetBodyConjugateGradientStats(const Component* body, int& iterations
     return false;
 }
 
+void World::FlushLocalPositionSnapshots()
+{
+    for (auto& e : orderedComponents) {
+        auto* c = dynamic_cast<TetMeshPhysicsComponent*>(e.second);
+        if (c && c->snapshotLoaded != c->snapshotWanted) RefreshLocalPositions(*c);
+    }
+}
+
+void World::RefreshLocalPositions(TetMeshPhysicsComponent& c) const
+{
+    if (c.snapshotLoaded == c.snapshotWanted) return;
+    const int count = c.globalNodeCount;
+    if (!scene || !scene->sys || c.globalNodeBeginIndex < 0 || count <= 0) {
+        c.snapshotLoaded = c.snapshotWanted;
+        return;
+    }
+    std::vector<float> x(3 * static_cast<std::size_t>(count));
+    Check(pk_system_get_snapshot_f32(scene->sys, c.globalNodeBeginIndex, count, x.data()), "get_snapshot");
+    c.nodePositions.resize(static_cast<std::size_t>(count));
+    for (int i = 0; i < count; ++i)
+        c.nodePositions[static_cast<std::size_t>(i)] = Vec3{x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+    c.snapshotLoaded = c.snapshotWanted;
+}
+
 int World::PrepareScene(bool upload)
 {
     CollectContributions(0.0f);
@@ -1234,6 +1260,21 @@ void World::RunSubstep(float dt)
         }
         Check(pk_system_set_state_f32(scene->sys, x.data(), v.data()), "set_state");
         deviceStale = false;
+    }
+    // Every active physics component syncs its local positions from the world at the start
+    // of the substep (TetMeshPhysicsComponent::UpdateSystem, TetMeshPhysicsComponent.cpp:293-300).
+    // The device copies the positions aside; a component's host copy is read from there
+    // on access.  A component that sits this substep out keeps its older snapshot, so it
+    // is fetched before the device copy is overwritten.
+    for (auto& e : orderedComponents) {
+        auto* c = dynamic_cast<TetMeshPhysicsComponent*>(e.second);
+        if (c && !c->active && c->snapshotLoaded != c->snapshotWanted) RefreshLocalPositions(*c);
+    }
+    Check(pk_system_snapshot_positions(scene->sys), "snapshot_positions");
+    ++snapshotGeneration;
+    for (auto& e : orderedComponents) {
+        auto* c = dynamic_cast<TetMeshPhysicsComponent*>(e.second);
+        if (c && c->active) c->snapshotWanted = snapshotGeneration;
     }
     if (scene->dynCount == 0) {
         // No dynamic node: PrecomputeImplicitSolve fails and nothing moves.

@@ -404,9 +404,11 @@ __device__ __forceinline__ void count_publish(ExSlot* slots, unsigned* counter, 
     }
 }
 
+// `limit`: polls before the wait gives up (the wait self-test passes a small one).
 template <class Acc, int N>
 __device__ bool count_finish(ExSlot* slots, unsigned* counter, int first, int size, GridSync* sync, unsigned gen,
-                             Acc (&v)[N], int& bad, Acc* sh, int* shi)
+                             Acc (&v)[N], int& bad, Acc* sh, int* shi,
+                             unsigned long long limit = kBarrierSpinLimit)
 {
     const int G = gridDim.x, tid = threadIdx.x, lane = tid & 31;
     if (size <= 1) return !*(volatile int*)&sync->err;
@@ -416,7 +418,7 @@ __device__ bool count_finish(ExSlot* slots, unsigned* counter, int first, int si
         int fail = 0;
         unsigned long long spins = 0;
         while ((int)(ld_acquire(counter) - target) < 0) {
-            if (++spins > kBarrierSpinLimit) {
+            if (++spins > limit) {
                 atomicExch(&sync->err, 1);
                 fail = 1;
                 break;
@@ -461,10 +463,11 @@ __device__ bool count_finish(ExSlot* slots, unsigned* counter, int first, int si
 
 template <class Acc, int N>
 __device__ __forceinline__ bool count_exchange(ExSlot* slots, unsigned* counter, int first, int size, GridSync* sync,
-                                               unsigned gen, Acc (&v)[N], int& bad, Acc* sh, int* shi)
+                                               unsigned gen, Acc (&v)[N], int& bad, Acc* sh, int* shi,
+                                               unsigned long long limit = kBarrierSpinLimit)
 {
     count_publish<Acc, N>(slots, counter, size, gen, v, bad, sh, shi);
-    return count_finish<Acc, N>(slots, counter, first, size, sync, gen, v, bad, sh, shi);
+    return count_finish<Acc, N>(slots, counter, first, size, sync, gen, v, bad, sh, shi, limit);
 }
 
 // The whole grid as one group (slots: two buffers of gridDim.x).

@@ -282,18 +282,24 @@ struct BatchPcgArgs {
 // ------------------------------------------------------------------ part-resident PCG
 // The part-resident ("slab") PCG kernel (pk_pcg_slab.cu; layout in pk_slab_plan.h): one
 // block per part, FP32 storage.  Shared memory: the window's search directions
-// (kSlabWinCap x 3 floats), the ring of kSlabStages tile stages, the part's tile table.
-constexpr int kSlabGroups = 3;
+// (kSlabWinCap x 3 floats), the ring of kSlabStages tile stages, the part's tile table,
+// and for the symmetric stream form the consumer groups' transposed-product rings.
 constexpr int kSlabGroupWarps = 4;
 constexpr int kSlabConsumerWarps = kSlabGroups * kSlabGroupWarps;
 constexpr int kSlabThreads = 32 * (kSlabConsumerWarps + 1);  // + one producer warp
 constexpr size_t kSlabWinBytes = 12 * size_t(kSlabWinCap);
 constexpr size_t kSlabRingOffset = kSlabWinBytes;
 constexpr size_t kSlabTableOffset = kSlabRingOffset + size_t(kSlabStages) * kSlabStageBytes;
-constexpr size_t kSlabSmemBytes = kSlabTableOffset + 16 * size_t(kSlabMaxTiles);
+constexpr size_t kSlabFullSmemBytes = kSlabTableOffset + 16 * size_t(kSlabMaxTiles);
+constexpr size_t kSlabSymTableOffset = kSlabRingOffset + size_t(kSlabStages) * kSymStageBytes;
+constexpr size_t kSlabSymTpOffset = kSlabSymTableOffset + 16 * size_t(kSlabMaxTiles);
+constexpr size_t kSlabSymSmemBytes = kSlabSymTpOffset + 12 * size_t(kSlabGroups) * kSymRingSlots;
+constexpr size_t kSlabSmemBytes = kSlabFullSmemBytes > kSlabSymSmemBytes ? kSlabFullSmemBytes : kSlabSymSmemBytes;
 static_assert(kSlabStages % kSlabGroups == 0, "a stage must always return to the same consumer group");
-static_assert(kSlabWinBytes % 128 == 0 && kSlabStageBytes % 128 == 0, "stages must stay 128-byte aligned");
+static_assert(kSlabWinBytes % 128 == 0 && kSlabStageBytes % 128 == 0 && kSymStageBytes % 128 == 0,
+              "stages must stay 128-byte aligned");
 static_assert(kSlabSmemBytes + 2048 <= 232448, "dynamic + static shared memory must fit one block per SM");
+static_assert(kSymRows == 2 * kSlabRows, "a symmetric tile is two passes of the group's rows");
 static_assert(kSlabRows * kSlabLanesPerRow == 32 * kSlabGroupWarps, "one tile row per lane group");
 static_assert(kSlabRowThreads == 32 * kSlabConsumerWarps, "the consumer warps own the rows");
 static_assert(kSlabGroups * kSlabRowsPerThread * 16 <= 512, "row records must fit tensor memory");

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <string>
 
@@ -36,7 +37,9 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) unsigned char g_pcg_scratch[kPcgScratchBytes];
 
 // Device address of g_pcg_scratch per device (host code may not use the symbol itself).
-void* g_scratch_ptr[kMaxDevices] = {};
+// Atomic slots: two host threads making their first call on one device at once both look
+// the address up and store the same value.
+std::atomic<void*> g_scratch_ptr[kMaxDevices] = {};
 
 thread_local std::string g_noalloc_error;
 
@@ -143,21 +146,23 @@ PKCUDA_API int pk_pcg_noalloc(int precision, int n, const int* row_start, const 
         out->converged = 1;
         return PK_OK;
     }
-    if (!row_start || !col_index || !values || !lt_start || !b || !minv || !x)
+    // Every index array is read by the kernel whenever n > 0 (a matrix without
+    // off-diagonal blocks still passes 1-element lt_row / lt_block buffers).
+    if (!row_start || !col_index || !values || !lt_start || !lt_row || !lt_block || !b || !minv || !x)
         return noalloc_fail(PK_ERR_ARG, "pk_pcg_noalloc: NULL device pointer");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices)
         return noalloc_fail(PK_ERR_NO_DEVICE, "pk_pcg_noalloc: no current CUDA device");
-    if (!g_scratch_ptr[dev]) {
-        void* ptr = nullptr;
-        e = cudaGetSymbolAddress(&ptr, g_pcg_scratch);
-        if (e != cudaSuccess || !ptr)
+    void* slot = g_scratch_ptr[dev].load(std::memory_order_acquire);
+    if (!slot) {
+        e = cudaGetSymbolAddress(&slot, g_pcg_scratch);
+        if (e != cudaSuccess || !slot)
             return noalloc_fail(PK_ERR_CUDA, std::string("pk_pcg_noalloc: cudaGetSymbolAddress: ") +
                                                  cudaGetErrorString(e));
-        g_scratch_ptr[dev] = ptr;
+        g_scratch_ptr[dev].store(slot, std::memory_order_release);
     }
-    unsigned char* scratch = static_cast<unsigned char*>(g_scratch_ptr[dev]);
+    unsigned char* scratch = static_cast<unsigned char*>(slot);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (precision == PK_PREC_FP32)
         return run<float, float>(n, row_start, col_index, values, lt_start, lt_row, lt_block, b, minv,

@@ -51,7 +51,34 @@ constexpr int kSlabPartInts = 8;
 constexpr unsigned kSlabNoPos = 0xffffffffu;   // a padding entry
 constexpr unsigned kSlabLowerBit = 0x80000000u; // the entry is the transpose of the block
 
+// The symmetric ("sym") form of the stream streams each in-part block once.  Every part is
+// cut into kSlabGroups sub-parts, one per consumer group, each ordered as a sweep along its
+// longest extent.  Inside a sub-part a coupled pair (r, c) with r before c is stored once,
+// in row r, as a "transposing" entry: its block B adds B d_c to q_r and B^T d_r to q_c.
+// The B^T d_r products go to the group's ring of kSymRingSlots 3-float slots in shared
+// memory, at slots fixed by the layout: row c's slots are [lbase(c), lbase(c + 1)) (mod
+// the ring), one per earlier coupled row of its sub-part, in sweep order, and row c's q is
+// its own entries' sum plus its slots' sum, in that fixed order.  Pairs across sub-parts or
+// parts are stored in both rows, as in the full form.  A tile is
+//     [kSymHeaderBytes: u16 row offsets (rows + 1), u16 ring bases (rows + 1)]
+//     [entries x 9 floats] [entries x u16 window column] [entries x u16 ring slot]
+// (slot kSymNoSlot: a plain entry).  A group handles only its own sub-part's tiles,
+// strictly in order, so its slots need no synchronisation beyond its own barriers; the
+// layout checks that the slots alive at any time (the current tile's rows and every later
+// row some processed row already wrote to) fit the ring, else it does not apply.
+constexpr int kSlabGroups = 3;          // consumer groups (one sub-part each)
+constexpr int kSymRows = 64;            // rows per tile (two passes of 32)
+constexpr int kSymHeaderBytes = 272;    // 2 x u16[kSymRows + 1], padded to 16 bytes
+constexpr int kSymEntryBytes = 40;      // 9 floats + u16 column + u16 slot
+constexpr int kSymStageBytes = 17408;   // 128-byte multiple
+constexpr int kSymCapE = (kSymStageBytes - kSymHeaderBytes) / kSymEntryBytes / 8 * 8;
+constexpr int kSymRingSlots = 1024;     // per group, a power of two
+constexpr unsigned kSymNoSlot = 0xffffu;
+
 static_assert(kSlabHeaderBytes + kSlabCapE * kSlabEntryBytes <= kSlabStageBytes, "stage too small");
+static_assert(kSymHeaderBytes >= 4 * (kSymRows + 1) && kSymHeaderBytes % 16 == 0, "sym header");
+static_assert(kSymHeaderBytes + kSymCapE * kSymEntryBytes <= kSymStageBytes, "sym stage too small");
+static_assert((kSymRingSlots & (kSymRingSlots - 1)) == 0 && kSymRingSlots <= 65535, "ring slots");
 static_assert(kSlabCapE % 8 == 0, "entry cap must keep 16-byte alignment");
 static_assert(kSlabHeaderBytes % 16 == 0, "blocks must start on a 16-byte boundary");
 static_assert(2 * (kSlabRows + 1) <= kSlabHeaderBytes, "header too small");
@@ -69,14 +96,20 @@ struct SlabPlan {
     std::vector<int> part_body;  // body (segment) of each part; 0 for the coupled solve
     std::vector<int> launch_start;  // parts [launch_start[l], launch_start[l + 1]) form launch l
     int max_window = 0, max_tiles = 0, max_rows = 0;
+    bool sym = false;  // the symmetric form (tiles and headers as described above)
 };
+
+// Which stream form a layout build uses: the full symmetric rows, the symmetric form, or
+// the symmetric form where it applies and the full rows otherwise.
+enum SlabForm { kSlabFull = 0, kSlabSym = 1, kSlabAuto = 2 };
 
 // Builds the layout for `parts` parts of the upper-stored pattern (row_start, col) with
 // its transpose index (lt_start, lt_row, lt_block).  coords: 3 doubles per row (NULL:
 // contiguous parts of the dynamic-row order).  Returns "" on success, otherwise why the
 // layout does not apply (a window or a row too large); `out` is then unusable.
 std::string build_slab_plan(int n, const int* row_start, const int* col, const int* lt_start, const int* lt_row,
-                            const int* lt_block, const double* coords, int parts, SlabPlan& out);
+                            const int* lt_block, const double* coords, int parts, SlabPlan& out,
+                            int form = kSlabAuto);
 
 // The layout for per-body solves: the rows split into bodies (segments
 // [seg[b], seg[b + 1]), no block coupling two bodies), every body cut by coordinate
@@ -85,7 +118,7 @@ std::string build_slab_plan(int n, const int* row_start, const int* col, const i
 // max_blocks parts.  Returns "" on success, otherwise why the layout does not apply.
 std::string build_slab_plan_batched(int n, const int* row_start, const int* col, const int* lt_start,
                                     const int* lt_row, const int* lt_block, const double* coords, const int* seg,
-                                    int nseg, int max_blocks, SlabPlan& out);
+                                    int nseg, int max_blocks, SlabPlan& out, int form = kSlabAuto);
 
 // y = A x through the plan exactly as the kernel reads it (fill, then tile decoding with
 // the kernel's clamps), in double: the CPU self-check of a plan.

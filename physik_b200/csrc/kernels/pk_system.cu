@@ -256,8 +256,9 @@ struct pk_system {
     cudaGraphExec_t graph_exec = nullptr;
     pk_step_params graph_params{};
     int graph_kernels = 0;
-    // nodes
-    DevBuf x, v, mass, node_to_dyn;
+    // nodes; snap_x: positions at the start of the last substep (pk_system_snapshot_positions)
+    DevBuf x, v, mass, node_to_dyn, snap_x;
+    bool have_snapshot = false;
     // tets
     DevBuf tet_nodes, tet_enabled, dm_inv, tet_params, tet_rec;
     // rows
@@ -1203,6 +1204,7 @@ PKCUDA_API int pk_system_set_nodes(pk_system* s, int node_count, const int* node
     if (!s || node_count < 0 || (node_count > 0 && (!node_to_dyn || !mass))) return fail(PK_ERR_ARG, "set_nodes");
     PK_CHECK(cudaSetDevice(s->device));
     s->node_count = node_count;
+    s->have_snapshot = false;
     s->h_node_to_dyn.assign(node_to_dyn, node_to_dyn + node_count);
     s->h_mass.assign(mass, mass + node_count);
     int rc = upload_raw<int>(s->node_to_dyn, node_to_dyn, node_count, s->stream);
@@ -1271,6 +1273,38 @@ PKCUDA_API int pk_system_get_state_f32(pk_system* s, float* x, float* v)
     }
     if (x) PK_CHECK(cudaMemcpyAsync(x, s->x.p, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
     if (v) PK_CHECK(cudaMemcpyAsync(v, s->v.p, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_snapshot_positions(pk_system* s)
+{
+    if (!s || !s->have_nodes) return fail(PK_ERR_STATE, "snapshot before set_nodes");
+    PK_CHECK(cudaSetDevice(s->device));
+    const size_t bytes = 3 * static_cast<size_t>(s->node_count) * s->rsize();
+    PK_CHECK(s->snap_x.ensure(bytes));
+    if (bytes) PK_CHECK(cudaMemcpyAsync(s->snap_x.p, s->x.p, bytes, cudaMemcpyDeviceToDevice, s->stream));
+    s->have_snapshot = true;
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_get_snapshot_f32(pk_system* s, int first_node, int count, float* x)
+{
+    if (!s || !s->have_snapshot) return fail(PK_ERR_STATE, "get_snapshot before a snapshot");
+    if (first_node < 0 || count < 0 || first_node > s->node_count - count || (count > 0 && !x))
+        return fail(PK_ERR_ARG, "get_snapshot: node range");
+    if (count == 0) return PK_OK;
+    PK_CHECK(cudaSetDevice(s->device));
+    const size_t n = 3 * static_cast<size_t>(count), off = 3 * static_cast<size_t>(first_node);
+    if (s->precision == PK_PREC_FP64) {
+        std::vector<double> t(n);
+        PK_CHECK(cudaMemcpyAsync(t.data(), s->snap_x.as<double>() + off, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                 s->stream));
+        PK_CHECK(cudaStreamSynchronize(s->stream));
+        for (size_t i = 0; i < n; ++i) x[i] = static_cast<float>(t[i]);
+        return PK_OK;
+    }
+    PK_CHECK(cudaMemcpyAsync(x, s->snap_x.as<float>() + off, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
     PK_CHECK(cudaStreamSynchronize(s->stream));
     return PK_OK;
 }

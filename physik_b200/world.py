@@ -95,6 +95,24 @@ class SimWorld:
         if fn(self.h, _ptr(x), _ptr(v), self.node_count) < 0:
             raise PhysikError("SetNodeStates failed: " + self.error())
 
+    def local_positions(self, body: int):
+        """PHYSIK_GetTetMeshLocalCurrentPosition for every node of a mesh: the mesh's own
+        copy of its positions (float32, (count, 3))."""
+        comp = self.components[body]
+        count = self.X.PHYSIK_GetTetMeshNodeCount(self.h, comp)
+        out = np.zeros((max(count, 0), 3), np.float32)
+        fx, fy, fz = C.c_float(), C.c_float(), C.c_float()
+        for i in range(count):
+            if not self.X.PHYSIK_GetTetMeshLocalCurrentPosition(self.h, comp, i, C.byref(fx), C.byref(fy),
+                                                                C.byref(fz)):
+                raise PhysikError("GetTetMeshLocalCurrentPosition failed: " + self.error())
+            out[i] = (fx.value, fy.value, fz.value)
+        return out
+
+    def set_local_position(self, body: int, node: int, p) -> int:
+        return int(self.X.PHYSIK_SetTetMeshLocalCurrentPosition(self.h, self.components[body], int(node),
+                                                                *[float(c) for c in p]))
+
     def add_point_connection(self, nodes, weights, target, stiffness: float, damping: float = 0.0):
         """PHYSIK_AddPointConnection: a spring from sum_i weights[i] x(nodes[i]) to `target`,
         kept until the end of the next step."""

@@ -59,6 +59,19 @@ def test_pattern_mass_mapping_beam32_per_tet_young():
 
 
 @needs_ref
+def test_pattern_mass_mapping_block128():
+    """The 128x64x64 block of the roofline workload (545,025 nodes, 3.1 M tets, 4.2 M
+    upper blocks): the whole host scene against the reference's, bit for bit."""
+    _compare_with_reference(meshes.config4())
+
+
+@needs_ref
+def test_pattern_mass_mapping_batched256():
+    """The 256 uneven bodies of the batched workload, one world (bodies never couple)."""
+    _compare_with_reference(meshes.config3())
+
+
+@needs_ref
 def test_pattern_mass_mapping_two_bodies():
     s = meshes.small_box(2, 2, 2)
     s.bodies += meshes.small_box(3, 2, 2, young=5e4, seed=11).bodies

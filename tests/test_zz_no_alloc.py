@@ -7,8 +7,10 @@ They pass device buffers for the matrix, its transposed index, the rhs, the
 preconditioner and the solution; the solver's working vectors live in a fixed array
 inside the library.  This test calls it through the C ABI twice in a row (the second
 call reuses the array the first one left behind) and compares both results with
-pk_pcg on the same system, with the tolerances of the other PCG tests.  It also
-checks that a system larger than the fixed array is refused without touching the GPU.
+pk_pcg on the same system, with the tolerances of the other PCG tests.  At the size
+limit itself (32,768 rows, where the FP64 working vectors fill most of the array) it
+also checks both calls against the FP64 oracle's PCG.  It also checks that a system
+larger than the fixed array is refused without touching the GPU.
 
 This file is collected last so that a failure here cannot hide the other tests.
 """
@@ -52,6 +54,30 @@ def random_spd_bsr(n, density, seed):
         a = rng.normal(size=(3, 3))
         vals[rs[r]] = (a @ a.T + (rowsum[r] + 4.0) * np.eye(3)).T
     minv = np.stack([np.linalg.inv(vals[rs[r]].T).T for r in range(n)])
+    b = rng.normal(size=(n, 3))
+    return rs, col, vals, minv, b
+
+
+def banded_spd_bsr(n, seed):
+    """A sparse SPD system of n rows built without per-row Python loops: every row couples
+    to rows r+1, r+7 and r+61 (when they exist), diagonal blocks dominant."""
+    rng = np.random.default_rng(seed)
+    rows, cols = [np.arange(n)], [np.arange(n)]
+    for off in (1, 7, 61):
+        r = np.arange(n - off)
+        rows.append(r)
+        cols.append(r + off)
+    rs, col = po.oracle_build_pattern(n, np.concatenate(rows), np.concatenate(cols))
+    row_of = np.repeat(np.arange(n), np.diff(rs))
+    vals = rng.normal(size=(len(col), 3, 3))
+    off_sum = np.abs(vals).sum(axis=(1, 2))
+    off_sum[col == row_of] = 0.0
+    rowsum = np.bincount(row_of, off_sum, n) + np.bincount(col, off_sum, n)
+    diag = rs[:-1]
+    a = rng.normal(size=(n, 3, 3))
+    d = a @ np.transpose(a, (0, 2, 1)) + (rowsum + 4.0)[:, None, None] * np.eye(3)
+    vals[diag] = np.transpose(d, (0, 2, 1))
+    minv = np.transpose(np.linalg.inv(d), (0, 2, 1))
     b = rng.normal(size=(n, 3))
     return rs, col, vals, minv, b
 
@@ -106,6 +132,21 @@ def test_noalloc_matches_allocating_pcg_twice(prec, n, max_it):
         assert abs(res.iterations - r_ref.iterations) <= (1 if prec == L.PK_PREC_FP64 else 2)
         assert res.converged == r_ref.converged
         assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) < tol
+
+
+@pytest.mark.parametrize("prec", [L.PK_PREC_MIXED, L.PK_PREC_FP64])
+def test_noalloc_at_the_row_limit_matches_allocating_pcg_and_oracle(prec):
+    rs, col, vals, minv, b = banded_spd_bsr(MAX_ROWS, seed=7)
+    max_it, tol_cg = 10, 1e-12  # stops at the iteration cap (the oracle needs 12 to converge)
+    x_ref, r_ref = allocating_pcg(prec, rs, col, vals, b, minv, max_it, tol_cg)
+    x_ora, s_ora = po.oracle_pcg(rs, col, vals, b, minv, max_it, tol_cg, "f64")
+    tol = 1e-10 if prec == L.PK_PREC_FP64 else 5e-5
+    for _ in range(2):
+        x, res = noalloc_pcg(prec, rs, col, vals, b, minv, max_it, tol_cg)
+        assert res.have_solution == 1
+        assert res.iterations == r_ref.iterations == s_ora["iterations"] == max_it
+        assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) < tol
+        assert np.linalg.norm(x - x_ora) / np.linalg.norm(x_ora) < tol
 
 
 def test_noalloc_rejects_sizes_beyond_the_fixed_array():
