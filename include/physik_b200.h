@@ -223,6 +223,9 @@ PHYSIK_B200_API int PHYSIK_B200_Autotune(PhysikWorldHandle world, int repeats, d
  * TMA-staged, 2 unstaged, 3 part-resident, 4 batched) or -1; blocks (may be NULL)
  * receives the blocks it ran on. */
 PHYSIK_B200_API int PHYSIK_B200_GetPcgKernel(PhysikWorldHandle world, int* blocks);
+/* The part-resident kernel's stream form in the last step's solve (pk_system_slab_form:
+ * 0 full rows, 1 symmetric form, -1 another kernel).  No counterpart in the reference. */
+PHYSIK_B200_API int PHYSIK_B200_GetPcgStreamForm(PhysikWorldHandle world);
 /* FP64 outer true-residual refinement of the implicit solve for FP32 and mixed precision
  * (no counterpart in the reference; see pk_system_set_refinement): up to `passes`
  * correction solves (0..16, 0 = off, the default) within the step's iteration budget,

@@ -213,6 +213,10 @@ PKCUDA_API int pk_system_set_refinement(pk_system* sys, int passes);
  * (batched solve); -1 before the first solve (or a negative PK_ERR_*).
  * blocks (may be NULL) receives the blocks it ran on. */
 PKCUDA_API int pk_system_pcg_kernel(pk_system* sys, int* blocks);
+/* Stream form of the part-resident kernel's layout in the last solve: 0 full symmetric
+ * rows, 1 the symmetric form (each in-sub-part block streamed once); -1 when the last
+ * solve did not run on the part-resident kernel. */
+PKCUDA_API int pk_system_slab_form(pk_system* sys);
 /* Captures each step into a CUDA graph (relaxed capture mode) and replays it: the first
  * step after enabling runs normally (allocations, uploads), the next one with the same
  * parameters is captured, later ones launch the graph.  Any topology, segment, grid or
@@ -278,22 +282,27 @@ PKCUDA_API int pk_ring_tiling_selfcheck(int precision, int n, const int* row_sta
 
 /* CPU self-check of the part-resident PCG kernel's layout: builds it for the upper BSR
  * (parts parts, cut by coords -- 3 doubles per row -- or, when coords is NULL, as
- * contiguous row ranges), fills the block stream as the device fill does (float
- * storage) and evaluates y = A x by decoding the tiles exactly as the kernel's lanes read
- * them.  info (may be NULL) receives {parts, largest window, most tiles in a part, stream
- * KiB}.  PK_ERR_UNSUPPORTED when the layout does not apply (a window or a row too large).
- * No counterpart in the reference (it checks this library's own layout). */
+ * contiguous row ranges) in stream form `form` (0 full symmetric rows, 1 the symmetric
+ * form that streams each in-part block once, 2 the symmetric form where it applies),
+ * fills the block stream as the device fill does (float storage) and evaluates y = A x by
+ * decoding the tiles exactly as the kernel's lanes read them (for the symmetric form
+ * with its per-group rings of transposed products, wrap-around included).  info (may be
+ * NULL) receives {parts, largest window, most tiles in a part, stream KiB, 1 if the
+ * symmetric form was built}.  PK_ERR_UNSUPPORTED when the layout does not apply (a
+ * window or a row too large, or for the symmetric form a ring too small).  No
+ * counterpart in the reference (it checks this library's own layout). */
 PKCUDA_API int pk_slab_plan_selfcheck(int n, const int* row_start, const int* col_index, const double* values,
-                                      const double* x, const double* coords, int parts, double* y, int* info);
+                                      const double* x, const double* coords, int parts, int form, double* y,
+                                      int* info);
 
 /* The same for the per-body (batched) layout: rows in segments (bodies), every body cut
  * into parts that fit, bodies packed into launches of at most max_blocks parts; also
  * checks that every part's group is its body's consecutive parts within one launch.
  * info (may be NULL) receives {parts, largest window, most tiles in a part, stream KiB,
- * launches}. */
+ * launches, 1 if the symmetric form was built}. */
 PKCUDA_API int pk_slab_plan_batched_selfcheck(int n, const int* row_start, const int* col_index, const double* values,
                                               const double* x, const double* coords, const int* segment_row_start,
-                                              int segment_count, int max_blocks, double* y, int* info);
+                                              int segment_count, int max_blocks, int form, double* y, int* info);
 
 /* Builds the transposed index of an upper BSR: for row r the blocks (c, r), c < r.
  * lt_start[n+1]; lt_row / lt_block sized nnz - n.  Host-only, no device needed. */

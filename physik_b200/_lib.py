@@ -91,8 +91,8 @@ _SIGS = {
     "pk_system_set_batched": (_i, [_p, _i]),
     "pk_system_segment_stats": (_i, [_p, _i, _p, _p, _p, _p]),
     "pk_ring_tiling_selfcheck": (_i, [_i, _i, _p, _p, _p, _p, _p, _p, _p]),
-    "pk_slab_plan_selfcheck": (_i, [_i, _p, _p, _p, _p, _p, _i, _p, _p]),
-    "pk_slab_plan_batched_selfcheck": (_i, [_i, _p, _p, _p, _p, _p, _p, _i, _i, _p, _p]),
+    "pk_slab_plan_selfcheck": (_i, [_i, _p, _p, _p, _p, _p, _i, _i, _p, _p]),
+    "pk_slab_plan_batched_selfcheck": (_i, [_i, _p, _p, _p, _p, _p, _p, _i, _i, _i, _p, _p]),
     "pk_system_set_graph": (_i, [_p, _i]),
     "pk_system_adjoint_step": (_i, [_p, C.POINTER(PkStepParams), _p, _p, _p, _p, _p]),
     "pk_system_autotune": (_i, [_p, C.POINTER(PkStepParams), _i, _p, _p]),
@@ -174,6 +174,7 @@ _SIGS = {
     "PHYSIK_B200_GetTetCount": (_i, [_p]),
     "PHYSIK_B200_Autotune": (_i, [_p, _i, _p]),
     "PHYSIK_B200_GetPcgKernel": (_i, [_p, _p]),
+    "PHYSIK_B200_GetPcgStreamForm": (_i, [_p]),
     "PHYSIK_B200_SetRefinement": (_i, [_p, _i]),
     "PHYSIK_B200_GetBodyConjugateGradientStats": (_i, [_p, _H, _p, _p, _p, _p]),
     "PHYSIK_B200_GetStream": (_p, [_p]),

@@ -674,6 +674,13 @@ PHYSIK_B200_API int PHYSIK_B200_GetPcgKernel(PhysikWorldHandle world, int* block
     return Guard([&] { return w->GetPcgKernel(blocks); }, -1);
 }
 
+PHYSIK_B200_API int PHYSIK_B200_GetPcgStreamForm(PhysikWorldHandle world)
+{
+    World* w = AsWorld(world);
+    if (!w) return -1;
+    return Guard([&] { return w->GetPcgStreamForm(); }, -1);
+}
+
 PHYSIK_B200_API int PHYSIK_B200_SetRefinement(PhysikWorldHandle world, int passes)
 {
     World* w = AsWorld(world);

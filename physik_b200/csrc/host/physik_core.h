@@ -445,6 +445,8 @@ public:
     int Autotune(int repeats, double* bestMs);
     // PCG kernel of the last solve (see pk_system_pcg_kernel) and its block count.
     int GetPcgKernel(int* blocks) const;
+    // Stream form of the part-resident kernel in the last solve (pk_system_slab_form).
+    int GetPcgStreamForm() const;
 
     // Device precision (extension).  Changing it rebuilds the device scene.
     void SetPrecision(Precision p);

@@ -1164,6 +1164,12 @@ int World::GetPcgKernel(int* blocks) const
     return pk_system_pcg_kernel(scene->sys, blocks);
 }
 
+int World::GetPcgStreamForm() const
+{
+    if (!scene || !scene->sys) return -1;
+    return pk_system_slab_form(scene->sys);
+}
+
 int World::Autotune(int repeats, double* bestMs)
 {
     SyncStats();

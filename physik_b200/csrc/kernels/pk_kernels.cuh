@@ -340,6 +340,9 @@ struct SlabPcgArgs {
     int nbodies;
     BatchBodyStats* body_stats;
     unsigned* missing;
+    // Stream form (pk_slab_plan.h): 0 full symmetric rows, 1 the symmetric form (each
+    // in-sub-part block once, transposed products through the groups' shared-memory rings).
+    int sym;
 };
 
 // ------------------------------------------------------------------ FP64 refinement
@@ -439,7 +442,7 @@ int pcg_slab_max_grid();
 // tile (tile_desc: 4 ints per tile; tile_entry0: ntiles + 1 offsets into fill_src).
 cudaError_t launch_slab_fill_kernel(const float* values, int nnz, const int* tile_desc, const int* tile_entry0,
                                     int ntiles, const unsigned* fill_src, int nentries, float* stream,
-                                    unsigned long long stream_floats, cudaStream_t stream_);
+                                    unsigned long long stream_floats, int sym, cudaStream_t stream_);
 
 constexpr int kPcgThreads = 512;
 

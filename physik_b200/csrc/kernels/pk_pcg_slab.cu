@@ -22,6 +22,13 @@
 //   exchange reduces the blocks' partials in one fixed tree that every block evaluates
 //   identically: all blocks take the same decisions and a run repeats bit for bit.
 //
+// The symmetric stream form (pk_slab_plan.h) streams each block inside a sub-part once: a
+// consumer group takes only its own sub-part's tiles, and per tile first evaluates every
+// entry's product (a transposing entry also writes B^T d_r to its slot of the group's
+// shared-memory ring), waits at the group's named barrier, then completes each row's q
+// as its own sum plus its ring slots in order, and waits again before the next tile
+// writes.  All sums keep one fixed order, so runs still repeat bit for bit.
+//
 // Each row's x, r and M^-1 live in tensor memory (TMEM) for the whole solve: the twelve
 // consumer warps own rows t + 384k (t = their thread, k < 10), and warp w keeps row k at
 // TMEM lane 32 (w % 4) + lane, columns 160 (w / 4) + 16k .. + 15, read and written with
@@ -146,7 +153,11 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     const int sub = lane % LPR;
     float* win = reinterpret_cast<float*>(dyn);  // 3 floats per window row
     unsigned char* ring_base = dyn + kSlabRingOffset;
-    int4* table = reinterpret_cast<int4*>(dyn + kSlabTableOffset);
+    const bool sym = P.sym != 0;
+    const unsigned stage_bytes = sym ? (unsigned)kSymStageBytes : (unsigned)kSlabStageBytes;
+    int4* table = reinterpret_cast<int4*>(dyn + (sym ? kSlabSymTableOffset : kSlabTableOffset));
+    // symmetric form: this group's ring of transposed products (3 floats per slot)
+    float* tp = reinterpret_cast<float*>(dyn + kSlabSymTpOffset) + (size_t)3 * kSymRingSlots * (size_t)(group < kSlabGroups ? group : 0);
 
     // The part: rows [row0, row0 + m) of the slab order, halo rows halo_src[halo0 ..
     // halo0 + h), tiles [tile0, tile0 + ntiles).  A part that does not fit the block's
@@ -194,7 +205,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     const bool leader = P.grouped ? blk == gfirst : blk == 0;
     if (m < 0 || m > kSlabMaxRows || h < 0 || m + h > kSlabWinCap || row0 < 0 || row0 + m > P.n || ntiles < 0 ||
         ntiles > kSlabMaxTiles || halo0 < 0 || halo0 + h > P.halo_count || tile0 < 0 ||
-        tile0 + ntiles > P.tile_count) {
+        tile0 + ntiles > P.tile_count || (sym && ntiles % kSlabGroups != 0)) {
         m = h = ntiles = 0;
         row0 = 0;
         if (tid == 0) s_bad = 1;
@@ -204,11 +215,22 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     // tile and reports a breakdown.
     for (int i = tid; i < ntiles; i += blockDim.x) {
         int4 d = __ldg(P.tile_desc + tile0 + i);
-        const int ne = (d.y - kSlabHeaderBytes) / kSlabEntryBytes;
-        const bool ok = d.x >= 0 && d.y >= kSlabHeaderBytes && d.y <= kSlabStageBytes && (d.y & 15) == 0 &&
-                        d.y == kSlabHeaderBytes + kSlabEntryBytes * ne && ne <= kSlabCapE && d.w >= 1 &&
-                        d.w <= kSlabRows && d.z >= 0 && d.z + d.w <= m &&
-                        16ull * (unsigned long long)d.x + (unsigned long long)d.y <= P.stream_bytes;
+        bool ok;
+        if (sym) {
+            // a tile of the group's sub-part, or an empty position (the group has no more)
+            const int ne = (d.y - kSymHeaderBytes) / kSymEntryBytes;
+            ok = (d.y == 0 && d.w == 0) ||
+                 (d.x >= 0 && d.y >= kSymHeaderBytes && d.y <= kSymStageBytes && (d.y & 15) == 0 &&
+                  d.y == kSymHeaderBytes + kSymEntryBytes * ne && ne <= kSymCapE && (ne & 7) == 0 && d.w >= 1 &&
+                  d.w <= kSymRows && d.z >= 0 && d.z + d.w <= m &&
+                  16ull * (unsigned long long)d.x + (unsigned long long)d.y <= P.stream_bytes);
+        } else {
+            const int ne = (d.y - kSlabHeaderBytes) / kSlabEntryBytes;
+            ok = d.x >= 0 && d.y >= kSlabHeaderBytes && d.y <= kSlabStageBytes && (d.y & 15) == 0 &&
+                 d.y == kSlabHeaderBytes + kSlabEntryBytes * ne && ne <= kSlabCapE && d.w >= 1 && d.w <= kSlabRows &&
+                 d.z >= 0 && d.z + d.w <= m &&
+                 16ull * (unsigned long long)d.x + (unsigned long long)d.y <= P.stream_bytes;
+        }
         if (!ok) {
             d = make_int4(0, 0, 0, 0);
             s_bad = 1;
@@ -254,6 +276,136 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     unsigned issued = 0;  // ring positions issued by the producer (producer lane 0 only)
     unsigned xgen = 0;
 
+    // Phase A of the symmetric form, for one consumer group: its ring positions are
+    // ring + group, ring + group + 3, ... (ntiles is a multiple of 3 and ring starts at 0,
+    // so a position's group never changes).  Every warp of the group passes every
+    // position and both named barriers, whatever happened (a wait that gave up only
+    // empties its tile), so the barriers always complete.
+    auto phase_a_sym = [&](Acc& dq, int& qbad) {
+        const float* wv = win;
+        const int wmax = max(wn - 1, 0);
+        const unsigned gbar = 1u + (unsigned)group;  // named barrier of this group (0 is __syncthreads)
+        const int row_in_pass = ((warp % kSlabGroupWarps) * 32 + lane) / LPR;
+        for (unsigned p = ring + (unsigned)group; p < ring + (unsigned)ntiles; p += kSlabGroups) {
+            const int s = (int)(p % S);
+            const unsigned u = p / S;
+            bool ok = mbar_wait(&full_bar[s], u & 1u);
+            if (!ok) s_fail = 1;
+            const int4 d = table[p - ring];
+            ok = ok && d.y > 0;
+            const unsigned char* st = ring_base + (size_t)s * stage_bytes;
+            const int ne = ok ? (d.y - kSymHeaderBytes) / kSymEntryBytes : 0;
+            const int rows = ok ? d.w : 0;
+            const unsigned short* roff = reinterpret_cast<const unsigned short*>(st);
+            const unsigned short* lbase = roff + (kSymRows + 1);
+            const float* vals = reinterpret_cast<const float*>(st + kSymHeaderBytes);
+            const unsigned short* lcol = reinterpret_cast<const unsigned short*>(st + kSymHeaderBytes + 36 * ne);
+            const unsigned short* lslot = lcol + ne;
+            V3<float> accs[2];
+#pragma unroll
+            for (int pass = 0; pass < 2; ++pass) {
+                const int sr = pass * kSlabRows + row_in_pass;
+                const bool valid = sr < rows;
+                int e0 = 0, e1 = 0;
+                V3<float> dr{0.f, 0.f, 0.f};
+                if (valid) {
+                    e0 = min((int)roff[sr], ne);
+                    e1 = min((int)roff[sr + 1], ne);
+                    const int li = min(d.z + sr, wmax);
+                    dr = V3<float>{wv[3 * li], wv[3 * li + 1], wv[3 * li + 2]};
+                }
+                V3<float> acc{0.f, 0.f, 0.f};
+                constexpr int kEntries = 4;
+                for (int j0 = e0 + sub; j0 < e1; j0 += kEntries * LPR) {
+                    int jj[kEntries];
+                    bool live[kEntries];
+#pragma unroll
+                    for (int q = 0; q < kEntries; ++q) {
+                        jj[q] = j0 + q * LPR;
+                        live[q] = jj[q] < e1;
+                        if (!live[q]) jj[q] = j0;
+                    }
+                    float xv[kEntries][3], bv[kEntries][9];
+                    unsigned sl[kEntries];
+#pragma unroll
+                    for (int q = 0; q < kEntries; ++q) {
+                        const int c = 3 * min((int)lcol[jj[q]], wmax);
+                        xv[q][0] = wv[c];
+                        xv[q][1] = wv[c + 1];
+                        xv[q][2] = wv[c + 2];
+                        sl[q] = lslot[jj[q]];
+#pragma unroll
+                        for (int e = 0; e < 9; ++e) bv[q][e] = vals[9 * jj[q] + e];
+                    }
+#pragma unroll
+                    for (int q = 0; q < kEntries; ++q) {
+                        // Column-major block: element (i, c) is v[3c + i].
+                        const float* v = bv[q];
+                        if (live[q]) {
+                            acc.x += v[0] * xv[q][0] + v[3] * xv[q][1] + v[6] * xv[q][2];
+                            acc.y += v[1] * xv[q][0] + v[4] * xv[q][1] + v[7] * xv[q][2];
+                            acc.z += v[2] * xv[q][0] + v[5] * xv[q][1] + v[8] * xv[q][2];
+                            if (sl[q] != kSymNoSlot) {  // B^T d_r for the later row
+                                float* t = tp + 3 * (sl[q] & (unsigned)(kSymRingSlots - 1));
+                                t[0] = v[0] * dr.x + v[1] * dr.y + v[2] * dr.z;
+                                t[1] = v[3] * dr.x + v[4] * dr.y + v[5] * dr.z;
+                                t[2] = v[6] * dr.x + v[7] * dr.y + v[8] * dr.z;
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int off = LPR / 2; off > 0; off >>= 1) {
+                    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+                    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
+                    acc.z += __shfl_xor_sync(0xffffffffu, acc.z, off);
+                }
+                accs[pass] = acc;
+            }
+            // The ring bases of the tile's rows, read before the stage is released.
+            unsigned lb0[2] = {0u, 0u}, lbn[2] = {0u, 0u};
+#pragma unroll
+            for (int pass = 0; pass < 2; ++pass) {
+                const int sr = pass * kSlabRows + row_in_pass;
+                if (sr < rows) {
+                    lb0[pass] = lbase[sr];
+                    lbn[pass] = ((unsigned)lbase[sr + 1] - lb0[pass]) & (unsigned)(kSymRingSlots - 1);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive_slab(&empty_bar[s]);  // this warp is done with the stage
+            asm volatile("bar.sync %0, %1;" ::"r"(gbar), "r"(32 * kSlabGroupWarps) : "memory");
+            // q = own sum + the row's ring slots, in slot order (lanes take every LPR-th
+            // slot, then the fixed shuffle tree).
+#pragma unroll
+            for (int pass = 0; pass < 2; ++pass) {
+                const int sr = pass * kSlabRows + row_in_pass;
+                V3<float> ts{0.f, 0.f, 0.f};
+                for (unsigned k = (unsigned)sub; k < lbn[pass]; k += LPR) {
+                    const float* t = tp + 3 * ((lb0[pass] + k) & (unsigned)(kSymRingSlots - 1));
+                    ts.x += t[0];
+                    ts.y += t[1];
+                    ts.z += t[2];
+                }
+#pragma unroll
+                for (int off = LPR / 2; off > 0; off >>= 1) {
+                    ts.x += __shfl_xor_sync(0xffffffffu, ts.x, off);
+                    ts.y += __shfl_xor_sync(0xffffffffu, ts.y, off);
+                    ts.z += __shfl_xor_sync(0xffffffffu, ts.z, off);
+                }
+                if (sr < rows && sub == 0) {
+                    const V3<float> q{accs[pass].x + ts.x, accs[pass].y + ts.y, accs[pass].z + ts.z};
+                    const int li = d.z + sr;
+                    stv4(P.qs + 4 * (size_t)(row0 + li), q);
+                    dq += dot_acc<Acc>(V3<float>{wv[3 * li], wv[3 * li + 1], wv[3 * li + 2]}, q);
+                    if (!finite3(q)) qbad = 1;
+                }
+            }
+            // the next tile's products may overwrite slots read above
+            asm volatile("bar.sync %0, %1;" ::"r"(gbar), "r"(32 * kSlabGroupWarps) : "memory");
+        }
+    };
+
     // Phase A: q = A d for the part's rows (d from the window), partial d.q.
     auto phase_a = [&](Acc& dq, int& qbad) {
         if (ntiles == 0) return;
@@ -272,11 +424,13 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                     const int4 d = table[p % (unsigned)ntiles];
                     mbar_arrive_expect_tx(&full_bar[s], (unsigned)d.y);
                     if (d.y > 0)
-                        bulk_g2s_hint(ring_base + (size_t)s * kSlabStageBytes, P.stream + 16 * (size_t)d.x,
+                        bulk_g2s_hint(ring_base + (size_t)s * stage_bytes, P.stream + 16 * (size_t)d.x,
                                       (unsigned)d.y, &full_bar[s], pol);
                 }
             }
             __syncwarp();
+        } else if (consumer && sym) {
+            phase_a_sym(dq, qbad);
         } else if (consumer) {
             const float* wv = win;
             const int wmax = max(wn - 1, 0);
@@ -289,7 +443,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                     break;
                 }
                 const int4 d = table[p - ring];
-                const unsigned char* st = ring_base + (size_t)s * kSlabStageBytes;
+                const unsigned char* st = ring_base + (size_t)s * stage_bytes;
                 const int ne = d.y > 0 ? (d.y - kSlabHeaderBytes) / kSlabEntryBytes : 0;
                 const unsigned short* roff = reinterpret_cast<const unsigned short*>(st);
                 const float* vals = reinterpret_cast<const float*>(st + kSlabHeaderBytes);
@@ -668,15 +822,16 @@ constexpr int kSlabFillThreads = 128;
 __global__ void __launch_bounds__(kSlabFillThreads)
     slab_fill_kernel(const float* __restrict__ values, int nnz, const int4* __restrict__ tile_desc,
                      const int* __restrict__ tile_entry0, int ntiles, const unsigned* __restrict__ fill_src,
-                     int nentries, float* __restrict__ out, unsigned long long out_floats)
+                     int nentries, float* __restrict__ out, unsigned long long out_floats, int header_bytes,
+                     int entry_bytes)
 {
     const int t = blockIdx.x;
     if (t >= ntiles) return;
     const int4 d = __ldg(tile_desc + t);
     const int e0 = __ldg(tile_entry0 + t), e1 = __ldg(tile_entry0 + t + 1);
     const int ne = e1 - e0;
-    const unsigned long long v0 = 4ull * (unsigned long long)d.x + kSlabHeaderBytes / 4;
-    if (e0 < 0 || ne < 0 || e1 > nentries || d.x < 0 || (ne & 7) != 0 || d.y != kSlabHeaderBytes + kSlabEntryBytes * ne ||
+    const unsigned long long v0 = 4ull * (unsigned long long)d.x + (unsigned long long)(header_bytes / 4);
+    if (e0 < 0 || ne <= 0 || e1 > nentries || d.x < 0 || (ne & 7) != 0 || d.y != header_bytes + entry_bytes * ne ||
         v0 + 9ull * (unsigned long long)ne > out_floats)
         return;
     float4* dst = reinterpret_cast<float4*>(out + v0);
@@ -736,12 +891,12 @@ cudaError_t launch_pcg_slab_kernel(const SlabPcgArgs<Acc>& args, int grid, cudaS
 
 cudaError_t launch_slab_fill_kernel(const float* values, int nnz, const int* tile_desc, const int* tile_entry0,
                                     int ntiles, const unsigned* fill_src, int nentries, float* out,
-                                    unsigned long long out_floats, cudaStream_t stream)
+                                    unsigned long long out_floats, int sym, cudaStream_t stream)
 {
     if (ntiles <= 0) return cudaSuccess;
-    slab_fill_kernel<<<ntiles, kSlabFillThreads, 0, stream>>>(values, nnz, reinterpret_cast<const int4*>(tile_desc),
-                                                               tile_entry0, ntiles, fill_src, nentries, out,
-                                                               out_floats);
+    slab_fill_kernel<<<ntiles, kSlabFillThreads, 0, stream>>>(
+        values, nnz, reinterpret_cast<const int4*>(tile_desc), tile_entry0, ntiles, fill_src, nentries, out, out_floats,
+        sym ? kSymHeaderBytes : kSlabHeaderBytes, sym ? kSymEntryBytes : kSlabEntryBytes);
     return cudaGetLastError();
 }
 

@@ -2,7 +2,9 @@
 #include "pk_slab_plan.h"
 
 #include <algorithm>
+#include <array>
 #include <atomic>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <numeric>
@@ -295,10 +297,424 @@ std::string build_layout(int n, const int* row_start, const int* col, const int*
     return "";
 }
 
+
+// ---------------------------------------------------------------- the symmetric form
+// Typical spacing of the rows along each axis: coupled rows differ along an axis either
+// by about one spacing or (for pairs in one plane across that axis) only by the mesh's
+// irregularity, so the spacing is the median of the differences above half the median.
+// A sweep ranks rows by their coordinates in units of these spacings, rounded, so rows of
+// one plane of a jittered grid share a rank.  1 along an axis with no spread.
+void axis_spacing(int n, const int* row_start, const int* col, const double* coords, double* sp)
+{
+    for (int a = 0; a < 3; ++a) {
+        std::vector<double> d;
+        const int stride = std::max(1, n / 50000);  // every block of a sample of rows is enough
+        for (int r = 0; r < n; r += stride)
+            for (int k = row_start[r]; k < row_start[r + 1]; ++k)
+                if (col[k] != r) d.push_back(std::fabs(coords[3 * (size_t)col[k] + a] - coords[3 * (size_t)r + a]));
+        sp[a] = 1.0;
+        if (d.empty()) continue;
+        std::sort(d.begin(), d.end());
+        const double half = 0.5 * d[d.size() / 2];
+        auto it = std::upper_bound(d.begin(), d.end(), half);
+        if (it == d.end() || !(*it > 0.0)) continue;
+        sp[a] = *(it + (d.end() - it) / 2);
+    }
+}
+
+// Sub-parts and sweep order of one part: its rows cut into `nsub` sub-parts by coordinate
+// bisection (NULL coords: contiguous ranges of equal weight), each ordered along the
+// longest extent of its bounding box, then the next, in units of the axis spacings (ties
+// by row).  Returns the part's rows in local order; sub_start[k] is the first local index
+// of sub-part k (sub_start[nsub] = rows).
+std::vector<int> sym_local_order(const std::vector<int>& rows, const double* coords, const double* sp,
+                                 const std::vector<double>& w, int nsub, std::vector<int>& sub_start)
+{
+    const int m = static_cast<int>(rows.size());
+    std::vector<int> sub(m, 0);
+    const int ns = std::min(nsub, m);
+    if (ns > 1) {
+        if (coords) {
+            std::vector<int> ids(m);
+            std::iota(ids.begin(), ids.end(), 0);
+            std::vector<double> xyz(3 * (size_t)m), wl(m);
+            for (int i = 0; i < m; ++i) {
+                for (int a = 0; a < 3; ++a) xyz[3 * (size_t)i + a] = coords[3 * (size_t)rows[i] + a];
+                wl[i] = w[rows[i]];
+            }
+            rcb(ids, 0, (size_t)m, 0, ns, xyz.data(), wl, sub, 8);  // depth 8: never threaded
+        } else {
+            double total = 0.0, acc = 0.0;
+            for (int i = 0; i < m; ++i) total += w[rows[i]];
+            for (int i = 0; i < m; ++i) {
+                sub[i] = std::min(ns - 1, static_cast<int>(acc * ns / total));
+                acc += w[rows[i]];
+            }
+        }
+    }
+    std::vector<int> order;
+    order.reserve(m);
+    sub_start.assign(nsub + 1, 0);
+    for (int k = 0; k < nsub; ++k) {
+        std::vector<int> mine;
+        for (int i = 0; i < m; ++i)
+            if (sub[i] == k) mine.push_back(rows[i]);
+        if (coords && mine.size() > 1) {
+            double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+            for (int r : mine)
+                for (int a = 0; a < 3; ++a) {
+                    mn[a] = std::min(mn[a], coords[3 * (size_t)r + a]);
+                    mx[a] = std::max(mx[a], coords[3 * (size_t)r + a]);
+                }
+            int ax[3] = {0, 1, 2};
+            std::sort(ax, ax + 3, [&](int a, int b) {
+                const double ea = (mx[a] - mn[a]) / sp[a], eb = (mx[b] - mn[b]) / sp[b];
+                return ea > eb || (ea == eb && a < b);
+            });
+            std::vector<std::pair<std::array<long long, 3>, int>> key(mine.size());
+            for (size_t i = 0; i < mine.size(); ++i) {
+                for (int j = 0; j < 3; ++j)
+                    key[i].first[j] = std::llround((coords[3 * (size_t)mine[i] + ax[j]] - mn[ax[j]]) / sp[ax[j]]);
+                key[i].second = mine[i];
+            }
+            std::sort(key.begin(), key.end());
+            for (size_t i = 0; i < mine.size(); ++i) mine[i] = key[i].second;
+        }
+        order.insert(order.end(), mine.begin(), mine.end());
+        sub_start[k + 1] = static_cast<int>(order.size());
+    }
+    return order;
+}
+
+// One tile of the symmetric form while it is built: its rows (local indices), their
+// entries and ring bases.
+struct SymTile {
+    int first = 0, rows = 0, ne = 0;     // ne padded to a multiple of 8
+    std::vector<unsigned short> roff;    // rows + 1
+    std::vector<unsigned short> lbase;   // rows + 1 (mod the ring)
+    std::vector<unsigned short> wcol, slot;
+    std::vector<unsigned> src;
+};
+
+// The tiles of one part in the symmetric form, group by group.  loc_of[c]: local index of
+// row c if it is in this part, else -1; win(c): window index of row c (any increasing
+// stand-in while only the fit is tested: entries are sorted by it, counts do not depend
+// on it).  Sub-part s belongs to group s / (subs / kSlabGroups), its rows are local indices
+// [sub_start[s], sub_start[s + 1]).  Returns "" or why the form does not fit.
+template <class Win>
+std::string sym_part_tiles(const int* row_start, const int* col, const int* lt_start, const int* lt_row,
+                           const int* lt_block, const std::vector<int>& order, const std::vector<int>& sub_start,
+                           const std::vector<int>& loc_of, Win&& win, std::vector<SymTile> (&tiles)[kSlabGroups])
+{
+    const int subs = static_cast<int>(sub_start.size()) - 1;
+    const int per_group = subs / kSlabGroups;
+    std::vector<int> sub_of_local(order.size());
+    for (int sb = 0; sb < subs; ++sb)
+        for (int i = sub_start[sb]; i < sub_start[sb + 1]; ++i) sub_of_local[i] = sb;
+    struct Ent {
+        int win;
+        unsigned src;
+        int target;  // local index of the row a transposing entry also feeds, or -1
+    };
+    for (int g = 0; g < kSlabGroups; ++g) {
+        tiles[g].clear();
+        // the group's rows: its sub-parts one after the other
+        const int a0 = sub_start[g * per_group], a1 = sub_start[(g + 1) * per_group], ms = a1 - a0;
+        if (ms <= 0) continue;
+        std::vector<std::vector<Ent>> ents(ms);
+        std::vector<std::vector<int>> lower(ms);
+        for (int i = a0; i < a1; ++i) {
+            const int r = order[i];
+            auto add = [&](int c, unsigned src) {
+                const int lc = loc_of[c];
+                const bool inside = lc >= 0 && sub_of_local[lc] == sub_of_local[i];
+                if (!inside || lc == i) {
+                    ents[i - a0].push_back({win(c), src, -1});
+                } else if (lc > i) {
+                    ents[i - a0].push_back({win(c), src, lc});
+                    lower[lc - a0].push_back(i);
+                }
+            };
+            for (int kk = row_start[r]; kk < row_start[r + 1]; ++kk) add(col[kk], static_cast<unsigned>(kk));
+            for (int e = lt_start[r]; e < lt_start[r + 1]; ++e)
+                add(lt_row[e], static_cast<unsigned>(lt_block[e]) | kSlabLowerBit);
+            std::sort(ents[i - a0].begin(), ents[i - a0].end(), [](const Ent& x, const Ent& y) { return x.win < y.win; });
+        }
+        std::vector<long long> L(ms + 1, 0);  // ring bases, not yet reduced mod the ring
+        for (int j = 0; j < ms; ++j) {
+            std::sort(lower[j].begin(), lower[j].end());
+            L[j + 1] = L[j] + static_cast<long long>(lower[j].size());
+        }
+        // tiles: consecutive rows, at most kSymRows rows and kSymCapE entries
+        int a = 0;
+        long long maxtgt = -1;  // furthest row a processed row wrote to
+        while (a < ms) {
+            int b = a, e = 0;
+            while (b < ms && b - a < kSymRows) {
+                const int e2 = e + static_cast<int>(ents[b].size());
+                if (((e2 + 7) & ~7) > kSymCapE) break;
+                e = e2;
+                ++b;
+            }
+            if (b == a) return "a row has more blocks than a tile holds";
+            SymTile tl;
+            tl.first = a0 + a;
+            tl.rows = b - a;
+            tl.ne = (e + 7) & ~7;
+            tl.roff.resize(tl.rows + 1);
+            tl.lbase.resize(tl.rows + 1);
+            tl.wcol.assign(tl.ne, 0);
+            tl.slot.assign(tl.ne, static_cast<unsigned short>(kSymNoSlot));
+            tl.src.assign(tl.ne, kSlabNoPos);
+            int j = 0;
+            for (int i = a; i < b; ++i) {
+                tl.roff[i - a] = static_cast<unsigned short>(j);
+                tl.lbase[i - a] = static_cast<unsigned short>(L[i] & (kSymRingSlots - 1));
+                for (const Ent& en : ents[i]) {
+                    tl.wcol[j] = static_cast<unsigned short>(en.win);
+                    tl.src[j] = en.src;
+                    if (en.target >= 0) {
+                        const int tj = en.target - a0;
+                        const std::vector<int>& lw = lower[tj];
+                        const long long rank = std::lower_bound(lw.begin(), lw.end(), a0 + i) - lw.begin();
+                        tl.slot[j] = static_cast<unsigned short>((L[tj] + rank) & (kSymRingSlots - 1));
+                        maxtgt = std::max<long long>(maxtgt, tj);
+                    }
+                    ++j;
+                }
+            }
+            tl.roff[b - a] = static_cast<unsigned short>(j);
+            tl.lbase[b - a] = static_cast<unsigned short>(L[b] & (kSymRingSlots - 1));
+            // alive while this tile runs: its own rows' slots and every later row's slots
+            // that a processed row has written
+            const long long last = std::max<long long>(maxtgt, b - 1);
+            if (L[last + 1] - L[a] > kSymRingSlots)
+                return "the transposed products in flight exceed the ring (" + std::to_string(L[last + 1] - L[a]) +
+                       " slots)";
+            tiles[g].push_back(std::move(tl));
+            a = b;
+        }
+    }
+    size_t most = 0;
+    for (int g = 0; g < kSlabGroups; ++g) most = std::max(most, tiles[g].size());
+    if (kSlabGroups * most > (size_t)kSlabMaxTiles) return "a part has more tiles than the table holds";
+    return "";
+}
+
+// The symmetric-form layout for a given assignment of rows to parts: local orders
+// (sub-parts, sweeps), windows, halos, tiles in ring order (group g at positions g, g + 3,
+// ...; empty positions where a group has fewer tiles), stream and fill list.  Every part
+// takes the fewest sub-parts per group (1 to 4) whose transposed products fit the rings.
+std::string build_layout_sym(int n, const int* row_start, const int* col, const int* lt_start, const int* lt_row,
+                             const int* lt_block, const double* coords, const std::vector<int>& part_of,
+                             const std::vector<double>& w, int parts, SlabPlan& out)
+{
+    const int nnz = row_start[n];
+    std::vector<int> count(parts + 1, 0);
+    for (int r = 0; r < n; ++r) ++count[part_of[r] + 1];
+    for (int p = 0; p < parts; ++p) count[p + 1] += count[p];
+    for (int p = 0; p < parts; ++p) {
+        if (count[p + 1] == count[p]) return "a part has no rows";
+        if (count[p + 1] - count[p] > kSlabMaxRows) return "a part has more rows than tensor memory holds";
+    }
+    std::vector<std::vector<int>> part_rows(parts);
+    for (int r = 0; r < n; ++r) part_rows[part_of[r]].push_back(r);
+    double sp[3] = {1.0, 1.0, 1.0};
+    if (coords) axis_spacing(n, row_start, col, coords, sp);
+    const int nt = std::min(parts, plan_threads());
+    std::vector<std::vector<int>> loc_of(nt);
+    // 1. local orders: the fewest sub-parts per group that fit
+    std::vector<std::vector<int>> sub_start(parts);
+    out.perm.assign(n, 0);
+    std::vector<std::string> errors(parts);
+    parallel_items(parts, [&](int p, int t) {
+        try {
+            std::vector<int>& lo = loc_of[t];
+            if (lo.empty()) lo.assign(n, -1);
+            std::string why, first_why;
+            for (int per = 1; per <= 4; ++per) {
+                std::vector<int> ss;
+                const std::vector<int> ord = sym_local_order(part_rows[p], coords, sp, w, kSlabGroups * per, ss);
+                for (size_t i = 0; i < ord.size(); ++i) lo[ord[i]] = static_cast<int>(i);
+                std::vector<SymTile> tiles[kSlabGroups];
+                why = sym_part_tiles(row_start, col, lt_start, lt_row, lt_block, ord, ss, lo,
+                                     [&](int c) { return lo[c] >= 0 ? lo[c] : n + c; }, tiles);
+                for (int r : ord) lo[r] = -1;
+                if (why.empty()) {
+                    std::copy(ord.begin(), ord.end(), out.perm.begin() + count[p]);
+                    sub_start[p] = ss;
+                    break;
+                }
+                if (first_why.empty()) first_why = why;
+            }
+            errors[p] = why.empty() ? why : first_why;  // the one-sub-part-per-group reason
+        } catch (...) {
+            errors[p] = "host memory exhausted while building the layout";
+        }
+    });
+    for (int p = 0; p < parts; ++p)
+        if (!errors[p].empty()) return errors[p];
+    std::vector<int> inv(n);
+    for (int g = 0; g < n; ++g) inv[out.perm[g]] = g;
+    out.n = n;
+    out.parts = parts;
+    out.sym = true;
+    out.part_info.assign((size_t)kSlabPartInts * parts, 0);
+    out.fill_src.clear();
+    out.tile_entry0.clear();
+    out.tile_desc.clear();
+    out.halo_src.clear();
+
+    // 2. per part: halo, window indices and the tiles with their real window columns
+    struct PartOut {
+        std::vector<int> halo;
+        std::vector<SymTile> tiles[kSlabGroups];
+    };
+    std::vector<PartOut> po(parts);
+    std::vector<std::vector<int>> win_of(nt);
+    auto build_part = [&](int p, int t) {
+        std::vector<int>& wo = win_of[t];
+        std::vector<int>& lo = loc_of[t];
+        if (wo.empty()) wo.assign(n, -1);
+        if (lo.empty()) lo.assign(n, -1);
+        const int g0 = count[p], g1 = count[p + 1], m = g1 - g0;
+        for (int g = g0; g < g1; ++g) wo[out.perm[g]] = lo[out.perm[g]] = g - g0;
+        std::vector<int>& halo = po[p].halo;
+        for (int g = g0; g < g1; ++g) {
+            const int r = out.perm[g];
+            for (int k = row_start[r]; k < row_start[r + 1]; ++k)
+                if (part_of[col[k]] != p) halo.push_back(inv[col[k]]);
+            for (int e = lt_start[r]; e < lt_start[r + 1]; ++e)
+                if (part_of[lt_row[e]] != p) halo.push_back(inv[lt_row[e]]);
+        }
+        std::sort(halo.begin(), halo.end());
+        halo.erase(std::unique(halo.begin(), halo.end()), halo.end());
+        const int h = static_cast<int>(halo.size());
+        if (m + h <= kSlabWinCap) {
+            for (int i = 0; i < h; ++i) wo[out.perm[halo[i]]] = m + i;
+            const std::vector<int> ord(out.perm.begin() + g0, out.perm.begin() + g1);
+            errors[p] = sym_part_tiles(row_start, col, lt_start, lt_row, lt_block, ord, sub_start[p], lo,
+                                       [&](int c) { return wo[c]; }, po[p].tiles);
+        } else {
+            errors[p] = "a part's window exceeds shared memory";
+        }
+        for (int g = g0; g < g1; ++g) wo[out.perm[g]] = lo[out.perm[g]] = -1;
+        for (int i = 0; i < h; ++i) wo[out.perm[halo[i]]] = -1;
+    };
+    parallel_items(parts, [&](int p, int t) {
+        try {
+            build_part(p, t);
+        } catch (...) {
+            errors[p] = "host memory exhausted while building the layout";
+        }
+    });
+    for (int p = 0; p < parts; ++p)
+        if (!errors[p].empty()) return errors[p];
+
+    // 3. stream offsets in part order, positions in ring order (group = position % 3)
+    size_t stream_bytes = 0, entries = 0;
+    std::vector<size_t> tile_off;  // stream byte offset of every position (empty: unused)
+    std::vector<const SymTile*> tile_ptr;
+    for (int p = 0; p < parts; ++p) {
+        const int m = count[p + 1] - count[p], h = static_cast<int>(po[p].halo.size());
+        size_t most = 0;
+        for (int k = 0; k < kSlabGroups; ++k) most = std::max(most, po[p].tiles[k].size());
+        int* pi = out.part_info.data() + (size_t)kSlabPartInts * p;
+        pi[0] = count[p];
+        pi[1] = m;
+        pi[2] = static_cast<int>(out.halo_src.size());
+        pi[3] = h;
+        pi[4] = static_cast<int>(out.tile_desc.size() / 4);
+        pi[5] = static_cast<int>(kSlabGroups * most);
+        out.halo_src.insert(out.halo_src.end(), po[p].halo.begin(), po[p].halo.end());
+        out.max_window = std::max(out.max_window, m + h);
+        out.max_tiles = std::max(out.max_tiles, pi[5]);
+        out.max_rows = std::max(out.max_rows, m);
+        for (size_t q = 0; q < most; ++q)
+            for (int k = 0; k < kSlabGroups; ++k) {
+                out.tile_entry0.push_back(static_cast<int>(entries));
+                if (q < po[p].tiles[k].size()) {
+                    const SymTile& tl = po[p].tiles[k][q];
+                    const size_t bytes = (size_t)kSymHeaderBytes + (size_t)kSymEntryBytes * tl.ne;
+                    if (stream_bytes / 16 > 0x7fffffffULL || (stream_bytes + bytes) / 4 >= 0xffffffffULL)
+                        return "stream too large";
+                    out.tile_desc.insert(out.tile_desc.end(),
+                                         {static_cast<int>(stream_bytes / 16), static_cast<int>(bytes), tl.first, tl.rows});
+                    tile_off.push_back(stream_bytes);
+                    tile_ptr.push_back(&tl);
+                    stream_bytes += bytes;  // a multiple of 16 (ne is a multiple of 8)
+                    entries += tl.ne;
+                    if (entries > 0x7fffffffu) return "stream too large";
+                } else {
+                    out.tile_desc.insert(out.tile_desc.end(), {0, 0, 0, 0});  // nothing for this group
+                    tile_off.push_back(0);
+                    tile_ptr.push_back(nullptr);
+                }
+            }
+    }
+    out.tile_entry0.push_back(static_cast<int>(entries));
+    out.stream.assign(stream_bytes, 0);
+    out.fill_src.assign(entries, kSlabNoPos);
+    // 4. tile contents (in parallel: every tile writes only its own bytes)
+    parallel_items(static_cast<int>(tile_ptr.size()), [&](int ti, int) {
+        const SymTile* tl = tile_ptr[ti];
+        if (!tl) return;
+        const size_t off = tile_off[ti];
+        for (int i = 0; i <= tl->rows; ++i) {
+            put_u16(out.stream, off + 2 * (size_t)i, tl->roff[i]);
+            put_u16(out.stream, off + 2 * (size_t)(kSymRows + 1) + 2 * (size_t)i, tl->lbase[i]);
+        }
+        const size_t col_off = off + kSymHeaderBytes + 36 * (size_t)tl->ne;
+        const size_t slot_off = col_off + 2 * (size_t)tl->ne;
+        for (int j = 0; j < tl->ne; ++j) {
+            put_u16(out.stream, col_off + 2 * (size_t)j, tl->wcol[j]);
+            put_u16(out.stream, slot_off + 2 * (size_t)j, tl->slot[j]);
+        }
+        std::copy(tl->src.begin(), tl->src.end(), out.fill_src.begin() + out.tile_entry0[ti]);
+    });
+    // 5. every block placed as its pair requires: once for the diagonal and for a pair
+    // inside one sub-part (as the block or its transpose), copy and transpose otherwise
+    std::vector<int> sub_of(n);
+    for (int p = 0; p < parts; ++p)
+        for (size_t sb = 0; sb + 1 < sub_start[p].size(); ++sb)
+            for (int i = sub_start[p][sb]; i < sub_start[p][sb + 1]; ++i) sub_of[out.perm[count[p] + i]] = (int)sb;
+    std::vector<unsigned char> seen(nnz, 0);
+    for (const unsigned src : out.fill_src) {
+        if (src == kSlabNoPos) continue;
+        const unsigned k = src & ~kSlabLowerBit;
+        const unsigned char bit = (src & kSlabLowerBit) ? 2 : 1;
+        if (k >= (unsigned)nnz || (seen[k] & bit)) return "internal: a block placed twice";
+        seen[k] |= bit;
+    }
+    for (int r = 0; r < n; ++r)
+        for (int k = row_start[r]; k < row_start[r + 1]; ++k) {
+            const int c = col[k];
+            const bool together = part_of[r] == part_of[c] && sub_of[r] == sub_of[c];
+            const unsigned char want = c == r ? 1 : (together ? 0 : 3);
+            if (want ? seen[k] != want : (seen[k] != 1 && seen[k] != 2)) return "internal: block placement mismatch";
+        }
+    return "";
+}
+
 }  // namespace
 
+// The symmetric form where the caller allows it and it applies, else the full rows.
+std::string build_layout_form(int n, const int* row_start, const int* col, const int* lt_start, const int* lt_row,
+                              const int* lt_block, const double* coords, const std::vector<int>& part_of,
+                              const std::vector<int>& len, const std::vector<double>& w, int parts, int form,
+                              SlabPlan& out)
+{
+    if (form != kSlabFull) {
+        const std::string why =
+            build_layout_sym(n, row_start, col, lt_start, lt_row, lt_block, coords, part_of, w, parts, out);
+        if (why.empty() || form == kSlabSym) return why;
+        out = SlabPlan{};
+    }
+    return build_layout(n, row_start, col, lt_start, lt_row, lt_block, part_of, len, parts, out);
+}
+
 std::string build_slab_plan(int n, const int* row_start, const int* col, const int* lt_start, const int* lt_row,
-                            const int* lt_block, const double* coords, int parts, SlabPlan& out)
+                            const int* lt_block, const double* coords, int parts, SlabPlan& out, int form)
 {
     out = SlabPlan{};
     if (n <= 0 || parts <= 0) return "empty system";
@@ -322,7 +738,8 @@ std::string build_slab_plan(int n, const int* row_start, const int* col, const i
             acc += w[r];
         }
     }
-    const std::string why = build_layout(n, row_start, col, lt_start, lt_row, lt_block, part_of, len, parts, out);
+    const std::string why =
+        build_layout_form(n, row_start, col, lt_start, lt_row, lt_block, coords, part_of, len, w, parts, form, out);
     if (!why.empty()) return why;
     for (int p = 0; p < parts; ++p) {
         out.part_info[(size_t)kSlabPartInts * p + 6] = 0;
@@ -335,7 +752,7 @@ std::string build_slab_plan(int n, const int* row_start, const int* col, const i
 
 std::string build_slab_plan_batched(int n, const int* row_start, const int* col, const int* lt_start,
                                     const int* lt_row, const int* lt_block, const double* coords, const int* seg,
-                                    int nseg, int max_blocks, SlabPlan& out)
+                                    int nseg, int max_blocks, SlabPlan& out, int form)
 {
     out = SlabPlan{};
     if (n <= 0 || nseg <= 0 || max_blocks <= 0) return "empty system";
@@ -484,7 +901,8 @@ std::string build_slab_plan_batched(int n, const int* row_start, const int* col,
     }
     const int parts = static_cast<int>(part_body.size());
     std::vector<int> launch_start = out.launch_start;
-    const std::string why = build_layout(n, row_start, col, lt_start, lt_row, lt_block, part_of, len, parts, out);
+    const std::string why =
+        build_layout_form(n, row_start, col, lt_start, lt_row, lt_block, coords, part_of, len, w, parts, form, out);
     if (!why.empty()) return why;
     for (int p = 0; p < parts; ++p) {
         out.part_info[(size_t)kSlabPartInts * p + 6] = group_first[p];
@@ -495,17 +913,90 @@ std::string build_slab_plan_batched(int n, const int* row_start, const int* col,
     return "";
 }
 
+namespace {
+
+// The symmetric form decoded as the kernel's consumer groups read it: each group's tiles
+// in ring order; per tile first every entry's product (transposing entries also writing
+// B^T d_r to their ring slot), then every row's q = own sum + its ring slots in order.
+// The ring is emulated with its wrap-around, so a slot reused too early shows up here.
+void slab_spmv_host_sym(const SlabPlan& plan, const std::vector<unsigned char>& s, const double* x, double* y)
+{
+    for (int p = 0; p < plan.parts; ++p) {
+        const int* pi = plan.part_info.data() + (size_t)kSlabPartInts * p;
+        const int g0 = pi[0], m = pi[1], halo0 = pi[2], h = pi[3], tile0 = pi[4], ntiles = pi[5];
+        const int wn = m + h;
+        std::vector<double> win(3 * (size_t)wn);
+        for (int wi = 0; wi < wn; ++wi) {
+            const int g = wi < m ? g0 + wi : plan.halo_src[halo0 + wi - m];
+            const int r = plan.perm[g];
+            for (int a = 0; a < 3; ++a)
+                win[3 * (size_t)wi + a] = static_cast<double>(static_cast<float>(x[3 * (size_t)r + a]));
+        }
+        for (int grp = 0; grp < kSlabGroups; ++grp) {
+            std::vector<double> ring(3 * (size_t)kSymRingSlots, std::nan(""));
+            for (int t = grp; t < ntiles; t += kSlabGroups) {
+                const int* d = plan.tile_desc.data() + 4 * (size_t)(tile0 + t);
+                if (d[1] == 0) continue;
+                const size_t off = 16 * (size_t)d[0];
+                const int ne = (d[1] - kSymHeaderBytes) / kSymEntryBytes;
+                const size_t vals_off = off + kSymHeaderBytes, col_off = vals_off + 36 * (size_t)ne,
+                             slot_off = col_off + 2 * (size_t)ne;
+                const int rows = std::min(d[3], kSymRows);
+                std::vector<double> own(3 * (size_t)rows, 0.0);
+                for (int i = 0; i < rows; ++i) {
+                    const int li = std::min(d[2] + i, std::max(wn - 1, 0));
+                    const int e0 = std::min<int>(get_u16(s, off + 2 * (size_t)i), ne);
+                    const int e1 = std::min<int>(get_u16(s, off + 2 * (size_t)(i + 1)), ne);
+                    for (int j = e0; j < e1; ++j) {
+                        const int c = std::min<int>(get_u16(s, col_off + 2 * (size_t)j), wn - 1);
+                        const unsigned sl = get_u16(s, slot_off + 2 * (size_t)j);
+                        float v[9];
+                        std::memcpy(v, s.data() + vals_off + 36 * (size_t)j, 36);
+                        for (int a = 0; a < 3; ++a)
+                            for (int mm = 0; mm < 3; ++mm) own[3 * (size_t)i + a] += double(v[3 * mm + a]) * win[3 * (size_t)c + mm];
+                        if (sl != kSymNoSlot) {
+                            const size_t q = 3 * (size_t)(sl & (kSymRingSlots - 1));
+                            for (int a = 0; a < 3; ++a) {
+                                double acc = 0.0;
+                                for (int mm = 0; mm < 3; ++mm) acc += double(v[3 * a + mm]) * win[3 * (size_t)li + mm];
+                                ring[q + a] = acc;
+                            }
+                        }
+                    }
+                }
+                const size_t lb_off = off + 2 * (size_t)(kSymRows + 1);
+                for (int i = 0; i < rows; ++i) {
+                    const unsigned b0 = get_u16(s, lb_off + 2 * (size_t)i), b1 = get_u16(s, lb_off + 2 * (size_t)(i + 1));
+                    const unsigned cnt = (b1 - b0) & (kSymRingSlots - 1);
+                    double q[3] = {own[3 * (size_t)i], own[3 * (size_t)i + 1], own[3 * (size_t)i + 2]};
+                    for (unsigned k = 0; k < cnt; ++k) {
+                        const size_t sl = 3 * (size_t)((b0 + k) & (kSymRingSlots - 1));
+                        for (int a = 0; a < 3; ++a) q[a] += ring[sl + a];
+                        for (int a = 0; a < 3; ++a) ring[sl + a] = std::nan("");  // consumed
+                    }
+                    const int r = plan.perm[g0 + d[2] + i];
+                    for (int a = 0; a < 3; ++a) y[3 * (size_t)r + a] = q[a];
+                }
+            }
+        }
+    }
+}
+
+}  // namespace
+
 void slab_spmv_host(const SlabPlan& plan, int nnz, const double* values, const double* x, double* y)
 {
     // Fill, as the fill kernel does (float storage).
     std::vector<unsigned char> s = plan.stream;
     const size_t sfloats = s.size() / 4;
     const size_t ntiles_all = plan.tile_desc.size() / 4;
+    const int header = plan.sym ? kSymHeaderBytes : kSlabHeaderBytes;
     for (size_t t = 0; t < ntiles_all; ++t) {
         // The tile's value area, float by float in stream order; element j = 3 c + i of a
         // transposed entry is element 3 i + c of its block.
         const int e0 = plan.tile_entry0[t], ne = plan.tile_entry0[t + 1] - e0;
-        const size_t v0 = 4 * (size_t)plan.tile_desc[4 * t] + kSlabHeaderBytes / 4;
+        if (ne == 0) continue;
+        const size_t v0 = 4 * (size_t)plan.tile_desc[4 * t] + header / 4;
         if (v0 + 9 * (size_t)ne > sfloats) continue;
         for (int f = 0; f < 9 * ne; ++f) {
             const int e = f / 9, j = f - 9 * e;
@@ -518,6 +1009,10 @@ void slab_spmv_host(const SlabPlan& plan, int nnz, const double* values, const d
             }
             std::memcpy(s.data() + 4 * (v0 + f), &v, 4);
         }
+    }
+    if (plan.sym) {
+        slab_spmv_host_sym(plan, s, x, y);
+        return;
     }
     // Decode tile by tile with the kernel's clamps.
     for (int p = 0; p < plan.parts; ++p) {

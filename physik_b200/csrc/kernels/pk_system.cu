@@ -232,6 +232,7 @@ struct pk_system {
     int slab_max_grid = 0;
     std::string slab_reason;      // why the layout does not apply
     unsigned long long slab_stream_bytes = 0;
+    bool slab_sym = false;        // the layout is the symmetric stream form
     DevBuf slab_part_info, slab_tiles, slab_stream, slab_halo, slab_perm, slab_fill_src, slab_tile_e0;
     int slab_fill_entries = 0;
     DevBuf slab_qs, slab_ss;
@@ -499,10 +500,21 @@ int slab_fill(pk_system* s)
     PK_CHECK(pk::launch_slab_fill_kernel(s->values.as<float>(), s->nnz, s->slab_tiles.as<int>(),
                                          s->slab_tile_e0.as<int>(), s->slab_tile_count,
                                          s->slab_fill_src.as<unsigned>(), s->slab_fill_entries,
-                                         s->slab_stream.as<float>(), s->slab_stream_bytes / 4, s->stream));
+                                         s->slab_stream.as<float>(), s->slab_stream_bytes / 4, s->slab_sym ? 1 : 0,
+                                         s->stream));
     s->launches += 1;
     s->slab_filled = true;
     return PK_OK;
+}
+
+// PK_SLAB_FORM=full / sym asks for one stream form of the part-resident kernel's layout;
+// by default the symmetric form where it applies, else the full rows.
+int requested_slab_form()
+{
+    const char* e = std::getenv("PK_SLAB_FORM");
+    if (e && std::strcmp(e, "full") == 0) return pk::kSlabFull;
+    if (e && std::strcmp(e, "sym") == 0) return pk::kSlabSym;
+    return pk::kSlabAuto;
 }
 
 bool slab_allowed(const pk_system* s)
@@ -557,9 +569,9 @@ int ensure_slab(pk_system* s)
     const std::string why =
         bodies ? pk::build_slab_plan_batched(n, s->h_row_start.data(), col.data(), s->h_lts.data(), ltr.data(),
                                              ltb.data(), coords.data(), s->seg_start.data(),
-                                             static_cast<int>(s->seg_start.size()) - 1, grid, plan)
+                                             static_cast<int>(s->seg_start.size()) - 1, grid, plan, requested_slab_form())
                : pk::build_slab_plan(n, s->h_row_start.data(), col.data(), s->h_lts.data(), ltr.data(), ltb.data(),
-                                     coords.data(), grid, plan);
+                                     coords.data(), grid, plan, requested_slab_form());
     if (!why.empty()) {
         s->slab_reason = why;
         return PK_OK;
@@ -586,6 +598,7 @@ int ensure_slab(pk_system* s)
     PK_CHECK(s->slab_ss.ensure(16 * rows));
     PK_CHECK(cudaStreamSynchronize(s->stream));
     s->slab_stream_bytes = plan.stream.size();
+    s->slab_sym = plan.sym;
     s->slab_tile_count = static_cast<int>(plan.tile_desc.size() / 4);
     s->slab_fill_entries = static_cast<int>(plan.fill_src.size());
     s->slab_halo_count = static_cast<int>(plan.halo_src.size());
@@ -652,6 +665,7 @@ int run_pcg_slab(pk_system* s, const pk_step_params& p, int skip_on_flags)
         a.nbodies = bodies ? nseg : 1;
         a.body_stats = bodies ? s->body_stats.as<pk::BatchBodyStats>() : nullptr;
         a.missing = &st->batch_missing;
+        a.sym = s->slab_sym ? 1 : 0;
         // One launch per group of parts (the coupled solve: one launch of all parts).
         const int launches = static_cast<int>(s->slab_launch.size()) - 1;
         for (int l = 0; l < launches; ++l) {
@@ -1683,6 +1697,12 @@ PKCUDA_API int pk_system_set_refinement(pk_system* s, int passes)
     return PK_OK;
 }
 
+PKCUDA_API int pk_system_slab_form(pk_system* s)
+{
+    if (!s || (s->last_kernel != 3 && s->last_kernel != 5)) return -1;
+    return s->slab_sym ? 1 : 0;
+}
+
 PKCUDA_API int pk_system_pcg_kernel(pk_system* s, int* blocks)
 {
     if (!s) return fail(PK_ERR_ARG, "pcg_kernel");
@@ -2092,7 +2112,7 @@ extern "C" {
 
 PKCUDA_API int pk_slab_plan_batched_selfcheck(int n, const int* row_start, const int* col_index, const double* values,
                                               const double* x, const double* coords, const int* segment_row_start,
-                                              int segment_count, int max_blocks, double* y, int* info)
+                                              int segment_count, int max_blocks, int form, double* y, int* info)
 {
     if (n <= 0 || segment_count <= 0 || max_blocks <= 0 || !row_start || !col_index || !values || !x || !y ||
         !segment_row_start)
@@ -2104,7 +2124,8 @@ PKCUDA_API int pk_slab_plan_batched_selfcheck(int n, const int* row_start, const
     build_transpose(n, row_start, col_index, lts, ltr, ltb);
     pk::SlabPlan plan;
     const std::string why = pk::build_slab_plan_batched(n, row_start, col_index, lts.data(), ltr.data(), ltb.data(),
-                                                        coords, segment_row_start, segment_count, max_blocks, plan);
+                                                        coords, segment_row_start, segment_count, max_blocks, plan,
+                                                        form);
     if (!why.empty()) return fail(PK_ERR_UNSUPPORTED, "slab layout: " + why);
     // Groups: consecutive parts of one body inside one launch, sizes matching.
     const int launches = static_cast<int>(plan.launch_start.size()) - 1;
@@ -2131,12 +2152,13 @@ PKCUDA_API int pk_slab_plan_batched_selfcheck(int n, const int* row_start, const
         info[2] = plan.max_tiles;
         info[3] = static_cast<int>(plan.stream.size() / 1024);
         info[4] = launches;
+        info[5] = plan.sym ? 1 : 0;
     }
     return PK_OK;
 }
 
 PKCUDA_API int pk_slab_plan_selfcheck(int n, const int* row_start, const int* col_index, const double* values,
-                                      const double* x, const double* coords, int parts, double* y, int* info)
+                                      const double* x, const double* coords, int parts, int form, double* y, int* info)
 {
     if (n <= 0 || parts <= 0 || !row_start || !col_index || !values || !x || !y)
         return fail(PK_ERR_ARG, "slab selfcheck");
@@ -2152,7 +2174,7 @@ PKCUDA_API int pk_slab_plan_selfcheck(int n, const int* row_start, const int* co
     build_transpose(n, row_start, col_index, lts, ltr, ltb);
     pk::SlabPlan plan;
     const std::string why =
-        pk::build_slab_plan(n, row_start, col_index, lts.data(), ltr.data(), ltb.data(), coords, parts, plan);
+        pk::build_slab_plan(n, row_start, col_index, lts.data(), ltr.data(), ltb.data(), coords, parts, plan, form);
     if (!why.empty()) return fail(PK_ERR_UNSUPPORTED, "slab layout: " + why);
     pk::slab_spmv_host(plan, row_start[n], values, x, y);
     if (info) {
@@ -2160,6 +2182,7 @@ PKCUDA_API int pk_slab_plan_selfcheck(int n, const int* row_start, const int* co
         info[1] = plan.max_window;
         info[2] = plan.max_tiles;
         info[3] = static_cast<int>(plan.stream.size() / 1024);
+        info[4] = plan.sym ? 1 : 0;
     }
     return PK_OK;
 }

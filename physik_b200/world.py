@@ -170,6 +170,10 @@ class SimWorld:
         k = self.X.PHYSIK_B200_GetPcgKernel(self.h, C.byref(blocks))
         return self.PCG_KERNELS.get(k, "none"), blocks.value
 
+    def pcg_stream_form(self) -> str:
+        """Stream form of the part-resident kernel in the last solve: "full", "sym" or "none"."""
+        return {0: "full", 1: "sym"}.get(self.X.PHYSIK_B200_GetPcgStreamForm(self.h), "none")
+
     def body_stats(self, i: int):
         it, conv, res, fl = C.c_int(), C.c_int(), C.c_float(), C.c_uint()
         if self.X.PHYSIK_B200_GetBodyConjugateGradientStats(self.h, self.components[i], C.byref(it), C.byref(conv),

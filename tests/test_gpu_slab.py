@@ -124,3 +124,84 @@ def test_slab_is_deterministic_and_graph_replay_is_bit_identical():
         np.testing.assert_array_equal(x, xa)
         np.testing.assert_array_equal(v, va)
     assert g.pcg_kernel()[0] == "slab"
+
+
+# ---------------------------------------------------------------- stream forms
+# The part-resident kernel streams either full symmetric rows or, where the layout fits,
+# the symmetric form (each block inside a sub-part streamed once, its transposed product
+# sent through the consumer group's ring of slots in shared memory).  PK_SLAB_FORM forces
+# one; both must follow the FP64 oracle, agree with each other to summation order, and
+# repeat bit for bit (also under CUDA-graph replay).
+
+
+def _world(scene, form, monkeypatch, precision="mixed", graph=False):
+    monkeypatch.setenv("PK_SLAB_FORM", form)
+    w = SimWorld(scene, precision=precision)
+    if graph:
+        w.set_graph(True)
+    return w
+
+
+@pytest.mark.parametrize("form", ["full", "sym"])
+@pytest.mark.parametrize("make", [meshes.config1, meshes.config2, two_bodies], ids=["cube8", "beam64", "two_bodies"])
+def test_stream_forms_follow_fp64_oracle(make, form, monkeypatch):
+    scene = make()
+    gpu = _world(scene, form, monkeypatch)
+    ora = po.Oracle(scene, "f64", float_inputs=True)
+    for _ in range(2):
+        gpu.set_state(ora.x, ora.v, f64=True)
+        gpu.step()
+        ora.step()
+        assert gpu.pcg_kernel()[0] == "slab" and gpu.pcg_stream_form() == form, (gpu.pcg_stream_form(), gpu.error())
+        x, v = gpu.state(f64=True)
+        st = gpu.cg_stats()
+        assert st["flags"] & L.FLAG_INTEGRATED, hex(st["flags"])
+        assert rel(x, ora.x) <= 1e-5
+        assert rel(v, ora.v) <= 2e-3
+        assert abs(st["iterations"] - ora.last_stats()["iterations"]) <= 3
+
+
+def test_stream_forms_agree_and_sym_is_the_default(monkeypatch):
+    scene = meshes.config2()
+    monkeypatch.delenv("PK_SLAB_FORM", raising=False)
+    auto = SimWorld(scene, precision="mixed")
+    auto.step()
+    assert auto.pcg_stream_form() == "sym"
+    full = _world(scene, "full", monkeypatch)
+    full.step()
+    xa, va = auto.state(f64=True)
+    xf, vf = full.state(f64=True)
+    assert rel(xa, xf) <= 1e-6
+    assert rel(va, vf) <= 1e-3
+    assert abs(auto.cg_stats()["iterations"] - full.cg_stats()["iterations"]) <= 2
+
+
+def test_sym_form_repeats_bit_for_bit_and_under_graph_replay(monkeypatch):
+    scene = two_bodies()
+    a = _world(scene, "sym", monkeypatch)
+    b = _world(scene, "sym", monkeypatch)
+    g = _world(scene, "sym", monkeypatch, graph=True)
+    for _ in range(5):
+        a.step()
+        b.step()
+        g.step()
+    xa, va = a.state(f64=True)
+    for w in (b, g):
+        x, v = w.state(f64=True)
+        np.testing.assert_array_equal(x, xa)
+        np.testing.assert_array_equal(v, va)
+    assert g.pcg_stream_form() == "sym"
+
+
+def test_sym_form_fp32_follows_fp32_reference(monkeypatch):
+    scene = meshes.config1()
+    gpu = _world(scene, "sym", monkeypatch, precision="fp32")
+    ora = po.Oracle(scene, "f32")
+    for _ in range(3):
+        gpu.set_state(ora.x, ora.v, f64=True)
+        gpu.step()
+        ora.step()
+        x, v = gpu.state(f64=True)
+        assert gpu.pcg_stream_form() == "sym"
+        assert rel(x, ora.x) <= 1e-6
+        assert rel(v, ora.v) <= 2e-3
