@@ -47,6 +47,9 @@ typedef struct PhysikMaterialDesc {
     float damping;
 } PhysikMaterialDesc;
 
+/* PhysiK::ExternalLogicCallback (Handles.h:23): a script's per-frame callback. */
+typedef void (*PhysikExternalLogicCallback)(PhysikWorldHandle world, void* userData);
+
 /* PhysiK::Vec3 (include/PhysiK/Math/Vec3.h:7-12): three packed floats. */
 typedef struct PhysikVec3 {
     float x, y, z;
@@ -120,6 +123,36 @@ PHYSIK_B200_API int PHYSIK_GetTetMeshLocalCurrentPosition(PhysikWorldHandle worl
                                                           int localNodeIndex, float* outX, float* outY, float* outZ);
 PHYSIK_B200_API void PHYSIK_SetTetMeshMaterial(PhysikWorldHandle world, PhysikComponentHandle component,
                                                const PhysikMaterialDesc* material);
+/* Collision spheres   PhysiKAPI.h:159-164, 288-298, 346-351; PhysiKAPI.cpp:685-701,
+ * 1180-1218, 1407-1429; CollisionSphereComponent.cpp, CollisionComponent.cpp.  Every substep
+ * each active tet of every active soft body whose centroid lies strictly inside an active
+ * sphere gets a point connection (weights 1/4) pulling its centroid to the sphere's
+ * surface, with the sphere's connection stiffness and damping (defaults 1000 and 10;
+ * negative or non-finite settings become 0).  The radius is clamped at 0.  A kinematic
+ * target moves the sphere at the next PHYSIK_Step's start.  The contacts are found on the
+ * GPU at the substep's positions (pk_system_sphere_contacts).  Invalid handles are
+ * ignored; getters leave their out-pointers alone then. */
+PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateCollisionSphereComponent(PhysikWorldHandle world, float x, float y,
+                                                                            float z, float radius);
+PHYSIK_B200_API void PHYSIK_SetCollisionSphereConnectionSettings(PhysikWorldHandle world,
+                                                                 PhysikComponentHandle sphereComponent,
+                                                                 float stiffness, float damping);
+PHYSIK_B200_API void PHYSIK_GetCollisionSphereConnectionSettings(PhysikWorldHandle world,
+                                                                 PhysikComponentHandle sphereComponent,
+                                                                 float* outStiffness, float* outDamping);
+PHYSIK_B200_API void PHYSIK_SetCollisionComponentKinematicTarget(PhysikWorldHandle world,
+                                                                 PhysikComponentHandle component, float x, float y,
+                                                                 float z);
+
+/* Script components   PhysiKAPI.h:166-177, PhysiKAPI.cpp:719-765; ScriptComponent.cpp: the
+ * callback runs once per PHYSIK_Step, before the substeps (Component::PreUpdate, in
+ * execution-priority order), with the world handle, so a script can call PHYSIK_* (add
+ * point connections, move nodes, ...) for the frame.  Invalid handles are ignored. */
+PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateScriptComponent(PhysikWorldHandle world);
+PHYSIK_B200_API void PHYSIK_SetScriptComponentCallback(PhysikWorldHandle world, PhysikComponentHandle scriptComponent,
+                                                       PhysikExternalLogicCallback callback, void* userData);
+PHYSIK_B200_API void PHYSIK_ClearScriptComponentCallback(PhysikWorldHandle world,
+                                                         PhysikComponentHandle scriptComponent);
 /* PhysiKAPI.h:300-334 */
 PHYSIK_B200_API void PHYSIK_DestroyComponent(PhysikWorldHandle world, PhysikComponentHandle component);
 PHYSIK_B200_API int PHYSIK_IsComponentHandleValid(PhysikWorldHandle world, PhysikComponentHandle component);
@@ -226,6 +259,10 @@ PHYSIK_B200_API int PHYSIK_B200_GetPcgKernel(PhysikWorldHandle world, int* block
 /* The part-resident kernel's stream form in the last step's solve (pk_system_slab_form:
  * 0 full rows, 1 symmetric form, -1 another kernel).  No counterpart in the reference. */
 PHYSIK_B200_API int PHYSIK_B200_GetPcgStreamForm(PhysikWorldHandle world);
+/* The world's device system (a pk_system* of include/pkcuda.h) once a step has uploaded it,
+ * else NULL: lets a caller use the device ABI on the world's own buffers (e.g.
+ * pk_system_sphere_contacts).  The world owns it.  No counterpart in the reference. */
+PHYSIK_B200_API void* PHYSIK_B200_GetDeviceSystem(PhysikWorldHandle world);
 /* FP64 outer true-residual refinement of the implicit solve for FP32 and mixed precision
  * (no counterpart in the reference; see pk_system_set_refinement): up to `passes`
  * correction solves (0..16, 0 = off, the default) within the step's iteration budget,

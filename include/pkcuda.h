@@ -121,6 +121,15 @@ PKCUDA_API int pk_system_get_state_f64(pk_system* sys, double* x, double* v);
  * pk_system_get_snapshot_f32 reads nodes [first_node, first_node + count) of the last
  * snapshot (3 floats each) and waits for the stream. */
 PKCUDA_API int pk_system_snapshot_positions(pk_system* sys);
+/* The tets (of those set with flag bit 2, "active") whose centroid lies strictly inside the
+ * sphere (center[3], radius), at the current node positions -- CollisionSphereComponent::
+ * UpdateSystem's test (CollisionSphereComponent.cpp:141-190): centroid = ((x0/4 + x1/4) +
+ * x2/4) + x3/4 and |centroid - center| computed in the state's precision with every
+ * operation rounded once.  Writes up to max_contacts tet indices (ascending) and their
+ * centroids (3 each); returns the number of contacts (when above max_contacts nothing is
+ * written), or a negative PK_ERR_*.  Waits for the stream. */
+PKCUDA_API int pk_system_sphere_contacts(pk_system* sys, const double* center, double radius, int max_contacts,
+                                         int* tets, double* points);
 PKCUDA_API int pk_system_get_snapshot_f32(pk_system* sys, int first_node, int count, float* x);
 
 /* Tets with world node ids and rest data already computed in the system precision

@@ -322,6 +322,25 @@ class Reference:
         y = np.ascontiguousarray(young, np.float64)
         self.lib.ref_set_tet_young(self.h, body, _ptr(y))
 
+    def add_sphere(self, center, radius, stiffness=1000.0, damping=10.0) -> int:
+        """A CollisionSphereComponent with its connection settings; returns its index."""
+        self.lib.ref_add_sphere.argtypes = [_p, _d, _d, _d, _d, _d, _d]
+        self.lib.ref_add_sphere.restype = _i
+        return self.lib.ref_add_sphere(self.h, *[float(c) for c in center], float(radius), float(stiffness),
+                                       float(damping))
+
+    def set_sphere_target(self, sphere, center):
+        self.lib.ref_sphere_target.argtypes = [_p, _i, _d, _d, _d]
+        self.lib.ref_sphere_target(self.h, sphere, *[float(c) for c in center])
+
+    def add_script(self, callback) -> int:
+        """A ScriptComponent calling `callback` (a ctypes CFUNCTYPE(None, c_void_p, c_void_p))
+        once per frame with the reference world's handle."""
+        self.lib.ref_add_script.argtypes = [_p, _p, _p]
+        self.lib.ref_add_script.restype = _i
+        self._script = callback  # keep the callback alive as long as the world
+        return self.lib.ref_add_script(self.h, C.cast(callback, C.c_void_p), None)
+
     def set_fem_model(self, body, model):
         """TetMeshPhysicsComponent::SetFemModel: 0 linear, 1 corotated, 2 NeoHookean."""
         self.lib.ref_set_fem_model.argtypes = [_p, _i, _i]

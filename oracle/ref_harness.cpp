@@ -27,6 +27,8 @@
 
 #define private public
 #define protected public
+#include "PhysiK/Components/CollisionSphereComponent.h"
+#include "PhysiK/Components/ScriptComponent.h"
 #include "PhysiK/Components/TetMeshPhysicsComponent.h"
 #include "PhysiK/Core/PhysicsConnections/PointConnection.h"
 #include "PhysiK/Core/Solvers/SolverData.h"
@@ -42,6 +44,7 @@ namespace {
 struct Harness {
     World world;
     std::vector<TetMeshPhysicsComponent*> bodies;
+    std::vector<CollisionSphereComponent*> spheres;
     std::unique_ptr<SolverData> dump;
     std::string error;
 };
@@ -123,6 +126,44 @@ __attribute__((visibility("default"))) void ref_set_local_position(void* h, int 
     H(h)->bodies.at(static_cast<std::size_t>(body))
         ->SetLocalCurrentPosition(node, Vec3{static_cast<Real>(x), static_cast<Real>(y), static_cast<Real>(z)});
 }
+
+// A ScriptComponent with its external callback (World::AddComponent,
+// ScriptComponent::SetExternalLogicCallback), as PHYSIK_CreateScriptComponent and
+// PHYSIK_SetScriptComponentCallback do.  Returns 1 on success.
+__attribute__((visibility("default"))) int ref_add_script(void* h, ExternalLogicCallback callback, void* user)
+{
+    auto component = std::make_unique<ScriptComponent>();
+    component->SetExternalLogicCallback(callback, user);
+    return H(h)->world.AddComponent(std::move(component)).IsValid() ? 1 : 0;
+}
+
+// A collision sphere (CollisionSphereComponent::Create + SetConnectionSettings +
+// World::AddComponent, as PHYSIK_CreateCollisionSphereComponent and
+// PHYSIK_SetCollisionSphereConnectionSettings do).  Returns its index, or -1.
+__attribute__((visibility("default"))) int ref_add_sphere(void* h, double x, double y, double z, double radius,
+                                                          double stiffness, double damping)
+{
+    auto sphere = CollisionSphereComponent::Create(
+        Vec3{static_cast<Real>(x), static_cast<Real>(y), static_cast<Real>(z)}, static_cast<Real>(radius));
+    sphere->SetConnectionSettings(static_cast<Real>(stiffness), static_cast<Real>(damping));
+    CollisionSphereComponent* raw = sphere.get();
+    if (!H(h)->world.AddComponent(std::move(sphere)).IsValid()) return -1;
+    H(h)->spheres.push_back(raw);
+    return static_cast<int>(H(h)->spheres.size()) - 1;
+}
+
+// CollisionComponent::SetKinematicTarget with the sphere's transform moved to (x, y, z),
+// as PHYSIK_SetCollisionComponentKinematicTarget does (PhysiKAPI.cpp:1407-1429).
+__attribute__((visibility("default"))) void ref_sphere_target(void* h, int sphere, double x, double y, double z)
+{
+    CollisionSphereComponent* c = H(h)->spheres.at(static_cast<std::size_t>(sphere));
+    Transform target = c->transform;
+    target.position = Vec3{static_cast<Real>(x), static_cast<Real>(y), static_cast<Real>(z)};
+    c->SetKinematicTarget(target);
+}
+
+// The reference world's handle, as the C ABI passes it to scripts.
+__attribute__((visibility("default"))) void* ref_world_handle(void* h) { return static_cast<WorldHandle>(&H(h)->world); }
 
 // TetMeshPhysicsComponent::SetFemModel (FemModel: 0 linear, 1 corotated, 2 NeoHookean).
 __attribute__((visibility("default"))) void ref_set_fem_model(void* h, int body, int model)

@@ -131,6 +131,13 @@ _SIGS = {
     "PHYSIK_GetTetMeshGlobalNodeBeginIndex": (_i, [_p, _H]),
     "PHYSIK_GetTetMeshGlobalNodeCount": (_i, [_p, _H]),
     "PHYSIK_GetTetMeshGlobalNodeIndex": (_i, [_p, _H, _i]),
+    "PHYSIK_CreateCollisionSphereComponent": (_H, [_p, _f, _f, _f, _f]),
+    "PHYSIK_SetCollisionSphereConnectionSettings": (_v, [_p, _H, _f, _f]),
+    "PHYSIK_GetCollisionSphereConnectionSettings": (_v, [_p, _H, _p, _p]),
+    "PHYSIK_SetCollisionComponentKinematicTarget": (_v, [_p, _H, _f, _f, _f]),
+    "PHYSIK_CreateScriptComponent": (_H, [_p]),
+    "PHYSIK_SetScriptComponentCallback": (_v, [_p, _H, _p, _p]),
+    "PHYSIK_ClearScriptComponentCallback": (_v, [_p, _H]),
     "PHYSIK_SetTetMeshLocalCurrentPosition": (_i, [_p, _H, _i, _f, _f, _f]),
     "PHYSIK_GetTetMeshLocalCurrentPosition": (_i, [_p, _H, _i, _p, _p, _p]),
     "PHYSIK_SetTetMeshMaterial": (_v, [_p, _H, C.POINTER(MaterialDesc)]),
@@ -175,6 +182,8 @@ _SIGS = {
     "PHYSIK_B200_Autotune": (_i, [_p, _i, _p]),
     "PHYSIK_B200_GetPcgKernel": (_i, [_p, _p]),
     "PHYSIK_B200_GetPcgStreamForm": (_i, [_p]),
+    "PHYSIK_B200_GetDeviceSystem": (_p, [_p]),
+    "pk_system_sphere_contacts": (_i, [_p, _p, C.c_double, _i, _p, _p]),
     "PHYSIK_B200_SetRefinement": (_i, [_p, _i]),
     "PHYSIK_B200_GetBodyConjugateGradientStats": (_i, [_p, _H, _p, _p, _p, _p]),
     "PHYSIK_B200_GetStream": (_p, [_p]),

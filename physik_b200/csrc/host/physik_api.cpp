@@ -258,6 +258,69 @@ PHYSIK_B200_API int PHYSIK_GetGeneratedTetMeshTetNodeIndex(PhysikGeneratedTetMes
     return 1;
 }
 
+PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateCollisionSphereComponent(PhysikWorldHandle world, float x, float y,
+                                                                            float z, float radius)
+{
+    World* w = AsWorld(world);
+    if (!w) return InvalidHandle();
+    return Guard([&] { return FromHandle(w->AddComponent(CollisionSphereComponent::Create(Vec3{x, y, z}, radius))); },
+                 InvalidHandle());
+}
+
+PHYSIK_B200_API void PHYSIK_SetCollisionSphereConnectionSettings(PhysikWorldHandle world,
+                                                                 PhysikComponentHandle sphereComponent,
+                                                                 float stiffness, float damping)
+{
+    World* w = AsWorld(world);
+    auto* c = w ? dynamic_cast<CollisionSphereComponent*>(w->GetComponent(ToHandle(sphereComponent))) : nullptr;
+    if (c) c->SetConnectionSettings(stiffness, damping);
+}
+
+PHYSIK_B200_API void PHYSIK_GetCollisionSphereConnectionSettings(PhysikWorldHandle world,
+                                                                 PhysikComponentHandle sphereComponent,
+                                                                 float* outStiffness, float* outDamping)
+{
+    World* w = AsWorld(world);
+    auto* c = w ? dynamic_cast<CollisionSphereComponent*>(w->GetComponent(ToHandle(sphereComponent))) : nullptr;
+    if (!c) return;
+    if (outStiffness) *outStiffness = c->GetConnectionStiffness();
+    if (outDamping) *outDamping = c->GetConnectionDamping();
+}
+
+PHYSIK_B200_API void PHYSIK_SetCollisionComponentKinematicTarget(PhysikWorldHandle world,
+                                                                 PhysikComponentHandle component, float x, float y,
+                                                                 float z)
+{
+    World* w = AsWorld(world);
+    auto* c = w ? dynamic_cast<CollisionComponent*>(w->GetComponent(ToHandle(component))) : nullptr;
+    if (!c) return;
+    Transform target = c->transform;
+    target.position = Vec3{x, y, z};
+    c->SetKinematicTarget(target);
+}
+
+PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateScriptComponent(PhysikWorldHandle world)
+{
+    World* w = AsWorld(world);
+    if (!w) return InvalidHandle();
+    return Guard([&] { return FromHandle(w->AddComponent(std::make_unique<ScriptComponent>())); }, InvalidHandle());
+}
+
+PHYSIK_B200_API void PHYSIK_SetScriptComponentCallback(PhysikWorldHandle world, PhysikComponentHandle scriptComponent,
+                                                       PhysikExternalLogicCallback callback, void* userData)
+{
+    World* w = AsWorld(world);
+    auto* c = w ? dynamic_cast<ScriptComponent*>(w->GetComponent(ToHandle(scriptComponent))) : nullptr;
+    if (c) c->SetExternalLogicCallback(reinterpret_cast<ExternalLogicCallback>(callback), userData);
+}
+
+PHYSIK_B200_API void PHYSIK_ClearScriptComponentCallback(PhysikWorldHandle world, PhysikComponentHandle scriptComponent)
+{
+    World* w = AsWorld(world);
+    auto* c = w ? dynamic_cast<ScriptComponent*>(w->GetComponent(ToHandle(scriptComponent))) : nullptr;
+    if (c) c->ClearExternalLogicCallback();
+}
+
 PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateTetMeshComponent(PhysikWorldHandle world,
                                                                      PhysikGeneratedTetMeshHandle mesh)
 {
@@ -679,6 +742,12 @@ PHYSIK_B200_API int PHYSIK_B200_GetPcgStreamForm(PhysikWorldHandle world)
     World* w = AsWorld(world);
     if (!w) return -1;
     return Guard([&] { return w->GetPcgStreamForm(); }, -1);
+}
+
+PHYSIK_B200_API void* PHYSIK_B200_GetDeviceSystem(PhysikWorldHandle world)
+{
+    World* w = AsWorld(world);
+    return w ? static_cast<void*>(w->GetDeviceSystem()) : nullptr;
 }
 
 PHYSIK_B200_API int PHYSIK_B200_SetRefinement(PhysikWorldHandle world, int passes)

@@ -277,6 +277,94 @@ public:
     virtual ~Component() = default;
 };
 
+// ScriptComponent (ScriptComponent.cpp): calls an external callback with the world once
+// per frame, in PreUpdate.
+using ExternalLogicCallback = void (*)(void* world, void* userData);
+class ScriptComponent : public Component {
+public:
+    ComponentExecutionPriority GetExecutionPriority() const override
+    {
+        return ComponentExecutionPriority::ScriptComponent;
+    }
+    void SetExternalLogicCallback(ExternalLogicCallback callback, void* userData)
+    {
+        externalLogicCallback = callback;
+        externalLogicUserData = userData;
+    }
+    void ClearExternalLogicCallback() { SetExternalLogicCallback(nullptr, nullptr); }
+    ExternalLogicCallback GetExternalLogicCallback() const { return externalLogicCallback; }
+    void* GetExternalLogicUserData() const { return externalLogicUserData; }
+    void PreUpdate(World& world, float) override
+    {
+        if (externalLogicCallback) externalLogicCallback(static_cast<void*>(&world), externalLogicUserData);
+    }
+
+private:
+    ExternalLogicCallback externalLogicCallback = nullptr;
+    void* externalLogicUserData = nullptr;
+};
+
+// Transform of a collision component (Transform.h:8-16; the sphere uses its position).
+struct Transform {
+    Vec3 position;
+};
+
+// CollisionComponent (CollisionComponent.h, .cpp): a kinematic target set by the C ABI is
+// applied at the next frame's PreUpdate.
+class CollisionComponent : public Component {
+public:
+    Transform transform;
+    bool generateConnections = true;
+    bool generateEvents = false;
+    bool isSensor = false;
+    float contactStiffness = 1000.0f;
+    float contactDamping = 10.0f;
+
+    void SetKinematicTarget(const Transform& target)
+    {
+        kinematicTarget = target;
+        hasKinematicTarget = true;
+    }
+    bool ConsumeKinematicTarget(Transform& out)
+    {
+        if (!hasKinematicTarget) return false;
+        out = kinematicTarget;
+        hasKinematicTarget = false;
+        return true;
+    }
+    void PreUpdate(World&, float) override
+    {
+        Transform target;
+        if (ConsumeKinematicTarget(target)) transform = target;
+    }
+
+private:
+    bool hasKinematicTarget = false;
+    Transform kinematicTarget;
+};
+
+// CollisionSphereComponent (CollisionSphereComponent.cpp): every substep, each active tet
+// of every active soft body whose centroid lies inside the sphere gets a point connection
+// from its centroid (weights 1/4) to the sphere's surface along the centre-to-centroid
+// direction.  UpdateSystem only registers the request; the world finds the contacts on
+// the device once the substep's state is there (World::AddSphereContacts) and adds the
+// connections in the same order as the reference.
+class CollisionSphereComponent : public CollisionComponent {
+public:
+    static std::unique_ptr<CollisionSphereComponent> Create(const Vec3& position, float radius);
+    ComponentExecutionPriority GetExecutionPriority() const override
+    {
+        return ComponentExecutionPriority::CollisionSphereComponent;
+    }
+    float radius = 0.5f;
+    void SetConnectionSettings(float stiffness, float damping);
+    void SetConnectionStiffness(float stiffness);
+    float GetConnectionStiffness() const { return contactStiffness; }
+    void SetConnectionDamping(float damping);
+    float GetConnectionDamping() const { return contactDamping; }
+    void UpdateSystem(World& world, SolverData& solverData, float dt) override;
+};
+
 class TetMeshComponent : public Component {
 public:
     std::vector<Vec3> restNodePositions;
@@ -469,6 +557,8 @@ public:
     // exist and are active; cleared when the next World::Step ends (those added during a
     // substep, after that substep).
     void AddPointConnection(const PointConnection& connection);
+    // A collision sphere asks for this substep's contacts (CollisionSphereComponent::UpdateSystem).
+    void RequestSphereContacts(const CollisionSphereComponent* sphere) { sphereRequests.push_back(sphere); }
     int GetTransientConnectionCount() const { return static_cast<int>(transientConnections.size()); }
     bool HasValidNodeIndices(const PointConnection& connection) const;
 
@@ -510,6 +600,7 @@ private:
     void CollectContributions(float dt);
     void EnsureScene(bool upload);
     void FlushLocalPositionSnapshots();  // host copies of every stale component snapshot
+    void AddSphereContacts();            // the requested spheres' contacts as point connections
     bool SyncConnections();
     void MarkSubstepConnectionBegin() { firstSubstepConnectionIndex = transientConnections.size(); }
     void ClearSubstepConnections();
@@ -548,6 +639,7 @@ private:
     mutable unsigned lastFlags = 0;
     mutable bool statsPending = false;
     std::uint64_t snapshotGeneration = 0;  // substeps whose start positions the device snapshot held
+    std::vector<const CollisionSphereComponent*> sphereRequests;  // this substep's, in update order
 };
 
 }  // namespace PhysiK

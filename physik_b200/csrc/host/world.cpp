@@ -487,7 +487,7 @@ void BuildHostScene(DeviceScene& sc, const World& w, const std::vector<const Tet
                 sc.tetNodes[4 * g + 2] = t.node2 + base;
                 sc.tetNodes[4 * g + 3] = t.node3 + base;
                 sc.enabled[g] = static_cast<unsigned char>((t.active && rd.volume > T(0) && femImplemented ? 1 : 0) |
-                                                           linearBit);
+                                                           linearBit | (t.active ? 4 : 0));
                 for (int c = 0; c < 3; ++c) {
                     sc.dmInv[9 * g + 3 * c + 0] = static_cast<double>(rd.dm_inv.c[c].x);
                     sc.dmInv[9 * g + 3 * c + 1] = static_cast<double>(rd.dm_inv.c[c].y);
@@ -928,9 +928,104 @@ void World::PostUpdateComponents(float dt)
         if (e.second && e.second->active) e.second->PostUpdate(*this, dt);
 }
 
+// ------------------------------------------------------------------ collision spheres
+std::unique_ptr<CollisionSphereComponent> CollisionSphereComponent::Create(const Vec3& position, float radius)
+{
+    auto c = std::make_unique<CollisionSphereComponent>();
+    c->transform.position = position;
+    c->radius = std::max(0.0f, radius);
+    return c;
+}
+
+namespace {
+float SanitizeConnectionValue(float v) { return std::isfinite(v) ? std::max(0.0f, v) : 0.0f; }
+}  // namespace
+
+void CollisionSphereComponent::SetConnectionSettings(float stiffness, float damping)
+{
+    SetConnectionStiffness(stiffness);
+    SetConnectionDamping(damping);
+}
+void CollisionSphereComponent::SetConnectionStiffness(float stiffness) { contactStiffness = SanitizeConnectionValue(stiffness); }
+void CollisionSphereComponent::SetConnectionDamping(float damping) { contactDamping = SanitizeConnectionValue(damping); }
+
+void CollisionSphereComponent::UpdateSystem(World& world, SolverData&, float)
+{
+    if (!active || radius <= 0.0f) return;
+    if (isSensor || !generateConnections) return;
+    world.RequestSphereContacts(this);
+}
+
+namespace {
+// The contact of CollisionSphereComponent::UpdateSystem and AddPointConnectionFromContact
+// (CollisionSphereComponent.cpp:46-66, 165-188) from a centroid, in the arithmetic T of the
+// state (float as the reference; double for FP64 worlds, rounded to the connection's
+// floats at the end).  Returns false when the penetration is not positive.
+template <class T>
+bool SphereContact(const double* point, const Vec3& center, float radius, float stiffness, float damping,
+                   const int* nodes, PointConnection& out)
+{
+    const T px = T(point[0]), py = T(point[1]), pz = T(point[2]);
+    const T cx = px - T(center.x), cy = py - T(center.y), cz = pz - T(center.z);
+    const T dist = std::sqrt(cx * cx + cy * cy + cz * cz);
+    T nx = T(0), ny = T(0), nz = T(1);  // NormalizeOrFallback
+    if (dist > T(0.00001f)) {
+        nx = cx / dist;
+        ny = cy / dist;
+        nz = cz / dist;
+    }
+    const T depth = T(radius) - dist;
+    if (!(depth > T(0))) return false;
+    out.node0 = nodes[0];
+    out.node1 = nodes[1];
+    out.node2 = nodes[2];
+    out.node3 = nodes[3];
+    out.barycentric = Vec4{0.25f, 0.25f, 0.25f, 0.25f};
+    out.targetPosition = Vec3{static_cast<float>(px + nx * depth), static_cast<float>(py + ny * depth),
+                              static_cast<float>(pz + nz * depth)};
+    out.stiffness = stiffness;
+    out.damping = damping;
+    return true;
+}
+}  // namespace
+
+void World::AddSphereContacts()
+{
+    if (sphereRequests.empty() || !scene || !scene->sys) return;
+    std::vector<int> tets;
+    std::vector<double> points;
+    for (const CollisionSphereComponent* sphere : sphereRequests) {
+        const double center[3] = {sphere->transform.position.x, sphere->transform.position.y,
+                                  sphere->transform.position.z};
+        const int n = pk_system_sphere_contacts(scene->sys, center, sphere->radius, 0, nullptr, nullptr);
+        Check(n < 0 ? n : 0, "sphere_contacts");
+        if (n == 0) continue;
+        tets.resize(static_cast<std::size_t>(n));
+        points.resize(3 * static_cast<std::size_t>(n));
+        Check(pk_system_sphere_contacts(scene->sys, center, sphere->radius, n, tets.data(), points.data()) == n ? 0
+                                                                                                              : PK_ERR_STATE,
+              "sphere_contacts");
+        for (int i = 0; i < n; ++i) {
+            const int t = tets[static_cast<std::size_t>(i)];
+            PointConnection c;
+            const bool ok =
+                precision == Precision::FP64
+                    ? SphereContact<double>(&points[3 * static_cast<std::size_t>(i)], sphere->transform.position,
+                                            sphere->radius, sphere->GetConnectionStiffness(),
+                                            sphere->GetConnectionDamping(), &scene->tetNodes[4 * static_cast<std::size_t>(t)], c)
+                    : SphereContact<float>(&points[3 * static_cast<std::size_t>(i)], sphere->transform.position,
+                                           sphere->radius, sphere->GetConnectionStiffness(),
+                                           sphere->GetConnectionDamping(), &scene->tetNodes[4 * static_cast<std::size_t>(t)], c);
+            if (ok) AddPointConnection(c);
+        }
+    }
+    sphereRequests.clear();
+}
+
 void World::CollectContributions(float dt)
 {
     solverData.ClearTransientState();
+    sphereRequests.clear();
     for (auto& e : orderedComponents)
         if (e.second && e.second->active) e.second->UpdateSystem(*this, solverData, dt);
     if (!solverData.GetNodeForces().empty() || !solverData.GetNodeMasses().empty() ||
@@ -1266,6 +1361,12 @@ void World::RunSubstep(float dt)
         }
         Check(pk_system_set_state_f32(scene->sys, x.data(), v.data()), "set_state");
         deviceStale = false;
+    }
+    // Collision spheres' contacts, found on the device at this substep's positions, join
+    // the point connections (after the frame's own ones, as the reference appends them).
+    if (!sphereRequests.empty()) {
+        AddSphereContacts();
+        EnsureScene(true);
     }
     // Every active physics component syncs its local positions from the world at the start
     // of the substep (TetMeshPhysicsComponent::UpdateSystem, TetMeshPhysicsComponent.cpp:293-300).

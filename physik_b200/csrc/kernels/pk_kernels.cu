@@ -194,6 +194,47 @@ __global__ void __launch_bounds__(256) tet_kernel(AssemblyArgs<Real> A)
     st_rec_rs(rec, w);
 }
 
+// ------------------------------------------------------------------ sphere contacts
+// CollisionSphereComponent::UpdateSystem (CollisionSphereComponent.cpp:112-190): a tet
+// whose centroid p = ((x0 w + x1 w) + x2 w) + x3 w (w = 1/4) lies strictly inside the
+// sphere, |p - c| < radius, becomes a contact.  The arithmetic rounds each operation once,
+// as the reference's Vec3 code does (no contraction into fused multiply-adds).  Only tets
+// marked active (flag bit 2) count.  Contacts are appended in any order; the host sorts
+// them by tet.
+__device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
+
+template <class Real>
+__global__ void sphere_contact_kernel(const int4* __restrict__ nodes, const unsigned char* __restrict__ flags,
+                                      const Real* __restrict__ x, int tet_count, Real cx, Real cy, Real cz,
+                                      Real radius, int max_out, int* count, int* out_tet, Real* out_point)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tet_count || !(__ldg(flags + t) & 4u)) return;
+    const int4 n = __ldg(nodes + t);
+    const int nd[4] = {n.x, n.y, n.z, n.w};
+    const Real w = Real(0.25);
+    Real p[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        Real acc = rn_mul(__ldg(x + 3 * (size_t)nd[0] + a), w);
+#pragma unroll
+        for (int k = 1; k < 4; ++k) acc = rn_add(acc, rn_mul(__ldg(x + 3 * (size_t)nd[k] + a), w));
+        p[a] = acc;
+    }
+    const Real dx = rn_add(p[0], -cx), dy = rn_add(p[1], -cy), dz = rn_add(p[2], -cz);
+    const Real d2 = rn_add(rn_add(rn_mul(dx, dx), rn_mul(dy, dy)), rn_mul(dz, dz));
+    if (!(sqrt(d2) < radius)) return;
+    const int slot = atomicAdd(count, 1);
+    if (slot >= max_out) return;
+    out_tet[slot] = t;
+    out_point[3 * (size_t)slot] = p[0];
+    out_point[3 * (size_t)slot + 1] = p[1];
+    out_point[3 * (size_t)slot + 2] = p[2];
+}
+
 template <class Real>
 __global__ void tet_pack_kernel(const Real* __restrict__ dm_inv, const Real* __restrict__ params, Real* rec,
                                 int tet_count)
@@ -506,6 +547,18 @@ cudaError_t launch_tet_pack(const Real* dm_inv, const Real* params, Real* rec, i
 }
 
 template <class Real>
+cudaError_t launch_sphere_contacts(const int* nodes, const unsigned char* flags, const Real* x, int tet_count,
+                                   const Real* center, Real radius, int max_out, int* count, int* out_tet,
+                                   Real* out_point, cudaStream_t stream)
+{
+    if (tet_count <= 0) return cudaSuccess;
+    sphere_contact_kernel<Real><<<(tet_count + 255) / 256, 256, 0, stream>>>(
+        reinterpret_cast<const int4*>(nodes), flags, x, tet_count, center[0], center[1], center[2], radius, max_out,
+        count, out_tet, out_point);
+    return cudaGetLastError();
+}
+
+template <class Real>
 cudaError_t launch_conn_kernel(const AssemblyArgs<Real>& args, cudaStream_t stream)
 {
     if (args.conn_count <= 0) return cudaSuccess;
@@ -554,6 +607,10 @@ template cudaError_t launch_tet_pack<float>(const float*, const float*, float*, 
 template cudaError_t launch_conn_kernel<float>(const AssemblyArgs<float>&, cudaStream_t);
 template cudaError_t launch_conn_kernel<double>(const AssemblyArgs<double>&, cudaStream_t);
 template cudaError_t launch_tet_pack<double>(const double*, const double*, double*, int, cudaStream_t);
+template cudaError_t launch_sphere_contacts<float>(const int*, const unsigned char*, const float*, int, const float*,
+                                                   float, int, int*, int*, float*, cudaStream_t);
+template cudaError_t launch_sphere_contacts<double>(const int*, const unsigned char*, const double*, int,
+                                                    const double*, double, int, int*, int*, double*, cudaStream_t);
 template cudaError_t launch_row_kernel<float>(const AssemblyArgs<float>&, int, cudaStream_t);
 template cudaError_t launch_row_kernel<double>(const AssemblyArgs<double>&, int, cudaStream_t);
 template cudaError_t launch_spmv_kernel<float>(const BsrView<float>&, const float*, float*, cudaStream_t);

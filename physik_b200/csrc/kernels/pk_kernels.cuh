@@ -407,6 +407,10 @@ cudaError_t launch_tet_kernel(const AssemblyArgs<Real>& args, bool fp64_polar_fa
 // The static part of the tet records (DmInv and the material of every tet).
 template <class Real>
 cudaError_t launch_tet_pack(const Real* dm_inv, const Real* params, Real* rec, int tet_count, cudaStream_t stream);
+template <class Real>
+cudaError_t launch_sphere_contacts(const int* nodes, const unsigned char* flags, const Real* x, int tet_count,
+                                   const Real* center, Real radius, int max_out, int* count, int* out_tet,
+                                   Real* out_point, cudaStream_t stream);
 // Per point connection, before the row kernel: its weighted point and velocity, whether it
 // applies this step, and its force (args.conn_eval).
 template <class Real>

@@ -259,6 +259,7 @@ struct pk_system {
     int graph_kernels = 0;
     // nodes; snap_x: positions at the start of the last substep (pk_system_snapshot_positions)
     DevBuf x, v, mass, node_to_dyn, snap_x;
+    DevBuf contact_count, contact_tet, contact_point;  // pk_system_sphere_contacts
     bool have_snapshot = false;
     // tets
     DevBuf tet_nodes, tet_enabled, dm_inv, tet_params, tet_rec;
@@ -1300,6 +1301,64 @@ PKCUDA_API int pk_system_snapshot_positions(pk_system* s)
     if (bytes) PK_CHECK(cudaMemcpyAsync(s->snap_x.p, s->x.p, bytes, cudaMemcpyDeviceToDevice, s->stream));
     s->have_snapshot = true;
     return PK_OK;
+}
+
+PKCUDA_API int pk_system_sphere_contacts(pk_system* s, const double* center, double radius, int max_contacts,
+                                         int* tets, double* points)
+{
+    if (!s || !center || max_contacts < 0 || (max_contacts > 0 && (!tets || !points)))
+        return fail(PK_ERR_ARG, "sphere_contacts");
+    if (!s->have_nodes || !s->have_tets) return fail(PK_ERR_STATE, "sphere_contacts before nodes and tets");
+    PK_CHECK(cudaSetDevice(s->device));
+    const int T = s->tet_count;
+    if (T == 0) return 0;
+    PK_CHECK(s->contact_count.ensure(sizeof(int)));
+    PK_CHECK(s->contact_tet.ensure(sizeof(int) * static_cast<size_t>(T)));
+    PK_CHECK(s->contact_point.ensure(3 * s->rsize() * static_cast<size_t>(T)));
+    PK_CHECK(cudaMemsetAsync(s->contact_count.p, 0, sizeof(int), s->stream));
+    if (s->precision == PK_PREC_FP64) {
+        PK_CHECK(pk::launch_sphere_contacts<double>(s->tet_nodes.as<int>(), s->tet_enabled.as<unsigned char>(),
+                                                    s->x.as<double>(), T, center, radius, T,
+                                                    s->contact_count.as<int>(), s->contact_tet.as<int>(),
+                                                    s->contact_point.as<double>(), s->stream));
+    } else {
+        const float c[3] = {static_cast<float>(center[0]), static_cast<float>(center[1]),
+                            static_cast<float>(center[2])};
+        PK_CHECK(pk::launch_sphere_contacts<float>(s->tet_nodes.as<int>(), s->tet_enabled.as<unsigned char>(),
+                                                   s->x.as<float>(), T, c, static_cast<float>(radius), T,
+                                                   s->contact_count.as<int>(), s->contact_tet.as<int>(),
+                                                   s->contact_point.as<float>(), s->stream));
+    }
+    int n = 0;
+    PK_CHECK(cudaMemcpyAsync(&n, s->contact_count.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    n = std::min(n, T);
+    if (n > max_contacts) return n;  // the caller's arrays are too small: only the count
+    std::vector<int> t(static_cast<size_t>(n));
+    std::vector<double> p(3 * static_cast<size_t>(n));
+    if (n > 0) {
+        PK_CHECK(cudaMemcpyAsync(t.data(), s->contact_tet.p, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
+        if (s->precision == PK_PREC_FP64) {
+            PK_CHECK(cudaMemcpyAsync(p.data(), s->contact_point.p, 3 * sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                     s->stream));
+            PK_CHECK(cudaStreamSynchronize(s->stream));
+        } else {
+            std::vector<float> pf(3 * static_cast<size_t>(n));
+            PK_CHECK(cudaMemcpyAsync(pf.data(), s->contact_point.p, 3 * sizeof(float) * n, cudaMemcpyDeviceToHost,
+                                     s->stream));
+            PK_CHECK(cudaStreamSynchronize(s->stream));
+            for (size_t i = 0; i < pf.size(); ++i) p[i] = pf[i];
+        }
+    }
+    // ascending tet order (the reference visits tets in order)
+    std::vector<int> order(static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return t[a] < t[b]; });
+    for (int i = 0; i < n; ++i) {
+        tets[i] = t[order[i]];
+        for (int a = 0; a < 3; ++a) points[3 * (size_t)i + a] = p[3 * (size_t)order[i] + a];
+    }
+    return n;
 }
 
 PKCUDA_API int pk_system_get_snapshot_f32(pk_system* s, int first_node, int count, float* x)

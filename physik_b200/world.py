@@ -113,6 +113,15 @@ class SimWorld:
         return int(self.X.PHYSIK_SetTetMeshLocalCurrentPosition(self.h, self.components[body], int(node),
                                                                 *[float(c) for c in p]))
 
+    def add_sphere(self, center, radius, stiffness=None, damping=None):
+        """PHYSIK_CreateCollisionSphereComponent (+ its connection settings when given)."""
+        h = self.X.PHYSIK_CreateCollisionSphereComponent(self.h, *[float(c) for c in center], float(radius))
+        if not h.valid():
+            raise PhysikError("PHYSIK_CreateCollisionSphereComponent failed: " + self.error())
+        if stiffness is not None:
+            self.X.PHYSIK_SetCollisionSphereConnectionSettings(self.h, h, float(stiffness), float(damping))
+        return h
+
     def add_point_connection(self, nodes, weights, target, stiffness: float, damping: float = 0.0):
         """PHYSIK_AddPointConnection: a spring from sum_i weights[i] x(nodes[i]) to `target`,
         kept until the end of the next step."""

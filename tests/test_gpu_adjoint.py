@@ -5,7 +5,8 @@ reference, checked three ways:
   with FP64 forward rollouts (the FP64 GPU path, itself checked against the FP64 oracle
   to 1e-12 per step), epsilon = 1e-3; relative error <= 1e-4 (the most sensitive
   coordinate of the 60-step rollout, where elements are crushed nearly flat and the
-  loss is far from quadratic at 1e-3, with epsilon = 1e-5);
+  loss is far from quadratic at 1e-3, with epsilon = 1e-5), each coordinate relative to
+  its own finite difference;
 * against an FP64 CPU reference gradient written independently in numpy on top of the
   FP64 oracle's assembled systems (tests/adjoint_harness.py), all coordinates, along the
   same trajectory (relative 1e-6);
@@ -93,13 +94,14 @@ def test_adjoint_small_box_against_fd_and_cpu():
     free = ~body.pinned
     assert np.linalg.norm(g_theta - c_theta) <= 1e-6 * np.linalg.norm(c_theta)
     assert np.linalg.norm(g_v0[free] - c_v0[free]) <= 1e-6 * np.linalg.norm(c_v0[free])
+    # Relative to each coordinate's own finite difference (no floor).
     for i in range(0, T, max(1, T // 8)):
         fd = fd_theta(world, young, x0, v0, steps, x_target, i)
-        assert abs(g_theta[i] - fd) <= 1e-4 * max(abs(fd), 1e-3 * np.abs(c_theta).max()), (i, g_theta[i], fd)
+        assert abs(g_theta[i] - fd) <= 1e-4 * abs(fd), (i, g_theta[i], fd)
     nodes = np.nonzero(free)[0]
     for node in nodes[:: max(1, len(nodes) // 4)]:
         fd = fd_v0(world, young, x0, v0, steps, x_target, node, 2)
-        assert abs(g_v0[node, 2] - fd) <= 1e-4 * max(abs(fd), 1e-3 * np.abs(c_v0).max()), (node, g_v0[node, 2], fd)
+        assert abs(g_v0[node, 2] - fd) <= 1e-4 * abs(fd), (node, g_v0[node, 2], fd)
 
 
 def test_adjoint_beam32_rollout_workload():
@@ -123,19 +125,16 @@ def test_adjoint_beam32_rollout_workload():
     # Central differences on 16 random coordinates of (log E, v0).
     rng = np.random.default_rng(16)
     free_nodes = np.nonzero(free)[0]
-    worst = 0.0
+    errors = []
     for c in range(16):
         if c % 2 == 0:
             i = int(rng.integers(0, T))
             fd, ad = fd_theta(world, young, x0, v0, steps, x_target, i), g_theta[i]
-            scale = np.abs(c_theta).max()
         else:
             node, comp = int(rng.choice(free_nodes)), int(rng.integers(0, 3))
             fd, ad = fd_v0(world, young, x0, v0, steps, x_target, node, comp), g_v0[node, comp]
-            scale = np.abs(c_v0[free]).max()
-        err = abs(ad - fd) / max(abs(fd), 1e-3 * scale)
-        worst = max(worst, err)
-    assert worst <= 1e-4, worst
+        errors.append((abs(ad - fd) / abs(fd), ad, fd))  # relative to the coordinate's own difference
+    assert max(e[0] for e in errors) <= 1e-4, errors
     # The most sensitive coordinate (a tet at the clamped end that is nearly crushed flat,
     # where the rollout is strongly nonlinear): central differences converge to the
     # adjoint as the step shrinks; at 1e-5 they agree to 1e-4.

@@ -9,8 +9,8 @@ float -> double (oracle/_ref/libphysik_ref_f64.so).  Every input is a float32 va
 ABI takes floats): dt 1/64, gravity -9.8125, Poisson's ratio 0.25, CG tolerance 2^-20.
 
 Tolerances (relative, 2-norm): FP64 system blocks and rhs 1e-12 of their largest entry,
-delta-v 1e-8; FP64 steps positions 1e-12, velocities 1e-8; mixed steps positions 1e-5 (the
-workload's bar), velocities 2e-3.
+delta-v 1e-8; FP64 steps positions 1e-14, velocities 1e-12; mixed steps positions 3e-7,
+velocities 2e-4 (about ten times the step errors measured without connections).
 """
 import numpy as np
 import pytest
@@ -99,7 +99,7 @@ def test_connection_system_matches_reference_fp64():
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_connection_steps_match_reference(precision):
     """Teacher-forced steps, the connections added again before each (frame lifetime)."""
-    tx, tv, ti = {"fp64": (1e-12, 1e-8, 1), "mixed": (1e-5, 2e-3, 3)}[precision]
+    tx, tv, ti = {"fp64": (1e-14, 1e-12, 1), "mixed": (3e-7, 2e-4, 1)}[precision]
     scene = exact_scene()
     gpu = SimWorld(scene, precision=precision)
     ref = po.Reference(scene, "f64")

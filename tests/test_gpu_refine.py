@@ -6,8 +6,8 @@ No counterpart in the reference (it solves once, in FP32).  Checked here, on the
   here in FP64 from the assembled system (SparseBlockMatrix::Multiply semantics,
   src/Math/SparseBlockMatrix.cpp:209-268), meets the reference's stopping target
   r^T M^-1 r <= tol^2 b^T M^-1 b (ConjugateGradientSolver.cpp:114-241), the total CG
-  iterations stay within the step's budget, and positions match the FP64 oracle to the
-  mixed-precision bar (1e-5);
+  iterations stay within the step's budget, and positions match the FP64 oracle to 3e-7
+  (ten times the mixed step's measured position error);
 * at the iteration cap (the 64x16x16 beam) no budget is left: the refined step equals
   the plain one;
 * FP64 worlds ignore it, and a world with graph capture on still steps (refined steps
@@ -57,7 +57,7 @@ def test_refined_step_meets_the_true_residual_target():
         assert st["flags"] & L.FLAG_INTEGRATED, hex(st["flags"])
         assert st["iterations"] <= scene.max_iterations
         x, _ = gpu.state(f64=True)
-        assert rel(x, ora.x) <= 1e-5
+        assert rel(x, ora.x) <= 3e-7
         if st["converged"]:
             rho, rho0 = true_residual(gpu)
             assert rho <= tol * tol * rho0 * (1 + 1e-3), (rho, tol * tol * rho0)

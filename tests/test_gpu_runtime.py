@@ -66,7 +66,7 @@ def test_each_pcg_kernel_matches_oracle(kernel, monkeypatch):
         gpu.step()
         ora.step()
         x, v = gpu.state(f64=True)
-        assert rel(x, ora.x) <= 1e-12 and rel(v, ora.v) <= 1e-8
+        assert rel(x, ora.x) <= 1e-14 and rel(v, ora.v) <= 1e-12
         assert abs(gpu.cg_stats()["iterations"] - ora.last_stats()["iterations"]) <= 1
 
 
@@ -81,7 +81,7 @@ def test_autotuned_choice_matches_oracle():
     gpu.step()
     ora.step()
     x, v = gpu.state(f64=True)
-    assert rel(x, ora.x) <= 1e-12 and rel(v, ora.v) <= 1e-8
+    assert rel(x, ora.x) <= 1e-14 and rel(v, ora.v) <= 1e-12
 
 
 def test_autotuned_batched_matches_untuned():

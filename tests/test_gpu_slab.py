@@ -1,16 +1,18 @@
 """The part-resident ("slab") PCG kernel on the GPU, against the oracle and the other kernels.
 
-The kernel keeps each part's search directions in shared memory and streams full
-symmetric rows; it runs wherever the storage is FP32 (FP32 and mixed precision) and the
-parts' windows fit.  Checked here:
+The kernel keeps each part's search directions in shared memory and streams the matrix as
+full symmetric rows or, by default where the layout fits, in the symmetric form (each
+block inside a sub-part once); it runs wherever the storage is FP32 (FP32 and mixed
+precision) and the parts' windows fit.  Tolerances are about ten times the errors measured
+on a B200.  Checked here:
 
 * it is the kernel the automatic choice picks for FP32-storage worlds, with one block per
   part, and not for FP64;
 * one mixed-precision step equals the FP64 oracle's step (the reference's CPU solve in
-  double, teacher-forced from the same state) within the mixed-precision bar (positions
-  1e-5 relative), on a box cut into a few parts, on the 64x16x16 beam cut into one part
+  double, teacher-forced from the same state) to positions 3e-7 and velocities 2e-4
+  (measured 3e-8 / 1.9e-5), on a box cut into a few parts, on the 64x16x16 beam cut into one part
   per SM (halos on every side), and on a two-body world;
-* FP32 steps follow the FP32 reference restatement within FP32 rounding;
+* FP32 steps follow the FP32 reference restatement (positions 3e-7, velocities 2.5e-5);
 * it agrees with the ring-staged kernel on the same step (both FP32 storage; they differ
   only in the order of sums);
 * the solve is deterministic: two worlds stepped alike are bit-identical, and a graph
@@ -65,9 +67,9 @@ def test_slab_mixed_matches_fp64_oracle(make):
         x, v = gpu.state(f64=True)
         st = gpu.cg_stats()
         assert st["flags"] & L.FLAG_INTEGRATED, hex(st["flags"])
-        assert rel(x, ora.x) <= 1e-5
-        assert rel(v, ora.v) <= 2e-3
-        assert abs(st["iterations"] - ora.last_stats()["iterations"]) <= 3
+        assert rel(x, ora.x) <= 3e-7
+        assert rel(v, ora.v) <= 2e-4
+        assert abs(st["iterations"] - ora.last_stats()["iterations"]) <= 1
 
 
 def test_slab_beam64_uses_one_block_per_part():
@@ -87,9 +89,9 @@ def test_slab_fp32_follows_fp32_reference():
         ora.step()
         x, v = gpu.state(f64=True)
         assert gpu.pcg_kernel()[0] == "slab"
-        assert rel(x, ora.x) <= 1e-6
-        assert rel(v, ora.v) <= 2e-3
-        assert abs(gpu.cg_stats()["iterations"] - ora.last_stats()["iterations"]) <= 3
+        assert rel(x, ora.x) <= 3e-7
+        assert rel(v, ora.v) <= 2.5e-5
+        assert abs(gpu.cg_stats()["iterations"] - ora.last_stats()["iterations"]) <= 1
 
 
 def test_slab_agrees_with_ring_kernel(monkeypatch):
@@ -103,8 +105,8 @@ def test_slab_agrees_with_ring_kernel(monkeypatch):
     assert ring.pcg_kernel()[0] == "ring"
     xs, vs = slab.state(f64=True)
     xr, vr = ring.state(f64=True)
-    assert rel(xs, xr) <= 1e-6
-    assert rel(vs, vr) <= 1e-3
+    assert rel(xs, xr) <= 3e-7
+    assert rel(vs, vr) <= 2e-4
     assert abs(slab.cg_stats()["iterations"] - ring.cg_stats()["iterations"]) <= 2
 
 
@@ -156,9 +158,9 @@ def test_stream_forms_follow_fp64_oracle(make, form, monkeypatch):
         x, v = gpu.state(f64=True)
         st = gpu.cg_stats()
         assert st["flags"] & L.FLAG_INTEGRATED, hex(st["flags"])
-        assert rel(x, ora.x) <= 1e-5
-        assert rel(v, ora.v) <= 2e-3
-        assert abs(st["iterations"] - ora.last_stats()["iterations"]) <= 3
+        assert rel(x, ora.x) <= 3e-7
+        assert rel(v, ora.v) <= 2e-4
+        assert abs(st["iterations"] - ora.last_stats()["iterations"]) <= 1
 
 
 def test_stream_forms_agree_and_sym_is_the_default(monkeypatch):
@@ -171,8 +173,8 @@ def test_stream_forms_agree_and_sym_is_the_default(monkeypatch):
     full.step()
     xa, va = auto.state(f64=True)
     xf, vf = full.state(f64=True)
-    assert rel(xa, xf) <= 1e-6
-    assert rel(va, vf) <= 1e-3
+    assert rel(xa, xf) <= 3e-7
+    assert rel(va, vf) <= 2e-4
     assert abs(auto.cg_stats()["iterations"] - full.cg_stats()["iterations"]) <= 2
 
 
@@ -203,5 +205,5 @@ def test_sym_form_fp32_follows_fp32_reference(monkeypatch):
         ora.step()
         x, v = gpu.state(f64=True)
         assert gpu.pcg_stream_form() == "sym"
-        assert rel(x, ora.x) <= 1e-6
-        assert rel(v, ora.v) <= 2e-3
+        assert rel(x, ora.x) <= 3e-7
+        assert rel(v, ora.v) <= 2.5e-5
