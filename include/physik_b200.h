@@ -114,9 +114,10 @@ PHYSIK_B200_API int PHYSIK_GetTetMeshGlobalNodeIndex(PhysikWorldHandle world, Ph
 /* PHYSIK_SetTetMeshLocalCurrentPosition / PHYSIK_GetTetMeshLocalCurrentPosition
  * PhysiKAPI.h:236-251, PhysiKAPI.cpp:992-1053: a tet mesh's own copy of its node
  * positions (TetMeshComponent::nodePositions).  A physics mesh's copy is the world's
- * positions at the start of the last substep it took part in (creation positions before
- * its first step); Set writes that copy only, not the world's node, and the next substep
- * overwrites it.  Return 1, or 0 for an invalid world, mesh, index or NULL out-pointer. */
+ * positions at the end of the last PHYSIK_Step (dt > 0) it took part in (its creation
+ * positions before that); Set writes that copy only, not the world's node, and the next
+ * step overwrites it.  Return 1, or 0 for an invalid world, mesh, index or NULL
+ * out-pointer. */
 PHYSIK_B200_API int PHYSIK_SetTetMeshLocalCurrentPosition(PhysikWorldHandle world, PhysikComponentHandle tetMesh,
                                                           int localNodeIndex, float x, float y, float z);
 PHYSIK_B200_API int PHYSIK_GetTetMeshLocalCurrentPosition(PhysikWorldHandle world, PhysikComponentHandle tetMesh,

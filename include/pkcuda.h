@@ -115,9 +115,9 @@ PKCUDA_API int pk_system_set_state_f64(pk_system* sys, const double* x, const do
 PKCUDA_API int pk_system_get_state_f32(pk_system* sys, float* x, float* v);
 PKCUDA_API int pk_system_get_state_f64(pk_system* sys, double* x, double* v);
 /* Copies the node positions, on the device and in stream order, into a snapshot buffer
- * (the host calls it at the start of every substep: TetMeshPhysicsComponent's
- * SyncCurrentPositionsFromWorld, TetMeshPhysicsComponent.cpp:234-252, keeps the positions
- * a component's GetLocalCurrentPosition returns, TetMeshComponent.cpp:113-122).
+ * (the host calls it at the end of every frame: TetMeshPhysicsComponent::PostUpdate's
+ * SyncCurrentPositionsFromWorld, TetMeshPhysicsComponent.cpp:234-252, 356-363, keeps the
+ * positions a component's GetLocalCurrentPosition returns, TetMeshComponent.cpp:113-122).
  * pk_system_get_snapshot_f32 reads nodes [first_node, first_node + count) of the last
  * snapshot (3 floats each) and waits for the stream. */
 PKCUDA_API int pk_system_snapshot_positions(pk_system* sys);

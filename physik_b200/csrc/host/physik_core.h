@@ -445,9 +445,9 @@ public:
 
     // Bumped whenever rest data, material or tet activity changes.
     std::uint64_t version = 1;
-    // nodePositions is the world's positions at the start of the last substep in which
-    // this component was active (SyncCurrentPositionsFromWorld).  The device keeps that
-    // snapshot; the host copy is refreshed on access: snapshotWanted is the world's
+    // nodePositions is the world's positions at the end of the last frame in which this
+    // component was active (SyncCurrentPositionsFromWorld in PostUpdate).  The device keeps
+    // that snapshot; the host copy is refreshed on access: snapshotWanted is the world's
     // snapshot generation this component's copy should show, snapshotLoaded the one it
     // holds.
     std::uint64_t snapshotWanted = 0, snapshotLoaded = 0;
@@ -587,6 +587,7 @@ public:
     // Brings a component's nodePositions up to the snapshot of the last substep it took part
     // in (TetMeshPhysicsComponent::SyncCurrentPositionsFromWorld, done lazily).
     void RefreshLocalPositions(TetMeshPhysicsComponent& component) const;
+    std::uint64_t GetSnapshotGeneration() const { return snapshotGeneration; }
     void MarkTopologyDirty() { ++topologyVersion; }
     std::uint64_t GetTopologyVersion() const { return topologyVersion; }
 
@@ -601,6 +602,7 @@ private:
     void EnsureScene(bool upload);
     void FlushLocalPositionSnapshots();  // host copies of every stale component snapshot
     void AddSphereContacts();            // the requested spheres' contacts as point connections
+    void SnapshotPositions();            // the frame's end positions for the components' copies
     bool SyncConnections();
     void MarkSubstepConnectionBegin() { firstSubstepConnectionIndex = transientConnections.size(); }
     void ClearSubstepConnections();

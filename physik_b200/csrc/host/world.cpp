@@ -335,7 +335,11 @@ void TetMeshPhysicsComponent::UpdateSystem(World&, SolverData& solverData, float
     solverData.AddFemBody(this);
 }
 
-void TetMeshPhysicsComponent::PostUpdate(World& world, float dt) { TetMeshComponent::PostUpdate(world, dt); }
+void TetMeshPhysicsComponent::PostUpdate(World& world, float dt)
+{
+    if (dt > 0.0f) snapshotWanted = world.GetSnapshotGeneration();  // SyncCurrentPositionsFromWorld, lazily
+    TetMeshComponent::PostUpdate(world, dt);
+}
 
 // ------------------------------------------------------------------ SolverData
 void SolverData::Clear()
@@ -1368,21 +1372,6 @@ void World::RunSubstep(float dt)
         AddSphereContacts();
         EnsureScene(true);
     }
-    // Every active physics component syncs its local positions from the world at the start
-    // of the substep (TetMeshPhysicsComponent::UpdateSystem, TetMeshPhysicsComponent.cpp:293-300).
-    // The device copies the positions aside; a component's host copy is read from there
-    // on access.  A component that sits this substep out keeps its older snapshot, so it
-    // is fetched before the device copy is overwritten.
-    for (auto& e : orderedComponents) {
-        auto* c = dynamic_cast<TetMeshPhysicsComponent*>(e.second);
-        if (c && !c->active && c->snapshotLoaded != c->snapshotWanted) RefreshLocalPositions(*c);
-    }
-    Check(pk_system_snapshot_positions(scene->sys), "snapshot_positions");
-    ++snapshotGeneration;
-    for (auto& e : orderedComponents) {
-        auto* c = dynamic_cast<TetMeshPhysicsComponent*>(e.second);
-        if (c && c->active) c->snapshotWanted = snapshotGeneration;
-    }
     if (scene->dynCount == 0) {
         // No dynamic node: PrecomputeImplicitSolve fails and nothing moves.
         if (solverMode == SolverMode::ImplicitEuler) lastConjugateGradientResult = ConjugateGradientResult{};
@@ -1439,8 +1428,25 @@ void World::Step(float frameDt)
         RunSubstep(dt);
         ClearSubstepConnections();
     }
+    SnapshotPositions();
     PostUpdateComponents(frameDt);
     ClearFrameConnections();
+}
+
+// Every active physics component copies the world's positions into its own at the end of
+// a frame (TetMeshPhysicsComponent::PostUpdate, TetMeshPhysicsComponent.cpp:356-363).  The
+// device copies the positions aside and a component's host copy is read from there on
+// access (RefreshLocalPositions); a component that sits the frame out keeps its older copy,
+// so it is fetched before the device copy is overwritten.
+void World::SnapshotPositions()
+{
+    if (!scene || !scene->sys || !scene->uploaded) return;
+    for (auto& e : orderedComponents) {
+        auto* c = dynamic_cast<TetMeshPhysicsComponent*>(e.second);
+        if (c && !c->active && c->snapshotLoaded != c->snapshotWanted) RefreshLocalPositions(*c);
+    }
+    Check(pk_system_snapshot_positions(scene->sys), "snapshot_positions");
+    ++snapshotGeneration;
 }
 
 }  // namespace PhysiK

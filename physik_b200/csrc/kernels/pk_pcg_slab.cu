@@ -282,10 +282,14 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     // position and both named barriers, whatever happened (a wait that gave up only
     // empties its tile), so the barriers always complete.
     auto phase_a_sym = [&](Acc& dq, int& qbad) {
+        // Two lanes per row: the group's 128 threads cover a whole tile (kSymRows rows) at
+        // once; each lane takes every other entry of its row.
+        constexpr int LS = 2;
         const float* wv = win;
         const int wmax = max(wn - 1, 0);
         const unsigned gbar = 1u + (unsigned)group;  // named barrier of this group (0 is __syncthreads)
-        const int row_in_pass = ((warp % kSlabGroupWarps) * 32 + lane) / LPR;
+        const int sr = ((warp % kSlabGroupWarps) * 32 + lane) / LS;  // tile row of this lane
+        const int ls = lane % LS;
         for (unsigned p = ring + (unsigned)group; p < ring + (unsigned)ntiles; p += kSlabGroups) {
             const int s = (int)(p % S);
             const unsigned u = p / S;
@@ -301,105 +305,82 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
             const float* vals = reinterpret_cast<const float*>(st + kSymHeaderBytes);
             const unsigned short* lcol = reinterpret_cast<const unsigned short*>(st + kSymHeaderBytes + 36 * ne);
             const unsigned short* lslot = lcol + ne;
-            V3<float> accs[2];
+            const bool valid = sr < rows;
+            int e0 = 0, e1 = 0;
+            unsigned lb0 = 0u, lbn = 0u;
+            V3<float> dr{0.f, 0.f, 0.f};
+            if (valid) {
+                e0 = min((int)roff[sr], ne);
+                e1 = min((int)roff[sr + 1], ne);
+                lb0 = lbase[sr];
+                lbn = ((unsigned)lbase[sr + 1] - lb0) & (unsigned)(kSymRingSlots - 1);
+                const int li = min(d.z + sr, wmax);
+                dr = V3<float>{wv[3 * li], wv[3 * li + 1], wv[3 * li + 2]};
+            }
+            V3<float> acc{0.f, 0.f, 0.f};
+            constexpr int kEntries = 4;
+            for (int j0 = e0 + ls; j0 < e1; j0 += kEntries * LS) {
+                int jj[kEntries];
+                bool live[kEntries];
 #pragma unroll
-            for (int pass = 0; pass < 2; ++pass) {
-                const int sr = pass * kSlabRows + row_in_pass;
-                const bool valid = sr < rows;
-                int e0 = 0, e1 = 0;
-                V3<float> dr{0.f, 0.f, 0.f};
-                if (valid) {
-                    e0 = min((int)roff[sr], ne);
-                    e1 = min((int)roff[sr + 1], ne);
-                    const int li = min(d.z + sr, wmax);
-                    dr = V3<float>{wv[3 * li], wv[3 * li + 1], wv[3 * li + 2]};
+                for (int q = 0; q < kEntries; ++q) {
+                    jj[q] = j0 + q * LS;
+                    live[q] = jj[q] < e1;
+                    if (!live[q]) jj[q] = j0;
                 }
-                V3<float> acc{0.f, 0.f, 0.f};
-                constexpr int kEntries = 4;
-                for (int j0 = e0 + sub; j0 < e1; j0 += kEntries * LPR) {
-                    int jj[kEntries];
-                    bool live[kEntries];
+                float xv[kEntries][3], bv[kEntries][9];
+                unsigned sl[kEntries];
 #pragma unroll
-                    for (int q = 0; q < kEntries; ++q) {
-                        jj[q] = j0 + q * LPR;
-                        live[q] = jj[q] < e1;
-                        if (!live[q]) jj[q] = j0;
-                    }
-                    float xv[kEntries][3], bv[kEntries][9];
-                    unsigned sl[kEntries];
+                for (int q = 0; q < kEntries; ++q) {
+                    const int c = 3 * min((int)lcol[jj[q]], wmax);
+                    xv[q][0] = wv[c];
+                    xv[q][1] = wv[c + 1];
+                    xv[q][2] = wv[c + 2];
+                    sl[q] = lslot[jj[q]];
 #pragma unroll
-                    for (int q = 0; q < kEntries; ++q) {
-                        const int c = 3 * min((int)lcol[jj[q]], wmax);
-                        xv[q][0] = wv[c];
-                        xv[q][1] = wv[c + 1];
-                        xv[q][2] = wv[c + 2];
-                        sl[q] = lslot[jj[q]];
+                    for (int e = 0; e < 9; ++e) bv[q][e] = vals[9 * jj[q] + e];
+                }
 #pragma unroll
-                        for (int e = 0; e < 9; ++e) bv[q][e] = vals[9 * jj[q] + e];
-                    }
-#pragma unroll
-                    for (int q = 0; q < kEntries; ++q) {
-                        // Column-major block: element (i, c) is v[3c + i].
-                        const float* v = bv[q];
-                        if (live[q]) {
-                            acc.x += v[0] * xv[q][0] + v[3] * xv[q][1] + v[6] * xv[q][2];
-                            acc.y += v[1] * xv[q][0] + v[4] * xv[q][1] + v[7] * xv[q][2];
-                            acc.z += v[2] * xv[q][0] + v[5] * xv[q][1] + v[8] * xv[q][2];
-                            if (sl[q] != kSymNoSlot) {  // B^T d_r for the later row
-                                float* t = tp + 3 * (sl[q] & (unsigned)(kSymRingSlots - 1));
-                                t[0] = v[0] * dr.x + v[1] * dr.y + v[2] * dr.z;
-                                t[1] = v[3] * dr.x + v[4] * dr.y + v[5] * dr.z;
-                                t[2] = v[6] * dr.x + v[7] * dr.y + v[8] * dr.z;
-                            }
+                for (int q = 0; q < kEntries; ++q) {
+                    // Column-major block: element (i, c) is v[3c + i].
+                    const float* v = bv[q];
+                    if (live[q]) {
+                        acc.x += v[0] * xv[q][0] + v[3] * xv[q][1] + v[6] * xv[q][2];
+                        acc.y += v[1] * xv[q][0] + v[4] * xv[q][1] + v[7] * xv[q][2];
+                        acc.z += v[2] * xv[q][0] + v[5] * xv[q][1] + v[8] * xv[q][2];
+                        if (sl[q] != kSymNoSlot) {  // B^T d_r for the later row
+                            float* t = tp + 3 * (sl[q] & (unsigned)(kSymRingSlots - 1));
+                            t[0] = v[0] * dr.x + v[1] * dr.y + v[2] * dr.z;
+                            t[1] = v[3] * dr.x + v[4] * dr.y + v[5] * dr.z;
+                            t[2] = v[6] * dr.x + v[7] * dr.y + v[8] * dr.z;
                         }
                     }
                 }
-#pragma unroll
-                for (int off = LPR / 2; off > 0; off >>= 1) {
-                    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
-                    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
-                    acc.z += __shfl_xor_sync(0xffffffffu, acc.z, off);
-                }
-                accs[pass] = acc;
             }
-            // The ring bases of the tile's rows, read before the stage is released.
-            unsigned lb0[2] = {0u, 0u}, lbn[2] = {0u, 0u};
-#pragma unroll
-            for (int pass = 0; pass < 2; ++pass) {
-                const int sr = pass * kSlabRows + row_in_pass;
-                if (sr < rows) {
-                    lb0[pass] = lbase[sr];
-                    lbn[pass] = ((unsigned)lbase[sr + 1] - lb0[pass]) & (unsigned)(kSymRingSlots - 1);
-                }
-            }
+            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
+            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
+            acc.z += __shfl_xor_sync(0xffffffffu, acc.z, 1);
             __syncwarp();
             if (lane == 0) mbar_arrive_slab(&empty_bar[s]);  // this warp is done with the stage
             asm volatile("bar.sync %0, %1;" ::"r"(gbar), "r"(32 * kSlabGroupWarps) : "memory");
-            // q = own sum + the row's ring slots, in slot order (lanes take every LPR-th
-            // slot, then the fixed shuffle tree).
-#pragma unroll
-            for (int pass = 0; pass < 2; ++pass) {
-                const int sr = pass * kSlabRows + row_in_pass;
-                V3<float> ts{0.f, 0.f, 0.f};
-                for (unsigned k = (unsigned)sub; k < lbn[pass]; k += LPR) {
-                    const float* t = tp + 3 * ((lb0[pass] + k) & (unsigned)(kSymRingSlots - 1));
-                    ts.x += t[0];
-                    ts.y += t[1];
-                    ts.z += t[2];
-                }
-#pragma unroll
-                for (int off = LPR / 2; off > 0; off >>= 1) {
-                    ts.x += __shfl_xor_sync(0xffffffffu, ts.x, off);
-                    ts.y += __shfl_xor_sync(0xffffffffu, ts.y, off);
-                    ts.z += __shfl_xor_sync(0xffffffffu, ts.z, off);
-                }
-                if (sr < rows && sub == 0) {
-                    const V3<float> q{accs[pass].x + ts.x, accs[pass].y + ts.y, accs[pass].z + ts.z};
-                    const int li = d.z + sr;
-                    stv4(P.qs + 4 * (size_t)(row0 + li), q);
-                    dq += dot_acc<Acc>(V3<float>{wv[3 * li], wv[3 * li + 1], wv[3 * li + 2]}, q);
-                    if (!finite3(q)) qbad = 1;
-                }
+            // q = own sum + the row's ring slots in slot order (the two lanes take alternate
+            // slots, then one fixed shuffle).
+            V3<float> ts{0.f, 0.f, 0.f};
+            for (unsigned k = (unsigned)ls; k < lbn; k += LS) {
+                const float* t = tp + 3 * ((lb0 + k) & (unsigned)(kSymRingSlots - 1));
+                ts.x += t[0];
+                ts.y += t[1];
+                ts.z += t[2];
+            }
+            ts.x += __shfl_xor_sync(0xffffffffu, ts.x, 1);
+            ts.y += __shfl_xor_sync(0xffffffffu, ts.y, 1);
+            ts.z += __shfl_xor_sync(0xffffffffu, ts.z, 1);
+            if (valid && ls == 0) {
+                const V3<float> q{acc.x + ts.x, acc.y + ts.y, acc.z + ts.z};
+                const int li = d.z + sr;
+                stv4(P.qs + 4 * (size_t)(row0 + li), q);
+                dq += dot_acc<Acc>(dr, q);
+                if (!finite3(q)) qbad = 1;
             }
             // the next tile's products may overwrite slots read above
             asm volatile("bar.sync %0, %1;" ::"r"(gbar), "r"(32 * kSlabGroupWarps) : "memory");

@@ -23,7 +23,8 @@ __global__ void __launch_bounds__(128) exchange_wait_selftest_kernel(ExSlot* slo
 {
     __shared__ double sh[3 * 32];
     __shared__ int shi[32];
-    double v[2] = {double(blockIdx.x + 1), 1.0};
+    // thread 0 holds the block's values (the exchange first sums over the block's threads)
+    double v[2] = {threadIdx.x == 0 ? double(blockIdx.x + 1) : 0.0, threadIdx.x == 0 ? 1.0 : 0.0};
     int bad = 0;
     const bool ok = count_exchange<double, 2>(slots, counter, 0, group, sync, 1u, v, bad, sh, shi, limit);
     if (threadIdx.x == 0) {

@@ -2,11 +2,12 @@
 (PhysiKAPI.h:236-251, PhysiKAPI.cpp:992-1053) against the reference.
 
 A tet mesh keeps its own copy of its node positions (TetMeshComponent::nodePositions).
-A physics mesh refreshes it from the world at the start of every substep it takes part
-in (TetMeshPhysicsComponent::UpdateSystem -> SyncCurrentPositionsFromWorld,
-TetMeshPhysicsComponent.cpp:234-252, 293-300), so after a step it holds the positions the
-step started from; before the first step it holds the generated mesh's positions.  Set
-writes that copy only (not the world's node) until the next substep overwrites it.
+A physics mesh refreshes it from the world in every substep it takes part in and again
+at the end of the frame (TetMeshPhysicsComponent::UpdateSystem and PostUpdate ->
+SyncCurrentPositionsFromWorld, TetMeshPhysicsComponent.cpp:234-252, 293-300, 356-363), so
+after a step it holds the positions the step ended with; before the first step it holds
+the generated mesh's positions.  Set writes that copy only (not the world's node) until
+the next step overwrites it.
 
 Without a GPU: creation positions, Set / Get round trips and the argument checks.  With a
 GPU (marked): the copies after steps, against the reference driven through the same calls.
@@ -82,41 +83,52 @@ def test_copies_after_steps_match_reference(precision):
     sizes = [b.positions.shape[0] for b in scene.bodies]
     begins = [w.X.PHYSIK_GetTetMeshGlobalNodeBeginIndex(w.h, c) for c in w.components]
     for step in range(3):
-        x_start, _ = w.state()  # the state this step starts from
         w.step()
         ref.step()
+        x_end, _ = w.state()  # the state this step ended with
+        xr, _ = ref.state()
         for body, count in enumerate(sizes):
             got = w.local_positions(body)
-            # exactly the positions the step started from (float32 copies of the state)
-            np.testing.assert_array_equal(got, x_start[begins[body]:begins[body] + count])
+            # exactly the world's positions after the step (float32 copies of the state)
+            np.testing.assert_array_equal(got, x_end[begins[body]:begins[body] + count])
             want = ref.local_positions(body, count)
-            if step == 0:
-                np.testing.assert_array_equal(got.astype(np.float64), want)  # both hold the initial state
-            else:
-                assert np.abs(got - want).max() <= 1e-5 * np.abs(want).max()
-        # a Set lasts until the next substep overwrites the copy
+            np.testing.assert_array_equal(want, xr[begins[body]:begins[body] + count])  # the reference's rule
+            assert np.abs(got - want).max() <= 3e-7 * np.abs(want).max() + 1e-9
+        # a Set lasts until the next step overwrites the copy, and does not move the node
         assert w.set_local_position(0, 2, (9.0, 9.0, 9.0)) == 1
         ref.set_local_position(0, 2, (9.0, 9.0, 9.0))
         assert tuple(w.local_positions(0)[2]) == (9.0, 9.0, 9.0)
         np.testing.assert_array_equal(w.local_positions(0)[2].astype(np.float64), ref.local_positions(0, sizes[0])[2])
+        np.testing.assert_array_equal(w.state()[0][begins[0] + 2], x_end[begins[0] + 2])
 
 
 @pytest.mark.gpu
 @needs_ref
-def test_copy_is_the_start_of_the_last_substep():
-    """With two substeps per step the copy holds the positions after the first substep."""
+def test_copy_with_substeps_is_the_end_of_the_frame():
+    """Two substeps per step: the copy holds the positions after the second substep."""
     scene = two_bodies()
     w = SimWorld(scene, precision="fp32")
     ref = po.Reference(scene, "f32", substeps=2)
     w.X.PHYSIK_SetSubstepCount(w.h, 2)
-    half = SimWorld(scene, precision="fp32")  # one substep of dt / 2 from the same state
     w.step()
     ref.step()
-    half.step(scene.dt / 2)
-    xh, _ = half.state()
+    x_end, _ = w.state()
     begin = w.X.PHYSIK_GetTetMeshGlobalNodeBeginIndex(w.h, w.components[1])
     count = scene.bodies[1].positions.shape[0]
     got = w.local_positions(1)
-    np.testing.assert_array_equal(got, xh[begin:begin + count])
+    np.testing.assert_array_equal(got, x_end[begin:begin + count])
     want = ref.local_positions(1, count)
-    assert np.abs(got - want).max() <= 1e-5 * np.abs(want).max()
+    assert np.abs(got - want).max() <= 3e-7 * np.abs(want).max() + 1e-9
+
+
+@pytest.mark.gpu
+def test_state_written_after_a_step_does_not_change_the_copy():
+    scene = two_bodies()
+    w = SimWorld(scene, precision="mixed")
+    w.step()
+    x_end, v_end = w.state()
+    before = w.local_positions(0).copy()
+    w.set_state(x_end + np.float32(1.0), v_end)  # moves every node; the copy keeps the frame's end
+    np.testing.assert_array_equal(w.local_positions(0), before)
+    w.step(0.0)  # a zero step runs no PostUpdate sync either
+    np.testing.assert_array_equal(w.local_positions(0), before)
