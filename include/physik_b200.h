@@ -145,6 +145,25 @@ PHYSIK_B200_API void PHYSIK_SetCollisionComponentKinematicTarget(PhysikWorldHand
                                                                  PhysikComponentHandle component, float x, float y,
                                                                  float z);
 
+/* Host-emitted SolverData contributions (extension; the reference offers them only to C++
+ * components: SolverData::AddNodeForce / AddNodeMass / AddStiffnessBlock, SolverData.h:41-54).
+ * A contribution component calls `callback(solverData, dt, userData)` from its UpdateSystem
+ * every substep, in execution-priority order (`priority` as ComponentExecutionPriority:
+ * 100 scripts ... 400 soft bodies ... 1000 default); the callback emits through the
+ * PHYSIK_B200_SolverDataAdd* functions on the handle it received, which is valid only
+ * during the call.  The device step assembles them as the reference's SolverData does:
+ * masses join the lumped masses (and may make nodes dynamic), forces the rhs, blocks the
+ * matrix (upper triangle) and -dt^2 B v the rhs; a non-finite block skips the substep.
+ * block9: the 3x3 block column-major (9 floats). */
+typedef void (*PhysikContributionCallback)(void* solverData, float dt, void* userData);
+PHYSIK_B200_API PhysikComponentHandle PHYSIK_B200_CreateContributionComponent(PhysikWorldHandle world, int priority);
+PHYSIK_B200_API void PHYSIK_B200_SetContributionCallback(PhysikWorldHandle world, PhysikComponentHandle component,
+                                                         PhysikContributionCallback callback, void* userData);
+PHYSIK_B200_API void PHYSIK_B200_SolverDataAddNodeForce(void* solverData, int node, float fx, float fy, float fz);
+PHYSIK_B200_API void PHYSIK_B200_SolverDataAddNodeMass(void* solverData, int node, float mass);
+PHYSIK_B200_API void PHYSIK_B200_SolverDataAddStiffnessBlock(void* solverData, int nodeA, int nodeB,
+                                                             const float* block9);
+
 /* Script components   PhysiKAPI.h:166-177, PhysiKAPI.cpp:719-765; ScriptComponent.cpp: the
  * callback runs once per PHYSIK_Step, before the substeps (Component::PreUpdate, in
  * execution-priority order), with the world handle, so a script can call PHYSIK_* (add

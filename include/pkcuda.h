@@ -160,6 +160,21 @@ PKCUDA_API int pk_system_set_pattern(pk_system* sys, int dyn_count, const int* d
 PKCUDA_API int pk_system_set_connections(pk_system* sys, int count, const int* nodes, const double* params,
                                          const int* inc_start, const int* inc_list);
 
+/* Host-emitted contributions of custom components for the next steps (SolverData::
+ * AddStiffnessBlock / AddNodeForce, SolverData.h:41-54, assembled as
+ * SolverData::AssembleImplicitMatrixAndRhs does, SolverData.cpp:308-465): blocks[9*count]
+ * (column-major) with block_nodes[2*count] {row node, column node}; per dynamic row the
+ * blocks whose row node is that row (rhs_start[dyn+1], rhs_list: the rhs gets
+ * -dt^2 B v_column) and the blocks it holds in its upper row (mat_start, mat_list: block
+ * index, | 0x80000000 for the transpose of a lower block); row_force[3*dyn] the summed
+ * node forces of each dynamic row (NULL: none).  Masses (AddNodeMass) enter the node
+ * masses (pk_system_set_nodes / set_masses).  The pattern must hold the blocks; count 0
+ * with row_force NULL removes them; set_pattern removes them too.  With blocks present the
+ * batched solve runs as one coupled solve and the adjoint step is refused. */
+PKCUDA_API int pk_system_set_extras(pk_system* sys, int block_count, const double* blocks, const int* block_nodes,
+                                    const int* rhs_start, const int* rhs_list, const int* mat_start,
+                                    const int* mat_list, const double* row_force);
+
 /* Batched per-body solve (no counterpart in the reference, whose World solves all of its
  * bodies as one coupled system): the dynamic rows split into independent segments
  * (bodies) [segment_row_start[b], segment_row_start[b+1]), covering all rows, with no

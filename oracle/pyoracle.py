@@ -333,6 +333,18 @@ class Reference:
         self.lib.ref_sphere_target.argtypes = [_p, _i, _d, _d, _d]
         self.lib.ref_sphere_target(self.h, sphere, *[float(c) for c in center])
 
+    def add_contribution(self, priority, callback) -> int:
+        """A component whose UpdateSystem calls `callback(solverData, dt, user)` (a ctypes
+        CFUNCTYPE(None, c_void_p, c_double, c_void_p)); emit with solverdata_add_*."""
+        L = self.lib
+        L.ref_add_contribution.argtypes = [_p, _i, _p, _p]
+        L.ref_add_contribution.restype = _i
+        L.ref_solverdata_add_force.argtypes = [_p, _i, _d, _d, _d]
+        L.ref_solverdata_add_mass.argtypes = [_p, _i, _d]
+        L.ref_solverdata_add_block.argtypes = [_p, _i, _i, _p]
+        self._contrib = getattr(self, "_contrib", []) + [callback]
+        return L.ref_add_contribution(self.h, priority, C.cast(callback, C.c_void_p), None)
+
     def add_script(self, callback) -> int:
         """A ScriptComponent calling `callback` (a ctypes CFUNCTYPE(None, c_void_p, c_void_p))
         once per frame with the reference world's handle."""

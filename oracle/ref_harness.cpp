@@ -127,6 +127,48 @@ __attribute__((visibility("default"))) void ref_set_local_position(void* h, int 
         ->SetLocalCurrentPosition(node, Vec3{static_cast<Real>(x), static_cast<Real>(y), static_cast<Real>(z)});
 }
 
+// A component that hands SolverData to a C callback from UpdateSystem (what a custom C++
+// component of the reference does), at the given execution priority; the callback emits
+// through ref_solverdata_add_* (SolverData::AddNodeForce / AddNodeMass / AddStiffnessBlock).
+namespace {
+using RefContribution = void (*)(void* solverData, double dt, void* user);
+class RefContributionComponent : public Component {
+public:
+    RefContributionComponent(int priority, RefContribution cb, void* user) : priority_(priority), cb_(cb), user_(user) {}
+    ComponentExecutionPriority GetExecutionPriority() const override
+    {
+        return static_cast<ComponentExecutionPriority>(priority_);
+    }
+    void UpdateSystem(World&, SolverData& solverData, Real dt) override { cb_(&solverData, dt, user_); }
+
+private:
+    int priority_;
+    RefContribution cb_;
+    void* user_;
+};
+}  // namespace
+
+__attribute__((visibility("default"))) int ref_add_contribution(void* h, int priority, RefContribution cb, void* user)
+{
+    return H(h)->world.AddComponent(std::make_unique<RefContributionComponent>(priority, cb, user)).IsValid() ? 1 : 0;
+}
+__attribute__((visibility("default"))) void ref_solverdata_add_force(void* sd, int node, double x, double y, double z)
+{
+    static_cast<SolverData*>(sd)->AddNodeForce(node, Vec3{static_cast<Real>(x), static_cast<Real>(y), static_cast<Real>(z)});
+}
+__attribute__((visibility("default"))) void ref_solverdata_add_mass(void* sd, int node, double m)
+{
+    static_cast<SolverData*>(sd)->AddNodeMass(node, static_cast<Real>(m));
+}
+__attribute__((visibility("default"))) void ref_solverdata_add_block(void* sd, int a, int b, const double* block9)
+{
+    Vec3 c[3];
+    for (int i = 0; i < 3; ++i)
+        c[i] = Vec3{static_cast<Real>(block9[3 * i]), static_cast<Real>(block9[3 * i + 1]),
+                    static_cast<Real>(block9[3 * i + 2])};
+    static_cast<SolverData*>(sd)->AddStiffnessBlock(a, b, Mat3::FromColumns(c[0], c[1], c[2]));
+}
+
 // A ScriptComponent with its external callback (World::AddComponent,
 // ScriptComponent::SetExternalLogicCallback), as PHYSIK_CreateScriptComponent and
 // PHYSIK_SetScriptComponentCallback do.  Returns 1 on success.

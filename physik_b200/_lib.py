@@ -135,6 +135,11 @@ _SIGS = {
     "PHYSIK_SetCollisionSphereConnectionSettings": (_v, [_p, _H, _f, _f]),
     "PHYSIK_GetCollisionSphereConnectionSettings": (_v, [_p, _H, _p, _p]),
     "PHYSIK_SetCollisionComponentKinematicTarget": (_v, [_p, _H, _f, _f, _f]),
+    "PHYSIK_B200_CreateContributionComponent": (_H, [_p, _i]),
+    "PHYSIK_B200_SetContributionCallback": (_v, [_p, _H, _p, _p]),
+    "PHYSIK_B200_SolverDataAddNodeForce": (_v, [_p, _i, _f, _f, _f]),
+    "PHYSIK_B200_SolverDataAddNodeMass": (_v, [_p, _i, _f]),
+    "PHYSIK_B200_SolverDataAddStiffnessBlock": (_v, [_p, _i, _i, _p]),
     "PHYSIK_CreateScriptComponent": (_H, [_p]),
     "PHYSIK_SetScriptComponentCallback": (_v, [_p, _H, _p, _p]),
     "PHYSIK_ClearScriptComponentCallback": (_v, [_p, _H]),

@@ -299,6 +299,41 @@ PHYSIK_B200_API void PHYSIK_SetCollisionComponentKinematicTarget(PhysikWorldHand
     c->SetKinematicTarget(target);
 }
 
+PHYSIK_B200_API PhysikComponentHandle PHYSIK_B200_CreateContributionComponent(PhysikWorldHandle world, int priority)
+{
+    World* w = AsWorld(world);
+    if (!w) return InvalidHandle();
+    return Guard([&] { return FromHandle(w->AddComponent(std::make_unique<ContributionComponent>(priority))); },
+                 InvalidHandle());
+}
+
+PHYSIK_B200_API void PHYSIK_B200_SetContributionCallback(PhysikWorldHandle world, PhysikComponentHandle component,
+                                                         PhysikContributionCallback callback, void* userData)
+{
+    World* w = AsWorld(world);
+    auto* c = w ? dynamic_cast<ContributionComponent*>(w->GetComponent(ToHandle(component))) : nullptr;
+    if (c) c->SetCallback(reinterpret_cast<ContributionCallback>(callback), userData);
+}
+
+PHYSIK_B200_API void PHYSIK_B200_SolverDataAddNodeForce(void* solverData, int node, float fx, float fy, float fz)
+{
+    if (solverData) static_cast<SolverData*>(solverData)->AddNodeForce(node, Vec3{fx, fy, fz});
+}
+
+PHYSIK_B200_API void PHYSIK_B200_SolverDataAddNodeMass(void* solverData, int node, float mass)
+{
+    if (solverData) static_cast<SolverData*>(solverData)->AddNodeMass(node, mass);
+}
+
+PHYSIK_B200_API void PHYSIK_B200_SolverDataAddStiffnessBlock(void* solverData, int nodeA, int nodeB,
+                                                             const float* block9)
+{
+    if (!solverData || !block9) return;
+    const Mat3 b = Mat3::FromColumns(Vec3{block9[0], block9[1], block9[2]}, Vec3{block9[3], block9[4], block9[5]},
+                                     Vec3{block9[6], block9[7], block9[8]});
+    static_cast<SolverData*>(solverData)->AddStiffnessBlock(nodeA, nodeB, b);
+}
+
 PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateScriptComponent(PhysikWorldHandle world)
 {
     World* w = AsWorld(world);

@@ -24,6 +24,7 @@
 #include <string>
 #include <unordered_map>
 #include <utility>
+#include <tuple>
 #include <vector>
 
 #include "physik_math.h"
@@ -215,7 +216,11 @@ public:
         stiffnessBlocks.push_back(StiffnessBlock{nodeA, nodeB, block});
     }
     // Device path: a soft body whose per-tet forces and stiffness the GPU computes.
-    void AddFemBody(const TetMeshPhysicsComponent* body) { femBodies.push_back(body); }
+    void AddFemBody(const TetMeshPhysicsComponent* body)
+    {
+        femBodies.push_back(body);
+        femMassMark.push_back(nodeMasses.size());  // masses emitted before this body's
+    }
 
     const std::vector<NodeForce>& GetNodeForces() const { return nodeForces; }
     const std::vector<NodeMass>& GetNodeMasses() const { return nodeMasses; }
@@ -250,6 +255,7 @@ private:
     std::vector<NodeMass> nodeMasses;
     std::vector<StiffnessBlock> stiffnessBlocks;
     std::vector<const TetMeshPhysicsComponent*> femBodies;
+    std::vector<std::size_t> femMassMark;  // per FEM body: nodeMasses.size() when it registered
 
     std::vector<float> assembledMasses;
     std::vector<Vec3> assembledForces;
@@ -302,6 +308,33 @@ public:
 private:
     ExternalLogicCallback externalLogicCallback = nullptr;
     void* externalLogicUserData = nullptr;
+};
+
+// A component whose UpdateSystem hands the substep's SolverData to an external callback,
+// which emits contributions through the C ABI (PHYSIK_B200_SolverDataAdd*) as a C++
+// component would through SolverData::AddNodeForce / AddNodeMass / AddStiffnessBlock.
+using ContributionCallback = void (*)(void* solverData, float dt, void* userData);
+class ContributionComponent : public Component {
+public:
+    explicit ContributionComponent(int priority) : priority_(priority) {}
+    ComponentExecutionPriority GetExecutionPriority() const override
+    {
+        return static_cast<ComponentExecutionPriority>(priority_);
+    }
+    void SetCallback(ContributionCallback cb, void* user)
+    {
+        callback = cb;
+        userData = user;
+    }
+    void UpdateSystem(World&, SolverData& solverData, float dt) override
+    {
+        if (callback) callback(static_cast<void*>(&solverData), dt, userData);
+    }
+
+private:
+    int priority_;
+    ContributionCallback callback = nullptr;
+    void* userData = nullptr;
 };
 
 // Transform of a collision component (Transform.h:8-16; the sphere uses its position).
@@ -588,6 +621,8 @@ public:
     // in (TetMeshPhysicsComponent::SyncCurrentPositionsFromWorld, done lazily).
     void RefreshLocalPositions(TetMeshPhysicsComponent& component) const;
     std::uint64_t GetSnapshotGeneration() const { return snapshotGeneration; }
+    // This substep's valid host-emitted masses (node, mass, after its body's lumped masses).
+    const std::vector<std::tuple<int, float, bool>>& GetExtraMasses() const { return extras.masses; }
     void MarkTopologyDirty() { ++topologyVersion; }
     std::uint64_t GetTopologyVersion() const { return topologyVersion; }
 
@@ -642,6 +677,19 @@ private:
     mutable bool statsPending = false;
     std::uint64_t snapshotGeneration = 0;  // substeps whose start positions the device snapshot held
     std::vector<const CollisionSphereComponent*> sphereRequests;  // this substep's, in update order
+    // Host-emitted SolverData contributions of this substep (custom components'
+    // AddNodeMass / AddNodeForce / AddStiffnessBlock), sorted out for the device step.
+    struct Extras {
+        bool any = false;     // some contribution was emitted
+        bool failed = false;  // a non-finite stiffness block: the step is not applied
+        // valid masses in emission order: node, mass, whether it comes after the node's
+        // soft body's own lumped masses
+        std::vector<std::tuple<int, float, bool>> masses;
+        std::vector<Vec3> force;  // per world node (empty: no force)
+        std::vector<SolverData::StiffnessBlock> blocks;  // those with both nodes in range
+    } extras;
+    void BuildExtras();
+    bool SyncExtras(std::vector<std::pair<int, int>>& pairs);  // device lists; adds the blocks' pattern pairs
 };
 
 }  // namespace PhysiK

@@ -355,6 +355,7 @@ void SolverData::ClearTransientState()
     nodeMasses.clear();
     stiffnessBlocks.clear();
     femBodies.clear();
+    femMassMark.clear();
     assembledMasses.clear();
     assembledForces.clear();
     nodeToDynamicBlock.clear();
@@ -434,6 +435,13 @@ struct DeviceScene {
     std::vector<int> femRowStart, femColIndex;
     std::vector<std::pair<int, int>> connPairs;
     std::uint64_t connVersion = 0;  // World::connectionVersion the connection arrays are for
+    std::vector<std::pair<int, int>> connOnlyPairs;  // the connections' own pairs (sorted)
+    std::vector<std::tuple<int, float, bool>> extraMasses;  // host-emitted masses this scene holds
+    // host-emitted blocks and forces (World::SyncExtras)
+    bool extOnDevice = false;       // the device holds host-emitted blocks / forces
+    int extCount = 0;
+    std::vector<double> extBlocks, extForce;
+    std::vector<int> extNodes, extRhsStart, extRhsList, extMatStart, extMatList;
     int connCount = 0;
     std::vector<int> connNodes, connIncStart, connIncList;
     std::vector<double> connParams;
@@ -448,6 +456,7 @@ struct DeviceScene {
     {
         if (!built || worldVersion != w.GetTopologyVersion() || precision != w.GetPrecision()) return false;
         if (fem.size() != bodies.size()) return false;
+        if (extraMasses != w.GetExtraMasses()) return false;
         for (std::size_t i = 0; i < fem.size(); ++i)
             if (fem[i] != bodies[i].first || fem[i]->version != bodies[i].second) return false;
         return true;
@@ -512,7 +521,13 @@ void BuildHostScene(DeviceScene& sc, const World& w, const std::vector<const Tet
         });
         first += tets.size();
     }
-    // Lumped mass rho V / 4 to the non-fixed nodes of active tets, summed in tet order.
+    // Host-emitted masses of custom components emitted before the node's soft body, then the
+    // lumped mass rho V / 4 to the non-fixed nodes of active tets, summed in tet order, then
+    // the host-emitted masses emitted after it (SolverData::AssembleMasses sums every mass
+    // in emission order).
+    const auto& extraMasses = w.GetExtraMasses();
+    for (const auto& e : extraMasses)
+        if (!std::get<2>(e)) massT[static_cast<std::size_t>(std::get<0>(e))] += T(std::get<1>(e));
     for (std::size_t g = 0; g < total; ++g) {
         if (!(nodal[g] > T(0))) continue;
         for (int k = 0; k < 4; ++k) {
@@ -520,6 +535,9 @@ void BuildHostScene(DeviceScene& sc, const World& w, const std::vector<const Tet
             if (!nodes[static_cast<std::size_t>(n)].fixed) massT[static_cast<std::size_t>(n)] += nodal[g];
         }
     }
+    for (const auto& e : extraMasses)
+        if (std::get<2>(e)) massT[static_cast<std::size_t>(std::get<0>(e))] += T(std::get<1>(e));
+    sc.extraMasses = extraMasses;
     // World::ValidateNodeMasses
     for (int i = 0; i < nn; ++i) {
         const Node& nd = nodes[static_cast<std::size_t>(i)];
@@ -1032,9 +1050,52 @@ void World::CollectContributions(float dt)
     sphereRequests.clear();
     for (auto& e : orderedComponents)
         if (e.second && e.second->active) e.second->UpdateSystem(*this, solverData, dt);
-    if (!solverData.GetNodeForces().empty() || !solverData.GetNodeMasses().empty() ||
-        !solverData.GetStiffnessBlocks().empty())
-        throw std::runtime_error("host-emitted SolverData contributions are not supported by the device step");
+    BuildExtras();
+}
+
+// The host-emitted contributions of custom components, checked as SolverData does:
+// masses that are out of range, not finite or not positive are dropped (AssembleMasses,
+// SolverData.cpp:87-101), so are forces out of range or not finite (PrecomputeImplicitSolve,
+// :145-154) and blocks with a node out of range (:337-343); a non-finite block fails the
+// step (:351-354).  A mass counts after its node's soft-body masses when it was emitted
+// after that body registered (execution priority), so the sums keep the reference's order.
+void World::BuildExtras()
+{
+    extras = Extras{};
+    const int nn = static_cast<int>(nodes.size());
+    const auto& masses = solverData.GetNodeMasses();
+    const auto& forces = solverData.GetNodeForces();
+    const auto& blocks = solverData.GetStiffnessBlocks();
+    extras.any = !masses.empty() || !forces.empty() || !blocks.empty();
+    if (!extras.any) return;
+    // The registration mark of the soft body holding each node (-1: none).
+    std::vector<long long> mark;
+    if (!masses.empty()) {
+        mark.assign(static_cast<std::size_t>(nn), -1);
+        const auto& fem = solverData.GetFemBodies();
+        for (std::size_t b = 0; b < fem.size(); ++b) {
+            const int b0 = fem[b]->GetGlobalNodeBeginIndex(), cnt = fem[b]->GetGlobalNodeCount();
+            for (int i = std::max(0, b0); i < std::min(nn, b0 + cnt); ++i)
+                mark[static_cast<std::size_t>(i)] = static_cast<long long>(solverData.femMassMark[b]);
+        }
+    }
+    for (std::size_t k = 0; k < masses.size(); ++k) {
+        const auto& m = masses[k];
+        if (m.node < 0 || m.node >= nn || !std::isfinite(m.mass) || !(m.mass > 0.0f)) continue;
+        const long long mk = mark[static_cast<std::size_t>(m.node)];
+        extras.masses.emplace_back(m.node, m.mass, mk >= 0 && static_cast<long long>(k) >= mk);
+    }
+    for (const auto& f : forces) {
+        if (f.node < 0 || f.node >= nn || !std::isfinite(f.force.x) || !std::isfinite(f.force.y) ||
+            !std::isfinite(f.force.z))
+            continue;
+        if (extras.force.empty()) extras.force.assign(static_cast<std::size_t>(nn), Vec3{});
+        extras.force[static_cast<std::size_t>(f.node)] += f.force;
+    }
+    for (const auto& b : blocks) {
+        if (b.nodeA < 0 || b.nodeA >= nn || b.nodeB < 0 || b.nodeB >= nn) continue;
+        extras.blocks.push_back(b);
+    }
 }
 
 void World::EnsureScene(bool upload)
@@ -1090,6 +1151,7 @@ void World::EnsureScene(bool upload)
         if (!scene->sys) Check(pk_system_create(device, static_cast<int>(precision), &scene->sys), "pk_system_create");
         UploadScene(*scene, positions, velocities);
         scene->connOnDevice = false;
+        scene->extOnDevice = false;
         deviceStale = false;
         hostStale = false;
     } else if (upload && patternChanged) {
@@ -1101,6 +1163,7 @@ void World::EnsureScene(bool upload)
         sc.devNnz = static_cast<int>(sc.colIndex.size());
         sc.batchedOnDevice = false;  // set_pattern drops the segments
         sc.connOnDevice = false;
+        sc.extOnDevice = false;
     }
     if (upload && scene->uploaded && !scene->connOnDevice) {
         DeviceScene& sc = *scene;
@@ -1109,6 +1172,109 @@ void World::EnsureScene(bool upload)
               "set_connections");
         sc.connOnDevice = true;
     }
+    if (upload && scene->uploaded && (extras.any || scene->extOnDevice) && !extras.failed) {
+        DeviceScene& sc = *scene;
+        const bool on = extras.any;
+        Check(pk_system_set_extras(sc.sys, on ? sc.extCount : 0, sc.extBlocks.data(), sc.extNodes.data(),
+                                   sc.extRhsStart.data(), sc.extRhsList.data(), sc.extMatStart.data(),
+                                   sc.extMatList.data(), on && !sc.extForce.empty() ? sc.extForce.data() : nullptr),
+              "set_extras");
+        sc.extOnDevice = on;
+    }
+}
+
+// The device lists of this substep's host-emitted blocks and forces (World::BuildExtras),
+// assembled as SolverData::AssembleImplicitMatrixAndRhs does (SolverData.cpp:308-465):
+// every block whose row node is dynamic adds -dt^2 B v_column to that row's rhs; when its
+// column node is dynamic too it is a matrix block, kept in the upper triangle -- B at
+// (row, column), or B^T at (column, row) for a lower block -- except a lower block whose
+// upper twin is emitted as well (by another host block, or by the soft bodies and point
+// connections, which emit both orientations).  The dynamic coordinate pairs of the kept
+// blocks join the pattern (`pairs`).  Returns whether host-emitted contributions exist.
+bool World::SyncExtras(std::vector<std::pair<int, int>>& pairs)
+{
+    DeviceScene& sc = *scene;
+    sc.extCount = 0;
+    sc.extBlocks.clear();
+    sc.extNodes.clear();
+    sc.extForce.clear();
+    sc.extRhsList.clear();
+    sc.extMatList.clear();
+    sc.extRhsStart.clear();
+    sc.extMatStart.clear();
+    extras.failed = false;
+    if (!extras.any) return false;
+    const int dyn = sc.dynCount;
+    auto dynOf = [&](int node) { return sc.nodeToDyn[static_cast<std::size_t>(node)]; };
+    auto key = [](int r, int c) {
+        return (static_cast<std::uint64_t>(static_cast<std::uint32_t>(r)) << 32) | static_cast<std::uint32_t>(c);
+    };
+    std::vector<std::pair<int, int>> rhsInc, matInc;  // (row, entry)
+    std::unordered_map<std::uint64_t, int> emitted;   // dynamic (row, column) coordinates emitted
+    std::vector<int> kept;                            // extras.blocks index of each device block
+    for (std::size_t i = 0; i < extras.blocks.size(); ++i) {
+        const auto& b = extras.blocks[i];
+        const int ra = dynOf(b.nodeA);
+        if (ra < 0) continue;
+        const Mat3& m = b.block;
+        for (int c = 0; c < 3; ++c)
+            if (!std::isfinite(m.columns[c].x) || !std::isfinite(m.columns[c].y) || !std::isfinite(m.columns[c].z)) {
+                extras.failed = true;
+                return true;
+            }
+        const int k = static_cast<int>(kept.size());
+        kept.push_back(static_cast<int>(i));
+        rhsInc.emplace_back(ra, k);
+        const int cb = dynOf(b.nodeB);
+        if (cb >= 0) emitted.emplace(key(ra, cb), 1);
+    }
+    auto femHas = [&](int r, int c) {  // the soft bodies couple dynamic rows r <= c
+        const auto b0 = sc.femColIndex.begin() + sc.femRowStart[static_cast<std::size_t>(r)];
+        const auto b1 = sc.femColIndex.begin() + sc.femRowStart[static_cast<std::size_t>(r) + 1];
+        return std::binary_search(b0, b1, c);
+    };
+    for (int k = 0; k < static_cast<int>(kept.size()); ++k) {
+        const auto& b = extras.blocks[static_cast<std::size_t>(kept[static_cast<std::size_t>(k)])];
+        const int ra = dynOf(b.nodeA), cb = dynOf(b.nodeB);
+        if (cb < 0) continue;
+        if (ra > cb && (emitted.count(key(cb, ra)) || femHas(cb, ra) ||
+                        std::binary_search(sc.connOnlyPairs.begin(), sc.connOnlyPairs.end(), std::make_pair(cb, ra))))
+            continue;
+        const bool tr = ra > cb;
+        matInc.emplace_back(tr ? cb : ra, k | (tr ? static_cast<int>(0x80000000u) : 0));
+        pairs.emplace_back(std::min(ra, cb), std::max(ra, cb));
+    }
+    sc.extCount = static_cast<int>(kept.size());
+    for (int k : kept) {
+        const auto& b = extras.blocks[static_cast<std::size_t>(k)];
+        for (int c = 0; c < 3; ++c) {
+            sc.extBlocks.push_back(b.block.columns[c].x);
+            sc.extBlocks.push_back(b.block.columns[c].y);
+            sc.extBlocks.push_back(b.block.columns[c].z);
+        }
+        sc.extNodes.push_back(b.nodeA);
+        sc.extNodes.push_back(b.nodeB);
+    }
+    auto csr = [&](const std::vector<std::pair<int, int>>& inc, std::vector<int>& start, std::vector<int>& list) {
+        start.assign(static_cast<std::size_t>(dyn) + 1, 0);
+        for (const auto& e : inc) start[static_cast<std::size_t>(e.first) + 1]++;
+        for (int r = 0; r < dyn; ++r) start[static_cast<std::size_t>(r) + 1] += start[static_cast<std::size_t>(r)];
+        list.assign(inc.size(), 0);
+        std::vector<int> fill(start.begin(), start.end() - 1);
+        for (const auto& e : inc) list[static_cast<std::size_t>(fill[static_cast<std::size_t>(e.first)]++)] = e.second;
+    };
+    csr(rhsInc, sc.extRhsStart, sc.extRhsList);
+    csr(matInc, sc.extMatStart, sc.extMatList);
+    if (!extras.force.empty()) {
+        sc.extForce.assign(3 * static_cast<std::size_t>(dyn), 0.0);
+        for (int r = 0; r < dyn; ++r) {
+            const Vec3& f = extras.force[static_cast<std::size_t>(sc.dynToNode[static_cast<std::size_t>(r)])];
+            sc.extForce[3 * static_cast<std::size_t>(r)] = f.x;
+            sc.extForce[3 * static_cast<std::size_t>(r) + 1] = f.y;
+            sc.extForce[3 * static_cast<std::size_t>(r) + 2] = f.z;
+        }
+    }
+    return true;
 }
 
 // The device arrays of the current point connections and the pattern they need:
@@ -1123,53 +1289,61 @@ void World::EnsureScene(bool upload)
 bool World::SyncConnections()
 {
     DeviceScene& sc = *scene;
-    if (sc.connVersion == connectionVersion) return false;
-    sc.connVersion = connectionVersion;
-    sc.connNodes.clear();
-    sc.connParams.clear();
+    const bool connChanged = sc.connVersion != connectionVersion;
+    if (!connChanged && !extras.any && !sc.extOnDevice) return false;
     std::vector<std::pair<int, int>> pairs;
-    std::vector<std::pair<int, int>> inc;  // (row, connection * 4 + corner)
-    int count = 0;
-    for (const PointConnection& pc : transientConnections) {
-        if (!HasValidNodeIndices(pc) || !std::isfinite(pc.stiffness) || !std::isfinite(pc.damping) ||
-            pc.stiffness < 0.0f || pc.damping < 0.0f || !std::isfinite(pc.targetPosition.x) ||
-            !std::isfinite(pc.targetPosition.y) || !std::isfinite(pc.targetPosition.z))
-            continue;
-        const int nd[4] = {pc.node0, pc.node1, pc.node2, pc.node3};
-        const float w[4] = {pc.barycentric.x, pc.barycentric.y, pc.barycentric.z, pc.barycentric.w};
-        for (int a = 0; a < 4; ++a) {
-            sc.connNodes.push_back(nd[a]);
-            sc.connParams.push_back(w[a]);
-        }
-        sc.connParams.push_back(pc.targetPosition.x);
-        sc.connParams.push_back(pc.targetPosition.y);
-        sc.connParams.push_back(pc.targetPosition.z);
-        sc.connParams.push_back(pc.stiffness);
-        sc.connParams.push_back(pc.damping);
-        for (int a = 0; a < 4; ++a) {
-            const int ra = sc.nodeToDyn[static_cast<std::size_t>(nd[a])];
-            if (w[a] == 0.0f || ra < 0) continue;
-            inc.emplace_back(ra, count * 4 + a);
-            if (!(pc.stiffness > 0.0f)) continue;
-            for (int b = 0; b < 4; ++b) {
-                const int rb = sc.nodeToDyn[static_cast<std::size_t>(nd[b])];
-                if (w[b] == 0.0f || rb < 0) continue;
-                pairs.emplace_back(std::min(ra, rb), std::max(ra, rb));
-            }
-        }
-        ++count;
-    }
-    sc.connCount = count;
     const int dyn = sc.dynCount;
-    sc.connIncStart.assign(static_cast<std::size_t>(dyn) + 1, 0);
-    for (const auto& e : inc) sc.connIncStart[static_cast<std::size_t>(e.first) + 1]++;
-    for (int r = 0; r < dyn; ++r) sc.connIncStart[r + 1] += sc.connIncStart[r];
-    sc.connIncList.assign(inc.size(), 0);
-    {
-        std::vector<int> fill(sc.connIncStart.begin(), sc.connIncStart.end() - 1);
-        for (const auto& e : inc) sc.connIncList[static_cast<std::size_t>(fill[e.first]++)] = e.second;
+    if (connChanged) {
+        sc.connVersion = connectionVersion;
+        sc.connNodes.clear();
+        sc.connParams.clear();
+        std::vector<std::pair<int, int>> inc;  // (row, connection * 4 + corner)
+        int count = 0;
+        for (const PointConnection& pc : transientConnections) {
+            if (!HasValidNodeIndices(pc) || !std::isfinite(pc.stiffness) || !std::isfinite(pc.damping) ||
+                pc.stiffness < 0.0f || pc.damping < 0.0f || !std::isfinite(pc.targetPosition.x) ||
+                !std::isfinite(pc.targetPosition.y) || !std::isfinite(pc.targetPosition.z))
+                continue;
+            const int nd[4] = {pc.node0, pc.node1, pc.node2, pc.node3};
+            const float w[4] = {pc.barycentric.x, pc.barycentric.y, pc.barycentric.z, pc.barycentric.w};
+            for (int a = 0; a < 4; ++a) {
+                sc.connNodes.push_back(nd[a]);
+                sc.connParams.push_back(w[a]);
+            }
+            sc.connParams.push_back(pc.targetPosition.x);
+            sc.connParams.push_back(pc.targetPosition.y);
+            sc.connParams.push_back(pc.targetPosition.z);
+            sc.connParams.push_back(pc.stiffness);
+            sc.connParams.push_back(pc.damping);
+            for (int a = 0; a < 4; ++a) {
+                const int ra = sc.nodeToDyn[static_cast<std::size_t>(nd[a])];
+                if (w[a] == 0.0f || ra < 0) continue;
+                inc.emplace_back(ra, count * 4 + a);
+                if (!(pc.stiffness > 0.0f)) continue;
+                for (int b = 0; b < 4; ++b) {
+                    const int rb = sc.nodeToDyn[static_cast<std::size_t>(nd[b])];
+                    if (w[b] == 0.0f || rb < 0) continue;
+                    pairs.emplace_back(std::min(ra, rb), std::max(ra, rb));
+                }
+            }
+            ++count;
+        }
+        sc.connCount = count;
+        sc.connIncStart.assign(static_cast<std::size_t>(dyn) + 1, 0);
+        for (const auto& e : inc) sc.connIncStart[static_cast<std::size_t>(e.first) + 1]++;
+        for (int r = 0; r < dyn; ++r) sc.connIncStart[r + 1] += sc.connIncStart[r];
+        sc.connIncList.assign(inc.size(), 0);
+        {
+            std::vector<int> fill(sc.connIncStart.begin(), sc.connIncStart.end() - 1);
+            for (const auto& e : inc) sc.connIncList[static_cast<std::size_t>(fill[e.first]++)] = e.second;
+        }
+        sc.connOnDevice = false;
+        std::sort(pairs.begin(), pairs.end());
+        pairs.erase(std::unique(pairs.begin(), pairs.end()), pairs.end());
+        sc.connOnlyPairs = pairs;
     }
-    sc.connOnDevice = false;
+    pairs = sc.connOnlyPairs;
+    SyncExtras(pairs);
     std::sort(pairs.begin(), pairs.end());
     pairs.erase(std::unique(pairs.begin(), pairs.end()), pairs.end());
     if (pairs == sc.connPairs) return false;
@@ -1371,6 +1545,14 @@ void World::RunSubstep(float dt)
     if (!sphereRequests.empty()) {
         AddSphereContacts();
         EnsureScene(true);
+    }
+    if (extras.failed) {
+        // A non-finite host-emitted block: the implicit system cannot be assembled and the
+        // substep is not applied (the reference would solve the part assembled so far).
+        lastConjugateGradientResult = ConjugateGradientResult{};
+        statsPending = false;
+        lastFlags = PK_FLAG_PRECOMPUTE_FAILED;
+        return;
     }
     if (scene->dynCount == 0) {
         // No dynamic node: PrecomputeImplicitSolve fails and nothing moves.

@@ -422,6 +422,49 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
             }
         }
     }
+    // Host-emitted contributions of custom components (SolverData::AddStiffnessBlock and
+    // AddNodeForce, SolverData.cpp:322-365, 407-462): -dt^2 B v_b into the rhs for every
+    // block whose row node is this row (column nodes of any kind), the blocks this row
+    // holds in its upper row (B, or B^T for a lower block whose upper twin was not
+    // emitted), and the summed forces.
+    if (A.ext_rhs_start) {
+        const int b0 = __ldg(A.ext_rhs_start + r), b1 = __ldg(A.ext_rhs_start + r + 1);
+        for (int i = b0; i < b1 && !A.explicit_mode; ++i) {
+            const int k = __ldg(A.ext_rhs_list + i);
+            const M3<Real> B = ld9(A.ext_blocks, (size_t)k);
+            const int2 nd = __ldg(A.ext_nodes + k);
+            const V3<Real> vb = ld3(A.v, nd.y);
+            bad |= !finite3(vb) || !finite9(B);
+            kv = kv + mul(B, vb);
+        }
+        const int m0 = __ldg(A.ext_mat_start + r), m1 = __ldg(A.ext_mat_start + r + 1);
+        for (int i = m0; i < m1 && !A.explicit_mode; ++i) {
+            const unsigned code = (unsigned)__ldg(A.ext_mat_list + i);
+            const int k = (int)(code & 0x7fffffffu);
+            const bool tr = (code & 0x80000000u) != 0;
+            M3<Real> B = ld9(A.ext_blocks, (size_t)k);
+            if (tr) B = transpose(B);
+            const int2 nd = __ldg(A.ext_nodes + k);
+            const int c = __ldg(A.node_to_dyn + (tr ? nd.x : nd.y));
+            int slot = nu;
+            if (MAXU > 0) {
+#pragma unroll
+                for (int j = (MAXU > 0 ? MAXU : 1) - 1; j >= 0; --j)
+                    if (colr[j] == c) slot = j;
+            } else {
+                slot = 0;
+                while (slot < nu && __ldg(A.a.col + ks + slot) != c) ++slot;
+            }
+            if (c < r || slot >= nu) {
+                bad = true;  // pattern does not hold the block: host/device mismatch
+                continue;
+            }
+            PK_ACC(slot, 0) += B.c[0].x; PK_ACC(slot, 1) += B.c[0].y; PK_ACC(slot, 2) += B.c[0].z;
+            PK_ACC(slot, 3) += B.c[1].x; PK_ACC(slot, 4) += B.c[1].y; PK_ACC(slot, 5) += B.c[1].z;
+            PK_ACC(slot, 6) += B.c[2].x; PK_ACC(slot, 7) += B.c[2].y; PK_ACC(slot, 8) += B.c[2].z;
+        }
+    }
+    if (A.ext_force) fsum = fsum + ld3(A.ext_force, r);
     const Real m = __ldg(A.mass + node);
     const V3<Real> grav{A.gravity[0], A.gravity[1], A.gravity[2]};
     fsum = fsum + grav * m;

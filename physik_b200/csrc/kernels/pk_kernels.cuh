@@ -103,6 +103,15 @@ struct AssemblyArgs {
     Real* conn_eval;                 // 4 per connection: its force (3) and 1 when it applies this step, else 0
     const int* conn_inc_start;       // per dyn row
     const int* conn_inc_list;        // connection*4 + corner (corners with a non-zero weight)
+    // Host-emitted stiffness blocks and forces (SolverData::AddStiffnessBlock / AddNodeForce
+    // from custom components); ext_rhs_start is NULL when there are none.
+    const Real* ext_blocks;          // 9 per block, column-major
+    const int2* ext_nodes;           // per block: its row node and column node
+    const int* ext_rhs_start;        // per dyn row: blocks whose row node is that row (rhs -dt^2 B v_col)
+    const int* ext_rhs_list;
+    const int* ext_mat_start;        // per dyn row: blocks it holds in its upper row
+    const int* ext_mat_list;         // block index, | 0x80000000 when the transpose is added
+    const Real* ext_force;           // 3 per dyn row, or NULL
 };
 constexpr int kConnParams = 9;
 

@@ -213,6 +213,10 @@ struct pk_system {
     // transient point connections (cleared by set_pattern)
     int conn_count = 0;
     DevBuf conn_nodes, conn_params, conn_eval, conn_inc_start, conn_inc_list;
+    // host-emitted blocks and forces of custom components (cleared by set_pattern)
+    bool ext_on = false, ext_force_on = false;
+    int ext_count = 0;
+    DevBuf ext_blocks, ext_nodes, ext_rhs_start, ext_rhs_list, ext_mat_start, ext_mat_list, ext_force;
     // batched per-body solve
     bool batched = false;
     std::vector<int> seg_start;   // body row ranges: [seg_start[b], seg_start[b+1])
@@ -326,6 +330,15 @@ pk::AssemblyArgs<Real> assembly_args(pk_system* s, const pk_step_params& p)
         a.conn_eval = s->conn_eval.as<Real>();
         a.conn_inc_start = s->conn_inc_start.as<int>();
         a.conn_inc_list = s->conn_inc_list.as<int>();
+    }
+    if (s->ext_on) {
+        a.ext_blocks = s->ext_blocks.as<Real>();
+        a.ext_nodes = s->ext_nodes.as<int2>();
+        a.ext_rhs_start = s->ext_rhs_start.as<int>();
+        a.ext_rhs_list = s->ext_rhs_list.as<int>();
+        a.ext_mat_start = s->ext_mat_start.as<int>();
+        a.ext_mat_list = s->ext_mat_list.as<int>();
+        a.ext_force = s->ext_force_on ? s->ext_force.as<Real>() : nullptr;
     }
     return a;
 }
@@ -526,7 +539,10 @@ bool slab_allowed(const pk_system* s)
 
 // Point connections may couple bodies: with any present the step solves one coupled
 // system, as the reference always does.
-bool batched_solve(const pk_system* s) { return s->batched && s->seg_start.size() >= 2 && s->conn_count == 0; }
+bool batched_solve(const pk_system* s)
+{
+    return s->batched && s->seg_start.size() >= 2 && s->conn_count == 0 && s->ext_count == 0;
+}
 
 // Builds and uploads the part-resident kernel's layout if it has not been tried yet for
 // this pattern and grid (synchronous: never called while a stream capture is open).
@@ -1430,6 +1446,62 @@ PKCUDA_API int pk_system_set_tets(pk_system* s, int tet_count, const int* tet_no
     return PK_OK;
 }
 
+PKCUDA_API int pk_system_set_extras(pk_system* s, int block_count, const double* blocks, const int* block_nodes,
+                                    const int* rhs_start, const int* rhs_list, const int* mat_start,
+                                    const int* mat_list, const double* row_force)
+{
+    if (!s || block_count < 0) return fail(PK_ERR_ARG, "set_extras");
+    const void* old_bufs[7] = {s->ext_blocks.p, s->ext_nodes.p, s->ext_rhs_start.p, s->ext_rhs_list.p,
+                               s->ext_mat_start.p, s->ext_mat_list.p, s->ext_force.p};
+    const bool old_on = s->ext_on, old_force = s->ext_force_on;
+    const int old_count = s->ext_count;
+    s->ext_on = s->ext_force_on = false;
+    s->ext_count = 0;
+    const int rc = [&]() -> int {
+        if (block_count == 0 && !row_force) return PK_OK;
+        if (!s->have_pattern) return fail(PK_ERR_STATE, "extras before the pattern");
+        if (block_count > (1 << 28)) return fail(PK_ERR_ARG, "too many blocks");
+        const int n = s->dyn_count;
+        if (block_count > 0 && (!blocks || !block_nodes || !rhs_start || !mat_start))
+            return fail(PK_ERR_ARG, "set_extras: NULL array");
+        PK_CHECK(cudaSetDevice(s->device));
+        std::vector<int> zeros(static_cast<size_t>(n) + 1, 0);
+        const int* rs = block_count > 0 ? rhs_start : zeros.data();
+        const int* ms = block_count > 0 ? mat_start : zeros.data();
+        if (rs[0] != 0 || ms[0] != 0) return fail(PK_ERR_ARG, "extras start[0] != 0");
+        for (int r = 0; r < n; ++r)
+            if (rs[r + 1] < rs[r] || ms[r + 1] < ms[r]) return fail(PK_ERR_ARG, "extras starts not monotone");
+        for (long long i = 0; i < 2ll * block_count; ++i)
+            if (block_nodes[i] < 0 || block_nodes[i] >= s->node_count) return fail(PK_ERR_ARG, "block node out of range");
+        for (int i = 0; i < rs[n]; ++i)
+            if (rhs_list[i] < 0 || rhs_list[i] >= block_count) return fail(PK_ERR_ARG, "bad rhs entry");
+        for (int i = 0; i < ms[n]; ++i)
+            if ((mat_list[i] & 0x7fffffff) >= block_count) return fail(PK_ERR_ARG, "bad matrix entry");
+        int r = PK_OK;
+        if (block_count > 0) {
+            r = upload_real_any(s, s->ext_blocks, blocks, 9 * static_cast<size_t>(block_count));
+            if (!r) r = upload_raw<int>(s->ext_nodes, block_nodes, 2 * static_cast<size_t>(block_count), s->stream);
+            if (!r && rs[n] > 0) r = upload_raw<int>(s->ext_rhs_list, rhs_list, rs[n], s->stream);
+            if (!r && ms[n] > 0) r = upload_raw<int>(s->ext_mat_list, mat_list, ms[n], s->stream);
+        }
+        if (!r) r = upload_raw<int>(s->ext_rhs_start, rs, static_cast<size_t>(n) + 1, s->stream);
+        if (!r) r = upload_raw<int>(s->ext_mat_start, ms, static_cast<size_t>(n) + 1, s->stream);
+        if (!r && row_force) r = upload_real_any(s, s->ext_force, row_force, 3 * static_cast<size_t>(n));
+        if (r) return r;
+        PK_CHECK(cudaStreamSynchronize(s->stream));  // the host arrays may go away
+        s->ext_on = true;
+        s->ext_force_on = row_force != nullptr;
+        s->ext_count = block_count;
+        return PK_OK;
+    }();
+    const void* new_bufs[7] = {s->ext_blocks.p, s->ext_nodes.p, s->ext_rhs_start.p, s->ext_rhs_list.p,
+                               s->ext_mat_start.p, s->ext_mat_list.p, s->ext_force.p};
+    bool same = rc == PK_OK && s->ext_on == old_on && s->ext_force_on == old_force && s->ext_count == old_count;
+    for (int i = 0; i < 7 && same; ++i) same = old_bufs[i] == new_bufs[i];
+    if (!same) drop_graph(s);
+    return rc;
+}
+
 PKCUDA_API int pk_system_set_connections(pk_system* s, int count, const int* nodes, const double* params,
                                          const int* inc_start, const int* inc_list)
 {
@@ -1526,6 +1598,8 @@ PKCUDA_API int pk_system_set_pattern(pk_system* s, int dyn_count, const int* dyn
     s->seg_start.clear();
     s->batch_parts = 0;
     s->conn_count = 0;
+    s->ext_on = s->ext_force_on = false;
+    s->ext_count = 0;
     s->assembled = false;
     drop_graph(s);
     s->h_row_start.assign(row_start, row_start + dyn_count + 1);
@@ -2026,6 +2100,7 @@ PKCUDA_API int pk_system_adjoint_step(pk_system* s, const pk_step_params* p, con
     if (!(p->dt > 0.0)) return fail(PK_ERR_ARG, "dt must be > 0");
     if (s->dyn_count > 0 && !s->diag_first) return fail(PK_ERR_ARG, "every dynamic row needs its diagonal block first");
     if (s->conn_count > 0) return fail(PK_ERR_STATE, "the adjoint step does not take point connections");
+    if (s->ext_on) return fail(PK_ERR_STATE, "the adjoint step does not take host-emitted contributions");
     PK_CHECK(cudaSetDevice(s->device));
     drop_graph(s);
     if (s->dyn_count == 0) {
