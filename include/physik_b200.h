@@ -173,6 +173,53 @@ PHYSIK_B200_API void PHYSIK_SetScriptComponentCallback(PhysikWorldHandle world, 
                                                        PhysikExternalLogicCallback callback, void* userData);
 PHYSIK_B200_API void PHYSIK_ClearScriptComponentCallback(PhysikWorldHandle world,
                                                          PhysikComponentHandle scriptComponent);
+/* Post-step geometry: render buffers rebuilt after each PHYSIK_Step (Component::PostUpdate).
+ * Surface extraction   PhysiKAPI.h:179-191, PhysiKAPI.cpp:767-823; SurfaceExtractionComponent.cpp:
+ *   the boundary faces of the host mesh's active tets (3 local node indices each), wound
+ *   away from their tet, rebuilt when the host's topology changed.
+ * Surface visual       PhysiKAPI.h:193-228, PhysiKAPI.cpp:825-980; SurfaceVisualComponent.cpp:
+ *   three vertices per surface triangle at the host's local current positions, index
+ *   buffer 0, 1, 2, ..., flat normals ((0, 1, 0) for a degenerate triangle).
+ * Visual mesh          PhysiKAPI.h:252-287, PhysiKAPI.cpp:703-717, 1055-1170; VisualMeshComponent.cpp:
+ *   a render mesh embedded in the host's rest shape (PHYSIK_BuildVisualMeshEmbedding
+ *   returns 1 if any vertex landed in an active tet), skinned with the world positions
+ *   of its tets' nodes; triangles with a vertex outside the active tets are filtered out.
+ * The per-frame vertex and normal updates run on the device for a physics host and stay
+ * there until a getter reads them.  Getters return 0 on an invalid handle, index or
+ * NULL out-pointer; the Copy* functions return the number of elements written. */
+PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateSurfaceExtractionComponent(PhysikWorldHandle world,
+                                                                              PhysikComponentHandle hostTetMesh);
+PHYSIK_B200_API int PHYSIK_GetSurfaceTriangleIndexCount(PhysikWorldHandle world, PhysikComponentHandle surfaceExtraction);
+PHYSIK_B200_API int PHYSIK_CopySurfaceTriangleIndices(PhysikWorldHandle world, PhysikComponentHandle surfaceExtraction,
+                                                      int* outIndices, int maxIndexCount);
+PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateSurfaceVisualComponent(PhysikWorldHandle world,
+                                                                          PhysikComponentHandle surfaceExtraction);
+PHYSIK_B200_API int PHYSIK_GetSurfaceVisualVertexCount(PhysikWorldHandle world, PhysikComponentHandle surfaceVisual);
+PHYSIK_B200_API int PHYSIK_GetSurfaceVisualTriangleIndexCount(PhysikWorldHandle world,
+                                                              PhysikComponentHandle surfaceVisual);
+PHYSIK_B200_API int PHYSIK_GetSurfaceVisualNormalCount(PhysikWorldHandle world, PhysikComponentHandle surfaceVisual);
+PHYSIK_B200_API int PHYSIK_GetSurfaceVisualVertex(PhysikWorldHandle world, PhysikComponentHandle surfaceVisual,
+                                                  int visualVertexIndex, float* outX, float* outY, float* outZ);
+PHYSIK_B200_API int PHYSIK_GetSurfaceVisualTriangleIndex(PhysikWorldHandle world, PhysikComponentHandle surfaceVisual,
+                                                         int triangleIndexArrayIndex, int* outIndex);
+PHYSIK_B200_API int PHYSIK_GetSurfaceVisualNormal(PhysikWorldHandle world, PhysikComponentHandle surfaceVisual,
+                                                  int visualNormalIndex, float* outX, float* outY, float* outZ);
+PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateVisualMeshComponent(PhysikWorldHandle world,
+                                                                       PhysikComponentHandle hostTetMesh);
+PHYSIK_B200_API void PHYSIK_SetVisualMeshData(PhysikWorldHandle world, PhysikComponentHandle visualMesh,
+                                              const PhysikVec3* vertices, int vertexCount, const int* triangleIndices,
+                                              int triangleIndexCount);
+PHYSIK_B200_API int PHYSIK_BuildVisualMeshEmbedding(PhysikWorldHandle world, PhysikComponentHandle visualMesh);
+PHYSIK_B200_API int PHYSIK_GetVisualMeshVertexCount(PhysikWorldHandle world, PhysikComponentHandle visualMesh);
+PHYSIK_B200_API int PHYSIK_GetVisualMeshTriangleIndexCount(PhysikWorldHandle world, PhysikComponentHandle visualMesh);
+PHYSIK_B200_API int PHYSIK_CopyVisualMeshVertices(PhysikWorldHandle world, PhysikComponentHandle visualMesh,
+                                                  PhysikVec3* outVertices, int maxVertexCount);
+PHYSIK_B200_API int PHYSIK_CopyVisualMeshTriangleIndices(PhysikWorldHandle world, PhysikComponentHandle visualMesh,
+                                                         int* outIndices, int maxIndexCount);
+/* Whether a surface visual's or visual mesh's last update ran on the device: 1 / 0, -1
+ * for another handle (extension). */
+PHYSIK_B200_API int PHYSIK_B200_GetVisualUpdateOnDevice(PhysikWorldHandle world, PhysikComponentHandle visual);
+
 /* PhysiKAPI.h:300-334 */
 PHYSIK_B200_API void PHYSIK_DestroyComponent(PhysikWorldHandle world, PhysikComponentHandle component);
 PHYSIK_B200_API int PHYSIK_IsComponentHandleValid(PhysikWorldHandle world, PhysikComponentHandle component);

@@ -132,6 +132,30 @@ PKCUDA_API int pk_system_sphere_contacts(pk_system* sys, const double* center, d
                                          int* tets, double* points);
 PKCUDA_API int pk_system_get_snapshot_f32(pk_system* sys, int first_node, int count, float* x);
 
+/* Post-step geometry on the device, read back only when asked for.
+ * kind 0, surface triangles (SurfaceVisualComponent::UpdateVisualSurfaceGeometry,
+ *   SurfaceVisualComponent.cpp:150-213): `count` triangles of 3 world nodes each; an update
+ *   writes per triangle its 3 vertices (the node positions) and its flat normal
+ *   Cross(p1 - p0, p2 - p0) / length ((0, 1, 0) when the length is at most 1e-6) for
+ *   each of them (9 + 9 floats).
+ * kind 1, embedded vertices (VisualMeshComponent::UpdateDeformedVertices,
+ *   VisualMeshComponent.cpp:257-333): `count` vertices with 4 world nodes and 4 weights
+ *   each; an update writes ((x0 w0 + x1 w1) + x2 w2) + x3 w3 for the vertices marked live,
+ *   the others keep their value (`initial` at creation; 3 floats per vertex).
+ * Updates read the current positions or the frame-end snapshot
+ * (pk_system_snapshot_positions), on the system's stream, rounded to float (the copies the
+ * components hold), every operation a float operation rounded once.  An update fails with
+ * PK_ERR_STATE when a node id is beyond the system's node count.  The visual keeps its own
+ * device buffers; pk_visual_read copies them to the host (normals: kind 0 only, may be
+ * NULL) and waits for the stream. */
+typedef struct pk_visual pk_visual;
+PKCUDA_API int pk_visual_create(pk_system* sys, int kind, int count, const int* nodes, const float* weights,
+                                const float* initial, const unsigned char* live, pk_visual** out);
+PKCUDA_API int pk_visual_set_live(pk_visual* visual, pk_system* sys, const unsigned char* live);
+PKCUDA_API int pk_visual_update(pk_visual* visual, pk_system* sys, int from_snapshot);
+PKCUDA_API int pk_visual_read(pk_visual* visual, pk_system* sys, float* vertices, float* normals);
+PKCUDA_API int pk_visual_destroy(pk_visual* visual);
+
 /* Tets with world node ids and rest data already computed in the system precision
  * (FEMModel::InitializeTetRestData, BuildElasticityMatrix's lambda and mu).
  * enabled[t]: bit 0 = tet active, rest volume > 0 and its body simulated; bit 1 = linear FEM

@@ -263,6 +263,11 @@ def oracle_polar(f9, precision="f64"):
     return out.reshape(3, 3), it.value
 
 
+class RefHandle(C.Structure):
+    """PhysiK::ComponentHandle (Handles.h:10-19)."""
+    _fields_ = [("index", C.c_uint32), ("generation", C.c_uint32)]
+
+
 class Reference:
     """The reference itself (compiled from its sources), driven through ref_harness.cpp."""
 
@@ -364,6 +369,30 @@ class Reference:
         self.lib.ref_get_local_positions.argtypes = [_p, _i, _p]
         self.lib.ref_get_local_positions(self.h, body, _ptr(out))
         return out
+
+    def body_handle(self, body):
+        """The reference's ComponentHandle of a body (for its own C ABI)."""
+        out = np.zeros(2, np.uint32)
+        self.lib.ref_body_handle.argtypes = [_p, _i, _p]
+        self.lib.ref_body_handle(self.h, body, _ptr(out))
+        return RefHandle(int(out[0]), int(out[1]))
+
+    def world_handle(self):
+        self.lib.ref_world_handle.restype = _p
+        self.lib.ref_world_handle.argtypes = [_p]
+        return self.lib.ref_world_handle(self.h)
+
+    def api(self, name, restype, argtypes):
+        """One of the reference's own PHYSIK_* C functions (its float arguments are double
+        in the float->double build: use `self.real`)."""
+        f = getattr(self.lib, name)
+        f.restype = restype
+        f.argtypes = argtypes
+        return f
+
+    @property
+    def real(self):
+        return C.c_float if self.precision == "f32" else C.c_double
 
     def set_local_position(self, body, node, p):
         self.lib.ref_set_local_position.argtypes = [_p, _i, _i, _d, _d, _d]

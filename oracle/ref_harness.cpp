@@ -44,6 +44,7 @@ namespace {
 struct Harness {
     World world;
     std::vector<TetMeshPhysicsComponent*> bodies;
+    std::vector<ComponentHandle> bodyHandles;
     std::vector<CollisionSphereComponent*> spheres;
     std::unique_ptr<SolverData> dump;
     std::string error;
@@ -95,7 +96,16 @@ __attribute__((visibility("default"))) int ref_add_body(void* h, const double* p
     ComponentHandle handle = hh->world.AddComponent(std::move(component));
     if (!handle.IsValid()) return -1;
     hh->bodies.push_back(raw);
+    hh->bodyHandles.push_back(handle);
     return raw->GetGlobalNodeBeginIndex();
+}
+
+// The component handle of a body, for the reference's own C ABI (index, generation).
+__attribute__((visibility("default"))) void ref_body_handle(void* h, int body, std::uint32_t* out2)
+{
+    const ComponentHandle c = H(h)->bodyHandles.at(static_cast<std::size_t>(body));
+    out2[0] = c.index;
+    out2[1] = c.generation;
 }
 
 __attribute__((visibility("default"))) int ref_body_tet_count(void* h, int body)

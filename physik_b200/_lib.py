@@ -192,6 +192,24 @@ _SIGS = {
     "PHYSIK_B200_SetRefinement": (_i, [_p, _i]),
     "PHYSIK_B200_GetBodyConjugateGradientStats": (_i, [_p, _H, _p, _p, _p, _p]),
     "PHYSIK_B200_GetStream": (_p, [_p]),
+    "PHYSIK_CreateSurfaceExtractionComponent": (_H, [_p, _H]),
+    "PHYSIK_GetSurfaceTriangleIndexCount": (_i, [_p, _H]),
+    "PHYSIK_CopySurfaceTriangleIndices": (_i, [_p, _H, _p, _i]),
+    "PHYSIK_CreateSurfaceVisualComponent": (_H, [_p, _H]),
+    "PHYSIK_GetSurfaceVisualVertexCount": (_i, [_p, _H]),
+    "PHYSIK_GetSurfaceVisualTriangleIndexCount": (_i, [_p, _H]),
+    "PHYSIK_GetSurfaceVisualNormalCount": (_i, [_p, _H]),
+    "PHYSIK_GetSurfaceVisualVertex": (_i, [_p, _H, _i, _p, _p, _p]),
+    "PHYSIK_GetSurfaceVisualTriangleIndex": (_i, [_p, _H, _i, _p]),
+    "PHYSIK_GetSurfaceVisualNormal": (_i, [_p, _H, _i, _p, _p, _p]),
+    "PHYSIK_CreateVisualMeshComponent": (_H, [_p, _H]),
+    "PHYSIK_SetVisualMeshData": (_v, [_p, _H, _p, _i, _p, _i]),
+    "PHYSIK_BuildVisualMeshEmbedding": (_i, [_p, _H]),
+    "PHYSIK_GetVisualMeshVertexCount": (_i, [_p, _H]),
+    "PHYSIK_GetVisualMeshTriangleIndexCount": (_i, [_p, _H]),
+    "PHYSIK_CopyVisualMeshVertices": (_i, [_p, _H, _p, _i]),
+    "PHYSIK_CopyVisualMeshTriangleIndices": (_i, [_p, _H, _p, _i]),
+    "PHYSIK_B200_GetVisualUpdateOnDevice": (_i, [_p, _H]),
     "PHYSIK_B200_Synchronize": (_i, [_p]),
 }
 

@@ -356,6 +356,219 @@ PHYSIK_B200_API void PHYSIK_ClearScriptComponentCallback(PhysikWorldHandle world
     if (c) c->ClearExternalLogicCallback();
 }
 
+// ---- post-step geometry (PhysiKAPI.cpp:703-717, 767-980, 1055-1170) ----
+namespace {
+SurfaceExtractionComponent* AsSurfaceExtraction(World* w, PhysikComponentHandle h)
+{
+    return w ? dynamic_cast<SurfaceExtractionComponent*>(w->GetComponent(ToHandle(h))) : nullptr;
+}
+SurfaceVisualComponent* AsSurfaceVisual(World* w, PhysikComponentHandle h)
+{
+    return w ? dynamic_cast<SurfaceVisualComponent*>(w->GetComponent(ToHandle(h))) : nullptr;
+}
+VisualMeshComponent* AsVisualMesh(World* w, PhysikComponentHandle h)
+{
+    return w ? dynamic_cast<VisualMeshComponent*>(w->GetComponent(ToHandle(h))) : nullptr;
+}
+// Writes element i of a vector of Vec3 (getters fetch a pending device result first).
+int GetVec3(const std::vector<Vec3>& v, int i, float* x, float* y, float* z)
+{
+    if (i < 0 || i >= static_cast<int>(v.size())) return 0;
+    *x = v[static_cast<std::size_t>(i)].x;
+    *y = v[static_cast<std::size_t>(i)].y;
+    *z = v[static_cast<std::size_t>(i)].z;
+    return 1;
+}
+}  // namespace
+
+PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateSurfaceExtractionComponent(PhysikWorldHandle world,
+                                                                              PhysikComponentHandle hostTetMesh)
+{
+    World* w = AsWorld(world);
+    TetMeshComponent* host = AsTetMesh(w, hostTetMesh);
+    if (!w || !host) return InvalidHandle();
+    return Guard(
+        [&] {
+            return FromHandle(w->AddComponent(
+                std::make_unique<SurfaceExtractionComponent>(ToHandle(hostTetMesh), host->topologyEvents)));
+        },
+        InvalidHandle());
+}
+
+PHYSIK_B200_API int PHYSIK_GetSurfaceTriangleIndexCount(PhysikWorldHandle world, PhysikComponentHandle surfaceExtraction)
+{
+    const SurfaceExtractionComponent* c = AsSurfaceExtraction(AsWorld(world), surfaceExtraction);
+    return c ? static_cast<int>(c->GetSurfaceTriangleIndices().size()) : 0;
+}
+
+PHYSIK_B200_API int PHYSIK_CopySurfaceTriangleIndices(PhysikWorldHandle world, PhysikComponentHandle surfaceExtraction,
+                                                      int* outIndices, int maxIndexCount)
+{
+    if (!outIndices || maxIndexCount <= 0) return 0;
+    const SurfaceExtractionComponent* c = AsSurfaceExtraction(AsWorld(world), surfaceExtraction);
+    if (!c) return 0;
+    const std::vector<int>& v = c->GetSurfaceTriangleIndices();
+    const int n = std::min(maxIndexCount, static_cast<int>(v.size()));
+    std::copy(v.begin(), v.begin() + n, outIndices);
+    return n;
+}
+
+PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateSurfaceVisualComponent(PhysikWorldHandle world,
+                                                                          PhysikComponentHandle surfaceExtraction)
+{
+    World* w = AsWorld(world);
+    const SurfaceExtractionComponent* ex = AsSurfaceExtraction(w, surfaceExtraction);
+    if (!w || !ex) return InvalidHandle();
+    const TetMeshComponent* host = AsTetMesh(w, FromHandle(ex->GetHostTetMeshHandle()));
+    const std::uint64_t seen = host ? host->topologyEvents : 0;
+    return Guard(
+        [&] {
+            return FromHandle(
+                w->AddComponent(std::make_unique<SurfaceVisualComponent>(ToHandle(surfaceExtraction), seen)));
+        },
+        InvalidHandle());
+}
+
+PHYSIK_B200_API int PHYSIK_GetSurfaceVisualVertexCount(PhysikWorldHandle world, PhysikComponentHandle surfaceVisual)
+{
+    const SurfaceVisualComponent* c = AsSurfaceVisual(AsWorld(world), surfaceVisual);
+    return c ? Guard([&] { return static_cast<int>(c->GetVisualVertices().size()); }, 0) : 0;
+}
+
+PHYSIK_B200_API int PHYSIK_GetSurfaceVisualTriangleIndexCount(PhysikWorldHandle world,
+                                                              PhysikComponentHandle surfaceVisual)
+{
+    const SurfaceVisualComponent* c = AsSurfaceVisual(AsWorld(world), surfaceVisual);
+    return c ? static_cast<int>(c->GetVisualTriangleIndices().size()) : 0;
+}
+
+PHYSIK_B200_API int PHYSIK_GetSurfaceVisualNormalCount(PhysikWorldHandle world, PhysikComponentHandle surfaceVisual)
+{
+    const SurfaceVisualComponent* c = AsSurfaceVisual(AsWorld(world), surfaceVisual);
+    return c ? Guard([&] { return static_cast<int>(c->GetVisualNormals().size()); }, 0) : 0;
+}
+
+PHYSIK_B200_API int PHYSIK_GetSurfaceVisualVertex(PhysikWorldHandle world, PhysikComponentHandle surfaceVisual,
+                                                  int visualVertexIndex, float* outX, float* outY, float* outZ)
+{
+    if (!outX || !outY || !outZ) return 0;
+    const SurfaceVisualComponent* c = AsSurfaceVisual(AsWorld(world), surfaceVisual);
+    if (!c) return 0;
+    return Guard([&] { return GetVec3(c->GetVisualVertices(), visualVertexIndex, outX, outY, outZ); }, 0);
+}
+
+PHYSIK_B200_API int PHYSIK_GetSurfaceVisualTriangleIndex(PhysikWorldHandle world, PhysikComponentHandle surfaceVisual,
+                                                         int triangleIndexArrayIndex, int* outIndex)
+{
+    if (!outIndex) return 0;
+    const SurfaceVisualComponent* c = AsSurfaceVisual(AsWorld(world), surfaceVisual);
+    if (!c) return 0;
+    const std::vector<int>& v = c->GetVisualTriangleIndices();
+    if (triangleIndexArrayIndex < 0 || triangleIndexArrayIndex >= static_cast<int>(v.size())) return 0;
+    *outIndex = v[static_cast<std::size_t>(triangleIndexArrayIndex)];
+    return 1;
+}
+
+PHYSIK_B200_API int PHYSIK_GetSurfaceVisualNormal(PhysikWorldHandle world, PhysikComponentHandle surfaceVisual,
+                                                  int visualNormalIndex, float* outX, float* outY, float* outZ)
+{
+    if (!outX || !outY || !outZ) return 0;
+    const SurfaceVisualComponent* c = AsSurfaceVisual(AsWorld(world), surfaceVisual);
+    if (!c) return 0;
+    return Guard([&] { return GetVec3(c->GetVisualNormals(), visualNormalIndex, outX, outY, outZ); }, 0);
+}
+
+PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateVisualMeshComponent(PhysikWorldHandle world,
+                                                                       PhysikComponentHandle hostTetMesh)
+{
+    World* w = AsWorld(world);
+    TetMeshComponent* host = AsTetMesh(w, hostTetMesh);
+    if (!w || !host) return InvalidHandle();
+    return Guard(
+        [&] {
+            return FromHandle(w->AddComponent(
+                std::make_unique<VisualMeshComponent>(ToHandle(hostTetMesh), std::string{}, host->topologyEvents)));
+        },
+        InvalidHandle());
+}
+
+PHYSIK_B200_API void PHYSIK_SetVisualMeshData(PhysikWorldHandle world, PhysikComponentHandle visualMesh,
+                                              const PhysikVec3* vertices, int vertexCount, const int* triangleIndices,
+                                              int triangleIndexCount)
+{
+    VisualMeshComponent* c = AsVisualMesh(AsWorld(world), visualMesh);
+    if (!c) return;
+    GuardVoid([&] {
+        c->SetVisualMesh(reinterpret_cast<const Vec3*>(vertices), vertexCount, triangleIndices, triangleIndexCount);
+    });
+}
+
+PHYSIK_B200_API int PHYSIK_BuildVisualMeshEmbedding(PhysikWorldHandle world, PhysikComponentHandle visualMesh)
+{
+    World* w = AsWorld(world);
+    VisualMeshComponent* c = AsVisualMesh(w, visualMesh);
+    if (!w || !c) return 0;
+    return Guard(
+        [&] {
+            c->BuildEmbedding(*w);
+            for (const EmbeddedVertex& e : c->embeddedVertices)
+                if (e.valid) return 1;
+            return 0;
+        },
+        0);
+}
+
+PHYSIK_B200_API int PHYSIK_GetVisualMeshVertexCount(PhysikWorldHandle world, PhysikComponentHandle visualMesh)
+{
+    const VisualMeshComponent* c = AsVisualMesh(AsWorld(world), visualMesh);
+    return c ? Guard([&] { return static_cast<int>(c->GetDeformedVertices().size()); }, 0) : 0;
+}
+
+PHYSIK_B200_API int PHYSIK_GetVisualMeshTriangleIndexCount(PhysikWorldHandle world, PhysikComponentHandle visualMesh)
+{
+    const VisualMeshComponent* c = AsVisualMesh(AsWorld(world), visualMesh);
+    return c ? static_cast<int>(c->GetTriangleIndices().size()) : 0;
+}
+
+PHYSIK_B200_API int PHYSIK_CopyVisualMeshVertices(PhysikWorldHandle world, PhysikComponentHandle visualMesh,
+                                                  PhysikVec3* outVertices, int maxVertexCount)
+{
+    if (!outVertices || maxVertexCount <= 0) return 0;
+    const VisualMeshComponent* c = AsVisualMesh(AsWorld(world), visualMesh);
+    if (!c) return 0;
+    return Guard(
+        [&] {
+            const std::vector<Vec3>& v = c->GetDeformedVertices();
+            const int n = std::min(maxVertexCount, static_cast<int>(v.size()));
+            for (int i = 0; i < n; ++i)
+                outVertices[i] = PhysikVec3{v[static_cast<std::size_t>(i)].x, v[static_cast<std::size_t>(i)].y,
+                                            v[static_cast<std::size_t>(i)].z};
+            return n;
+        },
+        0);
+}
+
+PHYSIK_B200_API int PHYSIK_CopyVisualMeshTriangleIndices(PhysikWorldHandle world, PhysikComponentHandle visualMesh,
+                                                         int* outIndices, int maxIndexCount)
+{
+    if (!outIndices || maxIndexCount <= 0) return 0;
+    const VisualMeshComponent* c = AsVisualMesh(AsWorld(world), visualMesh);
+    if (!c) return 0;
+    const std::vector<int>& v = c->GetTriangleIndices();
+    const int n = std::min(maxIndexCount, static_cast<int>(v.size()));
+    std::copy(v.begin(), v.begin() + n, outIndices);
+    return n;
+}
+
+// Whether a surface visual's / visual mesh's last update ran on the device (extension).
+PHYSIK_B200_API int PHYSIK_B200_GetVisualUpdateOnDevice(PhysikWorldHandle world, PhysikComponentHandle visual)
+{
+    World* w = AsWorld(world);
+    if (const SurfaceVisualComponent* s = AsSurfaceVisual(w, visual)) return s->LastUpdateOnDevice() ? 1 : 0;
+    if (const VisualMeshComponent* m = AsVisualMesh(w, visual)) return m->LastUpdateOnDevice() ? 1 : 0;
+    return -1;
+}
+
 PHYSIK_B200_API PhysikComponentHandle PHYSIK_CreateTetMeshComponent(PhysikWorldHandle world,
                                                                      PhysikGeneratedTetMeshHandle mesh)
 {

@@ -30,6 +30,7 @@
 #include "physik_math.h"
 
 struct pk_system;
+struct pk_visual;
 
 namespace PhysiK {
 
@@ -280,6 +281,9 @@ public:
     virtual void PreUpdate(World&, float) {}
     virtual void UpdateSystem(World&, SolverData&, float) {}
     virtual void PostUpdate(World&, float) {}
+    // Called before the world's device system is replaced: copy any result still on the
+    // device to the host and drop what was allocated on that system (extension).
+    virtual void ReleaseDeviceResources() {}
     virtual ~Component() = default;
 };
 
@@ -404,6 +408,12 @@ public:
     std::vector<Vec3> nodePositions;
     std::vector<Tet> tets;
     bool topologyDirty = false;
+    // TetMeshTopologyChanged events emitted so far (TetMeshComponent::PostUpdate,
+    // TetMeshComponent.cpp:190-206, emits one when topologyDirty is set).  Listeners keep
+    // the count they have seen and compare it in their own PostUpdate, which comes later in
+    // the frame, so they see an event in the frame it is emitted, as the reference's
+    // synchronous dispatch delivers it.
+    std::uint64_t topologyEvents = 0;
 
     ComponentExecutionPriority GetExecutionPriority() const override
     {
@@ -484,6 +494,144 @@ public:
     // snapshot generation this component's copy should show, snapshotLoaded the one it
     // holds.
     std::uint64_t snapshotWanted = 0, snapshotLoaded = 0;
+};
+
+// ------------------------------------------------------------------ post-step geometry
+// Render buffers built after the step (SurfaceExtractionComponent.cpp,
+// SurfaceVisualComponent.cpp, VisualMeshComponent.cpp).  The per-frame updates run on the
+// device when the positions they read are there (World::GeometrySystem): the frame-end
+// snapshot behind a physics body's local copies, or the world's current positions.  The
+// results stay on the device until a getter asks for them, so a frame costs no
+// device-to-host copy of the nodes.  Otherwise (a plain tet mesh, local copies edited on
+// the host, host-side state) the host computes them as the reference does.
+
+// A device visual (pk_visual) on the world's device system and whether it holds a result
+// the host buffers have not received yet.
+struct DeviceVisual {
+    pk_visual* visual = nullptr;
+    pk_system* system = nullptr;
+    bool pending = false;
+    DeviceVisual() = default;
+    DeviceVisual(const DeviceVisual&) = delete;
+    DeviceVisual& operator=(const DeviceVisual&) = delete;
+    ~DeviceVisual() { Release(); }
+    void Release();
+    // Copies a pending result (vertices: 3 floats each; normals may be null) and clears it.
+    void Fetch(float* vertices, float* normals);
+};
+
+// SurfaceExtractionComponent (SurfaceExtractionComponent.cpp:138-250): the boundary faces
+// of the host mesh's active tets, each oriented away from its tet's fourth node at the
+// local current positions, rebuilt in PostUpdate when the host's topology changed.
+class SurfaceExtractionComponent : public Component {
+public:
+    SurfaceExtractionComponent(ComponentHandle hostTetMeshHandle, std::uint64_t topologyEventsSeen);
+    ComponentExecutionPriority GetExecutionPriority() const override
+    {
+        return ComponentExecutionPriority::SurfaceExtractionComponent;
+    }
+    ComponentHandle hostTetMeshHandle;
+    std::vector<int> surfaceTriangleIndices;
+    bool surfaceDirty = true;
+
+    void RebuildSurface(World& world);
+    const std::vector<int>& GetSurfaceTriangleIndices() const { return surfaceTriangleIndices; }
+    ComponentHandle GetHostTetMeshHandle() const { return hostTetMeshHandle; }
+    void PostUpdate(World& world, float dt) override;
+
+private:
+    std::uint64_t topologyEventsSeen = 0;
+};
+
+// SurfaceVisualComponent (SurfaceVisualComponent.cpp): three unshared vertices per surface
+// triangle at the local current positions of its nodes, each with the triangle's flat
+// normal.  The topology is rebuilt when the extraction's host mesh changed; the vertices
+// and normals are recomputed every PostUpdate.
+class SurfaceVisualComponent : public Component {
+public:
+    SurfaceVisualComponent(ComponentHandle surfaceExtractionHandle, std::uint64_t topologyEventsSeen);
+    ComponentExecutionPriority GetExecutionPriority() const override
+    {
+        return ComponentExecutionPriority::SurfaceVisualComponent;
+    }
+    void RebuildVisualSurfaceTopology(World& world);
+    void UpdateVisualSurfaceGeometry(World& world);
+    const std::vector<Vec3>& GetVisualVertices() const;
+    const std::vector<int>& GetVisualTriangleIndices() const { return visualTriangleIndices; }
+    const std::vector<Vec3>& GetVisualNormals() const;
+    ComponentHandle GetSurfaceExtractionHandle() const { return surfaceExtractionHandle; }
+    void PostUpdate(World& world, float dt) override;
+    void ReleaseDeviceResources() override;
+    // Whether the last update ran on the device (extension, for tests).
+    bool LastUpdateOnDevice() const { return lastOnDevice; }
+
+private:
+    void FetchDevice() const;
+    ComponentHandle surfaceExtractionHandle;
+    mutable std::vector<Vec3> visualVertices;
+    std::vector<int> visualTriangleIndices;
+    mutable std::vector<Vec3> visualNormals;
+    std::vector<int> visualVertexSourceNodeIndices;
+    bool topologyDirty = true;
+    std::uint64_t topologyEventsSeen = 0;
+    bool lastOnDevice = false;
+    mutable DeviceVisual device;
+    int deviceNodeCount = -1;  // the host mesh's node count the device visual was built for
+};
+
+// VisualMeshComponent::EmbeddedVertex (VisualMeshComponent.h:10-15).
+struct EmbeddedVertex {
+    int tetIndex = -1;
+    Vec4 barycentric;
+    bool valid = false;
+};
+
+// ComputeTetBarycentric (VisualMeshComponent.cpp:14-42): the barycentric coordinates of p
+// in tet (a, b, c, d); false (and zeros) when |det| <= 1e-8.
+bool ComputeTetBarycentric(const Vec3& p, const Vec3& a, const Vec3& b, const Vec3& c, const Vec3& d,
+                           Vec4& outBarycentric);
+
+// VisualMeshComponent (VisualMeshComponent.cpp): a render mesh embedded in the host tet
+// mesh's rest shape (each vertex in the first active tet, in index order, that holds it
+// within -1e-4 barycentric slack), deformed every PostUpdate with the world positions of
+// that tet's nodes; triangles with a vertex outside the active tets are filtered out.
+class VisualMeshComponent : public Component {
+public:
+    VisualMeshComponent(ComponentHandle hostTetMeshHandle, std::string debugEntityName,
+                        std::uint64_t topologyEventsSeen);
+    ComponentExecutionPriority GetExecutionPriority() const override
+    {
+        return ComponentExecutionPriority::VisualMeshComponent;
+    }
+    ComponentHandle hostTetMeshHandle;
+    std::string debugEntityName;
+    bool topologyDirty = false;
+    std::vector<Vec3> restVisualVertices;
+    std::vector<int> triangleIndices;
+    std::vector<int> filteredTriangleIndices;
+    std::vector<EmbeddedVertex> embeddedVertices;
+    std::vector<bool> triangleValid;
+
+    void SetVisualMesh(const Vec3* vertices, int vertexCount, const int* triangleIndices, int triangleIndexCount);
+    void BuildEmbedding(World& world);
+    void UpdateTriangleValidity(World& world);
+    void UpdateDeformedVertices(World& world);
+    const std::vector<Vec3>& GetDeformedVertices() const;
+    const std::vector<int>& GetTriangleIndices() const { return filteredTriangleIndices; }
+    void PostUpdate(World& world, float dt) override;
+    void ReleaseDeviceResources() override;
+    bool LastUpdateOnDevice() const { return lastOnDevice; }
+
+private:
+    void FetchDevice() const;
+    mutable std::vector<Vec3> deformedVisualVertices;
+    std::uint64_t topologyEventsSeen = 0;
+    bool lastOnDevice = false;
+    mutable DeviceVisual device;
+    std::uint64_t embeddingVersion = 1;  // bumped by SetVisualMesh / BuildEmbedding
+    std::uint64_t deviceEmbedding = 0;   // the embedding the device visual was built from
+    std::uint64_t deviceBodyVersion = 0; // the host body's version its live flags follow
+    std::vector<unsigned char> LiveFlags(const TetMeshComponent& host) const;
 };
 
 // ------------------------------------------------------------------ world
@@ -623,6 +771,10 @@ public:
     std::uint64_t GetSnapshotGeneration() const { return snapshotGeneration; }
     // This substep's valid host-emitted masses (node, mass, after its body's lumped masses).
     const std::vector<std::tuple<int, float, bool>>& GetExtraMasses() const { return extras.masses; }
+    // The device system when it holds the positions a post-step geometry update reads:
+    // `body`'s frame-end local copies (snapshot, while the host copy has not been loaded
+    // or edited) or the world's current positions; nullptr when only the host has them.
+    pk_system* GeometrySystem(const TetMeshPhysicsComponent* body, bool snapshot) const;
     void MarkTopologyDirty() { ++topologyVersion; }
     std::uint64_t GetTopologyVersion() const { return topologyVersion; }
 

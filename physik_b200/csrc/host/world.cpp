@@ -237,7 +237,11 @@ int TetMeshComponent::GetActiveTetCount() const
     return c;
 }
 
-void TetMeshComponent::PostUpdate(World&, float) { topologyDirty = false; }
+void TetMeshComponent::PostUpdate(World&, float)
+{
+    if (topologyDirty) ++topologyEvents;  // TetMeshTopologyChanged (TetMeshComponent.cpp:190-206)
+    topologyDirty = false;
+}
 
 // ------------------------------------------------------------------ TetMeshPhysicsComponent
 std::unique_ptr<TetMeshPhysicsComponent> TetMeshPhysicsComponent::CreateFromGeneratedTetMesh(
@@ -741,7 +745,10 @@ ComponentHandle World::AddComponent(std::unique_ptr<Component> component)
         slot = static_cast<std::uint32_t>(components.size() - 1);
     }
     orderedComponents.emplace(static_cast<int>(raw->GetExecutionPriority()), raw);
-    ++topologyVersion;
+    // Render-buffer components add nothing to the implicit system.
+    const bool geometry = dynamic_cast<SurfaceExtractionComponent*>(raw) || dynamic_cast<SurfaceVisualComponent*>(raw) ||
+                          dynamic_cast<VisualMeshComponent*>(raw);
+    if (!geometry) ++topologyVersion;
     return ComponentHandle{slot, componentGenerations[slot]};
 }
 
@@ -761,12 +768,14 @@ void World::DestroyComponent(ComponentHandle h)
 {
     if (!IsComponentHandleValid(h)) return;
     Component* c = components[h.index].get();
+    const bool geometry = dynamic_cast<SurfaceExtractionComponent*>(c) || dynamic_cast<SurfaceVisualComponent*>(c) ||
+                          dynamic_cast<VisualMeshComponent*>(c);
     for (auto it = orderedComponents.begin(); it != orderedComponents.end();)
         it = it->second == c ? orderedComponents.erase(it) : std::next(it);
     components[h.index].reset();
     if (++componentGenerations[h.index] == 0u) componentGenerations[h.index] = 1u;
     freeComponentSlots.push_back(h.index);
-    ++topologyVersion;
+    if (!geometry) ++topologyVersion;
 }
 
 Node& World::GetNode(int index) { return nodes.at(static_cast<std::size_t>(index)); }
@@ -931,6 +940,17 @@ unsigned World::GetLastStepFlags() const
 }
 
 pk_system* World::GetDeviceSystem() { return scene && scene->uploaded ? scene->sys : nullptr; }
+
+pk_system* World::GeometrySystem(const TetMeshPhysicsComponent* body, bool snapshot) const
+{
+    if (!scene || !scene->sys) return nullptr;
+    if (snapshot)
+        return body && body->snapshotLoaded != body->snapshotWanted && body->snapshotWanted == snapshotGeneration
+                   ? scene->sys
+                   : nullptr;
+    const bool live = scene->uploaded && !deviceStale && scene->worldVersion == topologyVersion;
+    return live ? scene->sys : nullptr;
+}
 
 bool World::SceneMatchesDevice() const
 {
@@ -1103,6 +1123,8 @@ void World::EnsureScene(bool upload)
     const std::vector<const TetMeshPhysicsComponent*>& fem = solverData.GetFemBodies();
     if (!scene || scene->precision != precision || scene->device != device) {
         FlushLocalPositionSnapshots();
+        for (auto& c : components)
+            if (c) c->ReleaseDeviceResources();
         EnsureHostState();
         scene = std::make_unique<DeviceScene>();
         scene->precision = precision;

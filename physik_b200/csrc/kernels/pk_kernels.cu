@@ -235,6 +235,77 @@ __global__ void sphere_contact_kernel(const int4* __restrict__ nodes, const unsi
     out_point[3 * (size_t)slot + 2] = p[2];
 }
 
+// ------------------------------------------------------------------ post-step geometry
+// Surface triangles (SurfaceVisualComponent::UpdateVisualSurfaceGeometry,
+// SurfaceVisualComponent.cpp:150-213): each triangle's three node positions become its three
+// visual vertices and its flat normal Cross(p1 - p0, p2 - p0) / length (0, 1, 0 when the
+// length is at most 1e-6) their normals.  Embedded vertices (VisualMeshComponent::
+// UpdateDeformedVertices, VisualMeshComponent.cpp:257-333): ((x0 w0 + x1 w1) + x2 w2) + x3 w3
+// for the vertices marked live, the others keep their last value.  The positions these read
+// are the float copies the components hold (a double state is rounded to float first), and
+// every operation is a float operation rounded once, as the reference's Vec3 code does.
+template <class Real>
+__global__ void surface_triangle_kernel(const int* __restrict__ nodes, int count, const Real* __restrict__ x,
+                                        float* __restrict__ verts, float* __restrict__ normals)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    float p[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int n = __ldg(nodes + 3 * t + k);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) p[k][a] = static_cast<float>(__ldg(x + 3 * (size_t)n + a));
+    }
+    float e1[3], e2[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        e1[a] = __fsub_rn(p[1][a], p[0][a]);
+        e2[a] = __fsub_rn(p[2][a], p[0][a]);
+    }
+    const float cx = __fsub_rn(__fmul_rn(e1[1], e2[2]), __fmul_rn(e1[2], e2[1]));
+    const float cy = __fsub_rn(__fmul_rn(e1[2], e2[0]), __fmul_rn(e1[0], e2[2]));
+    const float cz = __fsub_rn(__fmul_rn(e1[0], e2[1]), __fmul_rn(e1[1], e2[0]));
+    const float len = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(cx, cx), __fmul_rn(cy, cy)), __fmul_rn(cz, cz)));
+    float nrm[3] = {0.0f, 1.0f, 0.0f};
+    if (len > 0.000001f) {
+        nrm[0] = __fdiv_rn(cx, len);
+        nrm[1] = __fdiv_rn(cy, len);
+        nrm[2] = __fdiv_rn(cz, len);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            verts[9 * (size_t)t + 3 * k + a] = p[k][a];
+            normals[9 * (size_t)t + 3 * k + a] = nrm[a];
+        }
+}
+
+template <class Real>
+__global__ void embedded_vertex_kernel(const int* __restrict__ nodes, const float* __restrict__ weights,
+                                       const unsigned char* __restrict__ live, int count, const Real* __restrict__ x,
+                                       float* __restrict__ verts)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= count || !__ldg(live + v)) return;
+    int n[4];
+    float w[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        n[k] = __ldg(nodes + 4 * v + k);
+        w[k] = __ldg(weights + 4 * v + k);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float acc = __fmul_rn(static_cast<float>(__ldg(x + 3 * (size_t)n[0] + a)), w[0]);
+#pragma unroll
+        for (int k = 1; k < 4; ++k)
+            acc = __fadd_rn(acc, __fmul_rn(static_cast<float>(__ldg(x + 3 * (size_t)n[k] + a)), w[k]));
+        verts[3 * (size_t)v + a] = acc;
+    }
+}
+
 template <class Real>
 __global__ void tet_pack_kernel(const Real* __restrict__ dm_inv, const Real* __restrict__ params, Real* rec,
                                 int tet_count)
@@ -602,6 +673,18 @@ cudaError_t launch_sphere_contacts(const int* nodes, const unsigned char* flags,
 }
 
 template <class Real>
+cudaError_t launch_visual_kernel(int kind, const int* nodes, const float* weights, const unsigned char* live, int count,
+                                 const Real* x, float* verts, float* normals, cudaStream_t stream)
+{
+    if (count <= 0) return cudaSuccess;
+    if (kind == 0)
+        surface_triangle_kernel<Real><<<(count + 127) / 128, 128, 0, stream>>>(nodes, count, x, verts, normals);
+    else
+        embedded_vertex_kernel<Real><<<(count + 127) / 128, 128, 0, stream>>>(nodes, weights, live, count, x, verts);
+    return cudaGetLastError();
+}
+
+template <class Real>
 cudaError_t launch_conn_kernel(const AssemblyArgs<Real>& args, cudaStream_t stream)
 {
     if (args.conn_count <= 0) return cudaSuccess;
@@ -650,6 +733,10 @@ template cudaError_t launch_tet_pack<float>(const float*, const float*, float*, 
 template cudaError_t launch_conn_kernel<float>(const AssemblyArgs<float>&, cudaStream_t);
 template cudaError_t launch_conn_kernel<double>(const AssemblyArgs<double>&, cudaStream_t);
 template cudaError_t launch_tet_pack<double>(const double*, const double*, double*, int, cudaStream_t);
+template cudaError_t launch_visual_kernel<float>(int, const int*, const float*, const unsigned char*, int,
+                                                 const float*, float*, float*, cudaStream_t);
+template cudaError_t launch_visual_kernel<double>(int, const int*, const float*, const unsigned char*, int,
+                                                  const double*, float*, float*, cudaStream_t);
 template cudaError_t launch_sphere_contacts<float>(const int*, const unsigned char*, const float*, int, const float*,
                                                    float, int, int*, int*, float*, cudaStream_t);
 template cudaError_t launch_sphere_contacts<double>(const int*, const unsigned char*, const double*, int,

@@ -417,6 +417,9 @@ cudaError_t launch_tet_kernel(const AssemblyArgs<Real>& args, bool fp64_polar_fa
 template <class Real>
 cudaError_t launch_tet_pack(const Real* dm_inv, const Real* params, Real* rec, int tet_count, cudaStream_t stream);
 template <class Real>
+cudaError_t launch_visual_kernel(int kind, const int* nodes, const float* weights, const unsigned char* live, int count,
+                                 const Real* x, float* verts, float* normals, cudaStream_t stream);
+template <class Real>
 cudaError_t launch_sphere_contacts(const int* nodes, const unsigned char* flags, const Real* x, int tet_count,
                                    const Real* center, Real radius, int max_out, int* count, int* out_tet,
                                    Real* out_point, cudaStream_t stream);

@@ -12,6 +12,7 @@
 #include <cstring>
 #include <string>
 #include <type_traits>
+#include <memory>
 #include <vector>
 
 #include "../../../include/pkcuda.h"
@@ -1375,6 +1376,99 @@ PKCUDA_API int pk_system_sphere_contacts(pk_system* s, const double* center, dou
         for (int a = 0; a < 3; ++a) points[3 * (size_t)i + a] = p[3 * (size_t)order[i] + a];
     }
     return n;
+}
+
+// ------------------------------------------------------------------ post-step geometry
+struct pk_visual {
+    int device = 0;
+    int kind = 0;
+    int count = 0;
+    int max_node = -1;  // the largest node id the visual reads; checked against the system at each update
+    DevBuf nodes, weights, live, verts, normals;
+};
+
+PKCUDA_API int pk_visual_create(pk_system* s, int kind, int count, const int* nodes, const float* weights,
+                                const float* initial, const unsigned char* live, pk_visual** out)
+{
+    if (!out) return fail(PK_ERR_ARG, "visual_create: out");
+    *out = nullptr;
+    if (!s || (kind != 0 && kind != 1) || count < 0 || (count > 0 && !nodes) ||
+        (kind == 1 && count > 0 && (!weights || !initial || !live)))
+        return fail(PK_ERR_ARG, "visual_create");
+    if (!s->have_nodes) return fail(PK_ERR_STATE, "visual_create before set_nodes");
+    const int per = kind == 0 ? 3 : 4;
+    int max_node = -1;
+    for (long long i = 0; i < static_cast<long long>(per) * count; ++i) {
+        if (nodes[i] < 0 || nodes[i] >= s->node_count) return fail(PK_ERR_ARG, "visual node out of range");
+        max_node = std::max(max_node, nodes[i]);
+    }
+    PK_CHECK(cudaSetDevice(s->device));
+    auto v = std::make_unique<pk_visual>();
+    v->device = s->device;
+    v->kind = kind;
+    v->count = count;
+    v->max_node = max_node;
+    const size_t n = static_cast<size_t>(count);
+    int rc = upload_raw<int>(v->nodes, nodes, per * n, s->stream);
+    if (!rc && kind == 1) rc = upload_raw<float>(v->weights, weights, 4 * n, s->stream);
+    if (!rc && kind == 1) rc = upload_raw<unsigned char>(v->live, live, n, s->stream);
+    if (!rc) PK_CHECK(v->verts.ensure(sizeof(float) * (kind == 0 ? 9 : 3) * std::max<size_t>(n, 1)));
+    if (!rc && kind == 0) PK_CHECK(v->normals.ensure(sizeof(float) * 9 * std::max<size_t>(n, 1)));
+    if (!rc && kind == 1) rc = upload_raw<float>(v->verts, initial, 3 * n, s->stream);
+    if (rc) return rc;
+    *out = v.release();
+    return PK_OK;
+}
+
+PKCUDA_API int pk_visual_set_live(pk_visual* v, pk_system* s, const unsigned char* live)
+{
+    if (!v || !s || v->kind != 1 || (v->count > 0 && !live)) return fail(PK_ERR_ARG, "visual_set_live");
+    if (v->device != s->device) return fail(PK_ERR_STATE, "visual on another device");
+    PK_CHECK(cudaSetDevice(v->device));
+    return upload_raw<unsigned char>(v->live, live, static_cast<size_t>(v->count), s->stream);
+}
+
+PKCUDA_API int pk_visual_update(pk_visual* v, pk_system* s, int from_snapshot)
+{
+    if (!v || !s) return fail(PK_ERR_ARG, "visual_update");
+    if (v->device != s->device) return fail(PK_ERR_STATE, "visual on another device");
+    if (from_snapshot && !s->have_snapshot) return fail(PK_ERR_STATE, "visual_update: no snapshot");
+    if (v->max_node >= s->node_count) return fail(PK_ERR_STATE, "visual_update: nodes beyond the system");
+    if (v->count == 0) return PK_OK;
+    PK_CHECK(cudaSetDevice(v->device));
+    const DevBuf& src = from_snapshot ? s->snap_x : s->x;
+    if (s->precision == PK_PREC_FP64)
+        PK_CHECK(pk::launch_visual_kernel<double>(v->kind, v->nodes.as<int>(), v->weights.as<float>(),
+                                                  v->live.as<unsigned char>(), v->count, src.as<double>(),
+                                                  v->verts.as<float>(), v->normals.as<float>(), s->stream));
+    else
+        PK_CHECK(pk::launch_visual_kernel<float>(v->kind, v->nodes.as<int>(), v->weights.as<float>(),
+                                                 v->live.as<unsigned char>(), v->count, src.as<float>(),
+                                                 v->verts.as<float>(), v->normals.as<float>(), s->stream));
+    s->launches += 1;
+    return PK_OK;
+}
+
+PKCUDA_API int pk_visual_read(pk_visual* v, pk_system* s, float* vertices, float* normals)
+{
+    if (!v || !s) return fail(PK_ERR_ARG, "visual_read");
+    if (v->device != s->device) return fail(PK_ERR_STATE, "visual on another device");
+    if (v->count == 0) return PK_OK;
+    PK_CHECK(cudaSetDevice(v->device));
+    const size_t n = static_cast<size_t>(v->count) * (v->kind == 0 ? 9 : 3);
+    if (vertices) PK_CHECK(cudaMemcpyAsync(vertices, v->verts.p, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    if (normals && v->kind == 0)
+        PK_CHECK(cudaMemcpyAsync(normals, v->normals.p, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    return PK_OK;
+}
+
+PKCUDA_API int pk_visual_destroy(pk_visual* v)
+{
+    if (!v) return PK_OK;
+    cudaSetDevice(v->device);
+    delete v;
+    return PK_OK;
 }
 
 PKCUDA_API int pk_system_get_snapshot_f32(pk_system* s, int first_node, int count, float* x)
