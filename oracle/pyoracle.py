@@ -143,8 +143,9 @@ class Oracle:
             self.h = None
 
     def set_state(self, x, v):
-        self.x = np.ascontiguousarray(x, dtype=self.dtype)
-        self.v = np.ascontiguousarray(v, dtype=self.dtype)
+        # copies: step() updates the state in place, so it must not alias a caller's array
+        self.x = np.array(x, dtype=self.dtype, order="C", copy=True)
+        self.v = np.array(v, dtype=self.dtype, order="C", copy=True)
 
     def set_tet_young(self, young):
         y = np.ascontiguousarray(young, dtype=self.dtype)

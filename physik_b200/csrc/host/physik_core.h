@@ -414,6 +414,9 @@ public:
     // the frame, so they see an event in the frame it is emitted, as the reference's
     // synchronous dispatch delivers it.
     std::uint64_t topologyEvents = 0;
+    // SetLocalCurrentPosition calls so far (a copy edited after the frame is no longer the
+    // frame-end snapshot the device holds).
+    std::uint64_t localEdits = 0;
 
     ComponentExecutionPriority GetExecutionPriority() const override
     {
@@ -494,6 +497,7 @@ public:
     // snapshot generation this component's copy should show, snapshotLoaded the one it
     // holds.
     std::uint64_t snapshotWanted = 0, snapshotLoaded = 0;
+    std::uint64_t snapshotEdits = 0;  // localEdits when the copy last became the frame-end snapshot
 };
 
 // ------------------------------------------------------------------ post-step geometry
@@ -827,7 +831,8 @@ private:
     mutable ConjugateGradientResult lastConjugateGradientResult;
     mutable unsigned lastFlags = 0;
     mutable bool statsPending = false;
-    std::uint64_t snapshotGeneration = 0;  // substeps whose start positions the device snapshot held
+    std::uint64_t snapshotGeneration = 0;  // frames whose end positions the device snapshot held
+    bool snapshotOnDevice = false;         // the device holds snapshot `snapshotGeneration`
     std::vector<const CollisionSphereComponent*> sphereRequests;  // this substep's, in update order
     // Host-emitted SolverData contributions of this substep (custom components'
     // AddNodeMass / AddNodeForce / AddStiffnessBlock), sorted out for the device step.

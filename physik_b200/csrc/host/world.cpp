@@ -176,6 +176,7 @@ void TetMeshComponent::SetLocalCurrentPosition(int i, const Vec3& p)
 {
     if (i < 0 || i >= static_cast<int>(nodePositions.size())) return;
     nodePositions[static_cast<std::size_t>(i)] = p;
+    ++localEdits;
 }
 
 int TetMeshComponent::GetLocalNodeIndexOf(int globalNodeIndex) const
@@ -341,7 +342,10 @@ void TetMeshPhysicsComponent::UpdateSystem(World&, SolverData& solverData, float
 
 void TetMeshPhysicsComponent::PostUpdate(World& world, float dt)
 {
-    if (dt > 0.0f) snapshotWanted = world.GetSnapshotGeneration();  // SyncCurrentPositionsFromWorld, lazily
+    if (dt > 0.0f) {  // SyncCurrentPositionsFromWorld, lazily
+        snapshotWanted = world.GetSnapshotGeneration();
+        snapshotEdits = localEdits;
+    }
     TetMeshComponent::PostUpdate(world, dt);
 }
 
@@ -945,7 +949,8 @@ pk_system* World::GeometrySystem(const TetMeshPhysicsComponent* body, bool snaps
 {
     if (!scene || !scene->sys) return nullptr;
     if (snapshot)
-        return body && body->snapshotLoaded != body->snapshotWanted && body->snapshotWanted == snapshotGeneration
+        return snapshotOnDevice && body && body->snapshotWanted == snapshotGeneration &&
+                       body->localEdits == body->snapshotEdits
                    ? scene->sys
                    : nullptr;
     const bool live = scene->uploaded && !deviceStale && scene->worldVersion == topologyVersion;
@@ -1123,6 +1128,7 @@ void World::EnsureScene(bool upload)
     const std::vector<const TetMeshPhysicsComponent*>& fem = solverData.GetFemBodies();
     if (!scene || scene->precision != precision || scene->device != device) {
         FlushLocalPositionSnapshots();
+        snapshotOnDevice = false;
         for (auto& c : components)
             if (c) c->ReleaseDeviceResources();
         EnsureHostState();
@@ -1169,6 +1175,7 @@ void World::EnsureScene(bool upload)
     const bool patternChanged = SyncConnections();
     if (upload && !scene->uploaded) {
         FlushLocalPositionSnapshots();  // the upload drops the device snapshot
+        snapshotOnDevice = false;
         EnsureHostState();
         if (!scene->sys) Check(pk_system_create(device, static_cast<int>(precision), &scene->sys), "pk_system_create");
         UploadScene(*scene, positions, velocities);
@@ -1651,6 +1658,7 @@ void World::SnapshotPositions()
     }
     Check(pk_system_snapshot_positions(scene->sys), "snapshot_positions");
     ++snapshotGeneration;
+    snapshotOnDevice = true;
 }
 
 }  // namespace PhysiK

@@ -188,10 +188,58 @@ __global__ void __launch_bounds__(256) tet_kernel(AssemblyArgs<Real> A)
     const Real sxy = vol * two_mu * exy, syz = vol * two_mu * eyz, sxz = vol * two_mu * exz;
     const M3<Real> sig = mcols(v3<Real>(sxx, sxy, sxz), v3<Real>(sxy, syy, syz), v3<Real>(sxz, syz, szz));
     const M3<Real> S = linear ? sig : mul(R, sig);
+    M3<Real> out = S;
+    Real form = Real(0);
+    if (A.inc_slot && !A.explicit_mode) {
+        // The tet's stiffness times the velocities, folded: with K_ab = R Ke_ab R^T and
+        // Ke_ab = V (lambda g_a g_b^T + mu g_b g_a^T + mu (g_a.g_b) I),
+        //   sum_b K_ab v_b = Q g_a,  Q = V R (lambda tr(G) I + mu (G + G^T)),
+        //   G = R^T sum_b v_b g_b^T = R^T [v1 - v0, v2 - v0, v3 - v0] DmInv,
+        // so the row kernel adds T g_a - dt c v_a with T = -(dt S + dt^2 Q) instead of
+        // building all 16 blocks.  Used only when every corner force -S g_k - c v_k (the
+        // row kernel's force term) and T are finite and no block can overflow; otherwise
+        // the row kernel takes the long way with S, which applies the reference's rules
+        // for non-finite forces and blocks.
+        const V3<Real> vk[4] = {ld3(A.v, n.x), ld3(A.v, n.y), ld3(A.v, n.z), ld3(A.v, n.w)};
+        const M3<Real> fd = mul(mcols(vk[1] - vk[0], vk[2] - vk[0], vk[3] - vk[0]), dmi);
+        const M3<Real> G = linear ? fd : mul(transpose(R), fd);
+        const Real ltr = vol * lam * ((G.c[0].x + G.c[1].y) + G.c[2].z);
+        const Real vm = vol * mu;
+        M3<Real> P;
+        P.c[0] = v3<Real>(ltr + vm * (G.c[0].x + G.c[0].x), vm * (G.c[0].y + G.c[1].x), vm * (G.c[0].z + G.c[2].x));
+        P.c[1] = v3<Real>(vm * (G.c[1].x + G.c[0].y), ltr + vm * (G.c[1].y + G.c[1].y), vm * (G.c[1].z + G.c[2].y));
+        P.c[2] = v3<Real>(vm * (G.c[2].x + G.c[0].z), vm * (G.c[2].y + G.c[1].z), ltr + vm * (G.c[2].z + G.c[2].z));
+        const M3<Real> Q = linear ? P : mul(R, P);
+        const Real dt = A.dt, dt2 = dt * dt;
+        M3<Real> T;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) T.c[j] = -(S.c[j] * dt + Q.c[j] * dt2);
+        const Real damp = rec[30];
+        V3<Real> gr[4];
+        gr[1] = v3<Real>(dmi.c[0].x, dmi.c[1].x, dmi.c[2].x);
+        gr[2] = v3<Real>(dmi.c[0].y, dmi.c[1].y, dmi.c[2].y);
+        gr[3] = v3<Real>(dmi.c[0].z, dmi.c[1].z, dmi.c[2].z);
+        gr[0] = -((gr[1] + gr[2]) + gr[3]);
+        bool ok = finite9(T);
+        Real g2 = Real(0);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            ok = ok && finite3((-mul(S, gr[k])) + vk[k] * (-damp));
+            g2 = fmax(g2, dot(gr[k], gr[k]));
+        }
+        // |K_ab entries| <= V (|lambda| + 2 |mu|) |g_a| |g_b|
+        const Real bound = vol * (fabs(lam) + Real(2) * fabs(mu)) * g2;
+        ok = ok && bound < Real(sizeof(Real) == 4 ? 1.0e37 : 1.0e306);
+        if (ok) {
+            out = T;
+            form = Real(1);
+        }
+    }
     Real w[18];
     st9(w, 0, R);
-    st9(w + 9, 0, S);
+    st9(w + 9, 0, out);
     st_rec_rs(rec, w);
+    rec[31] = form;
 }
 
 // ------------------------------------------------------------------ sphere contacts
@@ -306,6 +354,39 @@ __global__ void embedded_vertex_kernel(const int* __restrict__ nodes, const floa
     }
 }
 
+// Per incidence of row r (tet t, corner a): the row slot of each of the tet's nodes --
+// the index of its column among the row's upper blocks, kSlotNone for a column below the
+// row or a node without a row, kSlotMissing when the pattern lacks the block.
+__global__ void inc_slot_kernel(int n, const int* __restrict__ row_start, const int* __restrict__ col,
+                                const int* __restrict__ inc_start, const int* __restrict__ inc_list,
+                                const int4* __restrict__ tet_nodes, const int* __restrict__ node_to_dyn,
+                                unsigned* __restrict__ out)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const int ks = __ldg(row_start + r), ke = __ldg(row_start + r + 1);
+    for (int i = __ldg(inc_start + r); i < __ldg(inc_start + r + 1); ++i) {
+        const int4 tn = __ldg(tet_nodes + (__ldg(inc_list + i) >> 2));
+        const int nb[4] = {tn.x, tn.y, tn.z, tn.w};
+        unsigned code = 0u;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int c = __ldg(node_to_dyn + nb[b]);
+            unsigned sl = kSlotNone;
+            if (c >= r) {
+                sl = kSlotMissing;
+                for (int k = ks; k < ke; ++k)
+                    if (__ldg(col + k) == c) {
+                        sl = (unsigned)(k - ks);
+                        break;
+                    }
+            }
+            code |= sl << (8 * b);
+        }
+        out[i] = code;
+    }
+}
+
 template <class Real>
 __global__ void tet_pack_kernel(const Real* __restrict__ dm_inv, const Real* __restrict__ params, Real* rec,
                                 int tet_count)
@@ -350,41 +431,30 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
     V3<Real> fsum{Real(0), Real(0), Real(0)};
     V3<Real> kv{Real(0), Real(0), Real(0)};
     bool bad = false;
+    // Right-hand-side terms of the tets in the folded form: sum of T g_a - dt c v_a.
+    V3<Real> bsum{Real(0), Real(0), Real(0)};
     const int i0 = __ldg(A.inc_start + r), i1 = __ldg(A.inc_start + r + 1);
-    // The next incidence's code, tet nodes and their rows are loaded while this one is
-    // processed (the chain code -> nodes -> rows would otherwise start each iteration).
+    // The next incidence's code and slots are loaded while this one is processed.
     int code_n = 0;
-    int4 tn_n = make_int4(0, 0, 0, 0), dyn_n = make_int4(-1, -1, -1, -1);
+    unsigned slot_n = 0u;
     auto fetch = [&](int i) {
         code_n = __ldg(A.inc_list + i);
-        tn_n = __ldg(A.tets.nodes + (code_n >> 2));
-        if (!A.explicit_mode)
-            dyn_n = make_int4(__ldg(A.node_to_dyn + tn_n.x), __ldg(A.node_to_dyn + tn_n.y),
-                              __ldg(A.node_to_dyn + tn_n.z), __ldg(A.node_to_dyn + tn_n.w));
+        if (A.inc_slot) slot_n = __ldg(A.inc_slot + i);
     };
     if (i0 < i1) fetch(i0);
     for (int i = i0; i < i1; ++i) {
         const int code = code_n;
+        const unsigned slots = slot_n;
         const int t = code >> 2, a = code & 3;
-        const int4 tn = tn_n;
-        const int nb[4] = {tn.x, tn.y, tn.z, tn.w};
-        const int dyn[4] = {dyn_n.x, dyn_n.y, dyn_n.z, dyn_n.w};
         if (i + 1 < i1) fetch(i + 1);
-        V3<Real> vb[4];
-        if (!A.explicit_mode) {
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                vb[b] = ld3(A.v, nb[b]);
-                bad |= !finite3(vb[b]);
-            }
-        }
         // The tet's record (the tet kernel's, an earlier launch); R is NaN-marked for a
         // skipped tet.
         Real w[kTetRec];
         ld_rec(A.tets.rec + kTetRec * (size_t)t, w);
         const M3<Real> R = rd9(w);
         if (isnan(R.c[0].x)) continue;  // skipped tet: no force, no stiffness
-        const M3<Real> S = rd9(w + 9);
+        const M3<Real> SM = rd9(w + 9);  // S, or T in the folded form
+        const bool folded = w[31] != Real(0);
         const M3<Real> dmi = rd9(w + 18);
         const Real vol = w[27], lam = w[28], mu = w[29], damp = w[30];
         // Shape gradients: g1..g3 are the rows of DmInv, g0 = -(g1+g2+g3).
@@ -397,16 +467,34 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
 #pragma unroll
         for (int k = 1; k < 4; ++k)
             if (a == k) ga = gr[k];
-        // Force on node a from this tet: elastic -S g_a plus damping -c v_a.
-        const V3<Real> fa = (-mul(S, ga)) + vr * (-damp);
-        if (finite3(fa)) fsum = fsum + fa;
-        if (A.explicit_mode) continue;
+        if (folded) {
+            // T g_a - dt c v_a; the upper blocks from the slot table.
+            bsum = bsum + mul(SM, ga) + vr * (-(A.dt * damp));
+        } else {
+            // Force on node a from this tet: elastic -S g_a plus damping -c v_a.
+            const V3<Real> fa = (-mul(SM, ga)) + vr * (-damp);
+            if (finite3(fa)) fsum = fsum + fa;
+            if (A.explicit_mode) continue;
+        }
+        const int4 tn = folded ? make_int4(0, 0, 0, 0) : __ldg(A.tets.nodes + t);
+        const int nb[4] = {tn.x, tn.y, tn.z, tn.w};
         // K_ab = R Ke_ab R^T with Ke_ab = V (lambda g_a g_b^T + mu g_b g_a^T + mu (g_a.g_b) I)
         //      = V (lambda P_a P_b^T + mu P_b P_a^T + mu (g_a.g_b) R R^T),  P = R g.
         const V3<Real> pa = mul(R, ga);
         const M3<Real> rrt = mul(R, transpose(R));
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
+            int slot = nu;
+            if (folded) {
+                // only the blocks this row stores
+                const unsigned sl = (slots >> (8 * b)) & 255u;
+                if (sl == kSlotNone) continue;
+                if (sl == kSlotMissing) {
+                    bad = true;  // pattern does not hold the block: host/device mismatch
+                    continue;
+                }
+                slot = (int)sl;
+            }
             const V3<Real> gb = gr[b];
             const V3<Real> pb = mul(R, gb);
             const Real l = vol * lam, m = vol * mu, md = vol * mu * dot(ga, gb);
@@ -415,10 +503,12 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
             K.c[1] = pa * (l * pb.y) + pb * (m * pa.y) + rrt.c[1] * md;
             K.c[2] = pa * (l * pb.z) + pb * (m * pa.z) + rrt.c[2] * md;
             bad |= !finite9(K);
-            kv = kv + mul(K, vb[b]);
-            const int c = dyn[b];
-            if (c >= r) {
-                int slot = nu;
+            if (!folded) {
+                const V3<Real> vb = ld3(A.v, nb[b]);
+                bad |= !finite3(vb);
+                kv = kv + mul(K, vb);
+                const int c = __ldg(A.node_to_dyn + nb[b]);
+                if (c < r) continue;
                 if (MAXU > 0) {
 #pragma unroll
                     for (int j = (MAXU > 0 ? MAXU : 1) - 1; j >= 0; --j)
@@ -427,14 +517,14 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
                     slot = 0;
                     while (slot < nu && __ldg(A.a.col + ks + slot) != c) ++slot;
                 }
-                if (slot < nu) {
-                    PK_ACC(slot, 0) += K.c[0].x; PK_ACC(slot, 1) += K.c[0].y; PK_ACC(slot, 2) += K.c[0].z;
-                    PK_ACC(slot, 3) += K.c[1].x; PK_ACC(slot, 4) += K.c[1].y; PK_ACC(slot, 5) += K.c[1].z;
-                    PK_ACC(slot, 6) += K.c[2].x; PK_ACC(slot, 7) += K.c[2].y; PK_ACC(slot, 8) += K.c[2].z;
-                } else {
+                if (slot >= nu) {
                     bad = true;  // pattern does not hold the block: host/device mismatch
+                    continue;
                 }
             }
+            PK_ACC(slot, 0) += K.c[0].x; PK_ACC(slot, 1) += K.c[0].y; PK_ACC(slot, 2) += K.c[0].z;
+            PK_ACC(slot, 3) += K.c[1].x; PK_ACC(slot, 4) += K.c[1].y; PK_ACC(slot, 5) += K.c[1].z;
+            PK_ACC(slot, 6) += K.c[2].x; PK_ACC(slot, 7) += K.c[2].y; PK_ACC(slot, 8) += K.c[2].z;
         }
     }
     // Transient point connections with a corner at this row (PointConnection::UpdateSystem,
@@ -569,7 +659,7 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
         st9(A.values, (size_t)(ks + j), blk);
     }
 #undef PK_ACC
-    const V3<Real> b = kv * (-dt2) + fsum * dt;
+    const V3<Real> b = bsum + (kv * (-dt2) + fsum * dt);
     bad |= !finite3(kv) || !finite3(b);
     st3(A.rhs, r, b);
     if (bad) atomicOr(A.flags, kFlagPrecomputeFailed);
@@ -681,6 +771,16 @@ cudaError_t launch_visual_kernel(int kind, const int* nodes, const float* weight
         surface_triangle_kernel<Real><<<(count + 127) / 128, 128, 0, stream>>>(nodes, count, x, verts, normals);
     else
         embedded_vertex_kernel<Real><<<(count + 127) / 128, 128, 0, stream>>>(nodes, weights, live, count, x, verts);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_inc_slot_kernel(int n, const int* row_start, const int* col, const int* inc_start,
+                                   const int* inc_list, const int4* tet_nodes, const int* node_to_dyn, unsigned* out,
+                                   cudaStream_t stream)
+{
+    if (n <= 0) return cudaSuccess;
+    inc_slot_kernel<<<(n + 127) / 128, 128, 0, stream>>>(n, row_start, col, inc_start, inc_list, tet_nodes,
+                                                          node_to_dyn, out);
     return cudaGetLastError();
 }
 

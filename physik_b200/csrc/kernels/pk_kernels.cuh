@@ -64,13 +64,18 @@ struct TetView {
     const unsigned char* enabled;    // bit 0: active, rest volume > 0, body simulated; bit 1: linear FEM
     const Real* dm_inv;              // 9 per tet, column-major
     const Real* params;              // 4 per tet: rest volume, lambda, mu, damping
-    // kTetRec per tet, read by the row kernel (one aligned record per tet): R (9) and
-    // S = R * V * sigma (9), written by the tet kernel each step (rec[kTetRec t] = NaN when
-    // the tet is skipped this step), then DmInv (9), rest volume, lambda, mu, damping and
-    // one unused value, written once when the tets are set (launch_tet_pack).
+    // kTetRec per tet, read by the row kernel (one aligned record per tet): R (9), a 3x3
+    // matrix M (9) and a form value (index 31), written by the tet kernel each step
+    // (rec[kTetRec t] = NaN when the tet is skipped this step); DmInv (9), rest volume,
+    // lambda, mu, damping (18..30), written once when the tets are set (launch_tet_pack).
+    // Form 0: M = S = R * V * sigma, node a's elastic force is -S g_a.  Form 1 (the
+    // implicit step with a slot table): M = T = -(dt S + dt^2 Q), where Q g_a is the tet's
+    // sum_b K_ab v_b, so the tet adds T g_a - dt c v_a to row a's right-hand side.
     Real* rec;
 };
 constexpr int kTetRec = 32;
+constexpr unsigned kSlotNone = 255u, kSlotMissing = 254u;
+constexpr int kSlotMaxRow = 16;  // the row kernel's register-slot paths (MAXU 8 and 16)
 
 template <class Real>
 struct AssemblyArgs {
@@ -85,6 +90,11 @@ struct AssemblyArgs {
     Real* x_out;                     // explicit mode position update target
     const int* inc_start;            // per dyn row
     const int* inc_list;             // t*4 + a
+    // Per incidence, the row slots of the tet's 4 nodes (8 bits each, node b in bits
+    // 8b..8b+7): the block's index in the row's upper blocks, kSlotNone when the column is
+    // not in the upper row (a lower or non-dynamic node), kSlotMissing when the pattern
+    // lacks it.  NULL: no table (rows longer than kSlotMaxRow, or not built).
+    const unsigned* inc_slot;
     Real* values;                    // out: A blocks
     Real* rhs;                       // out: b
     Real* minv;                      // out: block-Jacobi inverse
@@ -352,6 +362,11 @@ struct SlabPcgArgs {
     // Stream form (pk_slab_plan.h): 0 full symmetric rows, 1 the symmetric form (each
     // in-sub-part block once, transposed products through the groups' shared-memory rings).
     int sym;
+    // L2 residency of the matrix stream, in 1/1024: the first l2_keep/1024 of each part's
+    // tiles are loaded with an L2 evict-last hint, so that share of the stream (the same
+    // every iteration) tends to stay in L2 between iterations; the rest stream with
+    // evict-first.
+    int l2_keep;
 };
 
 // ------------------------------------------------------------------ FP64 refinement
@@ -429,6 +444,10 @@ template <class Real>
 cudaError_t launch_conn_kernel(const AssemblyArgs<Real>& args, cudaStream_t stream);
 template <class Real>
 cudaError_t launch_row_kernel(const AssemblyArgs<Real>& args, int max_row_blocks, cudaStream_t stream);
+// Builds AssemblyArgs::inc_slot for the pattern, the incidences and the tets' nodes.
+cudaError_t launch_inc_slot_kernel(int n, const int* row_start, const int* col, const int* inc_start,
+                                   const int* inc_list, const int4* tet_nodes, const int* node_to_dyn, unsigned* out,
+                                   cudaStream_t stream);
 template <class Real, class Acc>
 cudaError_t launch_pcg_kernel(const PcgArgs<Real, Acc>& args, int grid, int threads, cudaStream_t stream);
 // Largest cooperative grid (one wave) for the staged (args.ntiles > 0) or unstaged kernel.

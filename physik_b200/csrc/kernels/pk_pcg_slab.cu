@@ -55,6 +55,12 @@ __device__ __forceinline__ unsigned long long l2_evict_first_policy()
     asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
     return pol;
 }
+__device__ __forceinline__ unsigned long long l2_evict_last_policy()
+{
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
 // Bulk copy global -> shared with an L2 cache-policy hint (no multicast).
 __device__ __forceinline__ void bulk_g2s_hint(void* dst, const void* src, unsigned bytes, unsigned long long* bar,
                                               unsigned long long pol)
@@ -271,7 +277,9 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     const int krows = (m + kSlabRowThreads - 1) / kSlabRowThreads;
     const unsigned tmem_row0 =
         s_tmem + ((32u * (unsigned)(warp % 4)) << 16) + (unsigned)((warp / 4) * kSlabRowsPerThread * 16);
-    const unsigned long long pol = l2_evict_first_policy();
+    const unsigned long long pol = l2_evict_first_policy(), pol_keep = l2_evict_last_policy();
+    // tiles [0, keep_tiles) of the part are the L2-resident share of its stream
+    const int keep_tiles = (int)(((long long)min(max(P.l2_keep, 0), 1024) * ntiles) / 1024);
     unsigned ring = 0;    // ring positions consumed so far (ntiles per iteration)
     unsigned issued = 0;  // ring positions issued by the producer (producer lane 0 only)
     unsigned xgen = 0;
@@ -402,11 +410,12 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                         s_fail = 1;
                         break;
                     }
-                    const int4 d = table[p % (unsigned)ntiles];
+                    const int ti = (int)(p % (unsigned)ntiles);
+                    const int4 d = table[ti];
                     mbar_arrive_expect_tx(&full_bar[s], (unsigned)d.y);
                     if (d.y > 0)
                         bulk_g2s_hint(ring_base + (size_t)s * stage_bytes, P.stream + 16 * (size_t)d.x,
-                                      (unsigned)d.y, &full_bar[s], pol);
+                                      (unsigned)d.y, &full_bar[s], ti < keep_tiles ? pol_keep : pol);
                 }
             }
             __syncwarp();

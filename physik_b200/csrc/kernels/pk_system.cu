@@ -270,6 +270,8 @@ struct pk_system {
     DevBuf tet_nodes, tet_enabled, dm_inv, tet_params, tet_rec;
     // rows
     DevBuf dyn_to_node, row_start, col, lt_start, lt_row, lt_block, inc_start, inc_list, values, rhs, minv;
+    DevBuf inc_slot;        // per incidence: the row slots of the tet's nodes (built on first use)
+    bool slots_ok = false;  // inc_slot matches the pattern, incidences, tets and node rows
     // solver
     DevBuf px, pr, psd0, psd1, pq, part_a, part_b, part_bad, sync, stats;
     pk::DevStats* host_stats = nullptr;  // pinned
@@ -313,6 +315,7 @@ pk::AssemblyArgs<Real> assembly_args(pk_system* s, const pk_step_params& p)
     a.x_out = s->x.as<Real>();
     a.inc_start = s->inc_start.as<int>();
     a.inc_list = s->inc_list.as<int>();
+    a.inc_slot = s->slots_ok ? s->inc_slot.as<unsigned>() : nullptr;
     a.values = s->values.as<Real>();
     a.rhs = s->rhs.as<Real>();
     a.minv = s->minv.as<Real>();
@@ -524,12 +527,30 @@ int slab_fill(pk_system* s)
 
 // PK_SLAB_FORM=full / sym asks for one stream form of the part-resident kernel's layout;
 // by default the symmetric form where it applies, else the full rows.
+// The part-resident kernel's stream form: full symmetric rows unless PK_SLAB_FORM asks for
+// the symmetric form ("sym") or the symmetric form where it fits ("auto").  The full form
+// is the default: on block128 it streams 1.5x the bytes but runs faster, the symmetric
+// form's extra products, ring traffic and group barriers cost more than the bytes saved.
 int requested_slab_form()
 {
     const char* e = std::getenv("PK_SLAB_FORM");
-    if (e && std::strcmp(e, "full") == 0) return pk::kSlabFull;
     if (e && std::strcmp(e, "sym") == 0) return pk::kSlabSym;
-    return pk::kSlabAuto;
+    if (e && std::strcmp(e, "auto") == 0) return pk::kSlabAuto;
+    return pk::kSlabFull;
+}
+
+// The L2-resident share of the matrix stream (SlabPcgArgs::l2_keep, in 1/1024): by
+// default as much as fits in 64 MB of the 126 MB L2, leaving the rest to the CG vectors
+// and the streamed tiles; PK_SLAB_L2_KEEP=<fraction> overrides it.
+int slab_l2_keep(const pk_system* s)
+{
+    if (const char* e = std::getenv("PK_SLAB_L2_KEEP")) {
+        const double f = std::atof(e);
+        return static_cast<int>(std::min(1.0, std::max(0.0, f)) * 1024.0);
+    }
+    const double budget = 64.0 * 1024.0 * 1024.0;
+    if (s->slab_stream_bytes == 0) return 0;
+    return static_cast<int>(std::min(1.0, budget / static_cast<double>(s->slab_stream_bytes)) * 1024.0);
 }
 
 bool slab_allowed(const pk_system* s)
@@ -684,6 +705,7 @@ int run_pcg_slab(pk_system* s, const pk_step_params& p, int skip_on_flags)
         a.body_stats = bodies ? s->body_stats.as<pk::BatchBodyStats>() : nullptr;
         a.missing = &st->batch_missing;
         a.sym = s->slab_sym ? 1 : 0;
+        a.l2_keep = slab_l2_keep(s);
         // One launch per group of parts (the coupled solve: one launch of all parts).
         const int launches = static_cast<int>(s->slab_launch.size()) - 1;
         for (int l = 0; l < launches; ++l) {
@@ -993,9 +1015,34 @@ int run_pcg_refined(pk_system* s, const pk_step_params& p, int skip_on_flags)
     return PK_OK;
 }
 
+// PK_ASSEMBLY_FOLD=0 keeps every tet on the long assembly path (all 16 blocks per tet
+// and K v in the row kernel), for comparisons; the default folds K v into the tet kernel.
+bool assembly_fold_enabled()
+{
+    const char* e = std::getenv("PK_ASSEMBLY_FOLD");
+    return !(e && e[0] == '0');
+}
+
+// The slot table of the folded assembly (rows of at most kSlotMaxRow upper blocks), built
+// on the device after the pattern, the incidences, the tets or the node rows changed.
+int ensure_inc_slots(pk_system* s)
+{
+    if (s->slots_ok || s->dyn_count <= 0 || s->inc_count <= 0 || !s->have_tets || s->max_row > pk::kSlotMaxRow ||
+        !assembly_fold_enabled())
+        return PK_OK;
+    PK_CHECK(s->inc_slot.ensure(sizeof(unsigned) * static_cast<size_t>(s->inc_count)));
+    PK_CHECK(pk::launch_inc_slot_kernel(s->dyn_count, s->row_start.as<int>(), s->col.as<int>(),
+                                        s->inc_start.as<int>(), s->inc_list.as<int>(), s->tet_nodes.as<int4>(),
+                                        s->node_to_dyn.as<int>(), s->inc_slot.as<unsigned>(), s->stream));
+    s->launches += 1;
+    s->slots_ok = true;
+    return PK_OK;
+}
+
 template <class Real>
 int run_step(pk_system* s, const pk_step_params& p)
 {
+    if (const int rc = ensure_inc_slots(s)) return rc;
     PK_CHECK(cudaMemsetAsync(s->stats.p, 0, sizeof(pk::DevStats), s->stream));
     int evi[3] = {-1, -1, -1};
     if (s->timing) {
@@ -1086,6 +1133,7 @@ int run_step_graph(pk_system* s, const pk_step_params& p)
         // Everything built lazily (allocations, uploads) must exist before the capture.
         int prc = ensure_batch_parts_any(s);
         if (!prc) prc = ensure_slab_any(s);
+        if (!prc) prc = ensure_inc_slots(s);
         if (prc) return prc;
         const bool timing = s->timing;
         const long long launches = s->launches;
@@ -1238,6 +1286,7 @@ PKCUDA_API int pk_system_set_nodes(pk_system* s, int node_count, const int* node
     s->node_count = node_count;
     s->have_snapshot = false;
     s->h_node_to_dyn.assign(node_to_dyn, node_to_dyn + node_count);
+    s->slots_ok = false;
     s->h_mass.assign(mass, mass + node_count);
     int rc = upload_raw<int>(s->node_to_dyn, node_to_dyn, node_count, s->stream);
     if (!rc) rc = upload_real_any(s, s->mass, mass, node_count);
@@ -1514,6 +1563,7 @@ PKCUDA_API int pk_system_set_tets(pk_system* s, int tet_count, const int* tet_no
     for (long long i = 0; i < 4ll * tet_count; ++i)
         if (tet_nodes[i] < 0 || tet_nodes[i] >= s->node_count) return fail(PK_ERR_ARG, "tet node out of range");
     s->tet_count = tet_count;
+    s->slots_ok = false;
     s->h_tet_nodes.assign(tet_nodes, tet_nodes + 4 * static_cast<size_t>(tet_count));
     s->h_enabled.assign(enabled, enabled + tet_count);
     s->h_damping.assign(damping, damping + tet_count);
@@ -1670,6 +1720,7 @@ PKCUDA_API int pk_system_set_pattern(pk_system* s, int dyn_count, const int* dyn
     s->nnz = nnz;
     s->lt_count = static_cast<int>(ltr.size());
     s->inc_count = inc;
+    s->slots_ok = false;
     s->max_row = max_row;
     s->diag_first = diag_first;
     int rc = upload_raw<int>(s->dyn_to_node, dyn_to_node, dyn_count, s->stream);

@@ -56,9 +56,14 @@ def test_settings_defaults_and_handles():
 
 
 def pressed_box():
-    """A 4x3x3 box (x=0 pinned) whose free end sits inside a sphere."""
-    s = meshes.small_box(4, 3, 3, young=2e4, seed=4)
-    return s, (1.0, 0.4, 0.75), 0.35
+    """A 4x3x3 box over 0.4 x 0.3 x 0.3 (x=0 pinned) whose free end sits inside a sphere
+    (14 tet centroids inside at rest).  Every input is exact in float (dt 1/64, gravity
+    -9.8125, Poisson 0.3125, the sphere's centre and radius), so the FP64 run and the
+    reference compiled in double see the same numbers."""
+    s = meshes.small_box(4, 3, 3, young=2e4, poisson=0.3125, seed=4)
+    s.dt = 1.0 / 64.0
+    s.gravity = (0.0, 0.0, -9.8125)
+    return s, (0.4375, 0.15625, 0.15625), 0.125
 
 
 def reference_contacts(x, tets, center, radius):
@@ -104,8 +109,7 @@ def test_pressed_box_with_moving_sphere_follows_reference(precision):
     s = ref.add_sphere(center, radius, 300.0, 1.0)
     tx, tv = (1e-6, 1e-4) if precision == "fp32" else (1e-9, 1e-7)
     for frame in range(3):
-        c = (center[0] - 0.02 * frame, center[1], center[2])
-        c = tuple(float(np.float32(v)) for v in c)
+        c = (center[0] - 0.015625 * frame, center[1], center[2])
         L.PX.PHYSIK_SetCollisionComponentKinematicTarget(gpu.h, h, *c)
         ref.set_sphere_target(s, c)
         gpu.step()

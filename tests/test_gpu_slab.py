@@ -129,11 +129,11 @@ def test_slab_is_deterministic_and_graph_replay_is_bit_identical():
 
 
 # ---------------------------------------------------------------- stream forms
-# The part-resident kernel streams either full symmetric rows or, where the layout fits,
-# the symmetric form (each block inside a sub-part streamed once, its transposed product
-# sent through the consumer group's ring of slots in shared memory).  PK_SLAB_FORM forces
-# one; both must follow the FP64 oracle, agree with each other to summation order, and
-# repeat bit for bit (also under CUDA-graph replay).
+# The part-resident kernel streams full symmetric rows (the default) or, where the layout
+# fits and PK_SLAB_FORM asks for it, the symmetric form (each block inside a sub-part
+# streamed once, its transposed product sent through the consumer group's ring of slots in
+# shared memory).  Both must follow the FP64 oracle, agree with each other to summation
+# order, and repeat bit for bit (also under CUDA-graph replay).
 
 
 def _world(scene, form, monkeypatch, precision="mixed", graph=False):
@@ -163,14 +163,18 @@ def test_stream_forms_follow_fp64_oracle(make, form, monkeypatch):
         assert abs(st["iterations"] - ora.last_stats()["iterations"]) <= 1
 
 
-def test_stream_forms_agree_and_sym_is_the_default(monkeypatch):
+def test_stream_forms_agree_and_full_is_the_default(monkeypatch):
     scene = meshes.config2()
     monkeypatch.delenv("PK_SLAB_FORM", raising=False)
-    auto = SimWorld(scene, precision="mixed")
+    default = SimWorld(scene, precision="mixed")
+    default.step()
+    assert default.pcg_stream_form() == "full"
+    auto = _world(scene, "auto", monkeypatch)  # the symmetric form where it fits
     auto.step()
     assert auto.pcg_stream_form() == "sym"
     full = _world(scene, "full", monkeypatch)
     full.step()
+    np.testing.assert_array_equal(default.state(f64=True)[0], full.state(f64=True)[0])
     xa, va = auto.state(f64=True)
     xf, vf = full.state(f64=True)
     assert rel(xa, xf) <= 3e-7
@@ -207,3 +211,23 @@ def test_sym_form_fp32_follows_fp32_reference(monkeypatch):
         assert gpu.pcg_stream_form() == "sym"
         assert rel(x, ora.x) <= 3e-7
         assert rel(v, ora.v) <= 2.5e-5
+
+
+def test_l2_resident_share_changes_no_bit(monkeypatch):
+    """The L2 hint on part of the matrix stream (PK_SLAB_L2_KEEP) only changes where the
+    tiles come from: results are bit-identical with none, the default and all of it."""
+    scene = meshes.config2()
+    states = []
+    for keep in ("0", None, "1"):
+        if keep is None:
+            monkeypatch.delenv("PK_SLAB_L2_KEEP", raising=False)
+        else:
+            monkeypatch.setenv("PK_SLAB_L2_KEEP", keep)
+        w = SimWorld(scene, precision="mixed")
+        for _ in range(2):
+            w.step()
+        assert w.pcg_kernel()[0] == "slab"
+        states.append(w.state(f64=True))
+    for x, v in states[1:]:
+        np.testing.assert_array_equal(x, states[0][0])
+        np.testing.assert_array_equal(v, states[0][1])
