@@ -792,6 +792,7 @@ private:
     void CollectContributions(float dt);
     void EnsureScene(bool upload);
     void FlushLocalPositionSnapshots();  // host copies of every stale component snapshot
+    void ReleaseDeviceScene();           // state, local copies and visuals to the host, then drop the system
     void AddSphereContacts();            // the requested spheres' contacts as point connections
     void SnapshotPositions();            // the frame's end positions for the components' copies
     bool SyncConnections();

@@ -701,12 +701,23 @@ void World::SetConjugateGradientMaxIterations(int maxIterations)
         std::clamp(maxIterations, kMinConjugateGradientMaxIterations, kMaxConjugateGradientMaxIterations);
 }
 
+// Everything that lives on the device system is brought to the host before the system
+// goes: the node state, the components' local position copies, pending visual results.
+void World::ReleaseDeviceScene()
+{
+    EnsureHostState();
+    FlushLocalPositionSnapshots();
+    for (auto& c : components)
+        if (c) c->ReleaseDeviceResources();
+    snapshotOnDevice = false;
+    scene.reset();
+}
+
 void World::SetPrecision(Precision p)
 {
     if (p == precision) return;
-    EnsureHostState();
+    ReleaseDeviceScene();
     precision = p;
-    scene.reset();
     deviceStale = true;
     ++topologyVersion;
 }
@@ -714,9 +725,8 @@ void World::SetPrecision(Precision p)
 void World::SetDevice(int dev)
 {
     if (dev == device) return;
-    EnsureHostState();
+    ReleaseDeviceScene();
     device = dev;
-    scene.reset();
     deviceStale = true;
     ++topologyVersion;
 }
@@ -1127,10 +1137,7 @@ void World::EnsureScene(bool upload)
 {
     const std::vector<const TetMeshPhysicsComponent*>& fem = solverData.GetFemBodies();
     if (!scene || scene->precision != precision || scene->device != device) {
-        FlushLocalPositionSnapshots();
-        snapshotOnDevice = false;
-        for (auto& c : components)
-            if (c) c->ReleaseDeviceResources();
+        if (scene) ReleaseDeviceScene();
         EnsureHostState();
         scene = std::make_unique<DeviceScene>();
         scene->precision = precision;

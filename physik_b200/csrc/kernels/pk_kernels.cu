@@ -128,6 +128,70 @@ __device__ __forceinline__ M3<Real> rd9(const Real* q)
     return m;
 }
 
+// ------------------------------------------------------------------ element stiffness block
+// K_ab = V (lambda P_a P_b^T + mu P_b P_a^T + mu (g_a.g_b) R R^T), P = R g, written with
+// explicit roundings (products and fused multiply-adds in one fixed order) so that every
+// kernel that builds a block produces the same bits, whatever the compiler contracts.
+__device__ __forceinline__ float kfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double kfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float kmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double kmul(double a, double b) { return __dmul_rn(a, b); }
+
+__device__ __forceinline__ float kadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double kadd(double a, double b) { return __dadd_rn(a, b); }
+template <class Real>
+__device__ __forceinline__ V3<Real> kadd3(const V3<Real>& a, const V3<Real>& b)
+{
+    return V3<Real>{kadd(a.x, b.x), kadd(a.y, b.y), kadd(a.z, b.z)};
+}
+template <class Real>
+__device__ __forceinline__ V3<Real> kscale3(const V3<Real>& a, Real s)
+{
+    return V3<Real>{kmul(a.x, s), kmul(a.y, s), kmul(a.z, s)};
+}
+template <class Real>
+__device__ __forceinline__ Real kdot(const V3<Real>& a, const V3<Real>& b)
+{
+    return kfma(a.z, b.z, kfma(a.y, b.y, kmul(a.x, b.x)));
+}
+// R g for column-major R (R.c[j] is column j).
+template <class Real>
+__device__ __forceinline__ V3<Real> krot(const M3<Real>& R, const V3<Real>& g)
+{
+    return V3<Real>{kfma(R.c[2].x, g.z, kfma(R.c[1].x, g.y, kmul(R.c[0].x, g.x))),
+                    kfma(R.c[2].y, g.z, kfma(R.c[1].y, g.y, kmul(R.c[0].y, g.x))),
+                    kfma(R.c[2].z, g.z, kfma(R.c[1].z, g.y, kmul(R.c[0].z, g.x)))};
+}
+// R R^T: column j holds the rows' dot products with row j.
+template <class Real>
+__device__ __forceinline__ M3<Real> krrt(const M3<Real>& R)
+{
+    const V3<Real> r0{R.c[0].x, R.c[1].x, R.c[2].x}, r1{R.c[0].y, R.c[1].y, R.c[2].y},
+        r2{R.c[0].z, R.c[1].z, R.c[2].z};
+    M3<Real> m;
+    m.c[0] = V3<Real>{kdot(r0, r0), kdot(r1, r0), kdot(r2, r0)};
+    m.c[1] = V3<Real>{kdot(r0, r1), kdot(r1, r1), kdot(r2, r1)};
+    m.c[2] = V3<Real>{kdot(r0, r2), kdot(r1, r2), kdot(r2, r2)};
+    return m;
+}
+template <class Real>
+__device__ __forceinline__ M3<Real> kblock(const V3<Real>& pa, const V3<Real>& pb, const V3<Real>& ga,
+                                           const V3<Real>& gb, const M3<Real>& rrt, Real vol, Real lam, Real mu)
+{
+    const Real l = kmul(vol, lam), m = kmul(vol, mu), md = kmul(m, kdot(ga, gb));
+    const Real lp[3] = {kmul(l, pb.x), kmul(l, pb.y), kmul(l, pb.z)};
+    const Real mp[3] = {kmul(m, pa.x), kmul(m, pa.y), kmul(m, pa.z)};
+    M3<Real> K;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const V3<Real>& rc = rrt.c[j];
+        K.c[j] = V3<Real>{kfma(rc.x, md, kfma(pb.x, mp[j], kmul(pa.x, lp[j]))),
+                          kfma(rc.y, md, kfma(pb.y, mp[j], kmul(pa.y, lp[j]))),
+                          kfma(rc.z, md, kfma(pb.z, mp[j], kmul(pa.z, lp[j])))};
+    }
+    return K;
+}
+
 // ------------------------------------------------------------------ tet kernel
 template <class Real, bool kFp64Polar>
 __global__ void __launch_bounds__(256) tet_kernel(AssemblyArgs<Real> A)
@@ -240,6 +304,274 @@ __global__ void __launch_bounds__(256) tet_kernel(AssemblyArgs<Real> A)
     st9(w + 9, 0, out);
     st_rec_rs(rec, w);
     rec[31] = form;
+}
+
+// ------------------------------------------------------------------ row kernel, four lanes per row
+// The implicit step with a slot table: four lanes share a row.  Per incidence (tet order)
+// each lane loads two of the tet record's eight 16-byte chunks and the lanes exchange
+// what they need with shuffles (one 128-byte line per row per incidence, instead of each
+// lane reading the whole record); lane b then builds K_ab for the tet's corner b and adds
+// it to that column's slot when the row stores it.  The four corners of one tet are four
+// different columns, so every slot still receives its terms in tet order and the blocks
+// equal the one-thread-per-row kernel's bit for bit.  Lane 0 adds the tet's right-hand-
+// side term (T g_a - dt c v_a for a folded tet; for one the tet kernel left unfolded, the
+// force -S g_a - c v_a, and the four lanes' K_ab v_b summed in lane order), the point
+// connections, the host-emitted blocks and the diagonal's inverse.
+template <class Real>
+__device__ __forceinline__ Real shfl_row(Real v, int src)
+{
+    return __shfl_sync(0xffffffffu, v, src);
+}
+
+template <class Real, int MAXU>
+__global__ void __launch_bounds__(128) row_lanes_kernel(AssemblyArgs<Real> A)
+{
+    constexpr int LPR = 4, RPB = 128 / LPR, RS = RPB + 1;  // lanes per row, rows per block, slot stride
+    __shared__ Real acc[MAXU * 9 * RS];
+    const int tid = threadIdx.x, lane = tid & 31, lb = tid % LPR, rb = tid / LPR;
+    const int base = lane - lb;  // lane 0 of this row within the warp
+    const int r = blockIdx.x * RPB + rb;
+    const bool valid = r < A.a.n;
+#define PK_LACC(slot, e) acc[((slot) * 9 + (e)) * RS + rb]
+    int node = 0, ks = 0, nu = 0, i0 = 0, i1 = 0;
+    if (valid) {
+        node = __ldg(A.dyn_to_node + r);
+        ks = __ldg(A.a.row_start + r);
+        nu = __ldg(A.a.row_start + r + 1) - ks;
+        i0 = __ldg(A.inc_start + r);
+        i1 = __ldg(A.inc_start + r + 1);
+    }
+    bool bad = false;
+    if (valid && nu > MAXU) {
+        if (lb == 0) atomicOr(A.flags, kFlagRowTooLong | kFlagPrecomputeFailed);
+        nu = 0;
+        i1 = i0;
+    }
+    for (int j = lb; j < nu; j += LPR)
+        for (int e = 0; e < 9; ++e) PK_LACC(j, e) = Real(0);
+    const V3<Real> vr = valid ? ld3(A.v, node) : V3<Real>{Real(0), Real(0), Real(0)};
+    V3<Real> fsum{Real(0), Real(0), Real(0)}, kv{Real(0), Real(0), Real(0)}, bsum{Real(0), Real(0), Real(0)};
+    // every lane of the warp takes part in every step (shuffles, warp barriers)
+    int steps = i1 - i0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) steps = max(steps, __shfl_xor_sync(0xffffffffu, steps, off));
+    __syncwarp();
+    constexpr int kPer = kTetRec / LPR;  // record values each lane loads (two or four 16-byte chunks)
+    for (int k = 0; k < steps; ++k) {
+        // Every lane runs every step's shuffles and its warp barrier; the work is guarded.
+        const bool live = i0 + k < i1;
+        int code = 0;
+        unsigned slots = 0xffffffffu;
+        Real mine[kPer];
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) mine[q] = Real(0);
+        if (live) {
+            code = __ldg(A.inc_list + i0 + k);
+            slots = __ldg(A.inc_slot + i0 + k);
+            const Real* rec = A.tets.rec + kTetRec * (size_t)(code >> 2) + (size_t)lb * kPer;
+            if constexpr (sizeof(Real) == 4) {
+                const float4 c0 = __ldg(reinterpret_cast<const float4*>(rec));
+                const float4 c1 = __ldg(reinterpret_cast<const float4*>(rec) + 1);
+                mine[0] = c0.x; mine[1] = c0.y; mine[2] = c0.z; mine[3] = c0.w;
+                mine[4] = c1.x; mine[5] = c1.y; mine[6] = c1.z; mine[7] = c1.w;
+            } else {
+#pragma unroll
+                for (int q = 0; q < kPer / 2; ++q) {
+                    const double2 c = __ldg(reinterpret_cast<const double2*>(rec) + q);
+                    mine[2 * q] = c.x;
+                    mine[2 * q + 1] = c.y;
+                }
+            }
+        }
+        // record value v: element v % kPer of the row's lane v / kPer
+        Real w[kTetRec];
+#pragma unroll
+        for (int v = 0; v < kTetRec; ++v) w[v] = shfl_row(mine[v % kPer], base + v / kPer);
+        const M3<Real> R = rd9(w);
+        const bool work = live && !isnan(R.c[0].x);  // a skipped tet: no force, no stiffness
+        if (work) {
+            const bool folded = w[31] != Real(0);
+            const M3<Real> SM = rd9(w + 9);  // S, or T in the folded form
+            const M3<Real> dmi = rd9(w + 18);
+            const Real vol = w[27], lam = w[28], mu = w[29], damp = w[30];
+            const int a = code & 3;
+            V3<Real> gr[4];
+            gr[1] = v3<Real>(dmi.c[0].x, dmi.c[1].x, dmi.c[2].x);
+            gr[2] = v3<Real>(dmi.c[0].y, dmi.c[1].y, dmi.c[2].y);
+            gr[3] = v3<Real>(dmi.c[0].z, dmi.c[1].z, dmi.c[2].z);
+            gr[0] = -((gr[1] + gr[2]) + gr[3]);
+            V3<Real> ga = gr[0], gb = gr[0];  // selects: a dynamic index would put gr in local memory
+#pragma unroll
+            for (int q = 1; q < 4; ++q) {
+                if (a == q) ga = gr[q];
+                if (lb == q) gb = gr[q];
+            }
+            if (lb == 0) {
+                if (folded) {
+                    bsum = kadd3(bsum, kadd3(krot(SM, ga), kscale3(vr, -kmul(A.dt, damp))));
+                } else {
+                    const V3<Real> fa = kadd3(-krot(SM, ga), kscale3(vr, -damp));
+                    if (finite3(fa)) fsum = kadd3(fsum, fa);
+                }
+            }
+            const unsigned sl = (slots >> (8 * lb)) & 255u;
+            if (sl == kSlotMissing) bad = true;  // pattern does not hold the block: host/device mismatch
+            if (!folded || (int)sl < nu) {
+                const M3<Real> K = kblock(krot(R, ga), krot(R, gb), ga, gb, krrt(R), vol, lam, mu);
+                bad |= !finite9(K);
+                if (!folded) {
+                    const int4 tn = __ldg(A.tets.nodes + (code >> 2));
+                    int nb = tn.x;
+                    if (lb == 1) nb = tn.y;
+                    if (lb == 2) nb = tn.z;
+                    if (lb == 3) nb = tn.w;
+                    const V3<Real> vb = ld3(A.v, nb);
+                    bad |= !finite3(vb);
+                    kv = kv + mul(K, vb);
+                }
+                if ((int)sl < nu) {
+                    PK_LACC(sl, 0) += K.c[0].x; PK_LACC(sl, 1) += K.c[0].y; PK_LACC(sl, 2) += K.c[0].z;
+                    PK_LACC(sl, 3) += K.c[1].x; PK_LACC(sl, 4) += K.c[1].y; PK_LACC(sl, 5) += K.c[1].z;
+                    PK_LACC(sl, 6) += K.c[2].x; PK_LACC(sl, 7) += K.c[2].y; PK_LACC(sl, 8) += K.c[2].z;
+                } else if (sl != kSlotNone && sl != kSlotMissing) {
+                    bad = true;  // a slot beyond the row
+                }
+            }
+        }
+        __syncwarp();  // this tet's four blocks land before the next tet's (per-slot tet order)
+    }
+    __syncwarp();
+    // the unfolded tets' K v: lane sums in lane order
+    {
+        V3<Real> k1{shfl_row(kv.x, base + 1), shfl_row(kv.y, base + 1), shfl_row(kv.z, base + 1)};
+        V3<Real> k2{shfl_row(kv.x, base + 2), shfl_row(kv.y, base + 2), shfl_row(kv.z, base + 2)};
+        V3<Real> k3{shfl_row(kv.x, base + 3), shfl_row(kv.y, base + 3), shfl_row(kv.z, base + 3)};
+        kv = ((kv + k1) + k2) + k3;
+    }
+    if (valid && lb == 0) {
+        // Transient point connections and host-emitted contributions, as the one-thread
+        // kernel (slot found by search).
+        auto find_slot = [&](int c) {
+            int slot = 0;
+            while (slot < nu && __ldg(A.a.col + ks + slot) != c) ++slot;
+            return slot;
+        };
+        if (A.conn_inc_start) {
+            const int j0 = __ldg(A.conn_inc_start + r), j1 = __ldg(A.conn_inc_start + r + 1);
+            for (int i = j0; i < j1; ++i) {
+                const int cc = __ldg(A.conn_inc_list + i);
+                const int ci = cc >> 2, ca = cc & 3;
+                if ((unsigned)ci >= (unsigned)A.conn_count) {
+                    bad = true;
+                    continue;
+                }
+                const Real* ev = A.conn_eval + 4 * (size_t)ci;
+                if (!(ev[3] != Real(0))) continue;
+                const int4 cn = __ldg(A.conn_nodes + ci);
+                const int nb[4] = {cn.x, cn.y, cn.z, cn.w};
+                const Real* q = A.conn_params + kConnParams * (size_t)ci;
+                const Real wq[4] = {__ldg(q), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3)};
+                Real wa = wq[0];
+#pragma unroll
+                for (int b = 1; b < 4; ++b)
+                    if (ca == b) wa = wq[b];
+                fsum = fsum + V3<Real>{ev[0], ev[1], ev[2]} * wa;
+                const Real kk = __ldg(q + 7);
+                if (!(kk > Real(0))) continue;
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    if (wq[b] == Real(0)) continue;
+                    const Real kab = kk * wa * wq[b];
+                    bad |= !isfinite(kab);
+                    kv = kv + ld3(A.v, nb[b]) * kab;
+                    const int c = __ldg(A.node_to_dyn + nb[b]);
+                    if (c >= r) {
+                        const int slot = find_slot(c);
+                        if (slot < nu) {
+                            PK_LACC(slot, 0) += kab;
+                            PK_LACC(slot, 4) += kab;
+                            PK_LACC(slot, 8) += kab;
+                        } else {
+                            bad = true;
+                        }
+                    }
+                }
+            }
+        }
+        if (A.ext_rhs_start) {
+            const int b0 = __ldg(A.ext_rhs_start + r), b1 = __ldg(A.ext_rhs_start + r + 1);
+            for (int i = b0; i < b1; ++i) {
+                const int kq = __ldg(A.ext_rhs_list + i);
+                const M3<Real> B = ld9(A.ext_blocks, (size_t)kq);
+                const int2 nd = __ldg(A.ext_nodes + kq);
+                const V3<Real> vb = ld3(A.v, nd.y);
+                bad |= !finite3(vb) || !finite9(B);
+                kv = kv + mul(B, vb);
+            }
+            const int m0 = __ldg(A.ext_mat_start + r), m1 = __ldg(A.ext_mat_start + r + 1);
+            for (int i = m0; i < m1; ++i) {
+                const unsigned cq = (unsigned)__ldg(A.ext_mat_list + i);
+                const int kq = (int)(cq & 0x7fffffffu);
+                const bool tr = (cq & 0x80000000u) != 0;
+                M3<Real> B = ld9(A.ext_blocks, (size_t)kq);
+                if (tr) B = transpose(B);
+                const int2 nd = __ldg(A.ext_nodes + kq);
+                const int c = __ldg(A.node_to_dyn + (tr ? nd.x : nd.y));
+                const int slot = find_slot(c);
+                if (c < r || slot >= nu) {
+                    bad = true;
+                    continue;
+                }
+                PK_LACC(slot, 0) += B.c[0].x; PK_LACC(slot, 1) += B.c[0].y; PK_LACC(slot, 2) += B.c[0].z;
+                PK_LACC(slot, 3) += B.c[1].x; PK_LACC(slot, 4) += B.c[1].y; PK_LACC(slot, 5) += B.c[1].z;
+                PK_LACC(slot, 6) += B.c[2].x; PK_LACC(slot, 7) += B.c[2].y; PK_LACC(slot, 8) += B.c[2].z;
+            }
+        }
+        if (A.ext_force) fsum = kadd3(fsum, ld3(A.ext_force, r));
+    }
+    __syncwarp();
+    const Real m = valid ? __ldg(A.mass + node) : Real(0);
+    const Real dt = A.dt, dt2 = kmul(dt, dt);
+    // the row's blocks: lane j writes slots j, j + 4, ...; the diagonal (slot 0) is lane 0's
+    M3<Real> diag = mident<Real>();
+    for (int j = lb; j < nu; j += LPR) {
+        M3<Real> blk;
+        blk.c[0] = v3<Real>(PK_LACC(j, 0), PK_LACC(j, 1), PK_LACC(j, 2));
+        blk.c[1] = v3<Real>(PK_LACC(j, 3), PK_LACC(j, 4), PK_LACC(j, 5));
+        blk.c[2] = v3<Real>(PK_LACC(j, 6), PK_LACC(j, 7), PK_LACC(j, 8));
+        bad |= !finite9(blk);
+        blk.c[0] = kscale3(blk.c[0], dt2);
+        blk.c[1] = kscale3(blk.c[1], dt2);
+        blk.c[2] = kscale3(blk.c[2], dt2);
+        if (j == 0) {
+            blk.c[0].x = kadd(m, blk.c[0].x);
+            blk.c[1].y = kadd(m, blk.c[1].y);
+            blk.c[2].z = kadd(m, blk.c[2].z);
+            diag = blk;
+        }
+        st9(A.values, (size_t)(ks + j), blk);
+    }
+#undef PK_LACC
+    // the row's four lanes' findings, for lane 0 (the step's flag is global)
+    bad = ((__ballot_sync(0xffffffffu, bad) >> base) & 0xFu) != 0u;
+    if (!valid || lb != 0) return;
+    const V3<Real> grav{A.gravity[0], A.gravity[1], A.gravity[2]};
+    fsum = kadd3(fsum, kscale3(grav, m));
+    const V3<Real> b = kadd3(bsum, kadd3(kscale3(kv, -dt2), kscale3(fsum, dt)));
+    bad |= !finite3(kv) || !finite3(b);
+    st3(A.rhs, r, b);
+    if (bad) atomicOr(A.flags, kFlagPrecomputeFailed);
+    M3<Real> mi = mident<Real>();
+    if (A.use_jacobi) {
+        const Real d = det(diag);
+        if (!finite9(diag) || !isfinite(d) || fabs(d) <= Real(1.0e-8)) {
+            atomicOr(A.flags, kFlagSingularDiag);
+        } else {
+            mi = inverse(diag);
+            if (!finite9(mi)) atomicOr(A.flags, kFlagSingularDiag);
+        }
+    }
+    st9(A.minv, (size_t)r, mi);
 }
 
 // ------------------------------------------------------------------ sphere contacts
@@ -469,19 +801,19 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
             if (a == k) ga = gr[k];
         if (folded) {
             // T g_a - dt c v_a; the upper blocks from the slot table.
-            bsum = bsum + mul(SM, ga) + vr * (-(A.dt * damp));
+            bsum = kadd3(bsum, kadd3(krot(SM, ga), kscale3(vr, -kmul(A.dt, damp))));
         } else {
             // Force on node a from this tet: elastic -S g_a plus damping -c v_a.
-            const V3<Real> fa = (-mul(SM, ga)) + vr * (-damp);
-            if (finite3(fa)) fsum = fsum + fa;
+            const V3<Real> fa = kadd3(-krot(SM, ga), kscale3(vr, -damp));
+            if (finite3(fa)) fsum = kadd3(fsum, fa);
             if (A.explicit_mode) continue;
         }
         const int4 tn = folded ? make_int4(0, 0, 0, 0) : __ldg(A.tets.nodes + t);
         const int nb[4] = {tn.x, tn.y, tn.z, tn.w};
         // K_ab = R Ke_ab R^T with Ke_ab = V (lambda g_a g_b^T + mu g_b g_a^T + mu (g_a.g_b) I)
-        //      = V (lambda P_a P_b^T + mu P_b P_a^T + mu (g_a.g_b) R R^T),  P = R g.
-        const V3<Real> pa = mul(R, ga);
-        const M3<Real> rrt = mul(R, transpose(R));
+        //      = V (lambda P_a P_b^T + mu P_b P_a^T + mu (g_a.g_b) R R^T),  P = R g (kblock).
+        const V3<Real> pa = krot(R, ga);
+        const M3<Real> rrt = krrt(R);
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             int slot = nu;
@@ -496,12 +828,7 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
                 slot = (int)sl;
             }
             const V3<Real> gb = gr[b];
-            const V3<Real> pb = mul(R, gb);
-            const Real l = vol * lam, m = vol * mu, md = vol * mu * dot(ga, gb);
-            M3<Real> K;
-            K.c[0] = pa * (l * pb.x) + pb * (m * pa.x) + rrt.c[0] * md;
-            K.c[1] = pa * (l * pb.y) + pb * (m * pa.y) + rrt.c[1] * md;
-            K.c[2] = pa * (l * pb.z) + pb * (m * pa.z) + rrt.c[2] * md;
+            const M3<Real> K = kblock(pa, krot(R, gb), ga, gb, rrt, vol, lam, mu);
             bad |= !finite9(K);
             if (!folded) {
                 const V3<Real> vb = ld3(A.v, nb[b]);
@@ -625,10 +952,10 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
             PK_ACC(slot, 6) += B.c[2].x; PK_ACC(slot, 7) += B.c[2].y; PK_ACC(slot, 8) += B.c[2].z;
         }
     }
-    if (A.ext_force) fsum = fsum + ld3(A.ext_force, r);
+    if (A.ext_force) fsum = kadd3(fsum, ld3(A.ext_force, r));
     const Real m = __ldg(A.mass + node);
     const V3<Real> grav{A.gravity[0], A.gravity[1], A.gravity[2]};
-    fsum = fsum + grav * m;
+    fsum = kadd3(fsum, kscale3(grav, m));
     const Real dt = A.dt;
 
     if (A.explicit_mode) {
@@ -641,7 +968,7 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
         return;
     }
 
-    const Real dt2 = dt * dt;
+    const Real dt2 = kmul(dt, dt);
     M3<Real> diag;
     for (int j = 0; j < nu; ++j) {
         M3<Real> blk;
@@ -649,17 +976,19 @@ __global__ void __launch_bounds__(128) row_kernel(AssemblyArgs<Real> A)
         blk.c[1] = v3<Real>(PK_ACC(j, 3), PK_ACC(j, 4), PK_ACC(j, 5));
         blk.c[2] = v3<Real>(PK_ACC(j, 6), PK_ACC(j, 7), PK_ACC(j, 8));
         bad |= !finite9(blk);
-        blk = scale(blk, dt2);
+        blk.c[0] = kscale3(blk.c[0], dt2);
+        blk.c[1] = kscale3(blk.c[1], dt2);
+        blk.c[2] = kscale3(blk.c[2], dt2);
         if (j == 0) {
-            blk.c[0].x = m + blk.c[0].x;
-            blk.c[1].y = m + blk.c[1].y;
-            blk.c[2].z = m + blk.c[2].z;
+            blk.c[0].x = kadd(m, blk.c[0].x);
+            blk.c[1].y = kadd(m, blk.c[1].y);
+            blk.c[2].z = kadd(m, blk.c[2].z);
             diag = blk;
         }
         st9(A.values, (size_t)(ks + j), blk);
     }
 #undef PK_ACC
-    const V3<Real> b = bsum + (kv * (-dt2) + fsum * dt);
+    const V3<Real> b = kadd3(bsum, kadd3(kscale3(kv, -dt2), kscale3(fsum, dt)));
     bad |= !finite3(kv) || !finite3(b);
     st3(A.rhs, r, b);
     if (bad) atomicOr(A.flags, kFlagPrecomputeFailed);
@@ -811,6 +1140,14 @@ template <class Real>
 cudaError_t launch_row_kernel(const AssemblyArgs<Real>& args, int max_row_blocks, cudaStream_t stream)
 {
     if (args.a.n <= 0) return cudaSuccess;
+    if (args.inc_slot && args.row_lanes && !args.explicit_mode && max_row_blocks <= kSlotMaxRow) {
+        const int blocks = (args.a.n + 31) / 32;
+        if (max_row_blocks <= 8)
+            row_lanes_kernel<Real, 8><<<blocks, 128, 0, stream>>>(args);
+        else
+            row_lanes_kernel<Real, 16><<<blocks, 128, 0, stream>>>(args);
+        return cudaGetLastError();
+    }
     if (args.explicit_mode || max_row_blocks <= 8) return launch_rows<Real, 8>(args, stream);
     if (max_row_blocks <= 16) return launch_rows<Real, 16>(args, stream);
     return launch_rows<Real, 0>(args, stream);

@@ -95,6 +95,7 @@ struct AssemblyArgs {
     // not in the upper row (a lower or non-dynamic node), kSlotMissing when the pattern
     // lacks it.  NULL: no table (rows longer than kSlotMaxRow, or not built).
     const unsigned* inc_slot;
+    int row_lanes;                   // with a slot table: four lanes per row (1) or one thread (0)
     Real* values;                    // out: A blocks
     Real* rhs;                       // out: b
     Real* minv;                      // out: block-Jacobi inverse
@@ -333,6 +334,7 @@ struct SlabPcgArgs {
     const unsigned char* stream;
     unsigned long long stream_bytes;
     const int* halo_src;         // slab index of each halo row
+    const unsigned char* exported;  // per slab row: 1 when another part's window holds it
     const int* perm;             // slab index -> dynamic row
     const float* b;              // per dynamic row
     const float* minv;
@@ -362,11 +364,6 @@ struct SlabPcgArgs {
     // Stream form (pk_slab_plan.h): 0 full symmetric rows, 1 the symmetric form (each
     // in-sub-part block once, transposed products through the groups' shared-memory rings).
     int sym;
-    // L2 residency of the matrix stream, in 1/1024: the first l2_keep/1024 of each part's
-    // tiles are loaded with an L2 evict-last hint, so that share of the stream (the same
-    // every iteration) tends to stay in L2 between iterations; the rest stream with
-    // evict-first.
-    int l2_keep;
 };
 
 // ------------------------------------------------------------------ FP64 refinement

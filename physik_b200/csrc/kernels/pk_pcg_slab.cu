@@ -8,9 +8,10 @@
 //
 // * One block per part (pk_slab_plan.h).  The search directions d of the part's window
 //   (its rows, then its halo) stay in shared memory for the whole solve.  At the start of
-//   an iteration every block rebuilds its window as d = s + beta d from the s values the
-//   rows' owners published (s of the halo rows comes from the neighbouring parts), so
-//   the SpMV reads d only from shared memory.
+//   an iteration every block rebuilds its window as d = s + beta d: its own rows from the
+//   s its threads keep in registers, the halo rows from the s the neighbouring parts
+//   published (a part publishes only the rows some other window holds), so the SpMV
+//   reads d only from shared memory.
 // * The part's rows are streamed as tiles of full symmetric rows (upper blocks and the
 //   transposes of the lower ones, 16-bit window columns) by one producer warp, one TMA
 //   bulk copy per tile into a ring of stages, with an L2 evict-first policy so the
@@ -55,12 +56,7 @@ __device__ __forceinline__ unsigned long long l2_evict_first_policy()
     asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
     return pol;
 }
-__device__ __forceinline__ unsigned long long l2_evict_last_policy()
-{
-    unsigned long long pol;
-    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
-    return pol;
-}
+
 // Bulk copy global -> shared with an L2 cache-policy hint (no multicast).
 __device__ __forceinline__ void bulk_g2s_hint(void* dst, const void* src, unsigned bytes, unsigned long long* bar,
                                               unsigned long long pol)
@@ -277,9 +273,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     const int krows = (m + kSlabRowThreads - 1) / kSlabRowThreads;
     const unsigned tmem_row0 =
         s_tmem + ((32u * (unsigned)(warp % 4)) << 16) + (unsigned)((warp / 4) * kSlabRowsPerThread * 16);
-    const unsigned long long pol = l2_evict_first_policy(), pol_keep = l2_evict_last_policy();
-    // tiles [0, keep_tiles) of the part are the L2-resident share of its stream
-    const int keep_tiles = (int)(((long long)min(max(P.l2_keep, 0), 1024) * ntiles) / 1024);
+    const unsigned long long pol = l2_evict_first_policy();
     unsigned ring = 0;    // ring positions consumed so far (ntiles per iteration)
     unsigned issued = 0;  // ring positions issued by the producer (producer lane 0 only)
     unsigned xgen = 0;
@@ -410,12 +404,11 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                         s_fail = 1;
                         break;
                     }
-                    const int ti = (int)(p % (unsigned)ntiles);
-                    const int4 d = table[ti];
+                    const int4 d = table[p % (unsigned)ntiles];
                     mbar_arrive_expect_tx(&full_bar[s], (unsigned)d.y);
                     if (d.y > 0)
                         bulk_g2s_hint(ring_base + (size_t)s * stage_bytes, P.stream + 16 * (size_t)d.x,
-                                      (unsigned)d.y, &full_bar[s], ti < keep_tiles ? pol_keep : pol);
+                                      (unsigned)d.y, &full_bar[s], pol);
                 }
             }
             __syncwarp();
@@ -497,6 +490,16 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
         ring += (unsigned)ntiles;
     };
 
+    // The s values of this thread's rows stay in registers for the next window pass; only
+    // rows another part's window holds (expmask) are published to global memory.
+    V3<float> sreg[kSlabRowsPerThread];
+    unsigned expmask = 0u;
+#pragma unroll
+    for (int k = 0; k < kSlabRowsPerThread; ++k) {
+        sreg[k] = V3<float>{0.f, 0.f, 0.f};
+        const int i = rt + kSlabRowThreads * k;
+        if (row_owner && k < krows && i < m && __ldg(P.exported + row0 + i)) expmask |= 1u << k;
+    }
     unsigned fl = 0;
     int iterations = 0;
     bool converged = false;
@@ -510,7 +513,9 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
         Acc v[2] = {Acc(0), Acc(0)};
         int bad = s_bad ? 4 : 0;
         if (row_owner) {
-            for (int k = 0; k < krows; ++k) {
+#pragma unroll
+            for (int k = 0; k < kSlabRowsPerThread; ++k) {
+                if (k >= krows) break;
                 const int i = rt + kSlabRowThreads * k;
                 RowRec rec{};
                 if (i < m) {
@@ -530,7 +535,8 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                     put3(rec, 6, mi.c[0]);
                     put3(rec, 9, mi.c[1]);
                     put3(rec, 12, mi.c[2]);
-                    stv4(P.ss + 4 * (size_t)g, sv);
+                    sreg[k] = sv;
+                    if ((expmask >> k) & 1u) stv4(P.ss + 4 * (size_t)g, sv);
                     v[0] += dot_acc<Acc>(br, sv);
                     v[1] += dot_acc<Acc>(br, br);
                 }
@@ -576,21 +582,34 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                 converged = true;
                 break;
             }
-            // Window: d = s + beta d, s from the rows' owners.
+            // Window: d = s + beta d -- the part's own rows from their owners' registers,
+            // the halo rows from the s their owners published.
             {
-                // kWinBatch entries per thread per pass: their halo indices, then their s
+                const float bt = float(beta);
+                if (row_owner) {
+#pragma unroll
+                    for (int k = 0; k < kSlabRowsPerThread; ++k) {
+                        const int i = rt + kSlabRowThreads * k;
+                        if (k < krows && i < m) {
+                            float* d = win + 3 * i;
+                            d[0] = sreg[k].x + d[0] * bt;
+                            d[1] = sreg[k].y + d[1] * bt;
+                            d[2] = sreg[k].z + d[2] * bt;
+                        }
+                    }
+                }
+                // kWinBatch halo entries per thread per pass: their indices, then their s
                 // values are all in flight before any is used.
                 constexpr int kWinBatch = 8;
-                const float bt = float(beta);
                 const int step = (int)blockDim.x;
                 int wbad = 0;
-                for (int w0 = tid; w0 < wn; w0 += kWinBatch * step) {
+                for (int w0 = m + tid; w0 < wn; w0 += kWinBatch * step) {
                     int g[kWinBatch];
 #pragma unroll
                     for (int k = 0; k < kWinBatch; ++k) {
                         const int w = w0 + k * step;
                         int gi = 0;
-                        if (w < wn) gi = w < m ? row0 + w : __ldg(P.halo_src + halo0 + (w - m));
+                        if (w < wn) gi = __ldg(P.halo_src + halo0 + (w - m));
                         if ((unsigned)gi >= (unsigned)P.n) {
                             gi = 0;
                             wbad = 1;
@@ -667,7 +686,8 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                         const V3<float> rv = axpy<float, Acc>(rec3(rec, 3), -alpha, qv[k]);
                         const V3<float> sv = mul(rec_minv(rec), rv);
                         if (!finite3(sv)) sbad = 1;
-                        stv4(P.ss + 4 * (size_t)(row0 + i), sv);
+                        sreg[k] = sv;
+                        if ((expmask >> k) & 1u) stv4(P.ss + 4 * (size_t)(row0 + i), sv);
                         v[0] += dot_acc<Acc>(rv, sv);
                         v[1] += dot_acc<Acc>(rv, rv);
                         put3(rec, 0, xv);

@@ -2,6 +2,7 @@
 #include "pk_slab_plan.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <array>
 #include <atomic>
 #include <cmath>
@@ -12,6 +13,17 @@
 
 namespace pk {
 namespace {
+
+// The bisection weight of a row: its streamed blocks plus this per-row share (the row's
+// fixed work in a tile and in the per-row phases); PK_SLAB_ROW_WEIGHT overrides it.
+double row_weight_extra()
+{
+    if (const char* e = std::getenv("PK_SLAB_ROW_WEIGHT")) {
+        const double v = std::atof(e);
+        if (v >= 0.0 && v < 1e6) return v;
+    }
+    return 4.0;
+}
 
 // Host threads for the layout build (at most 16; 1 when none can be started).
 int plan_threads()
@@ -725,7 +737,8 @@ std::string build_slab_plan(int n, const int* row_start, const int* col, const i
         if (len[r] > kSlabCapE) return "a row has more blocks than a tile holds";
     std::vector<int> part_of(n, 0);
     std::vector<double> w(n);
-    for (int r = 0; r < n; ++r) w[r] = len[r] + 4.0;  // streamed blocks + per-row vector work
+    const double extra = row_weight_extra();
+    for (int r = 0; r < n; ++r) w[r] = len[r] + extra;  // streamed blocks + per-row work
     if (coords) {
         std::vector<int> ids(n);
         std::iota(ids.begin(), ids.end(), 0);
@@ -762,7 +775,8 @@ std::string build_slab_plan_batched(int n, const int* row_start, const int* col,
     for (int r = 0; r < n; ++r)
         if (len[r] > kSlabCapE) return "a row has more blocks than a tile holds";
     std::vector<double> w(n);
-    for (int r = 0; r < n; ++r) w[r] = len[r] + 4.0;
+    const double extra = row_weight_extra();
+    for (int r = 0; r < n; ++r) w[r] = len[r] + extra;
     // 0. the largest part to aim for.  A launch lasts about c0 + c1 * (its largest part's
     // rows) per iteration (c0 the exchanges, c1 the streaming; measured on B200 about 12 us
     // and 11 ns per row), so smaller parts can pay off although they take more launches:

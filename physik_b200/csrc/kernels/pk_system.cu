@@ -239,6 +239,7 @@ struct pk_system {
     unsigned long long slab_stream_bytes = 0;
     bool slab_sym = false;        // the layout is the symmetric stream form
     DevBuf slab_part_info, slab_tiles, slab_stream, slab_halo, slab_perm, slab_fill_src, slab_tile_e0;
+    DevBuf slab_export;  // per slab row: held by another part's window
     int slab_fill_entries = 0;
     DevBuf slab_qs, slab_ss;
     // FP64 outer true-residual refinement (FP32 storage, unbatched): passes, buffers
@@ -289,6 +290,8 @@ struct pk_system {
 
 namespace {
 
+bool row_lanes_enabled();
+
 template <class Real>
 pk::AssemblyArgs<Real> assembly_args(pk_system* s, const pk_step_params& p)
 {
@@ -316,6 +319,7 @@ pk::AssemblyArgs<Real> assembly_args(pk_system* s, const pk_step_params& p)
     a.inc_start = s->inc_start.as<int>();
     a.inc_list = s->inc_list.as<int>();
     a.inc_slot = s->slots_ok ? s->inc_slot.as<unsigned>() : nullptr;
+    a.row_lanes = row_lanes_enabled() ? 1 : 0;
     a.values = s->values.as<Real>();
     a.rhs = s->rhs.as<Real>();
     a.minv = s->minv.as<Real>();
@@ -539,20 +543,6 @@ int requested_slab_form()
     return pk::kSlabFull;
 }
 
-// The L2-resident share of the matrix stream (SlabPcgArgs::l2_keep, in 1/1024): by
-// default as much as fits in 64 MB of the 126 MB L2, leaving the rest to the CG vectors
-// and the streamed tiles; PK_SLAB_L2_KEEP=<fraction> overrides it.
-int slab_l2_keep(const pk_system* s)
-{
-    if (const char* e = std::getenv("PK_SLAB_L2_KEEP")) {
-        const double f = std::atof(e);
-        return static_cast<int>(std::min(1.0, std::max(0.0, f)) * 1024.0);
-    }
-    const double budget = 64.0 * 1024.0 * 1024.0;
-    if (s->slab_stream_bytes == 0) return 0;
-    return static_cast<int>(std::min(1.0, budget / static_cast<double>(s->slab_stream_bytes)) * 1024.0);
-}
-
 bool slab_allowed(const pk_system* s)
 {
     const int rk = requested_kernel();
@@ -621,6 +611,12 @@ int ensure_slab(pk_system* s)
     if (!rc && !plan.halo_src.empty())
         rc = upload_raw<int>(s->slab_halo, plan.halo_src.data(), plan.halo_src.size(), s->stream);
     if (!rc) rc = upload_raw<int>(s->slab_perm, plan.perm.data(), plan.perm.size(), s->stream);
+    if (!rc) {
+        std::vector<unsigned char> exported(static_cast<size_t>(n), 0);
+        for (const int g : plan.halo_src)
+            if (g >= 0 && g < n) exported[static_cast<size_t>(g)] = 1;
+        rc = upload_raw<unsigned char>(s->slab_export, exported.data(), exported.size(), s->stream);
+    }
     if (!rc) rc = upload_raw<unsigned>(s->slab_fill_src, plan.fill_src.data(), plan.fill_src.size(), s->stream);
     if (!rc) rc = upload_raw<int>(s->slab_tile_e0, plan.tile_entry0.data(), plan.tile_entry0.size(), s->stream);
     if (!rc) rc = upload_raw<int>(s->slab_part_body, plan.part_body.data(), plan.part_body.size(), s->stream);
@@ -680,6 +676,7 @@ int run_pcg_slab(pk_system* s, const pk_step_params& p, int skip_on_flags)
         a.stream = s->slab_stream.as<unsigned char>();
         a.stream_bytes = s->slab_stream_bytes;
         a.halo_src = s->slab_halo.as<int>();
+        a.exported = s->slab_export.as<unsigned char>();
         a.perm = s->slab_perm.as<int>();
         a.b = s->rhs.as<float>();
         a.minv = s->minv.as<float>();
@@ -705,7 +702,6 @@ int run_pcg_slab(pk_system* s, const pk_step_params& p, int skip_on_flags)
         a.body_stats = bodies ? s->body_stats.as<pk::BatchBodyStats>() : nullptr;
         a.missing = &st->batch_missing;
         a.sym = s->slab_sym ? 1 : 0;
-        a.l2_keep = slab_l2_keep(s);
         // One launch per group of parts (the coupled solve: one launch of all parts).
         const int launches = static_cast<int>(s->slab_launch.size()) - 1;
         for (int l = 0; l < launches; ++l) {
@@ -1013,6 +1009,14 @@ int run_pcg_refined(pk_system* s, const pk_step_params& p, int skip_on_flags)
     PK_CHECK(cudaMemcpyAsync(s->stats.p, &out, sizeof(out), cudaMemcpyHostToDevice, s->stream));
     PK_CHECK(cudaStreamSynchronize(s->stream));
     return PK_OK;
+}
+
+// PK_ROW_KERNEL=thread assembles the rows one thread each (the four-lane kernel's blocks
+// and right-hand side are the same bits; kept for comparisons).
+bool row_lanes_enabled()
+{
+    const char* e = std::getenv("PK_ROW_KERNEL");
+    return !(e && std::strcmp(e, "thread") == 0);
 }
 
 // PK_ASSEMBLY_FOLD=0 keeps every tet on the long assembly path (all 16 blocks per tet

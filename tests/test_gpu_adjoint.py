@@ -4,10 +4,11 @@ reference, checked three ways:
 * against central finite differences of the loss L = 1/2 |x_T - x_target|^2 computed
   with FP64 forward rollouts (the FP64 GPU path, itself checked against the FP64 oracle
   to 1e-14 per step), epsilon = 1e-3 (on the rollout workload Richardson-extrapolated
-  from 1e-3 and 5e-4); relative error <= 1e-4 (the most sensitive
-  coordinate of the 60-step rollout, where elements are crushed nearly flat and the
-  loss is far from quadratic at 1e-3, with epsilon = 1e-5), each coordinate relative to
-  its own finite difference;
+  from 1e-3 and 5e-4), each coordinate relative to its own finite difference: 1e-4 (the
+  most sensitive coordinate of the 60-step rollout, where elements are crushed nearly flat
+  and the loss is far from quadratic at 1e-3, with epsilon = 1e-5); on the rollout
+  workload's random coordinates 1e-4 |fd| plus the CG tolerance times the gradient's
+  scale, the gap between differentiating exact solves and differencing CG-stopped ones;
 * against an FP64 CPU reference gradient written independently in numpy on top of the
   FP64 oracle's assembled systems (tests/adjoint_harness.py), all coordinates, along the
   same trajectory (relative 1e-6);
@@ -127,8 +128,14 @@ def test_adjoint_beam32_rollout_workload():
     rng = np.random.default_rng(16)
     free_nodes = np.nonzero(free)[0]
     # Each coordinate against its own central difference, Richardson-extrapolated from eps
-    # and eps/2 ((4 D(eps/2) - D(eps)) / 3: truncation error O(eps^4) instead of O(eps^2)),
-    # relative to that difference -- no floor.
+    # and eps/2 ((4 D(eps/2) - D(eps)) / 3: truncation error O(eps^4) instead of O(eps^2)):
+    # |adjoint - fd| <= 1e-4 |fd| + tol_cg |g|.  The second term is the one the method
+    # itself leaves: the adjoint differentiates steps whose solves are exact, the
+    # differences a rollout whose CG stops at relative residual tol_cg = 1e-8, and the two
+    # derivatives differ by about tol_cg times the gradient's scale (measured: a coordinate
+    # of 7.2e-6 whose differences agree to 5 digits from eps 2e-3 to 1e-4 sits 2.1e-9 from
+    # the adjoint, with |g| = 0.33).
+    gscale = float(np.sqrt(np.sum(g_theta ** 2) + np.sum(g_v0[free] ** 2)))
     errors = []
     for c in range(16):
         if c % 2 == 0:
@@ -142,8 +149,8 @@ def test_adjoint_beam32_rollout_workload():
             d2 = fd_v0(world, young, x0, v0, steps, x_target, node, comp, eps=5e-4)
             ad = g_v0[node, comp]
         fd = (4.0 * d2 - d1) / 3.0
-        errors.append((abs(ad - fd) / abs(fd), ad, fd, d1))
-    assert max(e[0] for e in errors) <= 1e-4, errors
+        errors.append((abs(ad - fd) / (1e-4 * abs(fd) + scene.tolerance * gscale), ad, fd, d1))
+    assert max(e[0] for e in errors) <= 1.0, errors
     # The most sensitive coordinate (a tet at the clamped end that is nearly crushed flat,
     # where the rollout is strongly nonlinear): central differences converge to the
     # adjoint as the step shrinks; at 1e-5 they agree to 1e-4.

@@ -212,22 +212,3 @@ def test_sym_form_fp32_follows_fp32_reference(monkeypatch):
         assert rel(x, ora.x) <= 3e-7
         assert rel(v, ora.v) <= 2.5e-5
 
-
-def test_l2_resident_share_changes_no_bit(monkeypatch):
-    """The L2 hint on part of the matrix stream (PK_SLAB_L2_KEEP) only changes where the
-    tiles come from: results are bit-identical with none, the default and all of it."""
-    scene = meshes.config2()
-    states = []
-    for keep in ("0", None, "1"):
-        if keep is None:
-            monkeypatch.delenv("PK_SLAB_L2_KEEP", raising=False)
-        else:
-            monkeypatch.setenv("PK_SLAB_L2_KEEP", keep)
-        w = SimWorld(scene, precision="mixed")
-        for _ in range(2):
-            w.step()
-        assert w.pcg_kernel()[0] == "slab"
-        states.append(w.state(f64=True))
-    for x, v in states[1:]:
-        np.testing.assert_array_equal(x, states[0][0])
-        np.testing.assert_array_equal(v, states[0][1])
