@@ -526,6 +526,8 @@ def main():
                     help="profiling mode: step the workload this many times, print what ran, no JSON line")
     ap.add_argument("--against-fp64", action="store_true",
                     help="with --profile-steps: per-step differences against an FP64 world")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched256 side measurement of a single-GPU block128 run")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -597,6 +599,19 @@ def main():
                    cuda_graph=r["batched"])
     if r["fp64"] is not None:
         cfg_out["fp64_gpu"] = r["fp64"]
+    if world == 1 and args.workload == "block128" and not args.no_batched:
+        # The batched workload (256 uneven bodies, one PCG per body) measured in the same run.
+        side = argparse.Namespace(**vars(args))
+        side.workload, side.no_fp64 = "batched256", True
+        bcfg, bdesc = WORKLOADS["batched256"]
+        b = run_ours(side, meshes.CONFIGS[bcfg](), rank, world, local, pg)
+        cfg_out["batched256"] = {
+            "workload": bdesc, "steps_per_s": b["value"], "ms_per_step": b["ms_per_step"],
+            "e2e_steps_per_s": args.steps / b["e2e_s"], "pcg_ms": b["solve_ms"], "assemble_ms": b["assemble_ms"],
+            "pcg_kernel": b["pcg_kernel"], "pcg_blocks": b["pcg_blocks"], "max_body_cg_iterations": b["iters"],
+            "algorithmic_bytes_per_solve": b["bytes_per_solve"], "spmv_gbs": b["achieved"],
+            "frac": (b["achieved"] / b["peak"]) if b["achieved"] else None, "cuda_graph": True,
+            "gpu_launches": b["launches"], "clocks": b["clocks"]}
     line = {
         "metric": METRIC, "value": r["value"], "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,

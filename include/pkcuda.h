@@ -66,6 +66,7 @@ extern "C" {
 #define PK_FLAG_SOLVED 0x1000u         /* SolveImplicitLinearSystem would return true */
 #define PK_FLAG_INTEGRATED 0x2000u     /* positions and velocities were advanced */
 #define PK_FLAG_CONVERGED 0x4000u      /* CG met its relative tolerance */
+#define PK_FLAG_REFINED_FP64 0x8000u   /* the refinement measured the FP64 system element by element */
 
 typedef struct pk_step_params {
     double dt;               /* substep size (World::Step divides the frame by the substep count) */
@@ -131,6 +132,18 @@ PKCUDA_API int pk_system_snapshot_positions(pk_system* sys);
 PKCUDA_API int pk_system_sphere_contacts(pk_system* sys, const double* center, double radius, int max_contacts,
                                          int* tets, double* points);
 PKCUDA_API int pk_system_get_snapshot_f32(pk_system* sys, int first_node, int count, float* x);
+
+/* FP64 rest data and lumped masses of an FP32-stored system (FP32 or mixed precision):
+ * DmInv (9 per tet, column-major), rest volume, lambda, mu, damping per tet and the mass
+ * per world node, computed in FP64 from the same inputs (FEMModel::InitializeTetRestData,
+ * FEMModel.cpp:504-548; BuildElasticityMatrix's lambda and mu; the lumped mass rho V / 4).
+ * With them the refinement (pk_system_set_refinement) measures the residual of the FP64
+ * system element by element instead of over the FP32-stored blocks, when the system has
+ * no point connections and no host-emitted blocks.  Must follow pk_system_set_tets and
+ * pk_system_set_nodes (the counts must match); those and pk_system_set_masses drop it. */
+PKCUDA_API int pk_system_set_rest64(pk_system* sys, int tet_count, const double* dm_inv, const double* volume,
+                                    const double* lambda, const double* mu, const double* damping, int node_count,
+                                    const double* mass);
 
 /* Post-step geometry on the device, read back only when asked for.
  * kind 0, surface triangles (SurfaceVisualComponent::UpdateVisualSurfaceGeometry,

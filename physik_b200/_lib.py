@@ -237,6 +237,7 @@ FLAG_BARRIER_TIMEOUT = 0x100
 FLAG_SOLVED = 0x1000
 FLAG_INTEGRATED = 0x2000
 FLAG_CONVERGED = 0x4000
+FLAG_REFINED_FP64 = 0x8000
 
 
 def last_error() -> str:

@@ -710,7 +710,12 @@ public:
     void SetGraphCapture(bool on) { graphCapture = on; }
     // FP64 outer true-residual refinement passes for FP32 storage (extension; see
     // pk_system_set_refinement).  0: off.
-    void SetRefinement(int passes) { refinePasses = passes < 0 ? 0 : passes; }
+    void SetRefinement(int passes)
+    {
+        const int p = passes < 0 ? 0 : passes;
+        if (p > 0 && refinePasses == 0 && precision != Precision::FP64) ++topologyVersion;  // FP64 rest data
+        refinePasses = p;
+    }
     int GetRefinement() const { return refinePasses; }
     // Autotuner (extension): picks the fastest PCG kernel / tile or part size for the
     // current scene by timing `repeats` solves of the last assembled system (call after a

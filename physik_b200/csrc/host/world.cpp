@@ -25,6 +25,7 @@
 #include <stdexcept>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "../../../include/pkcuda.h"
@@ -438,6 +439,10 @@ struct DeviceScene {
     int refineOnDevice = 0;
     std::vector<unsigned char> enabled;
     std::vector<double> mass, dmInv, volume, lam, mu, damp;
+    // FP32 storage with refinement on: the same rest data and masses in FP64
+    // (pk_system_set_rest64).
+    bool rest64 = false;
+    std::vector<double> mass64, dmInv64, volume64, lam64, mu64;
     // The FEM bodies' pattern; rowStart / colIndex above are it joined with the blocks of
     // the current point connections (connPairs, canonical row <= column).
     std::vector<int> femRowStart, femColIndex;
@@ -489,6 +494,22 @@ void BuildHostScene(DeviceScene& sc, const World& w, const std::vector<const Tet
     sc.damp.assign(total, 0.0);
     std::vector<T> nodal(total, T(0));  // each tet's lumped mass share (0: none)
     std::vector<T> massT(static_cast<std::size_t>(nn), T(0));
+    // FP32 storage with refinement: the rest data and masses once more in FP64.
+    sc.rest64 = !std::is_same<T, double>::value && w.GetRefinement() > 0;
+    std::vector<double> nodal64;
+    if (sc.rest64) {
+        sc.dmInv64.assign(9 * total, 0.0);
+        sc.volume64.assign(total, 0.0);
+        sc.lam64.assign(total, 0.0);
+        sc.mu64.assign(total, 0.0);
+        nodal64.assign(total, 0.0);
+    } else {
+        sc.dmInv64.clear();
+        sc.volume64.clear();
+        sc.lam64.clear();
+        sc.mu64.clear();
+        sc.mass64.clear();
+    }
     std::size_t first = 0;
     for (const TetMeshPhysicsComponent* body : fem) {
         const int base = body->GetGlobalNodeBeginIndex();
@@ -525,6 +546,26 @@ void BuildHostScene(DeviceScene& sc, const World& w, const std::vector<const Tet
                     const T share = density * rd.volume * T(0.25);
                     if (std::isfinite(static_cast<double>(share)) && share > T(0)) nodal[g] = share;
                 }
+                if (sc.rest64) {
+                    const RestData<double> r64 =
+                        ComputeRest<double>(body->restNodePositions[t.node0], body->restNodePositions[t.node1],
+                                            body->restNodePositions[t.node2], body->restNodePositions[t.node3]);
+                    for (int c = 0; c < 3; ++c) {
+                        sc.dmInv64[9 * g + 3 * c + 0] = r64.dm_inv.c[c].x;
+                        sc.dmInv64[9 * g + 3 * c + 1] = r64.dm_inv.c[c].y;
+                        sc.dmInv64[9 * g + 3 * c + 2] = r64.dm_inv.c[c].z;
+                    }
+                    sc.volume64[g] = r64.volume;
+                    double l64, m64;
+                    LameParameters<double>(t.youngModulus, t.poissonRatio, l64, m64);
+                    sc.lam64[g] = l64;
+                    sc.mu64[g] = m64;
+                    const double d64 = std::max(0.0, static_cast<double>(body->material.density));
+                    if (std::isfinite(d64) && t.active && std::isfinite(r64.volume) && r64.volume > 0.0) {
+                        const double share = d64 * r64.volume * 0.25;
+                        if (std::isfinite(share) && share > 0.0) nodal64[g] = share;
+                    }
+                }
             }
         });
         first += tets.size();
@@ -546,6 +587,21 @@ void BuildHostScene(DeviceScene& sc, const World& w, const std::vector<const Tet
     for (const auto& e : extraMasses)
         if (std::get<2>(e)) massT[static_cast<std::size_t>(std::get<0>(e))] += T(std::get<1>(e));
     sc.extraMasses = extraMasses;
+    if (sc.rest64) {
+        // the same sums in FP64, in the same order
+        sc.mass64.assign(static_cast<std::size_t>(nn), 0.0);
+        for (const auto& e : extraMasses)
+            if (!std::get<2>(e)) sc.mass64[static_cast<std::size_t>(std::get<0>(e))] += double(std::get<1>(e));
+        for (std::size_t g = 0; g < total; ++g) {
+            if (!(nodal64[g] > 0.0)) continue;
+            for (int k = 0; k < 4; ++k) {
+                const int n = sc.tetNodes[4 * g + k];
+                if (!nodes[static_cast<std::size_t>(n)].fixed) sc.mass64[static_cast<std::size_t>(n)] += nodal64[g];
+            }
+        }
+        for (const auto& e : extraMasses)
+            if (std::get<2>(e)) sc.mass64[static_cast<std::size_t>(std::get<0>(e))] += double(std::get<1>(e));
+    }
     // World::ValidateNodeMasses
     for (int i = 0; i < nn; ++i) {
         const Node& nd = nodes[static_cast<std::size_t>(i)];
@@ -656,6 +712,14 @@ void BuildHostScene(DeviceScene& sc, const World& w, const std::vector<const Tet
     sc.connOnDevice = false;
 }
 
+void UploadRest64(DeviceScene& sc)
+{
+    if (!sc.rest64) return;
+    Check(pk_system_set_rest64(sc.sys, sc.tetCount, sc.dmInv64.data(), sc.volume64.data(), sc.lam64.data(),
+                               sc.mu64.data(), sc.damp.data(), sc.nodeCount, sc.mass64.data()),
+          "set_rest64");
+}
+
 void UploadScene(DeviceScene& sc, const std::vector<Vec3>& positions, const std::vector<Vec3>& velocities)
 {
     const int nn = sc.nodeCount;
@@ -672,6 +736,7 @@ void UploadScene(DeviceScene& sc, const std::vector<Vec3>& positions, const std:
     Check(pk_system_set_pattern(sc.sys, sc.dynCount, sc.dynToNode.data(), sc.rowStart.data(), sc.colIndex.data(),
                                 sc.incStart.data(), sc.incList.data()),
           "set_pattern");
+    UploadRest64(sc);
     sc.devDyn = sc.dynCount;
     sc.devNnz = static_cast<int>(sc.colIndex.size());
     sc.batchedOnDevice = false;
@@ -1176,6 +1241,7 @@ void World::EnsureScene(bool upload)
             Check(pk_system_set_tets(sc.sys, sc.tetCount, sc.tetNodes.data(), sc.enabled.data(), sc.dmInv.data(),
                                      sc.volume.data(), sc.lam.data(), sc.mu.data(), sc.damp.data()),
                   "set_tets");
+            UploadRest64(sc);
             sc.uploaded = true;
         }
     }

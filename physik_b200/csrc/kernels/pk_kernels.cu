@@ -236,22 +236,8 @@ __global__ void __launch_bounds__(256) tet_kernel(AssemblyArgs<Real> A)
             atomicAdd(&A.stats->polar_identity_count, 1);
         }
     }
-    // Displacement gradient in the rotated frame: grad u = R^T F - I (u_0 = 0 by the
-    // node-0 anchoring of the corotated displacement), strain = sym(grad u).
-    const M3<Real> g = linear ? f : mul(transpose(R), f);
-    const Real exx = g.c[0].x - Real(1), eyy = g.c[1].y - Real(1), ezz = g.c[2].z - Real(1);
-    const Real exy = Real(0.5) * (g.c[1].x + g.c[0].y);
-    const Real eyz = Real(0.5) * (g.c[2].y + g.c[1].z);
-    const Real exz = Real(0.5) * (g.c[2].x + g.c[0].z);
     const Real lam = st[10], mu = st[11];
-    const Real tr = exx + eyy + ezz;
-    const Real two_mu = Real(2) * mu;
-    // V * sigma, sigma = lambda tr(eps) I + 2 mu eps  (engineering-shear D of BuildElasticityMatrix)
-    const Real sxx = vol * (lam * tr + two_mu * exx), syy = vol * (lam * tr + two_mu * eyy),
-               szz = vol * (lam * tr + two_mu * ezz);
-    const Real sxy = vol * two_mu * exy, syz = vol * two_mu * eyz, sxz = vol * two_mu * exz;
-    const M3<Real> sig = mcols(v3<Real>(sxx, sxy, sxz), v3<Real>(sxy, syy, syz), v3<Real>(sxz, syz, szz));
-    const M3<Real> S = linear ? sig : mul(R, sig);
+    const M3<Real> S = corotated_stress(f, R, linear, vol, lam, mu);
     M3<Real> out = S;
     Real form = Real(0);
     if (A.inc_slot && !A.explicit_mode) {
@@ -265,25 +251,14 @@ __global__ void __launch_bounds__(256) tet_kernel(AssemblyArgs<Real> A)
         // the row kernel takes the long way with S, which applies the reference's rules
         // for non-finite forces and blocks.
         const V3<Real> vk[4] = {ld3(A.v, n.x), ld3(A.v, n.y), ld3(A.v, n.z), ld3(A.v, n.w)};
-        const M3<Real> fd = mul(mcols(vk[1] - vk[0], vk[2] - vk[0], vk[3] - vk[0]), dmi);
-        const M3<Real> G = linear ? fd : mul(transpose(R), fd);
-        const Real ltr = vol * lam * ((G.c[0].x + G.c[1].y) + G.c[2].z);
-        const Real vm = vol * mu;
-        M3<Real> P;
-        P.c[0] = v3<Real>(ltr + vm * (G.c[0].x + G.c[0].x), vm * (G.c[0].y + G.c[1].x), vm * (G.c[0].z + G.c[2].x));
-        P.c[1] = v3<Real>(vm * (G.c[1].x + G.c[0].y), ltr + vm * (G.c[1].y + G.c[1].y), vm * (G.c[1].z + G.c[2].y));
-        P.c[2] = v3<Real>(vm * (G.c[2].x + G.c[0].z), vm * (G.c[2].y + G.c[1].z), ltr + vm * (G.c[2].z + G.c[2].z));
-        const M3<Real> Q = linear ? P : mul(R, P);
+        const M3<Real> Q = folded_stiffness(R, dmi, vk, linear, vol, lam, mu);
         const Real dt = A.dt, dt2 = dt * dt;
         M3<Real> T;
 #pragma unroll
         for (int j = 0; j < 3; ++j) T.c[j] = -(S.c[j] * dt + Q.c[j] * dt2);
         const Real damp = rec[30];
         V3<Real> gr[4];
-        gr[1] = v3<Real>(dmi.c[0].x, dmi.c[1].x, dmi.c[2].x);
-        gr[2] = v3<Real>(dmi.c[0].y, dmi.c[1].y, dmi.c[2].y);
-        gr[3] = v3<Real>(dmi.c[0].z, dmi.c[1].z, dmi.c[2].z);
-        gr[0] = -((gr[1] + gr[2]) + gr[3]);
+        shape_gradients(dmi, gr);
         bool ok = finite9(T);
         Real g2 = Real(0);
 #pragma unroll

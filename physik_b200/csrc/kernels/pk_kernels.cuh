@@ -25,6 +25,7 @@ enum : unsigned {
     kFlagSolved = 0x1000u,
     kFlagIntegrated = 0x2000u,
     kFlagConverged = 0x4000u,
+    kFlagRefinedFp64 = 0x8000u,
 };
 
 struct GridSync {
@@ -398,6 +399,43 @@ cudaError_t launch_refine_accumulate(double* x64, const Real* dx, int count, int
 // args.integrate, the update of velocities and positions when nothing failed.
 template <class Real>
 cudaError_t launch_refine_update(const RefineArgs<Real>& args, cudaStream_t stream);
+
+// The FP64 true residual of an FP32-stored step, from the tet data rather than the stored
+// blocks: r = b - A x with b = dt f - dt^2 K v + dt m g and A = M + dt^2 K evaluated
+// element by element in FP64 (FP64 rest data, FP64 polar rotation and stress), i.e.
+//   r_a = sum over a's tets of -(dt S + dt^2 Q(v + x~)) g_a - dt c v_a + dt m g - m x_a
+// (Q the folded stiffness, x~ the solution on the dynamic nodes and 0 elsewhere).
+template <class Real>
+struct ElemResidualArgs {
+    int n;                          // dynamic rows
+    int node_count;
+    int tet_count;
+    const int4* tet_nodes;
+    const unsigned char* enabled;   // bit 0 simulated, bit 1 linear
+    const double* dm_inv;           // FP64 rest data: 9 per tet
+    const double* params;           // 4 per tet: rest volume, lambda, mu, damping
+    const double* mass;             // FP64, per world node
+    const Real* x;                  // node state (storage type)
+    const Real* v;
+    const int* node_to_dyn;
+    const int* dyn_to_node;
+    const int* inc_start;
+    const int* inc_list;
+    const Real* minv;               // block-Jacobi inverse (storage type), for r^T M^-1 r
+    const double* x64;              // the FP64 solution so far (NULL: 0)
+    double* vx;                     // scratch: per world node v + x~
+    double* u;                      // scratch: per tet -(dt S + dt^2 Q(v + x~)), NaN when skipped
+    double dt;
+    double gravity[3];
+    int linear;
+    Real* rhs_out;                  // residual rounded to Real (may be NULL)
+    double* partials;               // 2 per block: r^T M^-1 r, r.r
+    int* bad;
+};
+template <class Real>
+int elem_residual_blocks(int n);
+template <class Real>
+cudaError_t launch_elem_residual(const ElemResidualArgs<Real>& args, cudaStream_t stream);
 
 // ------------------------------------------------------------------ adjoint step
 // Backward element kernel (pk_adjoint.cu): per tet, the sensitivities of

@@ -191,4 +191,56 @@ __host__ __device__ inline M3<T> polar_rotation(const M3<T>& f, int* iterations,
     return r;
 }
 
+// S = R V sigma of a corotated tet (V sigma for the linear model, R = I), so that corner
+// a's elastic force is -S g_a: the displacement gradient in the rotated frame is
+// g = R^T F - I (F - I for the linear model; the corotated displacement is anchored at
+// node 0), eps = sym(g), V sigma = V (lambda tr(eps) I + 2 mu eps) with the engineering-
+// shear D of FEMModel::BuildElasticityMatrix (FEMModel.cpp:174-200, 247-271, 336-424).
+template <class T>
+__host__ __device__ __forceinline__ M3<T> corotated_stress(const M3<T>& f, const M3<T>& R, bool linear, T vol, T lam,
+                                                          T mu)
+{
+    const M3<T> g = linear ? f : mul(transpose(R), f);
+    const T exx = g.c[0].x - T(1), eyy = g.c[1].y - T(1), ezz = g.c[2].z - T(1);
+    const T exy = T(0.5) * (g.c[1].x + g.c[0].y);
+    const T eyz = T(0.5) * (g.c[2].y + g.c[1].z);
+    const T exz = T(0.5) * (g.c[2].x + g.c[0].z);
+    const T tr = exx + eyy + ezz;
+    const T two_mu = T(2) * mu;
+    const T sxx = vol * (lam * tr + two_mu * exx), syy = vol * (lam * tr + two_mu * eyy),
+            szz = vol * (lam * tr + two_mu * ezz);
+    const T sxy = vol * two_mu * exy, syz = vol * two_mu * eyz, sxz = vol * two_mu * exz;
+    const M3<T> sig = mcols(v3<T>(sxx, sxy, sxz), v3<T>(sxy, syy, syz), v3<T>(sxz, syz, szz));
+    return linear ? sig : mul(R, sig);
+}
+
+// The tet's stiffness applied to per-node vectors u_0..u_3, folded: with
+// K_ab = R Ke_ab R^T and Ke_ab = V (lambda g_a g_b^T + mu g_b g_a^T + mu (g_a.g_b) I),
+//   sum_b K_ab u_b = Q g_a,  Q = V R (lambda tr(G) I + mu (G + G^T)),
+//   G = R^T sum_b u_b g_b^T = R^T [u1 - u0, u2 - u0, u3 - u0] DmInv   (R = I when linear).
+template <class T>
+__host__ __device__ __forceinline__ M3<T> folded_stiffness(const M3<T>& R, const M3<T>& dmi, const V3<T> (&u)[4],
+                                                          bool linear, T vol, T lam, T mu)
+{
+    const M3<T> fd = mul(mcols(u[1] - u[0], u[2] - u[0], u[3] - u[0]), dmi);
+    const M3<T> G = linear ? fd : mul(transpose(R), fd);
+    const T ltr = vol * lam * ((G.c[0].x + G.c[1].y) + G.c[2].z);
+    const T vm = vol * mu;
+    M3<T> P;
+    P.c[0] = v3<T>(ltr + vm * (G.c[0].x + G.c[0].x), vm * (G.c[0].y + G.c[1].x), vm * (G.c[0].z + G.c[2].x));
+    P.c[1] = v3<T>(vm * (G.c[1].x + G.c[0].y), ltr + vm * (G.c[1].y + G.c[1].y), vm * (G.c[1].z + G.c[2].y));
+    P.c[2] = v3<T>(vm * (G.c[2].x + G.c[0].z), vm * (G.c[2].y + G.c[1].z), ltr + vm * (G.c[2].z + G.c[2].z));
+    return linear ? P : mul(R, P);
+}
+
+// Shape-function gradients: g1..g3 are the rows of DmInv, g0 = -(g1 + g2 + g3).
+template <class T>
+__host__ __device__ __forceinline__ void shape_gradients(const M3<T>& dmi, V3<T> (&gr)[4])
+{
+    gr[1] = v3<T>(dmi.c[0].x, dmi.c[1].x, dmi.c[2].x);
+    gr[2] = v3<T>(dmi.c[0].y, dmi.c[1].y, dmi.c[2].y);
+    gr[3] = v3<T>(dmi.c[0].z, dmi.c[1].z, dmi.c[2].z);
+    gr[0] = -((gr[1] + gr[2]) + gr[3]);
+}
+
 }  // namespace pk

@@ -272,6 +272,10 @@ struct pk_system {
     // rows
     DevBuf dyn_to_node, row_start, col, lt_start, lt_row, lt_block, inc_start, inc_list, values, rhs, minv;
     DevBuf inc_slot;        // per incidence: the row slots of the tet's nodes (built on first use)
+    // FP64 rest data and masses of an FP32-stored system, for the refinement's element-
+    // wise FP64 residual (FP64 systems use their own arrays), and its scratch.
+    DevBuf dm_inv64, params64, mass64, elem_u, elem_vx;
+    bool rest64_ok = false;  // pk_system_set_rest64 matches the current tets and nodes
     bool slots_ok = false;  // inc_slot matches the pattern, incidences, tets and node rows
     // solver
     DevBuf px, pr, psd0, psd1, pq, part_a, part_b, part_bad, sync, stats;
@@ -926,13 +930,51 @@ int run_pcg_refined(pk_system* s, const pk_step_params& p, int skip_on_flags)
     a.minv = s->minv.as<Real>();
     a.partials = s->ref_part.as<double>();
     a.bad = s->ref_bad.as<int>();
-    std::vector<double> part(2 * static_cast<size_t>(blocks));
+    // The FP64 system's residual from the tet data when the world holds only soft bodies
+    // (point connections and host-emitted blocks exist only as stored blocks).
+    const bool elem = s->conn_count == 0 && !s->ext_on && s->tet_count > 0 && s->dyn_count > 0 &&
+                      s->precision != PK_PREC_FP64 && s->rest64_ok;
+    pk::ElemResidualArgs<Real> ea{};
+    const int eblocks = pk::elem_residual_blocks<Real>(n);
+    if (elem) {
+        PK_CHECK(s->elem_u.ensure(9 * sizeof(double) * static_cast<size_t>(s->tet_count)));
+        PK_CHECK(s->elem_vx.ensure(3 * sizeof(double) * static_cast<size_t>(std::max(1, s->node_count))));
+        ea.n = n;
+        ea.node_count = s->node_count;
+        ea.tet_count = s->tet_count;
+        ea.tet_nodes = s->tet_nodes.as<int4>();
+        ea.enabled = s->tet_enabled.as<unsigned char>();
+        ea.dm_inv = s->dm_inv64.as<double>();
+        ea.params = s->params64.as<double>();
+        ea.mass = s->mass64.as<double>();
+        ea.x = s->x.as<Real>();
+        ea.v = s->v.as<Real>();
+        ea.node_to_dyn = s->node_to_dyn.as<int>();
+        ea.dyn_to_node = s->dyn_to_node.as<int>();
+        ea.inc_start = s->inc_start.as<int>();
+        ea.inc_list = s->inc_list.as<int>();
+        ea.minv = s->minv.as<Real>();
+        ea.vx = s->elem_vx.as<double>();
+        ea.u = s->elem_u.as<double>();
+        ea.dt = static_cast<double>(static_cast<float>(p.dt));
+        for (int i = 0; i < 3; ++i) ea.gravity[i] = static_cast<double>(static_cast<float>(p.gravity[i]));
+        ea.linear = p.linear;
+        ea.partials = s->ref_part.as<double>();
+        ea.bad = s->ref_bad.as<int>();
+    }
+    std::vector<double> part(2 * static_cast<size_t>(elem ? eblocks : blocks));
     // r = b - A x (x == NULL: r = b); returns false on a non-finite residual.
     auto residual = [&](const double* x, Real* rhs_out, double& rho, double& rr) -> int {
         a.x64 = x;
         a.rhs_out = rhs_out;
         PK_CHECK(cudaMemsetAsync(s->ref_bad.p, 0, sizeof(int), s->stream));
-        PK_CHECK(pk::launch_refine_residual<Real>(a, s->stream));
+        if (elem) {
+            ea.x64 = x;
+            ea.rhs_out = rhs_out;
+            PK_CHECK(pk::launch_elem_residual<Real>(ea, s->stream));
+        } else {
+            PK_CHECK(pk::launch_refine_residual<Real>(a, s->stream));
+        }
         int bad = 0;
         PK_CHECK(cudaMemcpyAsync(part.data(), s->ref_part.p, sizeof(double) * part.size(), cudaMemcpyDeviceToHost,
                                  s->stream));
@@ -940,9 +982,9 @@ int run_pcg_refined(pk_system* s, const pk_step_params& p, int skip_on_flags)
         PK_CHECK(cudaStreamSynchronize(s->stream));
         rho = 0.0;
         rr = 0.0;
-        for (int i = 0; i < blocks; ++i) {
-            rho += part[2 * static_cast<size_t>(i)];
-            rr += part[2 * static_cast<size_t>(i) + 1];
+        for (size_t i = 0; 2 * i < part.size(); ++i) {
+            rho += part[2 * i];
+            rr += part[2 * i + 1];
         }
         return bad || !std::isfinite(rho) || !std::isfinite(rr) ? 1 : 0;
     };
@@ -1001,6 +1043,7 @@ int run_pcg_refined(pk_system* s, const pk_step_params& p, int skip_on_flags)
         if (p.integrate) fl |= (bad & 2) ? pk::kFlagIntegrateAbort : pk::kFlagIntegrated;
     }
     if (converged) fl |= pk::kFlagConverged;
+    if (elem) fl |= pk::kFlagRefinedFp64;
     pk::DevStats out = st;
     out.iterations = total;
     out.converged = converged ? 1 : 0;
@@ -1294,6 +1337,7 @@ PKCUDA_API int pk_system_set_nodes(pk_system* s, int node_count, const int* node
     s->h_mass.assign(mass, mass + node_count);
     int rc = upload_raw<int>(s->node_to_dyn, node_to_dyn, node_count, s->stream);
     if (!rc) rc = upload_real_any(s, s->mass, mass, node_count);
+    s->rest64_ok = false;
     if (rc) return rc;
     const size_t bytes = 3 * s->rsize() * static_cast<size_t>(std::max(1, node_count));
     PK_CHECK(s->x.ensure(bytes));
@@ -1552,6 +1596,7 @@ PKCUDA_API int pk_system_set_masses(pk_system* s, const double* mass)
     if (!s->have_nodes) return fail(PK_ERR_STATE, "masses before the nodes");
     PK_CHECK(cudaSetDevice(s->device));
     s->h_mass.assign(mass, mass + s->node_count);
+    s->rest64_ok = false;
     return upload_real_any(s, s->mass, mass, s->node_count);
 }
 
@@ -1582,6 +1627,7 @@ PKCUDA_API int pk_system_set_tets(pk_system* s, int tet_count, const int* tet_no
     if (!rc) rc = upload_raw<unsigned char>(s->tet_enabled, enabled, tet_count, s->stream);
     if (!rc) rc = upload_real_any(s, s->dm_inv, dm_inv, 9 * static_cast<size_t>(tet_count));
     if (!rc) rc = upload_real_any(s, s->tet_params, params.data(), params.size());
+    s->rest64_ok = false;
     if (rc) return rc;
     PK_CHECK(s->tet_rec.ensure(pk::kTetRec * s->rsize() * std::max<size_t>(1, tet_count)));
     if (s->precision == PK_PREC_FP64)
@@ -1591,6 +1637,33 @@ PKCUDA_API int pk_system_set_tets(pk_system* s, int tet_count, const int* tet_no
         PK_CHECK(pk::launch_tet_pack<float>(s->dm_inv.as<float>(), s->tet_params.as<float>(),
                                             s->tet_rec.as<float>(), tet_count, s->stream));
     s->have_tets = true;
+    return PK_OK;
+}
+
+PKCUDA_API int pk_system_set_rest64(pk_system* s, int tet_count, const double* dm_inv, const double* volume,
+                                    const double* lambda, const double* mu, const double* damping, int node_count,
+                                    const double* mass)
+{
+    if (!s || tet_count < 0 || node_count < 0) return fail(PK_ERR_ARG, "set_rest64");
+    if (!s->have_tets || !s->have_nodes || tet_count != s->tet_count || node_count != s->node_count)
+        return fail(PK_ERR_STATE, "set_rest64: not the system's tets and nodes");
+    if ((tet_count > 0 && (!dm_inv || !volume || !lambda || !mu || !damping)) || (node_count > 0 && !mass))
+        return fail(PK_ERR_ARG, "set_rest64: NULL array");
+    PK_CHECK(cudaSetDevice(s->device));
+    s->rest64_ok = false;
+    std::vector<double> params(4 * static_cast<size_t>(tet_count));
+    for (int t = 0; t < tet_count; ++t) {
+        params[4 * t + 0] = volume[t];
+        params[4 * t + 1] = lambda[t];
+        params[4 * t + 2] = mu[t];
+        params[4 * t + 3] = damping[t];
+    }
+    int rc = upload_raw<double>(s->dm_inv64, dm_inv, 9 * static_cast<size_t>(tet_count), s->stream);
+    if (!rc) rc = upload_raw<double>(s->params64, params.data(), params.size(), s->stream);
+    if (!rc) rc = upload_raw<double>(s->mass64, mass, static_cast<size_t>(node_count), s->stream);
+    if (rc) return rc;
+    PK_CHECK(cudaStreamSynchronize(s->stream));
+    s->rest64_ok = true;
     return PK_OK;
 }
 
