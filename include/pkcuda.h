@@ -313,9 +313,9 @@ PKCUDA_API int pk_pcg(int device, int precision, int n, const int* row_start, co
  * loads the library until exit: at most 32,768 rows (PK_ERR_UNSUPPORTED above that).
  * All calls on a device share that array and it keeps the last call's contents (the call
  * clears what must start at zero); calls whose GPU work overlaps race on it.  The first
- * call on a device looks up the array's address, with that device current; make it
- * before any stream capture begins.  Runs on `stream` of the current device and waits
- * for it to return the statistics. */
+ * call on a device looks up the array's address, with that device current.  Every call
+ * runs on `stream` of the current device and synchronises that stream to return the
+ * statistics, so it must not be called while the stream is being captured into a graph. */
 PKCUDA_API int pk_pcg_noalloc(int precision, int n, const int* row_start, const int* col_index, const void* values,
                               const int* lt_start, const int* lt_row, const int* lt_block, const void* b,
                               const void* minv, int max_iterations, double tolerance, void* x, pk_cg_result* out,

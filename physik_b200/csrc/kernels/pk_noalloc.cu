@@ -16,8 +16,9 @@
 //     the call clears what must start at zero.  Calls whose GPU work overlaps (two
 //     streams, or two host threads) race on it and corrupt each other.
 //   * The first call on a device looks up the array's device address (a one-time set-up
-//     per device, done with that device current); make that first call before any stream
-//     capture begins.
+//     per device, done with that device current).
+//   * Every call synchronises its stream to return the statistics: it must not be called
+//     while that stream is being captured into a CUDA graph.
 #include <cuda_runtime.h>
 
 #include <algorithm>
