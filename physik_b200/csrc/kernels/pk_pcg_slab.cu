@@ -133,6 +133,23 @@ __device__ __forceinline__ M3<float> rec_minv(const RowRec& r)
     return m;
 }
 
+// alpha split into two floats, hi = float(alpha) and lo = float(alpha - hi), so that the
+// FP32 updates x + alpha d and r - alpha q take two FMAs per component instead of the
+// float -> double -> float round trip (24 conversions a row, which bound phase B: the
+// conversion unit retires a quarter of a warp per cycle).  The result is within one
+// float ulp of the FP64 update; with FP32 reductions lo is zero and is not applied.
+template <class Acc>
+struct SplitAlpha {
+    float hi, lo;
+    __device__ __forceinline__ explicit SplitAlpha(Acc a) : hi(float(a)), lo(float(a - Acc(float(a)))) {}
+    __device__ __forceinline__ V3<float> axpy(V3<float> a, V3<float> b) const
+    {
+        V3<float> t{fmaf(hi, b.x, a.x), fmaf(hi, b.y, a.y), fmaf(hi, b.z, a.z)};
+        if constexpr (sizeof(Acc) == 8) t = V3<float>{fmaf(lo, b.x, t.x), fmaf(lo, b.y, t.y), fmaf(lo, b.z, t.z)};
+        return t;
+    }
+};
+
 template <class Acc>
 __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<Acc> P)
 {
@@ -673,6 +690,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
             Acc v[2] = {Acc(0), Acc(0)};
             int sbad = 0;
             if (row_owner) {
+                const SplitAlpha<Acc> pa(alpha), na(-alpha);
                 // Stores of x, r (8 columns) without waits: one wait after the loop.
 #pragma unroll
                 for (int k = 0; k < kSlabRowsPerThread; ++k) {
@@ -682,14 +700,16 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                     tmem_ld16(tmem_row0 + 16u * (unsigned)k, rec);
                     if (i < m) {
                         const float* d = win + 3 * i;
-                        const V3<float> xv = axpy<float, Acc>(rec3(rec, 0), alpha, V3<float>{d[0], d[1], d[2]});
-                        const V3<float> rv = axpy<float, Acc>(rec3(rec, 3), -alpha, qv[k]);
+                        const V3<float> xv = pa.axpy(rec3(rec, 0), V3<float>{d[0], d[1], d[2]});
+                        const V3<float> rv = na.axpy(rec3(rec, 3), qv[k]);
                         const V3<float> sv = mul(rec_minv(rec), rv);
                         if (!finite3(sv)) sbad = 1;
                         sreg[k] = sv;
                         if ((expmask >> k) & 1u) stv4(P.ss + 4 * (size_t)(row0 + i), sv);
-                        v[0] += dot_acc<Acc>(rv, sv);
-                        v[1] += dot_acc<Acc>(rv, rv);
+                        // r widened once for both dots
+                        const Acc r0 = Acc(rv.x), r1 = Acc(rv.y), r2 = Acc(rv.z);
+                        v[0] += r0 * Acc(sv.x) + r1 * Acc(sv.y) + r2 * Acc(sv.z);
+                        v[1] += r0 * r0 + r1 * r1 + r2 * r2;
                         put3(rec, 0, xv);
                         put3(rec, 3, rv);
                     }
