@@ -112,6 +112,11 @@ __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned coun
 {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
 }
+// Before an mbarrier's memory is initialised again (no thread may still wait on it).
+__device__ __forceinline__ void mbar_inval(unsigned long long* bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
 __device__ __forceinline__ void mbar_fence_init()
 {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");

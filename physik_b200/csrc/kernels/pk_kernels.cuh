@@ -325,10 +325,14 @@ static_assert(kSlabRows * kSlabLanesPerRow == 32 * kSlabGroupWarps, "one tile ro
 static_assert(kSlabRowThreads == 32 * kSlabConsumerWarps, "the consumer warps own the rows");
 static_assert(kSlabGroups * kSlabRowsPerThread * 16 <= 512, "row records must fit tensor memory");
 
+// A part_info row whose group is {kSlabNoGroup, 0}: the block has no part in that round.
+constexpr int kSlabNoGroup = -1;
+
 template <class Acc>
 struct SlabPcgArgs {
     int n;                       // dynamic rows
-    const int* part_info;        // kSlabPartInts per block
+    int rounds;                  // parts per block, taken in order (1 for the coupled solve)
+    const int* part_info;        // [rounds][grid] x kSlabPartInts
     const int4* tile_desc;       // per tile: stream offset / 16, bytes, first local row, rows
     int tile_count;
     int halo_count;
@@ -342,8 +346,8 @@ struct SlabPcgArgs {
     float* x;                    // per dynamic row: delta-v out
     float* qs;                   // 4 per slab row: q of phase A
     float* ss;                   // 4 per slab row: s published for the window passes
-    ExSlot* slots;               // [2][grid]
-    unsigned* group_count;       // [grid]: arrival counter of the group starting at each block (zeroed)
+    ExSlot* slots;               // [rounds][2][grid]
+    unsigned* group_count;       // [rounds][grid]: arrival counter of the group starting at each block (zeroed)
     GridSync* sync;              // err flag
     int max_iterations;
     Acc tolerance;
@@ -358,7 +362,7 @@ struct SlabPcgArgs {
     // Per-body solves (grouped): each block's body, the per-body statistics and the success
     // flags some body lacks; 0 / NULL for the coupled solve (one group of all blocks).
     int grouped;
-    const int* part_body;        // [grid]
+    const int* part_body;        // [rounds][grid]
     int nbodies;
     BatchBodyStats* body_stats;
     unsigned* missing;

@@ -162,6 +162,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     __shared__ int sh_int[32];
     __shared__ int s_fail;
     __shared__ int s_bad;
+    __shared__ int s_stop;  // a bulk copy may still be in flight: no further round
     __shared__ unsigned s_tmem;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, blk = blockIdx.x;
@@ -178,24 +179,55 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     // symmetric form: this group's ring of transposed products (3 floats per slot)
     float* tp = reinterpret_cast<float*>(dyn + kSlabSymTpOffset) + (size_t)3 * kSymRingSlots * (size_t)(group < kSlabGroups ? group : 0);
 
+    // Precompute failures upstream: every part reports zero statistics and nothing is solved.
+    const unsigned in_flags = *(volatile unsigned*)P.flags;
+    const bool skip = P.skip_on_flags && (in_flags & (kFlagPrecomputeFailed | kFlagSingularDiag));
+    // Tensor memory for the rows' x, r, M^-1 (all 512 columns: one block per SM), held
+    // across the rounds.
+    if (!skip && warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
+                     "r"(512u)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tmem_fence_before();
+    __syncthreads();
+    tmem_fence_after();
+
+    // One part per block and round (the coupled solve: one round).  A block takes its
+    // rounds in order, so a group of round l starts once each of its blocks has finished its
+    // parts of the earlier rounds: the group of the lowest unfinished round can always
+    // proceed, and no group waits on a later one.
+    bool bars_live = false;
+    if (tid == 0) s_stop = 0;
+    for (int round = 0; round < P.rounds; ++round) {
     // The part: rows [row0, row0 + m) of the slab order, halo rows halo_src[halo0 ..
     // halo0 + h), tiles [tile0, tile0 + ntiles).  A part that does not fit the block's
     // tables (the host never builds one) is emptied and reports a breakdown.
+    const size_t slot_of_part = (size_t)round * gridDim.x + (size_t)blk;
     int row0, m, halo0, h, tile0, ntiles, gfirst, gsize;
     {
-        const int4 a = __ldg(reinterpret_cast<const int4*>(P.part_info) + 2 * blk);
-        const int4 b = __ldg(reinterpret_cast<const int4*>(P.part_info) + 2 * blk + 1);
+        const int4 a = __ldg(reinterpret_cast<const int4*>(P.part_info) + 2 * slot_of_part);
+        const int4 b = __ldg(reinterpret_cast<const int4*>(P.part_info) + 2 * slot_of_part + 1);
         row0 = a.x;
         m = a.y;
         halo0 = a.z;
         h = a.w;
         tile0 = b.x;
         ntiles = b.y;
-        gfirst = b.z;  // this part's group: blocks [gfirst, gfirst + gsize) of the launch
+        gfirst = b.z;  // this part's group: blocks [gfirst, gfirst + gsize) of the round
         gsize = b.w;
     }
+    if (gfirst == kSlabNoGroup && gsize == 0) continue;  // no part for this block in this round
+    // The previous round is done with the barriers and tables: the stage barriers start
+    // again from phase 0 (the copies issued ahead have landed: see finish).
+    __syncthreads();
     if (tid == 0) {
         for (int s = 0; s < S; ++s) {
+            if (bars_live) {
+                mbar_inval(&full_bar[s]);
+                mbar_inval(&empty_bar[s]);
+            }
             mbar_init(&full_bar[s], 1);
             mbar_init(&empty_bar[s], kSlabGroupWarps);
         }
@@ -203,13 +235,14 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
         s_fail = 0;
         s_bad = 0;
     }
+    bars_live = true;
     __syncthreads();
     // A group must hold this block; the coupled solve is one group of the whole grid.
     const bool group_ok = gfirst >= 0 && gsize >= 1 && gfirst + gsize <= (int)gridDim.x && blk >= gfirst &&
                           blk < gfirst + gsize && (P.grouped || (gfirst == 0 && gsize == (int)gridDim.x));
     int body = 0;
     if (P.grouped) {
-        body = __ldg(P.part_body + blk);
+        body = __ldg(P.part_body + slot_of_part);
         if ((unsigned)body >= (unsigned)P.nbodies) body = -1;
     }
     if (!group_ok || body < 0) {
@@ -219,7 +252,9 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
         body = 0;
         if (tid == 0) s_bad = 1;
     }
-    unsigned* const gcount = P.group_count + gfirst;  // the group's arrival counter
+    // The round's exchange slots and its groups' arrival counters.
+    ExSlot* const slots = P.slots + (size_t)round * 2 * gridDim.x;
+    unsigned* const gcount = P.group_count + (size_t)round * gridDim.x + gfirst;
     BatchBodyStats* const bs = P.grouped ? P.body_stats + body : nullptr;
     const bool leader = P.grouped ? blk == gfirst : blk == 0;
     if (m < 0 || m > kSlabMaxRows || h < 0 || m + h > kSlabWinCap || row0 < 0 || row0 + m > P.n || ntiles < 0 ||
@@ -258,8 +293,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     }
     __syncthreads();
 
-    const unsigned in_flags = *(volatile unsigned*)P.flags;
-    if (P.skip_on_flags && (in_flags & (kFlagPrecomputeFailed | kFlagSingularDiag))) {
+    if (skip) {
         if (leader && tid == 0) {
             if (P.grouped) {
                 bs->iterations = 0;
@@ -272,19 +306,8 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                 P.stats->residual_norm = 0.0;
             }
         }
-        return;
+        continue;
     }
-
-    // Tensor memory for the rows' x, r, M^-1 (all 512 columns: one block per SM).
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
-                     "r"(512u)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    tmem_fence_before();
-    __syncthreads();
-    tmem_fence_after();
     const bool row_owner = warp < kSlabConsumerWarps;  // the 384 threads of the per-row phases
     const int rt = tid;                                 // rows rt + 384 k
     const int krows = (m + kSlabRowThreads - 1) / kSlabRowThreads;
@@ -561,7 +584,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
             }
         }
         for (int w = tid; w < 3 * wn; w += blockDim.x) win[w] = 0.f;
-        if (!count_exchange<Acc, 2>(P.slots, gcount, gfirst, gsize, P.sync, ++xgen, v, bad, sh_acc, sh_int)) {
+        if (!count_exchange<Acc, 2>(slots, gcount, gfirst, gsize, P.sync, ++xgen, v, bad, sh_acc, sh_int)) {
             timed_out = true;
             goto finish;
         }
@@ -658,7 +681,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                 qbad = 1;
                 atomicExch(&P.sync->err, 1);
             }
-            count_publish<Acc, 1>(P.slots, gcount, gsize, ++xgen, dq, qbad, sh_acc, sh_int);
+            count_publish<Acc, 1>(slots, gcount, gsize, ++xgen, dq, qbad, sh_acc, sh_int);
             // Phase B's q (written by other threads in phase A, visible after the publish's
             // block barrier) loads while the exchange completes.
             V3<float> qv[kSlabRowsPerThread];
@@ -668,7 +691,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                 qv[k] = (row_owner && k < krows && i < m) ? ldv4(P.qs + 4 * (size_t)(row0 + i))
                                                           : V3<float>{0.f, 0.f, 0.f};
             }
-            if (!count_finish<Acc, 1>(P.slots, gcount, gfirst, gsize, P.sync, xgen, dq, qbad, sh_acc, sh_int)) {
+            if (!count_finish<Acc, 1>(slots, gcount, gfirst, gsize, P.sync, xgen, dq, qbad, sh_acc, sh_int)) {
                 timed_out = true;
                 goto finish;
             }
@@ -717,7 +740,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                 }
                 tmem_wait_st();
             }
-            if (!count_exchange<Acc, 2>(P.slots, gcount, gfirst, gsize, P.sync, ++xgen, v, sbad, sh_acc, sh_int)) {
+            if (!count_exchange<Acc, 2>(slots, gcount, gfirst, gsize, P.sync, ++xgen, v, sbad, sh_acc, sh_int)) {
                 timed_out = true;
                 goto finish;
             }
@@ -773,7 +796,7 @@ final_check:
                 }
             }
         }
-        if (!count_exchange<Acc, 1>(P.slots, gcount, gfirst, gsize, P.sync, ++xgen, none, bad, sh_acc, sh_int)) {
+        if (!count_exchange<Acc, 1>(slots, gcount, gfirst, gsize, P.sync, ++xgen, none, bad, sh_acc, sh_int)) {
             timed_out = true;
             goto finish;
         }
@@ -808,16 +831,13 @@ finish:
     if (producer && lane == 0) {
         for (unsigned k = 0; k < (unsigned)S && k < issued; ++k) {
             const unsigned p = issued - 1 - k;
-            (void)mbar_wait(&full_bar[p % S], (p / S) & 1u);
+            if (!mbar_wait(&full_bar[p % S], (p / S) & 1u)) s_stop = 1;
         }
     }
-    // Release the tensor memory once every warp's accesses are done.
+    // The next round rewrites the tensor memory once every warp's accesses are done.
     tmem_fence_before();
     __syncthreads();
-    if (warp == 0) {
-        tmem_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s_tmem), "r"(512u) : "memory");
-    }
+    tmem_fence_after();
     if (leader && tid == 0 && P.grouped) {
         // Per body; world-wide: the largest iteration count and residual, the OR of the
         // failure flags and the AND of the success flags (missing: what some body lacks).
@@ -840,6 +860,23 @@ finish:
         atomicOr(P.flags, fl);
     } else if (timed_out && tid == 0) {
         atomicOr(P.flags, kFlagBarrierTimeout);
+    }
+    if (s_stop) {  // read after the round's last block barrier: the same for every thread
+        if (tid == 0) {
+            atomicExch(&P.sync->err, 1);
+            atomicOr(P.flags, kFlagBarrierTimeout);
+        }
+        break;
+    }
+    }  // rounds
+    // Release the tensor memory once every warp's accesses are done.
+    if (!skip) {
+        tmem_fence_before();
+        __syncthreads();
+        if (warp == 0) {
+            tmem_fence_after();
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s_tmem), "r"(512u) : "memory");
+        }
     }
 }
 

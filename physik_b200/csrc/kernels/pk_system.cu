@@ -232,7 +232,8 @@ struct pk_system {
     int slab_tile_count = 0, slab_halo_count = 0;
     bool slab_for_bodies = false;   // the layout is the per-body one (batched solve)
     bool batch_slab = true;         // batched solve: part-resident kernel where it applies
-    std::vector<int> slab_launch;   // per-body layout: parts of each launch
+    int slab_rounds = 0;            // parts per block of the one launch (the per-body layout's rounds)
+    int slab_grid = 0;              // blocks of the launch
     DevBuf slab_part_body, slab_gcount;
     int slab_max_grid = 0;
     std::string slab_reason;      // why the layout does not apply
@@ -609,7 +610,31 @@ int ensure_slab(pk_system* s)
         s->slab_reason = why;
         return PK_OK;
     }
-    int rc = upload_raw<int>(s->slab_part_info, plan.part_info.data(), plan.part_info.size(), s->stream);
+    // The plan's launches become rounds of one launch: block b of round l takes part
+    // launch_start[l] + b (its group's block numbers are those of the launch), or none.
+    const int rounds = static_cast<int>(plan.launch_start.size()) - 1;
+    int widest = 1;
+    for (int l = 0; l < rounds; ++l) widest = std::max(widest, plan.launch_start[l + 1] - plan.launch_start[l]);
+    std::vector<int> round_info(static_cast<size_t>(rounds) * widest * pk::kSlabPartInts, 0);
+    std::vector<int> round_body(static_cast<size_t>(rounds) * widest, 0);
+    const char* snake_env = std::getenv("PK_SLAB_SNAKE");
+    const bool snake = snake_env && snake_env[0] == '1';
+    for (int l = 0; l < rounds; ++l)
+        for (int b = 0; b < widest; ++b) {
+            int* dst = round_info.data() + (static_cast<size_t>(l) * widest + b) * pk::kSlabPartInts;
+            const int k = plan.launch_start[l + 1] - plan.launch_start[l];
+            const bool rev = snake && (l & 1);
+            const int p = plan.launch_start[l] + (rev ? k - 1 - b : b);
+            if (b < k) {
+                std::copy_n(plan.part_info.data() + static_cast<size_t>(pk::kSlabPartInts) * p, pk::kSlabPartInts, dst);
+                if (rev) dst[6] = k - (dst[6] + dst[7]);
+                round_body[static_cast<size_t>(l) * widest + b] = plan.part_body[p];
+            } else {
+                dst[6] = pk::kSlabNoGroup;
+                dst[7] = 0;
+            }
+        }
+    int rc = upload_raw<int>(s->slab_part_info, round_info.data(), round_info.size(), s->stream);
     if (!rc) rc = upload_raw<int>(s->slab_tiles, plan.tile_desc.data(), plan.tile_desc.size(), s->stream);
     if (!rc) rc = upload_raw<unsigned char>(s->slab_stream, plan.stream.data(), plan.stream.size(), s->stream);
     if (!rc && !plan.halo_src.empty())
@@ -623,15 +648,14 @@ int ensure_slab(pk_system* s)
     }
     if (!rc) rc = upload_raw<unsigned>(s->slab_fill_src, plan.fill_src.data(), plan.fill_src.size(), s->stream);
     if (!rc) rc = upload_raw<int>(s->slab_tile_e0, plan.tile_entry0.data(), plan.tile_entry0.size(), s->stream);
-    if (!rc) rc = upload_raw<int>(s->slab_part_body, plan.part_body.data(), plan.part_body.size(), s->stream);
+    if (!rc) rc = upload_raw<int>(s->slab_part_body, round_body.data(), round_body.size(), s->stream);
     if (rc) return rc;
-    int widest = 1;
-    for (size_t l = 0; l + 1 < plan.launch_start.size(); ++l)
-        widest = std::max(widest, plan.launch_start[l + 1] - plan.launch_start[l]);
-    PK_CHECK(s->slab_gcount.ensure(sizeof(unsigned) * static_cast<size_t>(widest)));
-    PK_CHECK(s->slots.ensure(2 * sizeof(pk::ExSlot) * static_cast<size_t>(widest)));
+    const size_t round_blocks = static_cast<size_t>(rounds) * widest;
+    PK_CHECK(s->slab_gcount.ensure(sizeof(unsigned) * round_blocks));
+    PK_CHECK(s->slots.ensure(2 * sizeof(pk::ExSlot) * round_blocks));
     if (bodies) PK_CHECK(s->body_stats.ensure(sizeof(pk::BatchBodyStats) * s->seg_start.size()));
-    s->slab_launch = plan.launch_start;
+    s->slab_rounds = rounds;
+    s->slab_grid = widest;
     const size_t rows = static_cast<size_t>(n);
     PK_CHECK(s->slab_qs.ensure(16 * rows));
     PK_CHECK(s->slab_ss.ensure(16 * rows));
@@ -658,7 +682,7 @@ int run_pcg_slab(pk_system* s, const pk_step_params& p, int skip_on_flags)
     if constexpr (!std::is_same<Real, float>::value) {
         return fail(PK_ERR_UNSUPPORTED, "part-resident PCG: FP32 storage only");
     } else {
-        if (s->slab_parts <= 0 || s->slab_launch.size() < 2)
+        if (s->slab_parts <= 0 || s->slab_rounds < 1 || s->slab_grid < 1)
             return fail(PK_ERR_UNSUPPORTED, "part-resident PCG layout not available");
         const bool bodies = s->slab_for_bodies;
         const int nseg = static_cast<int>(s->seg_start.size()) - 1;
@@ -706,18 +730,17 @@ int run_pcg_slab(pk_system* s, const pk_step_params& p, int skip_on_flags)
         a.body_stats = bodies ? s->body_stats.as<pk::BatchBodyStats>() : nullptr;
         a.missing = &st->batch_missing;
         a.sym = s->slab_sym ? 1 : 0;
-        // One launch per group of parts (the coupled solve: one launch of all parts).
-        const int launches = static_cast<int>(s->slab_launch.size()) - 1;
-        for (int l = 0; l < launches; ++l) {
-            const int p0 = s->slab_launch[l], grid = s->slab_launch[l + 1] - p0;
-            PK_CHECK(cudaMemsetAsync(s->slots.p, 0, 2 * sizeof(pk::ExSlot) * static_cast<size_t>(grid), s->stream));
-            PK_CHECK(cudaMemsetAsync(s->slab_gcount.p, 0, sizeof(unsigned) * static_cast<size_t>(grid), s->stream));
-            PK_CHECK(cudaMemsetAsync(s->sync.p, 0, sizeof(pk::GridSync), s->stream));
-            a.part_info = s->slab_part_info.as<int>() + static_cast<size_t>(pk::kSlabPartInts) * p0;
-            a.part_body = s->slab_part_body.as<int>() + p0;
-            PK_CHECK(pk::launch_pcg_slab_kernel<Acc>(a, grid, s->stream));
-            s->launches += 1;
-        }
+        // One persistent launch: every block takes its part of each round in turn (the
+        // coupled solve: one round of all parts).
+        const size_t round_blocks = static_cast<size_t>(s->slab_rounds) * s->slab_grid;
+        PK_CHECK(cudaMemsetAsync(s->slots.p, 0, 2 * sizeof(pk::ExSlot) * round_blocks, s->stream));
+        PK_CHECK(cudaMemsetAsync(s->slab_gcount.p, 0, sizeof(unsigned) * round_blocks, s->stream));
+        PK_CHECK(cudaMemsetAsync(s->sync.p, 0, sizeof(pk::GridSync), s->stream));
+        a.rounds = s->slab_rounds;
+        a.part_info = s->slab_part_info.as<int>();
+        a.part_body = s->slab_part_body.as<int>();
+        PK_CHECK(pk::launch_pcg_slab_kernel<Acc>(a, s->slab_grid, s->stream));
+        s->launches += 1;
         s->last_kernel = bodies ? 5 : 3;
         s->last_blocks = s->slab_parts;
         return PK_OK;
