@@ -780,40 +780,57 @@ std::string build_slab_plan_batched(int n, const int* row_start, const int* col,
     std::vector<double> w(n);
     const double extra = row_weight_extra();
     for (int r = 0; r < n; ++r) w[r] = len[r] + extra;
-    // 0. the largest part to aim for.  A launch lasts about c0 + c1 * (its largest part's
-    // rows) per iteration (c0 the exchanges, c1 the streaming; measured on B200 about 12 us
-    // and 11 ns per row), so smaller parts can pay off although they take more launches:
-    // the estimate over the candidate caps, bodies packed as in step 2, picks the cap.
+    // 0. the largest part to aim for.  The launch takes the packed launches (step 2) as
+    // rounds, each block its part of every round in turn, odd rounds in reverse block order
+    // (the runtime's round table), and a body's group starts once all its blocks are free.
+    // Per iteration a part costs about c0 + c1 * rows (c1 the streaming, ~12 ns per row on
+    // B200; c0 the window pass, phase B and the exchanges: ~11 us for a group of several
+    // parts, ~5 us for a body of one part, which exchanges nothing).  The schedule of each
+    // candidate cap is simulated with these costs and the cap with the earliest finish wins.
     int cap = kSlabMaxRows;
     {
         double best = 1e300;
         for (int c : {kSlabMaxRows, 3400, 3000, 2800, 2600, 2400, 2200, 2000}) {
             if (c > kSlabMaxRows) continue;
-            std::vector<std::pair<double, int>> pb;  // (rows per part, parts) per body
+            struct Bp {
+                double rows;  // per part
+                int k;        // parts
+            };
+            std::vector<Bp> pb;
+            bool fits = true;
             for (int b = 0; b < nseg; ++b) {
                 const int rows = seg[b + 1] - seg[b];
                 if (rows <= 0) continue;
                 const int k = (rows + c - 1) / c;
-                if (k > max_blocks) continue;
+                if (k > max_blocks) fits = false;
                 pb.push_back({double(rows) / k, k});
             }
-            std::stable_sort(pb.begin(), pb.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+            if (!fits) continue;
+            std::stable_sort(pb.begin(), pb.end(), [](const Bp& x, const Bp& y) { return x.rows > y.rows; });
             std::vector<int> fill;
-            std::vector<double> widest;
-            for (const auto& q : pb) {
+            std::vector<std::vector<std::pair<int, int>>> members;  // per round: (body index in pb, first block)
+            for (int i = 0; i < static_cast<int>(pb.size()); ++i) {
                 size_t l = 0;
-                while (l < fill.size() && fill[l] + q.second > max_blocks) ++l;
+                while (l < fill.size() && fill[l] + pb[i].k > max_blocks) ++l;
                 if (l == fill.size()) {
                     fill.push_back(0);
-                    widest.push_back(0.0);
+                    members.emplace_back();
                 }
-                fill[l] += q.second;
-                widest[l] = std::max(widest[l], q.first);
+                members[l].push_back({i, fill[l]});
+                fill[l] += pb[i].k;
             }
-            double t = 0.0;
-            for (double wdt : widest) t += 12.0 + 0.011 * wdt;
-            if (t < best) {
-                best = t;
+            std::vector<double> free_at(static_cast<size_t>(max_blocks), 0.0);
+            for (size_t l = 0; l < fill.size(); ++l)
+                for (const auto& [i, first] : members[l]) {
+                    const int b0 = (l & 1) ? fill[l] - first - pb[i].k : first;
+                    double start = 0.0;
+                    for (int q = b0; q < b0 + pb[i].k; ++q) start = std::max(start, free_at[q]);
+                    const double t = start + (pb[i].k > 1 ? 11.0 : 5.0) + 0.012 * pb[i].rows;
+                    for (int q = b0; q < b0 + pb[i].k; ++q) free_at[q] = t;
+                }
+            const double finish = *std::max_element(free_at.begin(), free_at.end());
+            if (finish < best) {
+                best = finish;
                 cap = c;
             }
         }
@@ -880,8 +897,8 @@ std::string build_slab_plan_batched(int n, const int* row_start, const int* col,
             }
         }
     }
-    // 2. bodies into launches, largest parts first (a launch lasts as long as its slowest
-    // part), at most max_blocks parts per launch, a body never split across launches
+    // 2. bodies into launches (the rounds of the persistent launch), largest parts first,
+    // at most max_blocks parts per launch, a body never split across launches
     std::vector<int> order;
     for (int b = 0; b < nseg; ++b)
         if (body_parts[b] > 0) order.push_back(b);

@@ -114,8 +114,9 @@ std::string build_slab_plan(int n, const int* row_start, const int* col, const i
 // The layout for per-body solves: the rows split into bodies (segments
 // [seg[b], seg[b + 1]), no block coupling two bodies), every body cut by coordinate
 // bisection (NULL coords: contiguous ranges) into as few parts as its rows and window
-// allow, and the bodies packed, largest parts first, into launches of at most
-// max_blocks parts.  Returns "" on success, otherwise why the layout does not apply.
+// allow, and the bodies packed, largest parts first, into "launches" of at most
+// max_blocks parts (launch_start), which the runtime runs as the rounds of one persistent
+// launch.  Returns "" on success, otherwise why the layout does not apply.
 std::string build_slab_plan_batched(int n, const int* row_start, const int* col, const int* lt_start,
                                     const int* lt_row, const int* lt_block, const double* coords, const int* seg,
                                     int nseg, int max_blocks, SlabPlan& out, int form = kSlabAuto);

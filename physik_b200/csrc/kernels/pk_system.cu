@@ -611,19 +611,19 @@ int ensure_slab(pk_system* s)
         return PK_OK;
     }
     // The plan's launches become rounds of one launch: block b of round l takes part
-    // launch_start[l] + b (its group's block numbers are those of the launch), or none.
+    // launch_start[l] + b (its group's block numbers are those of the launch), or none;
+    // odd rounds in reverse block order, so the blocks with the largest parts of one round
+    // (the plan sorts a launch's parts largest first) get the smallest of the next.
     const int rounds = static_cast<int>(plan.launch_start.size()) - 1;
     int widest = 1;
     for (int l = 0; l < rounds; ++l) widest = std::max(widest, plan.launch_start[l + 1] - plan.launch_start[l]);
     std::vector<int> round_info(static_cast<size_t>(rounds) * widest * pk::kSlabPartInts, 0);
     std::vector<int> round_body(static_cast<size_t>(rounds) * widest, 0);
-    const char* snake_env = std::getenv("PK_SLAB_SNAKE");
-    const bool snake = snake_env && snake_env[0] == '1';
     for (int l = 0; l < rounds; ++l)
         for (int b = 0; b < widest; ++b) {
             int* dst = round_info.data() + (static_cast<size_t>(l) * widest + b) * pk::kSlabPartInts;
             const int k = plan.launch_start[l + 1] - plan.launch_start[l];
-            const bool rev = snake && (l & 1);
+            const bool rev = (l & 1) != 0;
             const int p = plan.launch_start[l] + (rev ? k - 1 - b : b);
             if (b < k) {
                 std::copy_n(plan.part_info.data() + static_cast<size_t>(pk::kSlabPartInts) * p, pk::kSlabPartInts, dst);
