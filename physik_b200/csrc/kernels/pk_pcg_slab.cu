@@ -547,27 +547,63 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     bool have_x = true;
     bool timed_out = false;
     Acc delta = Acc(0), rr = Acc(0), target = Acc(0);
+    // The first ring positions of the solve, issued before the initial pass so that
+    // iteration 0 starts on landed tiles (the stages are not touched until phase A).
+    if (producer && lane == 0) {
+        const unsigned end = (unsigned)min(S, ntiles);
+        for (; issued < end; ++issued) {
+            const int s = (int)issued;
+            const int4 d = table[issued];
+            mbar_arrive_expect_tx(&full_bar[s], (unsigned)d.y);
+            if (d.y > 0)
+                bulk_g2s_hint(ring_base + (size_t)s * stage_bytes, P.stream + 16 * (size_t)d.x, (unsigned)d.y,
+                              &full_bar[s], pol);
+        }
+    }
     {
         // x = 0, r = b, M^-1 into tensor memory; s = M^-1 r published; d = 0 in the window;
         // r.s, |r|^2, finiteness.
         Acc v[2] = {Acc(0), Acc(0)};
         int bad = s_bad ? 4 : 0;
         if (row_owner) {
+            // The rows' dynamic indices all in flight at once, then b and M^-1 of two rows
+            // at a time (a tensor-memory store orders the loads after it).
+            int cidx[kSlabRowsPerThread];
 #pragma unroll
             for (int k = 0; k < kSlabRowsPerThread; ++k) {
+                const int i = rt + kSlabRowThreads * k;
+                int c = 0;
+                if (k < krows && i < m) {
+                    c = __ldg(P.perm + row0 + i);
+                    if ((unsigned)c >= (unsigned)P.n) {
+                        c = 0;
+                        bad |= 4;
+                    }
+                }
+                cidx[k] = c;
+            }
+#pragma unroll
+            for (int k0 = 0; k0 < kSlabRowsPerThread; k0 += 2) {
+                if (k0 >= krows) break;
+                V3<float> brs[2]{};
+                M3<float> mis[2]{};
+#pragma unroll
+                for (int u = 0; u < 2; ++u)
+                    if (k0 + u < krows && rt + kSlabRowThreads * (k0 + u) < m) {
+                        brs[u] = ld3(P.b, cidx[k0 + u]);
+                        mis[u] = ld9(P.minv, (size_t)cidx[k0 + u]);
+                    }
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                const int k = k0 + u;
                 if (k >= krows) break;
                 const int i = rt + kSlabRowThreads * k;
                 RowRec rec{};
                 if (i < m) {
                     const int g = row0 + i;
-                    int c = __ldg(P.perm + g);
-                    if ((unsigned)c >= (unsigned)P.n) {
-                        c = 0;
-                        bad |= 4;
-                    }
-                    const V3<float> br = ld3(P.b, c);
+                    const V3<float> br = brs[u];
                     if (!finite3(br)) bad |= 1;
-                    const M3<float> mi = ld9(P.minv, (size_t)c);
+                    const M3<float> mi = mis[u];
                     const V3<float> sv = mul(mi, br);
                     if (!finite9(mi) || !finite3(sv)) bad |= 2;
                     put3(rec, 0, V3<float>{0.f, 0.f, 0.f});
@@ -581,6 +617,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                     v[1] += dot_acc<Acc>(br, br);
                 }
                 tmem_st16(tmem_row0 + 16u * (unsigned)k, rec);
+                }
             }
         }
         for (int w = tid; w < 3 * wn; w += blockDim.x) win[w] = 0.f;
@@ -769,30 +806,60 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
 final_check:
     // delta-v back in dynamic-row order; the solve succeeds when it is present and
     // finite; integration is all-or-nothing.
+    // The thread's row and node indices and delta-v stay in registers for the integration
+    // pass; row and node indices load all at once, node states two rows at a time.
     {
         int bad = 0;
         Acc none[1] = {Acc(0)};
-        if (row_owner) {
-            for (int k = 0; k < krows; ++k) {
-                const int i = rt + kSlabRowThreads * k;
-                RowRec rec;
-                tmem_ld16(tmem_row0 + 16u * (unsigned)k, rec);
-                if (i >= m) continue;
-                const int g = row0 + i;
-                const int c = __ldg(P.perm + g);
-                if ((unsigned)c >= (unsigned)P.n) {
+        const V3<float> zero{0.f, 0.f, 0.f};
+        int cidx[kSlabRowsPerThread], nidx[kSlabRowsPerThread];
+        V3<float> dvs[kSlabRowsPerThread];
+#pragma unroll
+        for (int k = 0; k < kSlabRowsPerThread; ++k) {
+            const int i = rt + kSlabRowThreads * k;
+            cidx[k] = -1;
+            nidx[k] = 0;
+            dvs[k] = zero;
+            if (row_owner && k < krows && i < m) {
+                const int c = __ldg(P.perm + row0 + i);
+                if ((unsigned)c >= (unsigned)P.n)
                     bad |= 1;
-                    continue;
-                }
-                const V3<float> dv = have_x ? rec3(rec, 0) : V3<float>{0.f, 0.f, 0.f};
-                st3(P.x, c, dv);
-                if (!finite3(dv)) bad |= 1;
-                if (P.integrate) {
-                    const int node = __ldg(P.dyn_to_node + c);
-                    const V3<float> xo = ldplain3(P.node_x, node), vo = ldplain3(P.node_v, node);
-                    const V3<float> nv = vo + dv;
-                    const V3<float> nx = xo + nv * P.dt;
-                    if (!finite3(xo) || !finite3(vo) || !finite3(nv) || !finite3(nx)) bad |= 2;
+                else
+                    cidx[k] = c;
+            }
+        }
+        if (P.integrate) {
+#pragma unroll
+            for (int k = 0; k < kSlabRowsPerThread; ++k)
+                if (cidx[k] >= 0) nidx[k] = __ldg(P.dyn_to_node + cidx[k]);
+        }
+        if (row_owner) {
+#pragma unroll
+            for (int k0 = 0; k0 < kSlabRowsPerThread; k0 += 2) {
+                if (k0 >= krows) break;
+                V3<float> xo[2] = {zero, zero}, vo[2] = {zero, zero};
+#pragma unroll
+                for (int u = 0; u < 2; ++u)
+                    if (P.integrate && cidx[k0 + u] >= 0) {
+                        xo[u] = ldplain3(P.node_x, nidx[k0 + u]);
+                        vo[u] = ldplain3(P.node_v, nidx[k0 + u]);
+                    }
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int k = k0 + u;
+                    if (k >= krows) break;
+                    RowRec rec;
+                    tmem_ld16(tmem_row0 + 16u * (unsigned)k, rec);  // warp-wide
+                    if (cidx[k] < 0) continue;
+                    const V3<float> dv = have_x ? rec3(rec, 0) : zero;
+                    dvs[k] = dv;
+                    st3(P.x, cidx[k], dv);
+                    if (!finite3(dv)) bad |= 1;
+                    if (P.integrate) {
+                        const V3<float> nv = vo[u] + dv;
+                        const V3<float> nx = xo[u] + nv * P.dt;
+                        if (!finite3(xo[u]) || !finite3(vo[u]) || !finite3(nv) || !finite3(nx)) bad |= 2;
+                    }
                 }
             }
         }
@@ -808,15 +875,23 @@ final_check:
             if (bad & 2) {
                 fl |= kFlagIntegrateAbort;
             } else {
-                for (int i = row_owner ? rt : m; i < m; i += kSlabRowThreads) {
-                    const int g = row0 + i;
-                    const int c = __ldg(P.perm + g);
-                    const int node = __ldg(P.dyn_to_node + c);
-                    const V3<float> dv = ldplain3(P.x, c);  // written above by this thread
-                    const V3<float> nv = ldplain3(P.node_v, node) + dv;
-                    const V3<float> nx = ldplain3(P.node_x, node) + nv * P.dt;
-                    st3(P.node_v, node, nv);
-                    st3(P.node_x, node, nx);
+#pragma unroll
+                for (int k0 = 0; k0 < kSlabRowsPerThread; k0 += 2) {
+                    V3<float> xo[2] = {zero, zero}, vo[2] = {zero, zero};
+#pragma unroll
+                    for (int u = 0; u < 2; ++u)
+                        if (cidx[k0 + u] >= 0) {
+                            vo[u] = ldplain3(P.node_v, nidx[k0 + u]);
+                            xo[u] = ldplain3(P.node_x, nidx[k0 + u]);
+                        }
+#pragma unroll
+                    for (int u = 0; u < 2; ++u)
+                        if (cidx[k0 + u] >= 0) {
+                            const V3<float> nv = vo[u] + dvs[k0 + u];
+                            const V3<float> nx = xo[u] + nv * P.dt;
+                            st3(P.node_v, nidx[k0 + u], nv);
+                            st3(P.node_x, nidx[k0 + u], nx);
+                        }
                 }
                 fl |= kFlagIntegrated;
             }
