@@ -328,10 +328,43 @@ static_assert(kSlabGroups * kSlabRowsPerThread * 16 <= 512, "row records must fi
 // A part_info row whose group is {kSlabNoGroup, 0}: the block has no part in that round.
 constexpr int kSlabNoGroup = -1;
 
+// Round table of the per-body (batched) launch, rebuilt on the device before every solve
+// from the previous solve's per-body iteration counts (pk_pcg_slab.cu,
+// slab_schedule_kernel).  Bodies are placed longest estimated solve first; a body of k
+// parts takes the k consecutive blocks that are free earliest (ties: the lowest first
+// block), all in one round: the round after the latest of those blocks' earlier rounds
+// (blocks that reach it sooner idle through the rounds in between, which costs them
+// nothing).  Estimated duration of a body: iterations x (c0 + kSlabSchedRowUs x its
+// largest part's rows), c0 = kSlabSchedMultiUs for several parts (grid exchanges),
+// kSlabSchedSingleUs for one -- per-iteration costs measured on B200; iterations = the
+// body's count in the previous solve, or the iteration cap before the first.
+constexpr int kSlabSchedThreads = 256;
+constexpr int kSlabSchedMaxGrid = 256;
+constexpr int kSlabSchedMaxSort = 2048;  // more bodies: placed in the host's order
+constexpr float kSlabSchedMultiUs = 8.0f, kSlabSchedSingleUs = 4.0f, kSlabSchedRowUs = 0.012f;
+
+struct SlabScheduleArgs {
+    int grid;                  // blocks of the launch (<= kSlabSchedMaxGrid)
+    int rounds;                // rounds of the table (>= the number of bodies placed)
+    int nbodies;               // bodies with rows
+    const int* body_part0;     // [nbodies] first part (plan numbering); a body's parts are consecutive
+    const int* body_parts;     // [nbodies] its parts
+    const int* plan_info;      // [parts] x kSlabPartInts
+    const int* plan_body;      // [parts]
+    const BatchBodyStats* body_stats;  // the previous solve's, by body id
+    int nstats;                // entries of body_stats
+    int max_iterations;
+    int* out_info;             // [rounds][grid] x kSlabPartInts
+    int* out_body;             // [rounds][grid]
+    int* out_rounds;           // [grid]: rounds each block runs
+    unsigned* flags;           // kFlagBreakdown when a body finds no room (the host sizes the table)
+};
+
 template <class Acc>
 struct SlabPcgArgs {
     int n;                       // dynamic rows
     int rounds;                  // parts per block, taken in order (1 for the coupled solve)
+    const int* block_rounds;     // [grid]: rounds block b runs (NULL: all)
     const int* part_info;        // [rounds][grid] x kSlabPartInts
     const int4* tile_desc;       // per tile: stream offset / 16, bytes, first local row, rows
     int tile_count;
@@ -510,6 +543,7 @@ int pcg_ring_max_grid();
 // Part-resident PCG (pk_pcg_slab.cu): cooperative, one block of kSlabThreads per part.
 template <class Acc>
 cudaError_t launch_pcg_slab_kernel(const SlabPcgArgs<Acc>& args, int grid, cudaStream_t stream);
+cudaError_t launch_slab_schedule_kernel(const SlabScheduleArgs& args, cudaStream_t stream);
 template <class Acc>
 int pcg_slab_max_grid();
 // Writes the assembled upper blocks and their transposes into the slab stream, tile by

@@ -200,7 +200,8 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     // proceed, and no group waits on a later one.
     bool bars_live = false;
     if (tid == 0) s_stop = 0;
-    for (int round = 0; round < P.rounds; ++round) {
+    const int my_rounds = P.block_rounds ? min(P.rounds, __ldg(P.block_rounds + blk)) : P.rounds;
+    for (int round = 0; round < my_rounds; ++round) {
     // The part: rows [row0, row0 + m) of the slab order, halo rows halo_src[halo0 ..
     // halo0 + h), tiles [tile0, tile0 + ntiles).  A part that does not fit the block's
     // tables (the host never builds one) is emptied and reports a breakdown.
@@ -997,9 +998,123 @@ __global__ void __launch_bounds__(kSlabFillThreads)
     }
 }
 
+// The round table of the per-body launch (SlabScheduleArgs).  Deterministic: fixed-order
+// float sums, ties broken by index, so the same iteration counts build the same table; a
+// body's result does not depend on the table.
+__global__ void __launch_bounds__(kSlabSchedThreads) slab_schedule_kernel(SlabScheduleArgs A)
+{
+    __shared__ float load[kSlabSchedMaxGrid];
+    __shared__ int count[kSlabSchedMaxGrid];
+    __shared__ int order[kSlabSchedMaxSort];
+    __shared__ float dur[kSlabSchedMaxSort];
+    const int tid = threadIdx.x, lane = tid & 31, G = A.grid, nb = A.nbodies;
+    if (G <= 0 || G > kSlabSchedMaxGrid || A.rounds < 1) {
+        if (tid == 0) atomicOr(A.flags, kFlagBreakdown);
+        return;
+    }
+    // estimated duration of body i (plan order)
+    auto body_dur = [&](int i) -> float {
+        const int p0 = A.body_part0[i], k = A.body_parts[i];
+        const int id = A.plan_body[p0];
+        float it = float(A.max_iterations);
+        if ((unsigned)id < (unsigned)A.nstats) {
+            const BatchBodyStats st = A.body_stats[id];
+            if (st.flags != 0u || st.iterations != 0) it = float(min(max(st.iterations, 0), A.max_iterations));
+        }
+        int rows = 0;
+        for (int q = 0; q < k; ++q) rows = max(rows, A.plan_info[(size_t)kSlabPartInts * (p0 + q) + 1]);
+        return it * ((k > 1 ? kSlabSchedMultiUs : kSlabSchedSingleUs) + kSlabSchedRowUs * float(rows));
+    };
+    // every entry idle; blocks free at time 0
+    for (int i = tid; i < A.rounds * G; i += blockDim.x) {
+        int* dst = A.out_info + (size_t)kSlabPartInts * i;
+        for (int q = 0; q < kSlabPartInts; ++q) dst[q] = 0;
+        dst[6] = kSlabNoGroup;
+        A.out_body[i] = 0;
+    }
+    for (int b = tid; b < G; b += blockDim.x) {
+        load[b] = 0.f;
+        count[b] = 0;
+    }
+    // bodies ranked longest first (ties: plan order)
+    const bool ranked = nb <= kSlabSchedMaxSort;
+    if (ranked)
+        for (int i = tid; i < nb; i += blockDim.x) dur[i] = body_dur(i);
+    __syncthreads();
+    if (ranked)
+        for (int i = tid; i < nb; i += blockDim.x) {
+            const float c = dur[i];
+            int rank = 0;
+            for (int j = 0; j < nb; ++j) rank += (dur[j] > c || (dur[j] == c && j < i)) ? 1 : 0;
+            order[rank] = i;
+        }
+    __syncthreads();
+    // one warp places them
+    if (tid < 32) {
+        for (int t = 0; t < nb; ++t) {
+            const int i = ranked ? order[t] : t;
+            const float d = ranked ? dur[i] : body_dur(i);
+            const int k = A.body_parts[i];
+            // the window [b, b + k) that is free earliest and has a round left
+            float best = INFINITY;
+            int bb = 0x7fffffff;
+            for (int b = lane; b + k <= G; b += 32) {
+                float st = 0.f;
+                int rd = 0;
+                for (int q = b; q < b + k; ++q) {
+                    st = fmaxf(st, load[q]);
+                    rd = max(rd, count[q]);
+                }
+                if (rd < A.rounds && (st < best || (st == best && b < bb))) {
+                    best = st;
+                    bb = b;
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const float ob = __shfl_xor_sync(0xffffffffu, best, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, bb, off);
+                if (ob < best || (ob == best && oi < bb)) {
+                    best = ob;
+                    bb = oi;
+                }
+            }
+            if (bb == 0x7fffffff) {  // no room: the host sized the table too small
+                if (lane == 0) atomicOr(A.flags, kFlagBreakdown);
+                break;
+            }
+            if (lane == 0) {
+                int r = 0;
+                for (int q = bb; q < bb + k; ++q) r = max(r, count[q]);
+                const int p0 = A.body_part0[i];
+                for (int q = 0; q < k; ++q) {
+                    const size_t e = (size_t)r * G + bb + q;
+                    int* dst = A.out_info + (size_t)kSlabPartInts * e;
+                    const int* src = A.plan_info + (size_t)kSlabPartInts * (p0 + q);
+                    for (int c = 0; c < 6; ++c) dst[c] = src[c];
+                    dst[6] = bb;  // the group: blocks [bb, bb + k) of round r
+                    dst[7] = k;
+                    A.out_body[e] = A.plan_body[p0 + q];
+                    count[bb + q] = r + 1;
+                    load[bb + q] = best + d;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    for (int b = tid; b < G; b += blockDim.x) A.out_rounds[b] = count[b];
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ launchers
+cudaError_t launch_slab_schedule_kernel(const SlabScheduleArgs& args, cudaStream_t stream)
+{
+    slab_schedule_kernel<<<1, kSlabSchedThreads, 0, stream>>>(args);
+    return cudaGetLastError();
+}
+
 template <class Acc>
 static cudaError_t slab_prepare()
 {

@@ -234,6 +234,9 @@ struct pk_system {
     bool batch_slab = true;         // batched solve: part-resident kernel where it applies
     int slab_rounds = 0;            // parts per block of the one launch (the per-body layout's rounds)
     int slab_grid = 0;              // blocks of the launch
+    // per-body layout: the round table is rebuilt on the device before every solve
+    int slab_sched_bodies = 0;
+    DevBuf slab_plan_info, slab_plan_body, slab_body_part0, slab_body_parts, slab_block_rounds;
     DevBuf slab_part_body, slab_gcount;
     int slab_max_grid = 0;
     std::string slab_reason;      // why the layout does not apply
@@ -610,30 +613,53 @@ int ensure_slab(pk_system* s)
         s->slab_reason = why;
         return PK_OK;
     }
-    // The plan's launches become rounds of one launch: block b of round l takes part
-    // launch_start[l] + b (its group's block numbers are those of the launch), or none;
-    // odd rounds in reverse block order, so the blocks with the largest parts of one round
-    // (the plan sorts a launch's parts largest first) get the smallest of the next.
-    const int rounds = static_cast<int>(plan.launch_start.size()) - 1;
+    // Coupled solve: one round, block b takes part b.  Per-body solves: the device
+    // scheduler (slab_schedule_kernel) places the bodies into the rounds of one launch
+    // before every solve, from the previous solve's iteration counts; the plan's launches
+    // only bound the blocks.
     int widest = 1;
-    for (int l = 0; l < rounds; ++l) widest = std::max(widest, plan.launch_start[l + 1] - plan.launch_start[l]);
-    std::vector<int> round_info(static_cast<size_t>(rounds) * widest * pk::kSlabPartInts, 0);
-    std::vector<int> round_body(static_cast<size_t>(rounds) * widest, 0);
-    for (int l = 0; l < rounds; ++l)
-        for (int b = 0; b < widest; ++b) {
-            int* dst = round_info.data() + (static_cast<size_t>(l) * widest + b) * pk::kSlabPartInts;
-            const int k = plan.launch_start[l + 1] - plan.launch_start[l];
-            const bool rev = (l & 1) != 0;
-            const int p = plan.launch_start[l] + (rev ? k - 1 - b : b);
-            if (b < k) {
-                std::copy_n(plan.part_info.data() + static_cast<size_t>(pk::kSlabPartInts) * p, pk::kSlabPartInts, dst);
-                if (rev) dst[6] = k - (dst[6] + dst[7]);
-                round_body[static_cast<size_t>(l) * widest + b] = plan.part_body[p];
-            } else {
-                dst[6] = pk::kSlabNoGroup;
-                dst[7] = 0;
-            }
+    for (size_t l = 0; l + 1 < plan.launch_start.size(); ++l)
+        widest = std::max(widest, plan.launch_start[l + 1] - plan.launch_start[l]);
+    const int PI = pk::kSlabPartInts;
+    int rounds = 1;
+    std::vector<int> round_info, round_body;
+    if (!bodies) {
+        round_info.assign(plan.part_info.begin(), plan.part_info.end());
+        round_body.assign(static_cast<size_t>(plan.parts), 0);
+        widest = plan.parts;
+        s->slab_sched_bodies = 0;
+    } else {
+        if (widest > pk::kSlabSchedMaxGrid) {
+            s->slab_reason = "more blocks than the round scheduler holds";
+            return PK_OK;
         }
+        std::vector<int> part0, nparts;
+        int kmax = 1;
+        for (int p = 0; p < plan.parts;) {
+            const int k = std::max(1, plan.part_info[static_cast<size_t>(PI) * p + 7]);
+            part0.push_back(p);
+            nparts.push_back(k);
+            kmax = std::max(kmax, k);
+            p += k;
+        }
+        const int nb = static_cast<int>(part0.size());
+        // rounds: every placement raises a block's count by at most one, and the bodies
+        // spread over the blocks a body of kmax parts leaves free
+        const int spread = (nb + std::max(1, widest - kmax) - 1) / std::max(1, widest - kmax);
+        rounds = std::max(1, std::min(nb, 4 * spread + 16));
+        s->slab_sched_bodies = nb;
+        int rc = upload_raw<int>(s->slab_plan_info, plan.part_info.data(), plan.part_info.size(), s->stream);
+        if (!rc) rc = upload_raw<int>(s->slab_plan_body, plan.part_body.data(), plan.part_body.size(), s->stream);
+        if (!rc) rc = upload_raw<int>(s->slab_body_part0, part0.data(), part0.size(), s->stream);
+        if (!rc) rc = upload_raw<int>(s->slab_body_parts, nparts.data(), nparts.size(), s->stream);
+        if (!rc) {
+            std::vector<int> zero_rounds(static_cast<size_t>(widest), 0);
+            rc = upload_raw<int>(s->slab_block_rounds, zero_rounds.data(), zero_rounds.size(), s->stream);
+        }
+        if (rc) return rc;
+        round_info.assign(static_cast<size_t>(rounds) * widest * PI, 0);  // written by the scheduler
+        round_body.assign(static_cast<size_t>(rounds) * widest, 0);
+    }
     int rc = upload_raw<int>(s->slab_part_info, round_info.data(), round_info.size(), s->stream);
     if (!rc) rc = upload_raw<int>(s->slab_tiles, plan.tile_desc.data(), plan.tile_desc.size(), s->stream);
     if (!rc) rc = upload_raw<unsigned char>(s->slab_stream, plan.stream.data(), plan.stream.size(), s->stream);
@@ -653,7 +679,12 @@ int ensure_slab(pk_system* s)
     const size_t round_blocks = static_cast<size_t>(rounds) * widest;
     PK_CHECK(s->slab_gcount.ensure(sizeof(unsigned) * round_blocks));
     PK_CHECK(s->slots.ensure(2 * sizeof(pk::ExSlot) * round_blocks));
-    if (bodies) PK_CHECK(s->body_stats.ensure(sizeof(pk::BatchBodyStats) * s->seg_start.size()));
+    if (bodies) {
+        // no earlier solve on this layout: the first round table assumes the iteration cap
+        const size_t bytes = sizeof(pk::BatchBodyStats) * s->seg_start.size();
+        PK_CHECK(s->body_stats.ensure(bytes));
+        PK_CHECK(cudaMemsetAsync(s->body_stats.p, 0, bytes, s->stream));
+    }
     s->slab_rounds = rounds;
     s->slab_grid = widest;
     const size_t rows = static_cast<size_t>(n);
@@ -688,9 +719,30 @@ int run_pcg_slab(pk_system* s, const pk_step_params& p, int skip_on_flags)
         const int nseg = static_cast<int>(s->seg_start.size()) - 1;
         int rc = ensure_solver_buffers(s, 1);
         if (rc) return rc;
-        if (bodies)
+        pk::DevStats* st = s->stats.as<pk::DevStats>();
+        if (bodies) {
+            // This solve's round table from the previous solve's iteration counts, then the
+            // counts are cleared for this solve.
+            pk::SlabScheduleArgs sa{};
+            sa.grid = s->slab_grid;
+            sa.rounds = s->slab_rounds;
+            sa.nbodies = s->slab_sched_bodies;
+            sa.body_part0 = s->slab_body_part0.as<int>();
+            sa.body_parts = s->slab_body_parts.as<int>();
+            sa.plan_info = s->slab_plan_info.as<int>();
+            sa.plan_body = s->slab_plan_body.as<int>();
+            sa.body_stats = s->body_stats.as<pk::BatchBodyStats>();
+            sa.nstats = nseg;
+            sa.max_iterations = p.max_iterations;
+            sa.out_info = s->slab_part_info.as<int>();
+            sa.out_body = s->slab_part_body.as<int>();
+            sa.out_rounds = s->slab_block_rounds.as<int>();
+            sa.flags = &st->flags;
+            PK_CHECK(pk::launch_slab_schedule_kernel(sa, s->stream));
+            s->launches += 1;
             PK_CHECK(cudaMemsetAsync(s->body_stats.p, 0, sizeof(pk::BatchBodyStats) * static_cast<size_t>(nseg),
                                      s->stream));
+        }
         if (!s->slab_filled) {
             rc = slab_fill(s);
             if (rc) return rc;
@@ -721,7 +773,6 @@ int run_pcg_slab(pk_system* s, const pk_step_params& p, int skip_on_flags)
         a.dyn_to_node = s->dyn_to_node.as<int>();
         a.node_x = s->x.as<float>();
         a.node_v = s->v.as<float>();
-        pk::DevStats* st = s->stats.as<pk::DevStats>();
         a.flags = &st->flags;
         a.stats = st;
         a.group_count = s->slab_gcount.as<unsigned>();
@@ -737,6 +788,7 @@ int run_pcg_slab(pk_system* s, const pk_step_params& p, int skip_on_flags)
         PK_CHECK(cudaMemsetAsync(s->slab_gcount.p, 0, sizeof(unsigned) * round_blocks, s->stream));
         PK_CHECK(cudaMemsetAsync(s->sync.p, 0, sizeof(pk::GridSync), s->stream));
         a.rounds = s->slab_rounds;
+        a.block_rounds = bodies ? s->slab_block_rounds.as<int>() : nullptr;
         a.part_info = s->slab_part_info.as<int>();
         a.part_body = s->slab_part_body.as<int>();
         PK_CHECK(pk::launch_pcg_slab_kernel<Acc>(a, s->slab_grid, s->stream));

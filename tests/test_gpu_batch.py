@@ -6,8 +6,10 @@ step of a one-body world: here against the FP64 oracle run on each body alone (f
 same float32 inputs the C ABI passes) and against the unbatched GPU path on each body
 alone.  Bodies differ in size (some are split over several blocks), stiffness, rotation
 and initial velocity, as in the batched uneven-bodies workload.  With FP32 storage the
-batched solve runs on the part-resident kernel with one group of parts per body (checked
-also when the bodies need several launches); the per-body batch kernel serves FP64.  Tolerances as in the
+batched solve runs on the part-resident kernel with one group of parts per body in one
+persistent launch (checked also when the bodies need several rounds of it, and with the
+round table the device rebuilds before every solve from the previous iteration counts);
+the per-body batch kernel serves FP64.  Tolerances as in the
 step parity tests: FP64 positions 1e-14 / velocities 1e-12, mixed positions 3e-7 against
 the FP64 oracle; CG iterations within one.
 """
@@ -142,7 +144,7 @@ def test_batched_toggle_back_to_coupled():
 @pytest.mark.parametrize("blocks", [0, 2])
 def test_batched_part_resident_kernel_matches_one_body_worlds(blocks):
     """Mixed precision, batched: the part-resident kernel with a group of parts per body.
-    blocks = 2 caps a launch at two parts, so the five bodies take three launches."""
+    blocks = 2 caps the launch at two blocks, so the five bodies take several rounds."""
     scene = uneven_bodies(count=5, seed=7)
     gpu = SimWorld(scene, precision="mixed")
     gpu.set_batched(True)
@@ -185,3 +187,33 @@ def test_batched_part_resident_agrees_with_batch_kernel(monkeypatch):
     assert rel(xs, xo) <= 1e-6
     for i in range(len(scene.bodies)):
         assert abs(slab.body_stats(i)["iterations"] - other.body_stats(i)["iterations"]) <= 2
+
+
+def test_batched_round_table_does_not_change_results():
+    """The device rebuilds the round table before every solve from the previous solve's
+    per-body iteration counts; a body's solve must not depend on where it is placed.  A
+    world that has stepped before (its table follows those counts) and a fresh world (its
+    first table assumes the iteration cap) step from the same state bit for bit alike."""
+    scene = uneven_bodies(count=6, seed=5)
+    warm = SimWorld(scene, precision="mixed")
+    warm.set_batched(True)
+    warm.step()
+    warm.set_pcg_grid(3)  # a new layout of three blocks
+    for _ in range(2):
+        warm.step()
+    x0, v0 = warm.state(f64=True)
+    fresh = SimWorld(scene, precision="mixed")
+    fresh.set_batched(True)
+    fresh.step()
+    fresh.set_pcg_grid(3)  # the layout is rebuilt at the next solve, with no counts yet
+    fresh.set_state(x0, v0, f64=True)
+    fresh.step()
+    warm.set_state(x0, v0, f64=True)
+    warm.step()
+    assert warm.pcg_kernel()[0] == "slab-batched" and fresh.pcg_kernel()[0] == "slab-batched"
+    xw, vw = warm.state(f64=True)
+    xf, vf = fresh.state(f64=True)
+    np.testing.assert_array_equal(xw, xf)
+    np.testing.assert_array_equal(vw, vf)
+    for i in range(len(scene.bodies)):
+        assert warm.body_stats(i)["iterations"] == fresh.body_stats(i)["iterations"]
