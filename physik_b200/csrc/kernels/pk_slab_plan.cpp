@@ -780,21 +780,22 @@ std::string build_slab_plan_batched(int n, const int* row_start, const int* col,
     std::vector<double> w(n);
     const double extra = row_weight_extra();
     for (int r = 0; r < n; ++r) w[r] = len[r] + extra;
-    // 0. the largest part to aim for.  The launch takes the packed launches (step 2) as
-    // rounds, each block its part of every round in turn, odd rounds in reverse block order
-    // (the runtime's round table), and a body's group starts once all its blocks are free.
-    // Per iteration a part costs about c0 + c1 * rows (c1 the streaming, ~12 ns per row on
-    // B200; c0 the window pass, phase B and the exchanges: ~11 us for a group of several
-    // parts, ~5 us for a body of one part, which exchanges nothing).  The schedule of each
-    // candidate cap is simulated with these costs and the cap with the earliest finish wins.
+    // 0. the largest part to aim for.  The runtime places the bodies on the launch's blocks
+    // before every solve, longest first, a body of k parts on the k consecutive blocks free
+    // earliest (slab_schedule_kernel); per iteration a body costs about c0 + c1 * its
+    // largest part's rows (c1 the streaming, ~12 ns per row on B200; c0 the window pass,
+    // phase B and the exchanges: ~8 us for a group of several parts, ~4 us for a body of
+    // one part, which exchanges nothing).  That placement is simulated for each candidate
+    // cap with every body at the same iteration count, and the cap with the earliest
+    // finish wins.
     int cap = kSlabMaxRows;
     {
         double best = 1e300;
         for (int c : {kSlabMaxRows, 3400, 3000, 2800, 2600, 2400, 2200, 2000}) {
             if (c > kSlabMaxRows) continue;
             struct Bp {
-                double rows;  // per part
-                int k;        // parts
+                double dur;  // per iteration
+                int k;       // parts
             };
             std::vector<Bp> pb;
             bool fits = true;
@@ -803,31 +804,24 @@ std::string build_slab_plan_batched(int n, const int* row_start, const int* col,
                 if (rows <= 0) continue;
                 const int k = (rows + c - 1) / c;
                 if (k > max_blocks) fits = false;
-                pb.push_back({double(rows) / k, k});
+                pb.push_back({(k > 1 ? 8.0 : 4.0) + 0.012 * std::ceil(double(rows) / k), k});
             }
             if (!fits) continue;
-            std::stable_sort(pb.begin(), pb.end(), [](const Bp& x, const Bp& y) { return x.rows > y.rows; });
-            std::vector<int> fill;
-            std::vector<std::vector<std::pair<int, int>>> members;  // per round: (body index in pb, first block)
-            for (int i = 0; i < static_cast<int>(pb.size()); ++i) {
-                size_t l = 0;
-                while (l < fill.size() && fill[l] + pb[i].k > max_blocks) ++l;
-                if (l == fill.size()) {
-                    fill.push_back(0);
-                    members.emplace_back();
-                }
-                members[l].push_back({i, fill[l]});
-                fill[l] += pb[i].k;
-            }
+            std::stable_sort(pb.begin(), pb.end(), [](const Bp& x, const Bp& y) { return x.dur > y.dur; });
             std::vector<double> free_at(static_cast<size_t>(max_blocks), 0.0);
-            for (size_t l = 0; l < fill.size(); ++l)
-                for (const auto& [i, first] : members[l]) {
-                    const int b0 = (l & 1) ? fill[l] - first - pb[i].k : first;
-                    double start = 0.0;
-                    for (int q = b0; q < b0 + pb[i].k; ++q) start = std::max(start, free_at[q]);
-                    const double t = start + (pb[i].k > 1 ? 11.0 : 5.0) + 0.012 * pb[i].rows;
-                    for (int q = b0; q < b0 + pb[i].k; ++q) free_at[q] = t;
+            for (const Bp& q : pb) {
+                int b0 = 0;
+                double start = 1e300;
+                for (int b = 0; b + q.k <= max_blocks; ++b) {
+                    double st = 0.0;
+                    for (int j = b; j < b + q.k; ++j) st = std::max(st, free_at[j]);
+                    if (st < start) {
+                        start = st;
+                        b0 = b;
+                    }
                 }
+                for (int j = b0; j < b0 + q.k; ++j) free_at[j] = start + q.dur;
+            }
             const double finish = *std::max_element(free_at.begin(), free_at.end());
             if (finish < best) {
                 best = finish;
