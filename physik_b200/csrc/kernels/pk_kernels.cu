@@ -302,7 +302,11 @@ template <class Real, int MAXU>
 __global__ void __launch_bounds__(128) row_lanes_kernel(AssemblyArgs<Real> A)
 {
     constexpr int LPR = 4, RPB = 128 / LPR, RS = RPB + 1;  // lanes per row, rows per block, slot stride
+    // A row's tet record passes through its warp's staging row: 16 bytes of padding per row
+    // put the 8 rows of a warp on different banks for the 16-byte accesses.
+    constexpr int kStride = kTetRec + 16 / int(sizeof(Real));
     __shared__ Real acc[MAXU * 9 * RS];
+    __shared__ __align__(16) Real stage[128 / 32][32 / LPR][kStride];
     const int tid = threadIdx.x, lane = tid & 31, lb = tid % LPR, rb = tid / LPR;
     const int base = lane - lb;  // lane 0 of this row within the warp
     const int r = blockIdx.x * RPB + rb;
@@ -358,10 +362,35 @@ __global__ void __launch_bounds__(128) row_lanes_kernel(AssemblyArgs<Real> A)
                 }
             }
         }
-        // record value v: element v % kPer of the row's lane v / kPer
+        // record value v: element v % kPer of the row's lane v / kPer, through shared memory
+        // (16-byte stores and loads instead of one shuffle per value)
+        Real* row_stage = &stage[tid >> 5][lane / LPR][0];
         Real w[kTetRec];
+        if constexpr (sizeof(Real) == 4) {
+            float4* dst = reinterpret_cast<float4*>(row_stage + lb * kPer);
+            dst[0] = make_float4(mine[0], mine[1], mine[2], mine[3]);
+            dst[1] = make_float4(mine[4], mine[5], mine[6], mine[7]);
+            __syncwarp();
 #pragma unroll
-        for (int v = 0; v < kTetRec; ++v) w[v] = shfl_row(mine[v % kPer], base + v / kPer);
+            for (int q = 0; q < kTetRec / 4; ++q) {
+                const float4 c = reinterpret_cast<const float4*>(row_stage)[q];
+                w[4 * q] = c.x;
+                w[4 * q + 1] = c.y;
+                w[4 * q + 2] = c.z;
+                w[4 * q + 3] = c.w;
+            }
+        } else {
+            double2* dst = reinterpret_cast<double2*>(row_stage + lb * kPer);
+#pragma unroll
+            for (int q = 0; q < kPer / 2; ++q) dst[q] = make_double2(mine[2 * q], mine[2 * q + 1]);
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < kTetRec / 2; ++q) {
+                const double2 c = reinterpret_cast<const double2*>(row_stage)[q];
+                w[2 * q] = c.x;
+                w[2 * q + 1] = c.y;
+            }
+        }
         const M3<Real> R = rd9(w);
         const bool work = live && !isnan(R.c[0].x);  // a skipped tet: no force, no stiffness
         if (work) {
