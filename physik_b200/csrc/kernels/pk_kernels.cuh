@@ -307,7 +307,9 @@ struct BatchPcgArgs {
 // and for the symmetric stream form the consumer groups' transposed-product rings.
 constexpr int kSlabGroupWarps = 4;
 constexpr int kSlabConsumerWarps = kSlabGroups * kSlabGroupWarps;
-constexpr int kSlabThreads = 32 * (kSlabConsumerWarps + 1);  // + one producer warp
+// + one producer warp (the stream) and one halo warp (the window's halo rows, while the
+// consumers stream the part's interior tiles)
+constexpr int kSlabThreads = 32 * (kSlabConsumerWarps + 2);
 constexpr size_t kSlabWinBytes = 12 * size_t(kSlabWinCap);
 constexpr size_t kSlabRingOffset = kSlabWinBytes;
 constexpr size_t kSlabTableOffset = kSlabRingOffset + size_t(kSlabStages) * kSlabStageBytes;

@@ -133,6 +133,20 @@ __device__ __forceinline__ M3<float> rec_minv(const RowRec& r)
     return m;
 }
 
+// Waits (bounded) until the shared-memory flag holds `want`; false when it gave up.
+__device__ __forceinline__ bool wait_flag_shared(const int* flag, int want)
+{
+    for (unsigned long long spins = 0; *(const volatile int*)flag != want; ++spins) {
+        if (spins > kBarrierSpinLimit) return false;
+        __nanosleep(32);
+    }
+    __threadfence_block();
+    return true;
+}
+
+// Named barrier of the consumer warps (the symmetric form's groups use 1 .. kSlabGroups).
+constexpr unsigned kSlabOwnBar = 1 + kSlabGroups;
+
 // alpha split into two floats, hi = float(alpha) and lo = float(alpha - hi), so that the
 // FP32 updates x + alpha d and r - alpha q take two FMAs per component instead of the
 // float -> double -> float round trip (24 conversions a row, which bound phase B: the
@@ -163,11 +177,13 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     __shared__ int s_fail;
     __shared__ int s_bad;
     __shared__ int s_stop;  // a bulk copy may still be in flight: no further round
+    __shared__ int s_halo_gen;  // the iteration whose window halo the halo warp has filled
     __shared__ unsigned s_tmem;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, blk = blockIdx.x;
     const bool producer = warp == kSlabConsumerWarps;
     const bool consumer = warp < kSlabConsumerWarps;
+    const bool halo_warp = warp == kSlabConsumerWarps + 1;
     const int group = warp / kSlabGroupWarps;
     const int slot_row = ((warp % kSlabGroupWarps) * 32 + lane) / LPR;  // tile row of this lane
     const int sub = lane % LPR;
@@ -235,6 +251,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
         mbar_fence_init();
         s_fail = 0;
         s_bad = 0;
+        s_halo_gen = 0;
     }
     bars_live = true;
     __syncthreads();
@@ -318,6 +335,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
     unsigned ring = 0;    // ring positions consumed so far (ntiles per iteration)
     unsigned issued = 0;  // ring positions issued by the producer (producer lane 0 only)
     unsigned xgen = 0;
+    int hgen = 0;         // window passes so far (the halo flag's generation)
 
     // Phase A of the symmetric form, for one consumer group: its ring positions are
     // ring + group, ring + group + 3, ... (ntiles is a multiple of 3 and ring starts at 0,
@@ -458,6 +476,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
         } else if (consumer) {
             const float* wv = win;
             const int wmax = max(wn - 1, 0);
+            bool halo_in = false;
             const unsigned first = ring + (unsigned)((group - (int)(ring % kSlabGroups) + kSlabGroups) % kSlabGroups);
             for (unsigned p = first; p < ring + (unsigned)ntiles; p += kSlabGroups) {
                 const int s = (int)(p % S);
@@ -470,6 +489,11 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                 const unsigned char* st = ring_base + (size_t)s * stage_bytes;
                 const int ne = d.y > 0 ? (d.y - kSlabHeaderBytes) / kSlabEntryBytes : 0;
                 const unsigned short* roff = reinterpret_cast<const unsigned short*>(st);
+                // the first tile with a halo column waits until the halo warp has filled it
+                if (!halo_in && d.y > 0 && roff[kSlabHaloWord] != 0) {
+                    if (!wait_flag_shared(&s_halo_gen, hgen)) s_fail = 1;
+                    halo_in = true;
+                }
                 const float* vals = reinterpret_cast<const float*>(st + kSlabHeaderBytes);
                 const unsigned short* lcol = reinterpret_cast<const unsigned short*>(st + kSlabHeaderBytes + 36 * ne);
                 const bool valid = slot_row < d.w;
@@ -661,7 +685,12 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                 break;
             }
             // Window: d = s + beta d -- the part's own rows from their owners' registers,
-            // the halo rows from the s their owners published.
+            // the halo rows from the s their owners published.  Full form: the consumers
+            // write the own rows and start on the part's interior tiles (interior rows come
+            // first) while the halo warp fills the halo and then raises the halo flag.
+            // Symmetric form: every thread takes halo rows, and a block barrier ends the pass.
+            int hbad = 0;
+            ++hgen;
             {
                 const float bt = float(beta);
                 if (row_owner) {
@@ -679,42 +708,53 @@ __global__ void __launch_bounds__(kSlabThreads, 1) pcg_slab_kernel(SlabPcgArgs<A
                 // kWinBatch halo entries per thread per pass: their indices, then their s
                 // values are all in flight before any is used.
                 constexpr int kWinBatch = 8;
-                const int step = (int)blockDim.x;
-                int wbad = 0;
-                for (int w0 = m + tid; w0 < wn; w0 += kWinBatch * step) {
-                    int g[kWinBatch];
+                if (sym || halo_warp) {
+                    const int step = sym ? (int)blockDim.x : 32;
+                    for (int w0 = m + (sym ? tid : lane); w0 < wn; w0 += kWinBatch * step) {
+                        int g[kWinBatch];
 #pragma unroll
-                    for (int k = 0; k < kWinBatch; ++k) {
-                        const int w = w0 + k * step;
-                        int gi = 0;
-                        if (w < wn) gi = __ldg(P.halo_src + halo0 + (w - m));
-                        if ((unsigned)gi >= (unsigned)P.n) {
-                            gi = 0;
-                            wbad = 1;
+                        for (int k = 0; k < kWinBatch; ++k) {
+                            const int w = w0 + k * step;
+                            int gi = 0;
+                            if (w < wn) gi = __ldg(P.halo_src + halo0 + (w - m));
+                            if ((unsigned)gi >= (unsigned)P.n) {
+                                gi = 0;
+                                hbad = 1;
+                            }
+                            g[k] = gi;
                         }
-                        g[k] = gi;
-                    }
-                    float4 sv[kWinBatch];
+                        float4 sv[kWinBatch];
 #pragma unroll
-                    for (int k = 0; k < kWinBatch; ++k) sv[k] = __ldcg(reinterpret_cast<const float4*>(P.ss) + g[k]);
+                        for (int k = 0; k < kWinBatch; ++k)
+                            sv[k] = __ldcg(reinterpret_cast<const float4*>(P.ss) + g[k]);
 #pragma unroll
-                    for (int k = 0; k < kWinBatch; ++k) {
-                        const int w = w0 + k * step;
-                        if (w < wn) {
-                            float* d = win + 3 * w;
-                            d[0] = sv[k].x + d[0] * bt;
-                            d[1] = sv[k].y + d[1] * bt;
-                            d[2] = sv[k].z + d[2] * bt;
+                        for (int k = 0; k < kWinBatch; ++k) {
+                            const int w = w0 + k * step;
+                            if (w < wn) {
+                                float* d = win + 3 * w;
+                                d[0] = sv[k].x + d[0] * bt;
+                                d[1] = sv[k].y + d[1] * bt;
+                                d[2] = sv[k].z + d[2] * bt;
+                            }
                         }
                     }
                 }
-                if (wbad) s_bad = 1;
+                if (!sym && halo_warp) {
+                    __syncwarp();
+                    if (lane == 0) {
+                        __threadfence_block();
+                        *(volatile int*)&s_halo_gen = hgen;
+                    }
+                }
             }
-            __syncthreads();
+            if (sym)
+                __syncthreads();
+            else if (row_owner)  // every own row is written before a consumer reads it
+                asm volatile("bar.sync %0, %1;" ::"r"(kSlabOwnBar), "r"(kSlabRowThreads) : "memory");
             Acc dq[1] = {Acc(0)};
             int qbad = 0;
             phase_a(dq[0], qbad);
-            if (s_bad) qbad = 1;
+            if (s_bad || hbad) qbad = 1;
             if (s_fail) {
                 qbad = 1;
                 atomicExch(&P.sync->err, 1);

@@ -145,7 +145,8 @@ std::string build_layout(int n, const int* row_start, const int* col, const int*
                          SlabPlan& out)
 {
     const int nnz = row_start[n];
-    // slab order: parts in order, rows ascending inside a part
+    // slab order: parts in order; inside a part the interior rows (every block's column in
+    // the part), then the others, each ascending
     std::vector<int> count(parts + 1, 0);
     for (int r = 0; r < n; ++r) ++count[part_of[r] + 1];
     for (int p = 0; p < parts; ++p) count[p + 1] += count[p];
@@ -154,12 +155,21 @@ std::string build_layout(int n, const int* row_start, const int* col, const int*
     out.perm.assign(n, 0);
     std::vector<int> inv(n);
     {
-        std::vector<int> fill(count.begin(), count.end() - 1);
+        std::vector<unsigned char> interior(n, 1);
         for (int r = 0; r < n; ++r) {
-            const int g = fill[part_of[r]]++;
-            out.perm[g] = r;
-            inv[r] = g;
+            for (int k = row_start[r]; k < row_start[r + 1] && interior[r]; ++k)
+                if (part_of[col[k]] != part_of[r]) interior[r] = 0;
+            for (int e = lt_start[r]; e < lt_start[r + 1] && interior[r]; ++e)
+                if (part_of[lt_row[e]] != part_of[r]) interior[r] = 0;
         }
+        std::vector<int> fill(count.begin(), count.end() - 1);
+        for (int pass = 1; pass >= 0; --pass)
+            for (int r = 0; r < n; ++r) {
+                if (interior[r] != pass) continue;
+                const int g = fill[part_of[r]]++;
+                out.perm[g] = r;
+                inv[r] = g;
+            }
     }
     out.n = n;
     out.parts = parts;
@@ -263,6 +273,7 @@ std::string build_layout(int n, const int* row_start, const int* col, const int*
                 for (const Entry& en : row_entries) {
                     src[j] = static_cast<unsigned>(en.block) | (en.lower ? kSlabLowerBit : 0u);
                     put_u16(out.stream, col_off + 2 * (size_t)j, (unsigned)en.win);
+                    if (en.win >= m) put_u16(out.stream, off + 2 * (size_t)kSlabHaloWord, 1u);
                     ++j;
                 }
             }

@@ -2,8 +2,9 @@
 //
 // The rows of the solve are split into parts, one per block of the cooperative launch
 // (one block per SM), by recursive coordinate bisection of the rows' node positions.  A
-// part owns a set of rows (consecutive in "slab order": parts in order, each part's rows
-// in ascending dynamic-row order); its window is its own rows followed by its halo (the
+// part owns a set of rows, consecutive in "slab order": parts in order; inside a part
+// first the interior rows (whose blocks all lie in the part), then the others, each in
+// ascending dynamic-row order.  Its window is its own rows followed by its halo (the
 // rows of other parts its rows couple to).  The search direction of the whole window
 // lives in shared memory for the whole solve, so the SpMV gathers only from shared memory.
 //
@@ -12,7 +13,8 @@
 // stored upper blocks (r, c) and the transposes of the lower ones (c, r) -- so no block is
 // fetched by another row.  A tile is one contiguous run of bytes that one TMA bulk copy
 // moves into a ring stage:
-//     [kSlabHeaderBytes: u16 row offsets, rows + 1 used]
+//     [kSlabHeaderBytes: u16 row offsets, rows + 1 used; u16 word kSlabHaloWord: 1 when a
+//      block of the tile has its column in the halo]
 //     [entries x 9 floats: the blocks, column-major]
 //     [entries x u16: window index of each block's column]
 // with the entry count padded to a multiple of 8 so both arrays start on 16-byte
@@ -82,6 +84,12 @@ static_assert((kSymRingSlots & (kSymRingSlots - 1)) == 0 && kSymRingSlots <= 655
 static_assert(kSlabCapE % 8 == 0, "entry cap must keep 16-byte alignment");
 static_assert(kSlabHeaderBytes % 16 == 0, "blocks must start on a 16-byte boundary");
 static_assert(2 * (kSlabRows + 1) <= kSlabHeaderBytes, "header too small");
+// Inside a part the rows whose blocks all lie in the part ("interior" rows) come first, so
+// a part's first tiles need no halo: the kernel streams them while the halo of the window
+// is still being filled, and waits for it only at the first tile whose header word
+// kSlabHaloWord is set.
+constexpr int kSlabHaloWord = kSlabHeaderBytes / 2 - 1;
+static_assert(kSlabHaloWord >= kSlabRows + 1, "the halo word must not overlap the row offsets");
 
 struct SlabPlan {
     int n = 0;
