@@ -384,9 +384,15 @@ __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v)
 // must have seen every block publish g + 1, which each does only after reading g.
 //
 // Split in two halves so a block can issue independent loads while it waits:
-// count_publish reduces the block's partials (ending with a block barrier, so every
-// store of the block made before it is visible to the block) and publishes them;
-// count_finish waits and reduces.  count_exchange is both.
+// count_publish reduces the block's partials and publishes them; count_finish waits and
+// reduces.  count_exchange is both.  Shared scratch (sh: 3 x 32 Acc, shi: 32 ints, at
+// most 16 warps): the warps' partials in sh[k * 32 + warp] / shi[warp], the group result
+// in sh[64 + k] / shi[16], shi[17], so the result of one exchange and the partials of the
+// next never share a word and neither half needs a barrier after its last read.  Within
+// a group of more than one block only warp 0 needs the block's sums (to publish them):
+// one block barrier, then warp 0 reduces the warp partials in the same fixed shuffle tree
+// as block_sum_or; the barrier also orders every store the block made before it ahead
+// of the release that publishes.
 //
 // A group is `size` consecutive blocks starting at block `first` that share one arrival
 // counter `counter` (zero at launch); the whole grid is the group (0, gridDim.x).  Slots
@@ -396,16 +402,41 @@ __device__ __forceinline__ void count_publish(ExSlot* slots, unsigned* counter, 
                                               int& bad, Acc* sh, int* shi)
 {
     static_assert(N >= 1 && N <= 2, "two partials per slot");
-    block_sum_or<Acc, N>(v, bad, sh, shi);
-    const int G = gridDim.x;
-    if (size > 1 && threadIdx.x == 0) {
-        ExSlot* my = slots + (gen & 1u) * (unsigned)G + blockIdx.x;
-        my->v0 = double(v[0]);
-        my->v1 = N > 1 ? double(v[N - 1]) : 0.0;
-        my->bad = bad;
-        // The release increment: a release is cumulative, so it also orders the block's
-        // stores that the block barrier ordered before it (no separate fence).
-        red_release_add(counter, 1u);
+    if (size <= 1) {  // no other block: every thread needs the block's sums
+        block_sum_or<Acc, N>(v, bad, sh, shi);
+        return;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], off);
+    bad = (int)__reduce_or_sync(0xffffffffu, (unsigned)bad);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) sh[k * 32 + warp] = v[k];
+        shi[warp] = bad;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            Acc t = lane < nw ? sh[k * 32 + lane] : Acc(0);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+            v[k] = t;
+        }
+        int b = lane < nw ? shi[lane] : 0;
+        b = (int)__reduce_or_sync(0xffffffffu, (unsigned)b);
+        if (lane == 0) {
+            ExSlot* my = slots + (gen & 1u) * (unsigned)gridDim.x + blockIdx.x;
+            my->v0 = double(v[0]);
+            my->v1 = N > 1 ? double(v[N - 1]) : 0.0;
+            my->bad = b;
+            // The release increment: a release is cumulative, so it also orders the
+            // block's stores that the block barrier ordered before it (no separate fence).
+            red_release_add(counter, 1u);
+        }
     }
 }
 
@@ -452,17 +483,16 @@ __device__ bool count_finish(ExSlot* slots, unsigned* counter, int first, int si
         pb = (int)__reduce_or_sync(0xffffffffu, (unsigned)pb);
         if (lane == 0) {
 #pragma unroll
-            for (int k = 0; k < N; ++k) sh[N * 32 + k] = pv[k];
-            shi[0] = pb;
-            shi[1] = fail;
+            for (int k = 0; k < N; ++k) sh[64 + k] = pv[k];
+            shi[16] = pb;
+            shi[17] = fail;
         }
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < N; ++k) v[k] = sh[N * 32 + k];
-    bad = shi[0];
-    const int failed = shi[1];
-    __syncthreads();
+    for (int k = 0; k < N; ++k) v[k] = sh[64 + k];
+    bad = shi[16];
+    const int failed = shi[17];
     return !failed && !*(volatile int*)&sync->err;
 }
 
