@@ -342,7 +342,7 @@ constexpr int kSlabNoGroup = -1;
 // body's count in the previous solve, or the iteration cap before the first.
 constexpr int kSlabSchedThreads = 256;
 constexpr int kSlabSchedMaxGrid = 256;
-constexpr int kSlabSchedMaxSort = 2048;  // more bodies: placed in the host's order
+constexpr int kSlabSchedMaxSort = 2048;  // bodies it places (more: the batched layout does not apply)
 constexpr float kSlabSchedMultiUs = 8.0f, kSlabSchedSingleUs = 4.0f, kSlabSchedRowUs = 0.012f;
 
 struct SlabScheduleArgs {

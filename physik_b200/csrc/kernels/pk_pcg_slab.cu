@@ -1047,25 +1047,15 @@ __global__ void __launch_bounds__(kSlabSchedThreads) slab_schedule_kernel(SlabSc
     __shared__ int count[kSlabSchedMaxGrid];
     __shared__ int order[kSlabSchedMaxSort];
     __shared__ float dur[kSlabSchedMaxSort];
+    __shared__ int nparts[kSlabSchedMaxSort];  // then: the round the body went to
+    __shared__ int first[kSlabSchedMaxSort];   // the first block it went to (-1: none)
     const int tid = threadIdx.x, lane = tid & 31, G = A.grid, nb = A.nbodies;
-    if (G <= 0 || G > kSlabSchedMaxGrid || A.rounds < 1) {
-        if (tid == 0) atomicOr(A.flags, kFlagBreakdown);
+    if (G <= 0 || G > kSlabSchedMaxGrid || A.rounds < 1 || nb > kSlabSchedMaxSort) {
+        if (tid == 0) atomicOr(A.flags, kFlagBreakdown);  // the host never builds such a table
         return;
     }
-    // estimated duration of body i (plan order)
-    auto body_dur = [&](int i) -> float {
-        const int p0 = A.body_part0[i], k = A.body_parts[i];
-        const int id = A.plan_body[p0];
-        float it = float(A.max_iterations);
-        if ((unsigned)id < (unsigned)A.nstats) {
-            const BatchBodyStats st = A.body_stats[id];
-            if (st.flags != 0u || st.iterations != 0) it = float(min(max(st.iterations, 0), A.max_iterations));
-        }
-        int rows = 0;
-        for (int q = 0; q < k; ++q) rows = max(rows, A.plan_info[(size_t)kSlabPartInts * (p0 + q) + 1]);
-        return it * ((k > 1 ? kSlabSchedMultiUs : kSlabSchedSingleUs) + kSlabSchedRowUs * float(rows));
-    };
-    // every entry idle; blocks free at time 0
+    // every entry idle; blocks free at time 0; each body's parts and estimated duration:
+    // iterations x (c0 + row cost of its largest part)
     for (int i = tid; i < A.rounds * G; i += blockDim.x) {
         int* dst = A.out_info + (size_t)kSlabPartInts * i;
         for (int q = 0; q < kSlabPartInts; ++q) dst[q] = 0;
@@ -1076,25 +1066,34 @@ __global__ void __launch_bounds__(kSlabSchedThreads) slab_schedule_kernel(SlabSc
         load[b] = 0.f;
         count[b] = 0;
     }
-    // bodies ranked longest first (ties: plan order)
-    const bool ranked = nb <= kSlabSchedMaxSort;
-    if (ranked)
-        for (int i = tid; i < nb; i += blockDim.x) dur[i] = body_dur(i);
-    __syncthreads();
-    if (ranked)
-        for (int i = tid; i < nb; i += blockDim.x) {
-            const float c = dur[i];
-            int rank = 0;
-            for (int j = 0; j < nb; ++j) rank += (dur[j] > c || (dur[j] == c && j < i)) ? 1 : 0;
-            order[rank] = i;
+    for (int i = tid; i < nb; i += blockDim.x) {
+        const int p0 = A.body_part0[i], k = A.body_parts[i];
+        const int id = A.plan_body[p0];
+        float it = float(A.max_iterations);
+        if ((unsigned)id < (unsigned)A.nstats) {
+            const BatchBodyStats st = A.body_stats[id];
+            if (st.flags != 0u || st.iterations != 0) it = float(min(max(st.iterations, 0), A.max_iterations));
         }
+        int rows = 0;
+        for (int q = 0; q < k; ++q) rows = max(rows, A.plan_info[(size_t)kSlabPartInts * (p0 + q) + 1]);
+        dur[i] = it * ((k > 1 ? kSlabSchedMultiUs : kSlabSchedSingleUs) + kSlabSchedRowUs * float(rows));
+        nparts[i] = k;
+        first[i] = -1;
+    }
     __syncthreads();
-    // one warp places them
+    // bodies ranked longest first (ties: plan order)
+    for (int i = tid; i < nb; i += blockDim.x) {
+        const float c = dur[i];
+        int rank = 0;
+        for (int j = 0; j < nb; ++j) rank += (dur[j] > c || (dur[j] == c && j < i)) ? 1 : 0;
+        order[rank] = i;
+    }
+    __syncthreads();
+    // one warp places them, from shared memory only
     if (tid < 32) {
         for (int t = 0; t < nb; ++t) {
-            const int i = ranked ? order[t] : t;
-            const float d = ranked ? dur[i] : body_dur(i);
-            const int k = A.body_parts[i];
+            const int i = order[t];
+            const int k = nparts[i];
             // the window [b, b + k) that is free earliest and has a round left
             float best = INFINITY;
             int bb = 0x7fffffff;
@@ -1126,23 +1125,32 @@ __global__ void __launch_bounds__(kSlabSchedThreads) slab_schedule_kernel(SlabSc
             if (lane == 0) {
                 int r = 0;
                 for (int q = bb; q < bb + k; ++q) r = max(r, count[q]);
-                const int p0 = A.body_part0[i];
-                for (int q = 0; q < k; ++q) {
-                    const size_t e = (size_t)r * G + bb + q;
-                    int* dst = A.out_info + (size_t)kSlabPartInts * e;
-                    const int* src = A.plan_info + (size_t)kSlabPartInts * (p0 + q);
-                    for (int c = 0; c < 6; ++c) dst[c] = src[c];
-                    dst[6] = bb;  // the group: blocks [bb, bb + k) of round r
-                    dst[7] = k;
-                    A.out_body[e] = A.plan_body[p0 + q];
-                    count[bb + q] = r + 1;
-                    load[bb + q] = best + d;
+                for (int q = bb; q < bb + k; ++q) {
+                    count[q] = r + 1;
+                    load[q] = best + dur[i];
                 }
+                nparts[i] = r;  // k is not needed any more: the round
+                first[i] = bb;
             }
             __syncwarp();
         }
     }
     __syncthreads();
+    // the table entries of the placed bodies, in parallel
+    for (int i = tid; i < nb; i += blockDim.x) {
+        const int bb = first[i];
+        if (bb < 0) continue;
+        const int r = nparts[i], p0 = A.body_part0[i], k = A.body_parts[i];
+        for (int q = 0; q < k; ++q) {
+            const size_t e = (size_t)r * G + bb + q;
+            int* dst = A.out_info + (size_t)kSlabPartInts * e;
+            const int* src = A.plan_info + (size_t)kSlabPartInts * (p0 + q);
+            for (int c = 0; c < 6; ++c) dst[c] = src[c];
+            dst[6] = bb;  // the group: blocks [bb, bb + k) of round r
+            dst[7] = k;
+            A.out_body[e] = A.plan_body[p0 + q];
+        }
+    }
     for (int b = tid; b < G; b += blockDim.x) A.out_rounds[b] = count[b];
 }
 

@@ -237,6 +237,11 @@ struct pk_system {
     // per-body layout: the round table is rebuilt on the device before every solve
     int slab_sched_bodies = 0;
     DevBuf slab_plan_info, slab_plan_body, slab_body_part0, slab_body_parts, slab_block_rounds;
+    // The round table is built on a side stream while the step assembles (fork at the
+    // step's start, join before the solve).
+    cudaStream_t sched_stream = nullptr;
+    cudaEvent_t sched_fork = nullptr, sched_join = nullptr;
+    bool sched_pending = false;
     DevBuf slab_part_body, slab_gcount;
     int slab_max_grid = 0;
     std::string slab_reason;      // why the layout does not apply
@@ -643,6 +648,10 @@ int ensure_slab(pk_system* s)
             p += k;
         }
         const int nb = static_cast<int>(part0.size());
+        if (nb > pk::kSlabSchedMaxSort) {
+            s->slab_reason = "more bodies than the round scheduler places";
+            return PK_OK;
+        }
         // rounds: every placement raises a block's count by at most one, and the bodies
         // spread over the blocks a body of kmax parts leaves free
         const int spread = (nb + std::max(1, widest - kmax) - 1) / std::max(1, widest - kmax);
@@ -659,6 +668,9 @@ int ensure_slab(pk_system* s)
         if (rc) return rc;
         round_info.assign(static_cast<size_t>(rounds) * widest * PI, 0);  // written by the scheduler
         round_body.assign(static_cast<size_t>(rounds) * widest, 0);
+        if (!s->sched_stream) PK_CHECK(cudaStreamCreateWithFlags(&s->sched_stream, cudaStreamNonBlocking));
+        if (!s->sched_fork) PK_CHECK(cudaEventCreateWithFlags(&s->sched_fork, cudaEventDisableTiming));
+        if (!s->sched_join) PK_CHECK(cudaEventCreateWithFlags(&s->sched_join, cudaEventDisableTiming));
     }
     int rc = upload_raw<int>(s->slab_part_info, round_info.data(), round_info.size(), s->stream);
     if (!rc) rc = upload_raw<int>(s->slab_tiles, plan.tile_desc.data(), plan.tile_desc.size(), s->stream);
@@ -707,6 +719,29 @@ int ensure_slab_any(pk_system* s)
     return PK_OK;
 }
 
+// The per-body round table for the next solve (slab_schedule_kernel) on `stream`.
+int launch_slab_schedule(pk_system* s, int max_iterations, cudaStream_t stream)
+{
+    pk::SlabScheduleArgs sa{};
+    sa.grid = s->slab_grid;
+    sa.rounds = s->slab_rounds;
+    sa.nbodies = s->slab_sched_bodies;
+    sa.body_part0 = s->slab_body_part0.as<int>();
+    sa.body_parts = s->slab_body_parts.as<int>();
+    sa.plan_info = s->slab_plan_info.as<int>();
+    sa.plan_body = s->slab_plan_body.as<int>();
+    sa.body_stats = s->body_stats.as<pk::BatchBodyStats>();
+    sa.nstats = static_cast<int>(s->seg_start.size()) - 1;
+    sa.max_iterations = max_iterations;
+    sa.out_info = s->slab_part_info.as<int>();
+    sa.out_body = s->slab_part_body.as<int>();
+    sa.out_rounds = s->slab_block_rounds.as<int>();
+    sa.flags = &s->stats.as<pk::DevStats>()->flags;
+    PK_CHECK(pk::launch_slab_schedule_kernel(sa, stream));
+    s->launches += 1;
+    return PK_OK;
+}
+
 template <class Real, class Acc>
 int run_pcg_slab(pk_system* s, const pk_step_params& p, int skip_on_flags)
 {
@@ -721,25 +756,16 @@ int run_pcg_slab(pk_system* s, const pk_step_params& p, int skip_on_flags)
         if (rc) return rc;
         pk::DevStats* st = s->stats.as<pk::DevStats>();
         if (bodies) {
-            // This solve's round table from the previous solve's iteration counts, then the
-            // counts are cleared for this solve.
-            pk::SlabScheduleArgs sa{};
-            sa.grid = s->slab_grid;
-            sa.rounds = s->slab_rounds;
-            sa.nbodies = s->slab_sched_bodies;
-            sa.body_part0 = s->slab_body_part0.as<int>();
-            sa.body_parts = s->slab_body_parts.as<int>();
-            sa.plan_info = s->slab_plan_info.as<int>();
-            sa.plan_body = s->slab_plan_body.as<int>();
-            sa.body_stats = s->body_stats.as<pk::BatchBodyStats>();
-            sa.nstats = nseg;
-            sa.max_iterations = p.max_iterations;
-            sa.out_info = s->slab_part_info.as<int>();
-            sa.out_body = s->slab_part_body.as<int>();
-            sa.out_rounds = s->slab_block_rounds.as<int>();
-            sa.flags = &st->flags;
-            PK_CHECK(pk::launch_slab_schedule_kernel(sa, s->stream));
-            s->launches += 1;
+            // This solve's round table from the previous solve's iteration counts (built on
+            // the side stream while the step assembled, or here), then the counts are
+            // cleared for this solve.
+            if (s->sched_pending) {
+                PK_CHECK(cudaStreamWaitEvent(s->stream, s->sched_join, 0));
+                s->sched_pending = false;
+            } else {
+                rc = launch_slab_schedule(s, p.max_iterations, s->stream);
+                if (rc) return rc;
+            }
             PK_CHECK(cudaMemsetAsync(s->body_stats.p, 0, sizeof(pk::BatchBodyStats) * static_cast<size_t>(nseg),
                                      s->stream));
         }
@@ -1166,6 +1192,17 @@ int run_step(pk_system* s, const pk_step_params& p)
 {
     if (const int rc = ensure_inc_slots(s)) return rc;
     PK_CHECK(cudaMemsetAsync(s->stats.p, 0, sizeof(pk::DevStats), s->stream));
+    // A per-body part-resident layout from an earlier step: its round table for this solve
+    // is built on the side stream while the step assembles.
+    s->sched_pending = false;
+    if (std::is_same<Real, float>::value && !p.explicit_mode && batched_solve(s) && s->batch_slab &&
+        s->slab_parts > 0 && s->slab_for_bodies && s->sched_stream && s->dyn_count > 0) {
+        PK_CHECK(cudaEventRecord(s->sched_fork, s->stream));
+        PK_CHECK(cudaStreamWaitEvent(s->sched_stream, s->sched_fork, 0));
+        if (const int rc = launch_slab_schedule(s, p.max_iterations, s->sched_stream)) return rc;
+        PK_CHECK(cudaEventRecord(s->sched_join, s->sched_stream));
+        s->sched_pending = true;
+    }
     int evi[3] = {-1, -1, -1};
     if (s->timing) {
         for (int i = 0; i < 3; ++i) {
@@ -1215,6 +1252,10 @@ int run_step(pk_system* s, const pk_step_params& p)
         else
             rc = refine ? run_pcg_refined<float, double>(s, p, 1) : run_pcg<float, double>(s, p, 1);
         if (rc) return rc;
+    }
+    if (s->sched_pending) {  // the solve did not take the table: join the side stream anyway
+        PK_CHECK(cudaStreamWaitEvent(s->stream, s->sched_join, 0));
+        s->sched_pending = false;
     }
     if (s->timing) {
         PK_CHECK(cudaEventRecord(s->ev_pool[evi[2]], s->stream));
@@ -1393,6 +1434,12 @@ PKCUDA_API int pk_system_destroy(pk_system* s)
     drop_graph(s);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
     if (s->host_stats) cudaFreeHost(s->host_stats);
+    if (s->sched_stream) {
+        cudaStreamSynchronize(s->sched_stream);
+        cudaStreamDestroy(s->sched_stream);
+    }
+    if (s->sched_fork) cudaEventDestroy(s->sched_fork);
+    if (s->sched_join) cudaEventDestroy(s->sched_join);
     cudaStreamDestroy(s->stream);
     delete s;
     return PK_OK;
