@@ -11,7 +11,14 @@
 //   an iteration every block rebuilds its window as d = s + beta d: its own rows from the
 //   s its threads keep in registers, the halo rows from the s the neighbouring parts
 //   published (a part publishes only the rows some other window holds), so the SpMV
-//   reads d only from shared memory.
+//   reads d only from shared memory.  A part's interior rows (no halo column) come first,
+//   and a halo warp fills the halo rows while the consumers already stream the interior
+//   tiles; a consumer waits for the halo only at the first tile whose header flags a
+//   halo column.
+// * Per-body solves run as one persistent launch: each block takes one part per round,
+//   in order, from a round table the device rebuilds before every solve
+//   (slab_schedule_kernel); a body of several parts is a group of consecutive blocks in
+//   one round with its own exchange slots and counter.
 // * The part's rows are streamed as tiles of full symmetric rows (upper blocks and the
 //   transposes of the lower ones, 16-bit window columns) by one producer warp, one TMA
 //   bulk copy per tile into a ring of stages, with an L2 evict-first policy so the
