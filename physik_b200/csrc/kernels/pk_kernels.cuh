@@ -332,9 +332,9 @@ constexpr int kSlabNoGroup = -1;
 
 // Round table of the per-body (batched) launch, rebuilt on the device before every solve
 // from the previous solve's per-body iteration counts (pk_pcg_slab.cu,
-// slab_schedule_kernel).  Bodies are placed longest estimated solve first; a body of k
-// parts takes the k consecutive blocks that are free earliest (ties: the lowest first
-// block), all in one round: the round after the latest of those blocks' earlier rounds
+// slab_schedule_kernel).  Bodies are placed largest estimated work (duration x parts)
+// first; a body of k parts takes the k consecutive blocks that are free earliest (ties:
+// the lowest first block), all in one round: the round after the latest of those blocks' earlier rounds
 // (blocks that reach it sooner idle through the rounds in between, which costs them
 // nothing).  Estimated duration of a body: iterations x (c0 + kSlabSchedRowUs x its
 // largest part's rows), c0 = kSlabSchedMultiUs for several parts (grid exchanges),

@@ -1088,11 +1088,15 @@ __global__ void __launch_bounds__(kSlabSchedThreads) slab_schedule_kernel(SlabSc
         first[i] = -1;
     }
     __syncthreads();
-    // bodies ranked longest first (ties: plan order)
+    // bodies ranked by estimated work, duration x parts, largest first (ties: plan order):
+    // a group needs several blocks free at once, which gets harder as the blocks fill
     for (int i = tid; i < nb; i += blockDim.x) {
-        const float c = dur[i];
+        const float wi = dur[i] * float(nparts[i]);
         int rank = 0;
-        for (int j = 0; j < nb; ++j) rank += (dur[j] > c || (dur[j] == c && j < i)) ? 1 : 0;
+        for (int j = 0; j < nb; ++j) {
+            const float wj = dur[j] * float(nparts[j]);
+            rank += (wj > wi || (wj == wi && j < i)) ? 1 : 0;
+        }
         order[rank] = i;
     }
     __syncthreads();

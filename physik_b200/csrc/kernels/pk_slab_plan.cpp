@@ -792,8 +792,8 @@ std::string build_slab_plan_batched(int n, const int* row_start, const int* col,
     const double extra = row_weight_extra();
     for (int r = 0; r < n; ++r) w[r] = len[r] + extra;
     // 0. the largest part to aim for.  The runtime places the bodies on the launch's blocks
-    // before every solve, longest first, a body of k parts on the k consecutive blocks free
-    // earliest (slab_schedule_kernel); per iteration a body costs about c0 + c1 * its
+    // before every solve, largest work (duration x parts) first, a body of k parts on the k
+    // consecutive blocks free earliest (slab_schedule_kernel); per iteration a body costs about c0 + c1 * its
     // largest part's rows (c1 the streaming, ~12 ns per row on B200; c0 the window pass,
     // phase B and the exchanges: ~8 us for a group of several parts, ~4 us for a body of
     // one part, which exchanges nothing).  That placement is simulated for each candidate
@@ -818,7 +818,8 @@ std::string build_slab_plan_batched(int n, const int* row_start, const int* col,
                 pb.push_back({(k > 1 ? 8.0 : 4.0) + 0.012 * std::ceil(double(rows) / k), k});
             }
             if (!fits) continue;
-            std::stable_sort(pb.begin(), pb.end(), [](const Bp& x, const Bp& y) { return x.dur > y.dur; });
+            std::stable_sort(pb.begin(), pb.end(),
+                             [](const Bp& x, const Bp& y) { return x.dur * x.k > y.dur * y.k; });
             std::vector<double> free_at(static_cast<size_t>(max_blocks), 0.0);
             for (const Bp& q : pb) {
                 int b0 = 0;
