@@ -1024,6 +1024,45 @@ void slab_spmv_host_sym(const SlabPlan& plan, const std::vector<unsigned char>& 
 
 }  // namespace
 
+std::string slab_check_halo_order(const SlabPlan& plan, const int* row_start, const int* col, const int* lt_start,
+                                  const int* lt_row)
+{
+    if (plan.sym) return "";
+    const int n = plan.n;
+    std::vector<int> part_of_slab(n, -1), inv(n, -1);
+    for (int g = 0; g < n; ++g) inv[plan.perm[g]] = g;
+    for (int p = 0; p < plan.parts; ++p) {
+        const int* pi = plan.part_info.data() + (size_t)kSlabPartInts * p;
+        for (int g = pi[0]; g < pi[0] + pi[1]; ++g) part_of_slab[g] = p;
+    }
+    for (int p = 0; p < plan.parts; ++p) {
+        const int* pi = plan.part_info.data() + (size_t)kSlabPartInts * p;
+        const int g0 = pi[0], m = pi[1], tile0 = pi[4], ntiles = pi[5];
+        bool seen_boundary = false;
+        for (int g = g0; g < g0 + m; ++g) {
+            const int r = plan.perm[g];
+            bool interior = true;
+            for (int k = row_start[r]; k < row_start[r + 1] && interior; ++k) interior = part_of_slab[inv[col[k]]] == p;
+            for (int e = lt_start[r]; e < lt_start[r + 1] && interior; ++e)
+                interior = part_of_slab[inv[lt_row[e]]] == p;
+            if (!interior) seen_boundary = true;
+            if (interior && seen_boundary) return "an interior row after a boundary row";
+        }
+        for (int t = 0; t < ntiles; ++t) {
+            const int* d = plan.tile_desc.data() + 4 * (size_t)(tile0 + t);
+            const size_t off = 16 * (size_t)d[0];
+            const int ne = (d[1] - kSlabHeaderBytes) / kSlabEntryBytes;
+            const size_t col_off = off + kSlabHeaderBytes + 36 * (size_t)ne;
+            const int e1 = get_u16(plan.stream, off + 2 * (size_t)d[3]);
+            bool halo = false;
+            for (int j = 0; j < e1; ++j) halo = halo || static_cast<int>(get_u16(plan.stream, col_off + 2 * (size_t)j)) >= m;
+            const bool flag = get_u16(plan.stream, off + 2 * (size_t)kSlabHaloWord) != 0;
+            if (flag != halo) return "a tile's halo flag does not match its columns";
+        }
+    }
+    return "";
+}
+
 void slab_spmv_host(const SlabPlan& plan, int nnz, const double* values, const double* x, double* y)
 {
     // Fill, as the fill kernel does (float storage).

@@ -133,4 +133,10 @@ std::string build_slab_plan_batched(int n, const int* row_start, const int* col,
 // the kernel's clamps), in double: the CPU self-check of a plan.
 void slab_spmv_host(const SlabPlan& plan, int nnz, const double* values, const double* x, double* y);
 
+// The full form's halo order, checked on the host: inside every part the interior rows
+// (every block's column in the part) precede the others, and a tile's header flags a halo
+// column exactly when one of its blocks has its column in the halo.  "" when it holds.
+std::string slab_check_halo_order(const SlabPlan& plan, const int* row_start, const int* col, const int* lt_start,
+                                  const int* lt_row);
+
 }  // namespace pk

@@ -2623,6 +2623,8 @@ PKCUDA_API int pk_slab_plan_batched_selfcheck(int n, const int* row_start, const
                 return fail(PK_ERR_STATE, "slab layout: part outside its body");
         }
     }
+    const std::string order = pk::slab_check_halo_order(plan, row_start, col_index, lts.data(), ltr.data());
+    if (!order.empty()) return fail(PK_ERR_STATE, "slab layout: " + order);
     pk::slab_spmv_host(plan, row_start[n], values, x, y);
     if (info) {
         info[0] = plan.parts;
@@ -2654,6 +2656,8 @@ PKCUDA_API int pk_slab_plan_selfcheck(int n, const int* row_start, const int* co
     const std::string why =
         pk::build_slab_plan(n, row_start, col_index, lts.data(), ltr.data(), ltb.data(), coords, parts, plan, form);
     if (!why.empty()) return fail(PK_ERR_UNSUPPORTED, "slab layout: " + why);
+    const std::string order = pk::slab_check_halo_order(plan, row_start, col_index, lts.data(), ltr.data());
+    if (!order.empty()) return fail(PK_ERR_STATE, "slab layout: " + order);
     pk::slab_spmv_host(plan, row_start[n], values, x, y);
     if (info) {
         info[0] = plan.parts;
