@@ -11,7 +11,9 @@ slots (decoded with the ring's wrap-around, so a slot reused too early would sho
 (SparseBlockMatrix::Multiply, src/Math/SparseBlockMatrix.cpp:209-268) computed with
 numpy, for patterns built by the drop-in host layer: structured boxes, the 128x64x64
 block cut into 148 parts (the B200's SM count), a randomly numbered body, several
-bodies, and parts cut without positions.
+bodies, and parts cut without positions.  In the full form the self-check also requires
+every part's interior rows (no halo column) ahead of its other rows and each tile's halo
+flag to match its columns: the kernel streams the interior tiles before the halo exists.
 """
 import ctypes as C
 
